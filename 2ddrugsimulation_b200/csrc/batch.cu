@@ -1,0 +1,631 @@
+// Batched ionic-model runtime: device memory layout, the init / run / rates
+// kernels for every model and precision, and the cep_batch_* C ABI
+// (include/cep_b200.h).
+//
+// HBM layout of a batch of n instances (ld = n rounded up to 32 so every
+// row starts on a 256-byte boundary and a warp's accesses coalesce):
+//   states  [n_states][ld] f64   SoA, the reference STATES order
+//   params  [n_params][ld] f64   per-instance constants (Hill-scaled)
+//   clock   t[ld] f64, iout[ld] i32, status[ld] i32
+//   sched   [4][ld] i32          imax, steps_per_bcl, print_freq, first_pace
+//   bm      [kNumF][ld] f64, [kNumI][ld] i32   biomarker state machine
+//   ca ring [cap][ld] f64 x2     cai samples of the current beat
+// A launch keeps one instance per thread with its whole state in registers
+// for n_steps steps; HBM is touched once per launch.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cep_b200.h"
+#include "biomarkers.cuh"
+#include "cep_device.cuh"
+#include "model_ord2011.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CEP_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) return fail(CEP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kBlock = 128;
+
+}  // namespace
+
+struct cep_batch {
+  int model = 0, n = 0, ns = 0, np = 0, precision = 0;
+  int64_t ld = 0;
+  cudaStream_t stream = nullptr;
+  double *states = nullptr, *params = nullptr, *t = nullptr;
+  int *iout = nullptr, *status = nullptr, *sched = nullptr;
+  double *bmf = nullptr, *ca_t = nullptr, *ca_v = nullptr;
+  int *bmi = nullptr;
+  int ca_cap = 0;
+  bool initialized = false, has_protocol = false;
+  double dt = 0.005, dt_write = 1.0, qnet_thr = -1e300;
+  int n_pace = 0, first_pace = -1;
+  int block = 128;  // threads per block of the run kernel
+  std::vector<void *> allocs;
+};
+
+namespace cep {
+
+// ------------------------------------------------------------------ traits
+struct OrdModel {
+  static constexpr int kStates = ord::kNumStates;
+  static constexpr int kParams = ord::kNumParams;
+  static constexpr int kCai = ord::cai;
+  template <class G> using Y = ord::Y<G>;
+  template <class G> using Par = ord::Par<G>;
+  template <class G> using Cur = ord::Cur<G>;
+  template <class G>
+  __device__ static void load(Y<G> &y, const double *s, int64_t ld, int64_t i) { ord::load(y, s, ld, i); }
+  template <class G>
+  __device__ static void store(const Y<G> &y, double *s, int64_t ld, int64_t i) { ord::store(y, s, ld, i); }
+  template <class G>
+  __device__ static void load_par(Par<G> &q, const double *p, int64_t ld, int64_t i) { ord::load_par(q, p, ld, i); }
+  template <class P>
+  __device__ static void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                              int stim_mode, bool update, Cur<typename P::G> &c) {
+    ord::step<P>(y, q, t, dt, stim_mode, update, c);
+  }
+  __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
+                              const double *hill, unsigned flags) {
+    ord::init_instance(par, s, ld, i, ct, conc, hill, flags & CEP_FLAG_DUTTA, flags & CEP_FLAG_QUIRKS);
+  }
+  template <class G>
+  __device__ static double cai_of(const Y<G> &y) { return y.cai; }
+  __host__ __device__ static constexpr int p_bcl() { return ord::P_BCL; }
+  __host__ __device__ static constexpr int p_stim_start() { return ord::P_stim_start; }
+  __host__ __device__ static constexpr int p_duration() { return ord::P_duration; }
+  __host__ __device__ static constexpr int p_amp() { return ord::P_amp; }
+};
+
+// ----------------------------------------------------------------- kernels
+template <class M>
+__global__ void init_kernel(double *par, double *s, int64_t ld, int n, const double *celltype,
+                            const double *conc, const double *hill, int hill_stride, unsigned flags) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  M::init(par, s, ld, i, celltype ? celltype[i] : 0.0, conc ? conc[i] : 0.0,
+          hill ? hill + i * hill_stride : nullptr, flags);
+}
+
+__global__ void pacing_kernel(double *par, int64_t ld, int n, int p_bcl, int p_start, int p_dur, int p_amp,
+                              double bcl, double start, double dur, double amp_scale) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  par[p_bcl * ld + i] = bcl;
+  if (start >= 0) par[p_start * ld + i] = start;
+  if (dur >= 0) par[p_dur * ld + i] = dur;
+  par[p_amp * ld + i] *= amp_scale;
+}
+
+struct RunArgs {
+  double *y;
+  const double *par;
+  int64_t ld;
+  int n;
+  double *t;
+  int *iout;
+  int *status;
+  const int *sched;  // [4][ld]
+  double dt;
+  int n_steps;
+  int bm_on;
+  bm::View bv;
+  double qnet_thr;
+  int stim_mode;  // -1 periodic; 0/1 fixed tissue flag
+};
+
+__global__ void reset_kernel(RunArgs a, int p_bcl, int p_start, int cai_idx) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  a.t[i] = 0.0;
+  a.iout[i] = 0;
+  a.status[i] = CEP_INST_RUNNING;
+  if (a.bm_on)
+    bm::reset(a.bv, i, a.y[i], a.y[cai_idx * a.ld + i], a.par[p_bcl * a.ld + i], a.par[p_start * a.ld + i],
+              a.dt);
+}
+
+// K fixed steps per instance with the biomarker state machine fused. One
+// thread per instance; state, parameters and counters live in registers.
+template <class M, class P>
+__global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
+  using G = typename P::G;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  int st = a.status[i];
+  if (st != CEP_INST_RUNNING) return;
+  typename M::template Y<G> y;
+  typename M::template Par<G> q;
+  M::template load<G>(y, a.y, a.ld, i);
+  M::template load_par<G>(q, a.par, a.ld, i);
+  double t = a.t[i];
+  int iout = a.iout[i];
+  const bm::Sched sc{a.sched[i], a.sched[a.ld + i], a.sched[2 * a.ld + i], a.sched[3 * a.ld + i]};
+  const bool bm_on = a.bm_on && sc.first_pace >= 0;
+  int cnt_print = sc.print_freq > 0 ? sc.print_freq - (iout % sc.print_freq) : 0x7fffffff;
+  int cnt_bcl = sc.steps_per_bcl > 0 ? sc.steps_per_bcl - (iout % sc.steps_per_bcl) : 0x7fffffff;
+  const double bcl = a.par[M::p_bcl() * a.ld + i];
+  const double stim_start = a.par[M::p_stim_start() * a.ld + i];
+  typename M::template Cur<G> c;
+  for (int k = 0; k <= a.n_steps; ++k) {
+    const bool can_update = iout < sc.imax;
+    if (can_update && k == a.n_steps) break;  // budget spent; sample iout is taken next launch
+    const double V0 = y.V;
+    const double cai0 = M::cai_of(y);
+    M::template step<P>(y, q, t, a.dt, a.stim_mode, can_update, c);
+    if (bm_on && iout >= 1)
+      bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
+                 (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
+                 cnt_print, cnt_bcl);
+    if (!can_update) {
+      st = CEP_INST_DONE;
+      break;
+    }
+    t += a.dt;
+    ++iout;
+    if (!isfinite(y.V)) {
+      st = CEP_INST_NONFINITE;
+      break;
+    }
+  }
+  M::template store<G>(y, a.y, a.ld, i);
+  a.t[i] = t;
+  a.iout[i] = iout;
+  a.status[i] = st;
+}
+
+// Rates at the current state (no update).
+template <class M>
+__global__ void rates_kernel(const double *s, const double *par, int64_t ld, int n, double t, int stim_mode,
+                             double *dvdt, double *cur) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  typename M::template Y<double> y;
+  typename M::template Par<double> q;
+  M::template load<double>(y, s, ld, i);
+  M::template load_par<double>(q, par, ld, i);
+  typename M::template Cur<double> c;
+  M::template step<F64>(y, q, t, 0.0, stim_mode, false, c);
+  if (dvdt) dvdt[i] = c.dVdt;
+  if (cur) {
+    cur[0 * (int64_t)n + i] = c.INa; cur[1 * (int64_t)n + i] = c.INaL; cur[2 * (int64_t)n + i] = c.Ito;
+    cur[3 * (int64_t)n + i] = c.ICaL; cur[4 * (int64_t)n + i] = c.IKr; cur[5 * (int64_t)n + i] = c.IKs;
+    cur[6 * (int64_t)n + i] = c.IK1;
+  }
+}
+
+__global__ void collect_bm_kernel(bm::View v, const int *status, int n, cep_biomarkers_t *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  cep_biomarkers_t r;
+  const int S = bm::F_S0;
+  r.qnet = v.F(S + bm::B_qnet, i) / 1000.0;
+  r.inal_auc = v.F(S + bm::B_inal, i);
+  r.ical_auc = v.F(S + bm::B_ical, i);
+  r.dvmdt_repol = v.F(S + bm::B_dvmdt_repol, i);
+  r.dvmdt_max = v.F(S + bm::B_dvmdt_max, i);
+  r.vm_peak = v.F(S + bm::B_vm_peak, i);
+  r.vm_valley = v.F(S + bm::B_vm_valley, i);
+  r.vm_dia = v.F(S + bm::B_vm_dia, i);
+  r.apd90 = v.F(S + bm::B_apd90, i);
+  r.apd50 = v.F(S + bm::B_apd50, i);
+  r.apd_tri = r.apd90 - r.apd50;
+  r.ca_peak = v.F(S + bm::B_ca_peak, i);
+  r.ca_valley = v.F(S + bm::B_ca_valley, i);
+  r.ca_dia = v.F(S + bm::B_ca_dia, i);
+  r.cad90 = v.F(S + bm::B_cad90, i);
+  r.cad50 = v.F(S + bm::B_cad50, i);
+  r.cad_tri = r.cad90 - r.cad50;
+  r.steepest_pace = v.I(bm::I_steepest, i);
+  r.n_eligible = v.I(bm::I_n_elig, i);
+  r.status = status[i];
+  r.reserved = 0;
+  out[i] = r;
+}
+
+// ------------------------------------------------------------- dispatch
+template <class M>
+struct Ops {
+  static int launch_init(cep_batch *b, const double *ct, const double *conc, const double *hill, int hs,
+                         unsigned flags) {
+    const int grid = (b->n + kBlock - 1) / kBlock;
+    init_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->params, b->states, b->ld, b->n, ct, conc, hill, hs, flags);
+    return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "init launch failed");
+  }
+  static int launch_pacing(cep_batch *b, double bcl, double start, double dur, double amp) {
+    const int grid = (b->n + kBlock - 1) / kBlock;
+    pacing_kernel<<<grid, kBlock, 0, b->stream>>>(b->params, b->ld, b->n, M::p_bcl(), M::p_stim_start(),
+                                                  M::p_duration(), M::p_amp(), bcl, start, dur, amp);
+    return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "pacing launch failed");
+  }
+  static int launch_reset(cep_batch *b, const RunArgs &a) {
+    const int grid = (b->n + kBlock - 1) / kBlock;
+    reset_kernel<<<grid, kBlock, 0, b->stream>>>(a, M::p_bcl(), M::p_stim_start(), M::kCai);
+    return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "reset launch failed");
+  }
+  static int launch_run(cep_batch *b, const RunArgs &a) {
+    const int block = b->block;
+    const int grid = (b->n + block - 1) / block;
+    if (b->precision == CEP_PREC_MIXED)
+      run_kernel<M, Mixed><<<grid, block, 0, b->stream>>>(a);
+    else
+      run_kernel<M, F64><<<grid, block, 0, b->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "run launch failed: %s", cudaGetErrorString(e));
+  }
+  static int launch_rates(cep_batch *b, double t, double *dvdt, double *cur) {
+    const int grid = (b->n + kBlock - 1) / kBlock;
+    rates_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->states, b->params, b->ld, b->n, t, -1, dvdt, cur);
+    return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "rates launch failed");
+  }
+};
+
+struct ModelInfo {
+  int ns, np, cai;
+  int (*init)(cep_batch *, const double *, const double *, const double *, int, unsigned);
+  int (*pacing)(cep_batch *, double, double, double, double);
+  int (*reset)(cep_batch *, const RunArgs &);
+  int (*run)(cep_batch *, const RunArgs &);
+  int (*rates)(cep_batch *, double, double *, double *);
+  int p_bcl;
+};
+
+const ModelInfo *model_info(int model) {
+  static const ModelInfo ord_info{OrdModel::kStates, OrdModel::kParams, OrdModel::kCai,
+                                  &Ops<OrdModel>::launch_init, &Ops<OrdModel>::launch_pacing,
+                                  &Ops<OrdModel>::launch_reset, &Ops<OrdModel>::launch_run,
+                                  &Ops<OrdModel>::launch_rates, OrdModel::p_bcl()};
+  switch (model) {
+    case CEP_MODEL_ORD2011: return &ord_info;
+    default: return nullptr;
+  }
+}
+
+}  // namespace cep
+
+using namespace cep;
+
+namespace {
+
+template <class T>
+int dev_alloc(cep_batch *b, T **p, size_t count) {
+  void *q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
+  if (e != cudaSuccess) return fail(CEP_ERR_OOM, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+  b->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return CEP_OK;
+}
+
+RunArgs make_args(cep_batch *b, long n_steps) {
+  RunArgs a;
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = b->t; a.iout = b->iout;
+  a.status = b->status; a.sched = b->sched; a.dt = b->dt; a.n_steps = (int)n_steps;
+  a.bm_on = (b->bmf != nullptr && b->first_pace >= 0) ? 1 : 0;
+  a.bv.f = b->bmf; a.bv.fi = b->bmi; a.bv.ca_t = b->ca_t; a.bv.ca_v = b->ca_v; a.bv.ca_cap = b->ca_cap;
+  a.bv.ld = b->ld;
+  a.qnet_thr = b->qnet_thr;
+  a.stim_mode = -1;
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cep_version(void) { return "cep_b200 0.1 (sm_100a)"; }
+const char *cep_last_error(void) { return g_last_error.c_str(); }
+
+int cep_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t *out) {
+  if (!out) return fail(CEP_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (n <= 0) return fail(CEP_ERR_ARG, "n must be positive (got %d)", n);
+  if (precision != CEP_PREC_FP64 && precision != CEP_PREC_MIXED) return fail(CEP_ERR_ARG, "bad precision %d", precision);
+  const ModelInfo *mi = model_info(model);
+  if (!mi) return fail(CEP_ERR_UNSUPPORTED, "model %d not built", model);
+  if (cep_device_count() == 0) return fail(CEP_ERR_NO_DEVICE, "no CUDA device visible");
+  cep_batch *b = new cep_batch();
+  b->model = model; b->n = n; b->ns = mi->ns; b->np = mi->np; b->precision = precision;
+  b->ld = ((int64_t)n + 31) / 32 * 32;
+  b->stream = static_cast<cudaStream_t>(stream);
+  // Launch shape: the run kernels hold ~250 registers per thread, so an SM
+  // keeps at most 8 warps. A population smaller than the GPU's resident
+  // capacity is spread as 1-warp blocks so that every SM gets work.
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    b->block = (n <= sms * 8 * 32) ? 32 : 128;
+  }
+  int rc = CEP_OK;
+  if ((rc = dev_alloc(b, &b->states, (size_t)b->ns * b->ld)) || (rc = dev_alloc(b, &b->params, (size_t)b->np * b->ld)) ||
+      (rc = dev_alloc(b, &b->t, (size_t)b->ld)) || (rc = dev_alloc(b, &b->iout, (size_t)b->ld)) ||
+      (rc = dev_alloc(b, &b->status, (size_t)b->ld)) || (rc = dev_alloc(b, &b->sched, (size_t)4 * b->ld))) {
+    cep_batch_destroy(b);
+    return rc;
+  }
+  cudaMemsetAsync(b->t, 0, sizeof(double) * b->ld, b->stream);
+  cudaMemsetAsync(b->iout, 0, sizeof(int) * b->ld, b->stream);
+  cudaMemsetAsync(b->status, 0, sizeof(int) * b->ld, b->stream);
+  // default schedule: unbounded run, biomarkers off
+  std::vector<int> sc((size_t)4 * b->ld, 0);
+  for (int64_t i = 0; i < b->ld; ++i) { sc[i] = 0x7fffffff; sc[3 * b->ld + i] = -1; }
+  if (cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cep_batch_destroy(b);
+    return fail(CEP_ERR_CUDA, "schedule upload failed");
+  }
+  *out = b;
+  return CEP_OK;
+}
+
+int cep_batch_destroy(cep_batch_t b) {
+  if (!b) return CEP_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream); else cudaDeviceSynchronize();
+  for (void *p : b->allocs) cudaFree(p);
+  delete b;
+  return CEP_OK;
+}
+
+int cep_batch_set_block(cep_batch_t b, int threads_per_block) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (threads_per_block != 32 && threads_per_block != 64 && threads_per_block != 96 && threads_per_block != 128)
+    return fail(CEP_ERR_ARG, "threads_per_block must be 32, 64, 96 or 128");
+  b->block = threads_per_block;
+  return CEP_OK;
+}
+
+int cep_batch_size(cep_batch_t b, int *n, int *n_states) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (n) *n = b->n;
+  if (n_states) *n_states = b->ns;
+  return CEP_OK;
+}
+
+int cep_batch_init(cep_batch_t b, const double *celltype, const double *conc, const double *hill, int hill_stride,
+                   unsigned flags) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (hill && hill_stride < 14) return fail(CEP_ERR_ARG, "hill_stride must be >= 14 (got %d)", hill_stride);
+  const ModelInfo *mi = model_info(b->model);
+  const int n = b->n;
+  // validate the drug inputs on the host: NaN/negative IC50 rows are rejected
+  if (conc)
+    for (int i = 0; i < n; ++i)
+      if (!(conc[i] >= 0.0) || !std::isfinite(conc[i])) return fail(CEP_ERR_ARG, "conc[%d] = %g is not a finite non-negative value", i, conc[i]);
+  if (hill)
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < hill_stride; ++k)
+        if (!std::isfinite(hill[(size_t)i * hill_stride + k]) || hill[(size_t)i * hill_stride + k] < 0.0)
+          if (k < 14) return fail(CEP_ERR_ARG, "hill[%d][%d] = %g is not a finite non-negative value", i, k, hill[(size_t)i * hill_stride + k]);
+  double *d_ct = nullptr, *d_conc = nullptr, *d_hill = nullptr;
+  const size_t bytes_h = hill ? (size_t)n * hill_stride * sizeof(double) : 0;
+  CEP_CUDA(cudaMallocAsync((void **)&d_ct, sizeof(double) * n * 2 + bytes_h + 64, b->stream));
+  d_conc = d_ct + n;
+  d_hill = hill ? d_conc + n : nullptr;
+  std::vector<double> zeros;
+  if (!celltype || !conc) zeros.assign(n, 0.0);
+  CEP_CUDA(cudaMemcpyAsync(d_ct, celltype ? celltype : zeros.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+  CEP_CUDA(cudaMemcpyAsync(d_conc, conc ? conc : zeros.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+  if (hill) CEP_CUDA(cudaMemcpyAsync(d_hill, hill, bytes_h, cudaMemcpyHostToDevice, b->stream));
+  int rc = mi->init(b, d_ct, d_conc, d_hill, hill_stride, flags);
+  CEP_CUDA(cudaFreeAsync(d_ct, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  if (rc) return rc;
+  b->initialized = true;
+  return CEP_OK;
+}
+
+int cep_batch_set_pacing(cep_batch_t b, double bcl, double stim_start, double stim_dur, double amp_scale) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (!(bcl > 0) || !std::isfinite(bcl)) return fail(CEP_ERR_ARG, "bcl must be positive");
+  return model_info(b->model)->pacing(b, bcl, stim_start, stim_dur, amp_scale);
+}
+
+int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,
+                           double qnet_vm_threshold) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (!(dt > 0) || !(dt_write > 0) || n_pace <= 0 || first_pace >= n_pace)
+    return fail(CEP_ERR_ARG, "bad protocol (dt=%g n_pace=%d first_pace=%d dt_write=%g)", dt, n_pace, first_pace, dt_write);
+  const ModelInfo *mi = model_info(b->model);
+  b->dt = dt; b->n_pace = n_pace; b->first_pace = first_pace; b->dt_write = dt_write;
+  b->qnet_thr = qnet_vm_threshold;
+  // per-instance loop bounds from each instance's BCL, computed as the
+  // reference computes them (cipa_drug_bench.cpp:136,188,240)
+  std::vector<double> bcl(b->n);
+  CEP_CUDA(cudaMemcpy(bcl.data(), b->params + (size_t)mi->p_bcl * b->ld, sizeof(double) * b->n, cudaMemcpyDeviceToHost));
+  std::vector<int> sc((size_t)4 * b->ld, 0);
+  const int print_freq = (int)((1. / dt) * dt_write);
+  int max_per_beat = 1;
+  for (int i = 0; i < b->n; ++i) {
+    sc[i] = (int)((n_pace * bcl[i]) / dt);
+    sc[b->ld + i] = (int)(bcl[i] / dt);
+    sc[2 * b->ld + i] = print_freq;
+    sc[3 * b->ld + i] = first_pace;
+    const int per_beat = print_freq > 0 ? sc[b->ld + i] / print_freq + 2 : 2;
+    if (per_beat > max_per_beat) max_per_beat = per_beat;
+  }
+  CEP_CUDA(cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (first_pace >= 0) {
+    if (!b->bmf) {
+      int rc;
+      if ((rc = dev_alloc(b, &b->bmf, (size_t)bm::kNumF * b->ld)) || (rc = dev_alloc(b, &b->bmi, (size_t)bm::kNumI * b->ld)))
+        return rc;
+    }
+    if (max_per_beat > b->ca_cap) {
+      int rc;
+      b->ca_cap = max_per_beat;
+      if ((rc = dev_alloc(b, &b->ca_t, (size_t)b->ca_cap * b->ld)) || (rc = dev_alloc(b, &b->ca_v, (size_t)b->ca_cap * b->ld)))
+        return rc;
+    }
+  }
+  b->has_protocol = true;
+  RunArgs a = make_args(b, 0);
+  int rc = mi->reset(b, a);
+  if (rc) return rc;
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_run(cep_batch_t b, long n_steps) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (n_steps < 0 || n_steps > 0x3fffffff) return fail(CEP_ERR_ARG, "n_steps out of range");
+  if (n_steps == 0) return CEP_OK;
+  RunArgs a = make_args(b, n_steps);
+  if (!b->has_protocol) a.bm_on = 0;
+  return model_info(b->model)->run(b, a);
+}
+
+int cep_batch_run_to_end(cep_batch_t b, long steps_per_launch) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->has_protocol) return fail(CEP_ERR_STATE, "cep_batch_set_protocol must come first");
+  if (steps_per_launch <= 0) steps_per_launch = 20000;
+  std::vector<int> st(b->n);
+  for (;;) {
+    int rc = cep_batch_run(b, steps_per_launch);
+    if (rc) return rc;
+    CEP_CUDA(cudaMemcpyAsync(st.data(), b->status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    CEP_CUDA(cudaStreamSynchronize(b->stream));
+    bool running = false;
+    for (int v : st) running |= (v == CEP_INST_RUNNING);
+    if (!running) break;
+  }
+  return CEP_OK;
+}
+
+int cep_batch_set_states(cep_batch_t b, const double *states, int layout) {
+  if (!b || !states) return fail(CEP_ERR_ARG, "null argument");
+  if (layout == CEP_LAYOUT_SOA) {
+    CEP_CUDA(cudaMemcpy2DAsync(b->states, sizeof(double) * b->ld, states, sizeof(double) * b->n,
+                               sizeof(double) * b->n, b->ns, cudaMemcpyHostToDevice, b->stream));
+  } else if (layout == CEP_LAYOUT_AOS) {
+    std::vector<double> soa((size_t)b->ns * b->n);
+    for (int i = 0; i < b->n; ++i)
+      for (int k = 0; k < b->ns; ++k) soa[(size_t)k * b->n + i] = states[(size_t)i * b->ns + k];
+    CEP_CUDA(cudaMemcpy2DAsync(b->states, sizeof(double) * b->ld, soa.data(), sizeof(double) * b->n,
+                               sizeof(double) * b->n, b->ns, cudaMemcpyHostToDevice, b->stream));
+    CEP_CUDA(cudaStreamSynchronize(b->stream));
+  } else {
+    return fail(CEP_ERR_ARG, "bad layout %d", layout);
+  }
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_get_states(cep_batch_t b, double *states, int layout) {
+  if (!b || !states) return fail(CEP_ERR_ARG, "null argument");
+  if (layout == CEP_LAYOUT_SOA) {
+    CEP_CUDA(cudaMemcpy2DAsync(states, sizeof(double) * b->n, b->states, sizeof(double) * b->ld,
+                               sizeof(double) * b->n, b->ns, cudaMemcpyDeviceToHost, b->stream));
+    CEP_CUDA(cudaStreamSynchronize(b->stream));
+  } else if (layout == CEP_LAYOUT_AOS) {
+    std::vector<double> soa((size_t)b->ns * b->n);
+    CEP_CUDA(cudaMemcpy2DAsync(soa.data(), sizeof(double) * b->n, b->states, sizeof(double) * b->ld,
+                               sizeof(double) * b->n, b->ns, cudaMemcpyDeviceToHost, b->stream));
+    CEP_CUDA(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < b->n; ++i)
+      for (int k = 0; k < b->ns; ++k) states[(size_t)i * b->ns + k] = soa[(size_t)k * b->n + i];
+  } else {
+    return fail(CEP_ERR_ARG, "bad layout %d", layout);
+  }
+  return CEP_OK;
+}
+
+int cep_batch_device_states(cep_batch_t b, void **dev_ptr, long *ld) {
+  if (!b || !dev_ptr) return fail(CEP_ERR_ARG, "null argument");
+  *dev_ptr = b->states;
+  if (ld) *ld = (long)b->ld;
+  return CEP_OK;
+}
+
+int cep_batch_get_biomarkers(cep_batch_t b, cep_biomarkers_t *out) {
+  if (!b || !out) return fail(CEP_ERR_ARG, "null argument");
+  if (!b->bmf) return fail(CEP_ERR_STATE, "biomarkers are off (set_protocol with first_pace >= 0)");
+  cep_biomarkers_t *d = nullptr;
+  CEP_CUDA(cudaMallocAsync((void **)&d, sizeof(cep_biomarkers_t) * b->n, b->stream));
+  bm::View v{b->bmf, b->bmi, b->ca_t, b->ca_v, b->ca_cap, b->ld};
+  collect_bm_kernel<<<(b->n + kBlock - 1) / kBlock, kBlock, 0, b->stream>>>(v, b->status, b->n, d);
+  CEP_CUDA(cudaGetLastError());
+  CEP_CUDA(cudaMemcpyAsync(out, d, sizeof(cep_biomarkers_t) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaFreeAsync(d, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_get_status(cep_batch_t b, int32_t *status) {
+  if (!b || !status) return fail(CEP_ERR_ARG, "null argument");
+  CEP_CUDA(cudaMemcpyAsync(status, b->status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_get_clock(cep_batch_t b, int i, long *step, double *t) {
+  if (!b || i < 0 || i >= b->n) return fail(CEP_ERR_ARG, "bad instance index");
+  int s = 0;
+  double tt = 0;
+  CEP_CUDA(cudaMemcpyAsync(&s, b->iout + i, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaMemcpyAsync(&tt, b->t + i, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  if (step) *step = s;
+  if (t) *t = tt;
+  return CEP_OK;
+}
+
+int cep_batch_sync(cep_batch_t b) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  double *d = nullptr;
+  CEP_CUDA(cudaMallocAsync((void **)&d, sizeof(double) * 8 * b->n, b->stream));
+  int rc = model_info(b->model)->rates(b, t, d, d + b->n);
+  if (rc) return rc;
+  if (dvdt) CEP_CUDA(cudaMemcpyAsync(dvdt, d, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  if (currents) CEP_CUDA(cudaMemcpyAsync(currents, d + b->n, sizeof(double) * 7 * b->n, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaFreeAsync(d, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+double cep_qinward(const cep_biomarkers_t *c, const cep_biomarkers_t *d) {
+  if (!c || !d) return NAN;
+  return ((d->inal_auc / c->inal_auc) + (d->ical_auc / c->ical_auc)) * 0.5;
+}
+
+}  // extern "C"

@@ -1,0 +1,529 @@
+// O'Hara-Rudy 2011 ventricular model, one cell per thread, register-resident
+// state, templated on the precision policy (cep_device.cuh).
+//
+// Equations and update scheme: DrugSimulation/cellmodels/Ohara_Rudy_2011.cpp
+// computeRates (:742-989) and the Rush-Larsen / forward-Euler branch of
+// solveAnalytical (:1036-1094). Model constants that do not depend on the
+// instance are compile-time constants here; the per-instance ones (celltype
+// scalings, Dutta scalings, Hill-scaled conductances, pacing) come from the
+// parameter block built by ord_init_kernel.
+#pragma once
+#include "cep_device.cuh"
+
+namespace cep {
+namespace ord {
+
+constexpr int kNumStates = 41;
+
+// STATES order of the reference (enums/enum_Ohara_Rudy_2011.hpp), which is
+// also the order of the C-ABI state arrays.
+enum : int {
+  V = 0, CaMKt, cass, nai, nass, ki, kss, cansr, cajsr, cai, m, hf, hs, j, hsp, jp, mL, hL, hLp, a,
+  iF, iS, ap, iFp, iSp, d, ff, fs, fcaf, fcas, jca, ffp, fcafp, nca, xrf, xrs, xs1, xs2, xk1,
+  Jrelnp, Jrelp
+};
+
+// Per-instance parameter block (one SoA row per entry).
+enum : int {
+  P_GNa = 0, P_GNaL, P_Gto, P_PCa, P_PCap, P_PCaNa, P_PCaK, P_PCaNap, P_PCaKp, P_GKr, P_GKs, P_GK1,
+  P_GKb, P_Gncx, P_Pnak, P_cmdnmax, P_upScale, P_Aff, P_Afs, P_tjca, P_H, P_celltype, P_fcafp_dt,
+  P_amp, P_BCL, P_stim_start, P_duration, kNumParams
+};
+
+// Instance-independent constants of ___initConsts (Ohara_Rudy_2011.cpp:494-678).
+namespace k {
+constexpr double nao = 140, cao = 1.8, ko = 5.4, R = 8314, T = 310, F = 96485, zna = 1, zca = 2, zk = 1;
+constexpr double L = 0.01, rad = 0.0011;
+constexpr double KmCaMK = 0.15, aCaMK = 0.05, bCaMK = 0.00068, CaMKo = 0.05, KmCaM = 0.0015;
+constexpr double kmcmdn = 0.00238, trpnmax = 0.07, kmtrpn = 0.0005, BSRmax = 0.047, KmBSR = 0.00087;
+constexpr double BSLmax = 1.124, KmBSL = 0.0087, csqnmax = 10, kmcsqn = 0.8, cm = 1, PKNa = 0.01833;
+constexpr double mssV1 = 39.57, mssV2 = 9.871, mtV1 = 11.64, mtV2 = 34.77, mtD1 = 6.765, mtD2 = 8.552;
+constexpr double mtV3 = 77.42, mtV4 = 5.955, hssV1 = 82.9, hssV2 = 6.086, Ahf = 0.99, Ahs = 1.0 - Ahf;
+constexpr double thL = 200, thLp = 3.0 * thL, Kmn = 0.002, k2n = 1000;
+constexpr double kna1 = 15, kna2 = 5, kna3 = 88.12, kasymm = 12.5, wna = 6e4, wca = 6e4, wnaca = 5e3;
+constexpr double kcaon = 1.5e6, kcaoff = 5e3, qna = 0.5224, qca = 0.167, KmCaAct = 150e-6;
+constexpr double k1p = 949.5, k1m = 182.4, k2p = 687.2, k2m = 39.4, k3p = 1899, k3m = 79300, k4p = 639;
+constexpr double k4m = 40, Knai0 = 9.073, Knao0 = 27.78, delta = -0.155, Kki = 0.5, Kko = 0.3582;
+constexpr double MgADP = 0.05, MgATP = 9.8, Kmgatp = 1.698e-7, eP = 4.2, Khp = 1.698e-7, Knap = 224;
+constexpr double Kxkur = 292, PNab = 3.75e-10, PCab = 2.5e-8, GpCa = 0.0005, KmCap = 0.0005, bt = 4.75;
+constexpr double a_rel = 0.5 * bt, btp = 1.25 * bt, a_relp = 0.5 * btp;
+constexpr double vcell = 1000.00 * 3.14000 * rad * rad * L;
+constexpr double Ageo = 2.0 * 3.14 * rad * rad + 2.0 * 3.14 * rad * L;
+constexpr double Acap = 2.0 * Ageo, vmyo = 0.68 * vcell, vnsr = 0.0552 * vcell;
+constexpr double vjsr = 0.0048 * vcell, vss = 0.02 * vcell;
+constexpr double h10 = kasymm + 1.0 + (nao / kna1) * (1.0 + nao / kna2);
+constexpr double h11 = (nao * nao) / (h10 * kna1 * kna2);
+constexpr double h12 = 1.0 / h10;
+constexpr double k1x = h12 * cao * kcaon, k2x = kcaoff, k5x = kcaoff;
+constexpr double b1 = k1m * MgADP, a2 = k2p;
+constexpr double a4 = ((k4p * MgATP) / Kmgatp) / (1.0 + MgATP / Kmgatp);
+constexpr double RTF = (R * T) / F;           // mV
+constexpr double FRT = F / (R * T);           // 1/mV
+constexpr double FFRT = F * F / (R * T);
+// ionic flux scalings of the RATES expressions
+constexpr double cAF_myo = cm * Acap / (F * vmyo), cAF_ss = cm * Acap / (F * vss);
+constexpr double sqrt_ko54 = 1.0;  // pow(ko/5.4, 1/2) with ko = 5.4
+constexpr double sqrt_ko = 2.32379000772445;  // pow(5.4, 1/2)
+constexpr double xk1_off = 2.55380 * ko + 144.590, xk1_den = 1.56920 * ko + 3.81150;
+constexpr double a3c = k3p * (ko / Kko) * (ko / Kko), ko_Kko_sq = (1.0 + ko / Kko) * (1.0 + ko / Kko);
+}  // namespace k
+
+template <class G>
+struct Y {
+  double V, CaMKt, cass, nai, nass, ki, kss, cansr, cajsr, cai;
+  G m, hf, hs, j, hsp, jp, mL, hL, hLp, a, iF, iS, ap, iFp, iSp, d, ff, fs, fcaf, fcas, jca, ffp,
+      fcafp, nca, xrf, xrs, xs1, xs2, xk1, Jrelnp, Jrelp;
+};
+
+template <class G>
+struct Par {
+  G GNa, GNaL, Gto, PCa, PCap, PCaNa, PCaK, PCaNap, PCaKp, GKr, GKs, GK1, GKb, Gncx, Pnak;
+  G cmdnmax, upScale, Aff, Afs, tjca, b3c;
+  G fcafp_dt;  // 0: use dt
+  int celltype;
+  double amp, BCL, stim_start, duration;
+};
+
+template <class G>
+struct Cur {
+  G INa, INaL, Ito, ICaL, IKr, IKs, IK1, dVdt;
+};
+
+// Loads/stores between the SoA arrays [kNumStates][ld] and registers.
+template <class G>
+__device__ __forceinline__ void load(Y<G> &y, const double *__restrict__ s, int64_t ld, int64_t i) {
+  y.V = s[V * ld + i]; y.CaMKt = s[CaMKt * ld + i]; y.cass = s[cass * ld + i];
+  y.nai = s[nai * ld + i]; y.nass = s[nass * ld + i]; y.ki = s[ki * ld + i];
+  y.kss = s[kss * ld + i]; y.cansr = s[cansr * ld + i]; y.cajsr = s[cajsr * ld + i];
+  y.cai = s[cai * ld + i];
+#define CEP_LD(n) y.n = (G)s[n * ld + i];
+  CEP_LD(m) CEP_LD(hf) CEP_LD(hs) CEP_LD(j) CEP_LD(hsp) CEP_LD(jp) CEP_LD(mL) CEP_LD(hL) CEP_LD(hLp)
+  CEP_LD(a) CEP_LD(iF) CEP_LD(iS) CEP_LD(ap) CEP_LD(iFp) CEP_LD(iSp) CEP_LD(d) CEP_LD(ff) CEP_LD(fs)
+  CEP_LD(fcaf) CEP_LD(fcas) CEP_LD(jca) CEP_LD(ffp) CEP_LD(fcafp) CEP_LD(nca) CEP_LD(xrf) CEP_LD(xrs)
+  CEP_LD(xs1) CEP_LD(xs2) CEP_LD(xk1) CEP_LD(Jrelnp) CEP_LD(Jrelp)
+#undef CEP_LD
+}
+
+template <class G>
+__device__ __forceinline__ void store(const Y<G> &y, double *__restrict__ s, int64_t ld, int64_t i) {
+  s[V * ld + i] = y.V; s[CaMKt * ld + i] = y.CaMKt; s[cass * ld + i] = y.cass;
+  s[nai * ld + i] = y.nai; s[nass * ld + i] = y.nass; s[ki * ld + i] = y.ki;
+  s[kss * ld + i] = y.kss; s[cansr * ld + i] = y.cansr; s[cajsr * ld + i] = y.cajsr;
+  s[cai * ld + i] = y.cai;
+#define CEP_ST(n) s[n * ld + i] = (double)y.n;
+  CEP_ST(m) CEP_ST(hf) CEP_ST(hs) CEP_ST(j) CEP_ST(hsp) CEP_ST(jp) CEP_ST(mL) CEP_ST(hL) CEP_ST(hLp)
+  CEP_ST(a) CEP_ST(iF) CEP_ST(iS) CEP_ST(ap) CEP_ST(iFp) CEP_ST(iSp) CEP_ST(d) CEP_ST(ff) CEP_ST(fs)
+  CEP_ST(fcaf) CEP_ST(fcas) CEP_ST(jca) CEP_ST(ffp) CEP_ST(fcafp) CEP_ST(nca) CEP_ST(xrf) CEP_ST(xrs)
+  CEP_ST(xs1) CEP_ST(xs2) CEP_ST(xk1) CEP_ST(Jrelnp) CEP_ST(Jrelp)
+#undef CEP_ST
+}
+
+template <class G>
+__device__ __forceinline__ void load_par(Par<G> &q, const double *__restrict__ p, int64_t ld, int64_t i) {
+  q.GNa = (G)p[P_GNa * ld + i]; q.GNaL = (G)p[P_GNaL * ld + i]; q.Gto = (G)p[P_Gto * ld + i];
+  q.PCa = (G)p[P_PCa * ld + i]; q.PCap = (G)p[P_PCap * ld + i]; q.PCaNa = (G)p[P_PCaNa * ld + i];
+  q.PCaK = (G)p[P_PCaK * ld + i]; q.PCaNap = (G)p[P_PCaNap * ld + i];
+  q.PCaKp = (G)p[P_PCaKp * ld + i]; q.GKr = (G)p[P_GKr * ld + i]; q.GKs = (G)p[P_GKs * ld + i];
+  q.GK1 = (G)p[P_GK1 * ld + i]; q.GKb = (G)p[P_GKb * ld + i]; q.Gncx = (G)p[P_Gncx * ld + i];
+  q.Pnak = (G)p[P_Pnak * ld + i]; q.cmdnmax = (G)p[P_cmdnmax * ld + i];
+  q.upScale = (G)p[P_upScale * ld + i]; q.Aff = (G)p[P_Aff * ld + i]; q.Afs = (G)p[P_Afs * ld + i];
+  q.tjca = (G)p[P_tjca * ld + i];
+  // b3 = k3m * P * H / (1 + MgATP/Kmgatp): fold the instance's H (the Dutta
+  // quirk scales H) into one factor.
+  q.b3c = (G)((k::k3m * 1.0) * p[P_H * ld + i] / (1.0 + k::MgATP / k::Kmgatp));
+  q.fcafp_dt = (G)p[P_fcafp_dt * ld + i];
+  q.celltype = (int)p[P_celltype * ld + i];
+  q.amp = p[P_amp * ld + i]; q.BCL = p[P_BCL * ld + i];
+  q.stim_start = p[P_stim_start * ld + i]; q.duration = p[P_duration * ld + i];
+}
+
+// Periodic single-cell stimulus of computeRates (Ohara_Rudy_2011.cpp:747);
+// stim_mode >= 0 selects the tissue form (isS1, :745).
+__device__ __forceinline__ bool stim_on(double t, double start, double bcl, double dur) {
+  return t >= start && (t - start) - floor((t - start) / bcl) * bcl <= dur;
+}
+
+// One cell step: rates at (t, y); if `update`, the Rush-Larsen / forward
+// Euler update of y by dt. `cur` receives the currents at (t, y).
+template <class P>
+__device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                                     int stim_mode, bool update, Cur<typename P::G> &cur) {
+  using G = typename P::G;
+  const G v = (G)y.V;
+  const G one = (G)1;
+  const bool on = stim_mode < 0 ? stim_on(t, q.stim_start, q.BCL, q.duration) : (stim_mode != 0);
+  const G Istim = on ? (G)q.amp : (G)0;
+  // gate steady states and time constants
+  const G hLss = one / (one + P::ex((v + (G)87.61) * (G)(1.0 / 7.488)));
+  const G hLssp = one / (one + P::ex((v + (G)93.81) * (G)(1.0 / 7.488)));
+  const G mss = one / (one + P::ex(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2)));
+  const G tm = one / ((G)k::mtD1 * P::ex((v + (G)k::mtV1) * (G)(1.0 / k::mtV2)) +
+                      (G)k::mtD2 * P::ex(-(v + (G)k::mtV3) * (G)(1.0 / k::mtV4)));
+  const G hss = one / (one + P::ex((v + (G)k::hssV1) * (G)(1.0 / k::hssV2)));
+  const G thf = one / ((G)1.432e-05 * P::ex(-(v + (G)1.196) * (G)(1.0 / 6.285)) +
+                       (G)6.149 * P::ex((v + (G)0.5096) * (G)(1.0 / 20.27)));
+  const G ths = one / ((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
+                       (G)0.3343 * P::ex((v + (G)5.73) * (G)(1.0 / 56.66)));
+  const G ass = one / (one + P::ex(-(v - (G)14.34) * (G)(1.0 / 14.82)));
+  const G ta = (G)1.0515 / (one / ((G)1.2089 * (one + P::ex(-(v - (G)18.4099) * (G)(1.0 / 29.3814)))) +
+                            (G)3.5 / (one + P::ex((v + (G)100.0) * (G)(1.0 / 29.3814))));
+  const G dss = one / (one + P::ex(-(v + (G)3.94) * (G)(1.0 / 4.23)));
+  const G td = (G)0.6 + one / (P::ex((G)-0.05 * (v + (G)6.0)) + P::ex((G)0.09 * (v + (G)14.0)));
+  const G fss = one / (one + P::ex((v + (G)19.58) * (G)(1.0 / 3.696)));
+  const G tff = (G)7.0 + one / ((G)0.0045 * P::ex(-(v + (G)20.0) * (G)0.1) + (G)0.0045 * P::ex((v + (G)20.0) * (G)0.1));
+  const G tfs = (G)1000.0 + one / ((G)3.5e-05 * P::ex(-(v + (G)5.0) * (G)0.25) +
+                                   (G)3.5e-05 * P::ex((v + (G)5.0) * (G)(1.0 / 6.0)));
+  const G fcass = fss;
+  const G km2n = y.jca;
+  const G cass_g = (G)y.cass;
+  const G anca = one / ((G)k::k2n / km2n + p4(one + (G)k::Kmn / cass_g));
+  const G xrss = one / (one + P::ex(-(v + (G)8.337) * (G)(1.0 / 6.789)));
+  const G txrf = (G)12.98 + one / ((G)0.3652 * P::ex((v - (G)31.66) * (G)(1.0 / 3.869)) +
+                                   (G)4.123e-05 * P::ex(-(v - (G)47.78) * (G)(1.0 / 20.38)));
+  const G txrs = (G)1.865 + one / ((G)0.06629 * P::ex((v - (G)34.70) * (G)(1.0 / 7.355)) +
+                                   (G)1.128e-05 * P::ex(-(v - (G)29.74) * (G)(1.0 / 25.94)));
+  const G xs1ss = one / (one + P::ex(-(v + (G)11.60) * (G)(1.0 / 8.932)));
+  const G txs1 = (G)817.3 + one / ((G)2.326e-04 * P::ex((v + (G)48.28) * (G)(1.0 / 17.80)) +
+                                   (G)0.001292 * P::ex(-(v + (G)210.0) * (G)(1.0 / 230.0)));
+  const G xk1ss = one / (one + P::ex(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den)));
+  const G txk1 = (G)122.2 / (P::ex(-(v + (G)127.2) * (G)(1.0 / 20.36)) + P::ex((v + (G)236.8) * (G)(1.0 / 69.33)));
+  const G jss = hss;
+  const G tj = (G)2.038 + one / ((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
+                                 (G)0.3052 * P::ex((v + (G)0.9941) * (G)(1.0 / 38.45)));
+  const G assp = one / (one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82)));
+  const G tfcaf = (G)7.0 + one / ((G)0.04 * P::ex(-(v - (G)4.0) * (G)(1.0 / 7.0)) +
+                                  (G)0.04 * P::ex((v - (G)4.0) * (G)(1.0 / 7.0)));
+  const G tfcas = (G)100.0 + one / ((G)0.00012 * P::ex(-v * (G)(1.0 / 3.0)) + (G)0.00012 * P::ex(v * (G)(1.0 / 7.0)));
+  const G tffp = (G)2.5 * tff;
+  const G xs2ss = xs1ss;
+  const G txs2 = one / ((G)0.01 * P::ex((v - (G)50.0) * (G)0.05) + (G)0.0193 * P::ex(-(v + (G)66.54) * (G)(1.0 / 31.0)));
+  // CaMKII (FP64 in both paths: CaMKt is integrated in FP64)
+  const double CaMKb = (k::CaMKo * (1.0 - y.CaMKt)) / (1.0 + k::KmCaM / y.cass);
+  const double CaMKa = CaMKb + y.CaMKt;
+  const G hssp = one / (one + P::ex((v + (G)89.1) * (G)(1.0 / 6.086)));
+  const G thsp = (G)3.0 * ths;
+  const G tjp = (G)1.46 * tj;
+  const G mLss = one / (one + P::ex(-(v + (G)42.85) * (G)(1.0 / 5.264)));
+  const G tmL = tm;
+  const G tfcafp = (G)2.5 * tfcaf;
+  const G iss = one / (one + P::ex((v + (G)43.94) * (G)(1.0 / 5.711)));
+  const G delta_epi = q.celltype == 1 ? one - (G)0.95 / (one + P::ex((v + (G)70.0) * (G)0.2)) : one;
+  const G tiF = ((G)4.562 + one / ((G)0.3933 * P::ex(-(v + (G)100.0) * (G)0.01) +
+                                   (G)0.08004 * P::ex((v + (G)50.0) * (G)(1.0 / 16.59)))) * delta_epi;
+  const G tiS = ((G)23.62 + one / ((G)0.001416 * P::ex(-(v + (G)96.52) * (G)(1.0 / 59.05)) +
+                                   (G)1.78e-08 * P::ex((v + (G)114.1) * (G)(1.0 / 8.079)))) * delta_epi;
+  const G dti_develop = (G)1.354 + (G)1e-4 / (P::ex((v - (G)167.4) * (G)(1.0 / 15.89)) +
+                                              P::ex(-(v - (G)12.23) * (G)(1.0 / 0.2154)));
+  const G dti_recover = one - (G)0.5 / (one + P::ex((v + (G)70.0) * (G)0.05));
+  const G tiFp = dti_develop * dti_recover * tiF;
+  const G tiSp = dti_develop * dti_recover * tiS;
+  // ICaL and its Na/K components
+  const G f = q.Aff * y.ff + q.Afs * y.fs;
+  const G Afcaf = (G)0.3 + (G)0.6 / (one + P::ex((v - (G)10.0) * (G)0.1));
+  const G Afcas = one - Afcaf;
+  const G fca = Afcaf * y.fcaf + Afcas * y.fcas;
+  const G fp = q.Aff * y.ffp + q.Afs * y.fs;
+  const G fcap = Afcaf * y.fcafp + Afcas * y.fcas;
+  const G fICaLp = (G)(1.0 / (1.0 + k::KmCaMK / CaMKa));
+  const G nca_ = y.nca;
+  const G gate_np = y.d * (f * (one - nca_) + y.jca * fca * nca_);
+  const G gate_p = y.d * (fp * (one - nca_) + y.jca * fcap * nca_);
+  G PhiCaL, PhiCaNa, PhiCaK, INab, ICab;
+  {
+    const G vfrt = v * (G)k::FRT;
+    if constexpr (P::kMixed) {
+      // GHK fluxes with the x/(e^x-1) factor evaluated stably
+      const G e1 = P::ex(vfrt), e2 = e1 * e1;
+      const G g1 = ghk_factor(vfrt) * (G)k::F;             // vffrt / (e^vfrt - 1)
+      const G g2 = (G)0.5 * ghk_factor((G)2 * vfrt) * (G)k::F;  // vffrt / (e^2vfrt - 1)
+      PhiCaL = (G)4.0 * g2 * (cass_g * e2 - (G)(0.341 * k::cao));
+      PhiCaNa = g1 * ((G)0.75 * (G)y.nass * e1 - (G)(0.75 * k::nao));
+      PhiCaK = g1 * ((G)0.75 * (G)y.kss * e1 - (G)(0.75 * k::ko));
+      INab = (G)k::PNab * g1 * ((G)y.nai * e1 - (G)k::nao);
+      ICab = (G)(k::PCab * 4.0) * g2 * ((G)y.cai * e2 - (G)(0.341 * k::cao));
+    } else {
+      const double vffrt = (y.V * k::F * k::F) / (k::R * k::T);
+      const double vfrt_d = (y.V * k::F) / (k::R * k::T);
+      const double e1 = ::exp(vfrt_d), e2 = ::exp(2.0 * vfrt_d);
+      PhiCaL = (4.0 * vffrt * (y.cass * e2 - 0.341 * k::cao)) / (e2 - 1.0);
+      PhiCaNa = (vffrt * (0.75 * y.nass * e1 - 0.75 * k::nao)) / (e1 - 1.0);
+      PhiCaK = (vffrt * (0.75 * y.kss * e1 - 0.75 * k::ko)) / (e1 - 1.0);
+      INab = (k::PNab * vffrt * (y.nai * e1 - k::nao)) / (e1 - 1.0);
+      ICab = (k::PCab * 4.0 * vffrt * (y.cai * e2 - 0.341 * k::cao)) / (e2 - 1.0);
+    }
+  }
+  const G ICaL = (one - fICaLp) * q.PCa * PhiCaL * gate_np + fICaLp * q.PCap * PhiCaL * gate_p;
+  const G ICaNa = (one - fICaLp) * q.PCaNa * PhiCaNa * gate_np + fICaLp * q.PCaNap * PhiCaNa * gate_p;
+  const G ICaK = (one - fICaLp) * q.PCaK * PhiCaK * gate_np + fICaLp * q.PCaKp * PhiCaK * gate_p;
+  // RyR release
+  const G cajsr_g = (G)y.cajsr;
+  const G rel_den = one + p8((G)1.5 / cajsr_g);
+  const G Jrel_inf_t = ((G)k::a_rel * -ICaL) / rel_den;
+  const G Jrel_inf = q.celltype == 2 ? Jrel_inf_t * (G)1.7 : Jrel_inf_t;
+  const G tau_rel_t = (G)k::bt / (one + (G)0.0123 / cajsr_g);
+  const G tau_rel = tau_rel_t < (G)0.001 ? (G)0.001 : tau_rel_t;
+  const G Jrel_t = ((G)k::a_relp * -ICaL) / rel_den;
+  const G Jrel_infp = q.celltype == 2 ? Jrel_t * (G)1.7 : Jrel_t;
+  const G tau_relp_t = (G)k::btp / (one + (G)0.0123 / cajsr_g);
+  const G tau_relp = tau_relp_t < (G)0.001 ? (G)0.001 : tau_relp_t;
+  // potassium currents
+  const G EK = (G)k::RTF * P::lg((G)k::ko / (G)y.ki);
+  const G AiF = one / (one + P::ex((v - (G)213.6) * (G)(1.0 / 151.2)));
+  const G AiS = one - AiF;
+  const G i_ = AiF * y.iF + AiS * y.iS;
+  const G ip = AiF * y.iFp + AiS * y.iSp;
+  const G fCaMKp = fICaLp;  // fItop, fINap, fINaLp, fJrelp, fJupp share 1/(1+KmCaMK/CaMKa)
+  const G Ito = q.Gto * (v - EK) * ((one - fCaMKp) * y.a * i_ + fCaMKp * y.ap * ip);
+  const G Axrf = one / (one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21)));
+  const G Axrs = one - Axrf;
+  const G xr = Axrf * y.xrf + Axrs * y.xrs;
+  const G rkr = (one / (one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0)))) / (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0)));
+  const G IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
+  const G EKs = (G)k::RTF * P::lg((G)(k::ko + k::PKNa * k::nao) / (G)(y.ki + k::PKNa * y.nai));
+  const G cai_g = (G)y.cai;
+  const G KsCa = one + (G)0.6 / (one + P::pw((G)3.8e-05 / cai_g, (G)1.4));
+  const G IKs = q.GKs * KsCa * y.xs1 * y.xs2 * (v - EKs);
+  const G rk1 = one / (one + P::ex(((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493)));
+  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * y.xk1 * (v - EK);
+  // Na/K pump
+  const G nai_g = (G)y.nai, ki_g = (G)y.ki;
+  const G Knao = (G)k::Knao0 * P::ex(((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+  const G Knai = (G)k::Knai0 * P::ex(((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+  const G nao_Knao3 = p3(one + (G)k::nao / Knao);
+  const G nak_den_o = (nao_Knao3 + (G)k::ko_Kko_sq) - one;
+  const G nai_Knai3 = p3(one + nai_g / Knai);
+  const G ki_Kki2 = p2(one + ki_g * (G)(1.0 / k::Kki));
+  const G nak_den_i = (nai_Knai3 + ki_Kki2) - one;
+  const G a3 = (G)k::a3c / nak_den_o;
+  // P = eP / (1 + H/Khp + nai/Knap + ki/Kxkur) with the instance's H folded
+  // into b3c = k3m*H/(1+MgATP/Kmgatp); H/Khp = b3c*(1+MgATP/Kmgatp)/(k3m*Khp).
+  const G H_Khp = q.b3c * (G)((1.0 + k::MgATP / k::Kmgatp) / (k::k3m * k::Khp));
+  const G PP = (G)k::eP / (one + H_Khp + nai_g * (G)(1.0 / k::Knap) + ki_g * (G)(1.0 / k::Kxkur));
+  const G b3 = q.b3c * PP;
+  const G a1 = ((G)k::k1p * p3(nai_g / Knai)) / nak_den_i;
+  const G b2 = ((G)k::k2m * p3((G)k::nao / Knao)) / nak_den_o;
+  const G b4 = ((G)k::k4m * p2(ki_g * (G)(1.0 / k::Kki))) / nak_den_i;
+  const G x1 = (G)k::a4 * a1 * (G)k::a2 + b2 * b4 * b3 + (G)k::a2 * b4 * b3 + b3 * a1 * (G)k::a2;
+  const G x2 = b2 * (G)k::b1 * b4 + a1 * (G)k::a2 * a3 + a3 * (G)k::b1 * b4 + (G)k::a2 * a3 * b4;
+  const G x3 = (G)k::a2 * a3 * (G)k::a4 + b3 * b2 * (G)k::b1 + b2 * (G)k::b1 * (G)k::a4 + a3 * (G)k::a4 * (G)k::b1;
+  const G x4 = b4 * b3 * b2 + a3 * (G)k::a4 * a1 + b2 * (G)k::a4 * a1 + b3 * b2 * a1;
+  const G xs_inv = one / (x1 + x2 + x3 + x4);
+  const G E1 = x1 * xs_inv, E2 = x2 * xs_inv, E3 = x3 * xs_inv, E4 = x4 * xs_inv;
+  const G JnakNa = (G)3.0 * (E1 * a3 - E2 * b3);
+  const G JnakK = (G)2.0 * (E4 * (G)k::b1 - E3 * a1);
+  const G INaK = q.Pnak * ((G)k::zna * JnakNa + (G)k::zk * JnakK);
+  const G xkb = one / (one + P::ex(-(v - (G)14.48) * (G)(1.0 / 18.34)));
+  const G IKb = q.GKb * xkb * (v - EK);
+  // sodium currents
+  const G ENa = (G)k::RTF * P::lg((G)k::nao / (G)y.nai);
+  const G h_ = (G)k::Ahf * y.hf + (G)k::Ahs * y.hs;
+  const G hp = (G)k::Ahf * y.hf + (G)k::Ahs * y.hsp;
+  const G INa = q.GNa * (v - ENa) * p3(y.m) * ((one - fCaMKp) * h_ * y.j + fCaMKp * hp * y.jp);
+  const G INaL = q.GNaL * (v - ENa) * y.mL * ((one - fCaMKp) * y.hL + fCaMKp * y.hLp);
+  // Na/Ca exchanger, myoplasmic and subspace compartments
+  const G hna = P::ex(((G)k::qna * v) * (G)k::FRT);
+  const G hca = P::ex(((G)k::qca * v) * (G)k::FRT);
+  const G h7 = one + ((G)k::nao / (G)k::kna3) * (one + one / hna);
+  const G h8 = (G)k::nao / ((G)k::kna3 * hna * h7);
+  const G k3pp = h8 * (G)k::wnaca;
+  const G k8 = h8 * (G)k::h11 * (G)k::wna;
+  const G k3p = ((G)1 / h7) * (G)k::wca;
+  const G k3 = k3p + k3pp;
+  G INaCa_i, INaCa_ss;
+  {
+    const G h1 = one + (nai_g / (G)k::kna3) * (one + hna);
+    const G h2 = (nai_g * hna) / ((G)k::kna3 * h1);
+    const G k4pp = h2 * (G)k::wnaca;
+    const G h4 = one + (nai_g / (G)k::kna1) * (one + nai_g / (G)k::kna2);
+    const G h5 = (nai_g * nai_g) / (h4 * (G)k::kna1 * (G)k::kna2);
+    const G k7 = h5 * h2 * (G)k::wna;
+    const G k4p = (((G)1 / h1) * (G)k::wca) / hca;
+    const G k4 = k4p + k4pp;
+    const G k6 = ((G)1 / h4) * cai_g * (G)k::kcaon;
+    const G x1i = (G)k::k2x * k4 * (k7 + k6) + (G)k::k5x * k7 * ((G)k::k2x + k3);
+    const G x2i = (G)k::k1x * k7 * (k4 + (G)k::k5x) + k4 * k6 * ((G)k::k1x + k8);
+    const G x3i = (G)k::k1x * k3 * (k7 + k6) + k8 * k6 * ((G)k::k2x + k3);
+    const G x4i = (G)k::k2x * k8 * (k4 + (G)k::k5x) + k3 * (G)k::k5x * ((G)k::k1x + k8);
+    const G inv = one / (x1i + x2i + x3i + x4i);
+    const G E1i = x1i * inv, E2i = x2i * inv, E3i = x3i * inv, E4i = x4i * inv;
+    const G allo = one / (one + p2((G)k::KmCaAct / cai_g));
+    const G JncxNa = ((G)3.0 * (E4i * k7 - E1i * k8) + E3i * k4pp) - E2i * k3pp;
+    const G JncxCa = E2i * (G)k::k2x - E1i * (G)k::k1x;
+    INaCa_i = (G)0.8 * q.Gncx * allo * ((G)k::zna * JncxNa + (G)k::zca * JncxCa);
+  }
+  {
+    const G nass_g = (G)y.nass;
+    const G h1 = one + (nass_g / (G)k::kna3) * (one + hna);
+    const G h2 = (nass_g * hna) / ((G)k::kna3 * h1);
+    const G k4pp = h2 * (G)k::wnaca;
+    const G h4 = one + (nass_g / (G)k::kna1) * (one + nass_g / (G)k::kna2);
+    const G h5 = (nass_g * nass_g) / (h4 * (G)k::kna1 * (G)k::kna2);
+    const G k7 = h5 * h2 * (G)k::wna;
+    const G k4p = (((G)1 / h1) * (G)k::wca) / hca;
+    const G k4 = k4p + k4pp;
+    const G k6 = ((G)1 / h4) * cass_g * (G)k::kcaon;
+    const G x1s = (G)k::k2x * k4 * (k7 + k6) + (G)k::k5x * k7 * ((G)k::k2x + k3);
+    const G x2s = (G)k::k1x * k7 * (k4 + (G)k::k5x) + k4 * k6 * ((G)k::k1x + k8);
+    const G x3s = (G)k::k1x * k3 * (k7 + k6) + k8 * k6 * ((G)k::k2x + k3);
+    const G x4s = (G)k::k2x * k8 * (k4 + (G)k::k5x) + k3 * (G)k::k5x * ((G)k::k1x + k8);
+    const G inv = one / (x1s + x2s + x3s + x4s);
+    const G E1s = x1s * inv, E2s = x2s * inv, E3s = x3s * inv, E4s = x4s * inv;
+    const G allo = one / (one + p2((G)k::KmCaAct / cass_g));
+    const G JncxNa = ((G)3.0 * (E4s * k7 - E1s * k8) + E3s * k4pp) - E2s * k3pp;
+    const G JncxCa = E2s * (G)k::k2x - E1s * (G)k::k1x;
+    INaCa_ss = (G)0.2 * q.Gncx * allo * ((G)k::zna * JncxNa + (G)k::zca * JncxCa);
+  }
+  const G IpCa = ((G)k::GpCa * cai_g) / ((G)k::KmCap + cai_g);
+  // fluxes: concentration differences are formed in FP64 before rounding
+  const G JdiffK = (G)((y.kss - y.ki) * 0.5);
+  const G JdiffNa = (G)((y.nass - y.nai) * 0.5);
+  const G Jdiff = (G)((y.cass - y.cai) * 5.0);
+  const G Jtr = (G)((y.cansr - y.cajsr) * 0.01);
+  const G Jrel = (one - fCaMKp) * y.Jrelnp + fCaMKp * y.Jrelp;
+  const G Bcass = one / (one + (G)(k::BSRmax * k::KmBSR) / p2((G)k::KmBSR + cass_g) +
+                         (G)(k::BSLmax * k::KmBSL) / p2((G)k::KmBSL + cass_g));
+  const G Jupnp = (q.upScale * (G)0.004375 * cai_g) / (cai_g + (G)0.00092);
+  const G Jupp = (q.upScale * (G)(2.75 * 0.004375) * cai_g) / ((cai_g + (G)0.00092) - (G)0.00017);
+  const G Jleak = (G)(0.0039375 / 15.0) * (G)y.cansr;
+  const G Jup = ((one - fCaMKp) * Jupnp + fCaMKp * Jupp) - Jleak;
+  const G Bcai = one / (one + (q.cmdnmax * (G)k::kmcmdn) / p2((G)k::kmcmdn + cai_g) +
+                        (G)(k::trpnmax * k::kmtrpn) / p2((G)k::kmtrpn + cai_g));
+  const G Bcajsr = one / (one + (G)(k::csqnmax * k::kmcsqn) / p2((G)k::kmcsqn + cajsr_g));
+  // RATES of the FP64-integrated variables
+  const G dV = -(INa + INaL + Ito + ICaL + ICaNa + ICaK + IKr + IKs + IK1 + INaCa_i + INaCa_ss + INaK +
+                 INab + IKb + IpCa + ICab + Istim);
+  cur.INa = INa; cur.INaL = INaL; cur.Ito = Ito; cur.ICaL = ICaL; cur.IKr = IKr; cur.IKs = IKs;
+  cur.IK1 = IK1; cur.dVdt = dV;
+  if (!update) return;
+  const G dki = (-((Ito + IKr + IKs + IK1 + IKb + Istim) - (G)2.0 * INaK)) * (G)k::cAF_myo +
+                JdiffK * (G)(k::vss / k::vmyo);
+  const G dkss = (-ICaK) * (G)k::cAF_ss - JdiffK;
+  const G dnai = (-(INa + INaL + (G)3.0 * INaCa_i + (G)3.0 * INaK + INab)) * (G)k::cAF_myo +
+                 JdiffNa * (G)(k::vss / k::vmyo);
+  const G dnass = (-(ICaNa + (G)3.0 * INaCa_ss)) * (G)k::cAF_ss - JdiffNa;
+  const G dcass = Bcass * (((-(ICaL - (G)2.0 * INaCa_ss)) * (G)(0.5 * k::cAF_ss) +
+                            Jrel * (G)(k::vjsr / k::vss)) - Jdiff);
+  const G dcai = Bcai * (((-((IpCa + ICab) - (G)2.0 * INaCa_i)) * (G)(0.5 * k::cAF_myo) -
+                          Jup * (G)(k::vnsr / k::vmyo)) + Jdiff * (G)(k::vss / k::vmyo));
+  const G dcansr = Jup - Jtr * (G)(k::vjsr / k::vnsr);
+  const G dcajsr = Bcajsr * (Jtr - Jrel);
+  const double dCaMKt = k::aCaMK * CaMKb * (CaMKb + y.CaMKt) - k::bCaMK * y.CaMKt;
+  // Rush-Larsen gates
+  const G gdt = (G)dt;
+  y.m = rush_larsen<P>(y.m, mss, tm, gdt);
+  y.hf = rush_larsen<P>(y.hf, hss, thf, gdt);
+  y.hs = rush_larsen<P>(y.hs, hss, ths, gdt);
+  y.j = rush_larsen<P>(y.j, jss, tj, gdt);
+  y.hsp = rush_larsen<P>(y.hsp, hssp, thsp, gdt);
+  y.jp = rush_larsen<P>(y.jp, jss, tjp, gdt);
+  y.mL = rush_larsen<P>(y.mL, mLss, tmL, gdt);
+  y.hL = rush_larsen<P>(y.hL, hLss, (G)k::thL, gdt);
+  y.hLp = rush_larsen<P>(y.hLp, hLssp, (G)k::thLp, gdt);
+  y.a = rush_larsen<P>(y.a, ass, ta, gdt);
+  y.iF = rush_larsen<P>(y.iF, iss, tiF, gdt);
+  y.iS = rush_larsen<P>(y.iS, iss, tiS, gdt);
+  y.ap = rush_larsen<P>(y.ap, assp, ta, gdt);
+  y.iFp = rush_larsen<P>(y.iFp, iss, tiFp, gdt);
+  y.iSp = rush_larsen<P>(y.iSp, iss, tiSp, gdt);
+  y.d = rush_larsen<P>(y.d, dss, td, gdt);
+  y.ff = rush_larsen<P>(y.ff, fss, tff, gdt);
+  y.fs = rush_larsen<P>(y.fs, fss, tfs, gdt);
+  y.fcaf = rush_larsen<P>(y.fcaf, fcass, tfcaf, gdt);
+  y.fcas = rush_larsen<P>(y.fcas, fcass, tfcas, gdt);
+  y.jca = rush_larsen<P>(y.jca, fcass, q.tjca, gdt);
+  y.ffp = rush_larsen<P>(y.ffp, fss, tffp, gdt);
+  y.fcafp = rush_larsen<P>(y.fcafp, fcass, tfcafp, q.fcafp_dt != (G)0 ? q.fcafp_dt : gdt);
+  {
+    const G nca_inf = anca * (G)k::k2n / km2n;
+    y.nca = nca_inf - (nca_inf - y.nca) * P::ex(-km2n * gdt);
+  }
+  y.xrf = rush_larsen<P>(y.xrf, xrss, txrf, gdt);
+  y.xrs = rush_larsen<P>(y.xrs, xrss, txrs, gdt);
+  y.xs1 = rush_larsen<P>(y.xs1, xs1ss, txs1, gdt);
+  y.xs2 = rush_larsen<P>(y.xs2, xs2ss, txs2, gdt);
+  y.xk1 = rush_larsen<P>(y.xk1, xk1ss, txk1, gdt);
+  y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, gdt);
+  y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, gdt);
+  // forward Euler, FP64 accumulation
+  y.CaMKt = y.CaMKt + dCaMKt * dt;
+  y.V = y.V + (double)dV * dt;
+  y.nai = y.nai + (double)dnai * dt;
+  y.nass = y.nass + (double)dnass * dt;
+  y.ki = y.ki + (double)dki * dt;
+  y.kss = y.kss + (double)dkss * dt;
+  y.cai = y.cai + (double)dcai * dt;
+  y.cass = y.cass + (double)dcass * dt;
+  y.cansr = y.cansr + (double)dcansr * dt;
+  y.cajsr = y.cajsr + (double)dcajsr * dt;
+}
+
+// Hill factor of ___applyDrugEffect (Ohara_Rudy_2011.cpp:469-485): block only
+// when both IC50 and h exceed 10E-14 (the reference reads NA as 0).
+__device__ __forceinline__ double hill_factor(double conc, double ic50, double h) {
+  return (ic50 > 10E-14 && h > 10E-14) ? 1. / (1. + ::pow(conc / ic50, h)) : 1.;
+}
+
+// initConsts(celltype, conc, ic50, is_dutta) for one instance
+// (Ohara_Rudy_2011.cpp:494-678 and :722-738), written into the parameter
+// block, and the model's initial STATES. `quirks` reproduces the reference's
+// documented quirks (celltype forced to endo, the mis-indexed Dutta scaling,
+// the drug block of PCa not reaching the derived permeabilities, and the
+// STATES enum value d = 25 used as the fcafp step).
+__device__ __forceinline__ void init_instance(double *__restrict__ par, double *__restrict__ s, int64_t ld,
+                                              int64_t i, double celltype_in, double conc,
+                                              const double *__restrict__ hill, bool dutta, bool quirks) {
+  const double ct = quirks ? 0.0 : celltype_in;
+  double GNaL = ct == 1.0 ? 0.0075 * 0.6 : 0.0075;
+  double Gto = ct == 1.0 ? 0.02 * 4.0 : ct == 2.0 ? 0.02 * 4.0 : 0.02;
+  double PCa = ct == 1.0 ? 0.0001 * 1.2 : ct == 2.0 ? 0.0001 * 2.5 : 0.0001;
+  double GKr = ct == 1.0 ? 0.046 * 1.3 : ct == 2.0 ? 0.046 * 0.8 : 0.046;
+  double GKs = ct == 1.0 ? 0.0034 * 1.4 : 0.0034;
+  double GK1 = ct == 1.0 ? 0.1908 * 1.2 : ct == 2.0 ? 0.1908 * 1.3 : 0.1908;
+  double GKb = ct == 1.0 ? 0.003 * 0.6 : 0.003;
+  double Gncx = ct == 1.0 ? 0.0008 * 1.1 : ct == 2.0 ? 0.0008 * 1.4 : 0.0008;
+  double Pnak = ct == 1.0 ? 30 * 0.9 : ct == 2.0 ? 30 * 0.7 : 30;
+  double cmdnmax = ct == 1.0 ? 0.05 * 1.3 : 0.05;
+  double upScale = ct == 1.0 ? 1.3 : 1.0;
+  double Aff = 0.6, tjca = 75.0, H = 1e-7, GNa = 75;
+  const double Afs = 1.0 - Aff;  // derived before the Dutta quirk scales Aff
+  double PCap = 1.1 * PCa, PCaNa = 0.00125 * PCa, PCaK = 0.0003574 * PCa;
+  double PCaNap = 0.00125 * PCap, PCaKp = 0.0003574 * PCap;
+  if (dutta) {
+    if (quirks) {  // ___applyDutta as written (Ohara_Rudy_2011.cpp:460-467)
+      Aff *= 1.870; GNaL *= 1.013; tjca *= 1.698; H *= 1.007;
+    } else {
+      GKs *= 1.870; GKr *= 1.013; GK1 *= 1.698; PCa *= 1.007; GNaL *= 2.661;
+      PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
+      PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
+    }
+  }
+  if (hill) {
+    PCa *= hill_factor(conc, hill[0], hill[1]);
+    GK1 *= hill_factor(conc, hill[2], hill[3]);
+    GKs *= hill_factor(conc, hill[4], hill[5]);
+    GNa *= hill_factor(conc, hill[6], hill[7]);
+    GNaL *= hill_factor(conc, hill[8], hill[9]);
+    Gto *= hill_factor(conc, hill[10], hill[11]);
+    GKr *= hill_factor(conc, hill[12], hill[13]);
+    if (!quirks) {
+      PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
+      PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
+    }
+  }
+  double *p = par + i;
+  p[P_GNa * ld] = GNa; p[P_GNaL * ld] = GNaL; p[P_Gto * ld] = Gto; p[P_PCa * ld] = PCa;
+  p[P_PCap * ld] = PCap; p[P_PCaNa * ld] = PCaNa; p[P_PCaK * ld] = PCaK; p[P_PCaNap * ld] = PCaNap;
+  p[P_PCaKp * ld] = PCaKp; p[P_GKr * ld] = GKr; p[P_GKs * ld] = GKs; p[P_GK1 * ld] = GK1;
+  p[P_GKb * ld] = GKb; p[P_Gncx * ld] = Gncx; p[P_Pnak * ld] = Pnak; p[P_cmdnmax * ld] = cmdnmax;
+  p[P_upScale * ld] = upScale; p[P_Aff * ld] = Aff; p[P_Afs * ld] = Afs; p[P_tjca * ld] = tjca;
+  p[P_H * ld] = H; p[P_celltype * ld] = ct; p[P_fcafp_dt * ld] = quirks ? 25.0 : 0.0;
+  p[P_amp * ld] = -80; p[P_BCL * ld] = 1000.0; p[P_stim_start * ld] = 10.0; p[P_duration * ld] = 0.5;
+  // initial STATES (Ohara_Rudy_2011.cpp:494-678)
+  const double y0[kNumStates] = {-87, 0, 1e-4, 7, 7, 145, 145, 1.2, 1.2, 1e-4, 0, 1, 1, 1, 1, 1, 0, 1, 1, 0, 1,
+                                 1, 0, 1, 1, 0, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 1, 0, 0};
+#pragma unroll
+  for (int k2 = 0; k2 < kNumStates; ++k2) s[k2 * ld + i] = y0[k2];
+}
+
+}  // namespace ord
+}  // namespace cep

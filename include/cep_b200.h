@@ -1,0 +1,158 @@
+/*
+ * cep_b200 -- B200-native cardiac drug-screening hot path: batched ionic-model
+ * stepping with Hill-equation drug block and on-device biomarkers, and the
+ * monodomain FEM diffusion solve.
+ *
+ * Plain C ABI: opaque handles, host pointers and sizes, int status codes. No
+ * CUDA or torch types appear in the signatures (device pointers are passed
+ * as void*). Every entry point returns CEP_OK (0) or a CEP_ERR_* code;
+ * cep_last_error() gives the message of the calling thread's last failure.
+ *
+ * Threading: a handle is bound to one CUDA stream and must not be used from
+ * two host threads at once. Handles are independent of each other.
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * within the kit-cml/2DDrugSimulation tree).
+ */
+#ifndef CEP_B200_H
+#define CEP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define CEP_OK 0
+#define CEP_ERR_ARG 1           /* invalid argument (null, size, range)     */
+#define CEP_ERR_OOM 2           /* device allocation failed                 */
+#define CEP_ERR_CUDA 3          /* CUDA runtime error                       */
+#define CEP_ERR_NOT_CONVERGED 4 /* iterative solve hit max_iter             */
+#define CEP_ERR_TIMEOUT 5       /* a bounded device wait ran out            */
+#define CEP_ERR_NONFINITE 6     /* a state became NaN/Inf (per instance)    */
+#define CEP_ERR_UNSUPPORTED 7   /* model/precision combination not built   */
+#define CEP_ERR_STATE 8         /* call out of order (e.g. run before init) */
+#define CEP_ERR_NO_DEVICE 9     /* no CUDA device visible                   */
+
+/* per-instance status words (cep_batch_get_status) */
+#define CEP_INST_RUNNING 0
+#define CEP_INST_DONE 1     /* reached the end of its protocol */
+#define CEP_INST_NONFINITE 2 /* state left the finite range; frozen */
+
+/* ----------------------------------------------------------------- models */
+#define CEP_MODEL_ORD2011 0   /* DrugSimulation/cellmodels/Ohara_Rudy_2011.cpp, 41 states */
+#define CEP_MODEL_CIPA2017 1  /* CEPCell_NEO/cellmodels/ohara_rudy_cipa_v1_2017.cpp, 49 states */
+#define CEP_MODEL_TT2006 2    /* CEPCell_NEO/cellmodels/ten_tusscher_model_2006_IK1Ko_epi_units.cpp, 19 states */
+#define CEP_MODEL_TT2004 3    /* CEPCell_NEO/cellmodels/tentusscher_noble_noble_panfilov_2004_b.cpp, 17 states */
+#define CEP_MODEL_TOMEK2019 4 /* CEPCell_NEO/cellmodels/Tomek_model.cpp, 43 states */
+
+#define CEP_PREC_FP64 0  /* everything in FP64                                  */
+#define CEP_PREC_MIXED 1 /* FP32 gates/rates/currents, FP64 V, ions, CaMKII     */
+
+/* init flags */
+#define CEP_FLAG_DUTTA 1u  /* Dutta et al. 2017 conductance scaling (ORd)          */
+#define CEP_FLAG_QUIRKS 2u /* reproduce the reference's documented quirks exactly  */
+
+/* state array layouts for set/get */
+#define CEP_LAYOUT_SOA 0 /* states[k * n + i] (k = state index, i = instance) */
+#define CEP_LAYOUT_AOS 1 /* states[i * n_states + k]                          */
+
+/* Width of one Hill row: 14 IC50/h pairs in the reference CSV column order
+ * (ICaL, IK1, IKs, INa, INaL, Ito, hERG: CEP5Cell/bin/drugs/<drug>/
+ * IC50_samples.csv:1), then the CiPA dynamic-hERG set Kmax, Ku, n,
+ * halfmax, Vhalf (CEPCell_NEO/cellmodels/ohara_rudy_cipa_v1_2017.cpp:1534-1538)
+ * and Kt. IC50 or h <= 1e-13 means "no block" (the reference reads NA as 0). */
+#define CEP_HILL_WIDTH 20
+
+/* One beat's biomarkers: the fields of cipa_t (CEPCell_NEO/modules/
+ * commons.hpp:18-36) as the CiPA bench prints them (cipa_drug_bench.cpp:
+ * 352-379). qnet is in the reference's printed unit (integral / 1000). */
+typedef struct {
+  double qnet, inal_auc, ical_auc;
+  double dvmdt_repol, dvmdt_max, vm_peak, vm_valley, vm_dia, apd90, apd50, apd_tri;
+  double ca_peak, ca_valley, ca_dia, cad90, cad50, cad_tri;
+  int32_t steepest_pace; /* pace index the result was taken from          */
+  int32_t n_eligible;    /* eligible beats evaluated                       */
+  int32_t status;        /* CEP_INST_*                                     */
+  int32_t reserved;
+} cep_biomarkers_t;
+
+typedef struct cep_batch *cep_batch_t;
+
+/* Library identity. */
+const char *cep_version(void);
+const char *cep_last_error(void);
+/* Number of visible CUDA devices (0 on a host without GPUs). */
+int cep_device_count(void);
+
+/* Create a batch of n instances of one model on the current CUDA device,
+ * bound to `stream` (a cudaStream_t, NULL = the legacy default stream).
+ * Replaces `new Ohara_Rudy_2011()` / `new ohara_rudy_cipa_v1_2017()` per
+ * instance (cellmodel.hpp:4-36, patch_clamp.hpp:4-26). */
+int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t *out);
+int cep_batch_destroy(cep_batch_t b);
+int cep_batch_size(cep_batch_t b, int *n, int *n_states);
+/* Threads per block of the run kernel (32, 64, 96 or 128); the default
+ * spreads small populations over every SM. Used by the autotuner. */
+int cep_batch_set_block(cep_batch_t b, int threads_per_block);
+
+/* initConsts for every instance and the model's initial STATES.
+ * celltype[n] (NULL = 0, endo), conc[n] (drug concentration, same unit as
+ * IC50), hill[n * hill_stride] (NULL = no drug), flags CEP_FLAG_*.
+ * Replaces Ohara_Rudy_2011::initConsts(type, conc, ic50, is_dutta)
+ * (Ohara_Rudy_2011.cpp:722-738) and ohara_rudy_cipa_v1_2017::
+ * initConsts(type, conc, hill) (ohara_rudy_cipa_v1_2017.cpp:1515-1539).
+ * The Hill scaling runs on the device. */
+int cep_batch_init(cep_batch_t b, const double *celltype, const double *conc, const double *hill,
+                   int hill_stride, unsigned flags);
+
+/* Pacing overrides applied after init: CONSTANTS[BCL] = bcl,
+ * CONSTANTS[stim_start], CONSTANTS[duration], CONSTANTS[amp] *= amp_scale
+ * (cipa_drug_bench.cpp:146-147). Negative stim_start / stim_dur keep the
+ * model defaults. */
+int cep_batch_set_pacing(cep_batch_t b, double bcl, double stim_start, double stim_dur, double amp_scale);
+
+/* Protocol of the run: fixed step dt (ms), n_pace paces at the instance's
+ * BCL, biomarkers evaluated on paces >= first_pace (first_pace = n_pace-250
+ * reproduces cipa_drug_bench.cpp:296; n_pace-1 is last-beat mode; -1 turns
+ * biomarkers off), Ca sampled every dt_write ms for CaD50/90, qNet summed
+ * while V > qnet_vm_threshold (-1e300: always, as cipa_drug_bench.cpp:225;
+ * -88: as heart.cpp:369). Resets every instance's clock to t = 0. */
+int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,
+                           double qnet_vm_threshold);
+
+/* Advance every unfinished instance by up to n_steps fixed steps of the
+ * reference scheme (computeRates then solveAnalytical, t += dt:
+ * cipa_drug_explicit_bench.cpp:119-127) with the biomarker state machine
+ * fused. Asynchronous on the batch's stream. */
+int cep_batch_run(cep_batch_t b, long n_steps);
+/* Run to the end of the protocol (blocking). */
+int cep_batch_run_to_end(cep_batch_t b, long steps_per_launch);
+
+/* Host <-> device state transfer (blocking). layout CEP_LAYOUT_*. */
+int cep_batch_set_states(cep_batch_t b, const double *states, int layout);
+int cep_batch_get_states(cep_batch_t b, double *states, int layout);
+/* Device pointer of the SoA state block ([n_states][ld] doubles). */
+int cep_batch_device_states(cep_batch_t b, void **dev_ptr, long *ld);
+
+int cep_batch_get_biomarkers(cep_batch_t b, cep_biomarkers_t *out /* [n] */);
+int cep_batch_get_status(cep_batch_t b, int32_t *status /* [n] */);
+/* Current step count and time of instance i. */
+int cep_batch_get_clock(cep_batch_t b, int i, long *step, double *t);
+int cep_batch_sync(cep_batch_t b);
+
+/* Rates at the current state without advancing it (computeRates,
+ * Ohara_Rudy_2011.cpp:742): dVdt[n] and the seven channel currents
+ * currents[7*n] (INa, INaL, Ito, ICaL, IKr, IKs, IK1; SoA). */
+int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
+
+/* qInward of a drug run against its control: 0.5*(INaL_auc_drug/
+ * INaL_auc_ctrl + ICaL_auc_drug/ICaL_auc_ctrl) (cipa_drug_bench.cpp:376). */
+double cep_qinward(const cep_biomarkers_t *control, const cep_biomarkers_t *drug);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,230 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU oracle and to the
+reference cell models compiled from their own sources.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
+this module, and only as the checker. The product library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libcep_oracle.so"
+REF_DIR = HERE / "_ref"
+
+MODELS = {"ord2011": 0, "cipa2017": 1, "tt2006": 2, "tt2004": 3, "tomek2019": 4}
+N_STATES = {"ord2011": 41, "cipa2017": 49, "tt2006": 19, "tt2004": 17, "tomek2019": 43}
+REF_LIBS = {
+    "ord2011": "libref_ord2011.so",
+    "ord2011_tissue": "libref_ord2011_tissue.so",
+    "cipa2017": "libref_cipa2017.so",
+    "tt2006": "libref_tt2006_epi.so",
+    "tt2006_tissue": "libref_tt2006_epi_tissue.so",
+    "tt2004": "libref_tt2004b.so",
+    "tomek2019": "libref_tomek2019.so",
+}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the oracle (and, where the reference tree exists, the
+    reference models) with the committed Makefile."""
+    out = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+
+
+class CepoCell(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int), ("quirks", ctypes.c_int), ("tissue_stim", ctypes.c_int),
+                ("is_s1", ctypes.c_int), ("p", ctypes.c_double * 160)]
+
+
+class CepoCurrents(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("INa", "INaL", "Ito", "ICaL", "IKr", "IKs", "IK1", "dVdt")]
+
+
+BEAT_FIELDS = ("qnet", "inal_auc", "ical_auc", "dvmdt_repol", "dvmdt_max", "vm_peak", "vm_valley",
+               "vm_dia", "apd90", "apd50", "ca_peak", "ca_valley", "ca_dia", "cad90", "cad50")
+
+
+class CepoBeat(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in BEAT_FIELDS]
+
+
+class CepoBiomarkers(ctypes.Structure):
+    _fields_ = [("result", CepoBeat), ("steepest_pace", ctypes.c_int), ("n_eligible", ctypes.c_int),
+                ("qnet_last", ctypes.c_double), ("status", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            build()
+        L = ctypes.CDLL(str(ORACLE_SO))
+        L.cepo_init.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cepo_init_states.argtypes = [ctypes.POINTER(CepoCell), _dp]
+        L.cepo_set_pacing.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double]
+        L.cepo_step.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_double, ctypes.c_double, _dp,
+                                ctypes.POINTER(CepoCurrents)]
+        L.cepo_rates.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_double, _dp, _dp,
+                                 ctypes.POINTER(CepoCurrents)]
+        L.cepo_run.argtypes = [ctypes.POINTER(CepoCell), _dp, ctypes.c_double, ctypes.c_long, _dp, _dp,
+                               ctypes.c_long]
+        L.cepo_run_biomarkers.argtypes = [ctypes.POINTER(CepoCell), _dp, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(CepoBiomarkers), _dp, ctypes.c_long, ctypes.c_long]
+        L.cepo_run_batch.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_long, _dp,
+                                     ctypes.c_int]
+        L.cepo_run_batch.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+class Cell:
+    """One oracle cell instance."""
+
+    def __init__(self, model: str, celltype: float = 0.0, conc: float = 0.0, hill=None,
+                 is_dutta: bool = False, quirks: bool = True, tissue_stim: bool = False):
+        self.model = model
+        self.c = CepoCell()
+        h = None if hill is None else np.ascontiguousarray(hill, dtype=np.float64)
+        rc = lib().cepo_init(ctypes.byref(self.c), MODELS[model], float(celltype), float(conc),
+                             _ptr(h), 0 if h is None else len(h), int(is_dutta), int(quirks))
+        if rc != 0:
+            raise RuntimeError(f"oracle init failed for {model}: {rc}")
+        self.c.tissue_stim = int(tissue_stim)
+        self.y = np.zeros(64)
+        lib().cepo_init_states(ctypes.byref(self.c), _ptr(self.y))
+
+    @property
+    def n(self) -> int:
+        return N_STATES[self.model]
+
+    @property
+    def states(self) -> np.ndarray:
+        return self.y[: self.n]
+
+    def set_pacing(self, bcl: float, stim_start: float = -1.0, stim_dur: float = -1.0, amp_scale: float = 1.0):
+        lib().cepo_set_pacing(ctypes.byref(self.c), bcl, stim_start, stim_dur, amp_scale)
+
+    def step(self, t: float, dt: float) -> CepoCurrents:
+        cur = CepoCurrents()
+        lib().cepo_step(ctypes.byref(self.c), t, dt, _ptr(self.y), ctypes.byref(cur))
+        return cur
+
+    def rates(self, t: float) -> tuple[np.ndarray, CepoCurrents]:
+        r = np.zeros(64)
+        cur = CepoCurrents()
+        lib().cepo_rates(ctypes.byref(self.c), t, _ptr(self.y), _ptr(r), ctypes.byref(cur))
+        return r[: self.n], cur
+
+    def run(self, t0: float, dt: float, n_steps: int, v_stride: int = 0):
+        t = ctypes.c_double(t0)
+        vt = np.zeros(max(1, n_steps // v_stride) if v_stride else 1)
+        lib().cepo_run(ctypes.byref(self.c), ctypes.byref(t), dt, n_steps, _ptr(self.y),
+                       _ptr(vt) if v_stride else None, v_stride)
+        return t.value, (vt if v_stride else None)
+
+    def run_biomarkers(self, dt: float, n_pace: int, first_pace: int, dt_write: float = 1.0,
+                       qnet_vm_threshold: float = -1e300, v_stride: int = 0, v_cap: int = 0):
+        bm = CepoBiomarkers()
+        vt = np.zeros(max(1, v_cap))
+        lib().cepo_run_biomarkers(ctypes.byref(self.c), _ptr(self.y), dt, n_pace, first_pace, dt_write,
+                                  qnet_vm_threshold, ctypes.byref(bm), _ptr(vt) if v_stride else None,
+                                  v_stride, v_cap)
+        out = {f: getattr(bm.result, f) for f in BEAT_FIELDS}
+        out.update(steepest_pace=bm.steepest_pace, n_eligible=bm.n_eligible, status=bm.status)
+        return out, (vt if v_stride else None)
+
+
+def run_batch(model: str, celltype, conc, hill, bcl: float, dt: float, n_steps: int,
+              is_dutta: bool = False, quirks: bool = True, n_threads: int = 1):
+    """Threaded fixed-step run over a batch (the CPU baseline)."""
+    n = len(conc)
+    ct = np.ascontiguousarray(celltype, dtype=np.float64)
+    cc = np.ascontiguousarray(conc, dtype=np.float64)
+    hh = np.ascontiguousarray(hill, dtype=np.float64)
+    out = np.zeros((n, N_STATES[model]))
+    used = lib().cepo_run_batch(MODELS[model], n, _ptr(ct), _ptr(cc), _ptr(hh), hh.shape[1], int(is_dutta),
+                                int(quirks), bcl, dt, n_steps, _ptr(out), n_threads)
+    return out, used
+
+
+class RefCell:
+    """The reference model object compiled from its own sources."""
+
+    def __init__(self, key: str, celltype: float = 0.0, conc: float = 0.0, hill=None, is_dutta: bool = False):
+        path = REF_DIR / REF_LIBS[key]
+        if not path.exists():
+            raise FileNotFoundError(path)
+        L = ctypes.CDLL(str(path))
+        L.ref_new.restype = ctypes.c_void_p
+        for f in ("ref_states", "ref_consts", "ref_rates", "ref_alg"):
+            getattr(L, f).restype = _dp
+            getattr(L, f).argtypes = [ctypes.c_void_p]
+        L.ref_init.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int]
+        L.ref_run.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_long, _dp, ctypes.c_long]
+        L.ref_compute_rates.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.ref_solve.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.ref_set_s1.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_set_ectopic.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_sizes.argtypes = [ctypes.c_void_p, _ip, _ip, _ip]
+        L.ref_free.argtypes = [ctypes.c_void_p]
+        self.L = L
+        self.h = L.ref_new()
+        self._hill = np.zeros(32) if hill is None else np.concatenate([np.asarray(hill, float), np.zeros(32)])
+        L.ref_init(self.h, float(celltype), float(conc), _ptr(self._hill), int(is_dutta))
+        ns, nc, na = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.ref_sizes(self.h, ctypes.byref(ns), ctypes.byref(nc), ctypes.byref(na))
+        self.n, self.nc, self.na = ns.value, nc.value, na.value
+        L.ref_set_s1(self.h, 0)
+        L.ref_set_ectopic(self.h, 0)
+
+    def __del__(self):
+        try:
+            self.L.ref_free(self.h)
+        except Exception:
+            pass
+
+    def arr(self, which: str, n: int) -> np.ndarray:
+        p = getattr(self.L, "ref_" + which)(self.h)
+        return np.ctypeslib.as_array(p, shape=(n,))
+
+    @property
+    def states(self) -> np.ndarray:
+        return self.arr("states", self.n)
+
+    @property
+    def consts(self) -> np.ndarray:
+        return self.arr("consts", self.nc)
+
+    def run(self, t0: float, dt: float, n_steps: int, v_stride: int = 0):
+        t = ctypes.c_double(t0)
+        vt = np.zeros(max(1, n_steps // v_stride) if v_stride else 1)
+        self.L.ref_run(self.h, ctypes.byref(t), dt, n_steps, _ptr(vt) if v_stride else None, v_stride)
+        return t.value, (vt if v_stride else None)
+
+
+def ref_available(key: str) -> bool:
+    return (REF_DIR / REF_LIBS[key]).exists()

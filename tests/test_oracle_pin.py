@@ -1,0 +1,80 @@
+"""Pin the CPU oracle: bitwise against the reference compiled from its own
+sources (where oracle/_ref exists) and against the committed golden
+fixtures generated from that reference (everywhere)."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLD = Path(__file__).resolve().parent / "golden"
+ORD_CASES = sorted(GOLD.glob("ord_*.npz"))
+
+
+@pytest.mark.parametrize("path", ORD_CASES, ids=lambda p: p.stem)
+def test_ord_oracle_matches_reference_golden(oracle, path):
+    g = np.load(path)
+    c = oracle.Cell("ord2011", float(g["celltype"]), float(g["conc"]), g["hill"], is_dutta=bool(g["dutta"]),
+                    quirks=True)
+    c.set_pacing(float(g["bcl"]))
+    assert np.array_equal(c.states, g["y0"])
+    r, _ = c.rates(0.0)
+    assert np.array_equal(r, g["rates0"]), "RATES at t=0 differ from the reference"
+    t, v = c.run(0.0, float(g["dt"]), int(g["n_steps"]), int(g["stride"]))
+    # the restatement follows the reference's evaluation order: bit-exact
+    assert np.array_equal(v, g["v_trace"])
+    assert np.array_equal(c.states, g["final_states"])
+    assert t == float(g["t_final"])
+
+
+@pytest.mark.parametrize("dutta", [0, 1])
+@pytest.mark.parametrize("celltype", [0.0, 1.0, 2.0])
+def test_ord_oracle_bitwise_vs_compiled_reference(oracle, dutta, celltype):
+    if not oracle.ref_available("ord2011"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    rng = np.random.default_rng(int(celltype * 10 + dutta))
+    hill = np.zeros(14)
+    hill[0::2] = 10 ** rng.uniform(-1, 2, 7)
+    hill[1::2] = rng.uniform(0.6, 1.8, 7)
+    hill[6] = 0.0  # INa NA -> no block
+    conc = 4.2
+    r = oracle.RefCell("ord2011", celltype, conc, hill, is_dutta=bool(dutta))
+    c = oracle.Cell("ord2011", celltype, conc, hill, is_dutta=bool(dutta), quirks=True)
+    n = 60000
+    t1, v1 = r.run(0.0, 0.005, n, 50)
+    t2, v2 = c.run(0.0, 0.005, n, 50)
+    assert np.array_equal(v1, v2)
+    assert np.array_equal(r.states, c.states)
+
+
+def test_ord_quirks_documented(oracle):
+    """The quirk switch changes exactly what the oracle header documents:
+    with no drug, no Dutta and celltype endo only the fcafp step differs."""
+    a = oracle.Cell("ord2011", 0.0, 0.0, None, quirks=True)
+    b = oracle.Cell("ord2011", 0.0, 0.0, None, quirks=False)
+    a.set_pacing(1000.0)
+    b.set_pacing(1000.0)
+    a.run(0.0, 0.005, 4000)
+    b.run(0.0, 0.005, 4000)
+    d = np.abs(a.states - b.states)
+    assert d[32] > 0  # fcafp (STATES index 32) uses 25 vs dt
+    # celltype is honoured only without quirks
+    e = oracle.Cell("ord2011", 1.0, 0.0, None, quirks=True)
+    f = oracle.Cell("ord2011", 0.0, 0.0, None, quirks=True)
+    e.run(0.0, 0.005, 2000)
+    f.run(0.0, 0.005, 2000)
+    assert np.array_equal(e.states, f.states)
+
+
+def test_biomarker_state_machine_last_beat(oracle):
+    """Last-beat biomarkers of the control ORd cell are physiological and
+    self-consistent (APD90 > APD50 > 0, CaD90 > CaD50 > 0, qNet finite)."""
+    c = oracle.Cell("ord2011", 0.0, 0.0, None, quirks=True)
+    c.set_pacing(1000.0)
+    bm, _ = c.run_biomarkers(0.005, 3, 2, dt_write=1.0)
+    assert bm["status"] == 0 and bm["n_eligible"] == 1
+    assert 150 < bm["apd90"] < 400 and 0 < bm["apd50"] < bm["apd90"]
+    assert 0 < bm["cad50"] < bm["cad90"]
+    assert bm["vm_peak"] > 0 and bm["dvmdt_max"] > 50
+    assert np.isfinite(bm["qnet"])
