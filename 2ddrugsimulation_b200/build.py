@@ -21,6 +21,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libcep_b200.so"
 BUILD_DIR = PKG / "_build"
+PROBE_LIB = LIB_DIR / "libcep_probe.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--prec-div=false",
@@ -70,6 +71,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         out = subprocess.run(cmd, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError(f"link failed:\n{out.stdout}\n{out.stderr}")
+    # measurement probes (bench.py roofline denominators), a separate library
+    probe_src = PKG / "probes" / "peaks.cu"
+    if probe_src.exists() and (force or not PROBE_LIB.exists() or probe_src.stat().st_mtime > PROBE_LIB.stat().st_mtime):
+        cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", str(probe_src), "-o",
+               str(PROBE_LIB)]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError(f"probe build failed:\n{out.stdout}\n{out.stderr}")
     if verbose:
         for l in logs:
             sys.stderr.write(l)

@@ -100,6 +100,24 @@ struct OrdModel {
   __host__ __device__ static constexpr int p_amp() { return ord::P_amp; }
 };
 
+struct CipaModel : OrdModel {
+  static constexpr int kStates = ord::cipa::kNumStates;
+  static constexpr int kCai = ord::cipa::cai;
+  template <class G>
+  __device__ static void load(Y<G> &y, const double *s, int64_t ld, int64_t i) { ord::load_cipa(y, s, ld, i); }
+  template <class G>
+  __device__ static void store(const Y<G> &y, double *s, int64_t ld, int64_t i) { ord::store_cipa(y, s, ld, i); }
+  template <class P>
+  __device__ static void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                              int stim_mode, bool update, Cur<typename P::G> &c) {
+    ord::step<P, true>(y, q, t, dt, stim_mode, update, c);
+  }
+  __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
+                              const double *hill, unsigned flags) {
+    ord::init_instance_cipa(par, s, ld, i, ct, conc, hill, flags & CEP_FLAG_QUIRKS);
+  }
+};
+
 // ----------------------------------------------------------------- kernels
 template <class M>
 __global__ void init_kernel(double *par, double *s, int64_t ld, int n, const double *celltype,
@@ -298,8 +316,13 @@ const ModelInfo *model_info(int model) {
                                   &Ops<OrdModel>::launch_init, &Ops<OrdModel>::launch_pacing,
                                   &Ops<OrdModel>::launch_reset, &Ops<OrdModel>::launch_run,
                                   &Ops<OrdModel>::launch_rates, OrdModel::p_bcl()};
+  static const ModelInfo cipa_info{CipaModel::kStates, CipaModel::kParams, CipaModel::kCai,
+                                   &Ops<CipaModel>::launch_init, &Ops<CipaModel>::launch_pacing,
+                                   &Ops<CipaModel>::launch_reset, &Ops<CipaModel>::launch_run,
+                                   &Ops<CipaModel>::launch_rates, CipaModel::p_bcl()};
   switch (model) {
     case CEP_MODEL_ORD2011: return &ord_info;
+    case CEP_MODEL_CIPA2017: return &cipa_info;
     default: return nullptr;
   }
 }

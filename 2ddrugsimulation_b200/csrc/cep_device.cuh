@@ -13,14 +13,37 @@
 
 namespace cep {
 
+// Reciprocal in FP64 by Newton-Raphson refinement of the hardware's 20-bit
+// reciprocal seed (rcp.approx.ftz.f64): two steps r <- r + r(1 - x r) give
+// a result within about an ulp. +-inf maps to +-0 as IEEE division would.
+__device__ __forceinline__ double rcp64(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  return isinf(x) ? copysign(0.0, x) : r;
+}
+// a / b as a * (1/b) with one residual correction (q + r (a - b q)).
+__device__ __forceinline__ double div64(double a, double b) {
+  const double r = rcp64(b);
+  const double q = a * r;
+  const double res = fma(-b, q, a);
+  const double out = fma(r, res, q);
+  return isinf(b) ? a * r : out;
+}
+
 struct F64 {
   using G = double;
   static constexpr bool kMixed = false;
   __device__ __forceinline__ static double ex(double x) { return ::exp(x); }
   __device__ __forceinline__ static double lg(double x) { return ::log(x); }
-  __device__ __forceinline__ static double dv(double a, double b) { return a / b; }
-  __device__ __forceinline__ static double rc(double x) { return 1.0 / x; }
-  __device__ __forceinline__ static double pw(double x, double y) { return ::pow(x, y); }
+  __device__ __forceinline__ static double dv(double a, double b) { return div64(a, b); }
+  __device__ __forceinline__ static double rc(double x) { return rcp64(x); }
+  // x^y for x > 0 as exp(y log x) (the exponents here are constants of
+  // order 1, so the error stays at a few ulp)
+  __device__ __forceinline__ static double pw(double x, double y) { return ::exp(y * ::log(x)); }
   __device__ __forceinline__ static double sq(double x) { return ::sqrt(x); }
 };
 
@@ -50,11 +73,29 @@ __device__ __forceinline__ float ghk_factor(float x) {
   return __fdividef(x, __expf(x) - 1.0f);
 }
 
-// Rush-Larsen update y_inf - (y_inf - y) * exp(-dt/tau).
-template <class P>
-__device__ __forceinline__ typename P::G rush_larsen(typename P::G y, typename P::G yinf,
-                                                     typename P::G tau, typename P::G dt) {
-  return yinf - (yinf - y) * P::ex(P::dv(-dt, tau));
+// Rush-Larsen update of a gate whose state is kept in FP64.
+//   F64  : y_inf - (y_inf - y) * exp(-dt/tau), the reference's form.
+//   Mixed: y + (y_inf - y) * (1 - exp(-dt/tau)) with the increment formed in
+//          FP32 and accumulated in FP64. At dt = 0.005 ms a gate with a time
+//          constant of a second changes by ~1e-7 per step, below FP32
+//          resolution of the state itself, so only the increment is FP32.
+//          `slow` gates (tau >= 0.5 ms everywhere) take 1 - e^-a from its
+//          Taylor series (a <= 0.01: relative error < 1e-10); the others
+//          from the SFU exponential.
+template <class P, bool slow = false>
+__device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, typename P::G tau, double dt) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) {
+    const G a = P::dv((G)dt, tau);
+    G f;
+    if constexpr (slow)
+      f = a * ((G)1 - a * ((G)0.5 - a * ((G)(1.0 / 6.0) - a * (G)(1.0 / 24.0))));
+    else
+      f = (G)1 - P::ex(-a);
+    return y + (double)((yinf - (G)y) * f);
+  } else {
+    return yinf - (yinf - y) * ::exp(div64(-dt, tau));
+  }
 }
 
 // Per-instance biomarker bookkeeping (the CiPA per-beat state machine) kept in

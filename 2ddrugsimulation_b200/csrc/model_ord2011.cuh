@@ -23,11 +23,38 @@ enum : int {
   Jrelnp, Jrelp
 };
 
+// CiPA-ORd v1 2017 STATES order (enums/enum_ohara_rudy_cipa_v1_2017.hpp):
+// the ORd states without xrf/xrs, the nine Markov IKr states and the drug
+// concentration D.
+namespace cipa {
+constexpr int kNumStates = 49;
+enum : int {
+  V = 0, CaMKt, cass, nai, nass, ki, kss, cansr, cajsr, cai, m, hf, hs, j, hsp, jp, mL, hL, hLp, a, iF,
+  iS, ap, iFp, iSp, d, ff, fs, fcaf, fcas, jca, ffp, fcafp, nca, IC1, IC2, C1, C2, O, IO, IObound, Obound,
+  Cbound, D, xs1, xs2, xk1, Jrelnp, Jrelp
+};
+// Q10 factors exp(((37 - 20) * log(q)) / 10) of the hERG transitions
+// (ohara_rudy_cipa_v1_2017.cpp:2157-2165), evaluated once in FP64.
+constexpr double Q1 = 14.611493102188247, Q2 = 11.608567327201762, Q3 = 15.227075177403329;
+constexpr double Q4 = 9.540792127868109, Q11 = 15.122885354397773, Q21 = 11.265446673074576;
+constexpr double Q31 = 11.561952122102017, Q41 = 1.9006143161790194, Q51 = 15.425846568000235;
+constexpr double Q52 = 13.700335619455835, Q53 = 4.4672619154839515, Q61 = 18.522034347349482;
+constexpr double Q62 = 15.425846568000235, Q63 = 19.171323250640047;
+// A and B of the transition rates A*exp(B*V)*Q (active ___initConsts block)
+constexpr double A1 = 0.0264, B1 = 4.631E-05, A2 = 4.986E-06, B2 = -0.004226, A3 = 0.001214, B3 = 0.008516;
+constexpr double A4 = 1.854E-05, B4 = -0.04641, A11 = 0.0007868, B11 = 1.535E-08, A21 = 5.455E-06;
+constexpr double B21 = -0.1688, A31 = 0.005509, B31 = 7.771E-09, A41 = 0.001416, B41 = -0.02877;
+constexpr double A51 = 0.4492, B51 = 0.008595, A52 = 0.3181, B52 = 3.613E-08, A53 = 0.149, B53 = 0.004668;
+constexpr double A61 = 0.01241, B61 = 0.1725, A62 = 0.3226, B62 = -0.0006575, A63 = 0.008978, B63 = -0.02215;
+}  // namespace cipa
+
 // Per-instance parameter block (one SoA row per entry).
 enum : int {
   P_GNa = 0, P_GNaL, P_Gto, P_PCa, P_PCap, P_PCaNa, P_PCaK, P_PCaNap, P_PCaKp, P_GKr, P_GKs, P_GK1,
   P_GKb, P_Gncx, P_Pnak, P_cmdnmax, P_upScale, P_Aff, P_Afs, P_tjca, P_H, P_celltype, P_fcafp_dt,
-  P_amp, P_BCL, P_stim_start, P_duration, kNumParams
+  P_amp, P_BCL, P_stim_start, P_duration,
+  P_bind, P_Ku, P_Kt, P_Vhalf,  // CiPA dynamic hERG drug binding
+  kNumParams
 };
 
 // Instance-independent constants of ___initConsts (Ohara_Rudy_2011.cpp:494-678).
@@ -70,9 +97,11 @@ constexpr double a3c = k3p * (ko / Kko) * (ko / Kko), ko_Kko_sq = (1.0 + ko / Kk
 
 template <class G>
 struct Y {
+  // every state is stored in FP64; the mixed path computes from FP32 copies
   double V, CaMKt, cass, nai, nass, ki, kss, cansr, cajsr, cai;
-  G m, hf, hs, j, hsp, jp, mL, hL, hLp, a, iF, iS, ap, iFp, iSp, d, ff, fs, fcaf, fcas, jca, ffp,
+  double m, hf, hs, j, hsp, jp, mL, hL, hLp, a, iF, iS, ap, iFp, iSp, d, ff, fs, fcaf, fcas, jca, ffp,
       fcafp, nca, xrf, xrs, xs1, xs2, xk1, Jrelnp, Jrelp;
+  double IC1, IC2, C1, C2, O, IO, IObound, Obound, Cbound;  // CiPA Markov IKr
 };
 
 template <class G>
@@ -82,6 +111,7 @@ struct Par {
   G fcafp_dt;  // 0: use dt
   int celltype;
   double amp, BCL, stim_start, duration;
+  G bind, Ku, Kt, Vhalf;  // CiPA: Kmax*Ku*D^n/(D^n + halfmax), unbinding, trapping
 };
 
 template <class G>
@@ -96,7 +126,7 @@ __device__ __forceinline__ void load(Y<G> &y, const double *__restrict__ s, int6
   y.nai = s[nai * ld + i]; y.nass = s[nass * ld + i]; y.ki = s[ki * ld + i];
   y.kss = s[kss * ld + i]; y.cansr = s[cansr * ld + i]; y.cajsr = s[cajsr * ld + i];
   y.cai = s[cai * ld + i];
-#define CEP_LD(n) y.n = (G)s[n * ld + i];
+#define CEP_LD(n) y.n = s[n * ld + i];
   CEP_LD(m) CEP_LD(hf) CEP_LD(hs) CEP_LD(j) CEP_LD(hsp) CEP_LD(jp) CEP_LD(mL) CEP_LD(hL) CEP_LD(hLp)
   CEP_LD(a) CEP_LD(iF) CEP_LD(iS) CEP_LD(ap) CEP_LD(iFp) CEP_LD(iSp) CEP_LD(d) CEP_LD(ff) CEP_LD(fs)
   CEP_LD(fcaf) CEP_LD(fcas) CEP_LD(jca) CEP_LD(ffp) CEP_LD(fcafp) CEP_LD(nca) CEP_LD(xrf) CEP_LD(xrs)
@@ -110,7 +140,7 @@ __device__ __forceinline__ void store(const Y<G> &y, double *__restrict__ s, int
   s[nai * ld + i] = y.nai; s[nass * ld + i] = y.nass; s[ki * ld + i] = y.ki;
   s[kss * ld + i] = y.kss; s[cansr * ld + i] = y.cansr; s[cajsr * ld + i] = y.cajsr;
   s[cai * ld + i] = y.cai;
-#define CEP_ST(n) s[n * ld + i] = (double)y.n;
+#define CEP_ST(n) s[n * ld + i] = y.n;
   CEP_ST(m) CEP_ST(hf) CEP_ST(hs) CEP_ST(j) CEP_ST(hsp) CEP_ST(jp) CEP_ST(mL) CEP_ST(hL) CEP_ST(hLp)
   CEP_ST(a) CEP_ST(iF) CEP_ST(iS) CEP_ST(ap) CEP_ST(iFp) CEP_ST(iSp) CEP_ST(d) CEP_ST(ff) CEP_ST(fs)
   CEP_ST(fcaf) CEP_ST(fcas) CEP_ST(jca) CEP_ST(ffp) CEP_ST(fcafp) CEP_ST(nca) CEP_ST(xrf) CEP_ST(xrs)
@@ -135,6 +165,34 @@ __device__ __forceinline__ void load_par(Par<G> &q, const double *__restrict__ p
   q.celltype = (int)p[P_celltype * ld + i];
   q.amp = p[P_amp * ld + i]; q.BCL = p[P_BCL * ld + i];
   q.stim_start = p[P_stim_start * ld + i]; q.duration = p[P_duration * ld + i];
+  q.bind = (G)p[P_bind * ld + i]; q.Ku = (G)p[P_Ku * ld + i]; q.Kt = (G)p[P_Kt * ld + i];
+  q.Vhalf = (G)p[P_Vhalf * ld + i];
+}
+
+// CiPA state layout <-> registers
+template <class G>
+__device__ __forceinline__ void load_cipa(Y<G> &y, const double *__restrict__ s, int64_t ld, int64_t i) {
+#define CEP_LD(n) y.n = s[cipa::n * ld + i];
+  CEP_LD(V) CEP_LD(CaMKt) CEP_LD(cass) CEP_LD(nai) CEP_LD(nass) CEP_LD(ki) CEP_LD(kss) CEP_LD(cansr)
+  CEP_LD(cajsr) CEP_LD(cai) CEP_LD(m) CEP_LD(hf) CEP_LD(hs) CEP_LD(j) CEP_LD(hsp) CEP_LD(jp) CEP_LD(mL)
+  CEP_LD(hL) CEP_LD(hLp) CEP_LD(a) CEP_LD(iF) CEP_LD(iS) CEP_LD(ap) CEP_LD(iFp) CEP_LD(iSp) CEP_LD(d)
+  CEP_LD(ff) CEP_LD(fs) CEP_LD(fcaf) CEP_LD(fcas) CEP_LD(jca) CEP_LD(ffp) CEP_LD(fcafp) CEP_LD(nca)
+  CEP_LD(IC1) CEP_LD(IC2) CEP_LD(C1) CEP_LD(C2) CEP_LD(O) CEP_LD(IO) CEP_LD(IObound) CEP_LD(Obound)
+  CEP_LD(Cbound) CEP_LD(xs1) CEP_LD(xs2) CEP_LD(xk1) CEP_LD(Jrelnp) CEP_LD(Jrelp)
+#undef CEP_LD
+  y.xrf = 0.0; y.xrs = 0.0;
+}
+
+template <class G>
+__device__ __forceinline__ void store_cipa(const Y<G> &y, double *__restrict__ s, int64_t ld, int64_t i) {
+#define CEP_ST(n) s[cipa::n * ld + i] = y.n;
+  CEP_ST(V) CEP_ST(CaMKt) CEP_ST(cass) CEP_ST(nai) CEP_ST(nass) CEP_ST(ki) CEP_ST(kss) CEP_ST(cansr)
+  CEP_ST(cajsr) CEP_ST(cai) CEP_ST(m) CEP_ST(hf) CEP_ST(hs) CEP_ST(j) CEP_ST(hsp) CEP_ST(jp) CEP_ST(mL)
+  CEP_ST(hL) CEP_ST(hLp) CEP_ST(a) CEP_ST(iF) CEP_ST(iS) CEP_ST(ap) CEP_ST(iFp) CEP_ST(iSp) CEP_ST(d)
+  CEP_ST(ff) CEP_ST(fs) CEP_ST(fcaf) CEP_ST(fcas) CEP_ST(jca) CEP_ST(ffp) CEP_ST(fcafp) CEP_ST(nca)
+  CEP_ST(IC1) CEP_ST(IC2) CEP_ST(C1) CEP_ST(C2) CEP_ST(O) CEP_ST(IO) CEP_ST(IObound) CEP_ST(Obound)
+  CEP_ST(Cbound) CEP_ST(xs1) CEP_ST(xs2) CEP_ST(xk1) CEP_ST(Jrelnp) CEP_ST(Jrelp)
+#undef CEP_ST
 }
 
 // Periodic single-cell stimulus of computeRates (Ohara_Rudy_2011.cpp:747);
@@ -145,13 +203,20 @@ __device__ __forceinline__ bool stim_on(double t, double start, double bcl, doub
 
 // One cell step: rates at (t, y); if `update`, the Rush-Larsen / forward
 // Euler update of y by dt. `cur` receives the currents at (t, y).
-template <class P>
+template <class P, bool kCipa = false>
 __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
                                      int stim_mode, bool update, Cur<typename P::G> &cur) {
   using G = typename P::G;
   const G v = (G)y.V;
   const G one = (G)1;
   const bool on = stim_mode < 0 ? stim_on(t, q.stim_start, q.BCL, q.duration) : (stim_mode != 0);
+  // FP32 (mixed) or FP64 working copies of the gates
+  const G g_m = (G)y.m, g_hf = (G)y.hf, g_hs = (G)y.hs, g_j = (G)y.j, g_hsp = (G)y.hsp, g_jp = (G)y.jp;
+  const G g_mL = (G)y.mL, g_hL = (G)y.hL, g_hLp = (G)y.hLp, g_a = (G)y.a, g_iF = (G)y.iF, g_iS = (G)y.iS;
+  const G g_ap = (G)y.ap, g_iFp = (G)y.iFp, g_iSp = (G)y.iSp, g_d = (G)y.d, g_ff = (G)y.ff, g_fs = (G)y.fs;
+  const G g_fcaf = (G)y.fcaf, g_fcas = (G)y.fcas, g_jca = (G)y.jca, g_ffp = (G)y.ffp, g_fcafp = (G)y.fcafp, g_nca = (G)y.nca;
+  const G g_xrf = (G)y.xrf, g_xrs = (G)y.xrs, g_xs1 = (G)y.xs1, g_xs2 = (G)y.xs2, g_xk1 = (G)y.xk1, g_Jrelnp = (G)y.Jrelnp;
+  const G g_Jrelp = (G)y.Jrelp;
   const G Istim = on ? (G)q.amp : (G)0;
   // gate steady states and time constants
   const G hLss = one / (one + P::ex((v + (G)87.61) * (G)(1.0 / 7.488)));
@@ -174,7 +239,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G tfs = (G)1000.0 + one / ((G)3.5e-05 * P::ex(-(v + (G)5.0) * (G)0.25) +
                                    (G)3.5e-05 * P::ex((v + (G)5.0) * (G)(1.0 / 6.0)));
   const G fcass = fss;
-  const G km2n = y.jca;
+  const G km2n = g_jca;
   const G cass_g = (G)y.cass;
   const G anca = one / ((G)k::k2n / km2n + p4(one + (G)k::Kmn / cass_g));
   const G xrss = one / (one + P::ex(-(v + (G)8.337) * (G)(1.0 / 6.789)));
@@ -218,16 +283,16 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G tiFp = dti_develop * dti_recover * tiF;
   const G tiSp = dti_develop * dti_recover * tiS;
   // ICaL and its Na/K components
-  const G f = q.Aff * y.ff + q.Afs * y.fs;
+  const G f = q.Aff * g_ff + q.Afs * g_fs;
   const G Afcaf = (G)0.3 + (G)0.6 / (one + P::ex((v - (G)10.0) * (G)0.1));
   const G Afcas = one - Afcaf;
-  const G fca = Afcaf * y.fcaf + Afcas * y.fcas;
-  const G fp = q.Aff * y.ffp + q.Afs * y.fs;
-  const G fcap = Afcaf * y.fcafp + Afcas * y.fcas;
+  const G fca = Afcaf * g_fcaf + Afcas * g_fcas;
+  const G fp = q.Aff * g_ffp + q.Afs * g_fs;
+  const G fcap = Afcaf * g_fcafp + Afcas * g_fcas;
   const G fICaLp = (G)(1.0 / (1.0 + k::KmCaMK / CaMKa));
-  const G nca_ = y.nca;
-  const G gate_np = y.d * (f * (one - nca_) + y.jca * fca * nca_);
-  const G gate_p = y.d * (fp * (one - nca_) + y.jca * fcap * nca_);
+  const G nca_ = g_nca;
+  const G gate_np = g_d * (f * (one - nca_) + g_jca * fca * nca_);
+  const G gate_p = g_d * (fp * (one - nca_) + g_jca * fcap * nca_);
   G PhiCaL, PhiCaNa, PhiCaK, INab, ICab;
   {
     const G vfrt = v * (G)k::FRT;
@@ -241,6 +306,25 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
       PhiCaK = g1 * ((G)0.75 * (G)y.kss * e1 - (G)(0.75 * k::ko));
       INab = (G)k::PNab * g1 * ((G)y.nai * e1 - (G)k::nao);
       ICab = (G)(k::PCab * 4.0) * g2 * ((G)y.cai * e2 - (G)(0.341 * k::cao));
+    } else if constexpr (kCipa) {
+      // CiPA-ORd v1 form A*U/(e^U - 1) with the |U| <= 1e-7 guard
+      // (ohara_rudy_cipa_v1_2017.cpp:2287-2289 and the INab/ICab/ICaNa/ICaK
+      // analogues); e^U is the same exponential as the numerator's.
+      const double vfrt_d = y.V * k::FRT, ffrt = k::F * k::FRT;
+      const double e1 = ::exp(vfrt_d), e2 = ::exp(2.0 * vfrt_d);
+      const double U1 = (2.0 * k::FRT) * y.V, U2 = k::FRT * y.V;
+      const bool s1 = -1.0e-07 <= U1 && U1 <= 1.0e-07, s2 = -1.0e-07 <= U2 && U2 <= 1.0e-07;
+      const double A1 = (4.0 * ffrt * (y.cass * e2 - 0.341 * k::cao)) / (2.0 * k::FRT);
+      const double A2 = (0.75 * ffrt * (y.nass * e1 - k::nao)) / k::FRT;
+      const double A3 = (0.75 * ffrt * (y.kss * e1 - k::ko)) / k::FRT;
+      const double An = (k::PNab * ffrt * (y.nai * e1 - k::nao)) / k::FRT;
+      const double Ac = (k::PCab * 4.0 * ffrt * (y.cai * e2 - 0.341 * k::cao)) / (2.0 * k::FRT);
+      const double r1 = div64(U1, e2 - 1.0), r2 = div64(U2, e1 - 1.0);
+      PhiCaL = s1 ? A1 * (1.0 - 0.5 * U1) : A1 * r1;
+      PhiCaNa = s2 ? A2 * (1.0 - 0.5 * U2) : A2 * r2;
+      PhiCaK = s2 ? A3 * (1.0 - 0.5 * U2) : A3 * r2;
+      INab = s2 ? An * (1.0 - 0.5 * U2) : An * r2;
+      ICab = s1 ? Ac * (1.0 - 0.5 * U1) : Ac * r1;
     } else {
       const double vffrt = (y.V * k::F * k::F) / (k::R * k::T);
       const double vfrt_d = (y.V * k::F) / (k::R * k::T);
@@ -270,21 +354,27 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G EK = (G)k::RTF * P::lg((G)k::ko / (G)y.ki);
   const G AiF = one / (one + P::ex((v - (G)213.6) * (G)(1.0 / 151.2)));
   const G AiS = one - AiF;
-  const G i_ = AiF * y.iF + AiS * y.iS;
-  const G ip = AiF * y.iFp + AiS * y.iSp;
+  const G i_ = AiF * g_iF + AiS * g_iS;
+  const G ip = AiF * g_iFp + AiS * g_iSp;
   const G fCaMKp = fICaLp;  // fItop, fINap, fINaLp, fJrelp, fJupp share 1/(1+KmCaMK/CaMKa)
-  const G Ito = q.Gto * (v - EK) * ((one - fCaMKp) * y.a * i_ + fCaMKp * y.ap * ip);
-  const G Axrf = one / (one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21)));
-  const G Axrs = one - Axrf;
-  const G xr = Axrf * y.xrf + Axrs * y.xrs;
-  const G rkr = (one / (one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0)))) / (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0)));
-  const G IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
+  const G Ito = q.Gto * (v - EK) * ((one - fCaMKp) * g_a * i_ + fCaMKp * g_ap * ip);
+  G IKr;
+  if constexpr (kCipa) {
+    // dynamic hERG: IKr = GKr sqrt(ko/5.4) O (V - EK) (ohara_rudy_cipa_v1_2017.cpp:2307)
+    IKr = q.GKr * (G)k::sqrt_ko54 * (G)y.O * (v - EK);
+  } else {
+    const G Axrf = one / (one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21)));
+    const G Axrs = one - Axrf;
+    const G xr = Axrf * g_xrf + Axrs * g_xrs;
+    const G rkr = (one / (one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0)))) / (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0)));
+    IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
+  }
   const G EKs = (G)k::RTF * P::lg((G)(k::ko + k::PKNa * k::nao) / (G)(y.ki + k::PKNa * y.nai));
   const G cai_g = (G)y.cai;
   const G KsCa = one + (G)0.6 / (one + P::pw((G)3.8e-05 / cai_g, (G)1.4));
-  const G IKs = q.GKs * KsCa * y.xs1 * y.xs2 * (v - EKs);
+  const G IKs = q.GKs * KsCa * g_xs1 * g_xs2 * (v - EKs);
   const G rk1 = one / (one + P::ex(((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493)));
-  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * y.xk1 * (v - EK);
+  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * g_xk1 * (v - EK);
   // Na/K pump
   const G nai_g = (G)y.nai, ki_g = (G)y.ki;
   const G Knao = (G)k::Knao0 * P::ex(((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
@@ -316,10 +406,10 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G IKb = q.GKb * xkb * (v - EK);
   // sodium currents
   const G ENa = (G)k::RTF * P::lg((G)k::nao / (G)y.nai);
-  const G h_ = (G)k::Ahf * y.hf + (G)k::Ahs * y.hs;
-  const G hp = (G)k::Ahf * y.hf + (G)k::Ahs * y.hsp;
-  const G INa = q.GNa * (v - ENa) * p3(y.m) * ((one - fCaMKp) * h_ * y.j + fCaMKp * hp * y.jp);
-  const G INaL = q.GNaL * (v - ENa) * y.mL * ((one - fCaMKp) * y.hL + fCaMKp * y.hLp);
+  const G h_ = (G)k::Ahf * g_hf + (G)k::Ahs * g_hs;
+  const G hp = (G)k::Ahf * g_hf + (G)k::Ahs * g_hsp;
+  const G INa = q.GNa * (v - ENa) * p3(g_m) * ((one - fCaMKp) * h_ * g_j + fCaMKp * hp * g_jp);
+  const G INaL = q.GNaL * (v - ENa) * g_mL * ((one - fCaMKp) * g_hL + fCaMKp * g_hLp);
   // Na/Ca exchanger, myoplasmic and subspace compartments
   const G hna = P::ex(((G)k::qna * v) * (G)k::FRT);
   const G hca = P::ex(((G)k::qca * v) * (G)k::FRT);
@@ -379,7 +469,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G JdiffNa = (G)((y.nass - y.nai) * 0.5);
   const G Jdiff = (G)((y.cass - y.cai) * 5.0);
   const G Jtr = (G)((y.cansr - y.cajsr) * 0.01);
-  const G Jrel = (one - fCaMKp) * y.Jrelnp + fCaMKp * y.Jrelp;
+  const G Jrel = (one - fCaMKp) * g_Jrelnp + fCaMKp * g_Jrelp;
   const G Bcass = one / (one + (G)(k::BSRmax * k::KmBSR) / p2((G)k::KmBSR + cass_g) +
                          (G)(k::BSLmax * k::KmBSL) / p2((G)k::KmBSL + cass_g));
   const G Jupnp = (q.upScale * (G)0.004375 * cai_g) / (cai_g + (G)0.00092);
@@ -409,41 +499,84 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   const G dcajsr = Bcajsr * (Jtr - Jrel);
   const double dCaMKt = k::aCaMK * CaMKb * (CaMKb + y.CaMKt) - k::bCaMK * y.CaMKt;
   // Rush-Larsen gates
-  const G gdt = (G)dt;
-  y.m = rush_larsen<P>(y.m, mss, tm, gdt);
-  y.hf = rush_larsen<P>(y.hf, hss, thf, gdt);
-  y.hs = rush_larsen<P>(y.hs, hss, ths, gdt);
-  y.j = rush_larsen<P>(y.j, jss, tj, gdt);
-  y.hsp = rush_larsen<P>(y.hsp, hssp, thsp, gdt);
-  y.jp = rush_larsen<P>(y.jp, jss, tjp, gdt);
-  y.mL = rush_larsen<P>(y.mL, mLss, tmL, gdt);
-  y.hL = rush_larsen<P>(y.hL, hLss, (G)k::thL, gdt);
-  y.hLp = rush_larsen<P>(y.hLp, hLssp, (G)k::thLp, gdt);
-  y.a = rush_larsen<P>(y.a, ass, ta, gdt);
-  y.iF = rush_larsen<P>(y.iF, iss, tiF, gdt);
-  y.iS = rush_larsen<P>(y.iS, iss, tiS, gdt);
-  y.ap = rush_larsen<P>(y.ap, assp, ta, gdt);
-  y.iFp = rush_larsen<P>(y.iFp, iss, tiFp, gdt);
-  y.iSp = rush_larsen<P>(y.iSp, iss, tiSp, gdt);
-  y.d = rush_larsen<P>(y.d, dss, td, gdt);
-  y.ff = rush_larsen<P>(y.ff, fss, tff, gdt);
-  y.fs = rush_larsen<P>(y.fs, fss, tfs, gdt);
-  y.fcaf = rush_larsen<P>(y.fcaf, fcass, tfcaf, gdt);
-  y.fcas = rush_larsen<P>(y.fcas, fcass, tfcas, gdt);
-  y.jca = rush_larsen<P>(y.jca, fcass, q.tjca, gdt);
-  y.ffp = rush_larsen<P>(y.ffp, fss, tffp, gdt);
-  y.fcafp = rush_larsen<P>(y.fcafp, fcass, tfcafp, q.fcafp_dt != (G)0 ? q.fcafp_dt : gdt);
-  {
-    const G nca_inf = anca * (G)k::k2n / km2n;
-    y.nca = nca_inf - (nca_inf - y.nca) * P::ex(-km2n * gdt);
+  y.m = rush_larsen<P>(y.m, mss, tm, dt);
+  y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
+  y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
+  y.j = rush_larsen<P, true>(y.j, jss, tj, dt);
+  y.hsp = rush_larsen<P, true>(y.hsp, hssp, thsp, dt);
+  y.jp = rush_larsen<P, true>(y.jp, jss, tjp, dt);
+  y.mL = rush_larsen<P>(y.mL, mLss, tmL, dt);
+  y.hL = rush_larsen<P, true>(y.hL, hLss, (G)k::thL, dt);
+  y.hLp = rush_larsen<P, true>(y.hLp, hLssp, (G)k::thLp, dt);
+  y.a = rush_larsen<P, true>(y.a, ass, ta, dt);
+  y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
+  y.iS = rush_larsen<P, true>(y.iS, iss, tiS, dt);
+  y.ap = rush_larsen<P, true>(y.ap, assp, ta, dt);
+  y.iFp = rush_larsen<P, true>(y.iFp, iss, tiFp, dt);
+  y.iSp = rush_larsen<P, true>(y.iSp, iss, tiSp, dt);
+  y.d = rush_larsen<P, true>(y.d, dss, td, dt);
+  y.ff = rush_larsen<P, true>(y.ff, fss, tff, dt);
+  y.fs = rush_larsen<P, true>(y.fs, fss, tfs, dt);
+  y.fcaf = rush_larsen<P, true>(y.fcaf, fcass, tfcaf, dt);
+  y.fcas = rush_larsen<P, true>(y.fcas, fcass, tfcas, dt);
+  y.jca = rush_larsen<P, true>(y.jca, fcass, q.tjca, dt);
+  y.ffp = rush_larsen<P, true>(y.ffp, fss, tffp, dt);
+  // quirk (1): the reference steps fcafp by d = 25 (exp(-25/tfcafp)), far
+  // outside the Taylor range, so that case takes the exponential form
+  if (q.fcafp_dt != (G)0)
+    y.fcafp = rush_larsen<P>(y.fcafp, fcass, tfcafp, (double)q.fcafp_dt);
+  else
+    y.fcafp = rush_larsen<P, true>(y.fcafp, fcass, tfcafp, dt);
+  // nca relaxes at rate km2n towards anca*k2n/km2n (Ohara_Rudy_2011.cpp:1065-1066)
+  y.nca = rush_larsen<P, true>(y.nca, anca * (G)k::k2n / km2n, (G)1 / km2n, dt);
+  if constexpr (!kCipa) {
+    y.xrf = rush_larsen<P, true>(y.xrf, xrss, txrf, dt);
+    y.xrs = rush_larsen<P, true>(y.xrs, xrss, txrs, dt);
+  } else {
+    // Markov IKr with drug binding and trapping (ohara_rudy_cipa_v1_2017.cpp:
+    // 2157-2165), forward Euler like every other non-gate state. Rates
+    // k = A exp(B V) Q10; bound-drug states use the instance's bind = Kmax Ku
+    // D^n/(D^n + halfmax), Ku, and Kt / (1 + exp(-(V - Vhalf)/6.789)).
+    const G k1 = (G)cipa::A1 * P::ex((G)cipa::B1 * v) * (G)cipa::Q1;
+    const G k2 = (G)cipa::A2 * P::ex((G)cipa::B2 * v) * (G)cipa::Q2;
+    const G k3 = (G)cipa::A3 * P::ex((G)cipa::B3 * v) * (G)cipa::Q3;
+    const G k4 = (G)cipa::A4 * P::ex((G)cipa::B4 * v) * (G)cipa::Q4;
+    const G k11 = (G)cipa::A11 * P::ex((G)cipa::B11 * v) * (G)cipa::Q11;
+    const G k21 = (G)cipa::A21 * P::ex((G)cipa::B21 * v) * (G)cipa::Q21;
+    const G k31 = (G)cipa::A31 * P::ex((G)cipa::B31 * v) * (G)cipa::Q31;
+    const G k41 = (G)cipa::A41 * P::ex((G)cipa::B41 * v) * (G)cipa::Q41;
+    const G k51 = (G)cipa::A51 * P::ex((G)cipa::B51 * v) * (G)cipa::Q51;
+    const G k52 = (G)cipa::A52 * P::ex((G)cipa::B52 * v) * (G)cipa::Q52;
+    const G k53 = (G)cipa::A53 * P::ex((G)cipa::B53 * v) * (G)cipa::Q53;
+    const G k61 = (G)cipa::A61 * P::ex((G)cipa::B61 * v) * (G)cipa::Q61;
+    const G k62 = (G)cipa::A62 * P::ex((G)cipa::B62 * v) * (G)cipa::Q62;
+    const G k63 = (G)cipa::A63 * P::ex((G)cipa::B63 * v) * (G)cipa::Q63;
+    const G unb = P::dv(q.Ku * k53, k63);
+    const G trap = P::dv(q.Kt, one + P::ex(-(v - q.Vhalf) * (G)(1.0 / 6.789)));
+    const G IC1 = (G)y.IC1, IC2 = (G)y.IC2, C1 = (G)y.C1, C2 = (G)y.C2, O = (G)y.O, IO = (G)y.IO;
+    const G IOb = (G)y.IObound, Ob = (G)y.Obound, Cb = (G)y.Cbound;
+    const G f11 = k11 * IC1 - k21 * IC2, f51 = k51 * C1 - k61 * IC1, f3 = k3 * IC2 - k4 * IO;
+    const G f52 = k52 * C2 - k62 * IC2, f1 = k1 * C1 - k2 * C2, f31 = k31 * C2 - k41 * O;
+    const G f53 = k53 * O - k63 * IO, fbo = q.bind * O - q.Ku * Ob, fbi = q.bind * IO - unb * IOb;
+    const G ftc = trap * Cb;
+    const G dIC1 = -f11 + f51;
+    const G dIC2 = (f11 - f3) + f52;
+    const G dC1 = -f1 - f51;
+    const G dC2 = (f1 - f31) - f52;
+    const G dO = (f31 - f53) - fbo;
+    const G dIO = (f3 + f53) - fbi;
+    const G dIOb = (fbi + ftc) - q.Kt * IOb;
+    const G dOb = (fbo + ftc) - q.Kt * Ob;
+    const G dCb = -(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb);
+    y.IC1 += (double)dIC1 * dt; y.IC2 += (double)dIC2 * dt; y.C1 += (double)dC1 * dt;
+    y.C2 += (double)dC2 * dt; y.O += (double)dO * dt; y.IO += (double)dIO * dt;
+    y.IObound += (double)dIOb * dt; y.Obound += (double)dOb * dt; y.Cbound += (double)dCb * dt;
   }
-  y.xrf = rush_larsen<P>(y.xrf, xrss, txrf, gdt);
-  y.xrs = rush_larsen<P>(y.xrs, xrss, txrs, gdt);
-  y.xs1 = rush_larsen<P>(y.xs1, xs1ss, txs1, gdt);
-  y.xs2 = rush_larsen<P>(y.xs2, xs2ss, txs2, gdt);
-  y.xk1 = rush_larsen<P>(y.xk1, xk1ss, txk1, gdt);
-  y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, gdt);
-  y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, gdt);
+  y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
+  y.xs2 = rush_larsen<P, true>(y.xs2, xs2ss, txs2, dt);
+  y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
+  y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, dt);
+  y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, dt);
   // forward Euler, FP64 accumulation
   y.CaMKt = y.CaMKt + dCaMKt * dt;
   y.V = y.V + (double)dV * dt;
@@ -523,6 +656,78 @@ __device__ __forceinline__ void init_instance(double *__restrict__ par, double *
                                  1, 0, 1, 1, 0, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 1, 0, 0};
 #pragma unroll
   for (int k2 = 0; k2 < kNumStates; ++k2) s[k2 * ld + i] = y0[k2];
+}
+
+// initConsts(type, conc, hill) of CiPA-ORd v1 2017 for one instance
+// (ohara_rudy_cipa_v1_2017.cpp:1246-1501 active block and :1515-1539): the
+// Hill block of seven channels and the dynamic-hERG drug parameters
+// hill[14..18] = Kmax, Ku, n, halfmax, Vhalf (zero keeps the model value);
+// hill[19] = Kt, the trapping rate the reference leaves at 0. The binding
+// rate Kmax*Ku*D^n/(D^n + halfmax) is constant per instance (D is) and is
+// folded here. `quirks` forces endo and leaves the derived permeabilities
+// unblocked, as the reference does.
+__device__ __forceinline__ void init_instance_cipa(double *__restrict__ par, double *__restrict__ s, int64_t ld,
+                                                   int64_t i, double celltype_in, double conc,
+                                                   const double *__restrict__ hill, bool quirks) {
+  const double ct = quirks ? 0.0 : celltype_in;
+  const double GNaL_b = 0.019957499999999975, PCa_b = 0.0001007, GKr_b = 0.04658545454545456;
+  const double GKs_b = 0.006358000000000001, GK1_b = 0.3239783999999998;
+  double GNaL = ct == 1.0 ? GNaL_b * 0.6 : GNaL_b;
+  double Gto = ct == 1.0 ? 0.02 * 4.0 : ct == 2.0 ? 0.02 * 4.0 : 0.02;
+  double PCa = ct == 1.0 ? PCa_b * 1.2 : ct == 2.0 ? PCa_b * 2.5 : PCa_b;
+  double GKr = ct == 1.0 ? GKr_b * 1.3 : ct == 2.0 ? GKr_b * 0.8 : GKr_b;
+  double GKs = ct == 1.0 ? GKs_b * 1.4 : GKs_b;
+  double GK1 = ct == 1.0 ? GK1_b * 1.2 : ct == 2.0 ? GK1_b * 1.3 : GK1_b;
+  const double GKb = ct == 1.0 ? 0.003 * 0.6 : 0.003;
+  const double Gncx = ct == 1.0 ? 0.0008 * 1.1 : ct == 2.0 ? 0.0008 * 1.4 : 0.0008;
+  const double Pnak = ct == 1.0 ? 30 * 0.9 : ct == 2.0 ? 30 * 0.7 : 30;
+  const double cmdnmax = ct == 1.0 ? 0.05 * 1.3 : 0.05;
+  const double upScale = ct == 1.0 ? 1.3 : 1.0;
+  double GNa = 75;
+  double PCap = 1.1 * PCa, PCaNa = 0.00125 * PCa, PCaK = 0.0003574 * PCa;
+  double PCaNap = 0.00125 * PCap, PCaKp = 0.0003574 * PCap;
+  double Kmax = 0, Ku = 0, nn = 1, halfmax = 1, Vhalf = 1, Kt = 0;
+  if (hill) {
+    PCa *= hill_factor(conc, hill[0], hill[1]);
+    GK1 *= hill_factor(conc, hill[2], hill[3]);
+    GKs *= hill_factor(conc, hill[4], hill[5]);
+    GNa *= hill_factor(conc, hill[6], hill[7]);
+    GNaL *= hill_factor(conc, hill[8], hill[9]);
+    Gto *= hill_factor(conc, hill[10], hill[11]);
+    GKr *= hill_factor(conc, hill[12], hill[13]);
+    if (!quirks) {
+      PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
+      PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
+    }
+    if (hill[14] > 10E-14) Kmax = hill[14];
+    if (hill[15] > 10E-14) Ku = hill[15];
+    if (hill[16] > 10E-14) nn = hill[16];
+    if (hill[17] > 10E-14) halfmax = hill[17];
+    if (hill[18] > 10E-14) Vhalf = hill[18];
+    if (hill[19] > 10E-14) Kt = hill[19];
+  }
+  const double Dn = ::exp(nn * ::log(conc));
+  const double bind = (Kmax * Ku * Dn) / (Dn + halfmax);
+  double *p = par + i;
+  p[P_GNa * ld] = GNa; p[P_GNaL * ld] = GNaL; p[P_Gto * ld] = Gto; p[P_PCa * ld] = PCa;
+  p[P_PCap * ld] = PCap; p[P_PCaNa * ld] = PCaNa; p[P_PCaK * ld] = PCaK; p[P_PCaNap * ld] = PCaNap;
+  p[P_PCaKp * ld] = PCaKp; p[P_GKr * ld] = GKr; p[P_GKs * ld] = GKs; p[P_GK1 * ld] = GK1;
+  p[P_GKb * ld] = GKb; p[P_Gncx * ld] = Gncx; p[P_Pnak * ld] = Pnak; p[P_cmdnmax * ld] = cmdnmax;
+  p[P_upScale * ld] = upScale; p[P_Aff * ld] = 0.6; p[P_Afs * ld] = 1.0 - 0.6; p[P_tjca * ld] = 75.0;
+  p[P_H * ld] = 1e-7; p[P_celltype * ld] = ct; p[P_fcafp_dt * ld] = 0.0;
+  p[P_amp * ld] = -80; p[P_BCL * ld] = 1000.0; p[P_stim_start * ld] = 10.0; p[P_duration * ld] = 0.5;
+  p[P_bind * ld] = bind; p[P_Ku * ld] = Ku; p[P_Kt * ld] = Kt; p[P_Vhalf * ld] = Vhalf;
+  const double y0[cipa::kNumStates] = {
+      -88.00190465, 0.0125840447, 8.49e-05, 7.268004498, 7.268089977, 144.6555918, 144.6555651, 1.619574538,
+      1.571234014, 8.6e-05, 0.007344121102, 0.6981071913, 0.6980895801, 0.6979908432, 0.4549485525,
+      0.6979245865, 0.0001882617273, 0.5008548855, 0.2693065357, 0.001001097687, 0.9995541745, 0.5865061736,
+      0.0005100862934, 0.9995541823, 0.6393399482, 2.34e-9, 0.9999999909, 0.9102412777, 0.9999999909,
+      0.9998046777, 0.9999738312, 0.9999999909, 0.9999999909, 0.002749414044, 0.999637, 6.83208e-05,
+      1.80145e-08, 8.26619e-05, 0.00015551, 5.67623e-05, 0, 0, 0, 0, 0.2707758025, 0.0001928503426,
+      0.9967597594, 2.5e-7, 3.12e-7};
+#pragma unroll
+  for (int k2 = 0; k2 < cipa::kNumStates; ++k2) s[k2 * ld + i] = y0[k2];
+  s[cipa::D * ld + i] = conc;
 }
 
 }  // namespace ord

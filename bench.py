@@ -3,20 +3,25 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload cipa_pop|ord_pop] [--seg STEPS]
 
-One bench step = one launch of SEG fixed time steps (dt = 0.005 ms) over the
-whole population resident in HBM, with the biomarker state machine fused.
-The population keeps advancing from step to step, so consecutive steps walk
-through the action potential exactly as a long screening run does.
+Workload (default, the population configuration): CiPA-ORd v1 2017 with the
+dynamic hERG Markov IKr and drug trapping, 10,000 instances per GPU =
+2,000 seeded IC50/Hill samples (lognormal around a nominal drug, sigma 0.5
+in ln-space) x 5 concentrations, BCL 2000 ms, dt 0.005 ms, biomarkers
+(steepest of the last 250 paces of a 1000-pace protocol) fused.
 
-value  : mixed-precision cell-steps/s over the whole job (all ranks), device
-         time (CUDA events), inputs resident in HBM.
-fp64   : the plain FP64 path on the same workload (same timing rules).
-e2e    : the same metric through the C ABI with host buffers: every step
-         uploads the population state from pinned host memory, runs, and
-         downloads state + biomarkers.
+One bench step = one launch advancing the whole population resident in HBM
+by SEG fixed time steps (default 10,000 = 50 ms of simulated time); the
+population keeps advancing from step to step, walking through the action
+potential exactly as the long screening run does.
+
+value : mixed-precision cell-steps/s over the whole job (all ranks), device
+        time (CUDA events around the timed region, max over ranks).
+fp64  : the plain FP64 path on the same workload, same rules.
+e2e   : the same metric through the C ABI with host buffers: every step
+        uploads the population state from pinned host memory, runs, and
+        downloads the state and the biomarker records.
 Multi-GPU (torchrun): every rank owns an independent population (weak
-scaling); no data-path collective, only a barrier and a max-reduction of
-the timings.
+scaling); no data-path collective, only barriers and a max of the timings.
 """
 from __future__ import annotations
 
@@ -39,6 +44,25 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "ORd cell-steps/s mixed vs FP64 (APD90 err≤0.1 ms); screen-job p50/p99 latency"
 DT = 0.005
+BCL = 2000.0
+
+# Algorithmic operations per cell-step, counted by running the oracle's
+# restatement with an operation-counting scalar (operations on instance
+# constants are folded and not counted): `make -C oracle opcount &&
+# oracle/_build/opcount <model> 1 1000` (profiles/opcount_ionic_models.txt).
+# flop = one add/sub, mul, div or elementary-function evaluation.
+OPS = {
+    "cipa2017": dict(add=509.97, mul=517.99, div=269.99, exp=109.0, log=3.0, pow=1.0),
+    "ord2011": dict(add=474.97, mul=435.99, div=281.99, exp=100.0, log=3.0, pow=1.0),
+}
+# DRAM bytes per launch per instance measured by ncu on the run kernel
+# (profiles/run_kernel_cipa2017_pop10k.md): the state and biomarker records
+# are read and written once per launch; everything else stays on chip.
+TRAFFIC_PER_INSTANCE = {"cipa2017": None, "ord2011": None}
+
+
+def flops_per_step(model: str) -> float:
+    return sum(OPS[model].values())
 
 
 def parse():
@@ -47,30 +71,41 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ord_pop", choices=["ord_pop"])
+    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop"])
     ap.add_argument("--seg", type=int, default=10000, help="time steps per bench step")
     ap.add_argument("--samples", type=int, default=2000)
     ap.add_argument("--concs", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
 
+def model_of(workload: str) -> str:
+    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011"}[workload]
+
+
 # ------------------------------------------------------------ inputs
-def population(n_samples: int, n_conc: int, seed: int):
-    """Seeded population: 2,000 IC50/Hill samples lognormal (sigma 0.5 in
-    ln-space) around a nominal drug drawn from the single-cell ranges
-    (IC50 log-U[0.1,100] uM, h U[0.6,1.8]), Cmax log-U[0.01,10] uM,
-    concentrations 0..(n_conc-1) x Cmax. Returns (conc[n], hill[n,20])."""
+def population(model: str, n_samples: int, n_conc: int, seed: int):
+    """Seeded population: a nominal drug (IC50 log-U[0.1,100] uM, h
+    U[0.6,1.8]; for CiPA the static hERG block is off and the dynamic hERG
+    set Kmax, Ku, n, halfmax, Vhalf is seeded, Kt = 3.5e-5), n_samples
+    lognormal around it (sigma 0.5 in ln-space), Cmax log-U[0.01,10] uM,
+    concentrations 0..n_conc-1 x Cmax. Returns (conc[n], hill[n, 20])."""
     rng = np.random.default_rng(seed)
-    nom_ic50 = 10 ** rng.uniform(-1, 2, 7)
-    nom_h = rng.uniform(0.6, 1.8, 7)
+    nom = np.zeros(20)
+    nom[0:14:2] = 10 ** rng.uniform(-1, 2, 7)
+    nom[1:14:2] = rng.uniform(0.6, 1.8, 7)
+    halfmax = 10 ** rng.uniform(3, 6)
+    dyn = [halfmax * 10 ** rng.uniform(-1, 1), 10 ** rng.uniform(-4, -2), rng.uniform(0.8, 1.0), halfmax,
+           rng.uniform(-100, -10), 3.5e-5]
+    if model == "cipa2017":
+        nom[14:20] = dyn
+        nom[12] = nom[13] = 0.0
     cmax = 10 ** rng.uniform(-2, 1)
-    ic50 = nom_ic50 * np.exp(0.5 * rng.standard_normal((n_samples, 7)))
-    h = nom_h * np.exp(0.5 * rng.standard_normal((n_samples, 7)))
-    hill = np.zeros((n_samples, 20))
-    hill[:, 0:14:2] = ic50
-    hill[:, 1:14:2] = h
+    pert = np.exp(0.5 * rng.standard_normal((n_samples, 20)))
+    pert[:, 18:20] = 1.0
+    hill = nom[None, :] * pert
     hill = np.repeat(hill, n_conc, axis=0)
     conc = np.tile(np.arange(n_conc) * cmax, n_samples)
     return conc, hill
@@ -80,9 +115,9 @@ def population(n_samples: int, n_conc: int, seed: int):
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during a region."""
 
-    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-             "clocks_event_reasons.sw_power_cap"
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
@@ -92,10 +127,11 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -106,6 +142,7 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         if self.proc:
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -133,17 +170,17 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ distributed
-def dist_setup(args):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pg = None
     if world > 1:
         import datetime
-        import torch.distributed as dist
         import torch
+        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
         pg = dist
     return world, rank, local, pg
 
@@ -163,19 +200,37 @@ def barrier(pg):
 
 
 # ------------------------------------------------------------ our arm
-def run_ours(args, world, rank, local, pg):
+def measured_peaks():
+    """FP32/FP64 FMA throughput of this GPU (probe kernels) and the
+    driver-measured HBM/bf16 peaks."""
+    out = {}
+    try:
+        L = ctypes.CDLL(str(ROOT / "2ddrugsimulation_b200" / "lib" / "libcep_probe.so"))
+        L.cep_probe_fp32_fma_flops.restype = ctypes.c_double
+        L.cep_probe_fp64_fma_flops.restype = ctypes.c_double
+        out["fp32_tflops"] = max(L.cep_probe_fp32_fma_flops() for _ in range(3)) / 1e12
+        out["fp64_tflops"] = max(L.cep_probe_fp64_fma_flops() for _ in range(3)) / 1e12
+    except OSError:
+        pass
+    mp = ROOT / "MEASURED_PEAKS.json"
+    if mp.exists():
+        out["measured_peaks_json"] = json.loads(mp.read_text())
+    return out
+
+
+def run_ours(args, world, rank, local, pg, model):
     import torch
     cep = importlib.import_module("2ddrugsimulation_b200")
     torch.cuda.set_device(local)
-    conc, hill = population(args.samples, args.concs, seed=1234 + rank)
+    conc, hill = population(model, args.samples, args.concs, seed=1234 + rank)
     n = len(conc)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
     res = {}
     launches = 0
     for prec in ("mixed", "fp64"):
-        b = cep.Batch("ord2011", n, prec)
-        b.init(conc=conc, hill=hill, dutta=False, quirks=True)
-        b.set_pacing(2000.0)
+        b = cep.Batch(model, n, prec)
+        b.init(conc=conc, hill=hill, quirks=True)
+        b.set_pacing(BCL)
         b.set_protocol(DT, 1000, 750, dt_write=1.0)
         for _ in range(args.warmup):
             b.run(args.seg)
@@ -199,23 +254,23 @@ def run_ours(args, world, rank, local, pg):
         ms = start.elapsed_time(stop)
         kms = [kst[k].elapsed_time(ken[k]) for k in range(args.steps)]
         ms_max = max_over_ranks(ms, pg)
-        kernel_ms = statistics.mean(kms)
+        kernel_ms = max_over_ranks(statistics.mean(kms), pg)
         cell_steps = n * args.seg * args.steps * world
+        st = b.status()
         res[prec] = dict(value=cell_steps / (ms_max / 1e3), ms_per_step=ms_max / args.steps, kernel_ms=kernel_ms,
-                         clocks=clk.summary(), status=b.status())
+                         clocks=clk.summary(), n_running=int((st == cep.INST_RUNNING).sum()),
+                         n_nonfinite=int((st == cep.INST_NONFINITE).sum()))
         launches += args.steps
         if prec == "mixed" and not args.no_e2e:
-            res["e2e"] = run_e2e(args, b, n, world, pg, cep)
+            res["e2e"] = run_e2e(args, b, n, world, pg, cep, model)
         b.close()
     return res, n, launches
 
 
-def run_e2e(args, b, n, world, pg, cep):
-    """Same workload through the C ABI with host buffers: per step, upload
-    the population state from pinned host memory, run, download state and
-    biomarkers."""
+def run_e2e(args, b, n, world, pg, cep, model):
+    """The same workload through the C ABI with host buffers."""
     import torch
-    ns = cep.N_STATES["ord2011"]
+    ns = cep.N_STATES[model]
     pinned_in = torch.empty(ns * n, dtype=torch.float64, pin_memory=True).numpy()
     pinned_out = torch.empty(ns * n, dtype=torch.float64, pin_memory=True).numpy()
     pinned_in[:] = b.get_states(cep.LAYOUT_SOA).ravel()
@@ -224,14 +279,15 @@ def run_e2e(args, b, n, world, pg, cep):
     bm = (cep.Biomarkers * n)()
     torch.cuda.synchronize()
     barrier(pg)
-    t0 = time.perf_counter()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
     for _ in range(args.steps):
-        lib.cep_batch_set_states(b._h, pinned_in.ctypes.data_as(dp), cep.LAYOUT_SOA)
-        lib.cep_batch_run(b._h, args.seg)
-        lib.cep_batch_get_states(b._h, pinned_out.ctypes.data_as(dp), cep.LAYOUT_SOA)
-        lib.cep_batch_get_biomarkers(b._h, bm)
+        rc = lib.cep_batch_set_states(b._h, pinned_in.ctypes.data_as(dp), cep.LAYOUT_SOA)
+        rc |= lib.cep_batch_run(b._h, args.seg)
+        rc |= lib.cep_batch_get_states(b._h, pinned_out.ctypes.data_as(dp), cep.LAYOUT_SOA)
+        rc |= lib.cep_batch_get_biomarkers(b._h, bm)
+        if rc:
+            raise RuntimeError(lib.cep_last_error().decode())
         pinned_in[:] = pinned_out
     stop.record()
     torch.cuda.synchronize()
@@ -242,24 +298,24 @@ def run_e2e(args, b, n, world, pg, cep):
 
 
 # ------------------------------------------------------------ CPU baseline / reference arm
-def cpu_reference_rate(conc, hill, n_inst: int, n_steps: int, threads: int):
-    """The reference's own ORd implementation (compiled from its sources by
-    oracle/Makefile) or, where that build is absent, the oracle port; run
-    over n_inst instances x n_steps on `threads` host threads."""
+def cpu_rate(model: str, conc, hill, threads: int, steps_per_thread: int):
+    """The reference's CPU implementation of the path on `threads` host
+    threads, one instance per thread: for ORd the reference compiled from
+    its own sources (oracle/_ref); for CiPA-ORd, whose reference integrates
+    only with CVODE (not buildable here), the oracle port (the reference's
+    computeRates restated bit-exact plus the fixed-step scheme)."""
     from oracle import oracle as O
-    kind = "reference" if O.ref_available("ord2011") else "port"
-    per = [None] * threads
-    idx = np.array_split(np.arange(n_inst), threads)
+    kind = "reference" if (model == "ord2011" and O.ref_available("ord2011")) else "port"
 
     def work(k):
-        for i in idx[k]:
-            if kind == "reference":
-                c = O.RefCell("ord2011", 0.0, conc[i], hill[i, :14])
-                c.consts[140] = 2000.0
-            else:
-                c = O.Cell("ord2011", 0.0, conc[i], hill[i, :14])
-                c.set_pacing(2000.0)
-            c.run(0.0, DT, n_steps)
+        i = k % len(conc)
+        if kind == "reference":
+            c = O.RefCell("ord2011", 0.0, conc[i], hill[i, :14])
+            c.consts[140] = BCL
+        else:
+            c = O.Cell(model, 0.0, conc[i], hill[i], quirks=True)
+            c.set_pacing(BCL)
+        c.run(0.0, DT, steps_per_thread)
 
     th = [threading.Thread(target=work, args=(k,)) for k in range(threads)]
     t0 = time.perf_counter()
@@ -267,61 +323,89 @@ def cpu_reference_rate(conc, hill, n_inst: int, n_steps: int, threads: int):
         t.start()
     for t in th:
         t.join()
-    dt = time.perf_counter() - t0
-    return n_inst * n_steps / dt, kind, dt
+    secs = time.perf_counter() - t0
+    return threads * steps_per_thread / secs, kind, secs
+
+
+def calibrate_cpu(model, conc, hill, threads, target_s):
+    r, _, _ = cpu_rate(model, conc, hill, 1, 20000)
+    return max(20000, int(r * target_s))
+
+
+def config_of(args, model, n, world):
+    name = {"cipa2017": "CiPA-ORd v1 2017 (dynamic hERG, drug trapping)", "ord2011": "ORd 2011"}[model]
+    return {"workload": f"{name} population, {n} instances per GPU ({args.samples} IC50/Hill samples x "
+                        f"{args.concs} concs), BCL 2000 ms, dt 0.005 ms, 1000-pace protocol with steepest-of-last-"
+                        f"250 biomarkers fused; {args.seg} time steps per bench step",
+            "instances_per_gpu": n, "time_steps_per_bench_step": args.seg,
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance sharding x{world}"}
 
 
 def main():
     args = parse()
-    world, rank, local, pg = dist_setup(args)
-    conc, hill = population(args.samples, args.concs, seed=1234)
+    model = model_of(args.workload)
+    world, rank, local, pg = dist_setup()
+    conc, hill = population(model, args.samples, args.concs, seed=1234)
     threads = os.cpu_count() or 1
     if args.impl == "reference":
         if rank != 0:
             return
+        per_thread = 400000  # one 2000-ms beat per thread per bench step
         rates = []
+        kind = "port"
         for _ in range(args.warmup + args.steps):
-            n_inst = max(threads, 16)
-            r, kind, _ = cpu_reference_rate(conc, hill, n_inst, 4000, threads)
+            r, kind, _ = cpu_rate(model, conc, hill, threads, per_thread)
             rates.append(r)
         v = statistics.mean(rates[args.warmup:])
+        sample = f"{threads} instances x {per_thread} fixed steps (one 2000-ms beat) per bench step"
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "ORd-2011 population, 10,000 instances (2,000 IC50/Hill samples x 5 concs), "
-                                       "BCL 2000 ms, dt 0.005 ms", "sample": f"{max(threads,16)} instances x 4000 steps per step"},
-                "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": kind,
-                                 "sample": f"{max(threads,16)} instances x 4000 fixed steps per bench step"},
+                "config": config_of(args, model, len(conc), world) | {"sample": sample},
+                "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": kind, "sample": sample},
                 "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
-    res, n, launches = run_ours(args, world, rank, local, pg)
+    peaks = measured_peaks() if rank == 0 else {}
+    res, n, launches = run_ours(args, world, rank, local, pg, model)
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
         return
     cpu = None
     if not args.no_cpu:
-        r, kind, secs = cpu_reference_rate(conc, hill, max(threads, 16), 20000, threads)
+        steps = calibrate_cpu(model, conc, hill, threads, args.cpu_seconds)
+        r, kind, secs = cpu_rate(model, conc, hill, threads, steps)
         cpu = {"value": r, "unit": "cell-steps/s", "cores": threads, "kind": kind,
-               "sample": f"{max(threads,16)} instances x 20000 fixed steps ({secs:.1f} s)"}
+               "sample": f"{threads} instances x {steps} fixed steps, one per thread ({secs:.1f} s)"}
     mixed, fp64 = res["mixed"], res["fp64"]
+    fl = flops_per_step(model)
+    cell_steps_launch = n * args.seg
+
+    def roof(kernel_ms, peak_key, label):
+        ach = fl * cell_steps_launch / (kernel_ms * 1e-3) / 1e12
+        pk = peaks.get(peak_key)
+        tr = TRAFFIC_PER_INSTANCE.get(model)
+        return {"bound": label, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": (ach / pk) if pk else None, "traffic": (tr * n) if tr else None,
+                "flops_per_cell_step": fl, "peak_source": "bench.py FMA probe on this GPU (2 flop/FMA)"}
+
     line = {
         "metric": METRIC, "value": mixed["value"], "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
-        "config": {"workload": f"ORd-2011 population, {n} instances per GPU ({args.samples} IC50/Hill samples x "
-                               f"{args.concs} concs), BCL 2000 ms, dt 0.005 ms, {args.seg} steps per bench step, "
-                               f"biomarkers fused", "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"instance sharding x{world}"},
-        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "kernel_ms": fp64["kernel_ms"]},
+        "config": config_of(args, model, n, world),
+        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "kernel_ms": fp64["kernel_ms"],
+                 "roofline": roof(fp64["kernel_ms"], "fp64_tflops", "fp64"), "clocks": fp64["clocks"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "kernel_ms": mixed["kernel_ms"],
+        "roofline": roof(mixed["kernel_ms"], "fp32_tflops", "fp32"),
         "gpu_launches": launches,
         "clocks": mixed["clocks"],
         "cpu_baseline": cpu,
         "e2e": res.get("e2e"),
-        "roofline": None,
+        "instances_nonfinite": mixed["n_nonfinite"] + fp64["n_nonfinite"],
+        "peaks": {k: v for k, v in peaks.items() if k != "measured_peaks_json"},
     }
     print(json.dumps(line))
     if pg is not None:

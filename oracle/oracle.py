@@ -43,7 +43,7 @@ def build(quiet: bool = True) -> None:
 
 class CepoCell(ctypes.Structure):
     _fields_ = [("model", ctypes.c_int), ("quirks", ctypes.c_int), ("tissue_stim", ctypes.c_int),
-                ("is_s1", ctypes.c_int), ("p", ctypes.c_double * 160)]
+                ("is_s1", ctypes.c_int), ("p", ctypes.c_double * 256)]
 
 
 class CepoCurrents(ctypes.Structure):

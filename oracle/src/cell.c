@@ -17,7 +17,7 @@ void cepo_ord_step(const cepo_cell *, double, double, double *, cepo_currents *)
 void cepo_ord_rates(const cepo_cell *, double, const double *, double *, cepo_currents *);
 
 int cepo_cipa_init(cepo_cell *, double, double, const double *, int, int);
-void cepo_cipa_init_states(double *);
+void cepo_cipa_init_states(const cepo_cell *, double *);
 void cepo_cipa_set_pacing(cepo_cell *, double, double, double, double);
 void cepo_cipa_step(const cepo_cell *, double, double, double *, cepo_currents *);
 void cepo_cipa_rates(const cepo_cell *, double, const double *, double *, cepo_currents *);
@@ -100,7 +100,7 @@ int cepo_init(cepo_cell *c, int model, double celltype, double conc, const doubl
 void cepo_init_states(const cepo_cell *c, double *y) {
   switch (c->model) {
     case CEPO_ORD2011: cepo_ord_init_states(y); break;
-    case CEPO_CIPA2017: cepo_cipa_init_states(y); break;
+    case CEPO_CIPA2017: cepo_cipa_init_states(c, y); break;
     case CEPO_TT2006: cepo_tt06_init_states(y); break;
     case CEPO_TT2004: cepo_tt04_init_states(y); break;
     case CEPO_TOMEK2019: cepo_tomek_init_states(c, y); break;

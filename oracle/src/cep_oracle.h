@@ -20,7 +20,7 @@ enum { CEPO_ORD2011 = 0, CEPO_CIPA2017 = 1, CEPO_TT2006 = 2, CEPO_TT2004 = 3, CE
 
 /* Largest state / parameter counts over all models. */
 #define CEPO_MAX_STATES 64
-#define CEPO_MAX_PARAMS 160
+#define CEPO_MAX_PARAMS 256
 #define CEPO_MAX_HILL 20
 
 /* Named per-step outputs every model fills (biomarker inputs). */

@@ -60,7 +60,50 @@ def make_ord(n_beats: int = 2, dt: float = 0.005, stride: int = 200, bcl: float 
         print("wrote", c["name"], "vmax", v.max())
 
 
+def cipa_hill(rng: np.random.Generator) -> np.ndarray:
+    """Seeded CiPA row: seven IC50/h pairs (hERG static block off: the
+    dynamic model carries it), then Kmax, Ku, n, halfmax, Vhalf, Kt."""
+    h = hill_row(rng)
+    h[12] = h[13] = 0.0
+    halfmax = 10 ** rng.uniform(3, 6)
+    dyn = [halfmax * 10 ** rng.uniform(-1, 1), 10 ** rng.uniform(-4, -2), rng.uniform(0.8, 1.0), halfmax,
+           rng.uniform(-100, -10), 3.5e-5]
+    return np.concatenate([h, dyn])
+
+
+def make_cipa(dt: float = 0.005, bcl: float = 1000.0, n_steps: int = 200000, every: int = 10000):
+    """CiPA-ORd: the reference has no fixed-step integrator, so the fixture
+    holds states along the oracle's fixed-step trajectory and the
+    reference's RATES at each of them."""
+    rng = np.random.default_rng(99)
+    cases = [dict(name="cipa_control", conc=0.0, hill=np.zeros(20)),
+             dict(name="cipa_drug", conc=2.5, hill=cipa_hill(rng))]
+    for c in cases:
+        r = O.RefCell("cipa2017", 0.0, c["conc"], c["hill"])
+        cell = O.Cell("cipa2017", 0.0, c["conc"], c["hill"], quirks=True)
+        cell.set_pacing(bcl)
+        r.consts[15] = bcl  # CONSTANTS[stim_period]
+        if c["hill"][19] > 1e-13:
+            r.consts[100] = c["hill"][19]  # CONSTANTS[Kt]: the reference has no hill slot for it
+        states, rates, times = [], [], []
+        t = 0.0
+        for k in range(n_steps):
+            if k % every == 0:
+                r.states[:] = cell.states
+                r.L.ref_compute_rates(r.h, t)
+                states.append(cell.states.copy())
+                rates.append(r.arr("rates", r.n).copy())
+                times.append(t)
+            cell.step(t, dt)
+            t += dt
+        np.savez_compressed(OUT / f"{c['name']}.npz", conc=c["conc"], hill=c["hill"], dt=dt, bcl=bcl,
+                            times=np.array(times), states=np.array(states), ref_rates=np.array(rates),
+                            y0=r.states.copy() * 0 + np.array(states)[0])
+        print("wrote", c["name"])
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
     make_ord()
+    make_cipa()

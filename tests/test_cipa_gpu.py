@@ -1,0 +1,128 @@
+"""CiPA-ORd v1 2017 (dynamic hERG) on the GPU against the oracle.
+
+The reference integrates this model only with CVODE; parity here is against
+the oracle's fixed-step scheme (the reference's ORd update scheme applied to
+this model, with the reference's computeRates pinned bit for bit).
+Tolerances as in test_ord_gpu.py.
+"""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+VM_TOL_FP64 = 1e-6
+APD_TOL_FP64 = 0.01
+APD_TOL_MIXED = 0.1
+CAD_TOL_MIXED = 0.1
+QNET_RTOL_MIXED = 0.01
+
+
+def cipa_population(n_samples: int, n_conc: int, seed: int):
+    """Seeded CiPA population: a nominal drug (IC50 log-U[0.1,100] uM,
+    h U[0.6,1.8], static hERG block off, dynamic hERG Kmax/Ku/n/halfmax/
+    Vhalf seeded, Kt = 3.5e-5), samples lognormal around it (sigma 0.5 in
+    ln-space), concentrations 0..n_conc-1 x Cmax."""
+    rng = np.random.default_rng(seed)
+    nom = np.zeros(20)
+    nom[0:14:2] = 10 ** rng.uniform(-1, 2, 7)
+    nom[1:14:2] = rng.uniform(0.6, 1.8, 7)
+    halfmax = 10 ** rng.uniform(3, 6)
+    nom[14:20] = [halfmax * 10 ** rng.uniform(-1, 1), 10 ** rng.uniform(-4, -2), rng.uniform(0.8, 1.0), halfmax,
+                  rng.uniform(-100, -10), 3.5e-5]
+    nom[12] = nom[13] = 0.0
+    cmax = 10 ** rng.uniform(-2, 1)
+    hill = np.repeat(nom[None, :], n_samples, axis=0)
+    pert = np.exp(0.5 * rng.standard_normal((n_samples, 20)))
+    pert[:, 12:14] = 1.0
+    pert[:, 18:20] = 1.0  # Vhalf and Kt stay nominal
+    hill = hill * pert
+    hill = np.repeat(hill, n_conc, axis=0)
+    conc = np.tile(np.arange(n_conc) * cmax, n_samples)
+    return conc, hill
+
+
+def _oracle(oracle, conc, hill, n_pace, first_pace, dt, bcl):
+    out = [None] * len(conc)
+
+    def work(k):
+        c = oracle.Cell("cipa2017", 0.0, conc[k], hill[k], quirks=True)
+        c.set_pacing(bcl)
+        bm, _ = c.run_biomarkers(dt, n_pace, first_pace, dt_write=1.0)
+        bm["final"] = c.states.copy()
+        out[k] = bm
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(len(conc))]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    return out
+
+
+def _gpu(cep, conc, hill, precision, n_pace, first_pace, dt, bcl):
+    b = cep.Batch("cipa2017", len(conc), precision)
+    b.init(conc=conc, hill=hill, quirks=True)
+    b.set_pacing(bcl)
+    b.set_protocol(dt, n_pace, first_pace, dt_write=1.0)
+    b.run_to_end(50000)
+    return b.biomarkers(), b.get_states()
+
+
+@pytest.mark.gpu
+def test_cipa_fp64_trace_matches_oracle(cep, gpu, oracle):
+    conc, hill = cipa_population(2, 2, seed=3)
+    n = len(conc)
+    b = cep.Batch("cipa2017", n, "fp64")
+    b.init(conc=conc, hill=hill, quirks=True)
+    b.set_pacing(1000.0)
+    cells = []
+    for k in range(n):
+        c = oracle.Cell("cipa2017", 0.0, conc[k], hill[k], quirks=True)
+        c.set_pacing(1000.0)
+        cells.append(c)
+    y0 = b.get_states()
+    for k in range(n):
+        assert np.array_equal(y0[k], cells[k].states)
+    stride, n_chunks = 400, 500  # 1000 ms
+    vg = np.zeros((n_chunks, n))
+    vo = np.zeros((n_chunks, n))
+    t = 0.0
+    traces = [None] * n
+
+    def work(k):
+        _, traces[k] = cells[k].run(0.0, 0.005, stride * n_chunks, stride)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(n)]
+    [x.start() for x in th]
+    for i in range(n_chunks):
+        b.run(stride)
+        vg[i] = b.get_states()[:, 0]
+    [x.join() for x in th]
+    for k in range(n):
+        err = np.abs(vg[:, k] - traces[k]).max()
+        assert err <= VM_TOL_FP64, f"instance {k}: max |dVm| = {err:.3e} mV"
+    fin = b.get_states()
+    for k in range(n):
+        rel = np.abs(fin[k] - cells[k].states) / np.maximum(np.abs(cells[k].states), 1e-9)
+        assert rel.max() < 1e-5
+
+
+@pytest.mark.gpu
+def test_cipa_biomarkers_fp64_and_mixed(cep, gpu, oracle):
+    """Steepest-repolarisation selection over the evaluated paces (the
+    reference's last-250-paces rule, here the last 3 of 4 paces)."""
+    conc, hill = cipa_population(3, 3, seed=8)
+    ref = _oracle(oracle, conc, hill, 4, 1, 0.005, 1000.0)
+    b64, s64 = _gpu(cep, conc, hill, "fp64", 4, 1, 0.005, 1000.0)
+    bmx, _ = _gpu(cep, conc, hill, "mixed", 4, 1, 0.005, 1000.0)
+    for k, r in enumerate(ref):
+        assert b64["status"][k] == cep.INST_DONE
+        assert abs(s64[k, 0] - r["final"][0]) <= VM_TOL_FP64
+        assert b64["steepest_pace"][k] == r["steepest_pace"]
+        for key in ("apd90", "apd50", "cad90", "cad50"):
+            assert abs(b64[key][k] - r[key]) <= APD_TOL_FP64, (key, k, b64[key][k], r[key])
+        assert abs(b64["qnet"][k] - r["qnet"] / 1000) <= 1e-9 * max(1.0, abs(r["qnet"]))
+        assert abs(bmx["apd90"][k] - r["apd90"]) <= APD_TOL_MIXED, (k, bmx["apd90"][k], r["apd90"])
+        assert abs(bmx["cad90"][k] - r["cad90"]) <= CAD_TOL_MIXED, (k, bmx["cad90"][k], r["cad90"])
+        q = r["qnet"] / 1000
+        assert abs(bmx["qnet"][k] - q) <= QNET_RTOL_MIXED * abs(q), (k, bmx["qnet"][k], q)

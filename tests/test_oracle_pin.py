@@ -78,3 +78,52 @@ def test_biomarker_state_machine_last_beat(oracle):
     assert 0 < bm["cad50"] < bm["cad90"]
     assert bm["vm_peak"] > 0 and bm["dvmdt_max"] > 50
     assert np.isfinite(bm["qnet"])
+
+
+CIPA_CASES = sorted(GOLD.glob("cipa_*.npz"))
+
+
+@pytest.mark.parametrize("path", CIPA_CASES, ids=lambda p: p.stem)
+def test_cipa_oracle_rates_match_reference_golden(oracle, path):
+    """CiPA-ORd RATES of the oracle equal the reference computeRates bit for
+    bit at every fixture state, and the oracle's fixed-step trajectory
+    reproduces the fixture states exactly."""
+    g = np.load(path)
+    c = oracle.Cell("cipa2017", 0.0, float(g["conc"]), g["hill"], quirks=True)
+    c.set_pacing(float(g["bcl"]))
+    assert np.array_equal(c.states, g["states"][0])
+    for t, st, rr in zip(g["times"], g["states"], g["ref_rates"]):
+        c.y[: c.n] = st
+        r, _ = c.rates(float(t))
+        assert np.array_equal(r, rr), f"RATES differ at t={t}"
+    c2 = oracle.Cell("cipa2017", 0.0, float(g["conc"]), g["hill"], quirks=True)
+    c2.set_pacing(float(g["bcl"]))
+    every = int(round((g["times"][1] - g["times"][0]) / float(g["dt"])))
+    t = 0.0
+    for k in range(1, len(g["times"])):
+        for _ in range(every):
+            c2.step(t, float(g["dt"]))
+            t += float(g["dt"])
+        assert np.array_equal(c2.states, g["states"][k])
+
+
+def test_cipa_oracle_rates_bitwise_vs_compiled_reference(oracle):
+    if not oracle.ref_available("cipa2017"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    rng = np.random.default_rng(17)
+    hill = np.zeros(20)
+    hill[0:14:2] = 10 ** rng.uniform(-1, 2, 7)
+    hill[1:14:2] = rng.uniform(0.6, 1.8, 7)
+    hill[14:19] = [50.0, 0.002, 0.95, 300.0, -60.0]
+    r = oracle.RefCell("cipa2017", 0.0, 1.5, hill)
+    c = oracle.Cell("cipa2017", 0.0, 1.5, hill, quirks=True)
+    assert np.array_equal(r.states, c.states)
+    t = 0.0
+    for k in range(60000):
+        if k % 3000 == 0:
+            r.states[:] = c.states
+            r.L.ref_compute_rates(r.h, t)
+            mr, _ = c.rates(t)
+            assert np.array_equal(r.arr("rates", r.n), mr)
+        c.step(t, 0.005)
+        t += 0.005
