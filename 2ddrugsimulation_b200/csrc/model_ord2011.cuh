@@ -553,24 +553,42 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
     const G k63 = (G)cipa::A63 * P::ex((G)cipa::B63 * v) * (G)cipa::Q63;
     const G unb = P::dv(q.Ku * k53, k63);
     const G trap = P::dv(q.Kt, one + P::ex(-(v - q.Vhalf) * (G)(1.0 / 6.789)));
-    const G IC1 = (G)y.IC1, IC2 = (G)y.IC2, C1 = (G)y.C1, C2 = (G)y.C2, O = (G)y.O, IO = (G)y.IO;
-    const G IOb = (G)y.IObound, Ob = (G)y.Obound, Cb = (G)y.Cbound;
-    const G f11 = k11 * IC1 - k21 * IC2, f51 = k51 * C1 - k61 * IC1, f3 = k3 * IC2 - k4 * IO;
-    const G f52 = k52 * C2 - k62 * IC2, f1 = k1 * C1 - k2 * C2, f31 = k31 * C2 - k41 * O;
-    const G f53 = k53 * O - k63 * IO, fbo = q.bind * O - q.Ku * Ob, fbi = q.bind * IO - unb * IOb;
-    const G ftc = trap * Cb;
-    const G dIC1 = -f11 + f51;
-    const G dIC2 = (f11 - f3) + f52;
-    const G dC1 = -f1 - f51;
-    const G dC2 = (f1 - f31) - f52;
-    const G dO = (f31 - f53) - fbo;
-    const G dIO = (f3 + f53) - fbi;
-    const G dIOb = (fbi + ftc) - q.Kt * IOb;
-    const G dOb = (fbo + ftc) - q.Kt * Ob;
-    const G dCb = -(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb);
-    y.IC1 += (double)dIC1 * dt; y.IC2 += (double)dIC2 * dt; y.C1 += (double)dC1 * dt;
-    y.C2 += (double)dC2 * dt; y.O += (double)dO * dt; y.IO += (double)dIO * dt;
-    y.IObound += (double)dIOb * dt; y.Obound += (double)dOb * dt; y.Cbound += (double)dCb * dt;
+    // The chain is linear in its states for this step's V: when its largest
+    // outflow rate makes one Euler step unstable (dt*lam >= 2: fast drug
+    // binding, or IC1 -> C1 above ~43 mV) it takes N = ceil(dt*lam/1.8)
+    // Euler substeps with the same rates; N = 1 is the plain update.
+    G lam = k11 + k61;
+    lam = fmax(lam, k21 + k3 + k62);
+    lam = fmax(lam, k1 + k51);
+    lam = fmax(lam, k2 + k31 + k52);
+    lam = fmax(lam, k41 + k53 + q.bind);
+    lam = fmax(lam, k4 + k63 + q.bind);
+    lam = fmax(lam, unb + q.Kt);
+    lam = fmax(lam, q.Ku + q.Kt);
+    lam = fmax(lam, (G)2 * trap);
+    const G xs = (G)dt * lam * (G)(1.0 / 1.8);
+    const int nsub = xs <= (G)1 ? 1 : (xs < (G)256 ? (int)ceil(xs) : 256);
+    const double h = nsub == 1 ? dt : dt / nsub;
+    for (int sub = 0; sub < nsub; ++sub) {
+      const G IC1 = (G)y.IC1, IC2 = (G)y.IC2, C1 = (G)y.C1, C2 = (G)y.C2, O = (G)y.O, IO = (G)y.IO;
+      const G IOb = (G)y.IObound, Ob = (G)y.Obound, Cb = (G)y.Cbound;
+      const G f11 = k11 * IC1 - k21 * IC2, f51 = k51 * C1 - k61 * IC1, f3 = k3 * IC2 - k4 * IO;
+      const G f52 = k52 * C2 - k62 * IC2, f1 = k1 * C1 - k2 * C2, f31 = k31 * C2 - k41 * O;
+      const G f53 = k53 * O - k63 * IO, fbo = q.bind * O - q.Ku * Ob, fbi = q.bind * IO - unb * IOb;
+      const G ftc = trap * Cb;
+      const G dIC1 = -f11 + f51;
+      const G dIC2 = (f11 - f3) + f52;
+      const G dC1 = -f1 - f51;
+      const G dC2 = (f1 - f31) - f52;
+      const G dO = (f31 - f53) - fbo;
+      const G dIO = (f3 + f53) - fbi;
+      const G dIOb = (fbi + ftc) - q.Kt * IOb;
+      const G dOb = (fbo + ftc) - q.Kt * Ob;
+      const G dCb = -(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb);
+      y.IC1 += (double)dIC1 * h; y.IC2 += (double)dIC2 * h; y.C1 += (double)dC1 * h;
+      y.C2 += (double)dC2 * h; y.O += (double)dO * h; y.IO += (double)dIO * h;
+      y.IObound += (double)dIOb * h; y.Obound += (double)dOb * h; y.Cbound += (double)dCb * h;
+    }
   }
   y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
   y.xs2 = rush_larsen<P, true>(y.xs2, xs2ss, txs2, dt);
@@ -703,7 +721,8 @@ __device__ __forceinline__ void init_instance_cipa(double *__restrict__ par, dou
     if (hill[15] > 10E-14) Ku = hill[15];
     if (hill[16] > 10E-14) nn = hill[16];
     if (hill[17] > 10E-14) halfmax = hill[17];
-    if (hill[18] > 10E-14) Vhalf = hill[18];
+    // quirk: the reference's `> 10E-14` guard drops every negative Vhalf
+    if (quirks ? hill[18] > 10E-14 : hill[18] != 0.0) Vhalf = hill[18];
     if (hill[19] > 10E-14) Kt = hill[19];
   }
   const double Dn = ::exp(nn * ::log(conc));

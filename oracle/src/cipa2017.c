@@ -17,8 +17,8 @@
  * ten times finer step.)
  *
  * quirks = 1 reproduces the reference: ___initConsts resets CONSTANTS[0]
- * (celltype) to 0, and the drug block scales PCa after PCap/PCaNa/PCaK/
- * PCaNap/PCaKp were derived from it.
+ * (celltype) to 0, the drug block scales PCa after PCap/PCaNa/PCaK/
+ * PCaNap/PCaKp were derived from it, and a negative Vhalf is ignored.
  */
 #include <math.h>
 #include <string.h>
@@ -167,7 +167,13 @@ int cepo_cipa_init(cepo_cell *c, double celltype, double conc, const double *hil
   q->Ku = (hill[15] > 10E-14) ? hill[15] : q->Ku;
   q->n = (hill[16] > 10E-14) ? hill[16] : q->n;
   q->halfmax = (hill[17] > 10E-14) ? hill[17] : q->halfmax;
-  q->Vhalf = (hill[18] > 10E-14) ? hill[18] : q->Vhalf;
+  /* quirk (5): the reference's guard `> 10E-14` drops every negative Vhalf
+   * (:1538), and CiPA's fitted Vhalf values are negative; without quirks any
+   * non-zero Vhalf is used */
+  if (quirks)
+    q->Vhalf = (hill[18] > 10E-14) ? hill[18] : q->Vhalf;
+  else if (hill[18] != 0.0)
+    q->Vhalf = hill[18];
   if (hill[19] > 10E-14) q->Kt = hill[19];
   return 0;
 }
@@ -205,6 +211,9 @@ typedef struct {
   double mss, tm, hss, thf, ths, jss, tj, hssp, thsp, tjp, mLss, tmL, hLss, hLssp, ass, ta, iss, tiF, tiS,
       assp, tiFp, tiSp, dss, td, fss, tff, tfs, fcass, tfcaf, tfcas, tffp, tfcafp, anca, km2n, xs1ss, txs1,
       xs2ss, txs2, xk1ss, txk1, Jrel_inf, tau_rel, Jrel_infp, tau_relp;
+  /* Markov IKr: A*exp(B*V) of every transition (Q10 applied separately, as
+   * the reference orders the products), binding terms, largest outflow */
+  double e11, e21, e51, e61, e3, e4, e52, e62, e1, e2, e31, e41, e53, e63, bind, unb, trap, lam_max;
 } cipa_gates;
 
 /* Q10 factor exp(((Temp - 20) * log(q)) / 10) as the reference forms it */
@@ -234,9 +243,28 @@ static void cipa_compute(const cepo_cell *c, double TIME, const double *S, doubl
   const double t53 = q->A53 * exp(q->B53 * v) * S[O] * Q10(q->q53);
   const double t63 = q->A63 * exp(q->B63 * v) * S[IO] * Q10(q->q63);
   const double bind = (q->Kmax * q->Ku * exp(q->n * log(D))) / (exp(q->n * log(D)) + q->halfmax);
+  g->e11 = q->A11 * exp(q->B11 * v); g->e21 = q->A21 * exp(q->B21 * v); g->e51 = q->A51 * exp(q->B51 * v);
+  g->e61 = q->A61 * exp(q->B61 * v); g->e3 = q->A3 * exp(q->B3 * v); g->e4 = q->A4 * exp(q->B4 * v);
+  g->e52 = q->A52 * exp(q->B52 * v); g->e62 = q->A62 * exp(q->B62 * v); g->e1 = q->A1 * exp(q->B1 * v);
+  g->e2 = q->A2 * exp(q->B2 * v); g->e31 = q->A31 * exp(q->B31 * v); g->e41 = q->A41 * exp(q->B41 * v);
+  g->e53 = q->A53 * exp(q->B53 * v); g->e63 = q->A63 * exp(q->B63 * v);
   const double unbind_io = (q->Ku * q->A53 * exp(q->B53 * v) * Q10(q->q53)) /
                            (q->A63 * exp(q->B63 * v) * Q10(q->q63));
   const double trap = q->Kt / (1.00000 + exp(-(v - q->Vhalf) / 6.78900));
+  g->bind = bind; g->unb = unbind_io; g->trap = trap;
+  {
+    /* largest total outflow rate of a Markov state (1/ms) */
+    const double o[9] = {g->e11 * Q10(q->q11) + g->e61 * Q10(q->q61),
+                         g->e21 * Q10(q->q21) + g->e3 * Q10(q->q3) + g->e62 * Q10(q->q62),
+                         g->e1 * Q10(q->q1) + g->e51 * Q10(q->q51),
+                         g->e2 * Q10(q->q2) + g->e31 * Q10(q->q31) + g->e52 * Q10(q->q52),
+                         g->e41 * Q10(q->q41) + g->e53 * Q10(q->q53) + bind,
+                         g->e4 * Q10(q->q4) + g->e63 * Q10(q->q63) + bind,
+                         unbind_io + q->Kt, q->Ku + q->Kt, 2.0 * trap};
+    double mx = 0.0;
+    for (int k = 0; k < 9; ++k) mx = o[k] > mx ? o[k] : mx;
+    g->lam_max = mx;
+  }
   if (R_) {
     R_[Dst] = 0.0;
     R_[IC1] = (-(t11 - t21) + t51) - t61;
@@ -531,6 +559,32 @@ void cepo_cipa_rates(const cepo_cell *c, double t, const double *y, double *dydt
 
 #define RL(y, inf, tau) ((inf) - ((inf) - (y)) * exp(-dt / (tau)))
 
+/* forward-Euler substeps needed for stability of the Markov chain */
+static int markov_substeps(double lam_max, double dt) {
+  const double x = dt * lam_max / 1.8;
+  return x <= 1.0 ? 1 : (int)ceil(x);
+}
+
+/* Markov IKr derivatives at the step's rates (same terms as computeRates) */
+static void markov_rates(const cipa_p *q, const cipa_gates *g, const double *S, double *r) {
+  const double t11 = g->e11 * S[IC1] * Q10(q->q11), t21 = g->e21 * S[IC2] * Q10(q->q21);
+  const double t51 = g->e51 * S[C1] * Q10(q->q51), t61 = g->e61 * S[IC1] * Q10(q->q61);
+  const double t3 = g->e3 * S[IC2] * Q10(q->q3), t4 = g->e4 * S[IO] * Q10(q->q4);
+  const double t52 = g->e52 * S[C2] * Q10(q->q52), t62 = g->e62 * S[IC2] * Q10(q->q62);
+  const double t1 = g->e1 * S[C1] * Q10(q->q1), t2 = g->e2 * S[C2] * Q10(q->q2);
+  const double t31 = g->e31 * S[C2] * Q10(q->q31), t41 = g->e41 * S[O] * Q10(q->q41);
+  const double t53 = g->e53 * S[O] * Q10(q->q53), t63 = g->e63 * S[IO] * Q10(q->q63);
+  r[0] = (-(t11 - t21) + t51) - t61;
+  r[1] = (((t11 - t21) - (t3 - t4)) + t52) - t62;
+  r[2] = -(t1 - t2) - (t51 - t61);
+  r[3] = ((t1 - t2) - (t31 - t41)) - (t52 - t62);
+  r[4] = ((t31 - t41) - (t53 - t63)) - (g->bind * S[O] - q->Ku * S[Obound]);
+  r[5] = ((t3 - t4) + t53 - t63) - (g->bind * S[IO] - g->unb * S[IObound]);
+  r[6] = ((g->bind * S[IO] - g->unb * S[IObound]) + g->trap * S[Cbound]) - q->Kt * S[IObound];
+  r[7] = ((g->bind * S[O] - q->Ku * S[Obound]) + g->trap * S[Cbound]) - q->Kt * S[Obound];
+  r[8] = -(g->trap * S[Cbound] - q->Kt * S[Obound]) - (g->trap * S[Cbound] - q->Kt * S[IObound]);
+}
+
 /* Fixed-step scheme: Rush-Larsen gates, forward Euler for the Markov IKr
  * states, V, ions and CaMKII (the ORd scheme, Ohara_Rudy_2011.cpp:1036-1094). */
 void cepo_cipa_step(const cepo_cell *c, double t, double dt, double *S, cepo_currents *cur) {
@@ -569,17 +623,31 @@ void cepo_cipa_step(const cepo_cell *c, double t, double dt, double *S, cepo_cur
   S[Jrelnp] = RL(S[Jrelnp], g.Jrel_inf, g.tau_rel);
   S[Jrelp] = RL(S[Jrelp], g.Jrel_infp, g.tau_relp);
   /* Markov IKr states: forward Euler, as the reference scheme treats every
-   * non-gate state (stable at dt = 0.005 ms while V < ~43 mV, where the
-   * IC1 -> C1 rate stays below 2/dt) */
-  S[IC1] = S[IC1] + R_[IC1] * dt;
-  S[IC2] = S[IC2] + R_[IC2] * dt;
-  S[C1] = S[C1] + R_[C1] * dt;
-  S[C2] = S[C2] + R_[C2] * dt;
-  S[O] = S[O] + R_[O] * dt;
-  S[IO] = S[IO] + R_[IO] * dt;
-  S[IObound] = S[IObound] + R_[IObound] * dt;
-  S[Obound] = S[Obound] + R_[Obound] * dt;
-  S[Cbound] = S[Cbound] + R_[Cbound] * dt;
+   * non-gate state. The chain is linear in its states for the step's V, so
+   * when its largest outflow rate lam makes one Euler step unstable
+   * (dt*lam >= 2: fast drug binding, or the IC1 -> C1 rate above ~43 mV) the
+   * step is split into N = ceil(dt*lam/1.8) Euler substeps with the same
+   * rates. N = 1 is exactly the plain forward-Euler update. */
+  const int nsub = markov_substeps(g.lam_max, dt);
+  if (nsub <= 1) {
+    S[IC1] = S[IC1] + R_[IC1] * dt;
+    S[IC2] = S[IC2] + R_[IC2] * dt;
+    S[C1] = S[C1] + R_[C1] * dt;
+    S[C2] = S[C2] + R_[C2] * dt;
+    S[O] = S[O] + R_[O] * dt;
+    S[IO] = S[IO] + R_[IO] * dt;
+    S[IObound] = S[IObound] + R_[IObound] * dt;
+    S[Obound] = S[Obound] + R_[Obound] * dt;
+    S[Cbound] = S[Cbound] + R_[Cbound] * dt;
+  } else {
+    const double h = dt / nsub;
+    for (int k = 0; k < nsub; ++k) {
+      double r[9];
+      markov_rates(q, &g, S, r);
+      S[IC1] += r[0] * h; S[IC2] += r[1] * h; S[C1] += r[2] * h; S[C2] += r[3] * h; S[O] += r[4] * h;
+      S[IO] += r[5] * h; S[IObound] += r[6] * h; S[Obound] += r[7] * h; S[Cbound] += r[8] * h;
+    }
+  }
   S[CaMKt] = S[CaMKt] + R_[CaMKt] * dt;
   S[V] = S[V] + R_[V] * dt;
   S[nai] = S[nai] + R_[nai] * dt;

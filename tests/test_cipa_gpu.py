@@ -126,3 +126,26 @@ def test_cipa_biomarkers_fp64_and_mixed(cep, gpu, oracle):
         assert abs(bmx["cad90"][k] - r["cad90"]) <= CAD_TOL_MIXED, (k, bmx["cad90"][k], r["cad90"])
         q = r["qnet"] / 1000
         assert abs(bmx["qnet"][k] - q) <= QNET_RTOL_MIXED * abs(q), (k, bmx["qnet"][k], q)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cipa_stiff_drug_binding_stays_finite(cep, gpu, oracle, precision):
+    """A sample whose binding Hill coefficient (3.4) and concentration give a
+    drug-binding rate of ~780 /ms: one forward-Euler step of the Markov chain
+    is unstable at dt = 0.005 ms; the substepped update keeps it finite and
+    on the oracle's trajectory."""
+    hill = np.array([97.0292, 0.8377, 0.9136, 0.7587, 54.8446, 0.5487, 0.3744, 1.076, 0.8283, 2.6202,
+                     0.1226, 3.6055, 0.0, 0.0, 375209.231, 0.0082, 3.4183, 40305.2473, -84.514, 3.5e-5])
+    conc = 16.341988810388337
+    b = cep.Batch("cipa2017", 1, precision)
+    b.init(conc=conc, hill=hill, quirks=True)
+    b.set_pacing(2000.0)
+    b.run(80000)
+    st = b.get_states()[0]
+    assert np.isfinite(st).all() and b.status()[0] == cep.INST_RUNNING
+    c = oracle.Cell("cipa2017", 0.0, conc, hill, quirks=True)
+    c.set_pacing(2000.0)
+    c.run(0.0, 0.005, 80000)
+    tol = VM_TOL_FP64 if precision == "fp64" else 0.5
+    assert abs(st[0] - c.states[0]) <= tol
