@@ -59,6 +59,7 @@ _SIGS = {
     "cep_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "cep_batch_set_block": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cep_batch_set_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "cep_batch_init": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_int, ctypes.c_uint]),
     "cep_batch_set_pacing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_double]),
@@ -177,6 +178,11 @@ class Batch:
 
     def set_block(self, threads: int):
         _check(lib().cep_batch_set_block(self._h, threads))
+        return self
+
+    def set_kernel(self, variant: str):
+        """'cell' (one thread per cell) or 'roles' (4 warps per 32 cells)."""
+        _check(lib().cep_batch_set_kernel(self._h, {"cell": 0, "roles": 1}[variant]))
         return self
 
     def run(self, n_steps: int):

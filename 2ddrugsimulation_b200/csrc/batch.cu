@@ -25,7 +25,7 @@
 #include "../../include/cep_b200.h"
 #include "biomarkers.cuh"
 #include "cep_device.cuh"
-#include "model_ord2011.cuh"
+#include "model_ord.cuh"
 
 namespace {
 
@@ -63,7 +63,8 @@ struct cep_batch {
   bool initialized = false, has_protocol = false;
   double dt = 0.005, dt_write = 1.0, qnet_thr = -1e300;
   int n_pace = 0, first_pace = -1;
-  int block = 128;  // threads per block of the run kernel
+  int block = 128;    // threads per block of the one-thread-per-cell kernel
+  bool roles = false; // warp-specialised kernel (4 warps per 32 cells)
   std::vector<void *> allocs;
 };
 
@@ -71,6 +72,7 @@ namespace cep {
 
 // ------------------------------------------------------------------ traits
 struct OrdModel {
+  static constexpr bool kCipa = false;
   static constexpr int kStates = ord::kNumStates;
   static constexpr int kParams = ord::kNumParams;
   static constexpr int kCai = ord::cai;
@@ -101,6 +103,7 @@ struct OrdModel {
 };
 
 struct CipaModel : OrdModel {
+  static constexpr bool kCipa = true;
   static constexpr int kStates = ord::cipa::kNumStates;
   static constexpr int kCai = ord::cipa::cai;
   template <class G>
@@ -215,6 +218,108 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
   a.status[i] = st;
 }
 
+// Warp-specialised form of run_kernel for populations too small to fill the
+// GPU one thread per cell: a block of 4 warps advances 32 cells, warp r
+// evaluating role r of the model (the channel groups of model_ord.cuh) for
+// all 32. Each step the roles' contributions go through double-buffered
+// shared memory ([2][4 roles][8 fields][32 cells], lane-contiguous, no bank
+// conflicts) behind one barrier; every warp then applies the forward-Euler
+// update of V and the ions to its own copy of those FP64 states (identical
+// inputs and operations, so the copies stay identical) and warp 0 runs the
+// biomarker state machine. The trip count is the same for every lane;
+// finished or invalid lanes are predicated off so the barrier stays uniform.
+template <class M, class P, int R>
+__device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part)[4][8][32], int lane) {
+  using G = typename P::G;
+  const int64_t i = (int64_t)blockIdx.x * 32 + lane;
+  const bool valid = i < a.n;
+  const int64_t il = valid ? i : (int64_t)a.n - 1;
+  int st = a.status[il];
+  bool alive = valid && st == CEP_INST_RUNNING;
+  if (!__syncthreads_or(alive)) return;  // uniform: every warp sees the same 32 cells
+  typename M::template Y<G> y;
+  typename M::template Par<G> q;
+  M::template load<G>(y, a.y, a.ld, il);
+  M::template load_par<G>(q, a.par, a.ld, il);
+  double t = a.t[il];
+  int iout = a.iout[il];
+  const bm::Sched sc{a.sched[il], a.sched[a.ld + il], a.sched[2 * a.ld + il], a.sched[3 * a.ld + il]};
+  const bool bm_on = R == 0 && a.bm_on && sc.first_pace >= 0;
+  int cnt_print = sc.print_freq > 0 ? sc.print_freq - (iout % sc.print_freq) : 0x7fffffff;
+  int cnt_bcl = sc.steps_per_bcl > 0 ? sc.steps_per_bcl - (iout % sc.steps_per_bcl) : 0x7fffffff;
+  const double bcl = a.par[M::p_bcl() * a.ld + il];
+  const double stim_start = a.par[M::p_stim_start() * a.ld + il];
+  typename M::template Cur<G> c;
+  int buf = 0;
+  for (int k = 0; k <= a.n_steps; ++k) {
+    const bool can_update = iout < sc.imax;
+    const bool active = alive && !(can_update && k == a.n_steps);
+    const bool upd = active && can_update;
+    const double V0 = y.V;
+    const double cai0 = M::cai_of(y);
+    const auto ctx = ord::context<P>(y, q, t, a.stim_mode);
+    ord::Part<G> p;
+    ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      const int fld = ord::role_field(R, f);
+      if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
+    }
+    __syncthreads();
+    ord::Part<G> s;
+#pragma unroll
+    for (int f = 0; f < ord::kNumSums; ++f) s.f[f] = (G)0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        const int fld = ord::role_field(r, f);
+        if (fld >= 0) s.f[fld] += part[buf][r][f][lane];
+      }
+    }
+    ord::combine<P>(y, q, s, a.dt, upd, c);
+    if (bm_on && active && iout >= 1)
+      bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
+                 (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
+                 cnt_print, cnt_bcl);
+    if (active) {
+      if (!can_update) {
+        st = CEP_INST_DONE;
+        alive = false;
+      } else {
+        t += a.dt;
+        ++iout;
+        if (!isfinite(y.V)) {
+          st = CEP_INST_NONFINITE;
+          alive = false;
+        }
+      }
+    }
+    buf ^= 1;
+  }
+  if (valid) {
+    ord::store_role<M::kCipa>(R, y, a.y, a.ld, i);
+    if (R == 0) {
+      a.t[i] = t;
+      a.iout[i] = iout;
+      a.status[i] = st;
+    }
+  }
+}
+
+template <class M, class P>
+__global__ void __launch_bounds__(128) run_roles_kernel(RunArgs a) {
+  using G = typename P::G;
+  __shared__ G part[2][4][8][32];
+  const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  switch (role) {
+    case 0: role_loop<M, P, 0>(a, part, lane); break;
+    case 1: role_loop<M, P, 1>(a, part, lane); break;
+    case 2: role_loop<M, P, 2>(a, part, lane); break;
+    default: role_loop<M, P, 3>(a, part, lane); break;
+  }
+}
+
 // Rates at the current state (no update).
 template <class M>
 __global__ void rates_kernel(const double *s, const double *par, int64_t ld, int n, double t, int stim_mode,
@@ -285,12 +390,20 @@ struct Ops {
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "reset launch failed");
   }
   static int launch_run(cep_batch *b, const RunArgs &a) {
-    const int block = b->block;
-    const int grid = (b->n + block - 1) / block;
-    if (b->precision == CEP_PREC_MIXED)
-      run_kernel<M, Mixed><<<grid, block, 0, b->stream>>>(a);
-    else
-      run_kernel<M, F64><<<grid, block, 0, b->stream>>>(a);
+    if (b->roles) {
+      const int grid = (b->n + 31) / 32;
+      if (b->precision == CEP_PREC_MIXED)
+        run_roles_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
+      else
+        run_roles_kernel<M, F64><<<grid, 128, 0, b->stream>>>(a);
+    } else {
+      const int block = b->block;
+      const int grid = (b->n + block - 1) / block;
+      if (b->precision == CEP_PREC_MIXED)
+        run_kernel<M, Mixed><<<grid, block, 0, b->stream>>>(a);
+      else
+        run_kernel<M, F64><<<grid, block, 0, b->stream>>>(a);
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "run launch failed: %s", cudaGetErrorString(e));
   }
@@ -391,6 +504,9 @@ int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     b->block = (n <= sms * 8 * 32) ? 32 : 128;
+    // Below ~1.5 waves of one-thread-per-cell occupancy the 4-warps-per-32-
+    // cells kernel keeps 4x more warps in flight.
+    b->roles = model == CEP_MODEL_ORD2011 || model == CEP_MODEL_CIPA2017 ? (n <= sms * 12 * 32) : false;
   }
   int rc = CEP_OK;
   if ((rc = dev_alloc(b, &b->states, (size_t)b->ns * b->ld)) || (rc = dev_alloc(b, &b->params, (size_t)b->np * b->ld)) ||
@@ -426,6 +542,15 @@ int cep_batch_set_block(cep_batch_t b, int threads_per_block) {
   if (threads_per_block != 32 && threads_per_block != 64 && threads_per_block != 96 && threads_per_block != 128)
     return fail(CEP_ERR_ARG, "threads_per_block must be 32, 64, 96 or 128");
   b->block = threads_per_block;
+  return CEP_OK;
+}
+
+int cep_batch_set_kernel(cep_batch_t b, int variant) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (variant != CEP_KERNEL_CELL && variant != CEP_KERNEL_ROLES) return fail(CEP_ERR_ARG, "bad kernel variant %d", variant);
+  if (variant == CEP_KERNEL_ROLES && b->model != CEP_MODEL_ORD2011 && b->model != CEP_MODEL_CIPA2017)
+    return fail(CEP_ERR_UNSUPPORTED, "warp-specialised kernel exists for the ORd family only");
+  b->roles = variant == CEP_KERNEL_ROLES;
   return CEP_OK;
 }
 

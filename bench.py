@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "cell", "roles"],
+                    help="one thread per cell, 4 warps per 32 cells, or the library's default for the size")
     return ap.parse_args()
 
 
@@ -229,6 +231,8 @@ def run_ours(args, world, rank, local, pg, model):
     launches = 0
     for prec in ("mixed", "fp64"):
         b = cep.Batch(model, n, prec)
+        if args.kernel != "auto":
+            b.set_kernel(args.kernel)
         b.init(conc=conc, hill=hill, quirks=True)
         b.set_pacing(BCL)
         b.set_protocol(DT, 1000, 750, dt_write=1.0)
@@ -337,7 +341,7 @@ def config_of(args, model, n, world):
     return {"workload": f"{name} population, {n} instances per GPU ({args.samples} IC50/Hill samples x "
                         f"{args.concs} concs), BCL 2000 ms, dt 0.005 ms, 1000-pace protocol with steepest-of-last-"
                         f"250 biomarkers fused; {args.seg} time steps per bench step",
-            "instances_per_gpu": n, "time_steps_per_bench_step": args.seg,
+            "instances_per_gpu": n, "time_steps_per_bench_step": args.seg, "kernel": args.kernel,
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance sharding x{world}"}
 
 

@@ -97,6 +97,12 @@ int cep_batch_size(cep_batch_t b, int *n, int *n_states);
 /* Threads per block of the run kernel (32, 64, 96 or 128); the default
  * spreads small populations over every SM. Used by the autotuner. */
 int cep_batch_set_block(cep_batch_t b, int threads_per_block);
+/* Kernel form: one thread per cell, or 4 warps per 32 cells each evaluating
+ * one group of channels (the default for populations smaller than ~1.5
+ * waves of the GPU; ORd family only). Used by the autotuner. */
+#define CEP_KERNEL_CELL 0
+#define CEP_KERNEL_ROLES 1
+int cep_batch_set_kernel(cep_batch_t b, int variant);
 
 /* initConsts for every instance and the model's initial STATES.
  * celltype[n] (NULL = 0, endo), conc[n] (drug concentration, same unit as
