@@ -307,11 +307,28 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   }
 }
 
+// The role of a warp follows the SM sub-partition (SMSP) it was placed on
+// (the warp slot modulo 4) whenever the block's four warps sit on four
+// different SMSPs, so every SMSP streams one role's instructions and its
+// instruction cache holds a quarter of the step's code; otherwise the warp
+// index decides.
+__device__ __forceinline__ int pick_role() {
+  __shared__ int slot[4];
+  const int w = threadIdx.x >> 5;
+  unsigned wid;
+  asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
+  if ((threadIdx.x & 31) == 0) slot[w] = (int)(wid & 3u);
+  __syncthreads();
+  const int m = (1 << slot[0]) | (1 << slot[1]) | (1 << slot[2]) | (1 << slot[3]);
+  return m == 0xF ? slot[w] : w;
+}
+
 template <class M, class P>
 __global__ void __launch_bounds__(128) run_roles_kernel(RunArgs a) {
   using G = typename P::G;
   __shared__ G part[2][4][8][32];
-  const int role = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
+  const int role = pick_role();
   switch (role) {
     case 0: role_loop<M, P, 0>(a, part, lane); break;
     case 1: role_loop<M, P, 1>(a, part, lane); break;

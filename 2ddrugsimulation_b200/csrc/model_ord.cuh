@@ -246,7 +246,7 @@ __host__ __device__ constexpr int role_field(int role, int k) {
   constexpr int t[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, -1, -1, -1},
                            {S_iV, S_iK, S_Ito, S_IKr, S_IKs, S_IK1, -1, -1},
                            {S_iV, S_iNass, S_iKss, S_iCass, S_iCai, S_Jrel, S_ICaL, -1},
-                           {S_iV, S_iNa, S_iNass, S_iCass, S_iCai, S_Jup, S_IKr, -1}};
+                           {S_iV, S_iNa, S_iNass, S_iCass, S_iCai, S_Jup, S_IKr, S_iK}};
   return t[role][k];
 }
 
@@ -587,6 +587,7 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
   o.f[S_iCai] = -(G)2.0 * INaCa_i;
   o.f[S_Jup] = Jup;
   o.f[S_IKr] = IKr;
+  o.f[S_iK] = IKr;  // CiPA's IKr is a potassium flux too (zero for ORd: role 1 carries it)
   if constexpr (kCipa) {
     if (!update) return;
     // Markov IKr with drug binding and trapping (ohara_rudy_cipa_v1_2017.cpp:

@@ -44,7 +44,74 @@ static double measure(int iters) {
   return cudaGetLastError() == cudaSuccess && ms > 0 ? 2.0 * fmas / (ms * 1e-3) : -1.0;
 }
 
+// SFU (MUFU) throughput: independent ex2.approx chains.
+__global__ void sfu_loop(float *out, int iters) {
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 0.1f, x2 = x0 + 0.2f, x3 = x0 + 0.3f;
+  float x4 = x0 + 0.4f, x5 = x0 + 0.5f, x6 = x0 + 0.6f, x7 = x0 + 0.7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = exp2f(-x0); x1 = exp2f(-x1); x2 = exp2f(-x2); x3 = exp2f(-x3);
+      x4 = exp2f(-x4); x5 = exp2f(-x5); x6 = exp2f(-x6); x7 = exp2f(-x7);
+    }
+  }
+  const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == -12345.f) out[0] = s;
+}
+
+// Which SM sub-partition each warp of a 4-warp block lands on: out[b*4+w] =
+// %warpid & 3 for block b, warp w (launch shape of the ionic roles kernel).
+__global__ void warp_slot_probe(int *out) {
+  unsigned wid;
+  asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
+  if ((threadIdx.x & 31) == 0) out[blockIdx.x * 4 + (threadIdx.x >> 5)] = (int)(wid & 3u);
+}
+
 extern "C" {
+// SFU operations/s (ex2.approx) on the current device.
+double cep_probe_sfu_ops(void) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  float *out = nullptr;
+  if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) return -1.0;
+  const int block = 256, grid = sms * 8, iters = 512;
+  sfu_loop<<<grid, block>>>(out, 8);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  sfu_loop<<<grid, block>>>(out, iters);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double ops = (double)grid * block * iters * 16.0 * 8.0;
+  return cudaGetLastError() == cudaSuccess && ms > 0 ? ops / (ms * 1e-3) : -1.0;
+}
+
+// Fraction of 4-warp blocks (n_blocks of them, 128 threads) whose warps sit
+// on four distinct SM sub-partitions.
+double cep_probe_warp_slots(int n_blocks) {
+  int *d = nullptr;
+  if (n_blocks <= 0 || cudaMalloc(&d, sizeof(int) * 4 * n_blocks) != cudaSuccess) return -1.0;
+  warp_slot_probe<<<n_blocks, 128>>>(d);
+  int *h = new int[4 * n_blocks];
+  cudaMemcpy(h, d, sizeof(int) * 4 * n_blocks, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  int ok = 0;
+  for (int b = 0; b < n_blocks; ++b) {
+    int m = 0;
+    for (int w = 0; w < 4; ++w) m |= 1 << (h[b * 4 + w] & 3);
+    ok += (m == 0xF);
+  }
+  delete[] h;
+  return (double)ok / n_blocks;
+}
+
 // FP32 / FP64 FMA throughput in flop/s (2 per FMA) on the current device.
 double cep_probe_fp32_fma_flops(void) { return measure<float>(4096); }
 double cep_probe_fp64_fma_flops(void) { return measure<double>(1024); }

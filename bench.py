@@ -65,6 +65,13 @@ def flops_per_step(model: str) -> float:
     return sum(OPS[model].values())
 
 
+def sfu_ops_per_step(model: str) -> float:
+    """Operations that need the special-function unit in the mixed path
+    (exp2/log2/reciprocal for every division and elementary function)."""
+    o = OPS[model]
+    return o["div"] + o["exp"] + o["log"] + o["pow"]
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -212,6 +219,11 @@ def measured_peaks():
         L.cep_probe_fp64_fma_flops.restype = ctypes.c_double
         out["fp32_tflops"] = max(L.cep_probe_fp32_fma_flops() for _ in range(3)) / 1e12
         out["fp64_tflops"] = max(L.cep_probe_fp64_fma_flops() for _ in range(3)) / 1e12
+        L.cep_probe_sfu_ops.restype = ctypes.c_double
+        L.cep_probe_warp_slots.restype = ctypes.c_double
+        L.cep_probe_warp_slots.argtypes = [ctypes.c_int]
+        out["sfu_tops"] = max(L.cep_probe_sfu_ops() for _ in range(3)) / 1e12
+        out["role_blocks_on_distinct_smsp"] = L.cep_probe_warp_slots(313)
     except OSError:
         pass
     mp = ROOT / "MEASURED_PEAKS.json"
@@ -386,13 +398,15 @@ def main():
     fl = flops_per_step(model)
     cell_steps_launch = n * args.seg
 
-    def roof(kernel_ms, peak_key, label):
-        ach = fl * cell_steps_launch / (kernel_ms * 1e-3) / 1e12
+    def roof(kernel_ms, peak_key, label, per_step=fl, source="bench.py FMA probe on this GPU (2 flop/FMA)"):
+        ach = per_step * cell_steps_launch / (kernel_ms * 1e-3) / 1e12
         pk = peaks.get(peak_key)
         tr = TRAFFIC_PER_INSTANCE.get(model)
         return {"bound": label, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
                 "frac": (ach / pk) if pk else None, "traffic": (tr * n) if tr else None,
-                "flops_per_cell_step": fl, "peak_source": "bench.py FMA probe on this GPU (2 flop/FMA)"}
+                "flops_per_cell_step": per_step, "peak_source": source}
+
+    sfu = sfu_ops_per_step(model)
 
     line = {
         "metric": METRIC, "value": mixed["value"], "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
@@ -403,7 +417,13 @@ def main():
                  "roofline": roof(fp64["kernel_ms"], "fp64_tflops", "fp64"), "clocks": fp64["clocks"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "kernel_ms": mixed["kernel_ms"],
-        "roofline": roof(mixed["kernel_ms"], "fp32_tflops", "fp32"),
+        # The mixed kernel is bound by the special-function unit: every
+        # division, exponential and logarithm is one MUFU operation (16 per
+        # SM per clock on B200), ~390 per cell-step against ~1,900 issue
+        # slots. "flop" here = one such algorithmic operation.
+        "roofline": roof(mixed["kernel_ms"], "sfu_tops", "sfu", per_step=sfu,
+                         source="bench.py ex2.approx throughput probe on this GPU (1 op/MUFU)"),
+        "roofline_fp32_pipe": roof(mixed["kernel_ms"], "fp32_tflops", "fp32"),
         "gpu_launches": launches,
         "clocks": mixed["clocks"],
         "cpu_baseline": cpu,
