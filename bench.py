@@ -58,7 +58,7 @@ OPS = {
 # DRAM bytes per launch per instance measured by ncu on the run kernel
 # (profiles/run_kernel_cipa2017_pop10k.md): the state and biomarker records
 # are read and written once per launch; everything else stays on chip.
-TRAFFIC_PER_INSTANCE = {"cipa2017": None, "ord2011": None}
+TRAFFIC_PER_INSTANCE = {"cipa2017": 705.0, "ord2011": None}
 
 
 def flops_per_step(model: str) -> float:
