@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,8 @@
 #include "biomarkers.cuh"
 #include "cep_device.cuh"
 #include "model_ord.cuh"
+#include "model_tt2006.cuh"
+#include "internal.h"
 
 namespace {
 
@@ -121,6 +124,38 @@ struct CipaModel : OrdModel {
   }
 };
 
+struct Tt06Model {
+  static constexpr bool kCipa = false;
+  static constexpr int kStates = tt06::kNumStates;
+  static constexpr int kParams = tt06::kNumParams;
+  static constexpr int kCai = tt06::Ca_i;
+  template <class G> using Y = tt06::Y<G>;
+  template <class G> using Par = tt06::Par<G>;
+  template <class G> using Cur = tt06::Cur<G>;
+  template <class G>
+  __device__ static void load(Y<G> &y, const double *s, int64_t ld, int64_t i) { tt06::load(y, s, ld, i); }
+  template <class G>
+  __device__ static void store(const Y<G> &y, double *s, int64_t ld, int64_t i) { tt06::store(y, s, ld, i); }
+  template <class G>
+  __device__ static void load_par(Par<G> &q, const double *p, int64_t ld, int64_t i) { tt06::load_par(q, p, ld, i); }
+  template <class P>
+  __device__ static void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                              int stim_mode, bool update, Cur<typename P::G> &c) {
+    tt06::step<P>(y, q, t, dt, stim_mode, update, c);
+  }
+  __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
+                              const double *hill, unsigned flags) {
+    (void)ct; (void)flags;
+    tt06::init_instance(par, s, ld, i, conc, hill);
+  }
+  template <class G>
+  __device__ static double cai_of(const Y<G> &y) { return y.Ca_i; }
+  __host__ __device__ static constexpr int p_bcl() { return tt06::P_BCL; }
+  __host__ __device__ static constexpr int p_stim_start() { return tt06::P_stim_start; }
+  __host__ __device__ static constexpr int p_duration() { return tt06::P_duration; }
+  __host__ __device__ static constexpr int p_amp() { return tt06::P_amp; }
+};
+
 // ----------------------------------------------------------------- kernels
 template <class M>
 __global__ void init_kernel(double *par, double *s, int64_t ld, int n, const double *celltype,
@@ -156,7 +191,20 @@ struct RunArgs {
   bm::View bv;
   double qnet_thr;
   int stim_mode;  // -1 periodic; 0/1 fixed tissue flag
+  // tissue stimulus (heart.cpp:309-323): isS1 = s1_mask[i] inside the window
+  const unsigned char *s1_mask;
+  double s1_bcl, s1_tcrt, s1_dur;
+  int s1_npace;
 };
+
+// Stimulus mode of instance i at time t: the tissue window when a mask is set.
+__device__ __forceinline__ int stim_mode_at(const RunArgs &a, int64_t i, double t) {
+  if (!a.s1_mask) return a.stim_mode;
+  const int iia = (int)(t / a.s1_bcl);
+  const bool win = iia < a.s1_npace && t < (double)iia * a.s1_bcl + a.s1_dur + a.s1_tcrt &&
+                   t > (double)iia * a.s1_bcl + a.s1_tcrt;
+  return (win && a.s1_mask[i]) ? 1 : 0;
+}
 
 __global__ void reset_kernel(RunArgs a, int p_bcl, int p_start, int cai_idx) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -196,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
     if (can_update && k == a.n_steps) break;  // budget spent; sample iout is taken next launch
     const double V0 = y.V;
     const double cai0 = M::cai_of(y);
-    M::template step<P>(y, q, t, a.dt, a.stim_mode, can_update, c);
+    M::template step<P>(y, q, t, a.dt, stim_mode_at(a, i, t), can_update, c);
     if (bm_on && iout >= 1)
       bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
                  (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
@@ -257,7 +305,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     const bool upd = active && can_update;
     const double V0 = y.V;
     const double cai0 = M::cai_of(y);
-    const auto ctx = ord::context<P>(y, q, t, a.stim_mode);
+    const auto ctx = ord::context<P>(y, q, t, stim_mode_at(a, il, t));
     ord::Part<G> p;
     ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
 #pragma unroll
@@ -407,7 +455,14 @@ struct Ops {
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "reset launch failed");
   }
   static int launch_run(cep_batch *b, const RunArgs &a) {
-    if (b->roles) {
+    if constexpr (std::is_same<M, Tt06Model>::value) {
+      const int block = b->block;
+      const int grid = (b->n + block - 1) / block;
+      if (b->precision == CEP_PREC_MIXED)
+        run_kernel<M, Mixed><<<grid, block, 0, b->stream>>>(a);
+      else
+        run_kernel<M, F64><<<grid, block, 0, b->stream>>>(a);
+    } else if (b->roles) {
       const int grid = (b->n + 31) / 32;
       if (b->precision == CEP_PREC_MIXED)
         run_roles_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
@@ -450,7 +505,12 @@ const ModelInfo *model_info(int model) {
                                    &Ops<CipaModel>::launch_init, &Ops<CipaModel>::launch_pacing,
                                    &Ops<CipaModel>::launch_reset, &Ops<CipaModel>::launch_run,
                                    &Ops<CipaModel>::launch_rates, CipaModel::p_bcl()};
+  static const ModelInfo tt06_info{Tt06Model::kStates, Tt06Model::kParams, Tt06Model::kCai,
+                                   &Ops<Tt06Model>::launch_init, &Ops<Tt06Model>::launch_pacing,
+                                   &Ops<Tt06Model>::launch_reset, &Ops<Tt06Model>::launch_run,
+                                   &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl()};
   switch (model) {
+    case CEP_MODEL_TT2006: return &tt06_info;
     case CEP_MODEL_ORD2011: return &ord_info;
     case CEP_MODEL_CIPA2017: return &cipa_info;
     default: return nullptr;
@@ -482,6 +542,8 @@ RunArgs make_args(cep_batch *b, long n_steps) {
   a.bv.ld = b->ld;
   a.qnet_thr = b->qnet_thr;
   a.stim_mode = -1;
+  a.s1_mask = nullptr;
+  a.s1_bcl = 1.0; a.s1_tcrt = 0.0; a.s1_dur = 0.0; a.s1_npace = 0;
   return a;
 }
 
@@ -787,6 +849,20 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;
 }
+
+int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double bcl, double t_crt,
+                                   double dur, int n_pace, long n_steps) {
+  if (!b || !b->initialized) return fail(CEP_ERR_STATE, "tissue batch not initialised");
+  RunArgs a = make_args(b, n_steps);
+  a.bm_on = 0;
+  a.s1_mask = d_mask;
+  a.s1_bcl = bcl; a.s1_tcrt = t_crt; a.s1_dur = dur; a.s1_npace = n_pace;
+  return model_info(b->model)->run(b, a);
+}
+
+double *cep_internal_batch_v(cep_batch_t b) { return b ? b->states : nullptr; }
+void *cep_internal_batch_stream(cep_batch_t b) { return b ? (void *)b->stream : nullptr; }
+int cep_internal_set_fail(int code, const char *msg) { return fail(code, "%s", msg); }
 
 double cep_qinward(const cep_biomarkers_t *c, const cep_biomarkers_t *d) {
   if (!c || !d) return NAN;

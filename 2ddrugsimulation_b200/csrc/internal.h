@@ -1,0 +1,24 @@
+// Library-internal entry points shared between the translation units (not
+// part of the C ABI).
+#pragma once
+#include "../../include/cep_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// One Godunov ionic half-step for a tissue: every node of the batch advances
+// by n_steps fixed steps with the tissue stimulus flag isS1 = mask[i] while
+// iia*bcl + t_crt < t < iia*bcl + t_crt + dur and iia = (int)(t/bcl) < n_pace
+// (heart.cpp:309-323). d_mask is a device array of n bytes.
+int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double bcl, double t_crt,
+                                   double dur, int n_pace, long n_steps);
+// Device pointer of the membrane-potential row (n doubles) and the stream.
+double *cep_internal_batch_v(cep_batch_t b);
+void *cep_internal_batch_stream(cep_batch_t b);
+// Records an error message for cep_last_error and returns code.
+int cep_internal_set_fail(int code, const char *msg);
+
+#ifdef __cplusplus
+}
+#endif

@@ -103,6 +103,17 @@ int cepo_pcg(int n, const int *row_ptr, const int *col_idx, const double *a_val,
              double *x, double rtol, int max_iter, double *rel_res);
 void cepo_spmv(int n, const int *row_ptr, const int *col_idx, const double *val, const double *x,
                double *y);
+/* Same with the norm choice: precond_norm 1 = ||M^-1 r||/||M^-1 b|| (PETSc's
+ * default for CG), 0 = ||r||/||b||. */
+int cepo_pcg2(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b, double *x,
+              double rtol, int max_iter, int precond_norm, double *rel_res);
+/* Element matrices (nn x nn, row-major) of an axis-aligned element of edge h. */
+void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be);
+/* Godunov-split tissue run on a structured grid (heart.cpp:127-165). */
+long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+                     long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                     double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                     const double *celltype, double *V, int *iters_out);
 
 #ifdef __cplusplus
 }

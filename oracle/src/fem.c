@@ -1,0 +1,267 @@
+/*
+ * TEST INFRASTRUCTURE ONLY. CPU restatement of the reference's monodomain
+ * FEM diffusion solve (fem.cpp / heart.cpp) on structured grids.
+ *
+ * Elements: Q1 quadrilaterals (2D) and trilinear hexahedra (3D) with the
+ * reference's local node order and shape functions (fem.cpp:398-478), its
+ * Gauss points at +-0.57735 with unit weights (fem.cpp:231-271), and its
+ * element matrices (fem.cpp:628-661):
+ *   A_e[j][k] = sum_g Phi_j Phi_k detJ/dt + grad Phi_j . D grad Phi_k detJ
+ *   B_e[j][k] = sum_g Phi_j Phi_k detJ
+ * D per element is the reference's scalar DE (n_d == 1) or, as an
+ * extension for anisotropic tissue, a symmetric tensor. The global solve
+ * A V = B V* / dt uses Jacobi-preconditioned CG from a zero initial guess
+ * (fem.cpp:705-718, 753-760; PETSc KSPCG + PCJACOBI, KSPSetInitialGuessNonzero
+ * is never called). PETSc itself is not in the reference tree, so the
+ * stopping rule is stated here: ||M^-1 r||_2 <= rtol ||M^-1 b||_2 (PETSc's
+ * default preconditioned norm for CG) or ||r||_2 <= rtol ||b||_2.
+ * Parity of the solve with PETSc is unpinned.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "cep_oracle.h"
+
+static const double GA = 0.57735;
+
+long cepo_fem_nnz(int dim, int nx, int ny, int nz) {
+  /* stencil neighbours of every node, (3 or 2 per axis) */
+  long cx = 3L * nx - 2, cy = 3L * ny - 2, cz = dim == 3 ? 3L * nz - 2 : 1;
+  return cx * cy * cz;
+}
+
+/* local node offsets of the reference's node order */
+static void local_offsets(int dim, int off[8][3]) {
+  static const int q4[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}};
+  static const int h8[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  memcpy(off, dim == 2 ? (const void *)q4 : (const void *)h8, sizeof(int) * 3 * (dim == 2 ? 4 : 8));
+}
+
+/* Element matrices of an axis-aligned element of edge h (fem.cpp:628-661).
+ * D: 1 value (scalar) or 3 (2D: xx,xy,yy) / 6 (3D: xx,xy,xz,yy,yz,zz). */
+void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be) {
+  const int nn = dim == 2 ? 4 : 8;
+  double gp[8][3];
+  if (dim == 2) {
+    const double g4[4][2] = {{-GA, -GA}, {GA, -GA}, {GA, GA}, {-GA, GA}};
+    for (int g = 0; g < 4; ++g) { gp[g][0] = g4[g][0]; gp[g][1] = g4[g][1]; gp[g][2] = 0; }
+  } else {
+    const double aa[2] = {-GA, GA};
+    int n = 0;
+    for (int ix = 0; ix < 2; ++ix)
+      for (int iy = 0; iy < 2; ++iy)
+        for (int iz = 0; iz < 2; ++iz) { gp[n][0] = aa[ix]; gp[n][1] = aa[iy]; gp[n][2] = aa[iz]; ++n; }
+  }
+  double Dm[3][3] = {{0}};
+  if (n_d == 1) {
+    for (int a = 0; a < dim; ++a) Dm[a][a] = D[0];
+  } else if (dim == 2) {
+    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[1][1] = D[2];
+  } else {
+    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
+    Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
+  }
+  const double jac = 0.5 * h;                      /* dx/dxi on each axis */
+  const double detJ = dim == 2 ? jac * jac : jac * jac * jac;
+  const double inv = 1.0 / jac;
+  for (int j = 0; j < nn * nn; ++j) { Ae[j] = 0; Be[j] = 0; }
+  for (int g = 0; g < nn; ++g) {
+    const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
+    double Phi[8], dS[8][3];
+    if (dim == 2) {
+      Phi[0] = (1. - s) * (1. - t) / 4.; Phi[1] = (1. + s) * (1. - t) / 4.;
+      Phi[2] = (1. + s) * (1. + t) / 4.; Phi[3] = (1. - s) * (1. + t) / 4.;
+      dS[0][0] = -(1. - t) / 4.; dS[0][1] = -(1. - s) / 4.;
+      dS[1][0] = +(1. - t) / 4.; dS[1][1] = -(1. + s) / 4.;
+      dS[2][0] = +(1. + t) / 4.; dS[2][1] = +(1. + s) / 4.;
+      dS[3][0] = -(1. + t) / 4.; dS[3][1] = +(1. - s) / 4.;
+    } else {
+      const double sp = 1 + s, sm = 1 - s, tp = 1 + t, tm = 1 - t, zp = 1 + z, zm = 1 - z;
+      Phi[0] = sm * tm * zm / 8.; Phi[1] = sp * tm * zm / 8.; Phi[2] = sp * tp * zm / 8.; Phi[3] = sm * tp * zm / 8.;
+      Phi[4] = sm * tm * zp / 8.; Phi[5] = sp * tm * zp / 8.; Phi[6] = sp * tp * zp / 8.; Phi[7] = sm * tp * zp / 8.;
+      const double sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                               {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+      for (int n = 0; n < 8; ++n) {
+        const double fs = 1 + sg[n][0] * s, ft = 1 + sg[n][1] * t, fz = 1 + sg[n][2] * z;
+        dS[n][0] = sg[n][0] * ft * fz / 8.; dS[n][1] = sg[n][1] * fs * fz / 8.; dS[n][2] = sg[n][2] * fs * ft / 8.;
+      }
+    }
+    double dX[8][3];
+    for (int n = 0; n < nn; ++n)
+      for (int a = 0; a < dim; ++a) dX[n][a] = dS[n][a] * inv;
+    for (int j = 0; j < nn; ++j)
+      for (int k = 0; k < nn; ++k) {
+        double gdg = 0;
+        for (int a = 0; a < dim; ++a)
+          for (int b = 0; b < dim; ++b) gdg += dX[j][a] * Dm[a][b] * dX[k][b];
+        Ae[j * nn + k] += Phi[j] * Phi[k] * detJ / dt + gdg * detJ;
+        Be[j * nn + k] += Phi[j] * Phi[k] * detJ;
+      }
+  }
+}
+
+static long node_id(int dim, int nx, int ny, int i, int j, int k) {
+  (void)dim;
+  return (long)i + (long)nx * ((long)j + (long)ny * (long)k);
+}
+
+/* CSR over the structured grid: every row lists its stencil neighbours in
+ * ascending column order; values summed over the elements sharing both
+ * nodes. D holds n_d values per element (element-major). */
+int cepo_fem_assemble(int dim, int nx, int ny, int nz, double h, double dt, const double *D, int n_d,
+                      int *row_ptr, int *col_idx, double *a_val, double *b_val) {
+  if (dim == 2) nz = 1;
+  const long n = (long)nx * ny * nz;
+  long p = 0;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        row_ptr[node_id(dim, nx, ny, i, j, k)] = (int)p;
+        for (int dk = (dim == 3 ? -1 : 0); dk <= (dim == 3 ? 1 : 0); ++dk)
+          for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di) {
+              const int ii = i + di, jj = j + dj, kk = k + dk;
+              if (ii < 0 || ii >= nx || jj < 0 || jj >= ny || kk < 0 || kk >= nz) continue;
+              col_idx[p] = (int)node_id(dim, nx, ny, ii, jj, kk);
+              a_val[p] = 0;
+              b_val[p] = 0;
+              ++p;
+            }
+      }
+  row_ptr[n] = (int)p;
+  int off[8][3];
+  local_offsets(dim, off);
+  const int nn = dim == 2 ? 4 : 8;
+  const int ex = nx - 1, ey = ny - 1, ez = dim == 3 ? nz - 1 : 1;
+  double Ae[64], Be[64];
+  for (int ek = 0; ek < ez; ++ek)
+    for (int ej = 0; ej < ey; ++ej)
+      for (int ei = 0; ei < ex; ++ei) {
+        const long e = (long)ei + (long)ex * ((long)ej + (long)ey * ek);
+        cepo_fem_element(dim, h, dt, D + e * n_d, n_d, Ae, Be);
+        long gid[8];
+        for (int a = 0; a < nn; ++a) gid[a] = node_id(dim, nx, ny, ei + off[a][0], ej + off[a][1], ek + off[a][2]);
+        for (int a = 0; a < nn; ++a)
+          for (int b = 0; b < nn; ++b) {
+            int q = row_ptr[gid[a]];
+            while (col_idx[q] != gid[b]) ++q;
+            a_val[q] += Ae[a * nn + b];
+            b_val[q] += Be[a * nn + b];
+          }
+      }
+  return 0;
+}
+
+void cepo_spmv(int n, const int *row_ptr, const int *col_idx, const double *val, const double *x, double *y) {
+  for (int i = 0; i < n; ++i) {
+    double s = 0;
+    for (int q = row_ptr[i]; q < row_ptr[i + 1]; ++q) s += val[q] * x[col_idx[q]];
+    y[i] = s;
+  }
+}
+
+static double dot(int n, const double *a, const double *b) {
+  double s = 0;
+  for (int i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+/* Jacobi-PCG from x = 0. precond_norm: 1 -> ||M^-1 r|| / ||M^-1 b||
+ * (PETSc default for CG), 0 -> ||r|| / ||b||. Returns iterations (or
+ * -max_iter if not converged). */
+int cepo_pcg2(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b, double *x,
+              double rtol, int max_iter, int precond_norm, double *rel_res) {
+  double *dinv = malloc(sizeof(double) * n), *r = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n);
+  double *pv = malloc(sizeof(double) * n), *q = malloc(sizeof(double) * n);
+  for (int i = 0; i < n; ++i) {
+    double d = 1.0;
+    for (int k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+      if (col_idx[k] == i) d = a_val[k];
+    dinv[i] = 1.0 / d;
+    x[i] = 0.0;
+    r[i] = b[i];
+    z[i] = dinv[i] * r[i];
+    pv[i] = z[i];
+  }
+  double rz = dot(n, r, z);
+  const double n0 = precond_norm ? sqrt(dot(n, z, z)) : sqrt(dot(n, r, r));
+  int it = 0;
+  double res = n0 > 0 ? 1.0 : 0.0;
+  if (n0 == 0.0) goto done;
+  for (it = 1; it <= max_iter; ++it) {
+    cepo_spmv(n, row_ptr, col_idx, a_val, pv, q);
+    const double alpha = rz / dot(n, pv, q);
+    for (int i = 0; i < n; ++i) {
+      x[i] += alpha * pv[i];
+      r[i] -= alpha * q[i];
+      z[i] = dinv[i] * r[i];
+    }
+    const double rz_new = dot(n, r, z);
+    const double nr = precond_norm ? sqrt(dot(n, z, z)) : sqrt(dot(n, r, r));
+    res = nr / n0;
+    if (nr <= rtol * n0) break;
+    const double beta = rz_new / rz;
+    rz = rz_new;
+    for (int i = 0; i < n; ++i) pv[i] = z[i] + beta * pv[i];
+  }
+done:
+  if (rel_res) *rel_res = res;
+  free(dinv); free(r); free(z); free(pv); free(q);
+  return it > max_iter ? -max_iter : it;
+}
+
+int cepo_pcg(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b, double *x,
+             double rtol, int max_iter, double *rel_res) {
+  return cepo_pcg2(n, row_ptr, col_idx, a_val, b, x, rtol, max_iter, 1, rel_res);
+}
+
+/* Tissue: Godunov split of heart.cpp:127-165 / 274-430 on a structured grid.
+ * Per step: every node's ionic update (cepo_step with the tissue stimulus
+ * flag) at time t, then A V = B V* / dt by PCG. The S1 region is stimulated
+ * while iia*bcl + t_crt < t < iia*bcl + t_crt + dur for pace iia < n_pace
+ * (the "square" mesh rule, heart.cpp:309-323). Returns total CG iterations;
+ * V (n) receives the final potential, iters_out (n_steps, may be NULL) the
+ * iterations per step. */
+long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+                     long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                     double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                     const double *celltype, double *V, int *iters_out) {
+  if (dim == 2) nz = 1;
+  const int n = nx * ny * nz;
+  const long nnz = cepo_fem_nnz(dim, nx, ny, nz);
+  int *rp = malloc(sizeof(int) * (n + 1)), *ci = malloc(sizeof(int) * nnz);
+  double *av = malloc(sizeof(double) * nnz), *bv = malloc(sizeof(double) * nnz);
+  cepo_fem_assemble(dim, nx, ny, nz, h, dt, D, n_d, rp, ci, av, bv);
+  const int ns = cepo_n_states(model);
+  cepo_cell *cells = malloc(sizeof(cepo_cell) * n);
+  double *y = malloc(sizeof(double) * (size_t)n * CEPO_MAX_STATES);
+  double *vs = malloc(sizeof(double) * n), *b = malloc(sizeof(double) * n);
+  for (int i = 0; i < n; ++i) {
+    cepo_init(&cells[i], model, celltype ? celltype[i] : 0.0, conc, hill, n_hill, 0, celltype ? 0 : 1);
+    cells[i].tissue_stim = 1;
+    cepo_init_states(&cells[i], y + (size_t)i * CEPO_MAX_STATES);
+  }
+  double t = 0.0;
+  long total = 0;
+  for (long st = 0; st < n_steps; ++st) {
+    const int iia = (int)(t / bcl);
+    const int on = iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt;
+    for (int i = 0; i < n; ++i) {
+      cells[i].is_s1 = on && s1[i];
+      cepo_step(&cells[i], t, dt, y + (size_t)i * CEPO_MAX_STATES, NULL);
+      vs[i] = y[(size_t)i * CEPO_MAX_STATES];
+    }
+    cepo_spmv(n, rp, ci, bv, vs, b);
+    for (int i = 0; i < n; ++i) b[i] /= dt;
+    double rr;
+    const int it = cepo_pcg2(n, rp, ci, av, b, vs, rtol, 10000, precond_norm, &rr);
+    total += it < 0 ? -it : it;
+    if (iters_out) iters_out[st] = it;
+    for (int i = 0; i < n; ++i) y[(size_t)i * CEPO_MAX_STATES] = vs[i];
+    t += dt;
+  }
+  (void)ns;
+  for (int i = 0; i < n; ++i) V[i] = y[(size_t)i * CEPO_MAX_STATES];
+  free(rp); free(ci); free(av); free(bv); free(cells); free(y); free(vs); free(b);
+  return total;
+}
