@@ -47,6 +47,7 @@ class CepError(RuntimeError):
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
 _lib = None
 
 # Every symbol include/cep_b200.h declares, with its ctypes signature.
@@ -78,6 +79,33 @@ _SIGS = {
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
     "cep_qinward": (ctypes.c_double, [ctypes.POINTER(Biomarkers), ctypes.POINTER(Biomarkers)]),
+    "cep_fem_create_grid": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_fem_create_csr": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, _dp, ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_fem_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_fem_info": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_long), _ip, _ip]),
+    "cep_fem_set_format": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cep_fem_get_csr": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _dp, _dp]),
+    "cep_fem_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "cep_fem_spmv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp]),
+    "cep_fem_solve": (ctypes.c_int, [ctypes.c_void_p, _dp, _ip, _dp]),
+    "cep_fem_solve_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cep_fem_stats": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_long),
+                                     ctypes.POINTER(ctypes.c_long), _ip, _dp]),
+    "cep_tissue_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_tissue_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_tissue_set_stimulus": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "cep_tissue_set_activation_threshold": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "cep_tissue_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    "cep_tissue_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_tissue_get_v": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "cep_tissue_get_activation": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "cep_tissue_stats": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_long),
+                                        ctypes.POINTER(ctypes.c_long), _ip]),
 }
 
 
@@ -247,3 +275,168 @@ class Batch:
 
 def qinward(control: Biomarkers, drug: Biomarkers) -> float:
     return float(lib().cep_qinward(ctypes.byref(control), ctypes.byref(drug)))
+
+
+FEM_AUTO, FEM_CSR, FEM_ELL = -1, 0, 1
+
+
+def _iptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+class Fem:
+    """Monodomain diffusion operator A = M/dt + D K, B = M on the GPU with its
+    Jacobi-PCG solver (Cfem, fem.cpp)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+        n = ctypes.c_int()
+        nnz = ctypes.c_long()
+        fmt = ctypes.c_int()
+        w = ctypes.c_int()
+        _check(lib().cep_fem_info(self._h, ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(fmt), ctypes.byref(w)))
+        self.n, self.nnz, self.ell_width = n.value, nnz.value, w.value
+
+    @classmethod
+    def grid(cls, dim: int, nx: int, ny: int, nz: int, h: float, dt: float, D, fmt: int = FEM_ELL,
+             stream: int | None = None) -> "Fem":
+        """D: scalar, per-element array [n_elem] or [n_elem, 3|6] tensors."""
+        n_elem = (nx - 1) * (ny - 1) * ((nz - 1) if dim == 3 else 1)
+        d = np.asarray(D, np.float64)
+        if d.ndim == 0:
+            d = np.full((n_elem, 1), float(d))
+        elif d.ndim == 1:
+            d = d.reshape(n_elem, 1)
+        d = np.ascontiguousarray(d)
+        hnd = ctypes.c_void_p()
+        _check(lib().cep_fem_create_grid(dim, nx, ny, nz, h, dt, _dptr(d), d.shape[1], fmt, stream,
+                                         ctypes.byref(hnd)))
+        return cls(hnd)
+
+    @classmethod
+    def csr(cls, row_ptr, col_idx, a_val, b_val, dt: float, fmt: int = FEM_ELL, stream: int | None = None) -> "Fem":
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_idx, np.int32)
+        av = np.ascontiguousarray(a_val, np.float64)
+        bv = np.ascontiguousarray(b_val, np.float64)
+        hnd = ctypes.c_void_p()
+        _check(lib().cep_fem_create_csr(len(rp) - 1, _iptr(rp), _iptr(ci), _dptr(av), _dptr(bv), dt, fmt, stream,
+                                        ctypes.byref(hnd)))
+        return cls(hnd)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cep_fem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def format(self) -> int:
+        fmt = ctypes.c_int()
+        _check(lib().cep_fem_info(self._h, None, None, ctypes.byref(fmt), None))
+        return fmt.value
+
+    def set_format(self, fmt: int) -> "Fem":
+        _check(lib().cep_fem_set_format(self._h, fmt))
+        return self
+
+    def get_csr(self):
+        rp = np.zeros(self.n + 1, np.int32)
+        ci = np.zeros(self.nnz, np.int32)
+        av = np.zeros(self.nnz)
+        bv = np.zeros(self.nnz)
+        _check(lib().cep_fem_get_csr(self._h, _iptr(rp), _iptr(ci), _dptr(av), _dptr(bv)))
+        return rp, ci, av, bv
+
+    def set_solver(self, rtol: float = 1e-5, max_iter: int = 10000, precond_norm: bool = True) -> "Fem":
+        _check(lib().cep_fem_set_solver(self._h, rtol, max_iter, int(precond_norm)))
+        return self
+
+    def spmv(self, x, which: str = "A") -> np.ndarray:
+        xx = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.n)
+        _check(lib().cep_fem_spmv(self._h, {"A": 0, "B": 1}[which], _dptr(xx), _dptr(y)))
+        return y
+
+    def solve(self, v) -> tuple[np.ndarray, int, float]:
+        """One implicit step: returns (V, iterations, relative residual)."""
+        vv = np.array(v, np.float64)
+        it = ctypes.c_int()
+        res = ctypes.c_double()
+        _check(lib().cep_fem_solve(self._h, _dptr(vv), ctypes.byref(it), ctypes.byref(res)))
+        return vv, it.value, res.value
+
+    def stats(self) -> dict:
+        li, nc = ctypes.c_int(), ctypes.c_int()
+        tot, ns = ctypes.c_long(), ctypes.c_long()
+        res = ctypes.c_double()
+        _check(lib().cep_fem_stats(self._h, ctypes.byref(li), ctypes.byref(tot), ctypes.byref(ns), ctypes.byref(nc),
+                                   ctypes.byref(res)))
+        return {"last_iters": li.value, "total_iters": tot.value, "solves": ns.value, "not_converged": nc.value,
+                "last_res": res.value}
+
+
+class Tissue:
+    """Godunov-split monodomain tissue: a Batch (one instance per node) and a
+    Fem operator sharing one stream (Cheart, heart.cpp)."""
+
+    def __init__(self, cells: Batch, fem: Fem, dt: float):
+        self.cells, self.fem = cells, fem
+        self.n = fem.n
+        h = ctypes.c_void_p()
+        _check(lib().cep_tissue_create(cells._h, fem._h, dt, ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cep_tissue_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stimulus(self, mask, bcl: float, t_crt: float, dur: float, n_pace: int) -> "Tissue":
+        m = np.ascontiguousarray(mask, np.uint8)
+        _check(lib().cep_tissue_set_stimulus(self._h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt,
+                                             dur, n_pace))
+        return self
+
+    def set_activation_threshold(self, vm: float) -> "Tissue":
+        _check(lib().cep_tissue_set_activation_threshold(self._h, vm))
+        return self
+
+    def run(self, n_steps: int) -> "Tissue":
+        _check(lib().cep_tissue_run(self._h, int(n_steps)))
+        return self
+
+    def sync(self) -> "Tissue":
+        _check(lib().cep_tissue_sync(self._h))
+        return self
+
+    def v(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        _check(lib().cep_tissue_get_v(self._h, _dptr(out)))
+        return out
+
+    def activation(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        _check(lib().cep_tissue_get_activation(self._h, _dptr(out)))
+        return out
+
+    def stats(self) -> dict:
+        t = ctypes.c_double()
+        st, it = ctypes.c_long(), ctypes.c_long()
+        nc = ctypes.c_int()
+        _check(lib().cep_tissue_stats(self._h, ctypes.byref(t), ctypes.byref(st), ctypes.byref(it), ctypes.byref(nc)))
+        return {"time": t.value, "steps": st.value, "cg_iters": it.value, "not_converged": nc.value}

@@ -28,6 +28,11 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--prec-d
               "--prec-sqrt=false", "--ftz=true", "-Xptxas", "-v", "-I", str(PKG.parent / "include")]
 
 
+# Per-file additions: the grid assembly is compiled without FMA contraction
+# so every matrix entry is the same IEEE expression as a scalar assembly.
+FILE_FLAGS = {"fem_assembly.cu": ["-fmad=false"]}
+
+
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
         if cand and Path(cand).exists():
@@ -57,7 +62,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if not force and not _stale(obj, src):
             continue
         if src.suffix == ".cu":
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
         else:
             cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(PKG.parent / "include"),
                    "-c", str(src), "-o", str(obj)]

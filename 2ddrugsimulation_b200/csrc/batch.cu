@@ -234,8 +234,8 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
   int iout = a.iout[i];
   const bm::Sched sc{a.sched[i], a.sched[a.ld + i], a.sched[2 * a.ld + i], a.sched[3 * a.ld + i]};
   const bool bm_on = a.bm_on && sc.first_pace >= 0;
-  int cnt_print = sc.print_freq > 0 ? sc.print_freq - (iout % sc.print_freq) : 0x7fffffff;
-  int cnt_bcl = sc.steps_per_bcl > 0 ? sc.steps_per_bcl - (iout % sc.steps_per_bcl) : 0x7fffffff;
+  int cnt_print = bm::countdown(iout, sc.print_freq);
+  int cnt_bcl = bm::countdown(iout, sc.steps_per_bcl);
   const double bcl = a.par[M::p_bcl() * a.ld + i];
   const double stim_start = a.par[M::p_stim_start() * a.ld + i];
   typename M::template Cur<G> c;
@@ -293,8 +293,8 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   int iout = a.iout[il];
   const bm::Sched sc{a.sched[il], a.sched[a.ld + il], a.sched[2 * a.ld + il], a.sched[3 * a.ld + il]};
   const bool bm_on = R == 0 && a.bm_on && sc.first_pace >= 0;
-  int cnt_print = sc.print_freq > 0 ? sc.print_freq - (iout % sc.print_freq) : 0x7fffffff;
-  int cnt_bcl = sc.steps_per_bcl > 0 ? sc.steps_per_bcl - (iout % sc.steps_per_bcl) : 0x7fffffff;
+  int cnt_print = bm::countdown(iout, sc.print_freq);
+  int cnt_bcl = bm::countdown(iout, sc.steps_per_bcl);
   const double bcl = a.par[M::p_bcl() * a.ld + il];
   const double stim_start = a.par[M::p_stim_start() * a.ld + il];
   typename M::template Cur<G> c;
@@ -858,6 +858,26 @@ int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, d
   a.s1_mask = d_mask;
   a.s1_bcl = bcl; a.s1_tcrt = t_crt; a.s1_dur = dur; a.s1_npace = n_pace;
   return model_info(b->model)->run(b, a);
+}
+
+int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {
+  if (!b || !b->initialized) return fail(CEP_ERR_STATE, "tissue batch not initialised");
+  if (!(dt > 0)) return fail(CEP_ERR_ARG, "dt must be positive");
+  b->dt = dt; b->n_pace = 1; b->first_pace = -1; b->dt_write = 1.0; b->qnet_thr = -1e300;
+  std::vector<int> sc((size_t)4 * b->ld, 0);
+  for (int i = 0; i < b->n; ++i) {
+    sc[i] = 0x7fffffff;             // no protocol end
+    sc[b->ld + i] = 0x7fffffff;     // no beat boundary
+    sc[3 * b->ld + i] = -1;         // biomarkers off
+  }
+  CEP_CUDA(cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  b->has_protocol = true;
+  RunArgs a = make_args(b, 0);
+  a.bm_on = 0;
+  int rc = model_info(b->model)->reset(b, a);
+  if (rc) return rc;
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
 }
 
 double *cep_internal_batch_v(cep_batch_t b) { return b ? b->states : nullptr; }

@@ -76,6 +76,15 @@ __device__ __forceinline__ void beat_copy(const View &v, int64_t i, int dst, int
 __device__ __forceinline__ int peak_step(double bcl, int pace, double stim_start, double dt) {
   return (int)(((bcl * pace) + (stim_start + 6.)) / dt);
 }
+// Count-down for "iout % x == 0" tests: the number of sample calls, counting
+// the first one, until the next multiple of x. A launch that starts at iout0
+// makes its first sample call at max(iout0, 1) (sample 0 is the initial
+// state, which the reference never evaluates).
+__device__ __forceinline__ int countdown(int iout0, int x) {
+  if (x <= 0) return 0x7fffffff;
+  const int first = iout0 < 1 ? 1 : iout0;
+  return (x - first % x) % x + 1;
+}
 __device__ __forceinline__ int next_multiple(int iout, int x) {
   if (x <= 0) return 0x7fffffff;
   const int r = iout % x;

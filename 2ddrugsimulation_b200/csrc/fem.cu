@@ -1,0 +1,846 @@
+// Monodomain diffusion solve and the tissue driver: the cep_fem_* and
+// cep_tissue_* C ABI (include/cep_b200.h).
+//
+// Replaces Cfem::solve_Bmat (fem.cpp:705-718) with PETSc KSPCG + PCJACOBI
+// (fem.cpp:753-760) and the Godunov loop of Cheart::processing
+// (heart.cpp:127-165, 274-430).
+//
+// One solve is ONE cooperative persistent launch:
+//   phase 0   b = B V* / dt (the RHS build fused with the first residual),
+//             r = b, z = D^-1 r, p = z, partial sums of r.z and |z|^2
+//   per CG iteration (two grid barriers):
+//     A   p_k = z + beta p_{k-1} evaluated on the fly inside the SpMV,
+//         q = A p_k, partial p.q                             -> barrier
+//     B   x += alpha p, r -= alpha q, z = D^-1 r, partial r.z and |z|^2
+//                                                             -> barrier
+// Dots are FP64 and deterministic: every block writes one partial per
+// reduction and every block sums all partials in the same fixed order, so
+// each block holds bit-identical scalars and takes the same branch. x is
+// written straight into the caller's V vector (x0 = 0 is implicit), so the
+// solve works in place on the ionic state's V row.
+//
+// HBM layout of an operator with n rows (ld = n rounded up to 32):
+//   CSR    row_ptr[n+1] i32, col[nnz] i32, a[nnz] f64, b[nnz] f64
+//   ELL    col[width][ld] i32, a[width][ld] f64, b[width][ld] f64 (padding
+//          entries point at the row itself with weight 0)
+//   dinv[ld], r, z, p0, p1, q [ld] f64 each; partials [3][grid] f64
+//
+// The grid barrier spins with an iteration limit; a barrier that runs out
+// sets an error word, every block leaves at its next barrier, and the host
+// reports CEP_ERR_TIMEOUT.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cep_b200.h"
+#include "internal.h"
+
+extern "C" int cep_internal_fem_assemble_grid(int dim, int nx, int ny, int nz, double h, double dt, const double *d_D,
+                                              int n_d, const int *d_rp, int *d_col, double *d_a, double *d_b,
+                                              int width, int64_t ld, int *d_ecol, double *d_ea, double *d_eb,
+                                              double *d_dinv, void *stream);
+
+namespace {
+
+#define FEM_CUDA(call)                                                                                   \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) {                                                                             \
+      std::string m_ = std::string(#call) + ": " + cudaGetErrorString(e_);                               \
+      return cep_internal_set_fail(CEP_ERR_CUDA, m_.c_str());                                            \
+    }                                                                                                    \
+  } while (0)
+
+int fail_msg(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return cep_internal_set_fail(code, buf);
+}
+
+constexpr int kPcgBlock = 512;
+constexpr long kSpinLimit = 1L << 24;  // x ~64-128 ns sleeps: about a second or two
+
+}  // namespace
+
+namespace cep {
+namespace fem {
+
+struct Status {
+  int last_iters;           // iterations of the last solve (negative: hit max_iter)
+  int not_converged;        // solves that hit max_iter
+  long long total_iters;    // over all solves
+  long long solves;
+  double last_res;          // relative residual of the last solve
+};
+
+struct Ctl {
+  unsigned count, gen;  // grid barrier
+  int err;              // barrier timeout
+  int pad;
+};
+
+struct CsrView {
+  const int *rp, *col;
+  const double *a, *b;
+  template <class X>
+  __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
+    double s = 0.0;
+    const int e = rp[i + 1];
+    for (int k = rp[i]; k < e; ++k) s = fma(val[k], x(col[k]), s);
+    return s;
+  }
+};
+
+struct EllView {
+  const int *col;
+  const double *a, *b;
+  int width;
+  int64_t ld;
+  template <class X>
+  __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
+    double s = 0.0;
+#pragma unroll 9
+    for (int k = 0; k < width; ++k) s = fma(val[k * ld + i], x(col[k * ld + i]), s);
+    return s;
+  }
+};
+
+struct PcgArgs {
+  int64_t n;
+  double dt, rtol;
+  int max_iter, precond_norm;
+  double *v;  // in: V*, out: V
+  const double *dinv;
+  double *r, *z, *p0, *p1, *q;
+  double *part;  // [3][gridDim.x]
+  Ctl *ctl;
+  Status *st;
+  double *tact;  // activation times (may be null)
+  double t_new, act_thr;
+};
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
+__device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
+
+// Grid-wide barrier over co-resident blocks (cooperative launch), bounded.
+__device__ __forceinline__ bool grid_sync(Ctl *ctl) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_volatile(&ctl->gen);
+    __threadfence();
+    if (atomicAdd(&ctl->count, 1u) == gridDim.x - 1) {
+      atomicExch(&ctl->count, 0u);
+      __threadfence();
+      atomicAdd(&ctl->gen, 1u);
+    } else {
+      long spins = 0;
+      while (ld_volatile(&ctl->gen) == gen) {
+        if (++spins > kSpinLimit) {
+          atomicExch(&ctl->err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (ld_volatile(&ctl->err)) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Fixed-order block reduction of two values; thread 0 gets the sums.
+__device__ __forceinline__ void block_sum2(double &x, double &y) {
+  __shared__ double sx[kPcgBlock / 32], sy[kPcgBlock / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_down_sync(0xffffffffu, x, o);
+    y += __shfl_down_sync(0xffffffffu, y, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sx[w] = x;
+    sy[w] = y;
+  }
+  __syncthreads();
+  if (w == 0) {
+    x = l < kPcgBlock / 32 ? sx[l] : 0.0;
+    y = l < kPcgBlock / 32 ? sy[l] : 0.0;
+    for (int o = 8; o > 0; o >>= 1) {
+      x += __shfl_down_sync(0xffffffffu, x, o);
+      y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+  }
+  __syncthreads();
+}
+
+// Sum of gridDim.x partials in a fixed order, identical in every block; the
+// result is broadcast to the whole block.
+__device__ __forceinline__ void grid_total2(const double *pa, const double *pb, double &a, double &b) {
+  __shared__ double s[2];
+  if (threadIdx.x < 32) {
+    double x = 0.0, y = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
+      x += __ldcg(pa + k);
+      if (pb) y += __ldcg(pb + k);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(0xffffffffu, x, o);
+      y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    if (threadIdx.x == 0) {
+      s[0] = x;
+      s[1] = y;
+    }
+  }
+  __syncthreads();
+  a = s[0];
+  b = s[1];
+  __syncthreads();
+}
+
+template <class M>
+__global__ void __launch_bounds__(kPcgBlock) pcg_kernel(M m, PcgArgs a) {
+  const int64_t stride = (int64_t)gridDim.x * kPcgBlock;
+  const int64_t i0 = (int64_t)blockIdx.x * kPcgBlock + threadIdx.x;
+  const int G = gridDim.x;
+  double *part0 = a.part, *part1 = a.part + G, *part2 = a.part + 2 * G;
+  const double *v_in = a.v;
+  // phase 0: RHS and first residual
+  double s0 = 0.0, s1 = 0.0;
+  for (int64_t i = i0; i < a.n; i += stride) {
+    const double bi = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
+    const double zi = a.dinv[i] * bi;
+    a.r[i] = bi;
+    a.z[i] = zi;
+    a.p0[i] = zi;
+    s0 = fma(bi, zi, s0);
+    s1 = a.precond_norm ? fma(zi, zi, s1) : fma(bi, bi, s1);
+  }
+  block_sum2(s0, s1);
+  if (threadIdx.x == 0) {
+    part0[blockIdx.x] = s0;
+    part1[blockIdx.x] = s1;
+  }
+  if (!grid_sync(a.ctl)) return;
+  double rz, nn0;
+  grid_total2(part0, part1, rz, nn0);
+  const double n0 = sqrt(nn0);
+  int it = 0;
+  double res = n0 > 0.0 ? 1.0 : 0.0;
+  bool conv = false;
+  if (n0 == 0.0) {
+    for (int64_t i = i0; i < a.n; i += stride) a.v[i] = 0.0;
+    conv = true;
+  } else {
+    double *pc = a.p0, *pn = a.p1;
+    double beta = 0.0;
+    for (it = 1; it <= a.max_iter; ++it) {
+      // A: p_k (on the fly) and q = A p_k
+      double spq = 0.0, unused = 0.0;
+      if (it == 1) {
+        for (int64_t i = i0; i < a.n; i += stride) {
+          const double qi = m.apply(m.a, i, [&](int j) { return pc[j]; });
+          a.q[i] = qi;
+          spq = fma(pc[i], qi, spq);
+        }
+      } else {
+        const double *zc = a.z;
+        for (int64_t i = i0; i < a.n; i += stride) {
+          const double qi = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
+          const double pi = fma(beta, pc[i], zc[i]);
+          pn[i] = pi;
+          a.q[i] = qi;
+          spq = fma(pi, qi, spq);
+        }
+      }
+      block_sum2(spq, unused);
+      if (threadIdx.x == 0) part2[blockIdx.x] = spq;
+      if (!grid_sync(a.ctl)) return;
+      double pq, dummy;
+      grid_total2(part2, nullptr, pq, dummy);
+      const double alpha = rz / pq;
+      if (it > 1) {
+        double *t = pc;
+        pc = pn;
+        pn = t;
+      }
+      // B: x, r, z
+      double srz = 0.0, snr = 0.0;
+      for (int64_t i = i0; i < a.n; i += stride) {
+        const double pi = pc[i];
+        a.v[i] = it == 1 ? alpha * pi : fma(alpha, pi, a.v[i]);
+        const double ri = fma(-alpha, a.q[i], a.r[i]);
+        const double zi = a.dinv[i] * ri;
+        a.r[i] = ri;
+        a.z[i] = zi;
+        srz = fma(ri, zi, srz);
+        snr = a.precond_norm ? fma(zi, zi, snr) : fma(ri, ri, snr);
+      }
+      block_sum2(srz, snr);
+      if (threadIdx.x == 0) {
+        part0[blockIdx.x] = srz;
+        part1[blockIdx.x] = snr;
+      }
+      if (!grid_sync(a.ctl)) return;
+      double rz_new, nr2;
+      grid_total2(part0, part1, rz_new, nr2);
+      const double nr = sqrt(nr2);
+      res = nr / n0;
+      if (nr <= a.rtol * n0) {
+        conv = true;
+        break;
+      }
+      beta = rz_new / rz;
+      rz = rz_new;
+    }
+  }
+  if (a.tact)
+    for (int64_t i = i0; i < a.n; i += stride)
+      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = a.t_new;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int used = conv ? it : -a.max_iter;
+    a.st->last_iters = used;
+    a.st->last_res = res;
+    a.st->total_iters += conv ? it : a.max_iter;
+    a.st->solves += 1;
+    if (!conv) a.st->not_converged += 1;
+  }
+}
+
+// y = A x or B x (tests and the autotuner)
+template <class M>
+__global__ void spmv_kernel(M m, int which, int64_t n, const double *x, double *y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  y[i] = m.apply(which ? m.b : m.a, i, [&](int j) { return x[j]; });
+}
+
+__global__ void csr_to_ell_kernel(int64_t n, const int *rp, const int *col, const double *a, const double *b,
+                                  int width, int64_t ld, int *ecol, double *ea, double *eb, double *dinv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int slot = 0;
+  double diag = 1.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k, ++slot) {
+    ecol[slot * ld + i] = col[k];
+    ea[slot * ld + i] = a[k];
+    eb[slot * ld + i] = b[k];
+    if (col[k] == i) diag = a[k];
+  }
+  for (; slot < width; ++slot) {
+    ecol[slot * ld + i] = (int)i;
+    ea[slot * ld + i] = 0.0;
+    eb[slot * ld + i] = 0.0;
+  }
+  dinv[i] = 1.0 / diag;
+}
+
+}  // namespace fem
+}  // namespace cep
+
+using namespace cep::fem;
+
+struct cep_fem {
+  int n = 0;
+  int64_t ld = 0, nnz = 0;
+  int width = 0, format = CEP_FEM_ELL;
+  double dt = 0.0;
+  cudaStream_t stream = nullptr;
+  int *rp = nullptr, *col = nullptr, *ecol = nullptr;
+  double *a = nullptr, *b = nullptr, *ea = nullptr, *eb = nullptr, *dinv = nullptr;
+  double *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr;
+  Ctl *ctl = nullptr;
+  Status *st = nullptr;
+  int grid = 0;
+  double rtol = 1e-5;  // PETSc's default KSP rtol (the reference sets none)
+  int max_iter = 10000;
+  int precond_norm = 1;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+template <class T>
+int fem_alloc(cep_fem *f, T **p, size_t count) {
+  void *q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
+  if (e != cudaSuccess) return fail_msg(CEP_ERR_OOM, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+  f->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return CEP_OK;
+}
+
+void fem_free(cep_fem *f) {
+  for (void *p : f->allocs) cudaFree(p);
+  delete f;
+}
+
+CsrView csr_view(const cep_fem *f) { return CsrView{f->rp, f->col, f->a, f->b}; }
+EllView ell_view(const cep_fem *f) { return EllView{f->ecol, f->ea, f->eb, f->width, f->ld}; }
+
+// Buffers shared by both formats, the cooperative grid size, and zeroed
+// control words.
+int fem_finish_setup(cep_fem *f) {
+  int rc;
+  const size_t ld = (size_t)f->ld;
+  if ((rc = fem_alloc(f, &f->r, ld)) || (rc = fem_alloc(f, &f->z, ld)) || (rc = fem_alloc(f, &f->p0, ld)) ||
+      (rc = fem_alloc(f, &f->p1, ld)) || (rc = fem_alloc(f, &f->q, ld)))
+    return rc;
+  int dev = 0, sms = 0, per_sm_csr = 0, per_sm_ell = 0;
+  FEM_CUDA(cudaGetDevice(&dev));
+  FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_csr, pcg_kernel<CsrView>, kPcgBlock, 0));
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ell, pcg_kernel<EllView>, kPcgBlock, 0));
+  const int per_sm = std::max(1, std::min(per_sm_csr, per_sm_ell));
+  const int64_t need = (f->n + kPcgBlock - 1) / kPcgBlock;
+  f->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, need));
+  if ((rc = fem_alloc(f, &f->part, (size_t)3 * f->grid)) || (rc = fem_alloc(f, &f->ctl, 1)) ||
+      (rc = fem_alloc(f, &f->st, 1)))
+    return rc;
+  FEM_CUDA(cudaMemsetAsync(f->ctl, 0, sizeof(Ctl), f->stream));
+  FEM_CUDA(cudaMemsetAsync(f->st, 0, sizeof(Status), f->stream));
+  FEM_CUDA(cudaStreamSynchronize(f->stream));
+  return CEP_OK;
+}
+
+template <class M>
+int launch_pcg(cep_fem *f, const M &m, double *v, double *tact, double t_new, double thr) {
+  PcgArgs a;
+  a.n = f->n;
+  a.dt = f->dt;
+  a.rtol = f->rtol;
+  a.max_iter = f->max_iter;
+  a.precond_norm = f->precond_norm;
+  a.v = v;
+  a.dinv = f->dinv;
+  a.r = f->r; a.z = f->z; a.p0 = f->p0; a.p1 = f->p1; a.q = f->q;
+  a.part = f->part;
+  a.ctl = f->ctl;
+  a.st = f->st;
+  a.tact = tact;
+  a.t_new = t_new;
+  a.act_thr = thr;
+  M mm = m;
+  void *args[] = {&mm, &a};
+  FEM_CUDA(cudaMemsetAsync(f->ctl, 0, sizeof(Ctl), f->stream));
+  FEM_CUDA(cudaLaunchCooperativeKernel((const void *)pcg_kernel<M>, dim3(f->grid), dim3(kPcgBlock), args, 0,
+                                       f->stream));
+  return CEP_OK;
+}
+
+int fem_solve_async(cep_fem *f, double *d_v, double *tact, double t_new, double thr) {
+  if (f->format == CEP_FEM_CSR) return launch_pcg(f, csr_view(f), d_v, tact, t_new, thr);
+  return launch_pcg(f, ell_view(f), d_v, tact, t_new, thr);
+}
+
+int fem_check_ctl(cep_fem *f) {
+  Ctl c;
+  FEM_CUDA(cudaMemcpyAsync(&c, f->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, f->stream));
+  FEM_CUDA(cudaStreamSynchronize(f->stream));
+  if (c.err) return fail_msg(CEP_ERR_TIMEOUT, "PCG grid barrier ran out of its spin limit");
+  return CEP_OK;
+}
+
+// CSR vs ELL: time a few SpMVs of each and keep the faster.
+int fem_autotune(cep_fem *f) {
+  cudaEvent_t e0, e1;
+  FEM_CUDA(cudaEventCreate(&e0));
+  FEM_CUDA(cudaEventCreate(&e1));
+  const int block = 256;
+  const unsigned grid = (unsigned)((f->n + block - 1) / block);
+  float best = 1e30f;
+  int best_fmt = CEP_FEM_ELL;
+  for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL}) {
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(e0, f->stream);
+      for (int k = 0; k < 10; ++k) {
+        if (fmt == CEP_FEM_CSR)
+          spmv_kernel<<<grid, block, 0, f->stream>>>(csr_view(f), 0, (int64_t)f->n, f->p0, f->q);
+        else
+          spmv_kernel<<<grid, block, 0, f->stream>>>(ell_view(f), 0, (int64_t)f->n, f->p0, f->q);
+      }
+      cudaEventRecord(e1, f->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep == 1 && ms < best) {
+        best = ms;
+        best_fmt = fmt;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  FEM_CUDA(cudaGetLastError());
+  f->format = best_fmt;
+  return CEP_OK;
+}
+
+int fem_set_format(cep_fem *f, int format) {
+  if (format == CEP_FEM_AUTO) {
+    FEM_CUDA(cudaMemsetAsync(f->p0, 0, sizeof(double) * f->ld, f->stream));
+    return fem_autotune(f);
+  }
+  if (format != CEP_FEM_CSR && format != CEP_FEM_ELL) return fail_msg(CEP_ERR_ARG, "unknown sparse format %d", format);
+  f->format = format;
+  return CEP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- tissue
+struct cep_tissue {
+  cep_batch_t cells = nullptr;
+  cep_fem_t fem = nullptr;
+  cudaStream_t stream = nullptr;
+  int n = 0;
+  unsigned char *mask = nullptr;
+  double bcl = 1000.0, t_crt = 0.0, dur = 0.0;
+  int n_pace = 0;
+  double *tact = nullptr;
+  double act_thr = -30.0;
+  double dt = 0.01, t = 0.0;
+  long steps = 0;
+};
+
+extern "C" {
+
+int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, const double *D, int n_d, int format,
+                        void *stream, cep_fem_t *out) {
+  if (!out || !D) return fail_msg(CEP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (dim != 2 && dim != 3) return fail_msg(CEP_ERR_ARG, "dim must be 2 or 3 (got %d)", dim);
+  if (dim == 2) nz = 1;
+  if (nx < 2 || ny < 2 || (dim == 3 && nz < 2)) return fail_msg(CEP_ERR_ARG, "grid needs >= 2 nodes per axis");
+  if (!(h > 0) || !(dt > 0)) return fail_msg(CEP_ERR_ARG, "h and dt must be positive");
+  const int full = dim == 2 ? 3 : 6;
+  if (n_d != 1 && n_d != full) return fail_msg(CEP_ERR_ARG, "n_d must be 1 or %d for dim %d", full, dim);
+  const int64_t n = (int64_t)nx * ny * nz;
+  if (n > 0x7fffffffLL / 27) return fail_msg(CEP_ERR_ARG, "grid too large for 32-bit column indices");
+  const int64_t n_elem = (int64_t)(nx - 1) * (ny - 1) * (dim == 3 ? nz - 1 : 1);
+  for (int64_t e = 0; e < n_elem * n_d; ++e)
+    if (!std::isfinite(D[e])) return fail_msg(CEP_ERR_ARG, "D[%lld] is not finite", (long long)e);
+  cep_fem *f = new cep_fem;
+  f->n = (int)n;
+  f->ld = (n + 31) / 32 * 32;
+  f->dt = dt;
+  f->stream = (cudaStream_t)stream;
+  f->width = dim == 2 ? 9 : 27;
+  // row pointers: neighbours per axis are 1 + (i > 0) + (i < n-1)
+  std::vector<int> rp(n + 1);
+  int64_t p = 0;
+  auto cnt = [](int i, int m) { return 1 + (i > 0) + (i < m - 1); };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        rp[(size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)] = (int)p;
+        p += (int64_t)cnt(i, nx) * cnt(j, ny) * (dim == 3 ? cnt(k, nz) : 1);
+      }
+  rp[n] = (int)p;
+  f->nnz = p;
+  int rc;
+  double *d_D = nullptr;
+  if ((rc = fem_alloc(f, &f->rp, (size_t)n + 1)) || (rc = fem_alloc(f, &f->col, (size_t)p)) ||
+      (rc = fem_alloc(f, &f->a, (size_t)p)) || (rc = fem_alloc(f, &f->b, (size_t)p)) ||
+      (rc = fem_alloc(f, &f->ecol, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->ea, (size_t)f->width * f->ld)) ||
+      (rc = fem_alloc(f, &f->eb, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->dinv, (size_t)f->ld))) {
+    fem_free(f);
+    return rc;
+  }
+  if (cudaMalloc(&d_D, sizeof(double) * n_elem * n_d) != cudaSuccess) {
+    fem_free(f);
+    return fail_msg(CEP_ERR_OOM, "cudaMalloc for the conductivity field failed");
+  }
+  cudaError_t e = cudaMemcpyAsync(f->rp, rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_D, D, sizeof(double) * n_elem * n_d, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess && cep_internal_fem_assemble_grid(dim, nx, ny, nz, h, dt, d_D, n_d, f->rp, f->col, f->a, f->b,
+                                                        f->width, f->ld, f->ecol, f->ea, f->eb, f->dinv, f->stream))
+    e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  cudaFree(d_D);
+  if (e != cudaSuccess) {
+    fem_free(f);
+    return fail_msg(CEP_ERR_CUDA, "grid assembly failed: %s", cudaGetErrorString(e));
+  }
+  if ((rc = fem_finish_setup(f)) || (rc = fem_set_format(f, format))) {
+    fem_free(f);
+    return rc;
+  }
+  *out = f;
+  return CEP_OK;
+}
+
+int cep_fem_create_csr(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b_val,
+                       double dt, int format, void *stream, cep_fem_t *out) {
+  if (!out || !row_ptr || !col_idx || !a_val || !b_val) return fail_msg(CEP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (n <= 0 || !(dt > 0)) return fail_msg(CEP_ERR_ARG, "n and dt must be positive");
+  if (row_ptr[0] != 0) return fail_msg(CEP_ERR_ARG, "row_ptr[0] must be 0");
+  int width = 0;
+  for (int i = 0; i < n; ++i) {
+    if (row_ptr[i + 1] < row_ptr[i]) return fail_msg(CEP_ERR_ARG, "row_ptr is not monotone at row %d", i);
+    width = std::max(width, row_ptr[i + 1] - row_ptr[i]);
+  }
+  const int64_t nnz = row_ptr[n];
+  for (int64_t k = 0; k < nnz; ++k) {
+    if (col_idx[k] < 0 || col_idx[k] >= n) return fail_msg(CEP_ERR_ARG, "col_idx[%lld] = %d out of range", (long long)k, col_idx[k]);
+    if (!std::isfinite(a_val[k]) || !std::isfinite(b_val[k])) return fail_msg(CEP_ERR_ARG, "matrix entry %lld is not finite", (long long)k);
+  }
+  cep_fem *f = new cep_fem;
+  f->n = n;
+  f->ld = ((int64_t)n + 31) / 32 * 32;
+  f->nnz = nnz;
+  f->dt = dt;
+  f->width = std::max(width, 1);
+  f->stream = (cudaStream_t)stream;
+  int rc;
+  if ((rc = fem_alloc(f, &f->rp, (size_t)n + 1)) || (rc = fem_alloc(f, &f->col, (size_t)std::max<int64_t>(nnz, 1))) ||
+      (rc = fem_alloc(f, &f->a, (size_t)std::max<int64_t>(nnz, 1))) || (rc = fem_alloc(f, &f->b, (size_t)std::max<int64_t>(nnz, 1))) ||
+      (rc = fem_alloc(f, &f->ecol, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->ea, (size_t)f->width * f->ld)) ||
+      (rc = fem_alloc(f, &f->eb, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->dinv, (size_t)f->ld))) {
+    fem_free(f);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(f->rp, row_ptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->col, col_idx, sizeof(int) * nnz, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->a, a_val, sizeof(double) * nnz, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->b, b_val, sizeof(double) * nnz, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) {
+    csr_to_ell_kernel<<<(n + 127) / 128, 128, 0, f->stream>>>(n, f->rp, f->col, f->a, f->b, f->width, f->ld, f->ecol,
+                                                              f->ea, f->eb, f->dinv);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+  if (e != cudaSuccess) {
+    fem_free(f);
+    return fail_msg(CEP_ERR_CUDA, "CSR upload failed: %s", cudaGetErrorString(e));
+  }
+  if ((rc = fem_finish_setup(f)) || (rc = fem_set_format(f, format))) {
+    fem_free(f);
+    return rc;
+  }
+  *out = f;
+  return CEP_OK;
+}
+
+int cep_fem_destroy(cep_fem_t f) {
+  if (!f) return CEP_OK;
+  cudaStreamSynchronize(f->stream);
+  fem_free(f);
+  return CEP_OK;
+}
+
+int cep_fem_info(cep_fem_t f, int *n, long *nnz, int *format, int *ell_width) {
+  if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
+  if (n) *n = f->n;
+  if (nnz) *nnz = (long)f->nnz;
+  if (format) *format = f->format;
+  if (ell_width) *ell_width = f->width;
+  return CEP_OK;
+}
+
+int cep_fem_set_format(cep_fem_t f, int format) {
+  if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
+  return fem_set_format(f, format);
+}
+
+int cep_fem_get_csr(cep_fem_t f, int *row_ptr, int *col_idx, double *a_val, double *b_val) {
+  if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
+  if (row_ptr) FEM_CUDA(cudaMemcpyAsync(row_ptr, f->rp, sizeof(int) * (f->n + 1), cudaMemcpyDeviceToHost, f->stream));
+  if (col_idx) FEM_CUDA(cudaMemcpyAsync(col_idx, f->col, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, f->stream));
+  if (a_val) FEM_CUDA(cudaMemcpyAsync(a_val, f->a, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, f->stream));
+  if (b_val) FEM_CUDA(cudaMemcpyAsync(b_val, f->b, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, f->stream));
+  FEM_CUDA(cudaStreamSynchronize(f->stream));
+  return CEP_OK;
+}
+
+int cep_fem_set_solver(cep_fem_t f, double rtol, int max_iter, int precond_norm) {
+  if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
+  if (!(rtol > 0) || max_iter <= 0) return fail_msg(CEP_ERR_ARG, "rtol and max_iter must be positive");
+  f->rtol = rtol;
+  f->max_iter = max_iter;
+  f->precond_norm = precond_norm ? 1 : 0;
+  return CEP_OK;
+}
+
+int cep_fem_spmv(cep_fem_t f, int which, const double *x, double *y) {
+  if (!f || !x || !y) return fail_msg(CEP_ERR_ARG, "null argument");
+  double *dx = f->q, *dy = f->r;  // scratch vectors of the solver
+  FEM_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * f->n, cudaMemcpyHostToDevice, f->stream));
+  const unsigned grid = (unsigned)((f->n + 255) / 256);
+  if (f->format == CEP_FEM_CSR)
+    spmv_kernel<<<grid, 256, 0, f->stream>>>(csr_view(f), which ? 1 : 0, (int64_t)f->n, dx, dy);
+  else
+    spmv_kernel<<<grid, 256, 0, f->stream>>>(ell_view(f), which ? 1 : 0, (int64_t)f->n, dx, dy);
+  FEM_CUDA(cudaGetLastError());
+  FEM_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * f->n, cudaMemcpyDeviceToHost, f->stream));
+  FEM_CUDA(cudaStreamSynchronize(f->stream));
+  return CEP_OK;
+}
+
+int cep_fem_solve_device(cep_fem_t f, void *d_v) {
+  if (!f || !d_v) return fail_msg(CEP_ERR_ARG, "null argument");
+  return fem_solve_async(f, (double *)d_v, nullptr, 0.0, 0.0);
+}
+
+int cep_fem_solve(cep_fem_t f, double *v, int *iters, double *rel_res) {
+  if (!f || !v) return fail_msg(CEP_ERR_ARG, "null argument");
+  double *dv = nullptr;
+  FEM_CUDA(cudaMallocAsync((void **)&dv, sizeof(double) * f->n, f->stream));
+  int rc = CEP_OK;
+  cudaError_t e = cudaMemcpyAsync(dv, v, sizeof(double) * f->n, cudaMemcpyHostToDevice, f->stream);
+  if (e == cudaSuccess) rc = fem_solve_async(f, dv, nullptr, 0.0, 0.0);
+  if (e == cudaSuccess && rc == CEP_OK) e = cudaMemcpyAsync(v, dv, sizeof(double) * f->n, cudaMemcpyDeviceToHost, f->stream);
+  cudaFreeAsync(dv, f->stream);
+  if (e != cudaSuccess) return fail_msg(CEP_ERR_CUDA, "solve transfer failed: %s", cudaGetErrorString(e));
+  if (rc) return rc;
+  if ((rc = fem_check_ctl(f))) return rc;
+  Status s;
+  FEM_CUDA(cudaMemcpy(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  if (iters) *iters = s.last_iters;
+  if (rel_res) *rel_res = s.last_res;
+  if (s.last_iters < 0) return fail_msg(CEP_ERR_NOT_CONVERGED, "PCG hit max_iter (%d), relative residual %g", f->max_iter, s.last_res);
+  return CEP_OK;
+}
+
+int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves, int *not_converged, double *last_res) {
+  if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
+  int rc;
+  if ((rc = fem_check_ctl(f))) return rc;
+  Status s;
+  FEM_CUDA(cudaMemcpy(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  if (last_iters) *last_iters = s.last_iters;
+  if (total_iters) *total_iters = (long)s.total_iters;
+  if (solves) *solves = (long)s.solves;
+  if (not_converged) *not_converged = s.not_converged;
+  if (last_res) *last_res = s.last_res;
+  return CEP_OK;
+}
+
+// ---------------------------------------------------------------- tissue
+int cep_tissue_create(cep_batch_t cells, cep_fem_t fem, double dt, cep_tissue_t *out) {
+  if (!cells || !fem || !out) return fail_msg(CEP_ERR_ARG, "null argument");
+  *out = nullptr;
+  int n = 0, ns = 0;
+  int rc = cep_batch_size(cells, &n, &ns);
+  if (rc) return rc;
+  if (n != fem->n) return fail_msg(CEP_ERR_ARG, "batch has %d instances, operator has %d rows", n, fem->n);
+  if (!(dt > 0) || std::fabs(dt - fem->dt) > 1e-12 * dt)
+    return fail_msg(CEP_ERR_ARG, "dt %g differs from the operator's dt %g", dt, fem->dt);
+  if ((cudaStream_t)cep_internal_batch_stream(cells) != fem->stream)
+    return fail_msg(CEP_ERR_ARG, "batch and operator must share one stream");
+  if ((rc = cep_internal_batch_tissue_begin(cells, dt))) return rc;
+  cep_tissue *t = new cep_tissue;
+  t->cells = cells;
+  t->fem = fem;
+  t->stream = fem->stream;
+  t->n = n;
+  t->dt = dt;
+  if (cudaMalloc((void **)&t->mask, (size_t)n) != cudaSuccess || cudaMalloc((void **)&t->tact, sizeof(double) * n) != cudaSuccess) {
+    cudaFree(t->mask);
+    delete t;
+    return fail_msg(CEP_ERR_OOM, "tissue buffers");
+  }
+  std::vector<double> neg(n, -1.0);
+  cudaMemsetAsync(t->mask, 0, (size_t)n, t->stream);
+  cudaMemcpyAsync(t->tact, neg.data(), sizeof(double) * n, cudaMemcpyHostToDevice, t->stream);
+  if (cudaStreamSynchronize(t->stream) != cudaSuccess) {
+    cudaFree(t->mask);
+    cudaFree(t->tact);
+    delete t;
+    return fail_msg(CEP_ERR_CUDA, "tissue set-up failed");
+  }
+  *out = t;
+  return CEP_OK;
+}
+
+int cep_tissue_destroy(cep_tissue_t t) {
+  if (!t) return CEP_OK;
+  cudaStreamSynchronize(t->stream);
+  cudaFree(t->mask);
+  cudaFree(t->tact);
+  delete t;
+  return CEP_OK;
+}
+
+int cep_tissue_set_stimulus(cep_tissue_t t, const unsigned char *s1_mask, double bcl, double t_crt, double dur,
+                            int n_pace) {
+  if (!t || !s1_mask) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (!(bcl > 0) || !(dur >= 0) || n_pace < 0) return fail_msg(CEP_ERR_ARG, "bad stimulus protocol");
+  FEM_CUDA(cudaMemcpyAsync(t->mask, s1_mask, (size_t)t->n, cudaMemcpyHostToDevice, t->stream));
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  t->bcl = bcl;
+  t->t_crt = t_crt;
+  t->dur = dur;
+  t->n_pace = n_pace;
+  return CEP_OK;
+}
+
+int cep_tissue_set_activation_threshold(cep_tissue_t t, double vm_threshold) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  t->act_thr = vm_threshold;
+  return CEP_OK;
+}
+
+int cep_tissue_run(cep_tissue_t t, long n_steps) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");
+  double *v = cep_internal_batch_v(t->cells);
+  for (long s = 0; s < n_steps; ++s) {
+    int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->bcl, t->t_crt, t->dur, t->n_pace, 1);
+    if (rc) return rc;
+    t->t += t->dt;
+    ++t->steps;
+    if ((rc = fem_solve_async(t->fem, v, t->tact, t->t, t->act_thr))) return rc;
+  }
+  return CEP_OK;
+}
+
+int cep_tissue_sync(cep_tissue_t t) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  return fem_check_ctl(t->fem);
+}
+
+int cep_tissue_get_v(cep_tissue_t t, double *v) {
+  if (!t || !v) return fail_msg(CEP_ERR_ARG, "null argument");
+  FEM_CUDA(cudaMemcpyAsync(v, cep_internal_batch_v(t->cells), sizeof(double) * t->n, cudaMemcpyDeviceToHost, t->stream));
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  return CEP_OK;
+}
+
+int cep_tissue_get_activation(cep_tissue_t t, double *t_act) {
+  if (!t || !t_act) return fail_msg(CEP_ERR_ARG, "null argument");
+  FEM_CUDA(cudaMemcpyAsync(t_act, t->tact, sizeof(double) * t->n, cudaMemcpyDeviceToHost, t->stream));
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  return CEP_OK;
+}
+
+int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, int *not_converged) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  int rc = cep_tissue_sync(t);
+  if (rc) return rc;
+  long total = 0;
+  int nc = 0;
+  if ((rc = cep_fem_stats(t->fem, nullptr, &total, nullptr, &nc, nullptr))) return rc;
+  if (time) *time = t->t;
+  if (steps) *steps = t->steps;
+  if (cg_iters) *cg_iters = total;
+  if (not_converged) *not_converged = nc;
+  return CEP_OK;
+}
+
+}  // extern "C"

@@ -13,6 +13,9 @@ extern "C" {
 // (heart.cpp:309-323). d_mask is a device array of n bytes.
 int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double bcl, double t_crt,
                                    double dur, int n_pace, long n_steps);
+// Tissue clock: every instance at t = 0 with no protocol end and biomarkers
+// off; the fixed step is dt.
+int cep_internal_batch_tissue_begin(cep_batch_t b, double dt);
 // Device pointer of the membrane-potential row (n doubles) and the stream.
 double *cep_internal_batch_v(cep_batch_t b);
 void *cep_internal_batch_stream(cep_batch_t b);

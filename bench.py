@@ -78,8 +78,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop"])
-    ap.add_argument("--seg", type=int, default=10000, help="time steps per bench step")
+    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop", "tt06_sheet"])
+    ap.add_argument("--seg", type=int, default=None,
+                    help="time steps per bench step (default 10000 for populations, 200 for tissue)")
+    ap.add_argument("--nx", type=int, default=512, help="tissue sheet edge in nodes")
     ap.add_argument("--samples", type=int, default=2000)
     ap.add_argument("--concs", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
@@ -87,11 +89,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--kernel", default="auto", choices=["auto", "cell", "roles"],
                     help="one thread per cell, 4 warps per 32 cells, or the library's default for the size")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.seg is None:
+        a.seg = 200 if a.workload == "tt06_sheet" else 10000
+    return a
 
 
 def model_of(workload: str) -> str:
-    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011"}[workload]
+    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011", "tt06_sheet": "tt2006"}[workload]
 
 
 # ------------------------------------------------------------ inputs
@@ -357,9 +362,211 @@ def config_of(args, model, n, world):
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance sharding x{world}"}
 
 
+# ------------------------------------------------------------ tissue workload
+TISSUE_DT, TISSUE_H, TISSUE_D, TISSUE_RTOL = 0.01, 0.025, 0.0013, 1e-8
+# Algorithmic bytes per row per CG iteration (FP64 values, int32 columns):
+# A row (w x 12 B), p and z of the row (16), p_k and q written (16); then p,
+# x (read+write), q, r (read+write), dinv read and z written (72).
+def cg_bytes_per_row(width: int) -> int:
+    return 12 * width + 16 + 16 + 72
+
+
+def tissue_inputs(seed: int, n_conc: int = 3):
+    """IKr block of one seeded drug: IC50 log-U[0.1,100] uM, h U[0.6,1.8],
+    Cmax log-U[0.01,10] uM; concentrations 0, 1x, 3x Cmax."""
+    rng = np.random.default_rng(seed)
+    hill = np.zeros(14)
+    hill[12] = 10 ** rng.uniform(-1, 2)
+    hill[13] = rng.uniform(0.6, 1.8)
+    cmax = 10 ** rng.uniform(-2, 1)
+    return [0.0, cmax, 3 * cmax][:n_conc], hill
+
+
+def make_sheet(cep, nx, prec, conc, hill):
+    n = nx * nx
+    cells = cep.Batch("tt2006", n, prec)
+    cells.init(conc=np.full(n, conc), hill=hill)
+    fem = cep.Fem.grid(2, nx, nx, 1, TISSUE_H, TISSUE_DT, TISSUE_D, fmt=cep.FEM_AUTO).set_solver(TISSUE_RTOL)
+    t = cep.Tissue(cells, fem, TISSUE_DT)
+    mask = np.zeros((nx, nx), np.uint8)
+    c = max(2, nx // 64)
+    mask[:c, :c] = 1  # corner S1
+    t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 2)
+    return t
+
+
+def run_tissue(args, world, rank, local, pg):
+    import torch
+    cep = importlib.import_module("2ddrugsimulation_b200")
+    torch.cuda.set_device(local)
+    concs, hill = tissue_inputs(4321 + rank)
+    nx = args.nx
+    n = nx * nx
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = {}
+    launches = 0
+    for prec in ("mixed", "fp64"):
+        sheets = [make_sheet(cep, nx, prec, c, hill) for c in concs]
+        for _ in range(args.warmup):
+            for t in sheets:
+                t.run(args.seg)
+            flush.zero_()
+        for t in sheets:
+            t.sync()
+        it0 = [t.stats()["cg_iters"] for t in sheets]
+        torch.cuda.synchronize()
+        barrier(pg)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            start.record()
+            for _ in range(args.steps):
+                for t in sheets:
+                    t.run(args.seg)
+                flush.zero_()
+            stop.record()
+            torch.cuda.synchronize()
+        barrier(pg)
+        ms = max_over_ranks(start.elapsed_time(stop), pg)
+        st = [t.stats() for t in sheets]
+        cg = sum(s["cg_iters"] for s in st) - sum(it0)
+        node_steps = n * len(sheets) * args.seg * args.steps * world
+        res[prec] = dict(value=node_steps / (ms / 1e3), ms_per_step=ms / args.steps, clocks=clk.summary(),
+                         cg_iters_per_solve=cg / (len(sheets) * args.seg * args.steps),
+                         not_converged=sum(s["not_converged"] for s in st), fmt=sheets[0].fem.format,
+                         ell_width=sheets[0].fem.ell_width)
+        launches += args.steps * len(sheets) * args.seg * 2
+        if prec == "mixed":
+            # PCG alone on the first sheet's current V (the dominant kernel)
+            f = sheets[0].fem
+            vptr, _ = sheets[0].cells.device_states()
+            lib = cep.lib()
+            k0 = f.stats()["total_iters"]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(50):
+                rc = lib.cep_fem_solve_device(f._h, ctypes.c_void_p(vptr))
+                if rc:
+                    raise RuntimeError(lib.cep_last_error().decode())
+            e1.record()
+            torch.cuda.synchronize()
+            pcg_ms = e0.elapsed_time(e1) / 50
+            iters = (f.stats()["total_iters"] - k0) / 50
+            res["pcg"] = dict(ms=pcg_ms, iters=iters, bytes=cg_bytes_per_row(f.ell_width) * n * iters)
+            if not args.no_e2e:
+                res["e2e"] = tissue_e2e(args, sheets, n, world, pg, cep)
+        for t in sheets:
+            t.close()
+    return res, n, launches
+
+
+def tissue_e2e(args, sheets, n, world, pg, cep):
+    """Each step through the C ABI with host buffers: upload every sheet's
+    state from pinned memory, run SEG Godunov steps, download V."""
+    import torch
+    ns = cep.N_STATES["tt2006"]
+    lib = cep.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    pin = [torch.empty(ns * n, dtype=torch.float64, pin_memory=True).numpy() for _ in sheets]
+    vout = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in sheets]
+    for p, t in zip(pin, sheets):
+        p[:] = t.cells.get_states(cep.LAYOUT_SOA).ravel()
+    torch.cuda.synchronize()
+    barrier(pg)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        for p, v, t in zip(pin, vout, sheets):
+            rc = lib.cep_batch_set_states(t.cells._h, p.ctypes.data_as(dp), cep.LAYOUT_SOA)
+            rc |= lib.cep_tissue_run(t._h, args.seg)
+            rc |= lib.cep_tissue_get_v(t._h, v.ctypes.data_as(dp))
+            if rc:
+                raise RuntimeError(lib.cep_last_error().decode())
+    stop.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(start.elapsed_time(stop), pg)
+    node_steps = n * len(sheets) * args.seg * args.steps * world
+    return {"value": node_steps / (ms / 1e3), "unit": "node-steps/s", "h2d_bytes_per_step": ns * n * 8 * len(sheets),
+            "d2h_bytes_per_step": n * 8 * len(sheets), "ms_per_step": ms / args.steps}
+
+
+def tissue_cpu(args):
+    """The oracle's tissue loop (TT2006 step + CSR Jacobi-PCG, one core) on
+    a 128x128 sheet, 400 Godunov steps (about 10 s)."""
+    from oracle import oracle as O
+    concs, hill = tissue_inputs(4321)
+    nx, steps = 128, 400
+    mask = np.zeros((nx, nx), np.uint8)
+    mask[:2, :2] = 1
+    t0 = time.perf_counter()
+    O.tissue_run("tt2006", 2, nx, nx, 1, TISSUE_H, TISSUE_D, TISSUE_DT, steps, mask.ravel(), 1000.0, 0.0, 1.0, 2,
+                 conc=concs[1], hill=hill, rtol=TISSUE_RTOL)
+    secs = time.perf_counter() - t0
+    return {"value": nx * nx * steps / secs, "unit": "node-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{nx}x{nx} sheet, {steps} Godunov steps ({secs:.1f} s)"}
+
+
+def tissue_main(args, world, rank, local, pg):
+    peaks = measured_peaks() if rank == 0 else {}
+    res, n, launches = run_tissue(args, world, rank, local, pg)
+    if rank != 0:
+        return
+    mixed, fp64, pcg = res["mixed"], res["fp64"], res["pcg"]
+    hbm = None
+    mp = peaks.get("measured_peaks_json") or {}
+    for k in ("hbm_gbs", "hbm_GBs", "hbm_gb_s"):
+        if k in mp:
+            hbm = float(mp[k])
+    src = "MEASURED_PEAKS.json hbm_gbs (measured)" if hbm else "fallback 6650 GB/s"
+    hbm = hbm or 6650.0
+    ach = pcg["bytes"] / (pcg["ms"] * 1e-3) / 1e9
+    line = {
+        "metric": "TT2006 monodomain node-steps/s (Godunov: ionic + Jacobi-PCG), mixed vs FP64",
+        "value": mixed["value"], "unit": "node-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (mixed ionic), f64 PCG", "data": "synthetic",
+        "config": {"workload": f"2D TT2006 epi sheet {args.nx}x{args.nx} Q1 nodes, dx 0.025 cm, D 0.0013 cm^2/ms, "
+                               f"dt 0.01 ms, Jacobi-PCG rtol 1e-8, corner S1 at BCL 1000 ms, IKr Hill block at 3 "
+                               f"concentrations (3 sheets per GPU); {args.seg} Godunov steps per sheet per bench step",
+                   "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell"][mixed["fmt"]],
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"sheet sharding x{world}"},
+        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
+                 "cg_iters_per_solve": fp64["cg_iters_per_solve"]},
+        "mixed_over_fp64": mixed["value"] / fp64["value"],
+        "cg_iters_per_solve": mixed["cg_iters_per_solve"], "not_converged": mixed["not_converged"] + fp64["not_converged"],
+        "roofline": {"bound": "hbm", "kernel": "pcg_kernel (one cooperative launch per solve)", "achieved": ach,
+                     "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "bytes_per_row_per_iter": cg_bytes_per_row(mixed["ell_width"]), "pcg_ms": pcg["ms"],
+                     "pcg_iters": pcg["iters"], "peak_source": src,
+                     "note": "the 2D operator (~47 MB ELL) and vectors stay in the 126 MB L2 across iterations"},
+        "gpu_launches": launches, "clocks": mixed["clocks"],
+        "cpu_baseline": None if args.no_cpu else tissue_cpu(args),
+        "e2e": res.get("e2e"),
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     model = model_of(args.workload)
+    if args.workload == "tt06_sheet":
+        world, rank, local, pg = dist_setup()
+        if args.impl == "reference":
+            if rank == 0:
+                cpu = tissue_cpu(args)
+                print(json.dumps({"impl": "reference", "metric": "TT2006 monodomain node-steps/s", "value": cpu["value"],
+                                  "unit": "node-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+                                  "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                                  "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                                  "config": {"workload": "TT2006 sheet (oracle port; the reference tissue solver "
+                                                         "needs PETSc, absent)", "sample": cpu["sample"]},
+                                  "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "node-steps/s",
+                                                               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            return
+        tissue_main(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     world, rank, local, pg = dist_setup()
     conc, hill = population(model, args.samples, args.concs, seed=1234)
     threads = os.cpu_count() or 1

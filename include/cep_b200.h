@@ -158,6 +158,79 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
  * INaL_auc_ctrl + ICaL_auc_drug/ICaL_auc_ctrl) (cipa_drug_bench.cpp:376). */
 double cep_qinward(const cep_biomarkers_t *control, const cep_biomarkers_t *drug);
 
+/* ------------------------------------------------------ monodomain FEM */
+/* The diffusion operator of one tissue: A = M/dt + D K and B = M, with the
+ * implicit step A V = B V* / dt solved by Jacobi-preconditioned CG from a
+ * zero initial guess. Replaces Cfem::assemble_Amat_Bmat (fem.cpp:721-763),
+ * Cfem::set_amat_bmat (fem.cpp:628-661) and Cfem::solve_Bmat
+ * (fem.cpp:705-718) with PETSc KSPCG + PCJACOBI (fem.cpp:753-760). */
+typedef struct cep_fem *cep_fem_t;
+
+#define CEP_FEM_AUTO (-1) /* time both formats on this operator, keep the faster */
+#define CEP_FEM_CSR 0
+#define CEP_FEM_ELL 1     /* column-major ELL, padded to the widest row */
+
+/* Structured grid of nx*ny (dim 2, Q1 quadrilaterals) or nx*ny*nz (dim 3,
+ * trilinear hexahedra) nodes at spacing h (cm), node id i + nx*(j + ny*k),
+ * the reference's "square" / hex meshes (mesh.cpp, fem.cpp:231-271,398-478).
+ * D holds n_d values per element, element id ex + (nx-1)*(ey + (ny-1)*ez):
+ * n_d = 1 is the reference's scalar DE (fem.cpp:656); n_d = 3 (2D: xx, xy,
+ * yy) or 6 (3D: xx, xy, xz, yy, yz, zz) is a conductivity tensor. Assembly
+ * runs on the device. stream as in cep_batch_create. */
+int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, const double *D, int n_d,
+                        int format, void *stream, cep_fem_t *out);
+/* An operator assembled by the caller (any mesh), CSR with sorted columns. */
+int cep_fem_create_csr(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b_val,
+                       double dt, int format, void *stream, cep_fem_t *out);
+int cep_fem_destroy(cep_fem_t f);
+int cep_fem_info(cep_fem_t f, int *n, long *nnz, int *format, int *ell_width);
+int cep_fem_set_format(cep_fem_t f, int format);
+/* Host copy of the assembled CSR (row_ptr[n+1], col_idx/a_val/b_val[nnz]). */
+int cep_fem_get_csr(cep_fem_t f, int *row_ptr, int *col_idx, double *a_val, double *b_val);
+/* Stopping rule ||r|| <= rtol ||b|| after at most max_iter iterations, in the
+ * preconditioned norm ||D^-1 r|| (precond_norm = 1, PETSc's default for CG)
+ * or the plain 2-norm. Defaults: rtol 1e-5 (PETSc's default; the reference
+ * sets none), max_iter 10000, preconditioned norm. */
+int cep_fem_set_solver(cep_fem_t f, double rtol, int max_iter, int precond_norm);
+/* y = A x (which = 0) or B x (which = 1); host vectors of n doubles. */
+int cep_fem_spmv(cep_fem_t f, int which, const double *x, double *y);
+/* One implicit diffusion step on a host vector: in V*, out V (blocking). */
+int cep_fem_solve(cep_fem_t f, double *v, int *iters, double *rel_res);
+/* The same on a device vector of n doubles, asynchronous on the stream. */
+int cep_fem_solve_device(cep_fem_t f, void *d_v);
+/* Solver counters (blocking): iterations of the last solve (negative when
+ * it hit max_iter), iterations and solves summed, solves that hit max_iter,
+ * relative residual of the last solve. CEP_ERR_TIMEOUT if a device barrier
+ * ran out of its spin limit. */
+int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves, int *not_converged,
+                  double *last_res);
+
+/* ---------------------------------------------------------------- tissue */
+/* Godunov-split monodomain tissue: per step every node's ionic update (the
+ * batch, one instance per node, tissue stimulus flag isS1) then the implicit
+ * diffusion solve on the V row, in place on the device (Cheart::processing,
+ * heart.cpp:127-165; Cheart::cellular_reaction, heart.cpp:274-430). The
+ * batch must be initialised, have as many instances as the operator has
+ * rows, share its stream, and dt must equal the operator's. Creating the
+ * tissue resets the batch's clock to t = 0 and turns its biomarkers off. */
+typedef struct cep_tissue *cep_tissue_t;
+int cep_tissue_create(cep_batch_t cells, cep_fem_t fem, double dt, cep_tissue_t *out);
+int cep_tissue_destroy(cep_tissue_t t);
+/* S1 nodes (mask[n], nonzero = stimulated) are driven while
+ * iia*bcl + t_crt < t < iia*bcl + t_crt + dur for pace iia = (int)(t/bcl)
+ * < n_pace (the "square" mesh rule, heart.cpp:309-323). */
+int cep_tissue_set_stimulus(cep_tissue_t t, const unsigned char *s1_mask, double bcl, double t_crt, double dur,
+                            int n_pace);
+/* Activation time of a node = the first step end at which V >= threshold
+ * (default -30 mV); -1 until then. No counterpart in the reference. */
+int cep_tissue_set_activation_threshold(cep_tissue_t t, double vm_threshold);
+/* Advance n_steps Godunov steps (asynchronous). */
+int cep_tissue_run(cep_tissue_t t, long n_steps);
+int cep_tissue_sync(cep_tissue_t t);
+int cep_tissue_get_v(cep_tissue_t t, double *v);
+int cep_tissue_get_activation(cep_tissue_t t, double *t_act);
+int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, int *not_converged);
+
 #ifdef __cplusplus
 }
 #endif

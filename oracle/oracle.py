@@ -90,6 +90,22 @@ def lib() -> ctypes.CDLL:
                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_long, _dp,
                                      ctypes.c_int]
         L.cepo_run_batch.restype = ctypes.c_int
+        _ip = ctypes.POINTER(ctypes.c_int)
+        L.cepo_fem_nnz.argtypes = [ctypes.c_int] * 4
+        L.cepo_fem_nnz.restype = ctypes.c_long
+        L.cepo_fem_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, _dp, ctypes.c_int, _ip, _ip, _dp, _dp]
+        L.cepo_fem_element.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp, _dp]
+        L.cepo_spmv.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
+        L.cepo_pcg2.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                _dp]
+        L.cepo_pcg2.restype = ctypes.c_int
+        L.cepo_tissue_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_long,
+                                      ctypes.POINTER(ctypes.c_uint8), ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_int, _dp, _dp, _ip, ctypes.c_double, _dp]
+        L.cepo_tissue_run.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -228,3 +244,85 @@ class RefCell:
 
 def ref_available(key: str) -> bool:
     return (REF_DIR / REF_LIBS[key]).exists()
+
+
+# ------------------------------------------------------------------ FEM
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def _iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+def element_D(dim: int, nx: int, ny: int, nz: int, D) -> np.ndarray:
+    n_elem = (nx - 1) * (ny - 1) * ((nz - 1) if dim == 3 else 1)
+    d = np.asarray(D, np.float64)
+    if d.ndim == 0:
+        d = np.full((n_elem, 1), float(d))
+    elif d.ndim == 1:
+        d = d.reshape(n_elem, 1)
+    return np.ascontiguousarray(d)
+
+
+def fem_assemble(dim: int, nx: int, ny: int, nz: int, h: float, dt: float, D):
+    """CSR (row_ptr, col, A, B) of the structured-grid operator."""
+    if dim == 2:
+        nz = 1
+    d = element_D(dim, nx, ny, nz, D)
+    n = nx * ny * nz
+    nnz = lib().cepo_fem_nnz(dim, nx, ny, nz)
+    rp = np.zeros(n + 1, np.int32)
+    ci = np.zeros(nnz, np.int32)
+    av = np.zeros(nnz)
+    bv = np.zeros(nnz)
+    lib().cepo_fem_assemble(dim, nx, ny, nz, h, dt, _ptr(d), d.shape[1], _iptr(rp), _iptr(ci), _ptr(av), _ptr(bv))
+    return rp, ci, av, bv
+
+
+def fem_element(dim: int, h: float, dt: float, D) -> tuple[np.ndarray, np.ndarray]:
+    d = np.ascontiguousarray(np.atleast_1d(np.asarray(D, np.float64)))
+    nn = 4 if dim == 2 else 8
+    ae = np.zeros(nn * nn)
+    be = np.zeros(nn * nn)
+    lib().cepo_fem_element(dim, h, dt, _ptr(d), len(d), _ptr(ae), _ptr(be))
+    return ae.reshape(nn, nn), be.reshape(nn, nn)
+
+
+def spmv(rp, ci, val, x) -> np.ndarray:
+    xx = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(len(rp) - 1)
+    lib().cepo_spmv(len(rp) - 1, _iptr(rp), _iptr(ci), _ptr(np.ascontiguousarray(val)), _ptr(xx), _ptr(y))
+    return y
+
+
+def pcg(rp, ci, a_val, b, rtol: float, max_iter: int = 10000, precond_norm: bool = True):
+    """Jacobi-PCG from x = 0: (x, iterations (negative if not converged), rel. residual)."""
+    bb = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(len(rp) - 1)
+    res = ctypes.c_double()
+    it = lib().cepo_pcg2(len(rp) - 1, _iptr(rp), _iptr(ci), _ptr(np.ascontiguousarray(a_val)), _ptr(bb), _ptr(x),
+                         rtol, max_iter, int(precond_norm), ctypes.byref(res))
+    return x, it, res.value
+
+
+def tissue_run(model: str, dim: int, nx: int, ny: int, nz: int, h: float, D, dt: float, n_steps: int, s1_mask,
+               bcl: float, t_crt: float, dur: float, n_pace: int, conc: float = 0.0, hill=None,
+               rtol: float = 1e-5, precond_norm: bool = True, celltype=None, act_thr: float = -30.0):
+    """Godunov-split tissue run: (final V, CG iterations per step, activation times)."""
+    if dim == 2:
+        nz = 1
+    d = element_D(dim, nx, ny, nz, D)
+    n = nx * ny * nz
+    m = np.ascontiguousarray(s1_mask, np.uint8)
+    hh = None if hill is None else np.ascontiguousarray(hill, np.float64)
+    ct = None if celltype is None else np.ascontiguousarray(celltype, np.float64)
+    v = np.zeros(n)
+    its = np.zeros(n_steps, np.int32)
+    tact = np.zeros(n)
+    lib().cepo_tissue_run(MODELS[model], dim, nx, ny, nz, h, _ptr(d), d.shape[1], dt, n_steps,
+                          m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt, dur, n_pace, conc,
+                          _ptr(hh) if hh is not None else None, 0 if hh is None else len(hh), rtol,
+                          int(precond_norm), _ptr(ct) if ct is not None else None, _ptr(v), _iptr(its), act_thr,
+                          _ptr(tact))
+    return v, its, tact

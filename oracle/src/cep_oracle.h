@@ -113,7 +113,7 @@ void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, do
 long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                      double conc, const double *hill, int n_hill, double rtol, int precond_norm,
-                     const double *celltype, double *V, int *iters_out);
+                     const double *celltype, double *V, int *iters_out, double act_thr, double *t_act);
 
 #ifdef __cplusplus
 }

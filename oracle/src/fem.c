@@ -221,11 +221,12 @@ int cepo_pcg(int n, const int *row_ptr, const int *col_idx, const double *a_val,
  * while iia*bcl + t_crt < t < iia*bcl + t_crt + dur for pace iia < n_pace
  * (the "square" mesh rule, heart.cpp:309-323). Returns total CG iterations;
  * V (n) receives the final potential, iters_out (n_steps, may be NULL) the
- * iterations per step. */
+ * iterations per step, t_act (n, may be NULL) the first step end at which
+ * V >= act_thr (-1 if never). */
 long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                      double conc, const double *hill, int n_hill, double rtol, int precond_norm,
-                     const double *celltype, double *V, int *iters_out) {
+                     const double *celltype, double *V, int *iters_out, double act_thr, double *t_act) {
   if (dim == 2) nz = 1;
   const int n = nx * ny * nz;
   const long nnz = cepo_fem_nnz(dim, nx, ny, nz);
@@ -243,6 +244,8 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
   }
   double t = 0.0;
   long total = 0;
+  if (t_act)
+    for (int i = 0; i < n; ++i) t_act[i] = -1.0;
   for (long st = 0; st < n_steps; ++st) {
     const int iia = (int)(t / bcl);
     const int on = iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt;
@@ -259,6 +262,9 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
     if (iters_out) iters_out[st] = it;
     for (int i = 0; i < n; ++i) y[(size_t)i * CEPO_MAX_STATES] = vs[i];
     t += dt;
+    if (t_act)
+      for (int i = 0; i < n; ++i)
+        if (t_act[i] < 0.0 && vs[i] >= act_thr) t_act[i] = t;
   }
   (void)ns;
   for (int i = 0; i < n; ++i) V[i] = y[(size_t)i * CEPO_MAX_STATES];

@@ -1,0 +1,165 @@
+"""Monodomain FEM on the GPU against the oracle: device assembly (bit for
+bit), SpMV, the persistent Jacobi-PCG solve, and a Godunov-split tissue run.
+
+Tolerances: assembly is exact (the device builds each entry with the same
+IEEE expression, summed over elements in the same order). SpMV rows use
+FMA, so they agree to 1e-13 relative. The PCG's dot products are tree sums,
+so iterates differ by rounding: iteration counts may differ by one at the
+stopping boundary and converged solutions agree to the solver tolerance.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def _tensor_field(dim, n_elem, seed):
+    rng = np.random.default_rng(seed)
+    if dim == 2:
+        D = np.zeros((n_elem, 3))
+        D[:, 0] = rng.uniform(5e-4, 2e-3, n_elem)
+        D[:, 2] = rng.uniform(5e-4, 2e-3, n_elem)
+        D[:, 1] = 0.3 * np.sqrt(D[:, 0] * D[:, 2]) * rng.uniform(-1, 1, n_elem)
+    else:
+        D = np.zeros((n_elem, 6))
+        for c in (0, 3, 5):
+            D[:, c] = rng.uniform(5e-4, 2e-3, n_elem)
+        D[:, 1] = 0.2 * np.sqrt(D[:, 0] * D[:, 3]) * rng.uniform(-1, 1, n_elem)
+    return D
+
+
+CASES = [(2, (13, 9, 1), "scalar"), (2, (11, 17, 1), "tensor"), (3, (6, 5, 4), "scalar"), (3, (7, 6, 5), "tensor")]
+
+
+def _field(dim, shape, kind, seed=0):
+    nx, ny, nz = shape
+    n_elem = (nx - 1) * (ny - 1) * ((nz - 1) if dim == 3 else 1)
+    if kind == "scalar":
+        return np.random.default_rng(seed).uniform(5e-4, 2e-3, n_elem)
+    return _tensor_field(dim, n_elem, seed)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,shape,kind", CASES)
+def test_grid_assembly_bitwise(cep, gpu, oracle, dim, shape, kind):
+    D = _field(dim, shape, kind)
+    nx, ny, nz = shape
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D)
+    rp, ci, a, b = f.get_csr()
+    orp, oci, oa, ob = oracle.fem_assemble(dim, nx, ny, nz, 0.025, 0.01, D)
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    assert np.array_equal(a, oa), np.abs(a - oa).max()
+    assert np.array_equal(b, ob), np.abs(b - ob).max()
+    assert f.ell_width == (9 if dim == 2 else 27)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt", ["csr", "ell"])
+@pytest.mark.parametrize("dim,shape,kind", CASES)
+def test_spmv(cep, gpu, oracle, dim, shape, kind, fmt):
+    D = _field(dim, shape, kind, seed=1)
+    nx, ny, nz = shape
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D, fmt=cep.FEM_CSR if fmt == "csr" else cep.FEM_ELL)
+    rp, ci, a, b = oracle.fem_assemble(dim, nx, ny, nz, 0.025, 0.01, D)
+    x = np.random.default_rng(2).uniform(-90, 30, f.n)
+    for which, val in (("A", a), ("B", b)):
+        y = f.spmv(x, which)
+        ref = oracle.spmv(rp, ci, val, x)
+        scale = oracle.spmv(rp, ci, np.abs(val), np.abs(x))
+        assert np.all(np.abs(y - ref) <= 1e-13 * scale), (which, np.abs(y - ref).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precond_norm", [True, False])
+@pytest.mark.parametrize("dim,shape,kind", CASES)
+def test_pcg_matches_oracle(cep, gpu, oracle, dim, shape, kind, precond_norm):
+    D = _field(dim, shape, kind, seed=3)
+    nx, ny, nz = shape
+    dt = 0.01
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, dt, D)
+    rp, ci, a, b = oracle.fem_assemble(dim, nx, ny, nz, 0.025, dt, D)
+    v = np.random.default_rng(5).uniform(-90, 30, f.n)
+    rhs = oracle.spmv(rp, ci, b, v) / dt
+    for rtol in (1e-5, 1e-8, 1e-12):
+        f.set_solver(rtol, 1000, precond_norm)
+        xg, itg, resg = f.solve(v)
+        xo, ito, reso = oracle.pcg(rp, ci, a, rhs, rtol, 1000, precond_norm)
+        assert abs(itg - ito) <= 1, (rtol, itg, ito)
+        assert resg <= rtol
+        tol = 1e-9 if itg == ito else 10 * rtol
+        assert np.abs(xg - xo).max() <= tol * np.abs(xo).max(), (rtol, np.abs(xg - xo).max())
+
+
+@pytest.mark.gpu
+def test_pcg_from_user_csr_and_autotune(cep, gpu, oracle):
+    nx, ny = 40, 33
+    D = _field(2, (nx, ny, 1), "tensor", seed=9)
+    rp, ci, a, b = oracle.fem_assemble(2, nx, ny, 1, 0.025, 0.01, D)
+    g = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, D).set_solver(1e-10)
+    u = cep.Fem.csr(rp, ci, a, b, 0.01, fmt=cep.FEM_AUTO).set_solver(1e-10)
+    assert u.format in (cep.FEM_CSR, cep.FEM_ELL)
+    v = np.random.default_rng(1).uniform(-90, 30, g.n)
+    xg, itg, _ = g.solve(v)
+    xu, itu, _ = u.solve(v)
+    assert itg == itu and np.array_equal(xg, xu)  # same matrix, same order: bitwise
+    u.set_format(cep.FEM_CSR)
+    xc, itc, _ = u.solve(v)
+    assert itc == itg and np.abs(xc - xg).max() <= 1e-12 * np.abs(xg).max()
+
+
+@pytest.mark.gpu
+def test_pcg_edge_cases(cep, gpu, oracle):
+    f = cep.Fem.grid(2, 9, 7, 1, 0.025, 0.01, 0.0013)
+    x, it, res = f.solve(np.zeros(f.n))
+    assert it == 0 and not x.any()
+    # uniform V is reproduced exactly up to rounding (K annihilates constants)
+    x, it, _ = f.set_solver(1e-12).solve(np.full(f.n, -85.0))
+    assert np.abs(x + 85.0).max() < 1e-9
+    # a capped iteration count reports NOT_CONVERGED, and the counters say so
+    f.set_solver(1e-15, 2)
+    v = np.random.default_rng(0).uniform(-90, 30, f.n)
+    with pytest.raises(cep.CepError) as e:
+        f.solve(v)
+    assert e.value.code == cep.ERR_NOT_CONVERGED
+    st = f.stats()
+    assert st["not_converged"] == 1 and st["last_iters"] == -2
+    # deterministic reductions: repeated solves are bit-identical
+    f.set_solver(1e-8)
+    x1, _, _ = f.solve(v)
+    x2, _, _ = f.solve(v)
+    assert np.array_equal(x1, x2)
+
+
+def _tissue(cep, precision, nx, ny, mask, conc=0.0, hill=None, rtol=1e-10):
+    n = nx * ny
+    cells = cep.Batch("tt2006", n, precision)
+    cells.init(conc=np.full(n, conc), hill=hill)
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(rtol)
+    t = cep.Tissue(cells, fem, 0.01)
+    t.set_stimulus(mask, 1000.0, 0.0, 1.0, 1)
+    return t
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tissue_tt2006_matches_oracle(cep, gpu, oracle, precision):
+    """20 x 16 TT2006 sheet, corner S1, 12 ms (1200 Godunov steps)."""
+    nx, ny, steps = 20, 16, 1200
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:3, :3] = 1
+    hill = np.zeros(14)
+    hill[12], hill[13] = 0.5, 1.0  # IKr block
+    vo, itso, tacto = oracle.tissue_run("tt2006", 2, nx, ny, 1, 0.025, 0.0013, 0.01, steps, mask.ravel(), 1000.0,
+                                        0.0, 1.0, 1, conc=0.3, hill=hill, rtol=1e-10)
+    t = _tissue(cep, precision, nx, ny, mask.ravel(), conc=0.3, hill=hill)
+    t.run(steps)
+    st = t.stats()
+    assert st["steps"] == steps and st["not_converged"] == 0
+    vg, tactg = t.v(), t.activation()
+    assert (tacto > 0).all() and (tactg > 0).all()
+    if precision == "fp64":
+        assert np.abs(vg - vo).max() <= 1e-6, np.abs(vg - vo).max()
+        assert np.array_equal(tactg, tacto)
+        assert abs(st["cg_iters"] - int(itso.sum())) <= 0.02 * itso.sum()
+    else:
+        assert np.abs(tactg - tacto).max() <= 0.1 + 1e-9, np.abs(tactg - tacto).max()

@@ -165,7 +165,13 @@ def test_ord_split_launches_equal_single_launch(cep, gpu):
     """K steps in one launch equal the same K steps in many launches
     (state, clock and biomarker state persist exactly across launches)."""
     cases = _config1_cases(seed=5, n_conc=3)
-    a, sa = _gpu_biomarkers(cep, cases, "fp64", 3, 2, 0.005, 1000.0)
+    one = cep.Batch("ord2011", 3, "fp64")
+    one.init(conc=np.array([c["conc"] for c in cases]), hill=np.stack([c["hill"] for c in cases]))
+    one.set_pacing(1000.0)
+    one.set_protocol(0.005, 3, 2, dt_write=1.0)
+    one.run_to_end(700000)  # the whole protocol in one launch
+    a, sa = one.biomarkers(), one.get_states()
+    assert one.clock(0)[0] == 600000
     b = cep.Batch("ord2011", 3, "fp64")
     b.init(conc=np.array([c["conc"] for c in cases]), hill=np.stack([c["hill"] for c in cases]))
     b.set_pacing(1000.0)
