@@ -191,20 +191,7 @@ struct RunArgs {
   bm::View bv;
   double qnet_thr;
   int stim_mode;  // -1 periodic; 0/1 fixed tissue flag
-  // tissue stimulus (heart.cpp:309-323): isS1 = s1_mask[i] inside the window
-  const unsigned char *s1_mask;
-  double s1_bcl, s1_tcrt, s1_dur;
-  int s1_npace;
 };
-
-// Stimulus mode of instance i at time t: the tissue window when a mask is set.
-__device__ __forceinline__ int stim_mode_at(const RunArgs &a, int64_t i, double t) {
-  if (!a.s1_mask) return a.stim_mode;
-  const int iia = (int)(t / a.s1_bcl);
-  const bool win = iia < a.s1_npace && t < (double)iia * a.s1_bcl + a.s1_dur + a.s1_tcrt &&
-                   t > (double)iia * a.s1_bcl + a.s1_tcrt;
-  return (win && a.s1_mask[i]) ? 1 : 0;
-}
 
 __global__ void reset_kernel(RunArgs a, int p_bcl, int p_start, int cai_idx) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,7 +231,7 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
     if (can_update && k == a.n_steps) break;  // budget spent; sample iout is taken next launch
     const double V0 = y.V;
     const double cai0 = M::cai_of(y);
-    M::template step<P>(y, q, t, a.dt, stim_mode_at(a, i, t), can_update, c);
+    M::template step<P>(y, q, t, a.dt, a.stim_mode, can_update, c);
     if (bm_on && iout >= 1)
       bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
                  (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
@@ -305,7 +292,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     const bool upd = active && can_update;
     const double V0 = y.V;
     const double cai0 = M::cai_of(y);
-    const auto ctx = ord::context<P>(y, q, t, stim_mode_at(a, il, t));
+    const auto ctx = ord::context<P>(y, q, t, a.stim_mode);
     ord::Part<G> p;
     ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
 #pragma unroll
@@ -383,6 +370,33 @@ __global__ void __launch_bounds__(128) run_roles_kernel(RunArgs a) {
     case 2: role_loop<M, P, 2>(a, part, lane); break;
     default: role_loop<M, P, 3>(a, part, lane); break;
   }
+}
+
+// One Godunov ionic step of a tissue: every node advances by dt from the
+// tissue clock t with the stimulus flag of its S1 mask window; no biomarker
+// bookkeeping, so only the state and the parameters cross HBM.
+struct TissueArgs {
+  double *y;
+  const double *par;
+  int64_t ld;
+  int n;
+  double t, dt;
+  const unsigned char *mask;
+  int stim_on;  // the window test, uniform over the tissue
+};
+
+template <class M, class P>
+__global__ void __launch_bounds__(128) tissue_kernel(TissueArgs a) {
+  using G = typename P::G;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  typename M::template Y<G> y;
+  typename M::template Par<G> q;
+  M::template load<G>(y, a.y, a.ld, i);
+  M::template load_par<G>(q, a.par, a.ld, i);
+  typename M::template Cur<G> c;
+  M::template step<P>(y, q, a.t, a.dt, (a.stim_on && a.mask[i]) ? 1 : 0, true, c);
+  M::template store<G>(y, a.y, a.ld, i);
 }
 
 // Rates at the current state (no update).
@@ -479,6 +493,15 @@ struct Ops {
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "run launch failed: %s", cudaGetErrorString(e));
   }
+  static int launch_tissue(cep_batch *b, const TissueArgs &a) {
+    const int grid = (b->n + 127) / 128;
+    if (b->precision == CEP_PREC_MIXED)
+      tissue_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
+    else
+      tissue_kernel<M, F64><<<grid, 128, 0, b->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "tissue launch failed: %s", cudaGetErrorString(e));
+  }
   static int launch_rates(cep_batch *b, double t, double *dvdt, double *cur) {
     const int grid = (b->n + kBlock - 1) / kBlock;
     rates_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->states, b->params, b->ld, b->n, t, -1, dvdt, cur);
@@ -494,21 +517,22 @@ struct ModelInfo {
   int (*run)(cep_batch *, const RunArgs &);
   int (*rates)(cep_batch *, double, double *, double *);
   int p_bcl;
+  int (*tissue)(cep_batch *, const TissueArgs &);
 };
 
 const ModelInfo *model_info(int model) {
   static const ModelInfo ord_info{OrdModel::kStates, OrdModel::kParams, OrdModel::kCai,
                                   &Ops<OrdModel>::launch_init, &Ops<OrdModel>::launch_pacing,
                                   &Ops<OrdModel>::launch_reset, &Ops<OrdModel>::launch_run,
-                                  &Ops<OrdModel>::launch_rates, OrdModel::p_bcl()};
+                                  &Ops<OrdModel>::launch_rates, OrdModel::p_bcl(), &Ops<OrdModel>::launch_tissue};
   static const ModelInfo cipa_info{CipaModel::kStates, CipaModel::kParams, CipaModel::kCai,
                                    &Ops<CipaModel>::launch_init, &Ops<CipaModel>::launch_pacing,
                                    &Ops<CipaModel>::launch_reset, &Ops<CipaModel>::launch_run,
-                                   &Ops<CipaModel>::launch_rates, CipaModel::p_bcl()};
+                                   &Ops<CipaModel>::launch_rates, CipaModel::p_bcl(), &Ops<CipaModel>::launch_tissue};
   static const ModelInfo tt06_info{Tt06Model::kStates, Tt06Model::kParams, Tt06Model::kCai,
                                    &Ops<Tt06Model>::launch_init, &Ops<Tt06Model>::launch_pacing,
                                    &Ops<Tt06Model>::launch_reset, &Ops<Tt06Model>::launch_run,
-                                   &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl()};
+                                   &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl(), &Ops<Tt06Model>::launch_tissue};
   switch (model) {
     case CEP_MODEL_TT2006: return &tt06_info;
     case CEP_MODEL_ORD2011: return &ord_info;
@@ -542,8 +566,6 @@ RunArgs make_args(cep_batch *b, long n_steps) {
   a.bv.ld = b->ld;
   a.qnet_thr = b->qnet_thr;
   a.stim_mode = -1;
-  a.s1_mask = nullptr;
-  a.s1_bcl = 1.0; a.s1_tcrt = 0.0; a.s1_dur = 0.0; a.s1_npace = 0;
   return a;
 }
 
@@ -850,14 +872,15 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
   return CEP_OK;
 }
 
-int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double bcl, double t_crt,
-                                   double dur, int n_pace, long n_steps) {
+int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double t, double bcl, double t_crt,
+                                   double dur, int n_pace) {
   if (!b || !b->initialized) return fail(CEP_ERR_STATE, "tissue batch not initialised");
-  RunArgs a = make_args(b, n_steps);
-  a.bm_on = 0;
-  a.s1_mask = d_mask;
-  a.s1_bcl = bcl; a.s1_tcrt = t_crt; a.s1_dur = dur; a.s1_npace = n_pace;
-  return model_info(b->model)->run(b, a);
+  TissueArgs a;
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = t; a.dt = b->dt; a.mask = d_mask;
+  // the "square" mesh S1 window (heart.cpp:309-323)
+  const int iia = (int)(t / bcl);
+  a.stim_on = (iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt) ? 1 : 0;
+  return model_info(b->model)->tissue(b, a);
 }
 
 int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {

@@ -66,8 +66,8 @@ int fail_msg(int code, const char *fmt, ...) {
   return cep_internal_set_fail(code, buf);
 }
 
-constexpr int kPcgBlock = 512;
-constexpr long kSpinLimit = 1L << 24;  // x ~64-128 ns sleeps: about a second or two
+constexpr int kPcgBlock = 1024;
+constexpr long kSpinLimit = 1L << 22;  // polls of ~0.3-0.5 us: about a second or two
 
 }  // namespace
 
@@ -114,6 +114,39 @@ struct EllView {
   }
 };
 
+// Structured-grid operator with implicit columns: slot (dk+1)*9 + (dj+1)*3 +
+// (di+1) of row i couples node i with node i + di + nx*(dj + ny*dk); slots
+// outside the grid hold 0 and read the row's own entry. Slots run in
+// ascending column order, so a row sums its nonzeros in the same order as
+// CSR/ELL. Vector gathers are unit-stride across a warp.
+template <int DIM>
+struct StencilView {
+  const double *a, *b;  // [slots][ld]
+  int nx, ny, nz;
+  int64_t ld;
+  template <class X>
+  __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
+    const int64_t plane = (int64_t)nx * ny;
+    const int ix = (int)(i % nx);
+    const int iy = (int)((i / nx) % ny);
+    const int iz = DIM == 3 ? (int)(i / plane) : 0;
+    double s = 0.0;
+#pragma unroll
+    for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
+          const bool in = (unsigned)(ix + di) < (unsigned)nx && (unsigned)(iy + dj) < (unsigned)ny &&
+                          (DIM == 2 || (unsigned)(iz + dk) < (unsigned)nz);
+          const int64_t j = in ? i + di + (int64_t)nx * dj + plane * dk : i;
+          s = fma(val[slot * ld + i], x((int)j), s);
+        }
+    return s;
+  }
+};
+
 struct PcgArgs {
   int64_t n;
   double dt, rtol;
@@ -128,16 +161,22 @@ struct PcgArgs {
   double t_new, act_thr;
 };
 
-__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
-// Grid-wide barrier over co-resident blocks (cooperative launch), bounded.
+// Grid-wide barrier over co-resident blocks (cooperative launch), bounded:
+// one arrival atomic per block, the waiters poll the generation word with
+// acquire loads.
 __device__ __forceinline__ bool grid_sync(Ctl *ctl) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned gen = ld_volatile(&ctl->gen);
+    const unsigned gen = ld_acquire(&ctl->gen);
     __threadfence();
     if (atomicAdd(&ctl->count, 1u) == gridDim.x - 1) {
       atomicExch(&ctl->count, 0u);
@@ -145,13 +184,12 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl) {
       atomicAdd(&ctl->gen, 1u);
     } else {
       long spins = 0;
-      while (ld_volatile(&ctl->gen) == gen) {
+      while (ld_acquire(&ctl->gen) == gen) {
         if (++spins > kSpinLimit) {
           atomicExch(&ctl->err, 1);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
     __threadfence();
@@ -164,7 +202,8 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl) {
 
 // Fixed-order block reduction of two values; thread 0 gets the sums.
 __device__ __forceinline__ void block_sum2(double &x, double &y) {
-  __shared__ double sx[kPcgBlock / 32], sy[kPcgBlock / 32];
+  constexpr int kWarps = kPcgBlock / 32;
+  __shared__ double sx[kWarps], sy[kWarps];
   for (int o = 16; o > 0; o >>= 1) {
     x += __shfl_down_sync(0xffffffffu, x, o);
     y += __shfl_down_sync(0xffffffffu, y, o);
@@ -176,9 +215,9 @@ __device__ __forceinline__ void block_sum2(double &x, double &y) {
   }
   __syncthreads();
   if (w == 0) {
-    x = l < kPcgBlock / 32 ? sx[l] : 0.0;
-    y = l < kPcgBlock / 32 ? sy[l] : 0.0;
-    for (int o = 8; o > 0; o >>= 1) {
+    x = l < kWarps ? sx[l] : 0.0;
+    y = l < kWarps ? sy[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
       x += __shfl_down_sync(0xffffffffu, x, o);
       y += __shfl_down_sync(0xffffffffu, y, o);
     }
@@ -187,14 +226,26 @@ __device__ __forceinline__ void block_sum2(double &x, double &y) {
 }
 
 // Sum of gridDim.x partials in a fixed order, identical in every block; the
-// result is broadcast to the whole block.
+// result is broadcast to the whole block. Each lane issues all its loads
+// before adding so one L2 round trip covers them.
 __device__ __forceinline__ void grid_total2(const double *pa, const double *pb, double &a, double &b) {
   __shared__ double s[2];
   if (threadIdx.x < 32) {
+    constexpr int kU = 8;
     double x = 0.0, y = 0.0;
-    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
-      x += __ldcg(pa + k);
-      if (pb) y += __ldcg(pb + k);
+    for (int base = 0; base < (int)gridDim.x; base += 32 * kU) {
+      double xs[kU], ys[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = base + u * 32 + threadIdx.x;
+        xs[u] = k < (int)gridDim.x ? __ldcg(pa + k) : 0.0;
+        ys[u] = (pb && k < (int)gridDim.x) ? __ldcg(pb + k) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        x += xs[u];
+        y += ys[u];
+      }
     }
     for (int o = 16; o > 0; o >>= 1) {
       x += __shfl_down_sync(0xffffffffu, x, o);
@@ -348,6 +399,26 @@ __global__ void csr_to_ell_kernel(int64_t n, const int *rp, const int *col, cons
   dinv[i] = 1.0 / diag;
 }
 
+__global__ void csr_to_stencil_kernel(int64_t n, int nx, int ny, int dim, const int *rp, const int *col,
+                                      const double *a, const double *b, int64_t ld, double *sa, double *sb) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int slots = dim == 3 ? 27 : 9;
+  for (int k = 0; k < slots; ++k) {
+    sa[k * ld + i] = 0.0;
+    sb[k * ld + i] = 0.0;
+  }
+  const int64_t plane = (int64_t)nx * ny;
+  const int ix = (int)(i % nx), iy = (int)((i / nx) % ny), iz = (int)(i / plane);
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const int64_t j = col[k];
+    const int jx = (int)(j % nx), jy = (int)((j / nx) % ny), jz = (int)(j / plane);
+    const int slot = (dim == 3 ? (jz - iz + 1) * 9 : 0) + (jy - iy + 1) * 3 + (jx - ix + 1);
+    sa[slot * ld + i] = a[k];
+    sb[slot * ld + i] = b[k];
+  }
+}
+
 }  // namespace fem
 }  // namespace cep
 
@@ -361,6 +432,8 @@ struct cep_fem {
   cudaStream_t stream = nullptr;
   int *rp = nullptr, *col = nullptr, *ecol = nullptr;
   double *a = nullptr, *b = nullptr, *ea = nullptr, *eb = nullptr, *dinv = nullptr;
+  double *sa = nullptr, *sb = nullptr;  // stencil values (grid operators only)
+  int dim = 0, gnx = 0, gny = 0, gnz = 0;
   double *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr;
   Ctl *ctl = nullptr;
   Status *st = nullptr;
@@ -390,6 +463,18 @@ void fem_free(cep_fem *f) {
 
 CsrView csr_view(const cep_fem *f) { return CsrView{f->rp, f->col, f->a, f->b}; }
 EllView ell_view(const cep_fem *f) { return EllView{f->ecol, f->ea, f->eb, f->width, f->ld}; }
+template <int D>
+StencilView<D> stencil_view(const cep_fem *f) {
+  return StencilView<D>{f->sa, f->sb, f->gnx, f->gny, f->gnz, f->ld};
+}
+
+// Dispatch a functor on the operator's current format view.
+template <class Fn>
+auto with_view(const cep_fem *f, Fn fn) {
+  if (f->format == CEP_FEM_CSR) return fn(csr_view(f));
+  if (f->format == CEP_FEM_STENCIL) return f->dim == 3 ? fn(stencil_view<3>(f)) : fn(stencil_view<2>(f));
+  return fn(ell_view(f));
+}
 
 // Buffers shared by both formats, the cooperative grid size, and zeroed
 // control words.
@@ -404,9 +489,14 @@ int fem_finish_setup(cep_fem *f) {
   FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_csr, pcg_kernel<CsrView>, kPcgBlock, 0));
   FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ell, pcg_kernel<EllView>, kPcgBlock, 0));
-  const int per_sm = std::max(1, std::min(per_sm_csr, per_sm_ell));
+  int per_sm_s2 = 0, per_sm_s3 = 0;
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s2, pcg_kernel<StencilView<2>>, kPcgBlock, 0));
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s3, pcg_kernel<StencilView<3>>, kPcgBlock, 0));
+  // one block per SM: fewer arrivals per grid barrier and fewer partials
+  if (std::min(std::min(per_sm_csr, per_sm_ell), std::min(per_sm_s2, per_sm_s3)) < 1)
+    return fail_msg(CEP_ERR_CUDA, "PCG kernel does not fit on an SM");
   const int64_t need = (f->n + kPcgBlock - 1) / kPcgBlock;
-  f->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, need));
+  f->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms, need));
   if ((rc = fem_alloc(f, &f->part, (size_t)3 * f->grid)) || (rc = fem_alloc(f, &f->ctl, 1)) ||
       (rc = fem_alloc(f, &f->st, 1)))
     return rc;
@@ -442,8 +532,7 @@ int launch_pcg(cep_fem *f, const M &m, double *v, double *tact, double t_new, do
 }
 
 int fem_solve_async(cep_fem *f, double *d_v, double *tact, double t_new, double thr) {
-  if (f->format == CEP_FEM_CSR) return launch_pcg(f, csr_view(f), d_v, tact, t_new, thr);
-  return launch_pcg(f, ell_view(f), d_v, tact, t_new, thr);
+  return with_view(f, [&](auto m) { return launch_pcg(f, m, d_v, tact, t_new, thr); });
 }
 
 int fem_check_ctl(cep_fem *f) {
@@ -463,20 +552,21 @@ int fem_autotune(cep_fem *f) {
   const unsigned grid = (unsigned)((f->n + block - 1) / block);
   float best = 1e30f;
   int best_fmt = CEP_FEM_ELL;
-  for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL}) {
-    for (int rep = 0; rep < 2; ++rep) {
+  for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL, CEP_FEM_STENCIL}) {
+    if (fmt == CEP_FEM_STENCIL && !f->sa) continue;
+    f->format = fmt;
+    for (int rep = 0; rep < 4; ++rep) {
       cudaEventRecord(e0, f->stream);
-      for (int k = 0; k < 10; ++k) {
-        if (fmt == CEP_FEM_CSR)
-          spmv_kernel<<<grid, block, 0, f->stream>>>(csr_view(f), 0, (int64_t)f->n, f->p0, f->q);
-        else
-          spmv_kernel<<<grid, block, 0, f->stream>>>(ell_view(f), 0, (int64_t)f->n, f->p0, f->q);
-      }
+      for (int k = 0; k < 20; ++k)
+        with_view(f, [&](auto m) {
+          spmv_kernel<<<grid, block, 0, f->stream>>>(m, 0, (int64_t)f->n, f->p0, f->q);
+          return 0;
+        });
       cudaEventRecord(e1, f->stream);
       cudaEventSynchronize(e1);
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (rep == 1 && ms < best) {
+      if (rep >= 1 && ms < best) {
         best = ms;
         best_fmt = fmt;
       }
@@ -494,7 +584,10 @@ int fem_set_format(cep_fem *f, int format) {
     FEM_CUDA(cudaMemsetAsync(f->p0, 0, sizeof(double) * f->ld, f->stream));
     return fem_autotune(f);
   }
-  if (format != CEP_FEM_CSR && format != CEP_FEM_ELL) return fail_msg(CEP_ERR_ARG, "unknown sparse format %d", format);
+  if (format != CEP_FEM_CSR && format != CEP_FEM_ELL && format != CEP_FEM_STENCIL)
+    return fail_msg(CEP_ERR_ARG, "unknown sparse format %d", format);
+  if (format == CEP_FEM_STENCIL && !f->sa)
+    return fail_msg(CEP_ERR_ARG, "the stencil format needs an operator built on a structured grid");
   f->format = format;
   return CEP_OK;
 }
@@ -539,6 +632,7 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
   f->dt = dt;
   f->stream = (cudaStream_t)stream;
   f->width = dim == 2 ? 9 : 27;
+  f->dim = dim; f->gnx = nx; f->gny = ny; f->gnz = nz;
   // row pointers: neighbours per axis are 1 + (i > 0) + (i < n-1)
   std::vector<int> rp(n + 1);
   int64_t p = 0;
@@ -556,7 +650,8 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
   if ((rc = fem_alloc(f, &f->rp, (size_t)n + 1)) || (rc = fem_alloc(f, &f->col, (size_t)p)) ||
       (rc = fem_alloc(f, &f->a, (size_t)p)) || (rc = fem_alloc(f, &f->b, (size_t)p)) ||
       (rc = fem_alloc(f, &f->ecol, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->ea, (size_t)f->width * f->ld)) ||
-      (rc = fem_alloc(f, &f->eb, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->dinv, (size_t)f->ld))) {
+      (rc = fem_alloc(f, &f->eb, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->dinv, (size_t)f->ld)) ||
+      (rc = fem_alloc(f, &f->sa, (size_t)f->width * f->ld)) || (rc = fem_alloc(f, &f->sb, (size_t)f->width * f->ld))) {
     fem_free(f);
     return rc;
   }
@@ -569,6 +664,11 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
   if (e == cudaSuccess && cep_internal_fem_assemble_grid(dim, nx, ny, nz, h, dt, d_D, n_d, f->rp, f->col, f->a, f->b,
                                                         f->width, f->ld, f->ecol, f->ea, f->eb, f->dinv, f->stream))
     e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    csr_to_stencil_kernel<<<(unsigned)((n + 127) / 128), 128, 0, f->stream>>>(n, nx, ny, dim, f->rp, f->col, f->a, f->b,
+                                                                            f->ld, f->sa, f->sb);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
   cudaFree(d_D);
   if (e != cudaSuccess) {
@@ -681,10 +781,10 @@ int cep_fem_spmv(cep_fem_t f, int which, const double *x, double *y) {
   double *dx = f->q, *dy = f->r;  // scratch vectors of the solver
   FEM_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * f->n, cudaMemcpyHostToDevice, f->stream));
   const unsigned grid = (unsigned)((f->n + 255) / 256);
-  if (f->format == CEP_FEM_CSR)
-    spmv_kernel<<<grid, 256, 0, f->stream>>>(csr_view(f), which ? 1 : 0, (int64_t)f->n, dx, dy);
-  else
-    spmv_kernel<<<grid, 256, 0, f->stream>>>(ell_view(f), which ? 1 : 0, (int64_t)f->n, dx, dy);
+  with_view(f, [&](auto m) {
+    spmv_kernel<<<grid, 256, 0, f->stream>>>(m, which ? 1 : 0, (int64_t)f->n, dx, dy);
+    return 0;
+  });
   FEM_CUDA(cudaGetLastError());
   FEM_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * f->n, cudaMemcpyDeviceToHost, f->stream));
   FEM_CUDA(cudaStreamSynchronize(f->stream));
@@ -800,7 +900,7 @@ int cep_tissue_run(cep_tissue_t t, long n_steps) {
   if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");
   double *v = cep_internal_batch_v(t->cells);
   for (long s = 0; s < n_steps; ++s) {
-    int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->bcl, t->t_crt, t->dur, t->n_pace, 1);
+    int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
     if (rc) return rc;
     t->t += t->dt;
     ++t->steps;

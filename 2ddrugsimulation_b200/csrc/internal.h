@@ -7,12 +7,12 @@
 extern "C" {
 #endif
 
-// One Godunov ionic half-step for a tissue: every node of the batch advances
-// by n_steps fixed steps with the tissue stimulus flag isS1 = mask[i] while
+// One Godunov ionic step of a tissue at tissue time t: every node advances
+// by the batch's dt with the stimulus flag isS1 = mask[i] while
 // iia*bcl + t_crt < t < iia*bcl + t_crt + dur and iia = (int)(t/bcl) < n_pace
-// (heart.cpp:309-323). d_mask is a device array of n bytes.
-int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double bcl, double t_crt,
-                                   double dur, int n_pace, long n_steps);
+// (heart.cpp:309-323). d_mask is a device array of n bytes. Asynchronous.
+int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double t, double bcl, double t_crt,
+                                   double dur, int n_pace);
 // Tissue clock: every instance at t = 0 with no protocol end and biomarkers
 // off; the fixed step is dt.
 int cep_internal_batch_tissue_begin(cep_batch_t b, double dt);

@@ -528,7 +528,7 @@ def tissue_main(args, world, rank, local, pg):
         "config": {"workload": f"2D TT2006 epi sheet {args.nx}x{args.nx} Q1 nodes, dx 0.025 cm, D 0.0013 cm^2/ms, "
                                f"dt 0.01 ms, Jacobi-PCG rtol 1e-8, corner S1 at BCL 1000 ms, IKr Hill block at 3 "
                                f"concentrations (3 sheets per GPU); {args.seg} Godunov steps per sheet per bench step",
-                   "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell"][mixed["fmt"]],
+                   "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell", "stencil"][mixed["fmt"]],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"sheet sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
                  "cg_iters_per_solve": fp64["cg_iters_per_solve"]},

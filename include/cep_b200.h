@@ -169,6 +169,7 @@ typedef struct cep_fem *cep_fem_t;
 #define CEP_FEM_AUTO (-1) /* time both formats on this operator, keep the faster */
 #define CEP_FEM_CSR 0
 #define CEP_FEM_ELL 1     /* column-major ELL, padded to the widest row */
+#define CEP_FEM_STENCIL 2 /* grid operators: 9/27 fixed slots, implicit columns */
 
 /* Structured grid of nx*ny (dim 2, Q1 quadrilaterals) or nx*ny*nz (dim 3,
  * trilinear hexahedra) nodes at spacing h (cm), node id i + nx*(j + ny*k),

@@ -54,12 +54,13 @@ def test_grid_assembly_bitwise(cep, gpu, oracle, dim, shape, kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fmt", ["csr", "ell"])
+@pytest.mark.parametrize("fmt", ["csr", "ell", "stencil"])
 @pytest.mark.parametrize("dim,shape,kind", CASES)
 def test_spmv(cep, gpu, oracle, dim, shape, kind, fmt):
     D = _field(dim, shape, kind, seed=1)
     nx, ny, nz = shape
-    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D, fmt=cep.FEM_CSR if fmt == "csr" else cep.FEM_ELL)
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D,
+                     fmt={"csr": cep.FEM_CSR, "ell": cep.FEM_ELL, "stencil": cep.FEM_STENCIL}[fmt])
     rp, ci, a, b = oracle.fem_assemble(dim, nx, ny, nz, 0.025, 0.01, D)
     x = np.random.default_rng(2).uniform(-90, 30, f.n)
     for which, val in (("A", a), ("B", b)):
@@ -102,9 +103,30 @@ def test_pcg_from_user_csr_and_autotune(cep, gpu, oracle):
     xg, itg, _ = g.solve(v)
     xu, itu, _ = u.solve(v)
     assert itg == itu and np.array_equal(xg, xu)  # same matrix, same order: bitwise
+    with pytest.raises(cep.CepError) as e:
+        u.set_format(cep.FEM_STENCIL)  # no grid behind a user CSR
+    assert e.value.code == cep.ERR_ARG
     u.set_format(cep.FEM_CSR)
     xc, itc, _ = u.solve(v)
     assert itc == itg and np.abs(xc - xg).max() <= 1e-12 * np.abs(xg).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,shape,kind", CASES)
+def test_formats_give_identical_solves(cep, gpu, dim, shape, kind):
+    """ELL and the implicit-column stencil sum each row in the same order, so
+    their solves are bit-identical; CSR rows agree to rounding."""
+    D = _field(dim, shape, kind, seed=7)
+    nx, ny, nz = shape
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D).set_solver(1e-10)
+    v = np.random.default_rng(3).uniform(-90, 30, f.n)
+    out = {}
+    for fmt in (cep.FEM_ELL, cep.FEM_STENCIL, cep.FEM_CSR):
+        f.set_format(fmt)
+        out[fmt] = f.solve(v)
+    assert out[cep.FEM_ELL][1] == out[cep.FEM_STENCIL][1]
+    assert np.array_equal(out[cep.FEM_ELL][0], out[cep.FEM_STENCIL][0])
+    assert np.abs(out[cep.FEM_CSR][0] - out[cep.FEM_ELL][0]).max() <= 1e-9 * np.abs(v).max()
 
 
 @pytest.mark.gpu
