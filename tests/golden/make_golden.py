@@ -102,8 +102,34 @@ def make_cipa(dt: float = 0.005, bcl: float = 1000.0, n_steps: int = 200000, eve
         print("wrote", c["name"])
 
 
+def make_tt2006(dt: float = 0.01, stride: int = 100):
+    """ten Tusscher 2006 epi: the single-cell build (periodic stimulus, two
+    1000-ms beats) and the tissue build (isS1 held for the first 1 ms, then
+    released; 300 ms). The reference model has no drug hook."""
+    r = O.RefCell("tt2006")
+    y0 = r.states.copy()
+    r.L.ref_compute_rates(r.h, 0.0)
+    rates0 = r.arr("rates", r.n).copy()
+    n = int(round(2000.0 / dt))
+    t, v = r.run(0.0, dt, n, stride)
+    np.savez_compressed(OUT / "tt2006_single.npz", dt=dt, stride=stride, n_steps=n, y0=y0, rates0=rates0,
+                        v_trace=v, final_states=r.states.copy(), t_final=t)
+    print("wrote tt2006_single vmax", v.max())
+    r = O.RefCell("tt2006_tissue")
+    r.L.ref_set_s1(r.h, 1)
+    n_on = int(round(1.0 / dt))
+    t, v1 = r.run(0.0, dt, n_on, stride)
+    r.L.ref_set_s1(r.h, 0)
+    n_off = int(round(299.0 / dt))
+    t, v2 = r.run(t, dt, n_off, stride)
+    np.savez_compressed(OUT / "tt2006_tissue.npz", dt=dt, stride=stride, n_on=n_on, n_off=n_off,
+                        v_trace=np.concatenate([v1, v2]), final_states=r.states.copy(), t_final=t)
+    print("wrote tt2006_tissue vmax", max(v1.max(), v2.max()))
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
     make_ord()
     make_cipa()
+    make_tt2006()

@@ -127,3 +127,40 @@ def test_cipa_oracle_rates_bitwise_vs_compiled_reference(oracle):
             assert np.array_equal(r.arr("rates", r.n), mr)
         c.step(t, 0.005)
         t += 0.005
+
+
+def test_tt2006_oracle_matches_reference_golden(oracle):
+    """ten Tusscher 2006 epi, single-cell build: V trace, final STATES and
+    RATES at t = 0 equal the reference's bit for bit."""
+    g = np.load(GOLD / "tt2006_single.npz")
+    c = oracle.Cell("tt2006")
+    assert np.array_equal(c.states, g["y0"])
+    r, _ = c.rates(0.0)
+    assert np.array_equal(r, g["rates0"])
+    t, v = c.run(0.0, float(g["dt"]), int(g["n_steps"]), int(g["stride"]))
+    assert np.array_equal(v, g["v_trace"])
+    assert np.array_equal(c.states, g["final_states"])
+    assert t == float(g["t_final"])
+
+
+def test_tt2006_oracle_tissue_flag_matches_reference_golden(oracle):
+    """The tissue build's stimulus: isS1 held for 1 ms, then released."""
+    g = np.load(GOLD / "tt2006_tissue.npz")
+    c = oracle.Cell("tt2006", tissue_stim=True)
+    c.c.is_s1 = 1
+    t, v1 = c.run(0.0, float(g["dt"]), int(g["n_on"]), int(g["stride"]))
+    c.c.is_s1 = 0
+    t, v2 = c.run(t, float(g["dt"]), int(g["n_off"]), int(g["stride"]))
+    assert np.array_equal(np.concatenate([v1, v2]), g["v_trace"])
+    assert np.array_equal(c.states, g["final_states"])
+
+
+def test_tt2006_oracle_bitwise_vs_compiled_reference(oracle):
+    if not oracle.ref_available("tt2006"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    r = oracle.RefCell("tt2006")
+    c = oracle.Cell("tt2006")
+    t1, v1 = r.run(0.0, 0.01, 150000, 50)
+    t2, v2 = c.run(0.0, 0.01, 150000, 50)
+    assert np.array_equal(v1, v2)
+    assert np.array_equal(r.states, c.states)

@@ -104,3 +104,21 @@ def test_tt2006_biomarkers_fp64_and_mixed(cep, gpu, oracle):
             assert abs(b64[key][k] - r[key]) <= APD_TOL_FP64, (key, k, b64[key][k], r[key])
         assert abs(bmx["apd90"][k] - r["apd90"]) <= APD_TOL_MIXED, (k, bmx["apd90"][k], r["apd90"])
         assert abs(bmx["cad90"][k] - r["cad90"]) <= CAD_TOL_MIXED, (k, bmx["cad90"][k], r["cad90"])
+
+
+@pytest.mark.gpu
+def test_tt2006_fp64_matches_reference_golden(cep, gpu):
+    """Single-cell build of the reference, two beats: the GPU FP64 trace
+    against the reference's own trace."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "tt2006_single.npz")
+    b = cep.Batch("tt2006", 1, "fp64")
+    b.init()
+    assert np.array_equal(b.get_states()[0], g["y0"])
+    b.set_protocol(float(g["dt"]), 3, -1)
+    stride = int(g["stride"])
+    v = np.zeros(len(g["v_trace"]))
+    for k in range(len(v)):
+        b.run(stride)
+        v[k] = b.get_states()[0, 0]
+    assert np.abs(v - g["v_trace"]).max() <= VM_TOL_FP64
