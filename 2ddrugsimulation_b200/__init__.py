@@ -68,6 +68,7 @@ _SIGS = {
                                               ctypes.c_double, ctypes.c_double]),
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "cep_batch_set_states": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int]),
     "cep_batch_get_states": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int]),
     "cep_batch_device_states": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
@@ -215,6 +216,11 @@ class Batch:
 
     def run(self, n_steps: int):
         _check(lib().cep_batch_run(self._h, int(n_steps)))
+        return self
+
+    def step(self, t: float, dt: float, stim_mode: int = -1):
+        """One step of every instance from time t (computeRates + solveAnalytical)."""
+        _check(lib().cep_batch_step(self._h, t, dt, int(stim_mode)))
         return self
 
     def run_to_end(self, steps_per_launch: int = 20000):

@@ -381,8 +381,8 @@ struct TissueArgs {
   int64_t ld;
   int n;
   double t, dt;
-  const unsigned char *mask;
-  int stim_on;  // the window test, uniform over the tissue
+  const unsigned char *mask;  // null: stim_on is the mode of every instance
+  int stim_on;  // the window test, uniform over the tissue (or -1/0/1 without a mask)
 };
 
 template <class M, class P>
@@ -395,7 +395,8 @@ __global__ void __launch_bounds__(128) tissue_kernel(TissueArgs a) {
   M::template load<G>(y, a.y, a.ld, i);
   M::template load_par<G>(q, a.par, a.ld, i);
   typename M::template Cur<G> c;
-  M::template step<P>(y, q, a.t, a.dt, (a.stim_on && a.mask[i]) ? 1 : 0, true, c);
+  const int mode = a.mask ? ((a.stim_on && a.mask[i]) ? 1 : 0) : a.stim_on;
+  M::template step<P>(y, q, a.t, a.dt, mode, true, c);
   M::template store<G>(y, a.y, a.ld, i);
 }
 
@@ -906,6 +907,17 @@ int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {
 double *cep_internal_batch_v(cep_batch_t b) { return b ? b->states : nullptr; }
 void *cep_internal_batch_stream(cep_batch_t b) { return b ? (void *)b->stream : nullptr; }
 int cep_internal_set_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+
+int cep_batch_step(cep_batch_t b, double t, double dt, int stim_mode) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (!(dt > 0) || !std::isfinite(t)) return fail(CEP_ERR_ARG, "bad t or dt");
+  if (stim_mode < -1 || stim_mode > 1) return fail(CEP_ERR_ARG, "stim_mode must be -1, 0 or 1");
+  TissueArgs a;
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = t; a.dt = dt; a.mask = nullptr;
+  a.stim_on = stim_mode;
+  return model_info(b->model)->tissue(b, a);
+}
 
 double cep_qinward(const cep_biomarkers_t *c, const cep_biomarkers_t *d) {
   if (!c || !d) return NAN;

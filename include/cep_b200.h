@@ -134,6 +134,13 @@ int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace,
  * cipa_drug_explicit_bench.cpp:119-127) with the biomarker state machine
  * fused. Asynchronous on the batch's stream. */
 int cep_batch_run(cep_batch_t b, long n_steps);
+/* One fixed step of every instance from time t: the reference's loop body
+ * computeRates(t, ...); solveAnalytical(dt) (cipa_drug_explicit_bench.cpp:
+ * 119-127; heart.cpp:330-360 per node). stim_mode -1: the model's periodic
+ * single-cell stimulus at t; 0/1: the tissue flag isS1 for every instance.
+ * No biomarker bookkeeping and no clock update (the caller owns t).
+ * Asynchronous on the batch's stream. */
+int cep_batch_step(cep_batch_t b, double t, double dt, int stim_mode);
 /* Run to the end of the protocol (blocking). */
 int cep_batch_run_to_end(cep_batch_t b, long steps_per_launch);
 
