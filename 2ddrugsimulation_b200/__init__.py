@@ -95,6 +95,9 @@ _SIGS = {
     "cep_fem_solve_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "cep_fem_stats": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_long),
                                      ctypes.POINTER(ctypes.c_long), _ip, _dp]),
+    "cep_fem_solve_csr_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                 ctypes.c_void_p, ctypes.c_void_p, _ip]),
     "cep_tissue_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "cep_tissue_destroy": (ctypes.c_int, [ctypes.c_void_p]),

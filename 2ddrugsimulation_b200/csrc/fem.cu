@@ -35,6 +35,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -944,3 +945,110 @@ int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ allocation-free solve
+// Jacobi-PCG on a caller-owned device CSR operator with the solver's work
+// vectors in a fixed scratch area of this library (no counterpart in the
+// reference). The scratch is one file-scope device array; its address is
+// resolved once per device (the first call, which must precede any stream
+// capture) and every later call only launches work. Calls that overlap in
+// time on one device share the scratch and race: the caller serialises them.
+namespace {
+
+constexpr int64_t kNaRows = CEP_NOALLOC_MAX_ROWS;
+constexpr int kNaMaxGrid = 1024;
+// dinv, r, z, p0, p1, q | partials [3][kNaMaxGrid] | Ctl | Status
+constexpr int64_t kNaVecWords = 6 * kNaRows;
+constexpr int64_t kNaWords = kNaVecWords + 3 * kNaMaxGrid + 8 + 8;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNaWords];
+
+struct NaDevice {
+  double *base = nullptr;
+  int grid = 0;
+};
+NaDevice g_na_dev[64];
+std::mutex g_na_mu;
+
+__global__ void noalloc_dinv_kernel(int64_t n, const int *rp, const int *col, const double *a, double *dinv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double diag = 1.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k)
+    if (col[k] == i) diag = a[k];
+  dinv[i] = 1.0 / diag;
+}
+
+}  // namespace
+
+extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const void *d_col_idx, const void *d_a_val,
+                                         const void *d_b_val, double dt, double rtol, int max_iter, void *d_v,
+                                         void *stream, int *iters_out) {
+  if (!d_row_ptr || !d_col_idx || !d_a_val || !d_b_val || !d_v) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (n <= 0 || n > CEP_NOALLOC_MAX_ROWS)
+    return fail_msg(CEP_ERR_ARG, "n = %d outside 1..%d (CEP_NOALLOC_MAX_ROWS)", n, CEP_NOALLOC_MAX_ROWS);
+  if (!(dt > 0) || !(rtol > 0) || max_iter <= 0) return fail_msg(CEP_ERR_ARG, "dt, rtol and max_iter must be positive");
+  int dev = 0;
+  FEM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail_msg(CEP_ERR_ARG, "device %d out of range", dev);
+  NaDevice nd;
+  {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (!g_na_dev[dev].base) {  // set-up: once per device
+      void *p = nullptr;
+      FEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      int sms = 0, per_sm = 0;
+      FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<CsrView>, kPcgBlock, 0));
+      if (per_sm < 1) return fail_msg(CEP_ERR_CUDA, "PCG kernel does not fit on an SM");
+      g_na_dev[dev].grid = std::min(sms, kNaMaxGrid);
+      g_na_dev[dev].base = static_cast<double *>(p);
+    }
+    nd = g_na_dev[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  double *base = nd.base;
+  double *dinv = base, *r = base + kNaRows, *z = base + 2 * kNaRows, *p0 = base + 3 * kNaRows,
+         *p1 = base + 4 * kNaRows, *q = base + 5 * kNaRows, *part = base + kNaVecWords;
+  Ctl *ctl = reinterpret_cast<Ctl *>(part + 3 * kNaMaxGrid);
+  Status *stat = reinterpret_cast<Status *>(part + 3 * kNaMaxGrid + 8);
+  // the same grid rule as an operator handle: one block per SM, no more
+  // blocks than rows need
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nd.grid, (n + kPcgBlock - 1) / kPcgBlock));
+  // what must start at zero: the barrier words and the counters
+  FEM_CUDA(cudaMemsetAsync(ctl, 0, sizeof(Ctl), st));
+  FEM_CUDA(cudaMemsetAsync(stat, 0, sizeof(Status), st));
+  const CsrView m{static_cast<const int *>(d_row_ptr), static_cast<const int *>(d_col_idx),
+                  static_cast<const double *>(d_a_val), static_cast<const double *>(d_b_val)};
+  noalloc_dinv_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, m.rp, m.col, m.a, dinv);
+  FEM_CUDA(cudaGetLastError());
+  PcgArgs a;
+  a.n = n;
+  a.dt = dt;
+  a.rtol = rtol;
+  a.max_iter = max_iter;
+  a.precond_norm = 1;
+  a.v = static_cast<double *>(d_v);
+  a.dinv = dinv;
+  a.r = r; a.z = z; a.p0 = p0; a.p1 = p1; a.q = q;
+  a.part = part;
+  a.ctl = ctl;
+  a.st = stat;
+  a.tact = nullptr;
+  a.t_new = 0.0;
+  a.act_thr = 0.0;
+  CsrView mm = m;
+  void *args[] = {&mm, &a};
+  FEM_CUDA(cudaLaunchCooperativeKernel((const void *)pcg_kernel<CsrView>, dim3(grid), dim3(kPcgBlock), args, 0, st));
+  if (iters_out) {  // blocking status read
+    Ctl c;
+    Status s;
+    FEM_CUDA(cudaMemcpyAsync(&c, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA(cudaMemcpyAsync(&s, stat, sizeof(Status), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA(cudaStreamSynchronize(st));
+    if (c.err) return fail_msg(CEP_ERR_TIMEOUT, "PCG grid barrier ran out of its spin limit");
+    *iters_out = s.last_iters;
+    if (s.last_iters < 0) return fail_msg(CEP_ERR_NOT_CONVERGED, "PCG hit max_iter (%d)", max_iter);
+  }
+  return CEP_OK;
+}

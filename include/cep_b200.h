@@ -213,6 +213,24 @@ int cep_fem_solve_device(cep_fem_t f, void *d_v);
 int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves, int *not_converged,
                   double *last_res);
 
+/* Allocation-free solve. No counterpart in the reference. One implicit
+ * diffusion step A V = B V / dt, Jacobi-PCG from a zero guess with the
+ * default stopping rule (preconditioned norm), for a CSR operator the
+ * caller keeps in device memory (d_row_ptr[n+1], d_col_idx/d_a_val/
+ * d_b_val[nnz], sorted columns), in place on the device vector d_v[n].
+ * Nothing is allocated or freed: the solver's work vectors live in a fixed
+ * device scratch area of the library sized for CEP_NOALLOC_MAX_ROWS rows
+ * (larger n is rejected with CEP_ERR_ARG). The first call on a device
+ * resolves that area and must come before any stream capture. Calls that
+ * overlap in time on one device (two streams or two host threads) share
+ * the scratch and race: serialise them. Asynchronous on `stream` unless
+ * iters_out is non-null, in which case the call waits and stores the
+ * iteration count (CEP_ERR_NOT_CONVERGED past max_iter). */
+#define CEP_NOALLOC_MAX_ROWS 262144
+int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const void *d_col_idx, const void *d_a_val,
+                              const void *d_b_val, double dt, double rtol, int max_iter, void *d_v, void *stream,
+                              int *iters_out);
+
 /* ---------------------------------------------------------------- tissue */
 /* Godunov-split monodomain tissue: per step every node's ionic update (the
  * batch, one instance per node, tissue stimulus flag isS1) then the implicit
