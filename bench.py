@@ -52,7 +52,7 @@ BCL = 2000.0
 # oracle/_build/opcount <model> 1 1000` (profiles/opcount_ionic_models.txt).
 # flop = one add/sub, mul, div or elementary-function evaluation.
 OPS = {
-    "cipa2017": dict(add=509.97, mul=517.99, div=269.99, exp=109.0, log=3.0, pow=1.0),
+    "cipa2017": dict(add=520.97, mul=561.99, div=270.99, exp=123.0, log=3.0, pow=1.0),
     "ord2011": dict(add=474.97, mul=435.99, div=281.99, exp=100.0, log=3.0, pow=1.0),
 }
 # DRAM bytes per launch per instance measured by ncu on the run kernel

@@ -56,7 +56,7 @@ CMP(<) CMP(>) CMP(<=) CMP(>=) CMP(==) CMP(!=)
     if (g_on && !a.k) g_cnt.field++;                                         \
     return mk(std::name(a.v), a.k);                                          \
   }
-UN(exp, ex) UN(log, lg) UN(sqrt, sq) UN(floor, fl) UN(fabs, cmp)
+UN(exp, ex) UN(log, lg) UN(sqrt, sq) UN(floor, fl) UN(ceil, fl) UN(fabs, cmp)
 #undef UN
 static inline od pow(od a, od b) {
   if (g_on && !(a.k && b.k)) {
