@@ -22,7 +22,7 @@ LIB_PATH = PKG / "lib" / "libcep_b200.so"
 # status codes (cep_b200.h)
 OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_NOT_CONVERGED, ERR_TIMEOUT, ERR_NONFINITE, ERR_UNSUPPORTED, ERR_STATE, \
     ERR_NO_DEVICE = range(10)
-INST_RUNNING, INST_DONE, INST_NONFINITE = 0, 1, 2
+INST_RUNNING, INST_DONE, INST_NONFINITE, INST_IDLE = 0, 1, 2, 3
 MODELS = {"ord2011": 0, "cipa2017": 1, "tt2006": 2, "tt2004": 3, "tomek2019": 4}
 N_STATES = {"ord2011": 41, "cipa2017": 49, "tt2006": 19, "tt2004": 17, "tomek2019": 43}
 PREC = {"fp64": 0, "mixed": 1}
@@ -38,6 +38,27 @@ class Biomarkers(ctypes.Structure):
     _fields_ = [(f, ctypes.c_double) for f in BM_FIELDS] + [
         ("steepest_pace", ctypes.c_int32), ("n_eligible", ctypes.c_int32), ("status", ctypes.c_int32),
         ("reserved", ctypes.c_int32)]
+
+
+class CepJob(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("celltype", ctypes.POINTER(ctypes.c_double)),
+                ("conc", ctypes.POINTER(ctypes.c_double)), ("hill", ctypes.POINTER(ctypes.c_double)),
+                ("hill_stride", ctypes.c_int), ("bcl", ctypes.c_double), ("n_pace", ctypes.c_int),
+                ("first_pace", ctypes.c_int), ("flags", ctypes.c_uint)]
+
+
+class JobTimes(ctypes.Structure):
+    _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("cell_steps", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_int), ("queued", ctypes.c_int), ("running", ctypes.c_int),
+                ("slots_used", ctypes.c_int), ("completed", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+                ("cell_steps", ctypes.c_double), ("busy_ms", ctypes.c_double), ("wall_ms", ctypes.c_double)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 
 
 class CepError(RuntimeError):
@@ -79,6 +100,27 @@ _SIGS = {
                                            _dp]),
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
+    "cep_batch_reserve_biomarkers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_double]),
+    "cep_batch_init_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int,
+                                            ctypes.c_uint]),
+    "cep_batch_set_pacing_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "cep_batch_start_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "cep_batch_release_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "cep_batch_get_biomarkers_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.POINTER(Biomarkers)]),
+    "cep_serve_start": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_long, ctypes.c_double, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_serve_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CepJob), ctypes.POINTER(ctypes.c_uint64)]),
+    "cep_serve_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _ip]),
+    "cep_serve_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double]),
+    "cep_serve_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Biomarkers),
+                                        ctypes.POINTER(JobTimes)]),
+    "cep_serve_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "cep_serve_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServeStats)]),
+    "cep_serve_stop": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_qinward": (ctypes.c_double, [ctypes.POINTER(Biomarkers), ctypes.POINTER(Biomarkers)]),
     "cep_fem_create_grid": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
@@ -449,3 +491,72 @@ class Tissue:
         nc = ctypes.c_int()
         _check(lib().cep_tissue_stats(self._h, ctypes.byref(t), ctypes.byref(st), ctypes.byref(it), ctypes.byref(nc)))
         return {"time": t.value, "steps": st.value, "cg_iters": it.value, "not_converged": nc.value}
+
+
+class Server:
+    """Screening-job server with continuous batching (one resident pool)."""
+
+    def __init__(self, model: str, precision: str = "mixed", capacity: int = 0, dt: float = 0.005,
+                 dt_write: float = 1.0, max_bcl: float = 2000.0, steps_per_launch: int = 10000,
+                 hbm_fraction: float = 0.8, stream: int | None = None):
+        h = ctypes.c_void_p()
+        _check(lib().cep_serve_start(MODELS[model], PREC[precision], capacity, dt, dt_write, max_bcl,
+                                     steps_per_launch, hbm_fraction, stream, ctypes.byref(h)))
+        self._h = h
+        self.model = model
+        self._n = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cep_serve_stop(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, conc, hill=None, bcl: float = 1000.0, n_pace: int = 1, first_pace: int = 0,
+               celltype=None, quirks: bool = True, dutta: bool = False) -> int:
+        cc = np.ascontiguousarray(conc, np.float64)
+        n = len(cc)
+        hh = None
+        if hill is not None:
+            hh = np.asarray(hill, np.float64)
+            hh = np.ascontiguousarray(np.broadcast_to(hh, (n, hh.shape[-1])))
+        ct = None if celltype is None else np.ascontiguousarray(np.broadcast_to(celltype, (n,)), np.float64)
+        job = CepJob(n, _dptr(ct), _dptr(cc), _dptr(hh), 0 if hh is None else hh.shape[1], bcl, n_pace, first_pace,
+                     (FLAG_QUIRKS if quirks else 0) | (FLAG_DUTTA if dutta else 0))
+        jid = ctypes.c_uint64()
+        _check(lib().cep_serve_submit(self._h, ctypes.byref(job), ctypes.byref(jid)))
+        self._n[jid.value] = n
+        return jid.value
+
+    def poll(self, jid: int) -> int:
+        st = ctypes.c_int()
+        _check(lib().cep_serve_poll(self._h, jid, ctypes.byref(st)))
+        return st.value
+
+    def wait(self, jid: int, timeout_s: float = 0.0) -> None:
+        _check(lib().cep_serve_wait(self._h, jid, timeout_s))
+
+    def result(self, jid: int) -> tuple[dict, dict]:
+        n = self._n[jid]
+        arr = (Biomarkers * n)()
+        t = JobTimes()
+        _check(lib().cep_serve_result(self._h, jid, arr, ctypes.byref(t)))
+        raw = np.ctypeslib.as_array(arr)
+        out = {f: np.array(raw[f]) for f in BM_FIELDS}
+        for f in ("steepest_pace", "n_eligible", "status"):
+            out[f] = np.array(raw[f])
+        return out, {k: getattr(t, k) for k, _ in JobTimes._fields_}
+
+    def release(self, jid: int) -> None:
+        _check(lib().cep_serve_release(self._h, jid))
+        self._n.pop(jid, None)
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(lib().cep_serve_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServeStats._fields_}

@@ -157,19 +157,23 @@ struct Tt06Model {
 };
 
 // ----------------------------------------------------------------- kernels
+// Instance ranges: every set-up kernel works on [first, first + count);
+// the per-range inputs (celltype, conc, hill rows) are indexed from 0.
 template <class M>
-__global__ void init_kernel(double *par, double *s, int64_t ld, int n, const double *celltype,
+__global__ void init_kernel(double *par, double *s, int64_t ld, int64_t first, int count, const double *celltype,
                             const double *conc, const double *hill, int hill_stride, unsigned flags) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  M::init(par, s, ld, i, celltype ? celltype[i] : 0.0, conc ? conc[i] : 0.0,
-          hill ? hill + i * hill_stride : nullptr, flags);
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int64_t i = first + k;
+  M::init(par, s, ld, i, celltype ? celltype[k] : 0.0, conc ? conc[k] : 0.0,
+          hill ? hill + k * hill_stride : nullptr, flags);
 }
 
-__global__ void pacing_kernel(double *par, int64_t ld, int n, int p_bcl, int p_start, int p_dur, int p_amp,
-                              double bcl, double start, double dur, double amp_scale) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__global__ void pacing_kernel(double *par, int64_t ld, int64_t first, int count, int p_bcl, int p_start, int p_dur,
+                              int p_amp, double bcl, double start, double dur, double amp_scale) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int64_t i = first + k;
   par[p_bcl * ld + i] = bcl;
   if (start >= 0) par[p_start * ld + i] = start;
   if (dur >= 0) par[p_dur * ld + i] = dur;
@@ -193,9 +197,10 @@ struct RunArgs {
   int stim_mode;  // -1 periodic; 0/1 fixed tissue flag
 };
 
-__global__ void reset_kernel(RunArgs a, int p_bcl, int p_start, int cai_idx) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+__global__ void reset_kernel(RunArgs a, int64_t first, int count, int p_bcl, int p_start, int cai_idx) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int64_t i = first + k;
   a.t[i] = 0.0;
   a.iout[i] = 0;
   a.status[i] = CEP_INST_RUNNING;
@@ -420,9 +425,10 @@ __global__ void rates_kernel(const double *s, const double *par, int64_t ld, int
   }
 }
 
-__global__ void collect_bm_kernel(bm::View v, const int *status, int n, cep_biomarkers_t *out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__global__ void collect_bm_kernel(bm::View v, const int *status, int64_t first, int count, cep_biomarkers_t *out) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int64_t i = first + k;
   cep_biomarkers_t r;
   const int S = bm::F_S0;
   r.qnet = v.F(S + bm::B_qnet, i) / 1000.0;
@@ -446,27 +452,29 @@ __global__ void collect_bm_kernel(bm::View v, const int *status, int n, cep_biom
   r.n_eligible = v.I(bm::I_n_elig, i);
   r.status = status[i];
   r.reserved = 0;
-  out[i] = r;
+  out[k] = r;
 }
 
 // ------------------------------------------------------------- dispatch
 template <class M>
 struct Ops {
-  static int launch_init(cep_batch *b, const double *ct, const double *conc, const double *hill, int hs,
-                         unsigned flags) {
-    const int grid = (b->n + kBlock - 1) / kBlock;
-    init_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->params, b->states, b->ld, b->n, ct, conc, hill, hs, flags);
+  static int launch_init(cep_batch *b, int64_t first, int count, const double *ct, const double *conc,
+                         const double *hill, int hs, unsigned flags) {
+    const int grid = (count + kBlock - 1) / kBlock;
+    init_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->params, b->states, b->ld, first, count, ct, conc, hill, hs,
+                                                   flags);
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "init launch failed");
   }
-  static int launch_pacing(cep_batch *b, double bcl, double start, double dur, double amp) {
-    const int grid = (b->n + kBlock - 1) / kBlock;
-    pacing_kernel<<<grid, kBlock, 0, b->stream>>>(b->params, b->ld, b->n, M::p_bcl(), M::p_stim_start(),
+  static int launch_pacing(cep_batch *b, int64_t first, int count, double bcl, double start, double dur,
+                           double amp) {
+    const int grid = (count + kBlock - 1) / kBlock;
+    pacing_kernel<<<grid, kBlock, 0, b->stream>>>(b->params, b->ld, first, count, M::p_bcl(), M::p_stim_start(),
                                                   M::p_duration(), M::p_amp(), bcl, start, dur, amp);
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "pacing launch failed");
   }
-  static int launch_reset(cep_batch *b, const RunArgs &a) {
-    const int grid = (b->n + kBlock - 1) / kBlock;
-    reset_kernel<<<grid, kBlock, 0, b->stream>>>(a, M::p_bcl(), M::p_stim_start(), M::kCai);
+  static int launch_reset(cep_batch *b, const RunArgs &a, int64_t first, int count) {
+    const int grid = (count + kBlock - 1) / kBlock;
+    reset_kernel<<<grid, kBlock, 0, b->stream>>>(a, first, count, M::p_bcl(), M::p_stim_start(), M::kCai);
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "reset launch failed");
   }
   static int launch_run(cep_batch *b, const RunArgs &a) {
@@ -512,9 +520,9 @@ struct Ops {
 
 struct ModelInfo {
   int ns, np, cai;
-  int (*init)(cep_batch *, const double *, const double *, const double *, int, unsigned);
-  int (*pacing)(cep_batch *, double, double, double, double);
-  int (*reset)(cep_batch *, const RunArgs &);
+  int (*init)(cep_batch *, int64_t, int, const double *, const double *, const double *, int, unsigned);
+  int (*pacing)(cep_batch *, int64_t, int, double, double, double, double);
+  int (*reset)(cep_batch *, const RunArgs &, int64_t, int);
   int (*run)(cep_batch *, const RunArgs &);
   int (*rates)(cep_batch *, double, double *, double *);
   int p_bcl;
@@ -688,7 +696,7 @@ int cep_batch_init(cep_batch_t b, const double *celltype, const double *conc, co
   CEP_CUDA(cudaMemcpyAsync(d_ct, celltype ? celltype : zeros.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
   CEP_CUDA(cudaMemcpyAsync(d_conc, conc ? conc : zeros.data(), sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
   if (hill) CEP_CUDA(cudaMemcpyAsync(d_hill, hill, bytes_h, cudaMemcpyHostToDevice, b->stream));
-  int rc = mi->init(b, d_ct, d_conc, d_hill, hill_stride, flags);
+  int rc = mi->init(b, 0, b->n, d_ct, d_conc, d_hill, hill_stride, flags);
   CEP_CUDA(cudaFreeAsync(d_ct, b->stream));
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   if (rc) return rc;
@@ -700,7 +708,7 @@ int cep_batch_set_pacing(cep_batch_t b, double bcl, double stim_start, double st
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
   if (!(bcl > 0) || !std::isfinite(bcl)) return fail(CEP_ERR_ARG, "bcl must be positive");
-  return model_info(b->model)->pacing(b, bcl, stim_start, stim_dur, amp_scale);
+  return model_info(b->model)->pacing(b, 0, b->n, bcl, stim_start, stim_dur, amp_scale);
 }
 
 int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,
@@ -743,7 +751,7 @@ int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace,
   }
   b->has_protocol = true;
   RunArgs a = make_args(b, 0);
-  int rc = mi->reset(b, a);
+  int rc = mi->reset(b, a, 0, b->n);
   if (rc) return rc;
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;
@@ -827,7 +835,7 @@ int cep_batch_get_biomarkers(cep_batch_t b, cep_biomarkers_t *out) {
   cep_biomarkers_t *d = nullptr;
   CEP_CUDA(cudaMallocAsync((void **)&d, sizeof(cep_biomarkers_t) * b->n, b->stream));
   bm::View v{b->bmf, b->bmi, b->ca_t, b->ca_v, b->ca_cap, b->ld};
-  collect_bm_kernel<<<(b->n + kBlock - 1) / kBlock, kBlock, 0, b->stream>>>(v, b->status, b->n, d);
+  collect_bm_kernel<<<(b->n + kBlock - 1) / kBlock, kBlock, 0, b->stream>>>(v, b->status, 0, b->n, d);
   CEP_CUDA(cudaGetLastError());
   CEP_CUDA(cudaMemcpyAsync(out, d, sizeof(cep_biomarkers_t) * b->n, cudaMemcpyDeviceToHost, b->stream));
   CEP_CUDA(cudaFreeAsync(d, b->stream));
@@ -838,6 +846,142 @@ int cep_batch_get_biomarkers(cep_batch_t b, cep_biomarkers_t *out) {
 int cep_batch_get_status(cep_batch_t b, int32_t *status) {
   if (!b || !status) return fail(CEP_ERR_ARG, "null argument");
   CEP_CUDA(cudaMemcpyAsync(status, b->status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+// ------------------------------------------------------ instance ranges
+namespace {
+int check_range(cep_batch_t b, int first, int count) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (first < 0 || count <= 0 || (int64_t)first + count > b->n)
+    return fail(CEP_ERR_ARG, "range [%d, %d) outside the batch of %d", first, first + count, b->n);
+  return CEP_OK;
+}
+__global__ void fill_status_kernel(int *status, int64_t first, int count, int value) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count) status[first + k] = value;
+}
+}  // namespace
+
+int cep_batch_reserve_biomarkers(cep_batch_t b, int max_samples_per_beat, double dt, double dt_write,
+                                 double qnet_vm_threshold) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (max_samples_per_beat < 1 || !(dt > 0) || !(dt_write > 0)) return fail(CEP_ERR_ARG, "bad reservation");
+  int rc;
+  if (!b->bmf && ((rc = dev_alloc(b, &b->bmf, (size_t)bm::kNumF * b->ld)) ||
+                  (rc = dev_alloc(b, &b->bmi, (size_t)bm::kNumI * b->ld))))
+    return rc;
+  if (max_samples_per_beat + 2 > b->ca_cap) {
+    b->ca_cap = max_samples_per_beat + 2;
+    if ((rc = dev_alloc(b, &b->ca_t, (size_t)b->ca_cap * b->ld)) || (rc = dev_alloc(b, &b->ca_v, (size_t)b->ca_cap * b->ld)))
+      return rc;
+  }
+  b->dt = dt;
+  b->dt_write = dt_write;
+  b->qnet_thr = qnet_vm_threshold;
+  b->first_pace = 0;  // biomarkers possible; each instance's own first pace decides
+  b->has_protocol = true;
+  // every slot starts released
+  fill_status_kernel<<<(b->n + 255) / 256, 256, 0, b->stream>>>(b->status, 0, b->n, CEP_INST_IDLE);
+  CEP_CUDA(cudaGetLastError());
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_init_range(cep_batch_t b, int first, int count, const double *celltype, const double *conc,
+                         const double *hill, int hill_stride, unsigned flags) {
+  int rc = check_range(b, first, count);
+  if (rc) return rc;
+  if (hill && hill_stride < 14) return fail(CEP_ERR_ARG, "hill_stride must be >= 14 (got %d)", hill_stride);
+  if (conc)
+    for (int k = 0; k < count; ++k)
+      if (!(conc[k] >= 0.0) || !std::isfinite(conc[k]))
+        return fail(CEP_ERR_ARG, "conc[%d] = %g is not a finite non-negative value", k, conc[k]);
+  if (hill)
+    for (int k = 0; k < count; ++k)
+      for (int j = 0; j < 14; ++j)
+        if (!std::isfinite(hill[(size_t)k * hill_stride + j]) || hill[(size_t)k * hill_stride + j] < 0.0)
+          return fail(CEP_ERR_ARG, "hill[%d][%d] is not a finite non-negative value", k, j);
+  const size_t bytes_h = hill ? (size_t)count * hill_stride * sizeof(double) : 0;
+  double *d = nullptr;
+  CEP_CUDA(cudaMallocAsync((void **)&d, sizeof(double) * count * 2 + bytes_h + 64, b->stream));
+  double *d_ct = d, *d_conc = d + count, *d_hill = hill ? d + 2 * count : nullptr;
+  std::vector<double> zeros;
+  if (!celltype || !conc) zeros.assign(count, 0.0);
+  CEP_CUDA(cudaMemcpyAsync(d_ct, celltype ? celltype : zeros.data(), sizeof(double) * count, cudaMemcpyHostToDevice, b->stream));
+  CEP_CUDA(cudaMemcpyAsync(d_conc, conc ? conc : zeros.data(), sizeof(double) * count, cudaMemcpyHostToDevice, b->stream));
+  if (hill) CEP_CUDA(cudaMemcpyAsync(d_hill, hill, bytes_h, cudaMemcpyHostToDevice, b->stream));
+  rc = model_info(b->model)->init(b, first, count, d_ct, d_conc, d_hill, hill_stride, flags);
+  CEP_CUDA(cudaFreeAsync(d, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  if (!rc) b->initialized = true;
+  return rc;
+}
+
+int cep_batch_set_pacing_range(cep_batch_t b, int first, int count, double bcl, double stim_start, double stim_dur,
+                               double amp_scale) {
+  int rc = check_range(b, first, count);
+  if (rc) return rc;
+  if (!(bcl > 0) || !std::isfinite(bcl)) return fail(CEP_ERR_ARG, "bcl must be positive");
+  return model_info(b->model)->pacing(b, first, count, bcl, stim_start, stim_dur, amp_scale);
+}
+
+int cep_batch_start_range(cep_batch_t b, int first, int count, int n_pace, int first_pace) {
+  int rc = check_range(b, first, count);
+  if (rc) return rc;
+  if (!b->has_protocol) return fail(CEP_ERR_STATE, "cep_batch_reserve_biomarkers or cep_batch_set_protocol first");
+  if (n_pace <= 0 || first_pace >= n_pace) return fail(CEP_ERR_ARG, "bad protocol (n_pace=%d first_pace=%d)", n_pace, first_pace);
+  if (first_pace >= 0 && !b->bmf) return fail(CEP_ERR_STATE, "biomarkers were not reserved");
+  const ModelInfo *mi = model_info(b->model);
+  std::vector<double> bcl(count);
+  CEP_CUDA(cudaMemcpyAsync(bcl.data(), b->params + (size_t)mi->p_bcl * b->ld + first, sizeof(double) * count,
+                           cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  const double dt = b->dt;
+  const int print_freq = (int)((1. / dt) * b->dt_write);
+  std::vector<int> sc((size_t)4 * count);
+  for (int k = 0; k < count; ++k) {
+    sc[k] = (int)((n_pace * bcl[k]) / dt);
+    sc[count + k] = (int)(bcl[k] / dt);
+    sc[2 * count + k] = print_freq;
+    sc[3 * count + k] = first_pace;
+    const int per_beat = print_freq > 0 ? sc[count + k] / print_freq + 2 : 2;
+    if (first_pace >= 0 && per_beat > b->ca_cap)
+      return fail(CEP_ERR_ARG, "BCL %g needs %d Ca samples per beat, %d reserved", bcl[k], per_beat, b->ca_cap);
+  }
+  for (int r = 0; r < 4; ++r)
+    CEP_CUDA(cudaMemcpyAsync(b->sched + (size_t)r * b->ld + first, sc.data() + (size_t)r * count, sizeof(int) * count,
+                             cudaMemcpyHostToDevice, b->stream));
+  RunArgs a = make_args(b, 0);
+  a.bm_on = b->bmf ? 1 : 0;
+  rc = mi->reset(b, a, first, count);
+  if (rc) return rc;
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_release_range(cep_batch_t b, int first, int count) {
+  int rc = check_range(b, first, count);
+  if (rc) return rc;
+  fill_status_kernel<<<(count + 255) / 256, 256, 0, b->stream>>>(b->status, first, count, CEP_INST_IDLE);
+  CEP_CUDA(cudaGetLastError());
+  return CEP_OK;
+}
+
+int cep_batch_get_biomarkers_range(cep_batch_t b, int first, int count, cep_biomarkers_t *out) {
+  int rc = check_range(b, first, count);
+  if (rc) return rc;
+  if (!out) return fail(CEP_ERR_ARG, "null argument");
+  if (!b->bmf) return fail(CEP_ERR_STATE, "biomarkers are off");
+  cep_biomarkers_t *d = nullptr;
+  CEP_CUDA(cudaMallocAsync((void **)&d, sizeof(cep_biomarkers_t) * count, b->stream));
+  bm::View v{b->bmf, b->bmi, b->ca_t, b->ca_v, b->ca_cap, b->ld};
+  collect_bm_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, b->stream>>>(v, b->status, first, count, d);
+  CEP_CUDA(cudaGetLastError());
+  CEP_CUDA(cudaMemcpyAsync(out, d, sizeof(cep_biomarkers_t) * count, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaFreeAsync(d, b->stream));
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;
 }
@@ -898,7 +1042,7 @@ int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {
   b->has_protocol = true;
   RunArgs a = make_args(b, 0);
   a.bm_on = 0;
-  int rc = model_info(b->model)->reset(b, a);
+  int rc = model_info(b->model)->reset(b, a, 0, b->n);
   if (rc) return rc;
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;

@@ -1,0 +1,376 @@
+// Screening-job server with continuous batching: the cep_serve_* C ABI
+// (include/cep_b200.h). No counterpart in the reference, which runs one job
+// per MPI process (cipa_drug_bench.cpp).
+//
+// One resident batch is a pool of slots in HBM. A job is a list of
+// instances (samples x concentrations, each with its Hill row) and occupies
+// a contiguous slot range from admission to completion. A scheduler thread
+// loops:
+//   1. admit queued jobs, in arrival order, into the first free range that
+//      fits (a later, smaller job may pass a larger one that does not fit
+//      yet); admission initialises, paces and starts only that range;
+//   2. launch one run of K steps over the whole pool: every running slot
+//      advances, whatever job it belongs to and wherever that job is in its
+//      protocol; idle and finished slots return at once;
+//   3. read the per-slot status words; a job whose slots are all finished
+//      has its biomarkers collected and its range released.
+// Each instance's arithmetic does not depend on its neighbours, so a job's
+// results are bit-identical alone or in any mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/cep_b200.h"
+#include "internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  uint64_t id = 0;
+  int n = 0;
+  std::vector<double> celltype, conc, hill;
+  int hill_stride = 0;
+  double bcl = 1000.0;
+  int n_pace = 1, first_pace = 0;
+  unsigned flags = 0;
+  int first = -1;  // slot range while admitted
+  int state = CEP_JOB_QUEUED;
+  int error = CEP_OK;
+  std::vector<cep_biomarkers_t> result;
+  Clock::time_point t_submit, t_admit, t_done;
+  long long steps = 0;  // instance-steps of the whole job
+};
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct cep_server {
+  int model = 0, precision = 0, capacity = 0;
+  double dt = 0.005, dt_write = 1.0;
+  int max_per_beat = 0;
+  long steps_per_launch = 10000;
+  cep_batch_t pool = nullptr;
+  std::vector<int> owner;  // slot occupied (1) or free (-1)
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Job>> queue;
+  std::map<uint64_t, std::shared_ptr<Job>> jobs;
+  std::vector<std::shared_ptr<Job>> running;
+  uint64_t next_id = 1;
+  bool stop = false;
+  int fatal = CEP_OK;
+  std::thread worker;
+  long long launches = 0, steps_done = 0, completed = 0;
+  Clock::time_point t_start;
+  double busy_ms = 0.0;
+};
+
+namespace {
+
+// first free contiguous range of n slots
+int find_range(const std::vector<int> &owner, int n) {
+  int run = 0;
+  for (int i = 0; i < (int)owner.size(); ++i) {
+    run = owner[i] < 0 ? run + 1 : 0;
+    if (run == n) return i - n + 1;
+  }
+  return -1;
+}
+
+int admit(cep_server *s, Job &j) {
+  int rc;
+  if ((rc = cep_batch_init_range(s->pool, j.first, j.n, j.celltype.empty() ? nullptr : j.celltype.data(),
+                                 j.conc.data(), j.hill.empty() ? nullptr : j.hill.data(), j.hill_stride, j.flags)))
+    return rc;
+  if ((rc = cep_batch_set_pacing_range(s->pool, j.first, j.n, j.bcl, -1.0, -1.0, 1.0))) return rc;
+  return cep_batch_start_range(s->pool, j.first, j.n, j.n_pace, j.first_pace);
+}
+
+void fail_all(cep_server *s, int rc) {
+  s->fatal = rc;
+  for (auto &j : s->running) {
+    j->state = CEP_JOB_FAILED;
+    j->error = rc;
+  }
+  for (auto &j : s->queue) {
+    j->state = CEP_JOB_FAILED;
+    j->error = rc;
+  }
+  s->running.clear();
+  s->queue.clear();
+  s->stop = true;
+  s->cv_done.notify_all();
+}
+
+void worker_loop(cep_server *s) {
+  std::vector<int32_t> status(s->capacity);
+  for (;;) {
+    std::vector<std::shared_ptr<Job>> admitted;
+    {
+      std::unique_lock<std::mutex> lock(s->mu);
+      s->cv_work.wait(lock, [&] { return s->stop || !s->queue.empty() || !s->running.empty(); });
+      if (s->stop) return;
+      for (auto it = s->queue.begin(); it != s->queue.end();) {
+        const int first = find_range(s->owner, (*it)->n);
+        if (first < 0) {
+          ++it;
+          continue;
+        }
+        (*it)->first = first;
+        for (int k = 0; k < (*it)->n; ++k) s->owner[first + k] = 1;
+        admitted.push_back(*it);
+        it = s->queue.erase(it);
+      }
+    }
+    for (auto &j : admitted) {
+      const int rc = admit(s, *j);
+      std::lock_guard<std::mutex> lock(s->mu);
+      j->t_admit = Clock::now();
+      if (rc) {
+        j->state = CEP_JOB_FAILED;
+        j->error = rc;
+        for (int k = 0; k < j->n; ++k) s->owner[j->first + k] = -1;
+        cep_batch_release_range(s->pool, j->first, j->n);
+        s->cv_done.notify_all();
+      } else {
+        j->state = CEP_JOB_RUNNING;
+        s->running.push_back(j);
+      }
+    }
+    {
+      std::lock_guard<std::mutex> lock(s->mu);
+      if (s->running.empty()) continue;
+    }
+    const auto t0 = Clock::now();
+    int rc = cep_batch_run(s->pool, s->steps_per_launch);
+    if (!rc) rc = cep_batch_get_status(s->pool, status.data());
+    const auto t1 = Clock::now();
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->busy_ms += ms_between(t0, t1);
+    s->launches += 1;
+    if (rc) {  // the device is unusable: fail every job and stop
+      fail_all(s, rc);
+      return;
+    }
+    for (auto it = s->running.begin(); it != s->running.end();) {
+      Job &j = **it;
+      bool done = true;
+      for (int k = 0; k < j.n && done; ++k) done = status[j.first + k] != CEP_INST_RUNNING;
+      if (!done) {
+        ++it;
+        continue;
+      }
+      j.result.resize(j.n);
+      int rc2 = CEP_OK;
+      if (j.first_pace >= 0) {
+        rc2 = cep_batch_get_biomarkers_range(s->pool, j.first, j.n, j.result.data());
+      } else {
+        for (int k = 0; k < j.n; ++k) {
+          std::memset(&j.result[k], 0, sizeof(cep_biomarkers_t));
+          j.result[k].status = status[j.first + k];
+        }
+      }
+      cep_batch_release_range(s->pool, j.first, j.n);
+      for (int k = 0; k < j.n; ++k) s->owner[j.first + k] = -1;
+      j.t_done = Clock::now();
+      j.state = rc2 ? CEP_JOB_FAILED : CEP_JOB_DONE;
+      j.error = rc2;
+      s->steps_done += j.steps;
+      s->completed += 1;
+      it = s->running.erase(it);
+      s->cv_done.notify_all();
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cep_serve_start(int model, int precision, int capacity, double dt, double dt_write, double max_bcl,
+                    long steps_per_launch, double hbm_fraction, void *stream, cep_server_t *out) {
+  if (!out) return cep_internal_set_fail(CEP_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (!(dt > 0) || !(dt_write > 0) || !(max_bcl > 0) || steps_per_launch <= 0)
+    return cep_internal_set_fail(CEP_ERR_ARG, "dt, dt_write, max_bcl and steps_per_launch must be positive");
+  if (!(hbm_fraction > 0) || hbm_fraction > 1)
+    return cep_internal_set_fail(CEP_ERR_ARG, "hbm_fraction must be in (0, 1]");
+  if (cep_device_count() == 0) return cep_internal_set_fail(CEP_ERR_NO_DEVICE, "no CUDA device visible");
+  // Ca samples per beat exactly as cep_batch_start_range counts them
+  const int print_freq = (int)((1. / dt) * dt_write);
+  const int per_beat = (print_freq > 0 ? (int)(max_bcl / dt) / print_freq : 0) + 2;
+  // HBM admission: the pool may use hbm_fraction of the memory free now
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+    return cep_internal_set_fail(CEP_ERR_CUDA, "cudaMemGetInfo failed");
+  // states + parameters (<= 64 + 96 doubles), clock and schedule, biomarker
+  // records, two Ca rings of per_beat + 2 doubles
+  const double per_instance = 8.0 * (64 + 96 + 8 + 48 + 2.0 * (per_beat + 2)) + 64;
+  const long long fit = (long long)(hbm_fraction * (double)free_b / per_instance);
+  if (capacity <= 0) capacity = (int)std::min<long long>(fit, 1 << 24);
+  if ((long long)capacity > fit) return cep_internal_set_fail(CEP_ERR_OOM, "capacity exceeds the HBM budget");
+  if (capacity <= 0) return cep_internal_set_fail(CEP_ERR_OOM, "no room for a pool");
+  cep_server *s = new cep_server;
+  s->model = model;
+  s->precision = precision;
+  s->capacity = capacity;
+  s->dt = dt;
+  s->dt_write = dt_write;
+  s->max_per_beat = per_beat;
+  s->steps_per_launch = steps_per_launch;
+  int rc;
+  if ((rc = cep_batch_create(model, capacity, precision, stream, &s->pool)) ||
+      (rc = cep_batch_init(s->pool, nullptr, nullptr, nullptr, 0, CEP_FLAG_QUIRKS)) ||
+      (rc = cep_batch_reserve_biomarkers(s->pool, per_beat, dt, dt_write, -1e300))) {
+    if (s->pool) cep_batch_destroy(s->pool);
+    delete s;
+    return rc;
+  }
+  s->owner.assign(capacity, -1);
+  s->t_start = Clock::now();
+  s->worker = std::thread(worker_loop, s);
+  *out = s;
+  return CEP_OK;
+}
+
+int cep_serve_submit(cep_server_t s, const cep_job_t *job, uint64_t *id) {
+  if (!s || !job || !id) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
+  if (job->n <= 0 || job->n > s->capacity) return cep_internal_set_fail(CEP_ERR_ARG, "job size outside 1..capacity");
+  if (!job->conc) return cep_internal_set_fail(CEP_ERR_ARG, "conc is NULL");
+  if (job->hill && job->hill_stride < 14) return cep_internal_set_fail(CEP_ERR_ARG, "hill_stride must be >= 14");
+  if (!(job->bcl > 0) || job->n_pace <= 0 || job->first_pace >= job->n_pace)
+    return cep_internal_set_fail(CEP_ERR_ARG, "bad protocol");
+  const int print_freq = (int)((1. / s->dt) * s->dt_write);
+  if (job->first_pace >= 0 && print_freq > 0 && (int)(job->bcl / s->dt) / print_freq + 2 > s->max_per_beat)
+    return cep_internal_set_fail(CEP_ERR_ARG, "BCL longer than the server's max_bcl");
+  auto j = std::make_shared<Job>();
+  j->n = job->n;
+  j->conc.assign(job->conc, job->conc + job->n);
+  if (job->celltype) j->celltype.assign(job->celltype, job->celltype + job->n);
+  if (job->hill) j->hill.assign(job->hill, job->hill + (size_t)job->n * job->hill_stride);
+  j->hill_stride = job->hill ? job->hill_stride : 0;
+  j->bcl = job->bcl;
+  j->n_pace = job->n_pace;
+  j->first_pace = job->first_pace;
+  j->flags = job->flags;
+  j->steps = (long long)job->n * (long long)((job->n_pace * job->bcl) / s->dt);
+  j->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (s->stop) return cep_internal_set_fail(s->fatal ? s->fatal : CEP_ERR_STATE, "server stopped");
+  j->id = s->next_id++;
+  s->jobs[j->id] = j;
+  s->queue.push_back(j);
+  *id = j->id;
+  s->cv_work.notify_one();
+  return CEP_OK;
+}
+
+int cep_serve_poll(cep_server_t s, uint64_t id, int *state) {
+  if (!s || !state) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  *state = it->second->state;
+  return CEP_OK;
+}
+
+int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s) {
+  if (!s) return cep_internal_set_fail(CEP_ERR_ARG, "null server");
+  std::unique_lock<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  auto j = it->second;
+  auto finished = [&] { return j->state == CEP_JOB_DONE || j->state == CEP_JOB_FAILED; };
+  if (timeout_s > 0) {
+    if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), finished))
+      return cep_internal_set_fail(CEP_ERR_TIMEOUT, "job not finished within the timeout");
+  } else {
+    s->cv_done.wait(lock, finished);
+  }
+  if (j->state == CEP_JOB_FAILED) return cep_internal_set_fail(j->error ? j->error : CEP_ERR_STATE, "job failed");
+  return CEP_OK;
+}
+
+int cep_serve_result(cep_server_t s, uint64_t id, cep_biomarkers_t *out, cep_job_times_t *times) {
+  if (!s) return cep_internal_set_fail(CEP_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  Job &j = *it->second;
+  if (j.state != CEP_JOB_DONE) return cep_internal_set_fail(CEP_ERR_STATE, "job not done");
+  if (out) std::memcpy(out, j.result.data(), sizeof(cep_biomarkers_t) * j.n);
+  if (times) {
+    times->queue_ms = ms_between(j.t_submit, j.t_admit);
+    times->latency_ms = ms_between(j.t_submit, j.t_done);
+    times->run_ms = ms_between(j.t_admit, j.t_done);
+    times->cell_steps = (double)j.steps;
+  }
+  return CEP_OK;
+}
+
+int cep_serve_release(cep_server_t s, uint64_t id) {
+  if (!s) return cep_internal_set_fail(CEP_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  if (it->second->state != CEP_JOB_DONE && it->second->state != CEP_JOB_FAILED)
+    return cep_internal_set_fail(CEP_ERR_STATE, "job still queued or running");
+  s->jobs.erase(it);
+  return CEP_OK;
+}
+
+int cep_serve_stats(cep_server_t s, cep_serve_stats_t *st) {
+  if (!s || !st) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(s->mu);
+  st->capacity = s->capacity;
+  st->queued = (int)s->queue.size();
+  st->running = (int)s->running.size();
+  int used = 0;
+  for (int o : s->owner) used += o >= 0;
+  st->slots_used = used;
+  st->completed = s->completed;
+  st->launches = s->launches;
+  st->cell_steps = (double)s->steps_done;
+  st->busy_ms = s->busy_ms;
+  st->wall_ms = ms_between(s->t_start, Clock::now());
+  return CEP_OK;
+}
+
+int cep_serve_stop(cep_server_t s) {
+  if (!s) return CEP_OK;
+  {
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->stop = true;
+    for (auto &j : s->queue) {
+      j->state = CEP_JOB_FAILED;
+      j->error = CEP_ERR_STATE;
+    }
+    for (auto &j : s->running) {
+      j->state = CEP_JOB_FAILED;
+      j->error = CEP_ERR_STATE;
+    }
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  cep_batch_destroy(s->pool);
+  delete s;
+  return CEP_OK;
+}
+
+}  // extern "C"

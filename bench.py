@@ -78,7 +78,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop", "tt06_sheet"])
+    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop", "tt06_sheet", "serve"])
+    ap.add_argument("--jobs", type=int, default=40, help="serving trace length")
     ap.add_argument("--seg", type=int, default=None,
                     help="time steps per bench step (default 10000 for populations, 200 for tissue)")
     ap.add_argument("--nx", type=int, default=512, help="tissue sheet edge in nodes")
@@ -96,7 +97,7 @@ def parse():
 
 
 def model_of(workload: str) -> str:
-    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011", "tt06_sheet": "tt2006"}[workload]
+    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011", "tt06_sheet": "tt2006", "serve": "cipa2017"}[workload]
 
 
 # ------------------------------------------------------------ inputs
@@ -546,9 +547,104 @@ def tissue_main(args, world, rank, local, pg):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------ serving workload
+SERVE_BCL, SERVE_DT = 1000.0, 0.005
+
+
+def serve_trace(n_jobs: int, seed: int):
+    """Seeded screening jobs: CiPA populations of log-U[20, 500] samples x
+    1-4 concentrations, 1-2 paces at BCL 1000 ms (biomarkers on the last
+    pace), each around its own nominal drug."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n_jobs):
+        ns = int(round(10 ** rng.uniform(np.log10(20), np.log10(500))))
+        nc = int(rng.integers(1, 5))
+        paces = int(rng.integers(1, 3))
+        conc, hill = population("cipa2017", ns, nc, seed=seed * 1000 + k)
+        jobs.append(dict(conc=conc, hill=hill, n_pace=paces, first_pace=paces - 1))
+    return jobs
+
+
+def run_serving(cep, jobs, arrivals, mode: str, capacity: int, k_steps: int):
+    """Replay the trace: 'batched' submits every job at its arrival time
+    (continuous batching); 'serial' runs one job at a time in arrival order.
+    Returns per-job latencies (ms from arrival to completion), the makespan
+    and the server's counters."""
+    srv = cep.Server("cipa2017", "mixed", capacity=capacity, dt=SERVE_DT, max_bcl=SERVE_BCL, steps_per_launch=k_steps)
+    try:
+        t0 = time.perf_counter()
+        lat = [0.0] * len(jobs)
+        if mode == "batched":
+            ids = []
+            for j, ta in zip(jobs, arrivals):
+                d = t0 + ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids.append(srv.submit(j["conc"], j["hill"], bcl=SERVE_BCL, n_pace=j["n_pace"],
+                                      first_pace=j["first_pace"]))
+            for k, jid in enumerate(ids):
+                srv.wait(jid, 0)
+                _, tm = srv.result(jid)
+                lat[k] = tm["latency_ms"]
+        else:
+            for k, (j, ta) in enumerate(zip(jobs, arrivals)):
+                d = t0 + ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                jid = srv.submit(j["conc"], j["hill"], bcl=SERVE_BCL, n_pace=j["n_pace"], first_pace=j["first_pace"])
+                srv.wait(jid, 0)
+                lat[k] = (time.perf_counter() - (t0 + ta)) * 1e3
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+    finally:
+        srv.close()
+    return np.array(lat), makespan, st
+
+
+def serve_main(args):
+    cep = importlib.import_module("2ddrugsimulation_b200")
+    jobs = serve_trace(args.jobs, 777)
+    steps = [len(j["conc"]) * int(j["n_pace"] * SERVE_BCL / SERVE_DT) for j in jobs]
+    capacity, k_steps = 16384, 10000
+    # calibration: one-at-a-time service time per instance-step from three jobs
+    cal = [run_serving(cep, [jobs[k]], [0.0], "serial", capacity, k_steps)[0][0] for k in range(3)]
+    per_step_ms = float(np.mean([c / s for c, s in zip(cal, steps[:3])]))
+    mean_service = per_step_ms * float(np.mean(steps)) / 1e3  # s
+    rng = np.random.default_rng(778)
+    gaps = rng.exponential(mean_service / 1.2, len(jobs))  # offered load 1.2x one-at-a-time capacity
+    arrivals = np.cumsum(gaps) - gaps[0]
+    res = {}
+    for mode in ("batched", "serial"):
+        lat, span, st = run_serving(cep, jobs, arrivals, mode, capacity, k_steps)
+        res[mode] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "mean_ms": float(lat.mean()), "makespan_s": span,
+                     "cell_steps_per_s": float(sum(steps)) / span, "launches": int(st["launches"])}
+    b, s_ = res["batched"], res["serial"]
+    line = {
+        "metric": "screen-job p50/p99 latency (continuous batching vs one at a time), CiPA-ORd mixed",
+        "value": b["p99_ms"], "unit": "ms (p99 latency)", "n_gpus": 1, "steps": len(jobs), "warmup": 3,
+        "ms_per_step": b["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (mixed)", "data": "synthetic",
+        "config": {"workload": f"{len(jobs)} Poisson-arriving CiPA-ORd screening jobs (log-U[20,500] samples x 1-4 "
+                               f"concs, 1-2 paces at BCL 1000 ms, dt 0.005 ms, biomarkers on the last pace), offered "
+                               f"load 1.2x one-at-a-time capacity; pool of {capacity} slots, {k_steps} steps per "
+                               f"launch", "total_cell_steps": int(sum(steps))},
+        "latency_ms": {"p50": b["p50_ms"], "p99": b["p99_ms"]},
+        "serial": s_, "batched": b,
+        "p99_speedup_vs_serial": s_["p99_ms"] / b["p99_ms"],
+        "throughput_speedup_vs_serial": b["cell_steps_per_s"] / s_["cell_steps_per_s"],
+        "gpu_launches": b["launches"], "cpu_baseline": None, "e2e": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     model = model_of(args.workload)
+    if args.workload == "serve":
+        serve_main(args)
+        return
     if args.workload == "tt06_sheet":
         world, rank, local, pg = dist_setup()
         if args.impl == "reference":

@@ -40,6 +40,7 @@ extern "C" {
 #define CEP_INST_RUNNING 0
 #define CEP_INST_DONE 1     /* reached the end of its protocol */
 #define CEP_INST_NONFINITE 2 /* state left the finite range; frozen */
+#define CEP_INST_IDLE 3      /* slot released (cep_batch_release_range) */
 
 /* ----------------------------------------------------------------- models */
 #define CEP_MODEL_ORD2011 0   /* DrugSimulation/cellmodels/Ohara_Rudy_2011.cpp, 41 states */
@@ -160,6 +161,88 @@ int cep_batch_sync(cep_batch_t b);
  * Ohara_Rudy_2011.cpp:742): dVdt[n] and the seven channel currents
  * currents[7*n] (INa, INaL, Ito, ICaL, IKr, IKs, IK1; SoA). */
 int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
+
+/* ---------------------------------------------------- instance ranges */
+/* Heterogeneous batches: a batch used as a pool of slots whose ranges hold
+ * different jobs at different points of their protocols (the serving
+ * loop). No counterpart in the reference, which runs one job per process.
+ *
+ * reserve_biomarkers: fixes the batch-wide step dt, the Ca sampling
+ * interval and the qNet threshold, reserves the biomarker records and a Ca
+ * ring of max_samples_per_beat (= BCL/dt_write of the longest beat), and
+ * releases every slot. Instances of a running job are never touched by
+ * calls on other ranges. */
+int cep_batch_reserve_biomarkers(cep_batch_t b, int max_samples_per_beat, double dt, double dt_write,
+                                 double qnet_vm_threshold);
+/* initConsts for instances [first, first+count); inputs indexed from 0. */
+int cep_batch_init_range(cep_batch_t b, int first, int count, const double *celltype, const double *conc,
+                         const double *hill, int hill_stride, unsigned flags);
+int cep_batch_set_pacing_range(cep_batch_t b, int first, int count, double bcl, double stim_start,
+                               double stim_dur, double amp_scale);
+/* Start the range's protocol: n_pace paces at each instance's BCL with
+ * biomarkers from first_pace (-1: off); clocks reset to t = 0 and the
+ * instances marked running. */
+int cep_batch_start_range(cep_batch_t b, int first, int count, int n_pace, int first_pace);
+/* Mark the range idle: run launches skip it. */
+int cep_batch_release_range(cep_batch_t b, int first, int count);
+int cep_batch_get_biomarkers_range(cep_batch_t b, int first, int count, cep_biomarkers_t *out);
+
+/* --------------------------------------------------------------- serving */
+/* A screening-job server with continuous batching (no counterpart in the
+ * reference). One pool of `capacity` slots stays resident in HBM; each
+ * job (a list of instances: samples x concentrations with their Hill rows)
+ * is admitted into a free slot range as soon as one fits, runs inside the
+ * same launches as every other admitted job, and is collected and released
+ * when all its instances finish. A job's biomarkers are bit-identical alone
+ * or in any mix. capacity <= 0 sizes the pool to hbm_fraction of the free
+ * device memory (the admission budget); max_bcl bounds the BCL of jobs that
+ * want biomarkers (it sizes the Ca ring). One scheduler thread per server. */
+typedef struct cep_server *cep_server_t;
+
+#define CEP_JOB_QUEUED 0
+#define CEP_JOB_RUNNING 1
+#define CEP_JOB_DONE 2
+#define CEP_JOB_FAILED 3
+
+typedef struct {
+  int n;                  /* instances                                    */
+  const double *celltype; /* [n] or NULL (endo)                           */
+  const double *conc;     /* [n]                                          */
+  const double *hill;     /* [n * hill_stride] or NULL                    */
+  int hill_stride;
+  double bcl;             /* ms                                           */
+  int n_pace, first_pace; /* protocol as cep_batch_set_protocol           */
+  unsigned flags;         /* CEP_FLAG_*                                   */
+} cep_job_t;
+
+typedef struct {
+  double queue_ms;   /* submit -> admission                  */
+  double run_ms;     /* admission -> completion              */
+  double latency_ms; /* submit -> completion                 */
+  double cell_steps; /* instance-steps of the job            */
+} cep_job_times_t;
+
+typedef struct {
+  int capacity, queued, running, slots_used;
+  long long completed, launches;
+  double cell_steps; /* instance-steps of completed jobs      */
+  double busy_ms;    /* time inside launches + status reads  */
+  double wall_ms;    /* since start                          */
+} cep_serve_stats_t;
+
+int cep_serve_start(int model, int precision, int capacity, double dt, double dt_write, double max_bcl,
+                    long steps_per_launch, double hbm_fraction, void *stream, cep_server_t *out);
+int cep_serve_submit(cep_server_t s, const cep_job_t *job, uint64_t *id);
+int cep_serve_poll(cep_server_t s, uint64_t id, int *state);
+/* Block until the job is done (timeout_s <= 0: no limit). */
+int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s);
+/* out[job n] biomarkers (may be NULL) and timings (may be NULL). */
+int cep_serve_result(cep_server_t s, uint64_t id, cep_biomarkers_t *out, cep_job_times_t *times);
+/* Forget a finished job (frees its host-side record). */
+int cep_serve_release(cep_server_t s, uint64_t id);
+int cep_serve_stats(cep_server_t s, cep_serve_stats_t *st);
+/* Stop the scheduler (queued and running jobs fail), free the pool. */
+int cep_serve_stop(cep_server_t s);
 
 /* qInward of a drug run against its control: 0.5*(INaL_auc_drug/
  * INaL_auc_ctrl + ICaL_auc_drug/ICaL_auc_ctrl) (cipa_drug_bench.cpp:376). */

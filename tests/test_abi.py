@@ -36,3 +36,12 @@ def test_no_device_fails_loudly(cep):
     with pytest.raises(cep.CepError) as e:
         cep.Batch("ord2011", 4)
     assert e.value.code == cep.ERR_NO_DEVICE
+
+
+def test_server_without_device_fails_loudly(cep):
+    if cep.device_count() > 0:
+        return
+    import pytest
+    with pytest.raises(cep.CepError) as e:
+        cep.Server("ord2011")
+    assert e.value.code == cep.ERR_NO_DEVICE
