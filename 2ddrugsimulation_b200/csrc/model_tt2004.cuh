@@ -1,0 +1,244 @@
+// ten Tusscher - Noble - Noble - Panfilov 2004, one cell per thread,
+// templated on the precision policy (cep_device.cuh).
+//
+// Equations and update scheme: CEPCell_NEO/cellmodels/
+// tentusscher_noble_noble_panfilov_2004_b.cpp with every channel of its
+// header enabled: computeRates (:379-635, standard INa branch) and
+// solveAnalytical (:637-658): Rush-Larsen for f, s, r, Xr1, Xr2, Xs, m, h, j
+// and d; forward Euler for V, K_i, Na_i, Ca_i, Ca_SR and for fCa and g,
+// whose rates are held at 0 while they would rise at V > -60 mV. Hill hook
+// as initConsts(type, conc, hill) (:361-377). The NaCa voltage partition
+// gmma is a parameter: the reference leaves it unassigned (0 in effect,
+// kept under CEP_FLAG_QUIRKS), the published model has 0.35.
+#pragma once
+#include "cep_device.cuh"
+
+namespace cep {
+namespace tt04 {
+
+constexpr int kNumStates = 17;
+enum : int { V = 0, K_i, Na_i, Ca_i, Xr1, Xr2, Xs, m, h, j, d, f, fCa, s, r, Ca_SR, g };
+enum : int {
+  P_gCaL = 0, P_gK1, P_gKs, P_gNa, P_gto, P_gKr, P_gmma, P_amp, P_BCL, P_stim_start, P_duration, kNumParams
+};
+
+namespace k {
+constexpr double R = 8314.472, T = 310, F = 96485.3415, Cm = 0.185, V_c = 0.016404, P_kna = 0.03, K_o = 5.4;
+constexpr double Na_o = 140, Ca_o = 2, g_bna = 0.00029, g_bca = 0.000592, P_NaK = 1.362, K_mk = 1, K_mNa = 40;
+constexpr double K_NaCa = 1000, K_sat = 0.1, alpha = 2.5, Km_Ca = 1.38, Km_Nai = 87.5;
+constexpr double g_pCa = 0.825, K_pCa = 0.0005, g_pK = 0.0146, tau_g = 2, a_rel = 0.016464, b_rel = 0.25;
+constexpr double c_rel = 0.008232, K_up = 0.00025, V_leak = 8e-5, Vmax_up = 0.000425, Buf_c = 0.15;
+constexpr double K_buf_c = 0.001, Buf_sr = 10, K_buf_sr = 0.3, V_sr = 0.001094, tau_fCa = 2.0;
+constexpr double RT = R * T, RTF = (R * T) / F, FRT = F / (R * T);
+constexpr double nak_c = (P_NaK * K_o) / (K_o + K_mk);
+constexpr double naca_den = (Km_Nai * Km_Nai * Km_Nai + Na_o * Na_o * Na_o) * (Km_Ca + Ca_o);
+constexpr double Na_o3 = Na_o * Na_o * Na_o;
+constexpr double c_vcf = Cm / (V_c * F);  // current -> concentration rate
+}  // namespace k
+
+template <class G>
+struct Y {
+  double V, K_i, Na_i, Ca_i, Xr1, Xr2, Xs, m, h, j, d, f, fCa, s, r, Ca_SR, g;
+};
+template <class G>
+struct Par {
+  G gCaL, gK1, gKs, gNa, gto, gKr, gmma;
+  double amp, BCL, stim_start, duration;
+};
+template <class G>
+struct Cur {
+  G INa, INaL, Ito, ICaL, IKr, IKs, IK1, dVdt;
+};
+
+#define CEP_TT04_FIELDS(X) X(V) X(K_i) X(Na_i) X(Ca_i) X(Xr1) X(Xr2) X(Xs) X(m) X(h) X(j) X(d) X(f) X(fCa) \
+  X(s) X(r) X(Ca_SR) X(g)
+
+template <class G>
+__device__ __forceinline__ void load(Y<G> &y, const double *__restrict__ s_, int64_t ld, int64_t i) {
+#define CEP_LD(n) y.n = s_[n * ld + i];
+  CEP_TT04_FIELDS(CEP_LD)
+#undef CEP_LD
+}
+template <class G>
+__device__ __forceinline__ void store(const Y<G> &y, double *__restrict__ s_, int64_t ld, int64_t i) {
+#define CEP_ST(n) s_[n * ld + i] = y.n;
+  CEP_TT04_FIELDS(CEP_ST)
+#undef CEP_ST
+}
+template <class G>
+__device__ __forceinline__ void load_par(Par<G> &q, const double *__restrict__ p, int64_t ld, int64_t i) {
+  q.gCaL = (G)p[P_gCaL * ld + i]; q.gK1 = (G)p[P_gK1 * ld + i]; q.gKs = (G)p[P_gKs * ld + i];
+  q.gNa = (G)p[P_gNa * ld + i]; q.gto = (G)p[P_gto * ld + i]; q.gKr = (G)p[P_gKr * ld + i];
+  q.gmma = (G)p[P_gmma * ld + i];
+  q.amp = p[P_amp * ld + i]; q.BCL = p[P_BCL * ld + i]; q.stim_start = p[P_stim_start * ld + i];
+  q.duration = p[P_duration * ld + i];
+}
+
+// One cell step: rates at (t, y); if `update`, the reference's Rush-Larsen /
+// forward-Euler update by dt. stim_mode < 0: periodic single-cell stimulus;
+// 0/1: the tissue flag.
+template <class P>
+__device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                                     int stim_mode, bool update, Cur<typename P::G> &cur) {
+  using G = typename P::G;
+  const G v = (G)y.V, one = (G)1;
+  bool on;
+  if (stim_mode < 0) {
+    const double ph = t - floor(t / q.BCL) * q.BCL;
+    on = ph >= q.stim_start && ph <= q.stim_start + q.duration;
+  } else {
+    on = stim_mode != 0;
+  }
+  const G i_Stim = on ? -(G)q.amp : (G)0;
+  const G cai = (G)y.Ca_i, casr = (G)y.Ca_SR, nai = (G)y.Na_i, ki = (G)y.K_i;
+  // gates: steady states and time constants
+  const G tau_d = (P::dv((G)1.4, one + P::ex(((G)-35.0 - v) * (G)(1.0 / 13.0))) + (G)0.25) *
+                      P::dv((G)1.4, one + P::ex((v + (G)5.0) * (G)0.2)) +
+                  P::rc(one + P::ex(((G)50.0 - v) * (G)0.05));
+  const G tau_f = (G)1125.0 * P::ex(-p2(v + (G)27.0) * (G)(1.0 / 240.0)) + (G)80.0 +
+                  P::dv((G)165.0, one + P::ex(((G)25.0 - v) * (G)0.1));
+  const G d_inf = P::rc(one + P::ex(((G)-5.0 - v) * (G)(1.0 / 7.5)));
+  const G f_inf = P::rc(one + P::ex((v + (G)20.0) * (G)(1.0 / 7.0)));
+  const G alpha_fCa = P::rc(one + p8(cai * (G)(1.0 / 0.000325)));
+  const G beta_fCa = P::dv((G)0.1, one + P::ex((cai - (G)0.0005) * (G)10000.0));
+  const G gama_fCa = P::dv((G)0.2, one + P::ex((cai - (G)0.00075) * (G)1250.0));
+  const G fCa_inf = (alpha_fCa + beta_fCa + gama_fCa + (G)0.23) * (G)(1.0 / 1.46);
+  const G cr = cai * (G)(1.0 / 0.00035);
+  const G cr2 = cr * cr, cr4 = cr2 * cr2, cr8 = cr4 * cr4;
+  const G g_inf = cai < (G)0.00035 ? P::rc(one + cr4 * cr2) : P::rc(one + cr8 * cr8);
+  const G xr1_inf = P::rc(one + P::ex(((G)-26.0 - v) * (G)(1.0 / 7.0)));
+  const G tau_xr1 = P::dv((G)450.0, one + P::ex(((G)-45.0 - v) * (G)0.1)) * P::dv((G)6.0, one + P::ex((v + (G)30.0) * (G)(1.0 / 11.5)));
+  const G xr2_inf = P::rc(one + P::ex((v + (G)88.0) * (G)(1.0 / 24.0)));
+  const G tau_xr2 = P::dv((G)3.0, one + P::ex(((G)-60.0 - v) * (G)0.05)) * P::dv((G)1.12, one + P::ex((v - (G)60.0) * (G)0.05));
+  const G xs_inf = P::rc(one + P::ex(((G)-5.0 - v) * (G)(1.0 / 14.0)));
+  const G tau_xs = P::dv((G)1100.0, P::sq(one + P::ex(((G)-10.0 - v) * (G)(1.0 / 6.0)))) *
+                   P::rc(one + P::ex((v - (G)60.0) * (G)0.05));
+  const G m_inf = P::rc(p2(one + P::ex(((G)-56.86 - v) * (G)(1.0 / 9.03))));
+  const G tau_m = P::rc(one + P::ex(((G)-60.0 - v) * (G)0.2)) *
+                  (P::dv((G)0.1, one + P::ex((v + (G)35.0) * (G)0.2)) + P::dv((G)0.1, one + P::ex((v - (G)50.0) * (G)0.005)));
+  const G h_inf = P::rc(p2(one + P::ex((v + (G)71.55) * (G)(1.0 / 7.43))));
+  const bool lo = v < (G)-40.0;
+  const G alpha_h = lo ? (G)0.057 * P::ex(-(v + (G)80.0) * (G)(1.0 / 6.8)) : (G)0;
+  const G beta_h = lo ? (G)2.7 * P::ex((G)0.079 * v) + (G)310000.0 * P::ex((G)0.3485 * v)
+                      : P::dv((G)0.77, (G)0.13 * (one + P::ex((v + (G)10.66) * (G)(1.0 / -11.1))));
+  const G tau_h = P::rc(alpha_h + beta_h);
+  const G j_inf = h_inf;
+  const G alpha_j = lo ? P::dv(((G)-25428.0 * P::ex((G)0.2444 * v) - (G)6.948e-06 * P::ex((G)-0.04391 * v)) * (v + (G)37.78),
+                               one + P::ex((G)0.311 * (v + (G)79.23)))
+                       : (G)0;
+  const G beta_j = lo ? P::dv((G)0.02424 * P::ex((G)-0.01052 * v), one + P::ex((G)-0.1378 * (v + (G)40.14)))
+                      : P::dv((G)0.6 * P::ex((G)0.057 * v), one + P::ex((G)-0.1 * (v + (G)32.0)));
+  const G tau_j = P::rc(alpha_j + beta_j);
+  const G r_inf = P::rc(one + P::ex(((G)20.0 - v) * (G)(1.0 / 6.0)));
+  const G tau_r = (G)9.5 * P::ex(-p2(v + (G)40.0) * (G)(1.0 / 1800.0)) + (G)0.8;
+  const G s_inf = P::rc(one + P::ex((v + (G)20.0) * (G)0.2));
+  const G tau_s = (G)85.0 * P::ex(-p2(v + (G)45.0) * (G)(1.0 / 320.0)) + P::dv((G)5.0, one + P::ex((v - (G)20.0) * (G)0.2)) + (G)3.0;
+  // currents
+  const G i_NaK = P::dv((G)k::nak_c * nai, nai + (G)k::K_mNa) *
+                  P::rc(one + (G)0.1245 * P::ex((G)-0.1 * v * (G)k::FRT) + (G)0.0353 * P::ex(-v * (G)k::FRT));
+  const G E_Na = (G)k::RTF * P::lg(P::dv((G)k::Na_o, nai));
+  const G i_Na = q.gNa * p3((G)y.m) * (G)y.h * (G)y.j * (v - E_Na);
+  const G i_b_Na = (G)k::g_bna * (v - E_Na);
+  const G eg = P::ex(q.gmma * v * (G)k::FRT), eg1 = P::ex((q.gmma - one) * v * (G)k::FRT);
+  const G i_NaCa = P::dv((G)k::K_NaCa * (eg * p3(nai) * (G)k::Ca_o - eg1 * (G)k::Na_o3 * cai * (G)k::alpha),
+                         (G)k::naca_den * (one + (G)k::K_sat * eg1));
+  const G E_K = (G)k::RTF * P::lg(P::dv((G)k::K_o, ki));
+  const G vek = v - E_K;
+  const G alpha_K1 = P::dv((G)0.1, one + P::ex((G)0.06 * (vek - (G)200.0)));
+  const G beta_K1 = P::dv((G)3.0 * P::ex((G)0.0002 * (vek + (G)100.0)) + P::ex((G)0.1 * (vek - (G)10.0)),
+                          one + P::ex((G)-0.5 * vek));
+  const G i_K1 = q.gK1 * P::dv(alpha_K1, alpha_K1 + beta_K1) * vek;  // sqrt(K_o/5.4) = 1
+  const G i_to = q.gto * (G)y.r * (G)y.s * vek;
+  const G i_Kr = q.gKr * (G)y.Xr1 * (G)y.Xr2 * vek;
+  const G E_Ks = (G)k::RTF * P::lg(P::dv((G)(k::K_o + k::P_kna * k::Na_o), ki + (G)k::P_kna * nai));
+  const G i_Ks = q.gKs * p2((G)y.Xs) * (v - E_Ks);
+  G i_CaL;
+  if constexpr (P::kMixed) {
+    // g d f fCa 2F x/(e^x - 1) (Ca_i e^x - 0.341 Ca_o), x = 2 V F/(RT), with
+    // the x/(e^x - 1) factor evaluated stably near V = 0
+    const G x = (G)2.0 * v * (G)k::FRT;
+    const G e = P::ex(x);
+    i_CaL = q.gCaL * (G)y.d * (G)y.f * (G)y.fCa * (G)(2.0 * k::F) * ghk_factor(x) * (cai * e - (G)(0.341 * k::Ca_o));
+  } else {
+    const double vv = y.V;
+    const double e = ::exp((2.0 * vv * k::F) / k::RT);
+    i_CaL = div64(((q.gCaL * y.d * y.f * y.fCa * 4.0 * vv * (k::F * k::F)) / k::RT) * (y.Ca_i * e - 0.341 * k::Ca_o),
+                  e - 1.0);
+  }
+  const G E_Ca = (G)(0.5 * k::RTF) * P::lg(P::dv((G)k::Ca_o, cai));
+  const G i_b_Ca = (G)k::g_bca * (v - E_Ca);
+  const G i_p_K = P::dv((G)k::g_pK * vek, one + P::ex(((G)25.0 - v) * (G)(1.0 / 5.98)));
+  const G i_p_Ca = P::dv((G)k::g_pCa * cai, cai + (G)k::K_pCa);
+  const G dV = -(i_K1 + i_to + i_Kr + i_Ks + i_CaL + i_NaK + i_Na + i_b_Na + i_NaCa + i_b_Ca + i_p_K + i_p_Ca + i_Stim);
+  cur.INa = i_Na; cur.INaL = (G)0; cur.Ito = i_to; cur.ICaL = i_CaL; cur.IKr = i_Kr; cur.IKs = i_Ks;
+  cur.IK1 = i_K1; cur.dVdt = dV;
+  if (!update) return;
+  // calcium handling
+  const G i_up = P::dv((G)k::Vmax_up, one + P::dv((G)(k::K_up * k::K_up), p2(cai)));
+  const G i_leak = (G)((y.Ca_SR - y.Ca_i) * k::V_leak);
+  const G casr2 = p2(casr);
+  const G i_rel = (P::dv((G)k::a_rel * casr2, (G)(k::b_rel * k::b_rel) + casr2) + (G)k::c_rel) * (G)y.d * (G)y.g;
+  const G Ca_i_bufc = P::rc(one + P::dv((G)(k::Buf_c * k::K_buf_c), p2(cai + (G)k::K_buf_c)));
+  const G Ca_sr_bufsr = P::rc(one + P::dv((G)(k::Buf_sr * k::K_buf_sr), p2(casr + (G)k::K_buf_sr)));
+  const G dNa_i = -(i_Na + i_b_Na + (G)3.0 * i_NaK + (G)3.0 * i_NaCa) * (G)k::c_vcf;
+  const G dK_i = -((i_K1 + i_to + i_Kr + i_Ks + i_p_K + i_Stim) - (G)2.0 * i_NaK) * (G)k::c_vcf;
+  const G dCa_i = Ca_i_bufc * (((i_leak - i_up) + i_rel) - ((i_CaL + i_b_Ca + i_p_Ca) - (G)2.0 * i_NaCa) * (G)(0.5 * k::c_vcf));
+  const G dCa_SR = Ca_sr_bufsr * (G)(k::V_c / k::V_sr) * (i_up - (i_rel + i_leak));
+  const G dfCa = (fCa_inf > (G)y.fCa && v > (G)-60.0) ? (G)0 : (fCa_inf - (G)y.fCa) * (G)(1.0 / k::tau_fCa);
+  const G dg = (g_inf > (G)y.g && v > (G)-60.0) ? (G)0 : (g_inf - (G)y.g) * (G)(1.0 / k::tau_g);
+  // Rush-Larsen gates (the reference's ((y - inf) e^{-dt/tau}) + inf)
+  if constexpr (P::kMixed) {
+    y.f = rush_larsen<P, true>(y.f, f_inf, tau_f, dt);
+    y.s = rush_larsen<P, true>(y.s, s_inf, tau_s, dt);
+    y.r = rush_larsen<P>(y.r, r_inf, tau_r, dt);
+    y.Xr1 = rush_larsen<P>(y.Xr1, xr1_inf, tau_xr1, dt);
+    y.Xr2 = rush_larsen<P>(y.Xr2, xr2_inf, tau_xr2, dt);
+    y.Xs = rush_larsen<P, true>(y.Xs, xs_inf, tau_xs, dt);
+    y.m = rush_larsen<P>(y.m, m_inf, tau_m, dt);
+    y.h = rush_larsen<P>(y.h, h_inf, tau_h, dt);
+    y.j = rush_larsen<P>(y.j, j_inf, tau_j, dt);
+    y.d = rush_larsen<P>(y.d, d_inf, tau_d, dt);
+  } else {
+#define CEP_RL(n, inf, tau) y.n = ((y.n - (inf)) * ::exp(div64(-dt, (tau)))) + (inf);
+    CEP_RL(f, f_inf, tau_f) CEP_RL(s, s_inf, tau_s) CEP_RL(r, r_inf, tau_r) CEP_RL(Xr1, xr1_inf, tau_xr1)
+    CEP_RL(Xr2, xr2_inf, tau_xr2) CEP_RL(Xs, xs_inf, tau_xs) CEP_RL(m, m_inf, tau_m) CEP_RL(h, h_inf, tau_h)
+    CEP_RL(j, j_inf, tau_j) CEP_RL(d, d_inf, tau_d)
+#undef CEP_RL
+  }
+  y.g = y.g + (double)dg * dt;
+  y.fCa = y.fCa + (double)dfCa * dt;
+  y.Na_i = y.Na_i + (double)dNa_i * dt;
+  y.V = y.V + (double)dV * dt;
+  y.K_i = y.K_i + (double)dK_i * dt;
+  y.Ca_i = y.Ca_i + (double)dCa_i * dt;
+  y.Ca_SR = y.Ca_SR + (double)dCa_SR * dt;
+}
+
+__device__ __forceinline__ double hill_factor(double conc, double ic50, double h) {
+  return (ic50 > 10E-14 && h > 10E-14) ? 1. / (1. + ::pow(conc / ic50, h)) : 1.;
+}
+
+// initConsts (:185-359) plus the reference's Hill hook (:361-377).
+__device__ __forceinline__ void init_instance(double *__restrict__ par, double *__restrict__ s_, int64_t ld,
+                                              int64_t i, double conc, const double *__restrict__ hill,
+                                              bool quirks) {
+  double gCaL = 0.000175, gK1 = 5.405, gKs = 0.245, gNa = 14.838, gto = 0.294, gKr = 0.096;
+  if (hill) {
+    gCaL *= hill_factor(conc, hill[0], hill[1]);
+    gK1 *= hill_factor(conc, hill[2], hill[3]);
+    gKs *= hill_factor(conc, hill[4], hill[5]);
+    gNa *= hill_factor(conc, hill[6], hill[7]);
+    gto *= hill_factor(conc, hill[10], hill[11]);
+    gKr *= hill_factor(conc, hill[12], hill[13]);
+  }
+  double *p = par + i;
+  p[P_gCaL * ld] = gCaL; p[P_gK1 * ld] = gK1; p[P_gKs * ld] = gKs; p[P_gNa * ld] = gNa; p[P_gto * ld] = gto;
+  p[P_gKr * ld] = gKr; p[P_gmma * ld] = quirks ? 0.0 : 0.35;
+  p[P_amp * ld] = 52; p[P_BCL * ld] = 1000; p[P_stim_start * ld] = 10; p[P_duration * ld] = 1;
+  const double y0[kNumStates] = {-86.2, 138.3, 11.6, 0.0002, 0, 1, 0, 0, 0.75, 0.75, 0, 1, 1, 1, 0, 0.2, 1};
+#pragma unroll
+  for (int k2 = 0; k2 < kNumStates; ++k2) s_[k2 * ld + i] = y0[k2];
+}
+
+}  // namespace tt04
+}  // namespace cep

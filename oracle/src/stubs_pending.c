@@ -11,7 +11,5 @@
     (void)c; (void)t; (void)dt; (void)y; (void)k; }                                       \
   void cepo_##pfx##_rates(const cepo_cell *c, double t, const double *y, double *r, cepo_currents *k) { \
     (void)c; (void)t; (void)y; (void)r; (void)k; }
-STUB(tt04)
 STUB(tomek)
-void cepo_tt04_init_states(double *y) { (void)y; }
 void cepo_tomek_init_states(const cepo_cell *c, double *y) { (void)c; (void)y; }

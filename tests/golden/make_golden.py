@@ -127,9 +127,32 @@ def make_tt2006(dt: float = 0.01, stride: int = 100):
     print("wrote tt2006_tissue vmax", max(v1.max(), v2.max()))
 
 
+def make_tt2004(dt: float = 0.01, stride: int = 100):
+    """ten Tusscher 2004 (the reference's 2004_b build, every channel on):
+    control and a seeded drug row, two 1000-ms beats each. The reference
+    leaves CONSTANTS[gmma] unassigned; the fixture sets it to 0, the value
+    the reference's heap held when it was built here (a denormal that acts
+    as 0)."""
+    rng = np.random.default_rng(2004)
+    cases = [dict(name="tt2004_control", conc=0.0, hill=np.zeros(14)),
+             dict(name="tt2004_drug", conc=2.0, hill=hill_row(rng))]
+    for c in cases:
+        r = O.RefCell("tt2004", 0.0, c["conc"], c["hill"])
+        r.consts[27] = 0.0  # CONSTANTS[gmma]
+        y0 = r.states.copy()
+        r.L.ref_compute_rates(r.h, 0.0)
+        rates0 = r.arr("rates", r.n).copy()
+        n = int(round(2000.0 / dt))
+        t, v = r.run(0.0, dt, n, stride)
+        np.savez_compressed(OUT / f"{c['name']}.npz", conc=c["conc"], hill=c["hill"], dt=dt, stride=stride,
+                            n_steps=n, y0=y0, rates0=rates0, v_trace=v, final_states=r.states.copy(), t_final=t)
+        print("wrote", c["name"], "vmax", v.max())
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
     make_ord()
     make_cipa()
     make_tt2006()
+    make_tt2004()

@@ -164,3 +164,37 @@ def test_tt2006_oracle_bitwise_vs_compiled_reference(oracle):
     t2, v2 = c.run(0.0, 0.01, 150000, 50)
     assert np.array_equal(v1, v2)
     assert np.array_equal(r.states, c.states)
+
+
+TT04_CASES = sorted(GOLD.glob("tt2004_*.npz"))
+
+
+@pytest.mark.parametrize("path", TT04_CASES, ids=lambda p: p.stem)
+def test_tt2004_oracle_matches_reference_golden(oracle, path):
+    """ten Tusscher 2004 (2004_b build): V trace, final STATES and RATES at
+    t = 0 equal the reference's bit for bit (with the unassigned gmma at 0,
+    the oracle's quirk setting)."""
+    g = np.load(path)
+    c = oracle.Cell("tt2004", 0.0, float(g["conc"]), g["hill"], quirks=True)
+    assert np.array_equal(c.states, g["y0"])
+    r, _ = c.rates(0.0)
+    assert np.array_equal(r, g["rates0"])
+    t, v = c.run(0.0, float(g["dt"]), int(g["n_steps"]), int(g["stride"]))
+    assert np.array_equal(v, g["v_trace"])
+    assert np.array_equal(c.states, g["final_states"])
+
+
+def test_tt2004_oracle_bitwise_vs_compiled_reference(oracle):
+    if not oracle.ref_available("tt2004"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    rng = np.random.default_rng(41)
+    hill = np.zeros(14)
+    hill[0::2] = 10 ** rng.uniform(-1, 2, 7)
+    hill[1::2] = rng.uniform(0.6, 1.8, 7)
+    r = oracle.RefCell("tt2004", 0.0, 0.8, hill)
+    r.consts[27] = 0.0  # CONSTANTS[gmma], unassigned by the reference
+    c = oracle.Cell("tt2004", 0.0, 0.8, hill, quirks=True)
+    t1, v1 = r.run(0.0, 0.01, 120000, 50)
+    t2, v2 = c.run(0.0, 0.01, 120000, 50)
+    assert np.array_equal(v1, v2)
+    assert np.array_equal(r.states, c.states)
