@@ -242,7 +242,11 @@ def run_ours(args, world, rank, local, pg, model):
     import torch
     cep = importlib.import_module("2ddrugsimulation_b200")
     torch.cuda.set_device(local)
-    conc, hill = population(model, args.samples, args.concs, seed=1234 + rank)
+    # one screening job of samples x world, sharded by whole samples
+    shard = importlib.import_module("2ddrugsimulation_b200.shard")
+    conc_all, hill_all = population(model, args.samples * world, args.concs, seed=1234)
+    i0, i1 = shard.instance_range(args.samples * world, args.concs, world, rank)
+    conc, hill = conc_all[i0:i1], hill_all[i0:i1]
     n = len(conc)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
     res = {}
