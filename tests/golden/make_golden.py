@@ -149,6 +149,34 @@ def make_tt2004(dt: float = 0.01, stride: int = 100):
         print("wrote", c["name"], "vmax", v.max())
 
 
+def make_tomek(dt: float = 0.005, n_steps: int = 200000, every: int = 10000):
+    """ToR-ORd: the reference has no fixed-step integrator (its
+    solveAnalytical is empty), so like CiPA the fixture holds states along
+    the oracle's fixed-step trajectory and the reference's RATES at each of
+    them; endo control, epi with a drug row, mid with a drug row."""
+    rng = np.random.default_rng(2019)
+    cases = [dict(name="tomek_endo_control", celltype=0.0, conc=0.0, hill=np.zeros(14)),
+             dict(name="tomek_epi_drug", celltype=1.0, conc=1.5, hill=hill_row(rng)),
+             dict(name="tomek_mid_drug", celltype=2.0, conc=0.6, hill=hill_row(rng))]
+    for c in cases:
+        r = O.RefCell("tomek2019", c["celltype"], c["conc"], c["hill"])
+        cell = O.Cell("tomek2019", c["celltype"], c["conc"], c["hill"], quirks=True)
+        states, rates, times = [], [], []
+        t = 0.0
+        for k in range(n_steps):
+            if k % every == 0:
+                r.states[:] = cell.states
+                r.L.ref_compute_rates(r.h, t)
+                states.append(cell.states.copy())
+                rates.append(r.arr("rates", r.n).copy())
+                times.append(t)
+            cell.step(t, dt)
+            t += dt
+        np.savez_compressed(OUT / f"{c['name']}.npz", celltype=c["celltype"], conc=c["conc"], hill=c["hill"], dt=dt,
+                            times=np.array(times), states=np.array(states), ref_rates=np.array(rates))
+        print("wrote", c["name"])
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
@@ -156,3 +184,4 @@ if __name__ == "__main__":
     make_cipa()
     make_tt2006()
     make_tt2004()
+    make_tomek()

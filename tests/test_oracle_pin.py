@@ -198,3 +198,49 @@ def test_tt2004_oracle_bitwise_vs_compiled_reference(oracle):
     t2, v2 = c.run(0.0, 0.01, 120000, 50)
     assert np.array_equal(v1, v2)
     assert np.array_equal(r.states, c.states)
+
+
+TOMEK_CASES = sorted(GOLD.glob("tomek_*.npz"))
+
+
+@pytest.mark.parametrize("path", TOMEK_CASES, ids=lambda p: p.stem)
+def test_tomek_oracle_rates_match_reference_golden(oracle, path):
+    """ToR-ORd RATES of the oracle equal the reference computeRates bit for
+    bit at every fixture state (endo/epi/mid, with and without drug), and
+    the oracle's fixed-step trajectory reproduces the fixture states."""
+    g = np.load(path)
+    c = oracle.Cell("tomek2019", float(g["celltype"]), float(g["conc"]), g["hill"], quirks=True)
+    assert np.array_equal(c.states, g["states"][0])
+    for t, st, rr in zip(g["times"], g["states"], g["ref_rates"]):
+        c.y[: c.n] = st
+        r, _ = c.rates(float(t))
+        assert np.array_equal(r, rr), f"RATES differ at t={t}"
+    c2 = oracle.Cell("tomek2019", float(g["celltype"]), float(g["conc"]), g["hill"], quirks=True)
+    every = int(round((g["times"][1] - g["times"][0]) / float(g["dt"])))
+    t = 0.0
+    for k in range(1, len(g["times"])):
+        for _ in range(every):
+            c2.step(t, float(g["dt"]))
+            t += float(g["dt"])
+        assert np.array_equal(c2.states, g["states"][k])
+
+
+@pytest.mark.parametrize("celltype", [0.0, 1.0, 2.0])
+def test_tomek_oracle_rates_bitwise_vs_compiled_reference(oracle, celltype):
+    if not oracle.ref_available("tomek2019"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    rng = np.random.default_rng(int(celltype) + 5)
+    hill = np.zeros(14)
+    hill[0::2] = 10 ** rng.uniform(-1, 2, 7)
+    hill[1::2] = rng.uniform(0.6, 1.8, 7)
+    r = oracle.RefCell("tomek2019", celltype, 1.1, hill)
+    c = oracle.Cell("tomek2019", celltype, 1.1, hill, quirks=True)
+    assert np.array_equal(r.states, c.states)
+    t = 0.0
+    for k in range(16000):  # 80 ms: stimulus, upstroke, early plateau
+        if k % 1000 == 0:
+            r.states[:] = c.states
+            r.L.ref_compute_rates(r.h, t)
+            assert np.array_equal(r.arr("rates", r.n), c.rates(t)[0])
+        c.step(t, 0.005)
+        t += 0.005
