@@ -29,6 +29,7 @@
 #include "model_ord.cuh"
 #include "model_tt2006.cuh"
 #include "model_tt2004.cuh"
+#include "model_tomek.cuh"
 #include "internal.h"
 
 namespace {
@@ -187,6 +188,37 @@ struct Tt04Model {
   __host__ __device__ static constexpr int p_stim_start() { return tt04::P_stim_start; }
   __host__ __device__ static constexpr int p_duration() { return tt04::P_duration; }
   __host__ __device__ static constexpr int p_amp() { return tt04::P_amp; }
+};
+
+struct TomekModel {
+  static constexpr bool kCipa = false;
+  static constexpr int kStates = tomek::kNumStates;
+  static constexpr int kParams = tomek::kNumParams;
+  static constexpr int kCai = tomek::cai;
+  template <class G> using Y = tomek::Y<G>;
+  template <class G> using Par = tomek::Par<G>;
+  template <class G> using Cur = tomek::Cur<G>;
+  template <class G>
+  __device__ static void load(Y<G> &y, const double *s, int64_t ld, int64_t i) { tomek::load(y, s, ld, i); }
+  template <class G>
+  __device__ static void store(const Y<G> &y, double *s, int64_t ld, int64_t i) { tomek::store(y, s, ld, i); }
+  template <class G>
+  __device__ static void load_par(Par<G> &q, const double *p, int64_t ld, int64_t i) { tomek::load_par(q, p, ld, i); }
+  template <class P>
+  __device__ static void step(Y<typename P::G> &y, const Par<typename P::G> &q, double t, double dt,
+                              int stim_mode, bool update, Cur<typename P::G> &c) {
+    tomek::step<P>(y, q, t, dt, stim_mode, update, c);
+  }
+  __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
+                              const double *hill, unsigned flags) {
+    tomek::init_instance(par, s, ld, i, ct, conc, hill, (flags & CEP_FLAG_QUIRKS) != 0);
+  }
+  template <class G>
+  __device__ static double cai_of(const Y<G> &y) { return y.cai; }
+  __host__ __device__ static constexpr int p_bcl() { return tomek::P_BCL; }
+  __host__ __device__ static constexpr int p_stim_start() { return tomek::P_stim_start; }
+  __host__ __device__ static constexpr int p_duration() { return tomek::P_duration; }
+  __host__ __device__ static constexpr int p_amp() { return tomek::P_amp; }
 };
 
 // ----------------------------------------------------------------- kernels
@@ -511,7 +543,8 @@ struct Ops {
     return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "reset launch failed");
   }
   static int launch_run(cep_batch *b, const RunArgs &a) {
-    if constexpr (std::is_same<M, Tt06Model>::value || std::is_same<M, Tt04Model>::value) {
+    if constexpr (std::is_same<M, Tt06Model>::value || std::is_same<M, Tt04Model>::value ||
+                  std::is_same<M, TomekModel>::value) {
       const int block = b->block;
       const int grid = (b->n + block - 1) / block;
       if (b->precision == CEP_PREC_MIXED)
@@ -575,6 +608,10 @@ const ModelInfo *model_info(int model) {
                                    &Ops<Tt06Model>::launch_init, &Ops<Tt06Model>::launch_pacing,
                                    &Ops<Tt06Model>::launch_reset, &Ops<Tt06Model>::launch_run,
                                    &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl(), &Ops<Tt06Model>::launch_tissue};
+  static const ModelInfo tomek_info{TomekModel::kStates, TomekModel::kParams, TomekModel::kCai,
+                                   &Ops<TomekModel>::launch_init, &Ops<TomekModel>::launch_pacing,
+                                   &Ops<TomekModel>::launch_reset, &Ops<TomekModel>::launch_run,
+                                   &Ops<TomekModel>::launch_rates, TomekModel::p_bcl(), &Ops<TomekModel>::launch_tissue};
   static const ModelInfo tt04_info{Tt04Model::kStates, Tt04Model::kParams, Tt04Model::kCai,
                                    &Ops<Tt04Model>::launch_init, &Ops<Tt04Model>::launch_pacing,
                                    &Ops<Tt04Model>::launch_reset, &Ops<Tt04Model>::launch_run,
@@ -582,6 +619,7 @@ const ModelInfo *model_info(int model) {
   switch (model) {
     case CEP_MODEL_TT2006: return &tt06_info;
     case CEP_MODEL_TT2004: return &tt04_info;
+    case CEP_MODEL_TOMEK2019: return &tomek_info;
     case CEP_MODEL_ORD2011: return &ord_info;
     case CEP_MODEL_CIPA2017: return &cipa_info;
     default: return nullptr;
