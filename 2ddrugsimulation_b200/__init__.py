@@ -150,6 +150,10 @@ _SIGS = {
     "cep_tissue_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_tissue_get_v": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "cep_tissue_get_activation": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "cep_tissue_group_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_tissue_group_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    "cep_tissue_group_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_tissue_stats": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_long), _ip]),
 }
@@ -255,8 +259,9 @@ class Batch:
         return self
 
     def set_kernel(self, variant: str):
-        """'cell' (one thread per cell) or 'roles' (4 warps per 32 cells)."""
-        _check(lib().cep_batch_set_kernel(self._h, {"cell": 0, "roles": 1}[variant]))
+        """'cell' (one thread per cell), 'roles' (4 warps per 32 cells) or
+        'pairs' (2 warps per 32 cells)."""
+        _check(lib().cep_batch_set_kernel(self._h, {"cell": 0, "roles": 1, "pairs": 2}[variant]))
         return self
 
     def run(self, n_steps: int):
@@ -560,3 +565,29 @@ class Server:
         st = ServeStats()
         _check(lib().cep_serve_stats(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+
+class TissueGroup:
+    """Tissues stepped together with one batched diffusion solve per step."""
+
+    def __init__(self, tissues):
+        self.tissues = list(tissues)
+        arr = (ctypes.c_void_p * len(self.tissues))(*[t._h.value for t in self.tissues])
+        h = ctypes.c_void_p()
+        _check(lib().cep_tissue_group_create(arr, len(self.tissues), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cep_tissue_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, n_steps: int) -> "TissueGroup":
+        _check(lib().cep_tissue_group_run(self._h, int(n_steps)))
+        return self

@@ -69,7 +69,7 @@ struct cep_batch {
   double dt = 0.005, dt_write = 1.0, qnet_thr = -1e300;
   int n_pace = 0, first_pace = -1;
   int block = 128;    // threads per block of the one-thread-per-cell kernel
-  bool roles = false; // warp-specialised kernel (4 warps per 32 cells)
+  int variant = CEP_KERNEL_CELL;  // CEP_KERNEL_*: cell, roles (4 warps / 32 cells), pairs (2 warps)
   std::vector<void *> allocs;
 };
 
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
 // inputs and operations, so the copies stay identical) and warp 0 runs the
 // biomarker state machine. The trip count is the same for every lane;
 // finished or invalid lanes are predicated off so the barrier stays uniform.
-template <class M, class P, int R>
+template <class M, class P, int R, int R2 = -1>
 __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part)[4][8][32], int lane) {
   using G = typename P::G;
   const int64_t i = (int64_t)blockIdx.x * 32 + lane;
@@ -363,12 +363,23 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     const double V0 = y.V;
     const double cai0 = M::cai_of(y);
     const auto ctx = ord::context<P>(y, q, t, a.stim_mode);
-    ord::Part<G> p;
-    ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
+    {
+      ord::Part<G> p;
+      ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
 #pragma unroll
-    for (int f = 0; f < 8; ++f) {
-      const int fld = ord::role_field(R, f);
-      if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
+      for (int f = 0; f < 8; ++f) {
+        const int fld = ord::role_field(R, f);
+        if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
+      }
+    }
+    if constexpr (R2 >= 0) {  // a warp that carries two channel groups
+      ord::Part<G> p;
+      ord::role<P, M::kCipa, R2>(y, q, ctx, a.dt, upd, p);
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        const int fld = ord::role_field(R2, f);
+        if (fld >= 0) part[buf][R2][f][lane] = p.f[fld];
+      }
     }
     __syncthreads();
     ord::Part<G> s;
@@ -404,6 +415,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   }
   if (valid) {
     ord::store_role<M::kCipa>(R, y, a.y, a.ld, i);
+    if constexpr (R2 >= 0) ord::store_role<M::kCipa>(R2, y, a.y, a.ld, i);
     if (R == 0) {
       a.t[i] = t;
       a.iout[i] = iout;
@@ -440,6 +452,21 @@ __global__ void __launch_bounds__(128) run_roles_kernel(RunArgs a) {
     case 2: role_loop<M, P, 2>(a, part, lane); break;
     default: role_loop<M, P, 3>(a, part, lane); break;
   }
+}
+
+// Two warps per 32 cells, each carrying two channel groups (Na + Ca, K + the
+// rest): half the warps of run_roles_kernel, twice the code per warp. Of the
+// three pairings this one balanced the two warps best on the CiPA
+// population (4.79e9 vs 4.49e9 cell-steps/s for Na + K | Ca + rest).
+template <class M, class P>
+__global__ void __launch_bounds__(64) run_pairs_kernel(RunArgs a) {
+  using G = typename P::G;
+  __shared__ G part[2][4][8][32];
+  const int lane = threadIdx.x & 31;
+  if ((threadIdx.x >> 5) == 0)
+    role_loop<M, P, 0, 2>(a, part, lane);
+  else
+    role_loop<M, P, 1, 3>(a, part, lane);
 }
 
 // One Godunov ionic step of a tissue: every node advances by dt from the
@@ -551,12 +578,18 @@ struct Ops {
         run_kernel<M, Mixed><<<grid, block, 0, b->stream>>>(a);
       else
         run_kernel<M, F64><<<grid, block, 0, b->stream>>>(a);
-    } else if (b->roles) {
+    } else if (b->variant == CEP_KERNEL_ROLES) {
       const int grid = (b->n + 31) / 32;
       if (b->precision == CEP_PREC_MIXED)
         run_roles_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
       else
         run_roles_kernel<M, F64><<<grid, 128, 0, b->stream>>>(a);
+    } else if (b->variant == CEP_KERNEL_PAIRS) {
+      const int grid = (b->n + 31) / 32;
+      if (b->precision == CEP_PREC_MIXED)
+        run_pairs_kernel<M, Mixed><<<grid, 64, 0, b->stream>>>(a);
+      else
+        run_pairs_kernel<M, F64><<<grid, 64, 0, b->stream>>>(a);
     } else {
       const int block = b->block;
       const int grid = (b->n + block - 1) / block;
@@ -690,9 +723,11 @@ int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     b->block = (n <= sms * 8 * 32) ? 32 : 128;
-    // Below ~1.5 waves of one-thread-per-cell occupancy the 4-warps-per-32-
-    // cells kernel keeps 4x more warps in flight.
-    b->roles = model == CEP_MODEL_ORD2011 || model == CEP_MODEL_CIPA2017 ? (n <= sms * 12 * 32) : false;
+    // Below ~1.5 waves of one-thread-per-cell occupancy the 2-warps-per-32-
+    // cells kernel keeps twice the warps in flight (10,000 CiPA instances:
+    // 4.8e9 cell-steps/s against 3.6e9 for either other form).
+    b->variant = (model == CEP_MODEL_ORD2011 || model == CEP_MODEL_CIPA2017) && n <= sms * 12 * 32 ? CEP_KERNEL_PAIRS
+                                                                                               : CEP_KERNEL_CELL;
   }
   int rc = CEP_OK;
   if ((rc = dev_alloc(b, &b->states, (size_t)b->ns * b->ld)) || (rc = dev_alloc(b, &b->params, (size_t)b->np * b->ld)) ||
@@ -733,10 +768,11 @@ int cep_batch_set_block(cep_batch_t b, int threads_per_block) {
 
 int cep_batch_set_kernel(cep_batch_t b, int variant) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
-  if (variant != CEP_KERNEL_CELL && variant != CEP_KERNEL_ROLES) return fail(CEP_ERR_ARG, "bad kernel variant %d", variant);
-  if (variant == CEP_KERNEL_ROLES && b->model != CEP_MODEL_ORD2011 && b->model != CEP_MODEL_CIPA2017)
+  if (variant != CEP_KERNEL_CELL && variant != CEP_KERNEL_ROLES && variant != CEP_KERNEL_PAIRS)
+    return fail(CEP_ERR_ARG, "bad kernel variant %d", variant);
+  if (variant != CEP_KERNEL_CELL && b->model != CEP_MODEL_ORD2011 && b->model != CEP_MODEL_CIPA2017)
     return fail(CEP_ERR_UNSUPPORTED, "warp-specialised kernel exists for the ORd family only");
-  b->roles = variant == CEP_KERNEL_ROLES;
+  b->variant = variant;
   return CEP_OK;
 }
 

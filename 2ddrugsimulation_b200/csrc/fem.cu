@@ -372,6 +372,178 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_kernel(M m, PcgArgs a) {
   }
 }
 
+// Several independent operators of one format in one cooperative launch
+// (tissues of a batch: concentrations, requests): the grid is split into
+// contiguous block ranges, one per operator in proportion to its rows; each
+// operator runs its own Jacobi-PCG with its own scalars and stopping test
+// while all share the grid barriers, so the barrier latency is paid once
+// per iteration for the whole batch. An operator that has converged idles
+// through the barriers until the last one is done.
+template <class M>
+struct PcgOp {
+  M m;
+  PcgArgs a;       // a.part holds 3 * nblocks partials, a.ctl unused
+  int block0, nblocks;
+};
+
+__device__ __forceinline__ void range_total2(const double *pa, const double *pb, int nb, double &a, double &b) {
+  __shared__ double s[2];
+  if (threadIdx.x < 32) {
+    constexpr int kU = 8;
+    double x = 0.0, y = 0.0;
+    for (int base = 0; base < nb; base += 32 * kU) {
+      double xs[kU], ys[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = base + u * 32 + threadIdx.x;
+        xs[u] = k < nb ? __ldcg(pa + k) : 0.0;
+        ys[u] = (pb && k < nb) ? __ldcg(pb + k) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        x += xs[u];
+        y += ys[u];
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(0xffffffffu, x, o);
+      y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    if (threadIdx.x == 0) {
+      s[0] = x;
+      s[1] = y;
+    }
+  }
+  __syncthreads();
+  a = s[0];
+  b = s[1];
+  __syncthreads();
+}
+
+template <class M>
+__global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__restrict__ ops, int n_ops, Ctl *ctl,
+                                                             int *ops_done, double t_new) {
+  // this block's operator
+  int o = 0;
+  while (o + 1 < n_ops && (int)blockIdx.x >= ops[o + 1].block0) ++o;
+  const M m = ops[o].m;
+  const PcgArgs a = ops[o].a;
+  const int NB = ops[o].nblocks, lb = blockIdx.x - ops[o].block0;
+  const bool lead = lb == 0 && threadIdx.x == 0;
+  const int64_t stride = (int64_t)NB * kPcgBlock;
+  const int64_t i0 = (int64_t)lb * kPcgBlock + threadIdx.x;
+  double *part0 = a.part, *part1 = a.part + NB, *part2 = a.part + 2 * NB;
+  const double *v_in = a.v;
+  double s0 = 0.0, s1 = 0.0;
+  for (int64_t i = i0; i < a.n; i += stride) {
+    const double bi = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
+    const double zi = a.dinv[i] * bi;
+    a.r[i] = bi;
+    a.z[i] = zi;
+    a.p0[i] = zi;
+    s0 = fma(bi, zi, s0);
+    s1 = a.precond_norm ? fma(zi, zi, s1) : fma(bi, bi, s1);
+  }
+  block_sum2(s0, s1);
+  if (threadIdx.x == 0) {
+    part0[lb] = s0;
+    part1[lb] = s1;
+  }
+  if (!grid_sync(ctl)) return;
+  double rz, nn0;
+  range_total2(part0, part1, NB, rz, nn0);
+  const double n0 = sqrt(nn0);
+  int it = 0, used = 0;
+  double res = n0 > 0.0 ? 1.0 : 0.0;
+  bool conv = false, done = false, counted = false;
+  if (n0 == 0.0) {
+    for (int64_t i = i0; i < a.n; i += stride) a.v[i] = 0.0;
+    conv = done = true;
+  }
+  double *pc = a.p0, *pn = a.p1;
+  double beta = 0.0;
+  for (it = 1;; ++it) {
+    // A: p_k and q = A p_k (operators still iterating); report completions
+    if (!done) {
+      double spq = 0.0, unused = 0.0;
+      if (it == 1) {
+        for (int64_t i = i0; i < a.n; i += stride) {
+          const double qi = m.apply(m.a, i, [&](int j) { return pc[j]; });
+          a.q[i] = qi;
+          spq = fma(pc[i], qi, spq);
+        }
+      } else {
+        const double *zc = a.z;
+        for (int64_t i = i0; i < a.n; i += stride) {
+          const double qi = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
+          const double pi = fma(beta, pc[i], zc[i]);
+          pn[i] = pi;
+          a.q[i] = qi;
+          spq = fma(pi, qi, spq);
+        }
+      }
+      block_sum2(spq, unused);
+      if (threadIdx.x == 0) part2[lb] = spq;
+    } else if (!counted) {
+      if (lead) atomicAdd(ops_done, 1);
+      counted = true;
+    }
+    if (!grid_sync(ctl)) return;
+    if (ld_volatile(ops_done) == n_ops) break;  // every block reads the same count here
+    if (done) {
+      if (!grid_sync(ctl)) return;
+      continue;
+    }
+    double pq, dummy;
+    range_total2(part2, nullptr, NB, pq, dummy);
+    const double alpha = rz / pq;
+    if (it > 1) {
+      double *t = pc;
+      pc = pn;
+      pn = t;
+    }
+    double srz = 0.0, snr = 0.0;
+    for (int64_t i = i0; i < a.n; i += stride) {
+      const double pi = pc[i];
+      a.v[i] = it == 1 ? alpha * pi : fma(alpha, pi, a.v[i]);
+      const double ri = fma(-alpha, a.q[i], a.r[i]);
+      const double zi = a.dinv[i] * ri;
+      a.r[i] = ri;
+      a.z[i] = zi;
+      srz = fma(ri, zi, srz);
+      snr = a.precond_norm ? fma(zi, zi, snr) : fma(ri, ri, snr);
+    }
+    block_sum2(srz, snr);
+    if (threadIdx.x == 0) {
+      part0[lb] = srz;
+      part1[lb] = snr;
+    }
+    if (!grid_sync(ctl)) return;
+    double rz_new, nr2;
+    range_total2(part0, part1, NB, rz_new, nr2);
+    const double nr = sqrt(nr2);
+    res = nr / n0;
+    used = it;
+    if (nr <= a.rtol * n0) {
+      conv = done = true;
+    } else if (it >= a.max_iter) {
+      done = true;
+    }
+    beta = rz_new / rz;
+    rz = rz_new;
+  }
+  if (a.tact)
+    for (int64_t i = i0; i < a.n; i += stride)
+      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = t_new;
+  if (lead) {
+    a.st->last_iters = conv ? used : -a.max_iter;
+    a.st->last_res = res;
+    a.st->total_iters += conv ? used : a.max_iter;
+    a.st->solves += 1;
+    if (!conv) a.st->not_converged += 1;
+  }
+}
+
 // y = A x or B x (tests and the autotuner)
 template <class M>
 __global__ void spmv_kernel(M m, int which, int64_t n, const double *x, double *y) {
@@ -831,7 +1003,163 @@ int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves,
   return CEP_OK;
 }
 
+}  // extern "C"
+
+// --------------------------------------------------------- tissue groups
+struct cep_tissue_group {
+  std::vector<cep_tissue_t> ts;
+  int format = 0, dim = 0, grid = 0;
+  cudaStream_t stream = nullptr;
+  void *d_ops = nullptr;  // PcgOp<View>[count]
+  Ctl *ctl = nullptr;
+  int *ops_done = nullptr;
+};
+
+namespace {
+
+template <class M>
+int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const cep_fem *)) {
+  std::vector<PcgOp<M>> h(g->ts.size());
+  int b0 = 0;
+  for (size_t k = 0; k < g->ts.size(); ++k) {
+    cep_fem *f = g->ts[k]->fem;
+    PcgOp<M> &o = h[k];
+    o.m = view(f);
+    o.a.n = f->n; o.a.dt = f->dt; o.a.rtol = f->rtol; o.a.max_iter = f->max_iter;
+    o.a.precond_norm = f->precond_norm;
+    o.a.v = cep_internal_batch_v(g->ts[k]->cells);
+    o.a.dinv = f->dinv;
+    o.a.r = f->r; o.a.z = f->z; o.a.p0 = f->p0; o.a.p1 = f->p1; o.a.q = f->q;
+    o.a.part = f->part;
+    o.a.ctl = nullptr;
+    o.a.st = f->st;
+    o.a.tact = g->ts[k]->tact;
+    o.a.t_new = 0.0;
+    o.a.act_thr = g->ts[k]->act_thr;
+    o.block0 = b0;
+    o.nblocks = nb[k];
+    b0 += nb[k];
+  }
+  g->grid = b0;
+  FEM_CUDA(cudaMalloc(&g->d_ops, sizeof(PcgOp<M>) * h.size()));
+  FEM_CUDA(cudaMemcpy(g->d_ops, h.data(), sizeof(PcgOp<M>) * h.size(), cudaMemcpyHostToDevice));
+  return CEP_OK;
+}
+
+template <class M>
+int group_launch(cep_tissue_group *g, double t_new) {
+  const PcgOp<M> *ops = static_cast<const PcgOp<M> *>(g->d_ops);
+  int n = (int)g->ts.size();
+  Ctl *ctl = g->ctl;
+  int *done = g->ops_done;
+  void *args[] = {&ops, &n, &ctl, &done, &t_new};
+  FEM_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(Ctl) + 64, g->stream));
+  FEM_CUDA(cudaLaunchCooperativeKernel((const void *)pcg_many_kernel<M>, dim3(g->grid), dim3(kPcgBlock), args, 0,
+                                       g->stream));
+  return CEP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_t *out) {
+  if (!ts || !out || count <= 0) return fail_msg(CEP_ERR_ARG, "bad tissue list");
+  *out = nullptr;
+  int dev = 0, sms = 0;
+  FEM_CUDA(cudaGetDevice(&dev));
+  FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (count > sms) return fail_msg(CEP_ERR_ARG, "at most %d tissues per group (one SM each at least)", sms);
+  for (int k = 0; k < count; ++k) {
+    if (!ts[k]) return fail_msg(CEP_ERR_ARG, "tissue %d is NULL", k);
+    const cep_fem *f = ts[k]->fem, *f0 = ts[0]->fem;
+    if (f->stream != f0->stream) return fail_msg(CEP_ERR_ARG, "tissues of a group share one stream");
+    if (f->format != f0->format || f->dim != f0->dim)
+      return fail_msg(CEP_ERR_ARG, "tissues of a group share one sparse format (and grid dimension)");
+    if (ts[k]->dt != ts[0]->dt || ts[k]->t != ts[0]->t) return fail_msg(CEP_ERR_ARG, "tissues of a group share dt and time");
+    for (int j = 0; j < k; ++j)
+      if (ts[j] == ts[k]) return fail_msg(CEP_ERR_ARG, "tissue %d appears twice", k);
+  }
+  // blocks in proportion to rows, at least one each, at most the operator's
+  // own partial slots, in total one per SM
+  std::vector<int> nb(count);
+  double total = 0;
+  for (int k = 0; k < count; ++k) total += ts[k]->fem->n;
+  int sum = 0;
+  for (int k = 0; k < count; ++k) {
+    nb[k] = std::max(1, std::min(ts[k]->fem->grid, (int)std::floor(sms * ts[k]->fem->n / total)));
+    sum += nb[k];
+  }
+  while (sum > sms) {
+    int kmax = (int)(std::max_element(nb.begin(), nb.end()) - nb.begin());
+    nb[kmax] -= 1;
+    sum -= 1;
+  }
+  cep_tissue_group *g = new cep_tissue_group;
+  g->ts.assign(ts, ts + count);
+  g->format = ts[0]->fem->format;
+  g->dim = ts[0]->fem->dim;
+  g->stream = ts[0]->fem->stream;
+  if (cudaMalloc((void **)&g->ctl, sizeof(Ctl) + 64) != cudaSuccess) {
+    delete g;
+    return fail_msg(CEP_ERR_OOM, "group control words");
+  }
+  g->ops_done = reinterpret_cast<int *>(reinterpret_cast<char *>(g->ctl) + sizeof(Ctl));
+  int rc;
+  if (g->format == CEP_FEM_CSR)
+    rc = group_build(g, nb, csr_view);
+  else if (g->format == CEP_FEM_STENCIL)
+    rc = g->dim == 3 ? group_build(g, nb, stencil_view<3>) : group_build(g, nb, stencil_view<2>);
+  else
+    rc = group_build(g, nb, ell_view);
+  if (rc) {
+    cudaFree(g->ctl);
+    cudaFree(g->d_ops);
+    delete g;
+    return rc;
+  }
+  *out = g;
+  return CEP_OK;
+}
+
+int cep_tissue_group_destroy(cep_tissue_group_t g) {
+  if (!g) return CEP_OK;
+  cudaStreamSynchronize(g->stream);
+  cudaFree(g->ctl);
+  cudaFree(g->d_ops);
+  delete g;
+  return CEP_OK;
+}
+
+int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
+  if (!g) return fail_msg(CEP_ERR_ARG, "null group");
+  if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");
+  for (long s = 0; s < n_steps; ++s) {
+    for (cep_tissue_t t : g->ts) {
+      int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
+      if (rc) return rc;
+    }
+    const double t_new = g->ts[0]->t + g->ts[0]->dt;
+    int rc;
+    if (g->format == CEP_FEM_CSR)
+      rc = group_launch<CsrView>(g, t_new);
+    else if (g->format == CEP_FEM_STENCIL)
+      rc = g->dim == 3 ? group_launch<StencilView<3>>(g, t_new) : group_launch<StencilView<2>>(g, t_new);
+    else
+      rc = group_launch<EllView>(g, t_new);
+    if (rc) return rc;
+    for (cep_tissue_t t : g->ts) {
+      t->t += t->dt;
+      ++t->steps;
+    }
+  }
+  return CEP_OK;
+}
+
+}  // extern "C"
+
 // ---------------------------------------------------------------- tissue
+extern "C" {
 int cep_tissue_create(cep_batch_t cells, cep_fem_t fem, double dt, cep_tissue_t *out) {
   if (!cells || !fem || !out) return fail_msg(CEP_ERR_ARG, "null argument");
   *out = nullptr;

@@ -88,7 +88,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "cell", "roles"],
+    ap.add_argument("--kernel", default="auto", choices=["auto", "cell", "roles", "pairs"],
                     help="one thread per cell, 4 warps per 32 cells, or the library's default for the size")
     a = ap.parse_args()
     if a.seg is None:
@@ -387,11 +387,12 @@ def tissue_inputs(seed: int, n_conc: int = 3):
     return [0.0, cmax, 3 * cmax][:n_conc], hill
 
 
-def make_sheet(cep, nx, prec, conc, hill):
+def make_sheet(cep, nx, prec, conc, hill, fmt=None):
     n = nx * nx
     cells = cep.Batch("tt2006", n, prec)
     cells.init(conc=np.full(n, conc), hill=hill)
-    fem = cep.Fem.grid(2, nx, nx, 1, TISSUE_H, TISSUE_DT, TISSUE_D, fmt=cep.FEM_AUTO).set_solver(TISSUE_RTOL)
+    fem = cep.Fem.grid(2, nx, nx, 1, TISSUE_H, TISSUE_DT, TISSUE_D,
+                       fmt=cep.FEM_AUTO if fmt is None else fmt).set_solver(TISSUE_RTOL)
     t = cep.Tissue(cells, fem, TISSUE_DT)
     mask = np.zeros((nx, nx), np.uint8)
     c = max(2, nx // 64)
@@ -411,10 +412,11 @@ def run_tissue(args, world, rank, local, pg):
     res = {}
     launches = 0
     for prec in ("mixed", "fp64"):
-        sheets = [make_sheet(cep, nx, prec, c, hill) for c in concs]
+        sheets = [make_sheet(cep, nx, prec, concs[0], hill)]  # autotunes the sparse format
+        sheets += [make_sheet(cep, nx, prec, c, hill, sheets[0].fem.format) for c in concs[1:]]
+        group = cep.TissueGroup(sheets)  # one batched diffusion solve per step for all sheets
         for _ in range(args.warmup):
-            for t in sheets:
-                t.run(args.seg)
+            group.run(args.seg)
             flush.zero_()
         for t in sheets:
             t.sync()
@@ -425,8 +427,7 @@ def run_tissue(args, world, rank, local, pg):
         with ClockSampler(local) as clk:
             start.record()
             for _ in range(args.steps):
-                for t in sheets:
-                    t.run(args.seg)
+                group.run(args.seg)
                 flush.zero_()
             stop.record()
             torch.cuda.synchronize()
@@ -439,7 +440,7 @@ def run_tissue(args, world, rank, local, pg):
                          cg_iters_per_solve=cg / (len(sheets) * args.seg * args.steps),
                          not_converged=sum(s["not_converged"] for s in st), fmt=sheets[0].fem.format,
                          ell_width=sheets[0].fem.ell_width)
-        launches += args.steps * len(sheets) * args.seg * 2
+        launches += args.steps * (len(sheets) + 1) * args.seg
         if prec == "mixed":
             # PCG alone on the first sheet's current V (the dominant kernel)
             f = sheets[0].fem
@@ -460,6 +461,7 @@ def run_tissue(args, world, rank, local, pg):
             res["pcg"] = dict(ms=pcg_ms, iters=iters, bytes=cg_bytes_per_row(f.ell_width) * n * iters)
             if not args.no_e2e:
                 res["e2e"] = tissue_e2e(args, sheets, n, world, pg, cep)
+        group.close()
         for t in sheets:
             t.close()
     return res, n, launches
@@ -532,7 +534,8 @@ def tissue_main(args, world, rank, local, pg):
         "dtype": "f32+f64 (mixed ionic), f64 PCG", "data": "synthetic",
         "config": {"workload": f"2D TT2006 epi sheet {args.nx}x{args.nx} Q1 nodes, dx 0.025 cm, D 0.0013 cm^2/ms, "
                                f"dt 0.01 ms, Jacobi-PCG rtol 1e-8, corner S1 at BCL 1000 ms, IKr Hill block at 3 "
-                               f"concentrations (3 sheets per GPU); {args.seg} Godunov steps per sheet per bench step",
+                               f"concentrations (3 sheets per GPU stepped as one group: one batched PCG launch per "
+                               f"step); {args.seg} Godunov steps per sheet per bench step",
                    "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell", "stencil"][mixed["fmt"]],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"sheet sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],

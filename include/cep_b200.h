@@ -98,11 +98,13 @@ int cep_batch_size(cep_batch_t b, int *n, int *n_states);
 /* Threads per block of the run kernel (32, 64, 96 or 128); the default
  * spreads small populations over every SM. Used by the autotuner. */
 int cep_batch_set_block(cep_batch_t b, int threads_per_block);
-/* Kernel form: one thread per cell, or 4 warps per 32 cells each evaluating
- * one group of channels (the default for populations smaller than ~1.5
- * waves of the GPU; ORd family only). Used by the autotuner. */
+/* Kernel form: one thread per cell; 4 warps per 32 cells each evaluating
+ * one group of channels; or 2 warps per 32 cells with two groups each (the
+ * default for populations smaller than ~1.5 waves of the GPU; ORd family
+ * only). */
 #define CEP_KERNEL_CELL 0
 #define CEP_KERNEL_ROLES 1
+#define CEP_KERNEL_PAIRS 2 /* 2 warps per 32 cells, two channel groups each */
 int cep_batch_set_kernel(cep_batch_t b, int variant);
 
 /* initConsts for every instance and the model's initial STATES.
@@ -339,6 +341,18 @@ int cep_tissue_sync(cep_tissue_t t);
 int cep_tissue_get_v(cep_tissue_t t, double *v);
 int cep_tissue_get_activation(cep_tissue_t t, double *t_act);
 int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, int *not_converged);
+
+/* A group of tissues stepped together: each keeps its own cells, operator,
+ * stimulus and solver state, but their diffusion solves share one
+ * cooperative launch per step (grid blocks split in proportion to rows), so
+ * the CG barrier latency is paid once for the whole group. The tissues must
+ * share one stream, sparse format, dt and current time; at most one tissue
+ * per SM. Results are those of stepping each tissue alone. Replaces running
+ * one Cheart (heart.cpp) per concentration or request. */
+typedef struct cep_tissue_group *cep_tissue_group_t;
+int cep_tissue_group_create(const cep_tissue_t *tissues, int count, cep_tissue_group_t *out);
+int cep_tissue_group_run(cep_tissue_group_t g, long n_steps);
+int cep_tissue_group_destroy(cep_tissue_group_t g);
 
 #ifdef __cplusplus
 }

@@ -155,14 +155,14 @@ def test_cipa_stiff_drug_binding_stays_finite(cep, gpu, oracle, precision):
 @pytest.mark.parametrize("model", ["cipa2017", "ord2011"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_roles_kernel_matches_cell_kernel(cep, gpu, model, precision):
-    """The warp-specialised kernel (4 warps per 32 cells) and the
+    """The warp-specialised kernels (4 or 2 warps per 32 cells) and the
     one-thread-per-cell kernel compute the same trajectory and biomarkers
     (the roles' contributions are added in the same order in both)."""
     conc, hill = cipa_population(20, 3, seed=21)  # 60 instances: two blocks, one partial
     if model == "ord2011":
         hill = hill[:, :14].copy()
     out = {}
-    for kern in ("cell", "roles"):
+    for kern in ("cell", "roles", "pairs"):
         b = cep.Batch(model, len(conc), precision)
         b.set_kernel(kern)
         b.init(conc=conc, hill=hill, quirks=True)
@@ -171,9 +171,10 @@ def test_roles_kernel_matches_cell_kernel(cep, gpu, model, precision):
         b.run_to_end(30000)
         out[kern] = (b.get_states(), b.biomarkers())
     s0, b0 = out["cell"]
-    s1, b1 = out["roles"]
     tol = 1e-9 if precision == "fp64" else 1e-4
-    assert np.abs(s0[:, 0] - s1[:, 0]).max() <= tol
-    for key in ("apd90", "apd50", "cad90"):
-        assert np.abs(b0[key] - b1[key]).max() <= 0.01
-    assert np.array_equal(b0["status"], b1["status"])
+    for kern in ("roles", "pairs"):
+        s1, b1 = out[kern]
+        assert np.abs(s0[:, 0] - s1[:, 0]).max() <= tol, kern
+        for key in ("apd90", "apd50", "cad90"):
+            assert np.abs(b0[key] - b1[key]).max() <= 0.01, (kern, key)
+        assert np.array_equal(b0["status"], b1["status"]), kern

@@ -185,3 +185,59 @@ def test_tissue_tt2006_matches_oracle(cep, gpu, oracle, precision):
         assert abs(st["cg_iters"] - int(itso.sum())) <= 0.02 * itso.sum()
     else:
         assert np.abs(tactg - tacto).max() <= 0.1 + 1e-9, np.abs(tactg - tacto).max()
+
+
+def _sheet(cep, nx, ny, conc, hill, precision="fp64", rtol=1e-10):
+    n = nx * ny
+    cells = cep.Batch("tt2006", n, precision)
+    cells.init(conc=np.full(n, conc), hill=hill)
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(rtol)
+    t = cep.Tissue(cells, fem, 0.01)
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:2, :2] = 1
+    t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 1)
+    return t
+
+
+@pytest.mark.gpu
+def test_tissue_group_of_one_equals_alone(cep, gpu):
+    hill = np.zeros(14)
+    a = _sheet(cep, 18, 14, 0.0, hill)
+    b = _sheet(cep, 18, 14, 0.0, hill)
+    a.run(600)
+    g = cep.TissueGroup([b])
+    g.run(600)
+    b.sync()
+    assert np.array_equal(a.v(), b.v())
+    assert np.array_equal(a.activation(), b.activation())
+    assert a.stats()["cg_iters"] == b.stats()["cg_iters"]
+
+
+@pytest.mark.gpu
+def test_tissue_group_uneven_sheets_match_individual_runs(cep, gpu, oracle):
+    """Three sheets of different sizes and drug concentrations stepped as a
+    group give each sheet's own result (solver tolerance; activation times
+    equal) and the smallest one matches the oracle."""
+    hill = np.zeros(14)
+    hill[12], hill[13] = 0.5, 1.0
+    shapes = [(20, 16, 0.0), (12, 9, 0.3), (26, 21, 1.0)]
+    steps = 900
+    alone = []
+    for nx, ny, c in shapes:
+        t = _sheet(cep, nx, ny, c, hill)
+        t.run(steps)
+        alone.append((t.v(), t.activation()))
+    group = [_sheet(cep, nx, ny, c, hill) for nx, ny, c in shapes]
+    g = cep.TissueGroup(group)
+    g.run(steps)
+    for (v0, a0), t in zip(alone, group):
+        t.sync()
+        assert np.abs(t.v() - v0).max() <= 1e-6
+        assert np.array_equal(t.activation(), a0)
+        assert t.stats()["not_converged"] == 0
+    nx, ny, c = shapes[1]
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:2, :2] = 1
+    vo, _, _ = oracle.tissue_run("tt2006", 2, nx, ny, 1, 0.025, 0.0013, 0.01, steps, mask.ravel(), 1000.0, 0.0, 1.0,
+                                 1, conc=c, hill=hill, rtol=1e-10)
+    assert np.abs(group[1].v() - vo).max() <= 1e-6
