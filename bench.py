@@ -78,7 +78,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cipa_pop", choices=["cipa_pop", "ord_pop", "tt06_sheet", "serve"])
+    ap.add_argument("--workload", default="cipa_pop",
+                    choices=["cipa_pop", "ord_pop", "tt06_sheet", "ord_slab", "serve"])
     ap.add_argument("--jobs", type=int, default=40, help="serving trace length")
     ap.add_argument("--seg", type=int, default=None,
                     help="time steps per bench step (default 10000 for populations, 200 for tissue)")
@@ -92,12 +93,13 @@ def parse():
                     help="one thread per cell, 4 warps per 32 cells, or the library's default for the size")
     a = ap.parse_args()
     if a.seg is None:
-        a.seg = 200 if a.workload == "tt06_sheet" else 10000
+        a.seg = {"tt06_sheet": 200, "ord_slab": 20}.get(a.workload, 10000)
     return a
 
 
 def model_of(workload: str) -> str:
-    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011", "tt06_sheet": "tt2006", "serve": "cipa2017"}[workload]
+    return {"cipa_pop": "cipa2017", "ord_pop": "ord2011", "tt06_sheet": "tt2006", "serve": "cipa2017",
+            "ord_slab": "ord2011"}[workload]
 
 
 # ------------------------------------------------------------ inputs
@@ -649,9 +651,134 @@ def serve_main(args):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------ 3D ORd slab workload
+SLAB_NZ, SLAB_DL, SLAB_DT_ = 48, 0.0013, 0.00045
+
+
+def slab_fields(nx: int, ny: int, nz: int):
+    """Transmural layers (endo 30 % / M 40 % / epi 30 % of the depth, ORd
+    celltypes 0 / 2 / 1), fibre angle rotating linearly from -60 to +60 deg
+    from the endocardial (z = 0) to the epicardial face, conductivity
+    D = Dt I + (Dl - Dt) f f^T per element at its centroid depth, and the
+    endocardial surface (the first two node planes, 0.025 cm: one plane
+    alone does not excite the slab against its electrotonic load) as the S1
+    region, stimulated for 1 ms."""
+    z = np.arange(nz) / (nz - 1)
+    ct_z = np.where(z < 0.3, 0.0, np.where(z < 0.7, 2.0, 1.0))
+    celltype = np.repeat(ct_z, nx * ny)
+    zc = (np.arange(nz - 1) + 0.5) / (nz - 1)
+    th = np.deg2rad(-60.0 + 120.0 * zc)
+    fx, fy = np.cos(th), np.sin(th)
+    d = np.zeros((nz - 1, 6))  # xx, xy, xz, yy, yz, zz
+    d[:, 0] = SLAB_DT_ + (SLAB_DL - SLAB_DT_) * fx * fx
+    d[:, 1] = (SLAB_DL - SLAB_DT_) * fx * fy
+    d[:, 3] = SLAB_DT_ + (SLAB_DL - SLAB_DT_) * fy * fy
+    d[:, 5] = SLAB_DT_
+    D = np.repeat(d, (nx - 1) * (ny - 1), axis=0)
+    mask = np.zeros(nx * ny * nz, np.uint8)
+    mask[: 2 * nx * ny] = 1
+    return celltype, D, mask
+
+
+def slab_main(args, world, rank, local, pg):
+    import torch
+    cep = importlib.import_module("2ddrugsimulation_b200")
+    torch.cuda.set_device(local)
+    nx = args.nx if args.nx != 512 else 256
+    ny, nz = nx, SLAB_NZ
+    n = nx * ny * nz
+    celltype, D, mask = slab_fields(nx, ny, nz)
+    rng = np.random.default_rng(5150 + rank)
+    hill = np.zeros(14)
+    hill[0::2] = 10 ** rng.uniform(-1, 2, 7)
+    hill[1::2] = rng.uniform(0.6, 1.8, 7)
+    cmax = 10 ** rng.uniform(-2, 1)
+    concs = [cmax, 3 * cmax]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = {}
+    fmt = None
+    for prec in ("mixed", "fp64"):
+        slabs = []
+        for c in concs:
+            cells = cep.Batch("ord2011", n, prec)
+            cells.init(celltype=celltype, conc=np.full(n, c), hill=hill, quirks=False)
+            fem = cep.Fem.grid(3, nx, ny, nz, TISSUE_H, TISSUE_DT, D, fmt=cep.FEM_AUTO if fmt is None else fmt)
+            fem.set_solver(TISSUE_RTOL)
+            fmt = fem.format
+            t = cep.Tissue(cells, fem, TISSUE_DT)
+            t.set_stimulus(mask, 1000.0, 0.0, 1.0, 1)
+            slabs.append(t)
+        group = cep.TissueGroup(slabs)
+        for _ in range(args.warmup):
+            group.run(args.seg)
+            flush.zero_()
+        torch.cuda.synchronize()
+        it0 = sum(t.stats()["cg_iters"] for t in slabs)
+        barrier(pg)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            start.record()
+            for _ in range(args.steps):
+                group.run(args.seg)
+                flush.zero_()
+            stop.record()
+            torch.cuda.synchronize()
+        barrier(pg)
+        ms = max_over_ranks(start.elapsed_time(stop), pg)
+        st = [t.stats() for t in slabs]
+        cg = sum(x["cg_iters"] for x in st) - it0
+        res[prec] = dict(value=n * len(slabs) * args.seg * args.steps * world / (ms / 1e3), ms_per_step=ms / args.steps,
+                         clocks=clk.summary(), cg_iters_per_solve=cg / (len(slabs) * args.seg * args.steps),
+                         not_converged=sum(x["not_converged"] for x in st), width=slabs[0].fem.ell_width)
+        group.close()
+        for t in slabs:
+            t.close()
+        del slabs
+        torch.cuda.empty_cache()
+    if rank != 0:
+        return
+    mixed, fp64 = res["mixed"], res["fp64"]
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle as O
+        cx, cz, steps = 16, 8, 600
+        ct_s, D_s, m_s = slab_fields(cx, cx, cz)
+        t0 = time.perf_counter()
+        O.tissue_run("ord2011", 3, cx, cx, cz, TISSUE_H, D_s, TISSUE_DT, steps, m_s, 1000.0, 0.0, 1.0, 1, conc=concs[0],
+                     hill=hill, rtol=TISSUE_RTOL, celltype=ct_s)
+        secs = time.perf_counter() - t0
+        cpu = {"value": cx * cx * cz * steps / secs, "unit": "node-steps/s", "cores": 1, "kind": "port",
+               "sample": f"{cx}x{cx}x{cz} slab, {steps} Godunov steps ({secs:.1f} s)"}
+    line = {
+        "metric": "ORd 3D slab node-steps/s (Godunov: ionic + Jacobi-PCG, anisotropic), mixed vs FP64",
+        "value": mixed["value"], "unit": "node-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (mixed ionic), f64 PCG", "data": "synthetic",
+        "config": {"workload": f"3D slab {nx}x{ny}x{nz} trilinear hex nodes, dx 0.025 cm, endo/M/epi ORd layers "
+                               f"30/40/30 %, fibre angle -60..+60 deg transmurally, D 0.0013/0.00045 cm^2/ms, "
+                               f"endocardial-surface S1 (2 node planes, 1 ms), dt 0.01 ms, Jacobi-PCG rtol 1e-8, 7-channel Hill drug at 2 "
+                               f"concentrations (2 slabs stepped as one group); {args.seg} Godunov steps per bench step",
+                   "nodes_per_slab": n, "slabs_per_gpu": 2, "sparse_format": ["csr", "ell", "stencil"][fmt],
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"slab sharding x{world}"},
+        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
+                 "cg_iters_per_solve": fp64["cg_iters_per_solve"]},
+        "mixed_over_fp64": mixed["value"] / fp64["value"], "cg_iters_per_solve": mixed["cg_iters_per_solve"],
+        "not_converged": mixed["not_converged"] + fp64["not_converged"],
+        "roofline": None, "gpu_launches": args.steps * args.seg * 3 * 2, "clocks": mixed["clocks"],
+        "cpu_baseline": cpu, "e2e": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     model = model_of(args.workload)
+    if args.workload == "ord_slab":
+        world, rank, local, pg = dist_setup()
+        slab_main(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.workload == "serve":
         serve_main(args)
         return

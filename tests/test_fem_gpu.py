@@ -241,3 +241,28 @@ def test_tissue_group_uneven_sheets_match_individual_runs(cep, gpu, oracle):
     vo, _, _ = oracle.tissue_run("tt2006", 2, nx, ny, 1, 0.025, 0.0013, 0.01, steps, mask.ravel(), 1000.0, 0.0, 1.0,
                                  1, conc=c, hill=hill, rtol=1e-10)
     assert np.abs(group[1].v() - vo).max() <= 1e-6
+
+
+@pytest.mark.gpu
+def test_ord_slab_3d_anisotropic_matches_oracle(cep, gpu, oracle):
+    """3D ORd slab with endo/M/epi layers (per-node celltypes, quirks off),
+    a fibre-rotated conductivity tensor per element and an endocardial S1:
+    FP64 V and activation times against the oracle's tissue loop."""
+    import bench
+    nx, ny, nz, steps = 10, 9, 6, 500
+    ct, D, mask = bench.slab_fields(nx, ny, nz)
+    hill = np.zeros(14)
+    hill[12], hill[13] = 0.8, 1.1
+    vo, _, tacto = oracle.tissue_run("ord2011", 3, nx, ny, nz, 0.025, D, 0.01, steps, mask, 1000.0, 0.0, 1.0, 1,
+                                     conc=0.4, hill=hill, rtol=1e-10, celltype=ct)
+    n = nx * ny * nz
+    cells = cep.Batch("ord2011", n, "fp64")
+    cells.init(celltype=ct, conc=np.full(n, 0.4), hill=hill, quirks=False)
+    fem = cep.Fem.grid(3, nx, ny, nz, 0.025, 0.01, D).set_solver(1e-10)
+    t = cep.Tissue(cells, fem, 0.01)
+    t.set_stimulus(mask, 1000.0, 0.0, 1.0, 1)
+    t.run(steps)
+    assert t.stats()["not_converged"] == 0
+    assert (tacto > 0).all()
+    assert np.abs(t.v() - vo).max() <= 1e-6
+    assert np.array_equal(t.activation(), tacto)
