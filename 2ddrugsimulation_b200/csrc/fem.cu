@@ -434,15 +434,25 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
   const int64_t i0 = (int64_t)lb * kPcgBlock + threadIdx.x;
   double *part0 = a.part, *part1 = a.part + NB, *part2 = a.part + 2 * NB;
   const double *v_in = a.v;
+  // Rows are taken two at a time (i and i + stride, the second clamped to a
+  // valid row and masked) so each thread keeps both rows' gathers in
+  // flight; the per-thread sums still add rows in increasing order, so the
+  // result is bit-identical to one row at a time.
   double s0 = 0.0, s1 = 0.0;
-  for (int64_t i = i0; i < a.n; i += stride) {
-    const double bi = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
-    const double zi = a.dinv[i] * bi;
-    a.r[i] = bi;
-    a.z[i] = zi;
-    a.p0[i] = zi;
-    s0 = fma(bi, zi, s0);
-    s1 = a.precond_norm ? fma(zi, zi, s1) : fma(bi, bi, s1);
+  for (int64_t i = i0; i < a.n; i += 2 * stride) {
+    const bool two = i + stride < a.n;
+    const int64_t i2 = two ? i + stride : i;
+    const double b1 = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
+    const double b2 = m.apply(m.b, i2, [&](int j) { return v_in[j]; }) / a.dt;
+    const double z1 = a.dinv[i] * b1, z2 = a.dinv[i2] * b2;
+    a.r[i] = b1; a.z[i] = z1; a.p0[i] = z1;
+    s0 = fma(b1, z1, s0);
+    s1 = a.precond_norm ? fma(z1, z1, s1) : fma(b1, b1, s1);
+    if (two) {
+      a.r[i2] = b2; a.z[i2] = z2; a.p0[i2] = z2;
+      s0 = fma(b2, z2, s0);
+      s1 = a.precond_norm ? fma(z2, z2, s1) : fma(b2, b2, s1);
+    }
   }
   block_sum2(s0, s1);
   if (threadIdx.x == 0) {
@@ -467,19 +477,34 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
     if (!done) {
       double spq = 0.0, unused = 0.0;
       if (it == 1) {
-        for (int64_t i = i0; i < a.n; i += stride) {
-          const double qi = m.apply(m.a, i, [&](int j) { return pc[j]; });
-          a.q[i] = qi;
-          spq = fma(pc[i], qi, spq);
+        for (int64_t i = i0; i < a.n; i += 2 * stride) {
+          const bool two = i + stride < a.n;
+          const int64_t i2 = two ? i + stride : i;
+          const double q1 = m.apply(m.a, i, [&](int j) { return pc[j]; });
+          const double q2 = m.apply(m.a, i2, [&](int j) { return pc[j]; });
+          a.q[i] = q1;
+          spq = fma(pc[i], q1, spq);
+          if (two) {
+            a.q[i2] = q2;
+            spq = fma(pc[i2], q2, spq);
+          }
         }
       } else {
         const double *zc = a.z;
-        for (int64_t i = i0; i < a.n; i += stride) {
-          const double qi = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
-          const double pi = fma(beta, pc[i], zc[i]);
-          pn[i] = pi;
-          a.q[i] = qi;
-          spq = fma(pi, qi, spq);
+        for (int64_t i = i0; i < a.n; i += 2 * stride) {
+          const bool two = i + stride < a.n;
+          const int64_t i2 = two ? i + stride : i;
+          const double q1 = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
+          const double q2 = m.apply(m.a, i2, [&](int j) { return fma(beta, pc[j], zc[j]); });
+          const double p1 = fma(beta, pc[i], zc[i]), p2 = fma(beta, pc[i2], zc[i2]);
+          pn[i] = p1;
+          a.q[i] = q1;
+          spq = fma(p1, q1, spq);
+          if (two) {
+            pn[i2] = p2;
+            a.q[i2] = q2;
+            spq = fma(p2, q2, spq);
+          }
         }
       }
       block_sum2(spq, unused);
@@ -503,15 +528,22 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
       pn = t;
     }
     double srz = 0.0, snr = 0.0;
-    for (int64_t i = i0; i < a.n; i += stride) {
-      const double pi = pc[i];
-      a.v[i] = it == 1 ? alpha * pi : fma(alpha, pi, a.v[i]);
-      const double ri = fma(-alpha, a.q[i], a.r[i]);
-      const double zi = a.dinv[i] * ri;
-      a.r[i] = ri;
-      a.z[i] = zi;
-      srz = fma(ri, zi, srz);
-      snr = a.precond_norm ? fma(zi, zi, snr) : fma(ri, ri, snr);
+    for (int64_t i = i0; i < a.n; i += 2 * stride) {
+      const bool two = i + stride < a.n;
+      const int64_t i2 = two ? i + stride : i;
+      const double pa = pc[i], pb = pc[i2];
+      const double va = it == 1 ? alpha * pa : fma(alpha, pa, a.v[i]);
+      const double vb = it == 1 ? alpha * pb : fma(alpha, pb, a.v[i2]);
+      const double ra = fma(-alpha, a.q[i], a.r[i]), rb = fma(-alpha, a.q[i2], a.r[i2]);
+      const double za = a.dinv[i] * ra, zb = a.dinv[i2] * rb;
+      a.v[i] = va; a.r[i] = ra; a.z[i] = za;
+      srz = fma(ra, za, srz);
+      snr = a.precond_norm ? fma(za, za, snr) : fma(ra, ra, snr);
+      if (two) {
+        a.v[i2] = vb; a.r[i2] = rb; a.z[i2] = zb;
+        srz = fma(rb, zb, srz);
+        snr = a.precond_norm ? fma(zb, zb, snr) : fma(rb, rb, snr);
+      }
     }
     block_sum2(srz, snr);
     if (threadIdx.x == 0) {
