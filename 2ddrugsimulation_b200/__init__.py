@@ -333,7 +333,7 @@ def qinward(control: Biomarkers, drug: Biomarkers) -> float:
     return float(lib().cep_qinward(ctypes.byref(control), ctypes.byref(drug)))
 
 
-FEM_AUTO, FEM_CSR, FEM_ELL, FEM_STENCIL = -1, 0, 1, 2
+FEM_AUTO, FEM_CSR, FEM_ELL, FEM_STENCIL, FEM_CLASSED = -1, 0, 1, 2, 3
 
 
 def _iptr(a: np.ndarray | None):

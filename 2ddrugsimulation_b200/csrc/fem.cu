@@ -37,6 +37,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/cep_b200.h"
@@ -143,6 +144,42 @@ struct StencilView {
                           (DIM == 2 || (unsigned)(iz + dk) < (unsigned)nz);
           const int64_t j = in ? i + di + (int64_t)nx * dj + plane * dk : i;
           s = fma(val[slot * ld + i], x((int)j), s);
+        }
+    return s;
+  }
+};
+
+// Grid operator whose rows are grouped into classes of identical
+// coefficients (a uniform sheet has 9 classes; a slab whose conductivity
+// varies only with depth has a few per plane): each row stores a class
+// index, the coefficients live once per class in a table that stays in
+// cache, so an SpMV row reads 4 bytes of matrix instead of 8 per slot.
+// Slots and columns as StencilView, so each row's sum is bit-identical.
+template <int DIM>
+struct ClassView {
+  const int *cls;
+  const double *a, *b;  // [classes][slots]
+  int nx, ny, nz;
+  template <class X>
+  __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
+    constexpr int kSlots = DIM == 3 ? 27 : 9;
+    const int64_t plane = (int64_t)nx * ny;
+    const int ix = (int)(i % nx);
+    const int iy = (int)((i / nx) % ny);
+    const int iz = DIM == 3 ? (int)(i / plane) : 0;
+    const double *c = val + (int64_t)__ldg(cls + i) * kSlots;
+    double s = 0.0;
+#pragma unroll
+    for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
+          const bool in = (unsigned)(ix + di) < (unsigned)nx && (unsigned)(iy + dj) < (unsigned)ny &&
+                          (DIM == 2 || (unsigned)(iz + dk) < (unsigned)nz);
+          const int64_t j = in ? i + di + (int64_t)nx * dj + plane * dk : i;
+          s = fma(__ldg(c + slot), x((int)j), s);
         }
     return s;
   }
@@ -638,6 +675,9 @@ struct cep_fem {
   int *rp = nullptr, *col = nullptr, *ecol = nullptr;
   double *a = nullptr, *b = nullptr, *ea = nullptr, *eb = nullptr, *dinv = nullptr;
   double *sa = nullptr, *sb = nullptr;  // stencil values (grid operators only)
+  int *cls = nullptr;                   // row classes (grid operators with few distinct rows)
+  double *ca = nullptr, *cb = nullptr;  // [classes][slots]
+  int n_classes = 0;
   int dim = 0, gnx = 0, gny = 0, gnz = 0;
   double *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr;
   Ctl *ctl = nullptr;
@@ -673,12 +713,74 @@ StencilView<D> stencil_view(const cep_fem *f) {
   return StencilView<D>{f->sa, f->sb, f->gnx, f->gny, f->gnz, f->ld};
 }
 
+template <int D>
+ClassView<D> class_view(const cep_fem *f) {
+  return ClassView<D>{f->cls, f->ca, f->cb, f->gnx, f->gny, f->gnz};
+}
+
 // Dispatch a functor on the operator's current format view.
 template <class Fn>
 auto with_view(const cep_fem *f, Fn fn) {
   if (f->format == CEP_FEM_CSR) return fn(csr_view(f));
   if (f->format == CEP_FEM_STENCIL) return f->dim == 3 ? fn(stencil_view<3>(f)) : fn(stencil_view<2>(f));
+  if (f->format == CEP_FEM_CLASSED) return f->dim == 3 ? fn(class_view<3>(f)) : fn(class_view<2>(f));
   return fn(ell_view(f));
+}
+
+// Group identical stencil rows (A and B coefficients bit-equal) into
+// classes; skipped when distinct rows exceed an eighth of the rows, where
+// the index would save little.
+int fem_build_classes(cep_fem *f) {
+  const int slots = f->dim == 3 ? 27 : 9;
+  const int64_t n = f->n, ld = f->ld;
+  std::vector<double> sa((size_t)slots * ld), sb((size_t)slots * ld);
+  FEM_CUDA(cudaMemcpy(sa.data(), f->sa, sizeof(double) * sa.size(), cudaMemcpyDeviceToHost));
+  FEM_CUDA(cudaMemcpy(sb.data(), f->sb, sizeof(double) * sb.size(), cudaMemcpyDeviceToHost));
+  std::unordered_map<uint64_t, std::vector<int>> buckets;
+  std::vector<int> cls(ld, 0);
+  std::vector<double> ta, tb;
+  const int64_t limit = std::max<int64_t>(64, n / 8);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t hsh = 1469598103934665603ull;
+    for (int k = 0; k < slots; ++k) {
+      uint64_t u, w;
+      std::memcpy(&u, &sa[(size_t)k * ld + i], 8);
+      std::memcpy(&w, &sb[(size_t)k * ld + i], 8);
+      hsh = (hsh ^ u) * 1099511628211ull;
+      hsh = (hsh ^ w) * 1099511628211ull;
+    }
+    auto &bucket = buckets[hsh];
+    int found = -1;
+    for (int c : bucket) {
+      bool eq = true;
+      for (int k = 0; k < slots && eq; ++k)
+        eq = std::memcmp(&ta[(size_t)c * slots + k], &sa[(size_t)k * ld + i], 8) == 0 &&
+             std::memcmp(&tb[(size_t)c * slots + k], &sb[(size_t)k * ld + i], 8) == 0;
+      if (eq) {
+        found = c;
+        break;
+      }
+    }
+    if (found < 0) {
+      found = (int)(ta.size() / slots);
+      if (found >= limit) return CEP_OK;  // too many distinct rows: no classed form
+      for (int k = 0; k < slots; ++k) {
+        ta.push_back(sa[(size_t)k * ld + i]);
+        tb.push_back(sb[(size_t)k * ld + i]);
+      }
+      bucket.push_back(found);
+    }
+    cls[i] = found;
+  }
+  int rc;
+  if ((rc = fem_alloc(f, &f->cls, (size_t)ld)) || (rc = fem_alloc(f, &f->ca, ta.size())) ||
+      (rc = fem_alloc(f, &f->cb, tb.size())))
+    return rc;
+  FEM_CUDA(cudaMemcpy(f->cls, cls.data(), sizeof(int) * ld, cudaMemcpyHostToDevice));
+  FEM_CUDA(cudaMemcpy(f->ca, ta.data(), sizeof(double) * ta.size(), cudaMemcpyHostToDevice));
+  FEM_CUDA(cudaMemcpy(f->cb, tb.data(), sizeof(double) * tb.size(), cudaMemcpyHostToDevice));
+  f->n_classes = (int)(ta.size() / slots);
+  return CEP_OK;
 }
 
 // Buffers shared by both formats, the cooperative grid size, and zeroed
@@ -697,6 +799,11 @@ int fem_finish_setup(cep_fem *f) {
   int per_sm_s2 = 0, per_sm_s3 = 0;
   FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s2, pcg_kernel<StencilView<2>>, kPcgBlock, 0));
   FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s3, pcg_kernel<StencilView<3>>, kPcgBlock, 0));
+  int per_sm_c2 = 0, per_sm_c3 = 0;
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c2, pcg_kernel<ClassView<2>>, kPcgBlock, 0));
+  FEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c3, pcg_kernel<ClassView<3>>, kPcgBlock, 0));
+  per_sm_s2 = std::min(per_sm_s2, per_sm_c2);
+  per_sm_s3 = std::min(per_sm_s3, per_sm_c3);
   // one block per SM: fewer arrivals per grid barrier and fewer partials
   if (std::min(std::min(per_sm_csr, per_sm_ell), std::min(per_sm_s2, per_sm_s3)) < 1)
     return fail_msg(CEP_ERR_CUDA, "PCG kernel does not fit on an SM");
@@ -757,8 +864,9 @@ int fem_autotune(cep_fem *f) {
   const unsigned grid = (unsigned)((f->n + block - 1) / block);
   float best = 1e30f;
   int best_fmt = CEP_FEM_ELL;
-  for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL, CEP_FEM_STENCIL}) {
+  for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL, CEP_FEM_STENCIL, CEP_FEM_CLASSED}) {
     if (fmt == CEP_FEM_STENCIL && !f->sa) continue;
+    if (fmt == CEP_FEM_CLASSED && !f->cls) continue;
     f->format = fmt;
     for (int rep = 0; rep < 4; ++rep) {
       cudaEventRecord(e0, f->stream);
@@ -789,8 +897,10 @@ int fem_set_format(cep_fem *f, int format) {
     FEM_CUDA(cudaMemsetAsync(f->p0, 0, sizeof(double) * f->ld, f->stream));
     return fem_autotune(f);
   }
-  if (format != CEP_FEM_CSR && format != CEP_FEM_ELL && format != CEP_FEM_STENCIL)
+  if (format != CEP_FEM_CSR && format != CEP_FEM_ELL && format != CEP_FEM_STENCIL && format != CEP_FEM_CLASSED)
     return fail_msg(CEP_ERR_ARG, "unknown sparse format %d", format);
+  if (format == CEP_FEM_CLASSED && !f->cls)
+    return fail_msg(CEP_ERR_ARG, "the classed format needs a grid operator with few distinct rows");
   if (format == CEP_FEM_STENCIL && !f->sa)
     return fail_msg(CEP_ERR_ARG, "the stencil format needs an operator built on a structured grid");
   f->format = format;
@@ -880,7 +990,7 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
     fem_free(f);
     return fail_msg(CEP_ERR_CUDA, "grid assembly failed: %s", cudaGetErrorString(e));
   }
-  if ((rc = fem_finish_setup(f)) || (rc = fem_set_format(f, format))) {
+  if ((rc = fem_build_classes(f)) || (rc = fem_finish_setup(f)) || (rc = fem_set_format(f, format))) {
     fem_free(f);
     return rc;
   }
@@ -1142,6 +1252,8 @@ int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_
     rc = group_build(g, nb, csr_view);
   else if (g->format == CEP_FEM_STENCIL)
     rc = g->dim == 3 ? group_build(g, nb, stencil_view<3>) : group_build(g, nb, stencil_view<2>);
+  else if (g->format == CEP_FEM_CLASSED)
+    rc = g->dim == 3 ? group_build(g, nb, class_view<3>) : group_build(g, nb, class_view<2>);
   else
     rc = group_build(g, nb, ell_view);
   if (rc) {
@@ -1177,6 +1289,8 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
       rc = group_launch<CsrView>(g, t_new);
     else if (g->format == CEP_FEM_STENCIL)
       rc = g->dim == 3 ? group_launch<StencilView<3>>(g, t_new) : group_launch<StencilView<2>>(g, t_new);
+    else if (g->format == CEP_FEM_CLASSED)
+      rc = g->dim == 3 ? group_launch<ClassView<3>>(g, t_new) : group_launch<ClassView<2>>(g, t_new);
     else
       rc = group_launch<EllView>(g, t_new);
     if (rc) return rc;

@@ -538,7 +538,7 @@ def tissue_main(args, world, rank, local, pg):
                                f"dt 0.01 ms, Jacobi-PCG rtol 1e-8, corner S1 at BCL 1000 ms, IKr Hill block at 3 "
                                f"concentrations (3 sheets per GPU stepped as one group: one batched PCG launch per "
                                f"step); {args.seg} Godunov steps per sheet per bench step",
-                   "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell", "stencil"][mixed["fmt"]],
+                   "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell", "stencil", "classed"][mixed["fmt"]],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"sheet sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
                  "cg_iters_per_solve": fp64["cg_iters_per_solve"]},
@@ -758,7 +758,7 @@ def slab_main(args, world, rank, local, pg):
                                f"30/40/30 %, fibre angle -60..+60 deg transmurally, D 0.0013/0.00045 cm^2/ms, "
                                f"endocardial-surface S1 (2 node planes, 1 ms), dt 0.01 ms, Jacobi-PCG rtol 1e-8, 7-channel Hill drug at 2 "
                                f"concentrations (2 slabs stepped as one group); {args.seg} Godunov steps per bench step",
-                   "nodes_per_slab": n, "slabs_per_gpu": 2, "sparse_format": ["csr", "ell", "stencil"][fmt],
+                   "nodes_per_slab": n, "slabs_per_gpu": 2, "sparse_format": ["csr", "ell", "stencil", "classed"][fmt],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"slab sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
                  "cg_iters_per_solve": fp64["cg_iters_per_solve"]},

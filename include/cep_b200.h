@@ -262,6 +262,7 @@ typedef struct cep_fem *cep_fem_t;
 #define CEP_FEM_CSR 0
 #define CEP_FEM_ELL 1     /* column-major ELL, padded to the widest row */
 #define CEP_FEM_STENCIL 2 /* grid operators: 9/27 fixed slots, implicit columns */
+#define CEP_FEM_CLASSED 3 /* grid operators: a class index per row, coefficients per class */
 
 /* Structured grid of nx*ny (dim 2, Q1 quadrilaterals) or nx*ny*nz (dim 3,
  * trilinear hexahedra) nodes at spacing h (cm), node id i + nx*(j + ny*k),

@@ -129,6 +129,61 @@ def test_formats_give_identical_solves(cep, gpu, dim, shape, kind):
     assert np.abs(out[cep.FEM_CSR][0] - out[cep.FEM_ELL][0]).max() <= 1e-9 * np.abs(v).max()
 
 
+def _layered_field(nx, ny, nz):
+    """Fibre-rotated tensor that varies with depth only, so a 3D grid has a
+    few distinct rows per plane (the classed format applies)."""
+    n_elem = (nx - 1) * (ny - 1) * (nz - 1)
+    D = np.zeros((n_elem, 6))
+    z = np.repeat(np.arange(nz - 1), (nx - 1) * (ny - 1))
+    th = np.deg2rad(-60 + 120 * z / max(nz - 2, 1))
+    dl, dt = 2e-3, 6e-4
+    D[:, 0] = dt + (dl - dt) * np.cos(th) ** 2
+    D[:, 1] = (dl - dt) * np.cos(th) * np.sin(th)
+    D[:, 3] = dt + (dl - dt) * np.sin(th) ** 2
+    D[:, 5] = dt
+    return D
+
+
+CLASSED_CASES = [(2, (40, 33, 1), 0.0013), (3, (14, 12, 9), "layered")]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,shape,field", CLASSED_CASES)
+def test_classed_format_is_bitwise_stencil(cep, gpu, oracle, dim, shape, field):
+    """Rows grouped into coefficient classes read the same coefficients in
+    the same slot order as the stencil format: SpMV and solves are bit for
+    bit the stencil's, and the SpMV matches the oracle's CSR product."""
+    nx, ny, nz = shape
+    D = _layered_field(nx, ny, nz) if field == "layered" else field
+    f = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D, fmt=cep.FEM_CLASSED).set_solver(1e-10)
+    assert f.format == cep.FEM_CLASSED
+    rp, ci, a, b = oracle.fem_assemble(dim, nx, ny, nz, 0.025, 0.01, D)
+    x = np.random.default_rng(4).uniform(-90, 30, f.n)
+    ys = {}
+    for fmt in (cep.FEM_CLASSED, cep.FEM_STENCIL):
+        f.set_format(fmt)
+        ys[fmt] = (f.spmv(x, "A"), f.spmv(x, "B"), f.solve(x))
+    for k in range(2):
+        assert np.array_equal(ys[cep.FEM_CLASSED][k], ys[cep.FEM_STENCIL][k])
+    assert ys[cep.FEM_CLASSED][2][1] == ys[cep.FEM_STENCIL][2][1]
+    assert np.array_equal(ys[cep.FEM_CLASSED][2][0], ys[cep.FEM_STENCIL][2][0])
+    for which, val in ((0, a), (1, b)):
+        ref = oracle.spmv(rp, ci, val, x)
+        scale = oracle.spmv(rp, ci, np.abs(val), np.abs(x))
+        assert np.all(np.abs(ys[cep.FEM_CLASSED][which] - ref) <= 1e-13 * scale)
+
+
+@pytest.mark.gpu
+def test_classed_format_refused_for_irregular_fields(cep, gpu):
+    """Per-element random conductivities leave nearly every row distinct:
+    the operator keeps no class table and refuses the format."""
+    nx, ny = 30, 20
+    f = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, _field(2, (nx, ny, 1), "tensor", seed=2))
+    with pytest.raises(cep.CepError) as e:
+        f.set_format(cep.FEM_CLASSED)
+    assert e.value.code == cep.ERR_ARG
+
+
 @pytest.mark.gpu
 def test_pcg_edge_cases(cep, gpu, oracle):
     f = cep.Fem.grid(2, 9, 7, 1, 0.025, 0.01, 0.0013)
@@ -187,11 +242,11 @@ def test_tissue_tt2006_matches_oracle(cep, gpu, oracle, precision):
         assert np.abs(tactg - tacto).max() <= 0.1 + 1e-9, np.abs(tactg - tacto).max()
 
 
-def _sheet(cep, nx, ny, conc, hill, precision="fp64", rtol=1e-10):
+def _sheet(cep, nx, ny, conc, hill, precision="fp64", rtol=1e-10, fmt=None):
     n = nx * ny
     cells = cep.Batch("tt2006", n, precision)
     cells.init(conc=np.full(n, conc), hill=hill)
-    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(rtol)
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013, **({} if fmt is None else {"fmt": fmt})).set_solver(rtol)
     t = cep.Tissue(cells, fem, 0.01)
     mask = np.zeros((ny, nx), np.uint8)
     mask[:2, :2] = 1
@@ -241,6 +296,22 @@ def test_tissue_group_uneven_sheets_match_individual_runs(cep, gpu, oracle):
     vo, _, _ = oracle.tissue_run("tt2006", 2, nx, ny, 1, 0.025, 0.0013, 0.01, steps, mask.ravel(), 1000.0, 0.0, 1.0,
                                  1, conc=c, hill=hill, rtol=1e-10)
     assert np.abs(group[1].v() - vo).max() <= 1e-6
+
+
+@pytest.mark.gpu
+def test_tissue_group_classed_equals_stencil(cep, gpu):
+    """A group of uniform sheets stepped on the classed format gives the
+    stencil format's V and activation times bit for bit."""
+    hill = np.zeros(14)
+    out = {}
+    for fmt in (cep.FEM_STENCIL, cep.FEM_CLASSED):
+        sheets = [_sheet(cep, nx, ny, c, hill, fmt=fmt) for nx, ny, c in ((24, 18, 0.0), (16, 16, 0.5))]
+        cep.TissueGroup(sheets).run(700)
+        for t in sheets:
+            t.sync()
+        out[fmt] = [(t.v(), t.activation(), t.stats()["cg_iters"]) for t in sheets]
+    for (v0, a0, i0), (v1, a1, i1) in zip(out[cep.FEM_STENCIL], out[cep.FEM_CLASSED]):
+        assert np.array_equal(v0, v1) and np.array_equal(a0, a1) and i0 == i1
 
 
 @pytest.mark.gpu
