@@ -154,6 +154,9 @@ _SIGS = {
                                                ctypes.POINTER(ctypes.c_void_p)]),
     "cep_tissue_group_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_tissue_group_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_tissue_group_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cep_tissue_group_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long)]),
     "cep_tissue_stats": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_long), _ip]),
 }
@@ -591,3 +594,16 @@ class TissueGroup:
     def run(self, n_steps: int) -> "TissueGroup":
         _check(lib().cep_tissue_group_run(self._h, int(n_steps)))
         return self
+
+    def set_timing(self, on: bool = True) -> "TissueGroup":
+        """Bracket each step's ionic and diffusion launches with CUDA events
+        (resets the totals)."""
+        _check(lib().cep_tissue_group_set_timing(self._h, int(bool(on))))
+        return self
+
+    def timing(self) -> dict:
+        """Device milliseconds spent in the ionic and diffusion phases since
+        set_timing, and the steps they cover (waits for them)."""
+        a, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_long()
+        _check(lib().cep_tissue_group_timing(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))
+        return {"ionic_ms": a.value, "diffusion_ms": b.value, "steps": n.value}

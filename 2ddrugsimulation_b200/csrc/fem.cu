@@ -7,9 +7,10 @@
 //
 // One solve is ONE cooperative persistent launch:
 //   phase 0   b = B V* / dt (the RHS build fused with the first residual),
-//             r = b, z = D^-1 r, p = z, partial sums of r.z and |z|^2
+//             r = b, z = D^-1 r, p_0 = 0, partial sums of r.z and |z|^2
 //   per CG iteration (two grid barriers):
-//     A   p_k = z + beta p_{k-1} evaluated on the fly inside the SpMV,
+//     A   p_k = z + beta p_{k-1} evaluated on the fly inside the SpMV
+//         (p and z interleaved: one 16-byte gather per neighbour),
 //         q = A p_k, partial p.q                             -> barrier
 //     B   x += alpha p, r -= alpha q, z = D^-1 r, partial r.z and |z|^2
 //                                                             -> barrier
@@ -23,7 +24,11 @@
 //   CSR    row_ptr[n+1] i32, col[nnz] i32, a[nnz] f64, b[nnz] f64
 //   ELL    col[width][ld] i32, a[width][ld] f64, b[width][ld] f64 (padding
 //          entries point at the row itself with weight 0)
-//   dinv[ld], r, z, p0, p1, q [ld] f64 each; partials [3][grid] f64
+//   STENCIL a[slots][ld] f64, b[slots][ld] f64 (implicit columns)
+//   CLASSED class[ld] i32, a/b [classes][slots + 1] f64
+//   dinv[ld], r[ld], q[ld] f64; two (p, z) buffers [guard + ld + guard]
+//   f64x2 (guard = one plane + one line + one node for grid operators,
+//   zeros); partials [3][grid] f64
 //
 // The grid barrier spins with an iteration limit; a barrier that runs out
 // sets an error word, every block leaves at its next barrier, and the host
@@ -85,10 +90,22 @@ struct Status {
 };
 
 struct Ctl {
-  unsigned count, gen;  // grid barrier
-  int err;              // barrier timeout
+  unsigned count;  // grid barrier arrivals (bit 31: a wait ran out)
+  unsigned pad0;
+  int err;         // barrier timeout, for the host
   int pad;
 };
+
+// The CG direction vector is kept interleaved with the preconditioned
+// residual, pz[i] = (p_{k-1}, z_k), so one 16-byte gather gives a
+// neighbour's p_k = z_k + beta p_{k-1}. apply_pz(val, i, pz, beta) is row i
+// of val * p_k in the same summation order as apply().
+__device__ __forceinline__ double p_of(const double2 t, double beta) { return fma(beta, t.x, t.y); }
+
+// Bulk L2 prefetch of [p, p + bytes) (16-byte aligned, multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
 struct CsrView {
   const int *rp, *col;
@@ -100,6 +117,10 @@ struct CsrView {
     for (int k = rp[i]; k < e; ++k) s = fma(val[k], x(col[k]), s);
     return s;
   }
+  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
+    return apply(val, i, [&](int j) { return p_of(pz[j], beta); });
+  }
+  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const double2 *) const {}
 };
 
 struct EllView {
@@ -114,6 +135,10 @@ struct EllView {
     for (int k = 0; k < width; ++k) s = fma(val[k * ld + i], x(col[k * ld + i]), s);
     return s;
   }
+  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
+    return apply(val, i, [&](int j) { return p_of(pz[j], beta); });
+  }
+  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const double2 *) const {}
 };
 
 // Structured-grid operator with implicit columns: slot (dk+1)*9 + (dj+1)*3 +
@@ -128,10 +153,10 @@ struct StencilView {
   int64_t ld;
   template <class X>
   __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
-    const int64_t plane = (int64_t)nx * ny;
-    const int ix = (int)(i % nx);
-    const int iy = (int)((i / nx) % ny);
-    const int iz = DIM == 3 ? (int)(i / plane) : 0;
+    const int ii = (int)i, plane = nx * ny;
+    const int ix = ii % nx;
+    const int iy = (ii / nx) % ny;
+    const int iz = DIM == 3 ? ii / plane : 0;
     double s = 0.0;
 #pragma unroll
     for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
@@ -142,10 +167,39 @@ struct StencilView {
           const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
           const bool in = (unsigned)(ix + di) < (unsigned)nx && (unsigned)(iy + dj) < (unsigned)ny &&
                           (DIM == 2 || (unsigned)(iz + dk) < (unsigned)nz);
-          const int64_t j = in ? i + di + (int64_t)nx * dj + plane * dk : i;
-          s = fma(val[slot * ld + i], x((int)j), s);
+          const int j = in ? ii + di + nx * dj + plane * dk : ii;
+          s = fma(val[slot * ld + i], x(j), s);
         }
     return s;
+  }
+  // Unchecked gathers: a slot outside the grid has weight 0 and reads a
+  // finite value (a wrapped neighbour, or a zero guard row before row 0 /
+  // after row n-1), adding a zero as the checked form does.
+  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
+    const double2 *ci = pz + i;
+    const int plane = nx * ny;
+    double s = 0.0;
+#pragma unroll
+    for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj) {
+        const double2 *row = ci + (nx * dj + plane * dk);
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
+          s = fma(val[slot * ld + i], p_of(row[di], beta), s);
+        }
+      }
+    return s;
+  }
+  // Rows [b, b + count) come next: fetch into L2 what the sweep has not
+  // touched yet, the leading plane (3D) or line (2D) of their
+  // neighbourhood, and their coefficient slots.
+  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const double2 *pz) const {
+    const int64_t lead = DIM == 3 ? (int64_t)nx * ny : nx;
+    int64_t lo = b + lead - nx - 1, hi = b + count + lead + nx + 1;
+    if (hi > ld_rows) hi = ld_rows;
+    if (lo < hi) prefetch_l2(pz + lo, (unsigned)((hi - lo) * sizeof(double2)));
   }
 };
 
@@ -157,17 +211,18 @@ struct StencilView {
 // Slots and columns as StencilView, so each row's sum is bit-identical.
 template <int DIM>
 struct ClassView {
+  // class rows padded to an even slot count for 16-byte coefficient loads
+  static constexpr int kSlots = DIM == 3 ? 27 : 9, kStride = kSlots + 1;
   const int *cls;
-  const double *a, *b;  // [classes][slots]
+  const double *a, *b;  // [classes][kStride]
   int nx, ny, nz;
   template <class X>
   __device__ __forceinline__ double apply(const double *val, int64_t i, X x) const {
-    constexpr int kSlots = DIM == 3 ? 27 : 9;
-    const int64_t plane = (int64_t)nx * ny;
-    const int ix = (int)(i % nx);
-    const int iy = (int)((i / nx) % ny);
-    const int iz = DIM == 3 ? (int)(i / plane) : 0;
-    const double *c = val + (int64_t)__ldg(cls + i) * kSlots;
+    const int ii = (int)i, plane = nx * ny;
+    const int ix = ii % nx;
+    const int iy = (ii / nx) % ny;
+    const int iz = DIM == 3 ? ii / plane : 0;
+    const double *c = val + (int64_t)__ldg(cls + i) * kStride;
     double s = 0.0;
 #pragma unroll
     for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
@@ -178,10 +233,39 @@ struct ClassView {
           const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
           const bool in = (unsigned)(ix + di) < (unsigned)nx && (unsigned)(iy + dj) < (unsigned)ny &&
                           (DIM == 2 || (unsigned)(iz + dk) < (unsigned)nz);
-          const int64_t j = in ? i + di + (int64_t)nx * dj + plane * dk : i;
-          s = fma(__ldg(c + slot), x((int)j), s);
+          const int j = in ? ii + di + nx * dj + plane * dk : ii;
+          s = fma(__ldg(c + slot), x(j), s);
         }
     return s;
+  }
+  // Unchecked gathers as StencilView::apply_pz; coefficients two at a time.
+  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
+    const double2 *c2 = reinterpret_cast<const double2 *>(val + (int64_t)__ldg(cls + i) * kStride);
+    const double2 *ci = pz + i;
+    const int plane = nx * ny;
+    double s = 0.0;
+    double2 cp = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj) {
+        const double2 *row = ci + (nx * dj + plane * dk);
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
+          if ((slot & 1) == 0) cp = __ldg(c2 + (slot >> 1));
+          s = fma((slot & 1) ? cp.y : cp.x, p_of(row[di], beta), s);
+        }
+      }
+    return s;
+  }
+  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const double2 *pz) const {
+    const int64_t lead = DIM == 3 ? (int64_t)nx * ny : nx;
+    int64_t lo = b + lead - nx - 1, hi = b + count + lead + nx + 1;
+    if (hi > ld_rows) hi = ld_rows;
+    if (lo < hi) prefetch_l2(pz + lo, (unsigned)((hi - lo) * sizeof(double2)));
+    int64_t ce = b + count < ld_rows ? b + count : ld_rows;
+    if (b < ce) prefetch_l2(cls + b, (unsigned)((ce - b) * sizeof(int)));
   }
 };
 
@@ -191,8 +275,10 @@ struct PcgArgs {
   int max_iter, precond_norm;
   double *v;  // in: V*, out: V
   const double *dinv;
-  double *r, *z, *p0, *p1, *q;
-  double *part;  // [3][gridDim.x]
+  int64_t ld;          // rows allocated in each vector (n rounded up to 32)
+  double *r, *q;
+  double2 *pz0, *pz1;  // (p, z) interleaved; grid formats read guard rows around [0, n)
+  double *part;  // [3][blocks]
   Ctl *ctl;
   Status *st;
   double *tact;  // activation times (may be null)
@@ -206,32 +292,48 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
-// Grid-wide barrier over co-resident blocks (cooperative launch), bounded:
-// one arrival atomic per block, the waiters poll the generation word with
-// acquire loads.
-__device__ __forceinline__ bool grid_sync(Ctl *ctl) {
+// Grid-wide barrier over co-resident blocks (cooperative launch), bounded.
+// The arrival counter only grows within a launch (zeroed before it): the
+// e-th barrier is complete once it reaches e * gridDim.x, so each block
+// makes one acquire-release atomic and the last arriver needs no second
+// write. A block whose wait runs out of its spin limit sets the poison bit
+// in the counter (and the error word the host reads); every block sees it
+// at its next arrival or poll and leaves.
+constexpr unsigned kPoison = 0x80000000u;
+
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned &epoch) {
   __shared__ int s_ok;
   __syncthreads();
+  ++epoch;
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned gen = ld_acquire(&ctl->gen);
-    __threadfence();
-    if (atomicAdd(&ctl->count, 1u) == gridDim.x - 1) {
-      atomicExch(&ctl->count, 0u);
-      __threadfence();
-      atomicAdd(&ctl->gen, 1u);
-    } else {
+    const unsigned target = epoch * gridDim.x;
+    const unsigned old = atom_add_acq_rel(&ctl->count, 1u);
+    if (old & kPoison) {
+      ok = 0;
+    } else if (old + 1u < target) {
       long spins = 0;
-      while (ld_acquire(&ctl->gen) == gen) {
+      for (;;) {
+        const unsigned c = ld_acquire(&ctl->count);
+        if (c & kPoison) {
+          ok = 0;
+          break;
+        }
+        if (c >= target) break;
         if (++spins > kSpinLimit) {
+          atomicOr(&ctl->count, kPoison);
           atomicExch(&ctl->err, 1);
           ok = 0;
           break;
         }
       }
     }
-    __threadfence();
-    if (ld_volatile(&ctl->err)) ok = 0;
     s_ok = ok;
   }
   __syncthreads();
@@ -261,152 +363,6 @@ __device__ __forceinline__ void block_sum2(double &x, double &y) {
     }
   }
   __syncthreads();
-}
-
-// Sum of gridDim.x partials in a fixed order, identical in every block; the
-// result is broadcast to the whole block. Each lane issues all its loads
-// before adding so one L2 round trip covers them.
-__device__ __forceinline__ void grid_total2(const double *pa, const double *pb, double &a, double &b) {
-  __shared__ double s[2];
-  if (threadIdx.x < 32) {
-    constexpr int kU = 8;
-    double x = 0.0, y = 0.0;
-    for (int base = 0; base < (int)gridDim.x; base += 32 * kU) {
-      double xs[kU], ys[kU];
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        const int k = base + u * 32 + threadIdx.x;
-        xs[u] = k < (int)gridDim.x ? __ldcg(pa + k) : 0.0;
-        ys[u] = (pb && k < (int)gridDim.x) ? __ldcg(pb + k) : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        x += xs[u];
-        y += ys[u];
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      x += __shfl_down_sync(0xffffffffu, x, o);
-      y += __shfl_down_sync(0xffffffffu, y, o);
-    }
-    if (threadIdx.x == 0) {
-      s[0] = x;
-      s[1] = y;
-    }
-  }
-  __syncthreads();
-  a = s[0];
-  b = s[1];
-  __syncthreads();
-}
-
-template <class M>
-__global__ void __launch_bounds__(kPcgBlock) pcg_kernel(M m, PcgArgs a) {
-  const int64_t stride = (int64_t)gridDim.x * kPcgBlock;
-  const int64_t i0 = (int64_t)blockIdx.x * kPcgBlock + threadIdx.x;
-  const int G = gridDim.x;
-  double *part0 = a.part, *part1 = a.part + G, *part2 = a.part + 2 * G;
-  const double *v_in = a.v;
-  // phase 0: RHS and first residual
-  double s0 = 0.0, s1 = 0.0;
-  for (int64_t i = i0; i < a.n; i += stride) {
-    const double bi = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
-    const double zi = a.dinv[i] * bi;
-    a.r[i] = bi;
-    a.z[i] = zi;
-    a.p0[i] = zi;
-    s0 = fma(bi, zi, s0);
-    s1 = a.precond_norm ? fma(zi, zi, s1) : fma(bi, bi, s1);
-  }
-  block_sum2(s0, s1);
-  if (threadIdx.x == 0) {
-    part0[blockIdx.x] = s0;
-    part1[blockIdx.x] = s1;
-  }
-  if (!grid_sync(a.ctl)) return;
-  double rz, nn0;
-  grid_total2(part0, part1, rz, nn0);
-  const double n0 = sqrt(nn0);
-  int it = 0;
-  double res = n0 > 0.0 ? 1.0 : 0.0;
-  bool conv = false;
-  if (n0 == 0.0) {
-    for (int64_t i = i0; i < a.n; i += stride) a.v[i] = 0.0;
-    conv = true;
-  } else {
-    double *pc = a.p0, *pn = a.p1;
-    double beta = 0.0;
-    for (it = 1; it <= a.max_iter; ++it) {
-      // A: p_k (on the fly) and q = A p_k
-      double spq = 0.0, unused = 0.0;
-      if (it == 1) {
-        for (int64_t i = i0; i < a.n; i += stride) {
-          const double qi = m.apply(m.a, i, [&](int j) { return pc[j]; });
-          a.q[i] = qi;
-          spq = fma(pc[i], qi, spq);
-        }
-      } else {
-        const double *zc = a.z;
-        for (int64_t i = i0; i < a.n; i += stride) {
-          const double qi = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
-          const double pi = fma(beta, pc[i], zc[i]);
-          pn[i] = pi;
-          a.q[i] = qi;
-          spq = fma(pi, qi, spq);
-        }
-      }
-      block_sum2(spq, unused);
-      if (threadIdx.x == 0) part2[blockIdx.x] = spq;
-      if (!grid_sync(a.ctl)) return;
-      double pq, dummy;
-      grid_total2(part2, nullptr, pq, dummy);
-      const double alpha = rz / pq;
-      if (it > 1) {
-        double *t = pc;
-        pc = pn;
-        pn = t;
-      }
-      // B: x, r, z
-      double srz = 0.0, snr = 0.0;
-      for (int64_t i = i0; i < a.n; i += stride) {
-        const double pi = pc[i];
-        a.v[i] = it == 1 ? alpha * pi : fma(alpha, pi, a.v[i]);
-        const double ri = fma(-alpha, a.q[i], a.r[i]);
-        const double zi = a.dinv[i] * ri;
-        a.r[i] = ri;
-        a.z[i] = zi;
-        srz = fma(ri, zi, srz);
-        snr = a.precond_norm ? fma(zi, zi, snr) : fma(ri, ri, snr);
-      }
-      block_sum2(srz, snr);
-      if (threadIdx.x == 0) {
-        part0[blockIdx.x] = srz;
-        part1[blockIdx.x] = snr;
-      }
-      if (!grid_sync(a.ctl)) return;
-      double rz_new, nr2;
-      grid_total2(part0, part1, rz_new, nr2);
-      const double nr = sqrt(nr2);
-      res = nr / n0;
-      if (nr <= a.rtol * n0) {
-        conv = true;
-        break;
-      }
-      beta = rz_new / rz;
-      rz = rz_new;
-    }
-  }
-  if (a.tact)
-    for (int64_t i = i0; i < a.n; i += stride)
-      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = a.t_new;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const int used = conv ? it : -a.max_iter;
-    a.st->last_iters = used;
-    a.st->last_res = res;
-    a.st->total_iters += conv ? it : a.max_iter;
-    a.st->solves += 1;
-    if (!conv) a.st->not_converged += 1;
-  }
 }
 
 // Several independent operators of one format in one cooperative launch
@@ -457,24 +413,28 @@ __device__ __forceinline__ void range_total2(const double *pa, const double *pb,
   __syncthreads();
 }
 
+// Jacobi-PCG of one operator on block lb of the NB blocks it owns (the
+// whole grid for a single solve, a contiguous range of a batched launch).
+// Each thread takes rows two at a time (i and i + stride, the second
+// clamped to a valid row and masked) so both rows' gathers are in flight;
+// its partial sums still add rows in increasing order. In a batched launch
+// (n_ops > 1) an operator that has converged keeps taking the grid barriers
+// until every operator has, counted in ops_done.
+//
+// Vectors: r, q and the caller's V (x), and two (p, z) buffers used in
+// turn. Iteration k: pass A reads (p_{k-1}, z_{k-1}) around each row, forms
+// p_k, writes it to the other buffer's p half and q = A p_k; pass B updates
+// x and r and writes z_k into that buffer's z half.
 template <class M>
-__global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__restrict__ ops, int n_ops, Ctl *ctl,
-                                                             int *ops_done, double t_new) {
-  // this block's operator
-  int o = 0;
-  while (o + 1 < n_ops && (int)blockIdx.x >= ops[o + 1].block0) ++o;
-  const M m = ops[o].m;
-  const PcgArgs a = ops[o].a;
-  const int NB = ops[o].nblocks, lb = blockIdx.x - ops[o].block0;
+__device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, int lb, Ctl *ctl, int *ops_done,
+                                         int n_ops) {
   const bool lead = lb == 0 && threadIdx.x == 0;
   const int64_t stride = (int64_t)NB * kPcgBlock;
   const int64_t i0 = (int64_t)lb * kPcgBlock + threadIdx.x;
   double *part0 = a.part, *part1 = a.part + NB, *part2 = a.part + 2 * NB;
   const double *v_in = a.v;
-  // Rows are taken two at a time (i and i + stride, the second clamped to a
-  // valid row and masked) so each thread keeps both rows' gathers in
-  // flight; the per-thread sums still add rows in increasing order, so the
-  // result is bit-identical to one row at a time.
+  unsigned epoch = 0;  // grid barriers passed
+  // phase 0: b = B V / dt, r = b, z = D^-1 b, p_0 = 0
   double s0 = 0.0, s1 = 0.0;
   for (int64_t i = i0; i < a.n; i += 2 * stride) {
     const bool two = i + stride < a.n;
@@ -482,11 +442,13 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
     const double b1 = m.apply(m.b, i, [&](int j) { return v_in[j]; }) / a.dt;
     const double b2 = m.apply(m.b, i2, [&](int j) { return v_in[j]; }) / a.dt;
     const double z1 = a.dinv[i] * b1, z2 = a.dinv[i2] * b2;
-    a.r[i] = b1; a.z[i] = z1; a.p0[i] = z1;
+    a.r[i] = b1;
+    a.pz0[i] = make_double2(0.0, z1);
     s0 = fma(b1, z1, s0);
     s1 = a.precond_norm ? fma(z1, z1, s1) : fma(b1, b1, s1);
     if (two) {
-      a.r[i2] = b2; a.z[i2] = z2; a.p0[i2] = z2;
+      a.r[i2] = b2;
+      a.pz0[i2] = make_double2(0.0, z2);
       s0 = fma(b2, z2, s0);
       s1 = a.precond_norm ? fma(z2, z2, s1) : fma(b2, b2, s1);
     }
@@ -496,52 +458,42 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
     part0[lb] = s0;
     part1[lb] = s1;
   }
-  if (!grid_sync(ctl)) return;
+  if (!grid_sync(ctl, epoch)) return;
   double rz, nn0;
   range_total2(part0, part1, NB, rz, nn0);
   const double n0 = sqrt(nn0);
-  int it = 0, used = 0;
+  int used = 0;
   double res = n0 > 0.0 ? 1.0 : 0.0;
   bool conv = false, done = false, counted = false;
   if (n0 == 0.0) {
     for (int64_t i = i0; i < a.n; i += stride) a.v[i] = 0.0;
     conv = done = true;
   }
-  double *pc = a.p0, *pn = a.p1;
-  double beta = 0.0;
-  for (it = 1;; ++it) {
+  double2 *pc = a.pz0, *pn = a.pz1;
+  double beta = 0.0;  // p_1 = z_0 + 0 * p_0
+  for (int it = 1; !(n_ops == 1 && done); ++it) {
     // A: p_k and q = A p_k (operators still iterating); report completions
     if (!done) {
       double spq = 0.0, unused = 0.0;
-      if (it == 1) {
-        for (int64_t i = i0; i < a.n; i += 2 * stride) {
-          const bool two = i + stride < a.n;
-          const int64_t i2 = two ? i + stride : i;
-          const double q1 = m.apply(m.a, i, [&](int j) { return pc[j]; });
-          const double q2 = m.apply(m.a, i2, [&](int j) { return pc[j]; });
-          a.q[i] = q1;
-          spq = fma(pc[i], q1, spq);
-          if (two) {
-            a.q[i2] = q2;
-            spq = fma(pc[i2], q2, spq);
-          }
+      for (int64_t i = i0; i < a.n; i += 2 * stride) {
+        // the block's rows two trips ahead, fetched into L2 by one thread
+        if (threadIdx.x == 0) {
+          const int64_t nb = i + 2 * stride;
+          m.prefetch(nb, kPcgBlock, a.ld, pc);
+          m.prefetch(nb + stride, kPcgBlock, a.ld, pc);
         }
-      } else {
-        const double *zc = a.z;
-        for (int64_t i = i0; i < a.n; i += 2 * stride) {
-          const bool two = i + stride < a.n;
-          const int64_t i2 = two ? i + stride : i;
-          const double q1 = m.apply(m.a, i, [&](int j) { return fma(beta, pc[j], zc[j]); });
-          const double q2 = m.apply(m.a, i2, [&](int j) { return fma(beta, pc[j], zc[j]); });
-          const double p1 = fma(beta, pc[i], zc[i]), p2 = fma(beta, pc[i2], zc[i2]);
-          pn[i] = p1;
-          a.q[i] = q1;
-          spq = fma(p1, q1, spq);
-          if (two) {
-            pn[i2] = p2;
-            a.q[i2] = q2;
-            spq = fma(p2, q2, spq);
-          }
+        const bool two = i + stride < a.n;
+        const int64_t i2 = two ? i + stride : i;
+        const double q1 = m.apply_pz(m.a, i, pc, beta);
+        const double q2 = m.apply_pz(m.a, i2, pc, beta);
+        const double p1 = p_of(pc[i], beta), p2 = p_of(pc[i2], beta);
+        reinterpret_cast<double *>(pn + i)[0] = p1;
+        a.q[i] = q1;
+        spq = fma(p1, q1, spq);
+        if (two) {
+          reinterpret_cast<double *>(pn + i2)[0] = p2;
+          a.q[i2] = q2;
+          spq = fma(p2, q2, spq);
         }
       }
       block_sum2(spq, unused);
@@ -550,34 +502,40 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
       if (lead) atomicAdd(ops_done, 1);
       counted = true;
     }
-    if (!grid_sync(ctl)) return;
-    if (ld_volatile(ops_done) == n_ops) break;  // every block reads the same count here
-    if (done) {
-      if (!grid_sync(ctl)) return;
-      continue;
+    if (!grid_sync(ctl, epoch)) return;
+    if (n_ops > 1) {
+      if (ld_volatile(ops_done) == n_ops) break;  // every block reads the same count here
+      if (done) {
+        if (!grid_sync(ctl, epoch)) return;
+        continue;
+      }
     }
     double pq, dummy;
     range_total2(part2, nullptr, NB, pq, dummy);
     const double alpha = rz / pq;
-    if (it > 1) {
-      double *t = pc;
-      pc = pn;
-      pn = t;
-    }
+    double2 *t = pc;  // pn now holds p_k
+    pc = pn;
+    pn = t;
+    // B: x += alpha p, r -= alpha q, z = D^-1 r
     double srz = 0.0, snr = 0.0;
     for (int64_t i = i0; i < a.n; i += 2 * stride) {
       const bool two = i + stride < a.n;
       const int64_t i2 = two ? i + stride : i;
-      const double pa = pc[i], pb = pc[i2];
+      double *ha = reinterpret_cast<double *>(pc + i), *hb = reinterpret_cast<double *>(pc + i2);
+      const double pa = ha[0], pb = hb[0];
       const double va = it == 1 ? alpha * pa : fma(alpha, pa, a.v[i]);
       const double vb = it == 1 ? alpha * pb : fma(alpha, pb, a.v[i2]);
       const double ra = fma(-alpha, a.q[i], a.r[i]), rb = fma(-alpha, a.q[i2], a.r[i2]);
       const double za = a.dinv[i] * ra, zb = a.dinv[i2] * rb;
-      a.v[i] = va; a.r[i] = ra; a.z[i] = za;
+      a.v[i] = va;
+      a.r[i] = ra;
+      ha[1] = za;
       srz = fma(ra, za, srz);
       snr = a.precond_norm ? fma(za, za, snr) : fma(ra, ra, snr);
       if (two) {
-        a.v[i2] = vb; a.r[i2] = rb; a.z[i2] = zb;
+        a.v[i2] = vb;
+        a.r[i2] = rb;
+        hb[1] = zb;
         srz = fma(rb, zb, srz);
         snr = a.precond_norm ? fma(zb, zb, snr) : fma(rb, rb, snr);
       }
@@ -587,7 +545,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
       part0[lb] = srz;
       part1[lb] = snr;
     }
-    if (!grid_sync(ctl)) return;
+    if (!grid_sync(ctl, epoch)) return;
     double rz_new, nr2;
     range_total2(part0, part1, NB, rz_new, nr2);
     const double nr = sqrt(nr2);
@@ -603,7 +561,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
   }
   if (a.tact)
     for (int64_t i = i0; i < a.n; i += stride)
-      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = t_new;
+      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = a.t_new;
   if (lead) {
     a.st->last_iters = conv ? used : -a.max_iter;
     a.st->last_res = res;
@@ -613,12 +571,36 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__r
   }
 }
 
-// y = A x or B x (tests and the autotuner)
+// One operator over the whole cooperative grid.
+template <class M>
+__global__ void __launch_bounds__(kPcgBlock) pcg_kernel(M m, PcgArgs a) {
+  pcg_body(m, a, (int)gridDim.x, (int)blockIdx.x, a.ctl, nullptr, 1);
+}
+
+// Several operators, each on its own block range (see PcgOp).
+template <class M>
+__global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__restrict__ ops, int n_ops, Ctl *ctl,
+                                                             int *ops_done, double t_new) {
+  int o = 0;
+  while (o + 1 < n_ops && (int)blockIdx.x >= ops[o + 1].block0) ++o;
+  const M m = ops[o].m;
+  PcgArgs a = ops[o].a;
+  a.t_new = t_new;
+  pcg_body(m, a, ops[o].nblocks, (int)blockIdx.x - ops[o].block0, ctl, ops_done, n_ops);
+}
+
+// y = A x or B x (tests)
 template <class M>
 __global__ void spmv_kernel(M m, int which, int64_t n, const double *x, double *y) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   y[i] = m.apply(which ? m.b : m.a, i, [&](int j) { return x[j]; });
+}
+
+// A smooth membrane-potential-like field for the format autotuner.
+__global__ void smooth_field_kernel(int64_t n, double *v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = -40.0 + 45.0 * sin(1e-3 * (double)i);
 }
 
 __global__ void csr_to_ell_kernel(int64_t n, const int *rp, const int *col, const double *a, const double *b,
@@ -679,7 +661,9 @@ struct cep_fem {
   double *ca = nullptr, *cb = nullptr;  // [classes][slots]
   int n_classes = 0;
   int dim = 0, gnx = 0, gny = 0, gnz = 0;
-  double *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *part = nullptr;
+  double *r = nullptr, *q = nullptr, *part = nullptr;
+  double2 *pz0 = nullptr, *pz1 = nullptr;  // row 0 of [guard | ld | guard] zero-filled buffers
+  int64_t guard = 0;                       // rows a grid-format gather may reach past either end
   Ctl *ctl = nullptr;
   Status *st = nullptr;
   int grid = 0;
@@ -740,6 +724,7 @@ int fem_build_classes(cep_fem *f) {
   std::vector<int> cls(ld, 0);
   std::vector<double> ta, tb;
   const int64_t limit = std::max<int64_t>(64, n / 8);
+  const int stride = slots + 1;  // even, for 16-byte coefficient loads
   for (int64_t i = 0; i < n; ++i) {
     uint64_t hsh = 1469598103934665603ull;
     for (int k = 0; k < slots; ++k) {
@@ -754,20 +739,22 @@ int fem_build_classes(cep_fem *f) {
     for (int c : bucket) {
       bool eq = true;
       for (int k = 0; k < slots && eq; ++k)
-        eq = std::memcmp(&ta[(size_t)c * slots + k], &sa[(size_t)k * ld + i], 8) == 0 &&
-             std::memcmp(&tb[(size_t)c * slots + k], &sb[(size_t)k * ld + i], 8) == 0;
+        eq = std::memcmp(&ta[(size_t)c * stride + k], &sa[(size_t)k * ld + i], 8) == 0 &&
+             std::memcmp(&tb[(size_t)c * stride + k], &sb[(size_t)k * ld + i], 8) == 0;
       if (eq) {
         found = c;
         break;
       }
     }
     if (found < 0) {
-      found = (int)(ta.size() / slots);
+      found = (int)(ta.size() / stride);
       if (found >= limit) return CEP_OK;  // too many distinct rows: no classed form
       for (int k = 0; k < slots; ++k) {
         ta.push_back(sa[(size_t)k * ld + i]);
         tb.push_back(sb[(size_t)k * ld + i]);
       }
+      ta.push_back(0.0);
+      tb.push_back(0.0);
       bucket.push_back(found);
     }
     cls[i] = found;
@@ -779,7 +766,7 @@ int fem_build_classes(cep_fem *f) {
   FEM_CUDA(cudaMemcpy(f->cls, cls.data(), sizeof(int) * ld, cudaMemcpyHostToDevice));
   FEM_CUDA(cudaMemcpy(f->ca, ta.data(), sizeof(double) * ta.size(), cudaMemcpyHostToDevice));
   FEM_CUDA(cudaMemcpy(f->cb, tb.data(), sizeof(double) * tb.size(), cudaMemcpyHostToDevice));
-  f->n_classes = (int)(ta.size() / slots);
+  f->n_classes = (int)(ta.size() / stride);
   return CEP_OK;
 }
 
@@ -788,9 +775,15 @@ int fem_build_classes(cep_fem *f) {
 int fem_finish_setup(cep_fem *f) {
   int rc;
   const size_t ld = (size_t)f->ld;
-  if ((rc = fem_alloc(f, &f->r, ld)) || (rc = fem_alloc(f, &f->z, ld)) || (rc = fem_alloc(f, &f->p0, ld)) ||
-      (rc = fem_alloc(f, &f->p1, ld)) || (rc = fem_alloc(f, &f->q, ld)))
-    return rc;
+  if ((rc = fem_alloc(f, &f->r, ld)) || (rc = fem_alloc(f, &f->q, ld))) return rc;
+  // grid formats gather up to one plane + one line + one node either side
+  f->guard = f->dim == 3 ? (int64_t)f->gnx * f->gny + f->gnx + 1 : f->dim == 2 ? (int64_t)f->gnx + 1 : 0;
+  const size_t span = ld + 2 * (size_t)f->guard;
+  for (double2 **pz : {&f->pz0, &f->pz1}) {
+    if ((rc = fem_alloc(f, pz, span))) return rc;
+    FEM_CUDA(cudaMemsetAsync(*pz, 0, sizeof(double2) * span, f->stream));
+    *pz += f->guard;
+  }
   int dev = 0, sms = 0, per_sm_csr = 0, per_sm_ell = 0;
   FEM_CUDA(cudaGetDevice(&dev));
   FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -822,13 +815,14 @@ template <class M>
 int launch_pcg(cep_fem *f, const M &m, double *v, double *tact, double t_new, double thr) {
   PcgArgs a;
   a.n = f->n;
+  a.ld = f->ld;
   a.dt = f->dt;
   a.rtol = f->rtol;
   a.max_iter = f->max_iter;
   a.precond_norm = f->precond_norm;
   a.v = v;
   a.dinv = f->dinv;
-  a.r = f->r; a.z = f->z; a.p0 = f->p0; a.p1 = f->p1; a.q = f->q;
+  a.r = f->r; a.q = f->q; a.pz0 = f->pz0; a.pz1 = f->pz1;
   a.part = f->part;
   a.ctl = f->ctl;
   a.st = f->st;
@@ -855,28 +849,33 @@ int fem_check_ctl(cep_fem *f) {
   return CEP_OK;
 }
 
-// CSR vs ELL: time a few SpMVs of each and keep the faster.
+// Time short fixed-length CG solves (8 iterations, no early stop) in each
+// available format on a smooth synthetic field and keep the fastest. The
+// operator's counters and solver settings are restored afterwards.
 int fem_autotune(cep_fem *f) {
+  double *tv = nullptr;
+  FEM_CUDA(cudaMalloc(&tv, sizeof(double) * f->ld));
+  Status saved;
+  FEM_CUDA(cudaMemcpy(&saved, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  const double rtol = f->rtol;
+  const int max_iter = f->max_iter;
+  f->rtol = 1e-300;
+  f->max_iter = 8;
   cudaEvent_t e0, e1;
   FEM_CUDA(cudaEventCreate(&e0));
   FEM_CUDA(cudaEventCreate(&e1));
-  const int block = 256;
-  const unsigned grid = (unsigned)((f->n + block - 1) / block);
   float best = 1e30f;
-  int best_fmt = CEP_FEM_ELL;
+  int best_fmt = CEP_FEM_ELL, rc = CEP_OK;
   for (int fmt : {CEP_FEM_CSR, CEP_FEM_ELL, CEP_FEM_STENCIL, CEP_FEM_CLASSED}) {
     if (fmt == CEP_FEM_STENCIL && !f->sa) continue;
     if (fmt == CEP_FEM_CLASSED && !f->cls) continue;
     f->format = fmt;
-    for (int rep = 0; rep < 4; ++rep) {
+    for (int rep = 0; rep < 3 && rc == CEP_OK; ++rep) {
+      smooth_field_kernel<<<(unsigned)((f->n + 255) / 256), 256, 0, f->stream>>>((int64_t)f->n, tv);
       cudaEventRecord(e0, f->stream);
-      for (int k = 0; k < 20; ++k)
-        with_view(f, [&](auto m) {
-          spmv_kernel<<<grid, block, 0, f->stream>>>(m, 0, (int64_t)f->n, f->p0, f->q);
-          return 0;
-        });
+      rc = fem_solve_async(f, tv, nullptr, 0.0, 0.0);
       cudaEventRecord(e1, f->stream);
-      cudaEventSynchronize(e1);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail_msg(CEP_ERR_CUDA, "autotune solve failed");
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       if (rep >= 1 && ms < best) {
@@ -887,16 +886,19 @@ int fem_autotune(cep_fem *f) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  f->rtol = rtol;
+  f->max_iter = max_iter;
+  cudaFree(tv);
+  if (rc) return rc;
+  if ((rc = fem_check_ctl(f))) return rc;
+  FEM_CUDA(cudaMemcpy(f->st, &saved, sizeof(Status), cudaMemcpyHostToDevice));
   FEM_CUDA(cudaGetLastError());
   f->format = best_fmt;
   return CEP_OK;
 }
 
 int fem_set_format(cep_fem *f, int format) {
-  if (format == CEP_FEM_AUTO) {
-    FEM_CUDA(cudaMemsetAsync(f->p0, 0, sizeof(double) * f->ld, f->stream));
-    return fem_autotune(f);
-  }
+  if (format == CEP_FEM_AUTO) return fem_autotune(f);
   if (format != CEP_FEM_CSR && format != CEP_FEM_ELL && format != CEP_FEM_STENCIL && format != CEP_FEM_CLASSED)
     return fail_msg(CEP_ERR_ARG, "unknown sparse format %d", format);
   if (format == CEP_FEM_CLASSED && !f->cls)
@@ -1084,7 +1086,8 @@ int cep_fem_get_csr(cep_fem_t f, int *row_ptr, int *col_idx, double *a_val, doub
 
 int cep_fem_set_solver(cep_fem_t f, double rtol, int max_iter, int precond_norm) {
   if (!f) return fail_msg(CEP_ERR_ARG, "null operator");
-  if (!(rtol > 0) || max_iter <= 0) return fail_msg(CEP_ERR_ARG, "rtol and max_iter must be positive");
+  if (!(rtol > 0) || max_iter <= 0 || max_iter > CEP_FEM_MAX_ITER)
+    return fail_msg(CEP_ERR_ARG, "rtol must be positive and max_iter in 1..%d", CEP_FEM_MAX_ITER);
   f->rtol = rtol;
   f->max_iter = max_iter;
   f->precond_norm = precond_norm ? 1 : 0;
@@ -1155,9 +1158,44 @@ struct cep_tissue_group {
   void *d_ops = nullptr;  // PcgOp<View>[count]
   Ctl *ctl = nullptr;
   int *ops_done = nullptr;
+  // optional per-phase timing: three events per step (before the ionic
+  // launches, before the diffusion launch, after it), folded into the
+  // totals when read or when the pool is used up
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;
+  size_t ev_used = 0;
+  double ionic_ms = 0.0, diffusion_ms = 0.0;
+  long timed_steps = 0;
 };
 
 namespace {
+
+constexpr size_t kGroupEvents = 3 * 1024;
+
+int group_fold_timing(cep_tissue_group *g) {
+  if (g->ev_used == 0) return CEP_OK;
+  FEM_CUDA(cudaEventSynchronize(g->ev[g->ev_used - 1]));
+  for (size_t k = 0; k + 3 <= g->ev_used; k += 3) {
+    float a = 0.f, b = 0.f;
+    FEM_CUDA(cudaEventElapsedTime(&a, g->ev[k], g->ev[k + 1]));
+    FEM_CUDA(cudaEventElapsedTime(&b, g->ev[k + 1], g->ev[k + 2]));
+    g->ionic_ms += a;
+    g->diffusion_ms += b;
+    ++g->timed_steps;
+  }
+  g->ev_used = 0;
+  return CEP_OK;
+}
+
+int group_event(cep_tissue_group *g) {
+  if (g->ev_used == g->ev.size()) {
+    cudaEvent_t e;
+    FEM_CUDA(cudaEventCreate(&e));
+    g->ev.push_back(e);
+  }
+  FEM_CUDA(cudaEventRecord(g->ev[g->ev_used++], g->stream));
+  return CEP_OK;
+}
 
 template <class M>
 int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const cep_fem *)) {
@@ -1167,11 +1205,11 @@ int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const
     cep_fem *f = g->ts[k]->fem;
     PcgOp<M> &o = h[k];
     o.m = view(f);
-    o.a.n = f->n; o.a.dt = f->dt; o.a.rtol = f->rtol; o.a.max_iter = f->max_iter;
+    o.a.n = f->n; o.a.ld = f->ld; o.a.dt = f->dt; o.a.rtol = f->rtol; o.a.max_iter = f->max_iter;
     o.a.precond_norm = f->precond_norm;
     o.a.v = cep_internal_batch_v(g->ts[k]->cells);
     o.a.dinv = f->dinv;
-    o.a.r = f->r; o.a.z = f->z; o.a.p0 = f->p0; o.a.p1 = f->p1; o.a.q = f->q;
+    o.a.r = f->r; o.a.q = f->q; o.a.pz0 = f->pz0; o.a.pz1 = f->pz1;
     o.a.part = f->part;
     o.a.ctl = nullptr;
     o.a.st = f->st;
@@ -1269,9 +1307,30 @@ int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_
 int cep_tissue_group_destroy(cep_tissue_group_t g) {
   if (!g) return CEP_OK;
   cudaStreamSynchronize(g->stream);
+  for (cudaEvent_t e : g->ev) cudaEventDestroy(e);
   cudaFree(g->ctl);
   cudaFree(g->d_ops);
   delete g;
+  return CEP_OK;
+}
+
+int cep_tissue_group_set_timing(cep_tissue_group_t g, int on) {
+  if (!g) return fail_msg(CEP_ERR_ARG, "null group");
+  int rc;
+  if ((rc = group_fold_timing(g))) return rc;
+  g->timing = on != 0;
+  g->ionic_ms = g->diffusion_ms = 0.0;
+  g->timed_steps = 0;
+  return CEP_OK;
+}
+
+int cep_tissue_group_timing(cep_tissue_group_t g, double *ionic_ms, double *diffusion_ms, long *steps) {
+  if (!g) return fail_msg(CEP_ERR_ARG, "null group");
+  int rc;
+  if ((rc = group_fold_timing(g))) return rc;
+  if (ionic_ms) *ionic_ms = g->ionic_ms;
+  if (diffusion_ms) *diffusion_ms = g->diffusion_ms;
+  if (steps) *steps = g->timed_steps;
   return CEP_OK;
 }
 
@@ -1279,12 +1338,17 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
   if (!g) return fail_msg(CEP_ERR_ARG, "null group");
   if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");
   for (long s = 0; s < n_steps; ++s) {
+    int rc;
+    if (g->timing) {
+      if (g->ev_used + 3 > kGroupEvents && (rc = group_fold_timing(g))) return rc;
+      if ((rc = group_event(g))) return rc;
+    }
     for (cep_tissue_t t : g->ts) {
-      int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
+      rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
       if (rc) return rc;
     }
+    if (g->timing && (rc = group_event(g))) return rc;
     const double t_new = g->ts[0]->t + g->ts[0]->dt;
-    int rc;
     if (g->format == CEP_FEM_CSR)
       rc = group_launch<CsrView>(g, t_new);
     else if (g->format == CEP_FEM_STENCIL)
@@ -1294,6 +1358,7 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
     else
       rc = group_launch<EllView>(g, t_new);
     if (rc) return rc;
+    if (g->timing && (rc = group_event(g))) return rc;
     for (cep_tissue_t t : g->ts) {
       t->t += t->dt;
       ++t->steps;
@@ -1431,8 +1496,8 @@ namespace {
 
 constexpr int64_t kNaRows = CEP_NOALLOC_MAX_ROWS;
 constexpr int kNaMaxGrid = 1024;
-// dinv, r, z, p0, p1, q | partials [3][kNaMaxGrid] | Ctl | Status
-constexpr int64_t kNaVecWords = 6 * kNaRows;
+// dinv, r, q | (p, z) x 2 | partials [3][kNaMaxGrid] | Ctl | Status
+constexpr int64_t kNaVecWords = 7 * kNaRows;
 constexpr int64_t kNaWords = kNaVecWords + 3 * kNaMaxGrid + 8 + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNaWords];
@@ -1461,7 +1526,8 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   if (!d_row_ptr || !d_col_idx || !d_a_val || !d_b_val || !d_v) return fail_msg(CEP_ERR_ARG, "null argument");
   if (n <= 0 || n > CEP_NOALLOC_MAX_ROWS)
     return fail_msg(CEP_ERR_ARG, "n = %d outside 1..%d (CEP_NOALLOC_MAX_ROWS)", n, CEP_NOALLOC_MAX_ROWS);
-  if (!(dt > 0) || !(rtol > 0) || max_iter <= 0) return fail_msg(CEP_ERR_ARG, "dt, rtol and max_iter must be positive");
+  if (!(dt > 0) || !(rtol > 0) || max_iter <= 0 || max_iter > CEP_FEM_MAX_ITER)
+    return fail_msg(CEP_ERR_ARG, "dt and rtol must be positive and max_iter in 1..%d", CEP_FEM_MAX_ITER);
   int dev = 0;
   FEM_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail_msg(CEP_ERR_ARG, "device %d out of range", dev);
@@ -1482,8 +1548,8 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   }
   cudaStream_t st = (cudaStream_t)stream;
   double *base = nd.base;
-  double *dinv = base, *r = base + kNaRows, *z = base + 2 * kNaRows, *p0 = base + 3 * kNaRows,
-         *p1 = base + 4 * kNaRows, *q = base + 5 * kNaRows, *part = base + kNaVecWords;
+  double *dinv = base, *r = base + kNaRows, *q = base + 2 * kNaRows, *part = base + kNaVecWords;
+  double2 *pz0 = reinterpret_cast<double2 *>(base + 3 * kNaRows), *pz1 = reinterpret_cast<double2 *>(base + 5 * kNaRows);
   Ctl *ctl = reinterpret_cast<Ctl *>(part + 3 * kNaMaxGrid);
   Status *stat = reinterpret_cast<Status *>(part + 3 * kNaMaxGrid + 8);
   // the same grid rule as an operator handle: one block per SM, no more
@@ -1498,13 +1564,14 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   FEM_CUDA(cudaGetLastError());
   PcgArgs a;
   a.n = n;
+  a.ld = n;
   a.dt = dt;
   a.rtol = rtol;
   a.max_iter = max_iter;
   a.precond_norm = 1;
   a.v = static_cast<double *>(d_v);
   a.dinv = dinv;
-  a.r = r; a.z = z; a.p0 = p0; a.p1 = p1; a.q = q;
+  a.r = r; a.q = q; a.pz0 = pz0; a.pz1 = pz1;
   a.part = part;
   a.ctl = ctl;
   a.st = stat;

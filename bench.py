@@ -54,6 +54,9 @@ BCL = 2000.0
 OPS = {
     "cipa2017": dict(add=520.97, mul=561.99, div=270.99, exp=123.0, log=3.0, pow=1.0),
     "ord2011": dict(add=474.97, mul=435.99, div=281.99, exp=100.0, log=3.0, pow=1.0),
+    "tt2006": dict(add=220.89, mul=161.24, div=136.71, exp=62.62, log=4.0, pow=0.0, sqrt=1.0),
+    "tt2004": dict(add=184.95, mul=140.90, div=122.73, exp=57.71, log=4.0, pow=1.0, sqrt=1.0),
+    "tomek2019": dict(add=547.02, mul=560.61, div=275.99, exp=112.81, log=3.0, pow=1.0, sqrt=2.0),
 }
 # DRAM bytes per launch per instance measured by ncu on the run kernel
 # (profiles/run_kernel_cipa2017_pop10k.md): the state and biomarker records
@@ -62,14 +65,15 @@ TRAFFIC_PER_INSTANCE = {"cipa2017": 705.0, "ord2011": None}
 
 
 def flops_per_step(model: str) -> float:
-    return sum(OPS[model].values())
+    o = OPS[model]
+    return o["add"] + o["mul"] + o["div"] + o["exp"] + o["log"] + o["pow"]
 
 
 def sfu_ops_per_step(model: str) -> float:
     """Operations that need the special-function unit in the mixed path
     (exp2/log2/reciprocal for every division and elementary function)."""
     o = OPS[model]
-    return o["div"] + o["exp"] + o["log"] + o["pow"]
+    return o["div"] + o["exp"] + o["log"] + o["pow"] + o.get("sqrt", 0.0)
 
 
 def parse():
@@ -84,6 +88,8 @@ def parse():
     ap.add_argument("--seg", type=int, default=None,
                     help="time steps per bench step (default 10000 for populations, 200 for tissue)")
     ap.add_argument("--nx", type=int, default=512, help="tissue sheet edge in nodes")
+    ap.add_argument("--format", default="auto", choices=["auto", "csr", "ell", "stencil", "classed"],
+                    help="sparse format of the tissue operators (auto: timed on the first operator)")
     ap.add_argument("--samples", type=int, default=2000)
     ap.add_argument("--concs", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
@@ -374,8 +380,60 @@ TISSUE_DT, TISSUE_H, TISSUE_D, TISSUE_RTOL = 0.01, 0.025, 0.0013, 1e-8
 # Algorithmic bytes per row per CG iteration (FP64 values, int32 columns):
 # A row (w x 12 B), p and z of the row (16), p_k and q written (16); then p,
 # x (read+write), q, r (read+write), dinv read and z written (72).
-def cg_bytes_per_row(width: int) -> int:
-    return 12 * width + 16 + 16 + 72
+def pcg_bytes_per_row(fmt: int, slots: int, iters: float) -> float:
+    """Algorithmic bytes one row moves in one solve of the batched
+    Jacobi-PCG kernel, each vector element and matrix entry counted once per
+    pass. Setup: B v (the format's B entries, v), the Jacobi inverse, and
+    r, z, p written (40 B + matrix). Each iteration: the direction/product
+    pass reads p, z and A's entries and writes p, q; the update pass reads
+    p, v, q, r and the Jacobi inverse and writes v, r, z (96 B + matrix).
+    Matrix bytes per row: CSR 12 per entry + 4 (row pointer), ELL 12 per
+    slot, stencil 8 per slot (implicit columns), classed 4 (the class index;
+    the per-class table stays in cache)."""
+    mat = {0: 12 * slots + 4, 1: 12 * slots, 2: 8 * slots, 3: 4}[fmt]
+    return (40 + mat) + iters * (96 + mat)
+
+
+def hbm_peak(peaks: dict):
+    """The driver-measured HBM copy bandwidth, else the pool's fallback."""
+    mp = peaks.get("measured_peaks_json") or {}
+    for k in ("hbm_gbs", "hbm_GBs", "hbm_gb_s"):
+        if k in mp:
+            return float(mp[k]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s"
+
+
+def phase_rooflines(model: str, prec: str, cells: int, steps: int, timing: dict, fmt: int, slots: int,
+                    iters: float, n_states: int, peaks: dict, hbm: float, hbm_src: str) -> dict:
+    """Live per-phase device time of a tissue group (CUDA events around each
+    step's ionic launches and its batched PCG launch) against each phase's
+    roofline. `cells` = nodes of all tissues in the group, `steps` = Godunov
+    steps timed. Ionic: every cell reads and writes its state vector once
+    per step (16 B per state + 1 B stimulus mask) and, in the mixed path,
+    issues the model's special-function operations; the binding bound is
+    the slower of the two. Diffusion: pcg_bytes_per_row per row per solve."""
+    ion_ms, dif_ms = timing["ionic_ms"] / steps, timing["diffusion_ms"] / steps
+    ion_bytes = cells * (16 * n_states + 1)
+    ion_hbm_ms = ion_bytes / (hbm * 1e9) * 1e3
+    sfu = peaks.get("sfu_tops")
+    ion_sfu_ms = (sfu_ops_per_step(model) * cells / (sfu * 1e12) * 1e3) if (sfu and prec == "mixed") else 0.0
+    if ion_sfu_ms > ion_hbm_ms:
+        ion = {"bound": "sfu", "achieved": sfu_ops_per_step(model) * cells / (ion_ms * 1e-3) / 1e12, "peak": sfu,
+               "unit": "TFLOP/s", "peak_source": "bench.py ex2.approx throughput probe on this GPU (1 op/MUFU)",
+               "ops_per_cell_step": sfu_ops_per_step(model)}
+    else:
+        ion = {"bound": "hbm", "achieved": ion_bytes / (ion_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+               "peak_source": hbm_src, "bytes_per_cell_step": 16 * n_states + 1}
+    ion.update(kernel="tissue_kernel (ionic step + stimulus, one launch per tissue)", ms_per_step=ion_ms,
+               frac=ion["achieved"] / ion["peak"], traffic=None,
+               other_bound_ms={"hbm": ion_hbm_ms, "sfu": ion_sfu_ms or None})
+    dif_bytes = cells * pcg_bytes_per_row(fmt, slots, iters)
+    dif = {"bound": "hbm", "kernel": "pcg_many_kernel (one cooperative launch per step for the group)",
+           "achieved": dif_bytes / (dif_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s", "peak_source": hbm_src,
+           "ms_per_step": dif_ms, "traffic": None, "bytes_per_row_per_solve": pcg_bytes_per_row(fmt, slots, iters),
+           "cg_iters_per_solve": iters}
+    dif["frac"] = dif["achieved"] / hbm
+    return {"ionic": ion, "diffusion": dif, "ionic_share": ion_ms / (ion_ms + dif_ms)}
 
 
 def tissue_inputs(seed: int, n_conc: int = 3):
@@ -387,6 +445,12 @@ def tissue_inputs(seed: int, n_conc: int = 3):
     hill[13] = rng.uniform(0.6, 1.8)
     cmax = 10 ** rng.uniform(-2, 1)
     return [0.0, cmax, 3 * cmax][:n_conc], hill
+
+
+def format_arg(cep, args):
+    """The --format choice as a format id (None: autotune)."""
+    return {"auto": None, "csr": cep.FEM_CSR, "ell": cep.FEM_ELL, "stencil": cep.FEM_STENCIL,
+            "classed": cep.FEM_CLASSED}[args.format]
 
 
 def make_sheet(cep, nx, prec, conc, hill, fmt=None):
@@ -413,9 +477,11 @@ def run_tissue(args, world, rank, local, pg):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     res = {}
     launches = 0
+    fmt = format_arg(cep, args)
     for prec in ("mixed", "fp64"):
-        sheets = [make_sheet(cep, nx, prec, concs[0], hill)]  # autotunes the sparse format
-        sheets += [make_sheet(cep, nx, prec, c, hill, sheets[0].fem.format) for c in concs[1:]]
+        sheets = [make_sheet(cep, nx, prec, concs[0], hill, fmt)]  # auto: timed on the first sheet
+        fmt = sheets[0].fem.format
+        sheets += [make_sheet(cep, nx, prec, c, hill, fmt) for c in concs[1:]]
         group = cep.TissueGroup(sheets)  # one batched diffusion solve per step for all sheets
         for _ in range(args.warmup):
             group.run(args.seg)
@@ -424,6 +490,7 @@ def run_tissue(args, world, rank, local, pg):
             t.sync()
         it0 = [t.stats()["cg_iters"] for t in sheets]
         torch.cuda.synchronize()
+        group.set_timing(True)
         barrier(pg)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
@@ -434,6 +501,7 @@ def run_tissue(args, world, rank, local, pg):
             stop.record()
             torch.cuda.synchronize()
         barrier(pg)
+        timing = group.timing()
         ms = max_over_ranks(start.elapsed_time(stop), pg)
         st = [t.stats() for t in sheets]
         cg = sum(s["cg_iters"] for s in st) - sum(it0)
@@ -441,26 +509,9 @@ def run_tissue(args, world, rank, local, pg):
         res[prec] = dict(value=node_steps / (ms / 1e3), ms_per_step=ms / args.steps, clocks=clk.summary(),
                          cg_iters_per_solve=cg / (len(sheets) * args.seg * args.steps),
                          not_converged=sum(s["not_converged"] for s in st), fmt=sheets[0].fem.format,
-                         ell_width=sheets[0].fem.ell_width)
-        launches += args.steps * (len(sheets) + 1) * args.seg
+                         ell_width=sheets[0].fem.ell_width, timing=timing)
         if prec == "mixed":
-            # PCG alone on the first sheet's current V (the dominant kernel)
-            f = sheets[0].fem
-            vptr, _ = sheets[0].cells.device_states()
-            lib = cep.lib()
-            k0 = f.stats()["total_iters"]
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record()
-            for _ in range(50):
-                rc = lib.cep_fem_solve_device(f._h, ctypes.c_void_p(vptr))
-                if rc:
-                    raise RuntimeError(lib.cep_last_error().decode())
-            e1.record()
-            torch.cuda.synchronize()
-            pcg_ms = e0.elapsed_time(e1) / 50
-            iters = (f.stats()["total_iters"] - k0) / 50
-            res["pcg"] = dict(ms=pcg_ms, iters=iters, bytes=cg_bytes_per_row(f.ell_width) * n * iters)
+            launches = args.steps * (len(sheets) + 1) * args.seg  # ionic per sheet + one batched PCG, per step
             if not args.no_e2e:
                 res["e2e"] = tissue_e2e(args, sheets, n, world, pg, cep)
         group.close()
@@ -520,15 +571,14 @@ def tissue_main(args, world, rank, local, pg):
     res, n, launches = run_tissue(args, world, rank, local, pg)
     if rank != 0:
         return
-    mixed, fp64, pcg = res["mixed"], res["fp64"], res["pcg"]
-    hbm = None
-    mp = peaks.get("measured_peaks_json") or {}
-    for k in ("hbm_gbs", "hbm_GBs", "hbm_gb_s"):
-        if k in mp:
-            hbm = float(mp[k])
-    src = "MEASURED_PEAKS.json hbm_gbs (measured)" if hbm else "fallback 6650 GB/s"
-    hbm = hbm or 6650.0
-    ach = pcg["bytes"] / (pcg["ms"] * 1e-3) / 1e9
+    mixed, fp64 = res["mixed"], res["fp64"]
+    hbm, src = hbm_peak(peaks)
+    ns = importlib.import_module("2ddrugsimulation_b200").N_STATES["tt2006"]
+    roofs = {prec: phase_rooflines("tt2006", prec, 3 * n, args.steps * args.seg, res[prec]["timing"],
+                                   res[prec]["fmt"], res[prec]["ell_width"], res[prec]["cg_iters_per_solve"], ns,
+                                   peaks, hbm, src) for prec in ("mixed", "fp64")}
+    rm = roofs["mixed"]
+    dominant = rm["ionic"] if rm["ionic_share"] >= 0.5 else rm["diffusion"]
     line = {
         "metric": "TT2006 monodomain node-steps/s (Godunov: ionic + Jacobi-PCG), mixed vs FP64",
         "value": mixed["value"], "unit": "node-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -541,14 +591,10 @@ def tissue_main(args, world, rank, local, pg):
                    "nodes_per_sheet": n, "sheets_per_gpu": 3, "sparse_format": ["csr", "ell", "stencil", "classed"][mixed["fmt"]],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"sheet sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
-                 "cg_iters_per_solve": fp64["cg_iters_per_solve"]},
+                 "cg_iters_per_solve": fp64["cg_iters_per_solve"], "phases": roofs["fp64"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "cg_iters_per_solve": mixed["cg_iters_per_solve"], "not_converged": mixed["not_converged"] + fp64["not_converged"],
-        "roofline": {"bound": "hbm", "kernel": "pcg_kernel (one cooperative launch per solve)", "achieved": ach,
-                     "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
-                     "bytes_per_row_per_iter": cg_bytes_per_row(mixed["ell_width"]), "pcg_ms": pcg["ms"],
-                     "pcg_iters": pcg["iters"], "peak_source": src,
-                     "note": "the 2D operator (~47 MB ELL) and vectors stay in the 126 MB L2 across iterations"},
+        "roofline": dominant, "phases": rm,
         "gpu_launches": launches, "clocks": mixed["clocks"],
         "cpu_baseline": None if args.no_cpu else tissue_cpu(args),
         "e2e": res.get("e2e"),
@@ -696,7 +742,7 @@ def slab_main(args, world, rank, local, pg):
     concs = [cmax, 3 * cmax]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     res = {}
-    fmt = None
+    fmt = format_arg(cep, args)
     for prec in ("mixed", "fp64"):
         slabs = []
         for c in concs:
@@ -714,6 +760,7 @@ def slab_main(args, world, rank, local, pg):
             flush.zero_()
         torch.cuda.synchronize()
         it0 = sum(t.stats()["cg_iters"] for t in slabs)
+        group.set_timing(True)
         barrier(pg)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
@@ -724,12 +771,14 @@ def slab_main(args, world, rank, local, pg):
             stop.record()
             torch.cuda.synchronize()
         barrier(pg)
+        timing = group.timing()
         ms = max_over_ranks(start.elapsed_time(stop), pg)
         st = [t.stats() for t in slabs]
         cg = sum(x["cg_iters"] for x in st) - it0
         res[prec] = dict(value=n * len(slabs) * args.seg * args.steps * world / (ms / 1e3), ms_per_step=ms / args.steps,
                          clocks=clk.summary(), cg_iters_per_solve=cg / (len(slabs) * args.seg * args.steps),
-                         not_converged=sum(x["not_converged"] for x in st), width=slabs[0].fem.ell_width)
+                         not_converged=sum(x["not_converged"] for x in st), width=slabs[0].fem.ell_width,
+                         timing=timing)
         group.close()
         for t in slabs:
             t.close()
@@ -738,6 +787,12 @@ def slab_main(args, world, rank, local, pg):
     if rank != 0:
         return
     mixed, fp64 = res["mixed"], res["fp64"]
+    peaks = measured_peaks()
+    hbm, src = hbm_peak(peaks)
+    roofs = {prec: phase_rooflines("ord2011", prec, 2 * n, args.steps * args.seg, res[prec]["timing"], fmt,
+                                   res[prec]["width"], res[prec]["cg_iters_per_solve"], cep.N_STATES["ord2011"],
+                                   peaks, hbm, src) for prec in ("mixed", "fp64")}
+    rm = roofs["mixed"]
     cpu = None
     if not args.no_cpu:
         from oracle import oracle as O
@@ -761,10 +816,11 @@ def slab_main(args, world, rank, local, pg):
                    "nodes_per_slab": n, "slabs_per_gpu": 2, "sparse_format": ["csr", "ell", "stencil", "classed"][fmt],
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"slab sharding x{world}"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "clocks": fp64["clocks"],
-                 "cg_iters_per_solve": fp64["cg_iters_per_solve"]},
+                 "cg_iters_per_solve": fp64["cg_iters_per_solve"], "phases": roofs["fp64"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"], "cg_iters_per_solve": mixed["cg_iters_per_solve"],
         "not_converged": mixed["not_converged"] + fp64["not_converged"],
-        "roofline": None, "gpu_launches": args.steps * args.seg * 3 * 2, "clocks": mixed["clocks"],
+        "roofline": rm["ionic"] if rm["ionic_share"] >= 0.5 else rm["diffusion"], "phases": rm,
+        "gpu_launches": args.steps * args.seg * 3, "clocks": mixed["clocks"],
         "cpu_baseline": cpu, "e2e": None,
     }
     print(json.dumps(line))

@@ -284,7 +284,9 @@ int cep_fem_get_csr(cep_fem_t f, int *row_ptr, int *col_idx, double *a_val, doub
 /* Stopping rule ||r|| <= rtol ||b|| after at most max_iter iterations, in the
  * preconditioned norm ||D^-1 r|| (precond_norm = 1, PETSc's default for CG)
  * or the plain 2-norm. Defaults: rtol 1e-5 (PETSc's default; the reference
- * sets none), max_iter 10000, preconditioned norm. */
+ * sets none), max_iter 10000, preconditioned norm. max_iter is at most
+ * CEP_FEM_MAX_ITER (the grid barrier counts arrivals in 31 bits). */
+#define CEP_FEM_MAX_ITER 1000000
 int cep_fem_set_solver(cep_fem_t f, double rtol, int max_iter, int precond_norm);
 /* y = A x (which = 0) or B x (which = 1); host vectors of n doubles. */
 int cep_fem_spmv(cep_fem_t f, int which, const double *x, double *y);
@@ -354,6 +356,14 @@ typedef struct cep_tissue_group *cep_tissue_group_t;
 int cep_tissue_group_create(const cep_tissue_t *tissues, int count, cep_tissue_group_t *out);
 int cep_tissue_group_run(cep_tissue_group_t g, long n_steps);
 int cep_tissue_group_destroy(cep_tissue_group_t g);
+/* Per-phase device time of the steps run while timing is on: CUDA events
+ * on the group's stream before the ionic launches, before the diffusion
+ * launch and after it, each step. set_timing resets the totals; timing()
+ * waits for the recorded steps and returns the totals since then. No
+ * counterpart in the reference (its timing is host wall clock around the
+ * whole run, heart.cpp). */
+int cep_tissue_group_set_timing(cep_tissue_group_t g, int on);
+int cep_tissue_group_timing(cep_tissue_group_t g, double *ionic_ms, double *diffusion_ms, long *steps);
 
 #ifdef __cplusplus
 }

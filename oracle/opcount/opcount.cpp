@@ -86,6 +86,15 @@ static inline od copysign(od a, od b) { return mk(std::copysign(a.v, b.v), a.k &
 namespace cipa_ns {
 #include "../src/cipa2017.c"
 }
+namespace tt06_ns {
+#include "../src/tt2006.c"
+}
+namespace tt04_ns {
+#include "../src/tt2004.c"
+}
+namespace tomek_ns {
+#include "../src/tomek2019.c"
+}
 #undef double
 
 int main(int argc, char **argv) {
@@ -98,15 +107,36 @@ int main(int argc, char **argv) {
   od hill[20];
   for (int k = 0; k < 20; ++k) hill[k] = od(0.0);
   const long n = (long)(beats * bcl / dt);
+  void (*step)(const cepo_cell *, od, od, od *, cepo_currents *) = nullptr;
   if (!strcmp(model, "ord2011")) {
     cepo_ord_init(&c, od(0.0), od(0.0), hill, 0, 1);
     cepo_ord_set_pacing(&c, od(bcl), od(-1.0), od(-1.0), od(1.0));
     cepo_ord_init_states(y);
-  } else {
+    step = cepo_ord_step;
+  } else if (!strcmp(model, "cipa2017")) {
     hill[14] = 10; hill[15] = 0.001; hill[16] = 0.9; hill[17] = 1000; hill[18] = -50; hill[19] = 3.5e-5;
     cipa_ns::cepo_cipa_init(&c, od(0.0), od(1.0), hill, 0, 1);
     cipa_ns::cepo_cipa_set_pacing(&c, od(bcl), od(-1.0), od(-1.0), od(1.0));
     cipa_ns::cepo_cipa_init_states(&c, y);
+    step = cipa_ns::cepo_cipa_step;
+  } else if (!strcmp(model, "tt2006")) {  // epicardial, as the tissue sheets
+    tt06_ns::cepo_tt06_init(&c, od(2.0), od(0.0), hill, 0, 1);
+    tt06_ns::cepo_tt06_set_pacing(&c, od(bcl), od(-1.0), od(-1.0), od(1.0));
+    tt06_ns::cepo_tt06_init_states(y);
+    step = tt06_ns::cepo_tt06_step;
+  } else if (!strcmp(model, "tt2004")) {
+    tt04_ns::cepo_tt04_init(&c, od(2.0), od(0.0), hill, 0, 1);
+    tt04_ns::cepo_tt04_set_pacing(&c, od(bcl), od(-1.0), od(-1.0), od(1.0));
+    tt04_ns::cepo_tt04_init_states(y);
+    step = tt04_ns::cepo_tt04_step;
+  } else if (!strcmp(model, "tomek2019")) {
+    tomek_ns::cepo_tomek_init(&c, od(0.0), od(0.0), hill, 0, 1);
+    tomek_ns::cepo_tomek_set_pacing(&c, od(bcl), od(-1.0), od(-1.0), od(1.0));
+    tomek_ns::cepo_tomek_init_states(&c, y);
+    step = tomek_ns::cepo_tomek_step;
+  } else {
+    std::fprintf(stderr, "unknown model %s\n", model);
+    return 2;
   }
   c.tissue_stim = 0;
   for (int k = 0; k < 64; ++k) y[k].k = false;  // states are variables
@@ -114,10 +144,7 @@ int main(int argc, char **argv) {
   t.k = false;
   for (long s = 0; s < n; ++s) {
     g_on = true;
-    if (!strcmp(model, "ord2011"))
-      cepo_ord_step(&c, t, od(dt), y, nullptr);
-    else
-      cipa_ns::cepo_cipa_step(&c, t, od(dt), y, nullptr);
+    step(&c, t, od(dt), y, nullptr);
     g_on = false;
     t = mk(t.v + dt, false);
   }

@@ -315,6 +315,28 @@ def test_tissue_group_classed_equals_stencil(cep, gpu):
 
 
 @pytest.mark.gpu
+def test_tissue_group_phase_timing(cep, gpu):
+    """Per-phase events change nothing in the results and cover every
+    step run while timing is on."""
+    hill = np.zeros(14)
+    plain = [_sheet(cep, 20, 17, 0.0, hill), _sheet(cep, 15, 15, 0.2, hill)]
+    timed = [_sheet(cep, 20, 17, 0.0, hill), _sheet(cep, 15, 15, 0.2, hill)]
+    cep.TissueGroup(plain).run(400)
+    g = cep.TissueGroup(timed)
+    g.run(100)
+    g.set_timing(True)
+    g.run(300)
+    tm = g.timing()
+    assert tm["steps"] == 300 and tm["ionic_ms"] > 0 and tm["diffusion_ms"] > 0
+    g.set_timing(False)
+    assert g.timing()["steps"] == 0
+    for a, b in zip(plain, timed):
+        a.sync()
+        b.sync()
+        assert np.array_equal(a.v(), b.v())
+
+
+@pytest.mark.gpu
 def test_ord_slab_3d_anisotropic_matches_oracle(cep, gpu, oracle):
     """3D ORd slab with endo/M/epi layers (per-node celltypes, quirks off),
     a fibre-rotated conductivity tensor per element and an endocardial S1:
