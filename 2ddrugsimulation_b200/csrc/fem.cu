@@ -9,11 +9,11 @@
 //   phase 0   b = B V* / dt (the RHS build fused with the first residual),
 //             r = b, z = D^-1 r, p_0 = 0, partial sums of r.z and |z|^2
 //   per CG iteration (two grid barriers):
-//     A   p_k = z + beta p_{k-1} evaluated on the fly inside the SpMV
-//         (p and z interleaved: one 16-byte gather per neighbour),
+//     A   p_k = z + beta p_{k-1} evaluated on the fly inside the SpMV,
 //         q = A p_k, partial p.q                             -> barrier
-//     B   x += alpha p, r -= alpha q, z = D^-1 r, partial r.z and |z|^2
-//                                                             -> barrier
+//     B   r -= alpha q, z = D^-1 r, partial r.z and |z|^2  -> barrier
+//   (x += alpha_k p_k is applied by pass A of iteration k+1, which reads
+//   p_k anyway, or by a last pass after the final iteration)
 // Dots are FP64 and deterministic: every block writes one partial per
 // reduction and every block sums all partials in the same fixed order, so
 // each block holds bit-identical scalars and takes the same branch. x is
@@ -26,9 +26,9 @@
 //          entries point at the row itself with weight 0)
 //   STENCIL a[slots][ld] f64, b[slots][ld] f64 (implicit columns)
 //   CLASSED class[ld] i32, a/b [classes][slots + 1] f64
-//   dinv[ld], r[ld], q[ld] f64; two (p, z) buffers [guard + ld + guard]
-//   f64x2 (guard = one plane + one line + one node for grid operators,
-//   zeros); partials [3][grid] f64
+//   dinv[ld], r[ld], q[ld] f64; p0, p1, z [guard + ld + guard] f64 (guard =
+//   one plane + one line + one node for grid operators, zeros); partials
+//   [3][grid] f64
 //
 // The grid barrier spins with an iteration limit; a barrier that runs out
 // sets an error word, every block leaves at its next barrier, and the host
@@ -96,11 +96,14 @@ struct Ctl {
   int pad;
 };
 
-// The CG direction vector is kept interleaved with the preconditioned
-// residual, pz[i] = (p_{k-1}, z_k), so one 16-byte gather gives a
-// neighbour's p_k = z_k + beta p_{k-1}. apply_pz(val, i, pz, beta) is row i
-// of val * p_k in the same summation order as apply().
-__device__ __forceinline__ double p_of(const double2 t, double beta) { return fma(beta, t.x, t.y); }
+// The CG direction p_k = z_{k-1} + beta p_{k-1} of a neighbour, formed on
+// the fly from the previous direction and preconditioned residual (each in
+// its own array, written whole by one pass: no partial-sector writes).
+struct Dir {
+  const double *p, *z;
+  double beta;
+  __device__ __forceinline__ double operator()(int64_t j) const { return fma(beta, p[j], z[j]); }
+};
 
 // Bulk L2 prefetch of [p, p + bytes) (16-byte aligned, multiple of 16).
 __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
@@ -117,10 +120,10 @@ struct CsrView {
     for (int k = rp[i]; k < e; ++k) s = fma(val[k], x(col[k]), s);
     return s;
   }
-  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
-    return apply(val, i, [&](int j) { return p_of(pz[j], beta); });
+  __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
+    return apply(val, i, [&](int j) { return d(j); });
   }
-  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const double2 *) const {}
+  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const Dir &) const {}
 };
 
 struct EllView {
@@ -135,10 +138,10 @@ struct EllView {
     for (int k = 0; k < width; ++k) s = fma(val[k * ld + i], x(col[k * ld + i]), s);
     return s;
   }
-  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
-    return apply(val, i, [&](int j) { return p_of(pz[j], beta); });
+  __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
+    return apply(val, i, [&](int j) { return d(j); });
   }
-  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const double2 *) const {}
+  __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const Dir &) const {}
 };
 
 // Structured-grid operator with implicit columns: slot (dk+1)*9 + (dj+1)*3 +
@@ -175,31 +178,33 @@ struct StencilView {
   // Unchecked gathers: a slot outside the grid has weight 0 and reads a
   // finite value (a wrapped neighbour, or a zero guard row before row 0 /
   // after row n-1), adding a zero as the checked form does.
-  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
-    const double2 *ci = pz + i;
+  __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
     const int plane = nx * ny;
     double s = 0.0;
 #pragma unroll
     for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
 #pragma unroll
       for (int dj = -1; dj <= 1; ++dj) {
-        const double2 *row = ci + (nx * dj + plane * dk);
+        const int64_t row = i + (nx * dj + plane * dk);
 #pragma unroll
         for (int di = -1; di <= 1; ++di) {
           const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
-          s = fma(val[slot * ld + i], p_of(row[di], beta), s);
+          s = fma(val[slot * ld + i], d(row + di), s);
         }
       }
     return s;
   }
   // Rows [b, b + count) come next: fetch into L2 what the sweep has not
   // touched yet, the leading plane (3D) or line (2D) of their
-  // neighbourhood, and their coefficient slots.
-  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const double2 *pz) const {
+  // neighbourhood (rounded out to 16-byte boundaries).
+  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const Dir &d) const {
     const int64_t lead = DIM == 3 ? (int64_t)nx * ny : nx;
-    int64_t lo = b + lead - nx - 1, hi = b + count + lead + nx + 1;
+    int64_t lo = (b + lead - nx - 2) & ~(int64_t)1, hi = (b + count + lead + nx + 2) & ~(int64_t)1;
     if (hi > ld_rows) hi = ld_rows;
-    if (lo < hi) prefetch_l2(pz + lo, (unsigned)((hi - lo) * sizeof(double2)));
+    if (lo < hi) {
+      prefetch_l2(d.p + lo, (unsigned)((hi - lo) * sizeof(double)));
+      prefetch_l2(d.z + lo, (unsigned)((hi - lo) * sizeof(double)));
+    }
   }
 };
 
@@ -238,10 +243,9 @@ struct ClassView {
         }
     return s;
   }
-  // Unchecked gathers as StencilView::apply_pz; coefficients two at a time.
-  __device__ __forceinline__ double apply_pz(const double *val, int64_t i, const double2 *pz, double beta) const {
+  // Unchecked gathers as StencilView::apply_dir; coefficients two at a time.
+  __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
     const double2 *c2 = reinterpret_cast<const double2 *>(val + (int64_t)__ldg(cls + i) * kStride);
-    const double2 *ci = pz + i;
     const int plane = nx * ny;
     double s = 0.0;
     double2 cp = make_double2(0.0, 0.0);
@@ -249,22 +253,25 @@ struct ClassView {
     for (int dk = (DIM == 3 ? -1 : 0); dk <= (DIM == 3 ? 1 : 0); ++dk)
 #pragma unroll
       for (int dj = -1; dj <= 1; ++dj) {
-        const double2 *row = ci + (nx * dj + plane * dk);
+        const int64_t row = i + (nx * dj + plane * dk);
 #pragma unroll
         for (int di = -1; di <= 1; ++di) {
           const int slot = (DIM == 3 ? (dk + 1) * 9 : 0) + (dj + 1) * 3 + (di + 1);
           if ((slot & 1) == 0) cp = __ldg(c2 + (slot >> 1));
-          s = fma((slot & 1) ? cp.y : cp.x, p_of(row[di], beta), s);
+          s = fma((slot & 1) ? cp.y : cp.x, d(row + di), s);
         }
       }
     return s;
   }
-  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const double2 *pz) const {
+  __device__ __forceinline__ void prefetch(int64_t b, int64_t count, int64_t ld_rows, const Dir &d) const {
     const int64_t lead = DIM == 3 ? (int64_t)nx * ny : nx;
-    int64_t lo = b + lead - nx - 1, hi = b + count + lead + nx + 1;
+    int64_t lo = (b + lead - nx - 2) & ~(int64_t)1, hi = (b + count + lead + nx + 2) & ~(int64_t)1;
     if (hi > ld_rows) hi = ld_rows;
-    if (lo < hi) prefetch_l2(pz + lo, (unsigned)((hi - lo) * sizeof(double2)));
-    int64_t ce = b + count < ld_rows ? b + count : ld_rows;
+    if (lo < hi) {
+      prefetch_l2(d.p + lo, (unsigned)((hi - lo) * sizeof(double)));
+      prefetch_l2(d.z + lo, (unsigned)((hi - lo) * sizeof(double)));
+    }
+    const int64_t ce = b + count < ld_rows ? b + count : ld_rows;
     if (b < ce) prefetch_l2(cls + b, (unsigned)((ce - b) * sizeof(int)));
   }
 };
@@ -277,7 +284,7 @@ struct PcgArgs {
   const double *dinv;
   int64_t ld;          // rows allocated in each vector (n rounded up to 32)
   double *r, *q;
-  double2 *pz0, *pz1;  // (p, z) interleaved; grid formats read guard rows around [0, n)
+  double *p0, *p1, *z;  // grid formats read guard rows around [0, n) of these
   double *part;  // [3][blocks]
   Ctl *ctl;
   Status *st;
@@ -379,6 +386,15 @@ struct PcgOp {
   int block0, nblocks;
 };
 
+// The operators of a batched launch travel as a kernel parameter, so each
+// block reads its operator's fields from the constant bank on use instead
+// of holding a copy in registers.
+constexpr int kMaxGroup = 64;
+template <class M>
+struct PcgOps {
+  PcgOp<M> op[kMaxGroup];
+};
+
 __device__ __forceinline__ void range_total2(const double *pa, const double *pb, int nb, double &a, double &b) {
   __shared__ double s[2];
   if (threadIdx.x < 32) {
@@ -421,13 +437,13 @@ __device__ __forceinline__ void range_total2(const double *pa, const double *pb,
 // (n_ops > 1) an operator that has converged keeps taking the grid barriers
 // until every operator has, counted in ops_done.
 //
-// Vectors: r, q and the caller's V (x), and two (p, z) buffers used in
-// turn. Iteration k: pass A reads (p_{k-1}, z_{k-1}) around each row, forms
-// p_k, writes it to the other buffer's p half and q = A p_k; pass B updates
-// x and r and writes z_k into that buffer's z half.
+// Vectors: r, q, z, the caller's V (x), and two direction buffers used in
+// turn. Iteration k: pass A reads p_{k-1} and z_{k-1} around each row,
+// forms p_k into the other buffer, writes q = A p_k and applies the
+// previous iteration's x update; pass B updates r and writes z_k.
 template <class M>
 __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, int lb, Ctl *ctl, int *ops_done,
-                                         int n_ops) {
+                                         int n_ops, double t_new) {
   const bool lead = lb == 0 && threadIdx.x == 0;
   const int64_t stride = (int64_t)NB * kPcgBlock;
   const int64_t i0 = (int64_t)lb * kPcgBlock + threadIdx.x;
@@ -443,12 +459,14 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
     const double b2 = m.apply(m.b, i2, [&](int j) { return v_in[j]; }) / a.dt;
     const double z1 = a.dinv[i] * b1, z2 = a.dinv[i2] * b2;
     a.r[i] = b1;
-    a.pz0[i] = make_double2(0.0, z1);
+    a.z[i] = z1;
+    a.p0[i] = 0.0;
     s0 = fma(b1, z1, s0);
     s1 = a.precond_norm ? fma(z1, z1, s1) : fma(b1, b1, s1);
     if (two) {
       a.r[i2] = b2;
-      a.pz0[i2] = make_double2(0.0, z2);
+      a.z[i2] = z2;
+      a.p0[i2] = 0.0;
       s0 = fma(b2, z2, s0);
       s1 = a.precond_norm ? fma(z2, z2, s1) : fma(b2, b2, s1);
     }
@@ -469,31 +487,37 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
     for (int64_t i = i0; i < a.n; i += stride) a.v[i] = 0.0;
     conv = done = true;
   }
-  double2 *pc = a.pz0, *pn = a.pz1;
+  double *pc = a.p0, *pn = a.p1;
   double beta = 0.0;  // p_1 = z_0 + 0 * p_0
+  double alpha_prev = 0.0;
   for (int it = 1; !(n_ops == 1 && done); ++it) {
     // A: p_k and q = A p_k (operators still iterating); report completions
     if (!done) {
       double spq = 0.0, unused = 0.0;
       for (int64_t i = i0; i < a.n; i += 2 * stride) {
         // the block's rows two trips ahead, fetched into L2 by one thread
+        const Dir d{pc, a.z, beta};
         if (threadIdx.x == 0) {
           const int64_t nb = i + 2 * stride;
-          m.prefetch(nb, kPcgBlock, a.ld, pc);
-          m.prefetch(nb + stride, kPcgBlock, a.ld, pc);
+          m.prefetch(nb, kPcgBlock, a.ld, d);
+          m.prefetch(nb + stride, kPcgBlock, a.ld, d);
         }
         const bool two = i + stride < a.n;
         const int64_t i2 = two ? i + stride : i;
-        const double q1 = m.apply_pz(m.a, i, pc, beta);
-        const double q2 = m.apply_pz(m.a, i2, pc, beta);
-        const double p1 = p_of(pc[i], beta), p2 = p_of(pc[i2], beta);
-        reinterpret_cast<double *>(pn + i)[0] = p1;
+        const double q1 = m.apply_dir(m.a, i, d);
+        const double q2 = m.apply_dir(m.a, i2, d);
+        const double c1 = pc[i], c2 = pc[i2];
+        const double p1 = fma(beta, c1, a.z[i]), p2 = fma(beta, c2, a.z[i2]);
+        pn[i] = p1;
         a.q[i] = q1;
         spq = fma(p1, q1, spq);
+        // x_{k-1} += alpha_{k-1} p_{k-1}, deferred from the last iteration
+        if (it > 1) a.v[i] = it == 2 ? alpha_prev * c1 : fma(alpha_prev, c1, a.v[i]);
         if (two) {
-          reinterpret_cast<double *>(pn + i2)[0] = p2;
+          pn[i2] = p2;
           a.q[i2] = q2;
           spq = fma(p2, q2, spq);
+          if (it > 1) a.v[i2] = it == 2 ? alpha_prev * c2 : fma(alpha_prev, c2, a.v[i2]);
         }
       }
       block_sum2(spq, unused);
@@ -513,29 +537,23 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
     double pq, dummy;
     range_total2(part2, nullptr, NB, pq, dummy);
     const double alpha = rz / pq;
-    double2 *t = pc;  // pn now holds p_k
+    double *t = pc;  // pn now holds p_k
     pc = pn;
     pn = t;
-    // B: x += alpha p, r -= alpha q, z = D^-1 r
+    // B: r -= alpha q, z = D^-1 r (x += alpha p rides on the next pass A)
     double srz = 0.0, snr = 0.0;
     for (int64_t i = i0; i < a.n; i += 2 * stride) {
       const bool two = i + stride < a.n;
       const int64_t i2 = two ? i + stride : i;
-      double *ha = reinterpret_cast<double *>(pc + i), *hb = reinterpret_cast<double *>(pc + i2);
-      const double pa = ha[0], pb = hb[0];
-      const double va = it == 1 ? alpha * pa : fma(alpha, pa, a.v[i]);
-      const double vb = it == 1 ? alpha * pb : fma(alpha, pb, a.v[i2]);
       const double ra = fma(-alpha, a.q[i], a.r[i]), rb = fma(-alpha, a.q[i2], a.r[i2]);
       const double za = a.dinv[i] * ra, zb = a.dinv[i2] * rb;
-      a.v[i] = va;
       a.r[i] = ra;
-      ha[1] = za;
+      a.z[i] = za;
       srz = fma(ra, za, srz);
       snr = a.precond_norm ? fma(za, za, snr) : fma(ra, ra, snr);
       if (two) {
-        a.v[i2] = vb;
         a.r[i2] = rb;
-        hb[1] = zb;
+        a.z[i2] = zb;
         srz = fma(rb, zb, srz);
         snr = a.precond_norm ? fma(zb, zb, snr) : fma(rb, rb, snr);
       }
@@ -556,12 +574,17 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
     } else if (it >= a.max_iter) {
       done = true;
     }
+    alpha_prev = alpha;
+    if (done)  // the last iteration's x update: no pass A follows
+      for (int64_t i = i0; i < a.n; i += stride) {
+        a.v[i] = it == 1 ? alpha * pc[i] : fma(alpha, pc[i], a.v[i]);
+      }
     beta = rz_new / rz;
     rz = rz_new;
   }
   if (a.tact)
     for (int64_t i = i0; i < a.n; i += stride)
-      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = a.t_new;
+      if (a.tact[i] < 0.0 && a.v[i] >= a.act_thr) a.tact[i] = t_new;
   if (lead) {
     a.st->last_iters = conv ? used : -a.max_iter;
     a.st->last_res = res;
@@ -573,20 +596,19 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
 
 // One operator over the whole cooperative grid.
 template <class M>
-__global__ void __launch_bounds__(kPcgBlock) pcg_kernel(M m, PcgArgs a) {
-  pcg_body(m, a, (int)gridDim.x, (int)blockIdx.x, a.ctl, nullptr, 1);
+__global__ void __launch_bounds__(kPcgBlock) pcg_kernel(const __grid_constant__ M m,
+                                                        const __grid_constant__ PcgArgs a) {
+  pcg_body(m, a, (int)gridDim.x, (int)blockIdx.x, a.ctl, nullptr, 1, a.t_new);
 }
 
 // Several operators, each on its own block range (see PcgOp).
 template <class M>
-__global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const PcgOp<M> *__restrict__ ops, int n_ops, Ctl *ctl,
-                                                             int *ops_done, double t_new) {
+__global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const __grid_constant__ PcgOps<M> ops, int n_ops,
+                                                             Ctl *ctl, int *ops_done, double t_new) {
   int o = 0;
-  while (o + 1 < n_ops && (int)blockIdx.x >= ops[o + 1].block0) ++o;
-  const M m = ops[o].m;
-  PcgArgs a = ops[o].a;
-  a.t_new = t_new;
-  pcg_body(m, a, ops[o].nblocks, (int)blockIdx.x - ops[o].block0, ctl, ops_done, n_ops);
+  while (o + 1 < n_ops && (int)blockIdx.x >= ops.op[o + 1].block0) ++o;
+  const PcgOp<M> &op = ops.op[o];
+  pcg_body(op.m, op.a, op.nblocks, (int)blockIdx.x - op.block0, ctl, ops_done, n_ops, t_new);
 }
 
 // y = A x or B x (tests)
@@ -662,8 +684,8 @@ struct cep_fem {
   int n_classes = 0;
   int dim = 0, gnx = 0, gny = 0, gnz = 0;
   double *r = nullptr, *q = nullptr, *part = nullptr;
-  double2 *pz0 = nullptr, *pz1 = nullptr;  // row 0 of [guard | ld | guard] zero-filled buffers
-  int64_t guard = 0;                       // rows a grid-format gather may reach past either end
+  double *p0 = nullptr, *p1 = nullptr, *z = nullptr;  // row 0 of [guard | ld | guard] zero-filled buffers
+  int64_t guard = 0;  // rows a grid-format gather may reach past either end
   Ctl *ctl = nullptr;
   Status *st = nullptr;
   int grid = 0;
@@ -777,12 +799,14 @@ int fem_finish_setup(cep_fem *f) {
   const size_t ld = (size_t)f->ld;
   if ((rc = fem_alloc(f, &f->r, ld)) || (rc = fem_alloc(f, &f->q, ld))) return rc;
   // grid formats gather up to one plane + one line + one node either side
+  // (rounded up to 32 rows, so an even row index is 16-byte aligned)
   f->guard = f->dim == 3 ? (int64_t)f->gnx * f->gny + f->gnx + 1 : f->dim == 2 ? (int64_t)f->gnx + 1 : 0;
+  f->guard = (f->guard + 31) / 32 * 32;
   const size_t span = ld + 2 * (size_t)f->guard;
-  for (double2 **pz : {&f->pz0, &f->pz1}) {
-    if ((rc = fem_alloc(f, pz, span))) return rc;
-    FEM_CUDA(cudaMemsetAsync(*pz, 0, sizeof(double2) * span, f->stream));
-    *pz += f->guard;
+  for (double **v : {&f->p0, &f->p1, &f->z}) {
+    if ((rc = fem_alloc(f, v, span))) return rc;
+    FEM_CUDA(cudaMemsetAsync(*v, 0, sizeof(double) * span, f->stream));
+    *v += f->guard;
   }
   int dev = 0, sms = 0, per_sm_csr = 0, per_sm_ell = 0;
   FEM_CUDA(cudaGetDevice(&dev));
@@ -822,7 +846,7 @@ int launch_pcg(cep_fem *f, const M &m, double *v, double *tact, double t_new, do
   a.precond_norm = f->precond_norm;
   a.v = v;
   a.dinv = f->dinv;
-  a.r = f->r; a.q = f->q; a.pz0 = f->pz0; a.pz1 = f->pz1;
+  a.r = f->r; a.q = f->q; a.p0 = f->p0; a.p1 = f->p1; a.z = f->z;
   a.part = f->part;
   a.ctl = f->ctl;
   a.st = f->st;
@@ -1155,7 +1179,7 @@ struct cep_tissue_group {
   std::vector<cep_tissue_t> ts;
   int format = 0, dim = 0, grid = 0;
   cudaStream_t stream = nullptr;
-  void *d_ops = nullptr;  // PcgOp<View>[count]
+  std::vector<unsigned char> ops;  // PcgOps<View>, passed by value at each launch
   Ctl *ctl = nullptr;
   int *ops_done = nullptr;
   // optional per-phase timing: three events per step (before the ionic
@@ -1209,7 +1233,7 @@ int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const
     o.a.precond_norm = f->precond_norm;
     o.a.v = cep_internal_batch_v(g->ts[k]->cells);
     o.a.dinv = f->dinv;
-    o.a.r = f->r; o.a.q = f->q; o.a.pz0 = f->pz0; o.a.pz1 = f->pz1;
+    o.a.r = f->r; o.a.q = f->q; o.a.p0 = f->p0; o.a.p1 = f->p1; o.a.z = f->z;
     o.a.part = f->part;
     o.a.ctl = nullptr;
     o.a.st = f->st;
@@ -1221,18 +1245,17 @@ int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const
     b0 += nb[k];
   }
   g->grid = b0;
-  FEM_CUDA(cudaMalloc(&g->d_ops, sizeof(PcgOp<M>) * h.size()));
-  FEM_CUDA(cudaMemcpy(g->d_ops, h.data(), sizeof(PcgOp<M>) * h.size(), cudaMemcpyHostToDevice));
+  g->ops.assign(sizeof(PcgOps<M>), 0);
+  std::memcpy(g->ops.data(), h.data(), sizeof(PcgOp<M>) * h.size());
   return CEP_OK;
 }
 
 template <class M>
 int group_launch(cep_tissue_group *g, double t_new) {
-  const PcgOp<M> *ops = static_cast<const PcgOp<M> *>(g->d_ops);
   int n = (int)g->ts.size();
   Ctl *ctl = g->ctl;
   int *done = g->ops_done;
-  void *args[] = {&ops, &n, &ctl, &done, &t_new};
+  void *args[] = {g->ops.data(), &n, &ctl, &done, &t_new};
   FEM_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(Ctl) + 64, g->stream));
   FEM_CUDA(cudaLaunchCooperativeKernel((const void *)pcg_many_kernel<M>, dim3(g->grid), dim3(kPcgBlock), args, 0,
                                        g->stream));
@@ -1249,7 +1272,8 @@ int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_
   int dev = 0, sms = 0;
   FEM_CUDA(cudaGetDevice(&dev));
   FEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (count > sms) return fail_msg(CEP_ERR_ARG, "at most %d tissues per group (one SM each at least)", sms);
+  if (count > sms || count > kMaxGroup)
+    return fail_msg(CEP_ERR_ARG, "at most %d tissues per group (one SM each at least)", std::min(sms, kMaxGroup));
   for (int k = 0; k < count; ++k) {
     if (!ts[k]) return fail_msg(CEP_ERR_ARG, "tissue %d is NULL", k);
     const cep_fem *f = ts[k]->fem, *f0 = ts[0]->fem;
@@ -1296,7 +1320,6 @@ int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_
     rc = group_build(g, nb, ell_view);
   if (rc) {
     cudaFree(g->ctl);
-    cudaFree(g->d_ops);
     delete g;
     return rc;
   }
@@ -1309,7 +1332,6 @@ int cep_tissue_group_destroy(cep_tissue_group_t g) {
   cudaStreamSynchronize(g->stream);
   for (cudaEvent_t e : g->ev) cudaEventDestroy(e);
   cudaFree(g->ctl);
-  cudaFree(g->d_ops);
   delete g;
   return CEP_OK;
 }
@@ -1496,8 +1518,8 @@ namespace {
 
 constexpr int64_t kNaRows = CEP_NOALLOC_MAX_ROWS;
 constexpr int kNaMaxGrid = 1024;
-// dinv, r, q | (p, z) x 2 | partials [3][kNaMaxGrid] | Ctl | Status
-constexpr int64_t kNaVecWords = 7 * kNaRows;
+// dinv, r, q, p0, p1, z | partials [3][kNaMaxGrid] | Ctl | Status
+constexpr int64_t kNaVecWords = 6 * kNaRows;
 constexpr int64_t kNaWords = kNaVecWords + 3 * kNaMaxGrid + 8 + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNaWords];
@@ -1549,7 +1571,7 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   cudaStream_t st = (cudaStream_t)stream;
   double *base = nd.base;
   double *dinv = base, *r = base + kNaRows, *q = base + 2 * kNaRows, *part = base + kNaVecWords;
-  double2 *pz0 = reinterpret_cast<double2 *>(base + 3 * kNaRows), *pz1 = reinterpret_cast<double2 *>(base + 5 * kNaRows);
+  double *p0 = base + 3 * kNaRows, *p1 = base + 4 * kNaRows, *z = base + 5 * kNaRows;
   Ctl *ctl = reinterpret_cast<Ctl *>(part + 3 * kNaMaxGrid);
   Status *stat = reinterpret_cast<Status *>(part + 3 * kNaMaxGrid + 8);
   // the same grid rule as an operator handle: one block per SM, no more
@@ -1571,7 +1593,7 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   a.precond_norm = 1;
   a.v = static_cast<double *>(d_v);
   a.dinv = dinv;
-  a.r = r; a.q = q; a.pz0 = pz0; a.pz1 = pz1;
+  a.r = r; a.q = q; a.p0 = p0; a.p1 = p1; a.z = z;
   a.part = part;
   a.ctl = ctl;
   a.st = stat;
