@@ -384,14 +384,15 @@ def pcg_bytes_per_row(fmt: int, slots: int, iters: float) -> float:
     """Algorithmic bytes one row moves in one solve of the batched
     Jacobi-PCG kernel, each vector element and matrix entry counted once per
     pass. Setup: B v (the format's B entries, v), the Jacobi inverse, and
-    r, z, p written (40 B + matrix). Each iteration: the direction/product
-    pass reads p, z and A's entries and writes p, q; the update pass reads
-    p, v, q, r and the Jacobi inverse and writes v, r, z (96 B + matrix).
-    Matrix bytes per row: CSR 12 per entry + 4 (row pointer), ELL 12 per
-    slot, stencil 8 per slot (implicit columns), classed 4 (the class index;
-    the per-class table stays in cache)."""
+    r, z, p_0 written (40 B + matrix). Each iteration: the product pass
+    reads p, z, x and A's entries and writes p, q, x (the previous
+    iteration's x update rides on it); the update pass reads q, r and the
+    Jacobi inverse and writes r, z (88 B + matrix). A last pass applies the
+    final x update (24 B). Matrix bytes per row: CSR 12 per entry + 4 (row
+    pointer), ELL 12 per slot, stencil 8 per slot (implicit columns),
+    classed 4 (the class index; the per-class table stays in cache)."""
     mat = {0: 12 * slots + 4, 1: 12 * slots, 2: 8 * slots, 3: 4}[fmt]
-    return (40 + mat) + iters * (96 + mat)
+    return (40 + mat) + iters * (88 + mat) + 24
 
 
 def hbm_peak(peaks: dict):
