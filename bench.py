@@ -395,6 +395,15 @@ def pcg_bytes_per_row(fmt: int, slots: int, iters: float) -> float:
     return (40 + mat) + iters * (88 + mat) + 24
 
 
+# DRAM bytes (read + write) per unit measured by ncu on one launch of the
+# tissue kernels (profiles/pcg_many_kernel_tissue_groups.md,
+# profiles/tissue_kernel_ionic_step.md): PCG per row and solve (the sheets
+# stay L2-resident; the slab figure is the 192x192x48 capture, which scales
+# with rows), ionic step per cell.
+PCG_TRAFFIC_PER_ROW_SOLVE = {"tt2006": 37.95e6 / 786432, "ord2011": 4.328e9 / 3538944}
+IONIC_TRAFFIC_PER_CELL = {"tt2006": 61.63e6 / 262144, "ord2011": 1.4896e9 / 1769472}
+
+
 def hbm_peak(peaks: dict):
     """The driver-measured HBM copy bandwidth, else the pool's fallback."""
     mp = peaks.get("measured_peaks_json") or {}
@@ -425,13 +434,17 @@ def phase_rooflines(model: str, prec: str, cells: int, steps: int, timing: dict,
     else:
         ion = {"bound": "hbm", "achieved": ion_bytes / (ion_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                "peak_source": hbm_src, "bytes_per_cell_step": 16 * n_states + 1}
-    ion.update(kernel="tissue_kernel (ionic step + stimulus, one launch per tissue)", ms_per_step=ion_ms,
-               frac=ion["achieved"] / ion["peak"], traffic=None,
+    tr = IONIC_TRAFFIC_PER_CELL.get(model) if prec == "mixed" else None
+    ion.update(kernel="tissue_kernel (ionic step + stimulus, one launch per tissue; figures cover a step's "
+                      "launches for all tissues of the group)", ms_per_step=ion_ms,
+               frac=ion["achieved"] / ion["peak"], traffic=tr * cells if tr else None,
                other_bound_ms={"hbm": ion_hbm_ms, "sfu": ion_sfu_ms or None})
     dif_bytes = cells * pcg_bytes_per_row(fmt, slots, iters)
     dif = {"bound": "hbm", "kernel": "pcg_many_kernel (one cooperative launch per step for the group)",
            "achieved": dif_bytes / (dif_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s", "peak_source": hbm_src,
-           "ms_per_step": dif_ms, "traffic": None, "bytes_per_row_per_solve": pcg_bytes_per_row(fmt, slots, iters),
+           "ms_per_step": dif_ms,
+           "traffic": PCG_TRAFFIC_PER_ROW_SOLVE[model] * cells if (fmt == 3 and model in PCG_TRAFFIC_PER_ROW_SOLVE) else None,
+           "bytes_per_row_per_solve": pcg_bytes_per_row(fmt, slots, iters),
            "cg_iters_per_solve": iters}
     dif["frac"] = dif["achieved"] / hbm
     return {"ionic": ion, "diffusion": dif, "ionic_share": ion_ms / (ion_ms + dif_ms)}
