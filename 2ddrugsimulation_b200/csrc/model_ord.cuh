@@ -554,6 +554,63 @@ __device__ __forceinline__ typename P::G naca(typename P::G na, typename P::G ca
 
 // role 3: Na/Ca exchange (both compartments), SERCA uptake; CiPA: the
 // dynamic hERG Markov chain with drug binding/trapping and IKr
+// One backward-Euler step of the CiPA Markov IKr chain with the rates
+// frozen at the step's V: (I - h Q) x = g, g = h Q S (the forward-Euler
+// increments, in place in g on entry, x on return), states in the order
+// IC1, IC2, C1, C2, O, IO, IObound, Obound, Cbound; k = {k11, k21, k51,
+// k61, k3, k4, k52, k62, k1, k2, k31, k41, k53, k63, bind, Ku, unb, trap,
+// Kt}. The sparse system is eliminated in a fixed order (Cb; the bound pair
+// as affine functions of O and IO; IC1; C1; C2; the dense 3x3 IC2, O, IO)
+// with no pivoting (I - h Q is an M-matrix); total occupancy is kept.
+template <class P>
+__device__ __forceinline__ void markov_be(typename P::G h, const typename P::G *k, typename P::G *g) {
+  using G = typename P::G;
+  const G one = (G)1;
+  const G k11 = k[0], k21 = k[1], k51 = k[2], k61 = k[3], k3 = k[4], k4 = k[5], k52 = k[6], k62 = k[7];
+  const G k1 = k[8], k2 = k[9], k31 = k[10], k41 = k[11], k53 = k[12], k63 = k[13], bind = k[14];
+  const G Ku = k[15], unb = k[16], trap = k[17], Kt = k[18];
+  const G dIC1 = one + h * (k11 + k61), dIC2 = one + h * ((k21 + k3) + k62), dC1 = one + h * (k51 + k1);
+  const G dC2 = one + h * ((k2 + k52) + k31), dO = one + h * ((k41 + k53) + bind);
+  const G dIO = one + h * ((k4 + k63) + bind), dIOb = one + h * (unb + Kt), dOb = one + h * (Ku + Kt);
+  const G rCb = P::rc(one + h * ((G)2 * trap));
+  const G ht = h * trap, hK = h * Kt, hb = h * bind;
+  const G c = ht * hK * rCb, e = ht * g[8] * rCb;
+  const G a11 = dOb - c, a22 = dIOb - c, rdet = P::rc(a11 * a22 - c * c);
+  const G rOb = g[7] + e, rIOb = g[6] + e;
+  const G ob0 = (a22 * rOb + c * rIOb) * rdet, obO = a22 * hb * rdet, obIO = c * hb * rdet;
+  const G iob0 = (c * rOb + a11 * rIOb) * rdet, iobO = c * hb * rdet, iobIO = a11 * hb * rdet;
+  const G aOO = dO - h * Ku * obO, aOIO = -(h * k63 + h * Ku * obIO), aOC2 = -h * k31;
+  const G rO = g[4] + h * Ku * ob0;
+  const G aIOIO = dIO - h * unb * iobIO, aIOO = -(h * k53 + h * unb * iobO), aIOIC2 = -h * k3;
+  const G rIO = g[5] + h * unb * iob0;
+  const G rIC1 = P::rc(dIC1);
+  const G i0 = g[0] * rIC1, iI2 = h * k21 * rIC1, iC1 = h * k51 * rIC1;
+  const G re11 = P::rc(dC1 - h * k61 * iC1);
+  const G c0 = (g[2] + h * k61 * i0) * re11, cI2 = h * k61 * iI2 * re11, cC2 = h * k2 * re11;
+  const G bII = dIC2 - h * k11 * (iI2 + iC1 * cI2), bIC = -(h * k52 + h * k11 * iC1 * cC2);
+  const G bIIO = -h * k4, rI = g[1] + h * k11 * (i0 + iC1 * c0);
+  const G rCC = P::rc(dC2 - h * k1 * cC2), bCI = -(h * k62 + h * k1 * cI2), bCO = -h * k41;
+  const G rC = g[3] + h * k1 * c0;
+  const G m11 = bII - bIC * bCI * rCC, m12 = -bIC * bCO * rCC, m13 = bIIO, s1 = rI - bIC * rC * rCC;
+  const G m21 = -aOC2 * bCI * rCC, m22 = aOO - aOC2 * bCO * rCC, m23 = aOIO, s2 = rO - aOC2 * rC * rCC;
+  const G m31 = aIOIC2, m32 = aIOO, m33 = aIOIO, s3 = rIO;
+  const G r11 = P::rc(m11);
+  const G l21 = m21 * r11, l31 = m31 * r11;
+  const G n22 = m22 - l21 * m12, n23 = m23 - l21 * m13, t2 = s2 - l21 * s1;
+  const G n32 = m32 - l31 * m12, n33 = m33 - l31 * m13, t3 = s3 - l31 * s1;
+  const G r22 = P::rc(n22);
+  const G l32 = n32 * r22;
+  const G xIO = P::dv(t3 - l32 * t2, n33 - l32 * n23);
+  const G xO = (t2 - n23 * xIO) * r22;
+  const G xIC2 = ((s1 - m12 * xO) - m13 * xIO) * r11;
+  const G xC2 = ((rC - bCI * xIC2) - bCO * xO) * rCC;
+  const G xC1 = (c0 + cI2 * xIC2) + cC2 * xC2;
+  const G xOb = (ob0 + obO * xO) + obIO * xIO, xIOb = (iob0 + iobO * xO) + iobIO * xIO;
+  g[8] = (g[8] + hK * (xIOb + xOb)) * rCb;
+  g[0] = (i0 + iI2 * xIC2) + iC1 * xC1;
+  g[1] = xIC2; g[2] = xC1; g[3] = xC2; g[4] = xO; g[5] = xIO; g[6] = xIOb; g[7] = xOb;
+}
+
 template <class P, bool kCipa>
 __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                        double dt, bool update, Part<typename P::G> &o) {
@@ -610,10 +667,11 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
     const G k63 = (G)cipa::A63 * P::ex((G)cipa::B63 * v) * (G)cipa::Q63;
     const G unb = P::dv(q.Ku * k53, k63);
     const G trap = P::dv(q.Kt, one + P::ex(-(v - q.Vhalf) * (G)(1.0 / 6.789)));
-    // The chain is linear in its states for this step's V: when its largest
-    // outflow rate makes one Euler step unstable (dt*lam >= 2: fast drug
-    // binding, or IC1 -> C1 above ~43 mV) it takes N = ceil(dt*lam/1.8)
-    // Euler substeps with the same rates; N = 1 is the plain update.
+    // The chain is linear in its states for this step's V: forward Euler
+    // (the reference scheme for non-gate states) unless its largest outflow
+    // rate makes that step unsafe (dt*lam > 1.8: fast drug binding, the
+    // IC2 -> IC1 rate below ~-95 mV, IC1 -> C1 above ~43 mV); then one
+    // backward-Euler step of the chain (markov_be), stable for any rate.
     G lam = k11 + k61;
     lam = fmax(lam, k21 + k3m + k62);
     lam = fmax(lam, k1 + k51);
@@ -623,25 +681,27 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
     lam = fmax(lam, unb + q.Kt);
     lam = fmax(lam, q.Ku + q.Kt);
     lam = fmax(lam, (G)2 * trap);
-    const G xs = (G)dt * lam * (G)(1.0 / 1.8);
-    const int nsub = xs <= (G)1 ? 1 : (xs < (G)256 ? (int)ceil(xs) : 256);
-    const double h = nsub == 1 ? dt : P::dv(dt, nsub);
-    for (int sub = 0; sub < nsub; ++sub) {
-      const G IC1 = (G)y.IC1, IC2 = (G)y.IC2, C1 = (G)y.C1, C2 = (G)y.C2, O = (G)y.O, IO = (G)y.IO;
-      const G IOb = (G)y.IObound, Ob = (G)y.Obound, Cb = (G)y.Cbound;
-      const G f11 = k11 * IC1 - k21 * IC2, f51 = k51 * C1 - k61 * IC1, f3 = k3m * IC2 - k4m * IO;
-      const G f52 = k52 * C2 - k62 * IC2, f1 = k1 * C1 - k2 * C2, f31 = k31 * C2 - k41 * O;
-      const G f53 = k53 * O - k63 * IO, fbo = q.bind * O - q.Ku * Ob, fbi = q.bind * IO - unb * IOb;
-      const G ftc = trap * Cb;
-      y.IC1 += (double)(-f11 + f51) * h;
-      y.IC2 += (double)((f11 - f3) + f52) * h;
-      y.C1 += (double)(-f1 - f51) * h;
-      y.C2 += (double)((f1 - f31) - f52) * h;
-      y.O += (double)((f31 - f53) - fbo) * h;
-      y.IO += (double)((f3 + f53) - fbi) * h;
-      y.IObound += (double)((fbi + ftc) - q.Kt * IOb) * h;
-      y.Obound += (double)((fbo + ftc) - q.Kt * Ob) * h;
-      y.Cbound += (double)(-(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb)) * h;
+    const G IC1 = (G)y.IC1, IC2 = (G)y.IC2, C1 = (G)y.C1, C2 = (G)y.C2, O = (G)y.O, IO = (G)y.IO;
+    const G IOb = (G)y.IObound, Ob = (G)y.Obound, Cb = (G)y.Cbound;
+    const G f11 = k11 * IC1 - k21 * IC2, f51 = k51 * C1 - k61 * IC1, f3 = k3m * IC2 - k4m * IO;
+    const G f52 = k52 * C2 - k62 * IC2, f1 = k1 * C1 - k2 * C2, f31 = k31 * C2 - k41 * O;
+    const G f53 = k53 * O - k63 * IO, fbo = q.bind * O - q.Ku * Ob, fbi = q.bind * IO - unb * IOb;
+    const G ftc = trap * Cb;
+    G d[9] = {-f11 + f51, (f11 - f3) + f52, -f1 - f51, (f1 - f31) - f52, (f31 - f53) - fbo, (f3 + f53) - fbi,
+              (fbi + ftc) - q.Kt * IOb, (fbo + ftc) - q.Kt * Ob, -(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb)};
+    if ((G)dt * lam > (G)1.8) {
+      const G hh = (G)dt;
+#pragma unroll
+      for (int s = 0; s < 9; ++s) d[s] *= hh;
+      const G kr[19] = {k11, k21, k51, k61, k3m, k4m, k52, k62, k1, k2, k31, k41, k53, k63, q.bind, q.Ku, unb, trap, q.Kt};
+      markov_be<P>(hh, kr, d);
+      y.IC1 += (double)d[0]; y.IC2 += (double)d[1]; y.C1 += (double)d[2]; y.C2 += (double)d[3];
+      y.O += (double)d[4]; y.IO += (double)d[5]; y.IObound += (double)d[6]; y.Obound += (double)d[7];
+      y.Cbound += (double)d[8];
+    } else {
+      y.IC1 += (double)d[0] * dt; y.IC2 += (double)d[1] * dt; y.C1 += (double)d[2] * dt;
+      y.C2 += (double)d[3] * dt; y.O += (double)d[4] * dt; y.IO += (double)d[5] * dt;
+      y.IObound += (double)d[6] * dt; y.Obound += (double)d[7] * dt; y.Cbound += (double)d[8] * dt;
     }
   }
 }

@@ -52,7 +52,7 @@ BCL = 2000.0
 # oracle/_build/opcount <model> 1 1000` (profiles/opcount_ionic_models.txt).
 # flop = one add/sub, mul, div or elementary-function evaluation.
 OPS = {
-    "cipa2017": dict(add=520.97, mul=561.99, div=270.99, exp=123.0, log=3.0, pow=1.0),
+    "cipa2017": dict(add=520.97, mul=561.99, div=269.99, exp=123.0, log=3.0, pow=1.0),
     "ord2011": dict(add=474.97, mul=435.99, div=281.99, exp=100.0, log=3.0, pow=1.0),
     "tt2006": dict(add=220.89, mul=161.24, div=136.71, exp=62.62, log=4.0, pow=0.0, sqrt=1.0),
     "tt2004": dict(add=184.95, mul=140.90, div=122.73, exp=57.71, log=4.0, pow=1.0, sqrt=1.0),
@@ -246,6 +246,11 @@ def measured_peaks():
     return out
 
 
+def beat_launches(args) -> int:
+    """Launches of --seg time steps that make one BCL (at least one)."""
+    return max(1, int(round(BCL / DT / args.seg)))
+
+
 def run_ours(args, world, rank, local, pg, model):
     import torch
     cep = importlib.import_module("2ddrugsimulation_b200")
@@ -259,6 +264,11 @@ def run_ours(args, world, rank, local, pg, model):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
     res = {}
     launches = 0
+    # One bench step is one whole beat (BCL / dt time steps as launches of
+    # --seg steps): a step's cost varies within a beat (stiff Markov-chain
+    # phases of drugged instances in diastole), so the timed window covers
+    # whole beats, after whole warm-up beats.
+    per_beat = beat_launches(args)
     for prec in ("mixed", "fp64"):
         b = cep.Batch(model, n, prec)
         if args.kernel != "auto":
@@ -267,7 +277,8 @@ def run_ours(args, world, rank, local, pg, model):
         b.set_pacing(BCL)
         b.set_protocol(DT, 1000, 750, dt_write=1.0)
         for _ in range(args.warmup):
-            b.run(args.seg)
+            for _ in range(per_beat):
+                b.run(args.seg)
             flush.zero_()
         torch.cuda.synchronize()
         barrier(pg)
@@ -279,7 +290,8 @@ def run_ours(args, world, rank, local, pg, model):
             start.record()
             for k in range(args.steps):
                 kst[k].record()
-                b.run(args.seg)
+                for _ in range(per_beat):
+                    b.run(args.seg)
                 ken[k].record()
                 flush.zero_()
             stop.record()
@@ -289,12 +301,12 @@ def run_ours(args, world, rank, local, pg, model):
         kms = [kst[k].elapsed_time(ken[k]) for k in range(args.steps)]
         ms_max = max_over_ranks(ms, pg)
         kernel_ms = max_over_ranks(statistics.mean(kms), pg)
-        cell_steps = n * args.seg * args.steps * world
+        cell_steps = n * args.seg * per_beat * args.steps * world
         st = b.status()
         res[prec] = dict(value=cell_steps / (ms_max / 1e3), ms_per_step=ms_max / args.steps, kernel_ms=kernel_ms,
                          clocks=clk.summary(), n_running=int((st == cep.INST_RUNNING).sum()),
                          n_nonfinite=int((st == cep.INST_NONFINITE).sum()))
-        launches += args.steps
+        launches += args.steps * per_beat
         if prec == "mixed" and not args.no_e2e:
             res["e2e"] = run_e2e(args, b, n, world, pg, cep, model)
         b.close()
@@ -314,10 +326,11 @@ def run_e2e(args, b, n, world, pg, cep, model):
     torch.cuda.synchronize()
     barrier(pg)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps_per_beat = args.seg * beat_launches(args)
     start.record()
     for _ in range(args.steps):
         rc = lib.cep_batch_set_states(b._h, pinned_in.ctypes.data_as(dp), cep.LAYOUT_SOA)
-        rc |= lib.cep_batch_run(b._h, args.seg)
+        rc |= lib.cep_batch_run(b._h, steps_per_beat)
         rc |= lib.cep_batch_get_states(b._h, pinned_out.ctypes.data_as(dp), cep.LAYOUT_SOA)
         rc |= lib.cep_batch_get_biomarkers(b._h, bm)
         if rc:
@@ -326,7 +339,7 @@ def run_e2e(args, b, n, world, pg, cep, model):
     stop.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(start.elapsed_time(stop), pg)
-    cell_steps = n * args.seg * args.steps * world
+    cell_steps = n * steps_per_beat * args.steps * world
     return {"value": cell_steps / (ms / 1e3), "unit": "cell-steps/s", "h2d_bytes_per_step": ns * n * 8,
             "d2h_bytes_per_step": ns * n * 8 + n * ctypes.sizeof(cep.Biomarkers), "ms_per_step": ms / args.steps}
 
@@ -368,18 +381,18 @@ def calibrate_cpu(model, conc, hill, threads, target_s):
 
 def config_of(args, model, n, world):
     name = {"cipa2017": "CiPA-ORd v1 2017 (dynamic hERG, drug trapping)", "ord2011": "ORd 2011"}[model]
+    per_beat = beat_launches(args)
     return {"workload": f"{name} population, {n} instances per GPU ({args.samples} IC50/Hill samples x "
                         f"{args.concs} concs), BCL 2000 ms, dt 0.005 ms, 1000-pace protocol with steepest-of-last-"
-                        f"250 biomarkers fused; {args.seg} time steps per bench step",
-            "instances_per_gpu": n, "time_steps_per_bench_step": args.seg, "kernel": args.kernel,
+                        f"250 biomarkers fused; one bench step = one whole beat ({args.seg * per_beat} time steps "
+                        f"as {per_beat} launches of {args.seg})",
+            "instances_per_gpu": n, "time_steps_per_bench_step": args.seg * per_beat,
+            "launches_per_bench_step": per_beat, "kernel": args.kernel,
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance sharding x{world}"}
 
 
 # ------------------------------------------------------------ tissue workload
 TISSUE_DT, TISSUE_H, TISSUE_D, TISSUE_RTOL = 0.01, 0.025, 0.0013, 1e-8
-# Algorithmic bytes per row per CG iteration (FP64 values, int32 columns):
-# A row (w x 12 B), p and z of the row (16), p_k and q written (16); then p,
-# x (read+write), q, r (read+write), dinv read and z written (72).
 def pcg_bytes_per_row(fmt: int, slots: int, iters: float) -> float:
     """Algorithmic bytes one row moves in one solve of the batched
     Jacobi-PCG kernel, each vector element and matrix entry counted once per
@@ -906,7 +919,7 @@ def main():
                "sample": f"{threads} instances x {steps} fixed steps, one per thread ({secs:.1f} s)"}
     mixed, fp64 = res["mixed"], res["fp64"]
     fl = flops_per_step(model)
-    cell_steps_launch = n * args.seg
+    cell_steps_launch = n * args.seg * beat_launches(args)  # per bench step (kernel_ms is per bench step)
 
     def roof(kernel_ms, peak_key, label, per_step=fl, source="bench.py FMA probe on this GPU (2 flop/FMA)"):
         ach = per_step * cell_steps_launch / (kernel_ms * 1e-3) / 1e12

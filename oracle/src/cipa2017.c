@@ -559,30 +559,59 @@ void cepo_cipa_rates(const cepo_cell *c, double t, const double *y, double *dydt
 
 #define RL(y, inf, tau) ((inf) - ((inf) - (y)) * exp(-dt / (tau)))
 
-/* forward-Euler substeps needed for stability of the Markov chain */
-static int markov_substeps(double lam_max, double dt) {
-  const double x = dt * lam_max / 1.8;
-  return x <= 1.0 ? 1 : (int)ceil(x);
-}
-
-/* Markov IKr derivatives at the step's rates (same terms as computeRates) */
-static void markov_rates(const cipa_p *q, const cipa_gates *g, const double *S, double *r) {
-  const double t11 = g->e11 * S[IC1] * Q10(q->q11), t21 = g->e21 * S[IC2] * Q10(q->q21);
-  const double t51 = g->e51 * S[C1] * Q10(q->q51), t61 = g->e61 * S[IC1] * Q10(q->q61);
-  const double t3 = g->e3 * S[IC2] * Q10(q->q3), t4 = g->e4 * S[IO] * Q10(q->q4);
-  const double t52 = g->e52 * S[C2] * Q10(q->q52), t62 = g->e62 * S[IC2] * Q10(q->q62);
-  const double t1 = g->e1 * S[C1] * Q10(q->q1), t2 = g->e2 * S[C2] * Q10(q->q2);
-  const double t31 = g->e31 * S[C2] * Q10(q->q31), t41 = g->e41 * S[O] * Q10(q->q41);
-  const double t53 = g->e53 * S[O] * Q10(q->q53), t63 = g->e63 * S[IO] * Q10(q->q63);
-  r[0] = (-(t11 - t21) + t51) - t61;
-  r[1] = (((t11 - t21) - (t3 - t4)) + t52) - t62;
-  r[2] = -(t1 - t2) - (t51 - t61);
-  r[3] = ((t1 - t2) - (t31 - t41)) - (t52 - t62);
-  r[4] = ((t31 - t41) - (t53 - t63)) - (g->bind * S[O] - q->Ku * S[Obound]);
-  r[5] = ((t3 - t4) + t53 - t63) - (g->bind * S[IO] - g->unb * S[IObound]);
-  r[6] = ((g->bind * S[IO] - g->unb * S[IObound]) + g->trap * S[Cbound]) - q->Kt * S[IObound];
-  r[7] = ((g->bind * S[O] - q->Ku * S[Obound]) + g->trap * S[Cbound]) - q->Kt * S[Obound];
-  r[8] = -(g->trap * S[Cbound] - q->Kt * S[Obound]) - (g->trap * S[Cbound] - q->Kt * S[IObound]);
+/* One backward-Euler step of the Markov IKr chain (the rates frozen at the
+ * step's V): (I - dt Q) x = g with g = dt Q S the forward-Euler increments,
+ * S += x. The chain's graph is sparse, so the 9x9 system is eliminated in a
+ * fixed order: Cb, the bound pair {Ob, IOb} (2x2, in terms of O and IO),
+ * IC1, C1, C2, then the dense 3x3 {IC2, O, IO}. I - dt Q is an M-matrix
+ * (columns of Q sum to zero), so no pivoting is needed, and the step keeps
+ * the chain's total occupancy exactly. k[] = {k11, k21, k51, k61, k3, k4,
+ * k52, k62, k1, k2, k31, k41, k53, k63, bind, Ku, unb, trap, Kt}. */
+static void markov_backward_euler(double h, const double *k, const double *g, double *x) {
+  const double k11 = k[0], k21 = k[1], k51 = k[2], k61 = k[3], k3 = k[4], k4 = k[5], k52 = k[6], k62 = k[7];
+  const double k1 = k[8], k2 = k[9], k31 = k[10], k41 = k[11], k53 = k[12], k63 = k[13], bind = k[14];
+  const double Ku = k[15], unb = k[16], trap = k[17], Kt = k[18];
+  /* g and x in state order IC1, IC2, C1, C2, O, IO, IObound, Obound, Cbound */
+  const double dIC1 = 1.0 + h * (k11 + k61), dIC2 = 1.0 + h * ((k21 + k3) + k62), dC1 = 1.0 + h * (k51 + k1);
+  const double dC2 = 1.0 + h * ((k2 + k52) + k31), dO = 1.0 + h * ((k41 + k53) + bind);
+  const double dIO = 1.0 + h * ((k4 + k63) + bind), dIOb = 1.0 + h * (unb + Kt), dOb = 1.0 + h * (Ku + Kt);
+  const double dCb = 1.0 + h * (2.0 * trap);
+  /* Cb, then the bound pair as affine functions of dO, dIO */
+  const double ht = h * trap, hK = h * Kt, hb = h * bind;
+  const double c = ht * hK / dCb, e = ht * g[8] / dCb;
+  const double a11 = dOb - c, a22 = dIOb - c, det = a11 * a22 - c * c;
+  const double rOb = g[7] + e, rIOb = g[6] + e;
+  const double ob0 = (a22 * rOb + c * rIOb) / det, obO = a22 * hb / det, obIO = c * hb / det;
+  const double iob0 = (c * rOb + a11 * rIOb) / det, iobO = c * hb / det, iobIO = a11 * hb / det;
+  const double aOO = dO - h * Ku * obO, aOIO = -(h * k63 + h * Ku * obIO), aOC2 = -h * k31;
+  const double rO = g[4] + h * Ku * ob0;
+  const double aIOIO = dIO - h * unb * iobIO, aIOO = -(h * k53 + h * unb * iobO), aIOIC2 = -h * k3;
+  const double rIO = g[5] + h * unb * iob0;
+  /* IC1 and C1 as affine functions of IC2, C2 */
+  const double i0 = g[0] / dIC1, iI2 = h * k21 / dIC1, iC1 = h * k51 / dIC1;
+  const double e11 = dC1 - h * k61 * iC1;
+  const double c0 = (g[2] + h * k61 * i0) / e11, cI2 = h * k61 * iI2 / e11, cC2 = h * k2 / e11;
+  const double bII = dIC2 - h * k11 * (iI2 + iC1 * cI2), bIC = -(h * k52 + h * k11 * iC1 * cC2);
+  const double bIIO = -h * k4, rI = g[1] + h * k11 * (i0 + iC1 * c0);
+  const double bCC = dC2 - h * k1 * cC2, bCI = -(h * k62 + h * k1 * cI2), bCO = -h * k41;
+  const double rC = g[3] + h * k1 * c0;
+  /* C2 out, then the 3x3 {IC2, O, IO} */
+  const double m11 = bII - bIC * bCI / bCC, m12 = -bIC * bCO / bCC, m13 = bIIO, s1 = rI - bIC * rC / bCC;
+  const double m21 = -aOC2 * bCI / bCC, m22 = aOO - aOC2 * bCO / bCC, m23 = aOIO, s2 = rO - aOC2 * rC / bCC;
+  const double m31 = aIOIC2, m32 = aIOO, m33 = aIOIO, s3 = rIO;
+  const double l21 = m21 / m11, l31 = m31 / m11;
+  const double n22 = m22 - l21 * m12, n23 = m23 - l21 * m13, t2 = s2 - l21 * s1;
+  const double n32 = m32 - l31 * m12, n33 = m33 - l31 * m13, t3 = s3 - l31 * s1;
+  const double l32 = n32 / n22;
+  const double xIO = (t3 - l32 * t2) / (n33 - l32 * n23);
+  const double xO = (t2 - n23 * xIO) / n22;
+  const double xIC2 = ((s1 - m12 * xO) - m13 * xIO) / m11;
+  const double xC2 = ((rC - bCI * xIC2) - bCO * xO) / bCC;
+  const double xC1 = (c0 + cI2 * xIC2) + cC2 * xC2;
+  const double xOb = (ob0 + obO * xO) + obIO * xIO, xIOb = (iob0 + iobO * xO) + iobIO * xIO;
+  x[0] = (i0 + iI2 * xIC2) + iC1 * xC1;
+  x[1] = xIC2; x[2] = xC1; x[3] = xC2; x[4] = xO; x[5] = xIO; x[6] = xIOb; x[7] = xOb;
+  x[8] = (g[8] + hK * (xIOb + xOb)) / dCb;
 }
 
 /* Fixed-step scheme: Rush-Larsen gates, forward Euler for the Markov IKr
@@ -623,13 +652,12 @@ void cepo_cipa_step(const cepo_cell *c, double t, double dt, double *S, cepo_cur
   S[Jrelnp] = RL(S[Jrelnp], g.Jrel_inf, g.tau_rel);
   S[Jrelp] = RL(S[Jrelp], g.Jrel_infp, g.tau_relp);
   /* Markov IKr states: forward Euler, as the reference scheme treats every
-   * non-gate state. The chain is linear in its states for the step's V, so
-   * when its largest outflow rate lam makes one Euler step unstable
-   * (dt*lam >= 2: fast drug binding, or the IC1 -> C1 rate above ~43 mV) the
-   * step is split into N = ceil(dt*lam/1.8) Euler substeps with the same
-   * rates. N = 1 is exactly the plain forward-Euler update. */
-  const int nsub = markov_substeps(g.lam_max, dt);
-  if (nsub <= 1) {
+   * non-gate state. The chain is linear in its states for the step's V; when
+   * its largest outflow rate lam makes the Euler step unsafe (dt*lam > 1.8:
+   * fast drug binding, the IC2 -> IC1 rate below ~-95 mV, IC1 -> C1 above
+   * ~43 mV) the step is one backward-Euler step of the chain instead
+   * (stable for any rate, total occupancy kept). */
+  if (dt * g.lam_max <= 1.8) {
     S[IC1] = S[IC1] + R_[IC1] * dt;
     S[IC2] = S[IC2] + R_[IC2] * dt;
     S[C1] = S[C1] + R_[C1] * dt;
@@ -640,13 +668,16 @@ void cepo_cipa_step(const cepo_cell *c, double t, double dt, double *S, cepo_cur
     S[Obound] = S[Obound] + R_[Obound] * dt;
     S[Cbound] = S[Cbound] + R_[Cbound] * dt;
   } else {
-    const double h = dt / nsub;
-    for (int k = 0; k < nsub; ++k) {
-      double r[9];
-      markov_rates(q, &g, S, r);
-      S[IC1] += r[0] * h; S[IC2] += r[1] * h; S[C1] += r[2] * h; S[C2] += r[3] * h; S[O] += r[4] * h;
-      S[IO] += r[5] * h; S[IObound] += r[6] * h; S[Obound] += r[7] * h; S[Cbound] += r[8] * h;
-    }
+    const double kk[19] = {g.e11 * Q10(q->q11), g.e21 * Q10(q->q21), g.e51 * Q10(q->q51), g.e61 * Q10(q->q61),
+                           g.e3 * Q10(q->q3),   g.e4 * Q10(q->q4),   g.e52 * Q10(q->q52), g.e62 * Q10(q->q62),
+                           g.e1 * Q10(q->q1),   g.e2 * Q10(q->q2),   g.e31 * Q10(q->q31), g.e41 * Q10(q->q41),
+                           g.e53 * Q10(q->q53), g.e63 * Q10(q->q63), g.bind, q->Ku, g.unb, g.trap, q->Kt};
+    const double gg[9] = {R_[IC1] * dt, R_[IC2] * dt, R_[C1] * dt, R_[C2] * dt, R_[O] * dt, R_[IO] * dt,
+                          R_[IObound] * dt, R_[Obound] * dt, R_[Cbound] * dt};
+    double x[9];
+    markov_backward_euler(dt, kk, gg, x);
+    S[IC1] += x[0]; S[IC2] += x[1]; S[C1] += x[2]; S[C2] += x[3]; S[O] += x[4];
+    S[IO] += x[5]; S[IObound] += x[6]; S[Obound] += x[7]; S[Cbound] += x[8];
   }
   S[CaMKt] = S[CaMKt] + R_[CaMKt] * dt;
   S[V] = S[V] + R_[V] * dt;
