@@ -47,6 +47,13 @@ class CepJob(ctypes.Structure):
                 ("first_pace", ctypes.c_int), ("flags", ctypes.c_uint)]
 
 
+class TissueJob(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("h", ctypes.c_double), ("D", ctypes.c_double),
+                ("dt", ctypes.c_double), ("duration", ctypes.c_double), ("conc", ctypes.c_double),
+                ("hill", ctypes.POINTER(ctypes.c_double)), ("bcl", ctypes.c_double), ("stim_nx", ctypes.c_int),
+                ("stim_ny", ctypes.c_int), ("rtol", ctypes.c_double)]
+
+
 class JobTimes(ctypes.Structure):
     _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
                 ("cell_steps", ctypes.c_double)]
@@ -114,6 +121,10 @@ _SIGS = {
                                        ctypes.c_double, ctypes.c_long, ctypes.c_double, ctypes.c_void_p,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "cep_serve_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CepJob), ctypes.POINTER(ctypes.c_uint64)]),
+    "cep_serve_submit_tissue": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TissueJob),
+                                               ctypes.POINTER(ctypes.c_uint64)]),
+    "cep_serve_tissue_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(JobTimes)]),
     "cep_serve_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _ip]),
     "cep_serve_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double]),
     "cep_serve_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Biomarkers),
@@ -540,6 +551,26 @@ class Server:
         _check(lib().cep_serve_submit(self._h, ctypes.byref(job), ctypes.byref(jid)))
         self._n[jid.value] = n
         return jid.value
+
+    def submit_tissue(self, nx: int, ny: int, duration: float, conc: float = 0.0, hill=None, h: float = 0.025,
+                      D: float = 0.0013, dt: float = 0.01, bcl: float = 1000.0, stim=(2, 2),
+                      rtol: float = 1e-8) -> int:
+        """A 2D TT2006 patch job (corner S1 block of stim = (nx, ny) nodes)."""
+        hh = None if hill is None else np.ascontiguousarray(np.asarray(hill, np.float64)[:14])
+        job = TissueJob(nx, ny, h, D, dt, duration, conc, _dptr(hh), bcl, stim[0], stim[1], rtol)
+        jid = ctypes.c_uint64()
+        _check(lib().cep_serve_submit_tissue(self._h, ctypes.byref(job), ctypes.byref(jid)))
+        self._n[jid.value] = nx * ny
+        return jid.value
+
+    def tissue_result(self, jid: int) -> tuple[np.ndarray, np.ndarray, dict]:
+        """Final V, activation times (-1: never) and timings of a patch job."""
+        n = self._n[jid]
+        v = np.empty(n)
+        ta = np.empty(n)
+        t = JobTimes()
+        _check(lib().cep_serve_tissue_result(self._h, jid, _dptr(v), _dptr(ta), ctypes.byref(t)))
+        return v, ta, {k: getattr(t, k) for k, _ in JobTimes._fields_}
 
     def poll(self, jid: int) -> int:
         st = ctypes.c_int()

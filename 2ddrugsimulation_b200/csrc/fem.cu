@@ -604,11 +604,11 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_kernel(const __grid_constant__ 
 // Several operators, each on its own block range (see PcgOp).
 template <class M>
 __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const __grid_constant__ PcgOps<M> ops, int n_ops,
-                                                             Ctl *ctl, int *ops_done, double t_new) {
+                                                             Ctl *ctl, int *ops_done) {
   int o = 0;
   while (o + 1 < n_ops && (int)blockIdx.x >= ops.op[o + 1].block0) ++o;
   const PcgOp<M> &op = ops.op[o];
-  pcg_body(op.m, op.a, op.nblocks, (int)blockIdx.x - op.block0, ctl, ops_done, n_ops, t_new);
+  pcg_body(op.m, op.a, op.nblocks, (int)blockIdx.x - op.block0, ctl, ops_done, n_ops, op.a.t_new);
 }
 
 // y = A x or B x (tests)
@@ -1250,12 +1250,16 @@ int group_build(cep_tissue_group *g, const std::vector<int> &nb, M (*view)(const
   return CEP_OK;
 }
 
+// Each operator's activation time stamp is its own tissue's time after the
+// step (tissues of a group may run at different times and dt).
 template <class M>
-int group_launch(cep_tissue_group *g, double t_new) {
+int group_launch(cep_tissue_group *g) {
   int n = (int)g->ts.size();
+  PcgOps<M> *ops = reinterpret_cast<PcgOps<M> *>(g->ops.data());
+  for (int k = 0; k < n; ++k) ops->op[k].a.t_new = g->ts[k]->t + g->ts[k]->dt;
   Ctl *ctl = g->ctl;
   int *done = g->ops_done;
-  void *args[] = {g->ops.data(), &n, &ctl, &done, &t_new};
+  void *args[] = {g->ops.data(), &n, &ctl, &done};
   FEM_CUDA(cudaMemsetAsync(g->ctl, 0, sizeof(Ctl) + 64, g->stream));
   FEM_CUDA(cudaLaunchCooperativeKernel((const void *)pcg_many_kernel<M>, dim3(g->grid), dim3(kPcgBlock), args, 0,
                                        g->stream));
@@ -1280,7 +1284,6 @@ int cep_tissue_group_create(const cep_tissue_t *ts, int count, cep_tissue_group_
     if (f->stream != f0->stream) return fail_msg(CEP_ERR_ARG, "tissues of a group share one stream");
     if (f->format != f0->format || f->dim != f0->dim)
       return fail_msg(CEP_ERR_ARG, "tissues of a group share one sparse format (and grid dimension)");
-    if (ts[k]->dt != ts[0]->dt || ts[k]->t != ts[0]->t) return fail_msg(CEP_ERR_ARG, "tissues of a group share dt and time");
     for (int j = 0; j < k; ++j)
       if (ts[j] == ts[k]) return fail_msg(CEP_ERR_ARG, "tissue %d appears twice", k);
   }
@@ -1370,15 +1373,14 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
       if (rc) return rc;
     }
     if (g->timing && (rc = group_event(g))) return rc;
-    const double t_new = g->ts[0]->t + g->ts[0]->dt;
     if (g->format == CEP_FEM_CSR)
-      rc = group_launch<CsrView>(g, t_new);
+      rc = group_launch<CsrView>(g);
     else if (g->format == CEP_FEM_STENCIL)
-      rc = g->dim == 3 ? group_launch<StencilView<3>>(g, t_new) : group_launch<StencilView<2>>(g, t_new);
+      rc = g->dim == 3 ? group_launch<StencilView<3>>(g) : group_launch<StencilView<2>>(g);
     else if (g->format == CEP_FEM_CLASSED)
-      rc = g->dim == 3 ? group_launch<ClassView<3>>(g, t_new) : group_launch<ClassView<2>>(g, t_new);
+      rc = g->dim == 3 ? group_launch<ClassView<3>>(g) : group_launch<ClassView<2>>(g);
     else
-      rc = group_launch<EllView>(g, t_new);
+      rc = group_launch<EllView>(g);
     if (rc) return rc;
     if (g->timing && (rc = group_event(g))) return rc;
     for (cep_tissue_t t : g->ts) {

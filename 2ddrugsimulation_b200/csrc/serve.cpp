@@ -16,16 +16,26 @@
 //      has its biomarkers collected and its range released.
 // Each instance's arithmetic does not depend on its neighbours, so a job's
 // results are bit-identical alone or in any mix.
+//
+// Tissue-patch jobs (2D TT2006 sheets) get their own cells, operator and
+// tissue on a second stream, admitted against the HBM budget left after the
+// pool; each round the running patches advance together as one tissue group
+// (one batched PCG launch per step) while the pool's launch runs, so the two
+// kinds of work overlap on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -38,6 +48,7 @@ using Clock = std::chrono::steady_clock;
 
 struct Job {
   uint64_t id = 0;
+  bool tissue = false;
   int n = 0;
   std::vector<double> celltype, conc, hill;
   int hill_stride = 0;
@@ -47,10 +58,33 @@ struct Job {
   int first = -1;  // slot range while admitted
   int state = CEP_JOB_QUEUED;
   int error = CEP_OK;
+  std::string msg;  // the scheduler thread's error message when failed
   std::vector<cep_biomarkers_t> result;
   Clock::time_point t_submit, t_admit, t_done;
   long long steps = 0;  // instance-steps of the whole job
+  // tissue patch
+  cep_tissue_job_t tj{};
+  std::vector<double> thill;
+  cep_batch_t cells = nullptr;
+  cep_fem_t fem = nullptr;
+  cep_tissue_t tis = nullptr;
+  long t_total = 0, t_done_steps = 0;
+  size_t bytes = 0;
+  std::vector<double> v, tact;
 };
+
+// device bytes a tissue patch of n nodes may take (cells, operator in all
+// formats, work vectors), a generous bound for admission
+size_t tissue_bytes(int n) { return (size_t)n * 2048 + ((size_t)4 << 20); }
+
+int fail_fmt(int code, const char *fmt, ...) {
+  char buf[256];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return cep_internal_set_fail(code, buf);
+}
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -77,6 +111,15 @@ struct cep_server {
   long long launches = 0, steps_done = 0, completed = 0;
   Clock::time_point t_start;
   double busy_ms = 0.0;
+  // tissue patches
+  cudaStream_t tstream = nullptr;
+  std::deque<std::shared_ptr<Job>> tqueue;
+  std::vector<std::shared_ptr<Job>> trunning;
+  cep_tissue_group_t group = nullptr;
+  bool group_dirty = false;
+  size_t tissue_budget = 0, tissue_used = 0;
+  long tissue_steps_per_round = 200;
+  int max_tissues = 64;
 };
 
 namespace {
@@ -100,8 +143,46 @@ int admit(cep_server *s, Job &j) {
   return cep_batch_start_range(s->pool, j.first, j.n, j.n_pace, j.first_pace);
 }
 
+void tissue_free(Job &j) {
+  if (j.tis) cep_tissue_destroy(j.tis);
+  if (j.fem) cep_fem_destroy(j.fem);
+  if (j.cells) cep_batch_destroy(j.cells);
+  j.tis = nullptr;
+  j.fem = nullptr;
+  j.cells = nullptr;
+}
+
+int tissue_admit(cep_server *s, Job &j) {
+  const cep_tissue_job_t &q = j.tj;
+  const int n = q.nx * q.ny;
+  int rc;
+  if ((rc = cep_batch_create(CEP_MODEL_TT2006, n, s->precision, s->tstream, &j.cells))) return rc;
+  std::vector<double> conc((size_t)n, q.conc), hill;
+  if (!j.thill.empty()) {
+    hill.resize((size_t)n * 14);
+    for (int i = 0; i < n; ++i) std::copy(j.thill.begin(), j.thill.end(), hill.begin() + (size_t)i * 14);
+  }
+  if ((rc = cep_batch_init(j.cells, nullptr, conc.data(), hill.empty() ? nullptr : hill.data(), 14, CEP_FLAG_QUIRKS)))
+    return rc;
+  const std::vector<double> D((size_t)(q.nx - 1) * (q.ny - 1), q.D);  // one value per element
+  if ((rc = cep_fem_create_grid(2, q.nx, q.ny, 1, q.h, q.dt, D.data(), 1, CEP_FEM_CLASSED, s->tstream, &j.fem)))
+    return rc;
+  if ((rc = cep_fem_set_solver(j.fem, q.rtol > 0 ? q.rtol : 1e-8, 10000, 1))) return rc;
+  if ((rc = cep_tissue_create(j.cells, j.fem, q.dt, &j.tis))) return rc;
+  std::vector<unsigned char> mask((size_t)n, 0);
+  for (int y = 0; y < std::min(q.stim_ny, q.ny); ++y)
+    for (int x = 0; x < std::min(q.stim_nx, q.nx); ++x) mask[(size_t)y * q.nx + x] = 1;
+  const int n_pace = (int)std::ceil(q.duration / q.bcl);
+  return cep_tissue_set_stimulus(j.tis, mask.data(), q.bcl, 0.0, 1.0, std::max(1, n_pace));
+}
+
 void fail_all(cep_server *s, int rc) {
   s->fatal = rc;
+  const std::string msg = cep_last_error();
+  for (auto *list : {&s->running, &s->trunning})
+    for (auto &j : *list) j->msg = msg;
+  for (auto *list : {&s->queue, &s->tqueue})
+    for (auto &j : *list) j->msg = msg;
   for (auto &j : s->running) {
     j->state = CEP_JOB_FAILED;
     j->error = rc;
@@ -110,8 +191,19 @@ void fail_all(cep_server *s, int rc) {
     j->state = CEP_JOB_FAILED;
     j->error = rc;
   }
+  for (auto *list : {&s->trunning}) {
+    for (auto &j : *list) {
+      j->state = CEP_JOB_FAILED;
+      j->error = rc;
+    }
+  }
+  for (auto &j : s->tqueue) {
+    j->state = CEP_JOB_FAILED;
+    j->error = rc;
+  }
   s->running.clear();
   s->queue.clear();
+  s->tqueue.clear();
   s->stop = true;
   s->cv_done.notify_all();
 }
@@ -119,10 +211,12 @@ void fail_all(cep_server *s, int rc) {
 void worker_loop(cep_server *s) {
   std::vector<int32_t> status(s->capacity);
   for (;;) {
-    std::vector<std::shared_ptr<Job>> admitted;
+    std::vector<std::shared_ptr<Job>> admitted, tadmitted;
     {
       std::unique_lock<std::mutex> lock(s->mu);
-      s->cv_work.wait(lock, [&] { return s->stop || !s->queue.empty() || !s->running.empty(); });
+      s->cv_work.wait(lock, [&] {
+        return s->stop || !s->queue.empty() || !s->running.empty() || !s->tqueue.empty() || !s->trunning.empty();
+      });
       if (s->stop) return;
       for (auto it = s->queue.begin(); it != s->queue.end();) {
         const int first = find_range(s->owner, (*it)->n);
@@ -135,6 +229,16 @@ void worker_loop(cep_server *s) {
         admitted.push_back(*it);
         it = s->queue.erase(it);
       }
+      for (auto it = s->tqueue.begin(); it != s->tqueue.end();) {
+        if (s->tissue_used + (*it)->bytes > s->tissue_budget ||
+            (int)(s->trunning.size() + tadmitted.size()) >= s->max_tissues) {
+          ++it;
+          continue;
+        }
+        s->tissue_used += (*it)->bytes;
+        tadmitted.push_back(*it);
+        it = s->tqueue.erase(it);
+      }
     }
     for (auto &j : admitted) {
       const int rc = admit(s, *j);
@@ -143,6 +247,7 @@ void worker_loop(cep_server *s) {
       if (rc) {
         j->state = CEP_JOB_FAILED;
         j->error = rc;
+        j->msg = cep_last_error();
         for (int k = 0; k < j->n; ++k) s->owner[j->first + k] = -1;
         cep_batch_release_range(s->pool, j->first, j->n);
         s->cv_done.notify_all();
@@ -151,13 +256,51 @@ void worker_loop(cep_server *s) {
         s->running.push_back(j);
       }
     }
+    for (auto &j : tadmitted) {
+      const int rc = tissue_admit(s, *j);
+      std::lock_guard<std::mutex> lock(s->mu);
+      j->t_admit = Clock::now();
+      if (rc) {
+        j->msg = cep_last_error();
+        tissue_free(*j);
+        s->tissue_used -= j->bytes;
+        j->state = CEP_JOB_FAILED;
+        j->error = rc;
+        s->cv_done.notify_all();
+      } else {
+        j->state = CEP_JOB_RUNNING;
+        s->trunning.push_back(j);
+        s->group_dirty = true;
+      }
+    }
+    bool have_pop = false;
+    std::vector<std::shared_ptr<Job>> tl;
     {
       std::lock_guard<std::mutex> lock(s->mu);
-      if (s->running.empty()) continue;
+      have_pop = !s->running.empty();
+      tl = s->trunning;
     }
+    if (!have_pop && tl.empty()) continue;
     const auto t0 = Clock::now();
-    int rc = cep_batch_run(s->pool, s->steps_per_launch);
-    if (!rc) rc = cep_batch_get_status(s->pool, status.data());
+    int rc = CEP_OK;
+    long k_t = 0;
+    if (have_pop) rc = cep_batch_run(s->pool, s->steps_per_launch);
+    if (!rc && !tl.empty()) {
+      if (s->group_dirty) {
+        if (s->group) cep_tissue_group_destroy(s->group);
+        s->group = nullptr;
+        std::vector<cep_tissue_t> ts;
+        for (auto &j : tl) ts.push_back(j->tis);
+        rc = cep_tissue_group_create(ts.data(), (int)ts.size(), &s->group);
+        s->group_dirty = false;
+      }
+      k_t = s->tissue_steps_per_round;
+      for (auto &j : tl) k_t = std::min(k_t, j->t_total - j->t_done_steps);
+      if (!rc && k_t > 0) rc = cep_tissue_group_run(s->group, k_t);
+    }
+    if (!rc && have_pop) rc = cep_batch_get_status(s->pool, status.data());
+    if (!rc && !tl.empty() && cudaStreamSynchronize(s->tstream) != cudaSuccess)
+      rc = cep_internal_set_fail(CEP_ERR_CUDA, "tissue stream failed");
     const auto t1 = Clock::now();
     std::lock_guard<std::mutex> lock(s->mu);
     s->busy_ms += ms_between(t0, t1);
@@ -166,7 +309,7 @@ void worker_loop(cep_server *s) {
       fail_all(s, rc);
       return;
     }
-    for (auto it = s->running.begin(); it != s->running.end();) {
+    for (auto it = s->running.begin(); it != s->running.end() && have_pop;) {
       Job &j = **it;
       bool done = true;
       for (int k = 0; k < j.n && done; ++k) done = status[j.first + k] != CEP_INST_RUNNING;
@@ -192,6 +335,30 @@ void worker_loop(cep_server *s) {
       s->steps_done += j.steps;
       s->completed += 1;
       it = s->running.erase(it);
+      s->cv_done.notify_all();
+    }
+    for (auto it = s->trunning.begin(); it != s->trunning.end();) {
+      Job &j = **it;
+      j.t_done_steps += k_t;
+      if (j.t_done_steps < j.t_total) {
+        ++it;
+        continue;
+      }
+      const int n = j.tj.nx * j.tj.ny;
+      j.v.resize(n);
+      j.tact.resize(n);
+      int rc2 = cep_tissue_get_v(j.tis, j.v.data());
+      if (!rc2) rc2 = cep_tissue_get_activation(j.tis, j.tact.data());
+      if (rc2) j.msg = cep_last_error();
+      tissue_free(j);
+      s->tissue_used -= j.bytes;
+      j.t_done = Clock::now();
+      j.state = rc2 ? CEP_JOB_FAILED : CEP_JOB_DONE;
+      j.error = rc2;
+      s->steps_done += j.steps;
+      s->completed += 1;
+      s->group_dirty = true;
+      it = s->trunning.erase(it);
       s->cv_done.notify_all();
     }
   }
@@ -241,6 +408,17 @@ int cep_serve_start(int model, int precision, int capacity, double dt, double dt
     return rc;
   }
   s->owner.assign(capacity, -1);
+  const double pool_bytes = per_instance * (double)capacity;
+  const double budget = hbm_fraction * (double)free_b - pool_bytes;
+  s->tissue_budget = budget > 0 ? (size_t)budget : 0;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+    s->max_tissues = std::max(1, std::min(64, sms));
+  if (cudaStreamCreateWithFlags(&s->tstream, cudaStreamNonBlocking) != cudaSuccess) {
+    cep_batch_destroy(s->pool);
+    delete s;
+    return cep_internal_set_fail(CEP_ERR_CUDA, "stream for tissue jobs");
+  }
   s->t_start = Clock::now();
   s->worker = std::thread(worker_loop, s);
   *out = s;
@@ -279,6 +457,53 @@ int cep_serve_submit(cep_server_t s, const cep_job_t *job, uint64_t *id) {
   return CEP_OK;
 }
 
+int cep_serve_submit_tissue(cep_server_t s, const cep_tissue_job_t *job, uint64_t *id) {
+  if (!s || !job || !id) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
+  if (job->nx < 2 || job->ny < 2 || (long long)job->nx * job->ny > (1LL << 28))
+    return fail_fmt(CEP_ERR_ARG, "patch of %d x %d nodes", job->nx, job->ny);
+  if (!(job->h > 0) || !(job->D >= 0) || !(job->dt > 0) || !(job->duration > 0) || !(job->bcl > 0) || job->conc < 0)
+    return cep_internal_set_fail(CEP_ERR_ARG, "h, dt, duration and bcl must be positive, D and conc >= 0");
+  auto j = std::make_shared<Job>();
+  j->tissue = true;
+  j->tj = *job;
+  j->tj.hill = nullptr;
+  if (job->hill) j->thill.assign(job->hill, job->hill + 14);
+  j->n = job->nx * job->ny;
+  j->t_total = std::max(1L, (long)std::llround(job->duration / job->dt));
+  j->steps = (long long)j->n * j->t_total;
+  j->bytes = tissue_bytes(j->n);
+  j->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (s->stop) return cep_internal_set_fail(s->fatal ? s->fatal : CEP_ERR_STATE, "server stopped");
+  if (j->bytes > s->tissue_budget)
+    return fail_fmt(CEP_ERR_OOM, "patch needs %zu bytes, the tissue budget is %zu", j->bytes, s->tissue_budget);
+  j->id = s->next_id++;
+  s->jobs[j->id] = j;
+  s->tqueue.push_back(j);
+  *id = j->id;
+  s->cv_work.notify_one();
+  return CEP_OK;
+}
+
+int cep_serve_tissue_result(cep_server_t s, uint64_t id, double *v, double *t_act, cep_job_times_t *times) {
+  if (!s) return cep_internal_set_fail(CEP_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  Job &j = *it->second;
+  if (!j.tissue) return cep_internal_set_fail(CEP_ERR_ARG, "not a tissue job");
+  if (j.state != CEP_JOB_DONE) return cep_internal_set_fail(CEP_ERR_STATE, "job not done");
+  if (v) std::memcpy(v, j.v.data(), sizeof(double) * j.v.size());
+  if (t_act) std::memcpy(t_act, j.tact.data(), sizeof(double) * j.tact.size());
+  if (times) {
+    times->queue_ms = ms_between(j.t_submit, j.t_admit);
+    times->latency_ms = ms_between(j.t_submit, j.t_done);
+    times->run_ms = ms_between(j.t_admit, j.t_done);
+    times->cell_steps = (double)j.steps;
+  }
+  return CEP_OK;
+}
+
 int cep_serve_poll(cep_server_t s, uint64_t id, int *state) {
   if (!s || !state) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
   std::lock_guard<std::mutex> lock(s->mu);
@@ -301,7 +526,8 @@ int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s) {
   } else {
     s->cv_done.wait(lock, finished);
   }
-  if (j->state == CEP_JOB_FAILED) return cep_internal_set_fail(j->error ? j->error : CEP_ERR_STATE, "job failed");
+  if (j->state == CEP_JOB_FAILED)
+    return fail_fmt(j->error ? j->error : CEP_ERR_STATE, "job failed: %s", j->msg.empty() ? "stopped" : j->msg.c_str());
   return CEP_OK;
 }
 
@@ -312,6 +538,7 @@ int cep_serve_result(cep_server_t s, uint64_t id, cep_biomarkers_t *out, cep_job
   if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
   Job &j = *it->second;
   if (j.state != CEP_JOB_DONE) return cep_internal_set_fail(CEP_ERR_STATE, "job not done");
+  if (j.tissue) return cep_internal_set_fail(CEP_ERR_ARG, "a tissue job: use cep_serve_tissue_result");
   if (out) std::memcpy(out, j.result.data(), sizeof(cep_biomarkers_t) * j.n);
   if (times) {
     times->queue_ms = ms_between(j.t_submit, j.t_admit);
@@ -337,8 +564,8 @@ int cep_serve_stats(cep_server_t s, cep_serve_stats_t *st) {
   if (!s || !st) return cep_internal_set_fail(CEP_ERR_ARG, "null argument");
   std::lock_guard<std::mutex> lock(s->mu);
   st->capacity = s->capacity;
-  st->queued = (int)s->queue.size();
-  st->running = (int)s->running.size();
+  st->queued = (int)(s->queue.size() + s->tqueue.size());
+  st->running = (int)(s->running.size() + s->trunning.size());
   int used = 0;
   for (int o : s->owner) used += o >= 0;
   st->slots_used = used;
@@ -363,11 +590,24 @@ int cep_serve_stop(cep_server_t s) {
       j->state = CEP_JOB_FAILED;
       j->error = CEP_ERR_STATE;
     }
+    for (auto &j : s->tqueue) {
+      j->state = CEP_JOB_FAILED;
+      j->error = CEP_ERR_STATE;
+    }
+    for (auto &j : s->trunning) {
+      j->state = CEP_JOB_FAILED;
+      j->error = CEP_ERR_STATE;
+    }
     s->queue.clear();
+    s->tqueue.clear();
   }
   s->cv_work.notify_all();
   s->cv_done.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  if (s->group) cep_tissue_group_destroy(s->group);
+  for (auto &j : s->trunning) tissue_free(*j);
+  s->trunning.clear();
+  if (s->tstream) cudaStreamDestroy(s->tstream);
   cep_batch_destroy(s->pool);
   delete s;
   return CEP_OK;

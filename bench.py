@@ -634,18 +634,40 @@ SERVE_BCL, SERVE_DT = 1000.0, 0.005
 
 
 def serve_trace(n_jobs: int, seed: int):
-    """Seeded screening jobs: CiPA populations of log-U[20, 500] samples x
-    1-4 concentrations, 1-2 paces at BCL 1000 ms (biomarkers on the last
-    pace), each around its own nominal drug."""
+    """Seeded screening jobs: four in five are CiPA populations of
+    log-U[20, 500] samples x 1-4 concentrations, 1-2 paces at BCL 1000 ms
+    (biomarkers on the last pace), each around its own nominal drug; one in
+    five is a 2D TT2006 patch of log-U[64, 192]^2 nodes for U[50, 200] ms
+    (dt 0.01 ms, corner S1) with an IKr Hill block."""
     rng = np.random.default_rng(seed)
     jobs = []
     for k in range(n_jobs):
+        if rng.uniform() < 0.2:
+            nx = int(round(10 ** rng.uniform(np.log10(64), np.log10(192))))
+            hill = np.zeros(14)
+            hill[12], hill[13] = 10 ** rng.uniform(-1, 2), rng.uniform(0.6, 1.8)
+            jobs.append(dict(kind="tissue", nx=nx, duration=float(rng.uniform(50, 200)),
+                             conc=float(10 ** rng.uniform(-2, 1)), hill=hill))
+            continue
         ns = int(round(10 ** rng.uniform(np.log10(20), np.log10(500))))
         nc = int(rng.integers(1, 5))
         paces = int(rng.integers(1, 3))
         conc, hill = population("cipa2017", ns, nc, seed=seed * 1000 + k)
-        jobs.append(dict(conc=conc, hill=hill, n_pace=paces, first_pace=paces - 1))
+        jobs.append(dict(kind="pop", conc=conc, hill=hill, n_pace=paces, first_pace=paces - 1))
     return jobs
+
+
+def submit_job(srv, j):
+    if j["kind"] == "tissue":
+        return srv.submit_tissue(j["nx"], j["nx"], j["duration"], conc=j["conc"], hill=j["hill"],
+                                 stim=(max(2, j["nx"] // 32),) * 2)
+    return srv.submit(j["conc"], j["hill"], bcl=SERVE_BCL, n_pace=j["n_pace"], first_pace=j["first_pace"])
+
+
+def job_steps(j) -> int:
+    if j["kind"] == "tissue":
+        return j["nx"] * j["nx"] * int(round(j["duration"] / 0.01))
+    return len(j["conc"]) * int(j["n_pace"] * SERVE_BCL / SERVE_DT)
 
 
 def run_serving(cep, jobs, arrivals, mode: str, capacity: int, k_steps: int):
@@ -663,18 +685,17 @@ def run_serving(cep, jobs, arrivals, mode: str, capacity: int, k_steps: int):
                 d = t0 + ta - time.perf_counter()
                 if d > 0:
                     time.sleep(d)
-                ids.append(srv.submit(j["conc"], j["hill"], bcl=SERVE_BCL, n_pace=j["n_pace"],
-                                      first_pace=j["first_pace"]))
-            for k, jid in enumerate(ids):
+                ids.append(submit_job(srv, j))
+            for k, (j, jid) in enumerate(zip(jobs, ids)):
                 srv.wait(jid, 0)
-                _, tm = srv.result(jid)
+                tm = srv.tissue_result(jid)[2] if j["kind"] == "tissue" else srv.result(jid)[1]
                 lat[k] = tm["latency_ms"]
         else:
             for k, (j, ta) in enumerate(zip(jobs, arrivals)):
                 d = t0 + ta - time.perf_counter()
                 if d > 0:
                     time.sleep(d)
-                jid = srv.submit(j["conc"], j["hill"], bcl=SERVE_BCL, n_pace=j["n_pace"], first_pace=j["first_pace"])
+                jid = submit_job(srv, j)
                 srv.wait(jid, 0)
                 lat[k] = (time.perf_counter() - (t0 + ta)) * 1e3
         makespan = time.perf_counter() - t0
@@ -687,7 +708,7 @@ def run_serving(cep, jobs, arrivals, mode: str, capacity: int, k_steps: int):
 def serve_main(args):
     cep = importlib.import_module("2ddrugsimulation_b200")
     jobs = serve_trace(args.jobs, 777)
-    steps = [len(j["conc"]) * int(j["n_pace"] * SERVE_BCL / SERVE_DT) for j in jobs]
+    steps = [job_steps(j) for j in jobs]
     capacity, k_steps = 16384, 10000
     # calibration: every job once, back to back and one at a time, gives
     # each job's service time; arrivals are then Poisson at 1.2x the rate
@@ -706,14 +727,17 @@ def serve_main(args):
                      "cell_steps_per_s": float(sum(steps)) / span, "launches": int(st["launches"])}
     b, s_ = res["batched"], res["serial"]
     line = {
-        "metric": "screen-job p50/p99 latency (continuous batching vs one at a time), CiPA-ORd mixed",
+        "metric": "screen-job p50/p99 latency (continuous batching vs one at a time), CiPA-ORd populations and TT2006 patches, mixed",
         "value": b["p99_ms"], "unit": "ms (p99 latency)", "n_gpus": 1, "steps": len(jobs), "warmup": 3,
         "ms_per_step": b["mean_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 (mixed)", "data": "synthetic",
-        "config": {"workload": f"{len(jobs)} Poisson-arriving CiPA-ORd screening jobs (log-U[20,500] samples x 1-4 "
-                               f"concs, 1-2 paces at BCL 1000 ms, dt 0.005 ms, biomarkers on the last pace), offered "
-                               f"load 1.2x one-at-a-time capacity; pool of {capacity} slots, {k_steps} steps per "
-                               f"launch", "total_cell_steps": int(sum(steps)),
+        "config": {"workload": f"{len(jobs)} Poisson-arriving screening jobs: CiPA-ORd populations (log-U[20,500] "
+                               f"samples x 1-4 concs, 1-2 paces at BCL 1000 ms, dt 0.005 ms, biomarkers on the last "
+                               f"pace) and, one in five, 2D TT2006 patches (log-U[64,192]^2 nodes, U[50,200] ms, dt "
+                               f"0.01 ms, IKr block); offered load 1.2x one-at-a-time capacity; pool of {capacity} "
+                               f"slots, {k_steps} steps per launch (scaled down from 2,000 jobs of 100-5,000 samples "
+                               f"x 200-1,000 paces and 64^2-384^2 patches for 500-2,000 ms)",
+                   "n_tissue_jobs": sum(j["kind"] == "tissue" for j in jobs), "total_cell_steps": int(sum(steps)),
                    "mean_service_s_one_at_a_time": mean_service},
         "latency_ms": {"p50": b["p50_ms"], "p99": b["p99_ms"]},
         "serial": s_, "batched": b,

@@ -243,6 +243,31 @@ int cep_serve_result(cep_server_t s, uint64_t id, cep_biomarkers_t *out, cep_job
 /* Forget a finished job (frees its host-side record). */
 int cep_serve_release(cep_server_t s, uint64_t id);
 int cep_serve_stats(cep_server_t s, cep_serve_stats_t *st);
+
+/* A 2D TT2006 tissue patch as a screening job (an nx x ny sheet of Q1 nodes
+ * with a corner S1 block, the drug as one Hill row on every node). Admitted
+ * while the server's HBM budget has room for it, then stepped with every
+ * other running patch as one tissue group (one batched PCG launch per step)
+ * on a stream of its own, overlapping the population pool's launches. Its
+ * V and activation times are those of running the patch alone (to the
+ * PCG's tolerance). No counterpart in the reference (one Cheart per run,
+ * heart.cpp). */
+typedef struct {
+  int nx, ny;           /* nodes                                       */
+  double h;             /* node spacing, cm                            */
+  double D;             /* isotropic conductivity, cm^2/ms             */
+  double dt;            /* ionic and diffusion step, ms                */
+  double duration;      /* simulated time, ms                          */
+  double conc;          /* drug concentration                          */
+  const double *hill;   /* [14] Hill row (TT2006 uses IKr: hill[12..13]) or NULL */
+  double bcl;           /* S1 period, ms (S1 at t = k*bcl for 1 ms)     */
+  int stim_nx, stim_ny; /* S1 corner block, nodes                      */
+  double rtol;          /* PCG tolerance (<= 0: 1e-8)                  */
+} cep_tissue_job_t;
+int cep_serve_submit_tissue(cep_server_t s, const cep_tissue_job_t *job, uint64_t *id);
+/* Final V and activation times ([nx*ny] each, -1: never activated; either
+ * may be NULL) and timings of a finished tissue job. */
+int cep_serve_tissue_result(cep_server_t s, uint64_t id, double *v, double *t_act, cep_job_times_t *times);
 /* Stop the scheduler (queued and running jobs fail), free the pool. */
 int cep_serve_stop(cep_server_t s);
 
@@ -349,9 +374,11 @@ int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, 
  * stimulus and solver state, but their diffusion solves share one
  * cooperative launch per step (grid blocks split in proportion to rows), so
  * the CG barrier latency is paid once for the whole group. The tissues must
- * share one stream, sparse format, dt and current time; at most one tissue
- * per SM. Results are those of stepping each tissue alone. Replaces running
- * one Cheart (heart.cpp) per concentration or request. */
+ * share one stream and sparse format (and grid dimension); each keeps its
+ * own time and dt; at most one tissue per SM. Results are those of stepping
+ * each tissue alone (to the solver's tolerance: the PCG's block partition
+ * depends on the group). Replaces running one Cheart (heart.cpp) per
+ * concentration or request. */
 typedef struct cep_tissue_group *cep_tissue_group_t;
 int cep_tissue_group_create(const cep_tissue_t *tissues, int count, cep_tissue_group_t *out);
 int cep_tissue_group_run(cep_tissue_group_t g, long n_steps);

@@ -97,3 +97,71 @@ def test_admission_waits_for_free_slots(cep, gpu):
             srv.poll(j1)
     finally:
         srv.close()
+
+
+def _patch_alone(cep, nx, ny, steps, conc, hill, precision):
+    """The same TT2006 patch run directly (cells + operator + tissue)."""
+    n = nx * ny
+    cells = cep.Batch("tt2006", n, precision)
+    cells.init(conc=np.full(n, conc), hill=np.broadcast_to(hill, (n, 14)) if hill is not None else None)
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013, fmt=cep.FEM_CLASSED).set_solver(1e-10)
+    t = cep.Tissue(cells, fem, 0.01)
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:3, :3] = 1
+    t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 1)
+    t.run(steps)
+    return t.v(), t.activation()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tissue_jobs_alone_and_in_a_mix(cep, gpu, precision):
+    """Tissue-patch jobs of different sizes, durations and drugs, running
+    beside population jobs, give each patch's own result (V to the solver
+    tolerance, activation times equal) and leave the population jobs'
+    biomarkers bit-identical."""
+    hill = np.zeros(14)
+    hill[12], hill[13] = 0.4, 1.2
+    patches = [(24, 18, 450, 0.0), (16, 30, 300, 0.5), (20, 20, 600, 1.5)]
+    alone = [_patch_alone(cep, nx, ny, steps, c, hill, precision) for nx, ny, steps, c in patches]
+    srv = cep.Server("ord2011", precision, capacity=256, dt=0.005, max_bcl=1000.0, steps_per_launch=7000)
+    try:
+        a_conc, a_hill = _job(5, 10, 3)
+        ja = srv.submit(a_conc, a_hill, bcl=1000.0, n_pace=2, first_pace=1)
+        srv.wait(ja, 600)
+        pop_alone, _ = srv.result(ja)
+        ids = [srv.submit_tissue(nx, ny, steps * 0.01, conc=c, hill=hill, stim=(3, 3), rtol=1e-10)
+               for nx, ny, steps, c in patches]
+        ja2 = srv.submit(a_conc, a_hill, bcl=1000.0, n_pace=2, first_pace=1)
+        for j in ids + [ja2]:
+            srv.wait(j, 600)
+        for (v0, a0), j in zip(alone, ids):
+            v, ta, tm = srv.tissue_result(j)
+            assert np.abs(v - v0).max() <= 1e-6
+            assert np.array_equal(ta, a0)
+            assert tm["latency_ms"] >= tm["run_ms"] > 0
+        pop_mix, _ = srv.result(ja2)
+        for f in FIELDS:
+            assert np.array_equal(pop_alone[f], pop_mix[f]), f
+        with pytest.raises(cep.CepError):
+            srv.result(ids[0])  # a tissue job has no biomarker records
+    finally:
+        srv.close()
+
+
+@pytest.mark.gpu
+def test_tissue_job_rejections(cep, gpu):
+    srv = cep.Server("ord2011", "mixed", capacity=64, dt=0.005, max_bcl=1000.0, steps_per_launch=5000,
+                     hbm_fraction=0.5)
+    try:
+        with pytest.raises(cep.CepError) as e:
+            srv.submit_tissue(1, 10, 10.0)
+        assert e.value.code == cep.ERR_ARG
+        with pytest.raises(cep.CepError) as e:
+            srv.submit_tissue(10, 10, -1.0)
+        assert e.value.code == cep.ERR_ARG
+        with pytest.raises(cep.CepError) as e:
+            srv.submit_tissue(1 << 14, 1 << 14, 10.0)  # 2^28 nodes: over any HBM budget
+        assert e.value.code in (cep.ERR_OOM, cep.ERR_ARG)
+    finally:
+        srv.close()
