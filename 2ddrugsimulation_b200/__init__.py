@@ -165,6 +165,10 @@ _SIGS = {
                                                ctypes.POINTER(ctypes.c_void_p)]),
     "cep_tissue_group_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_tissue_group_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_tissue_set_electrodes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.c_long, ctypes.c_long]),
+    "cep_tissue_get_ecg": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_long)]),
     "cep_tissue_group_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "cep_tissue_group_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long)]),
@@ -481,6 +485,23 @@ class Tissue:
         _check(lib().cep_tissue_set_stimulus(self._h, m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt,
                                              dur, n_pace))
         return self
+
+    def set_electrodes(self, xyz, every: int = 1, max_records: int = 10000) -> "Tissue":
+        """Record the pseudo-ECG at electrodes xyz [n_el, 3] (cm) every
+        `every` steps (at most max_records records)."""
+        e = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+        self._n_el = e.shape[0]
+        _check(lib().cep_tissue_set_electrodes(self._h, self._n_el, _dptr(e), int(every), int(max_records)))
+        return self
+
+    def ecg(self) -> np.ndarray:
+        """Pseudo-ECG records so far, [n_records, n_el]."""
+        n = ctypes.c_long()
+        _check(lib().cep_tissue_get_ecg(self._h, None, ctypes.byref(n)))
+        out = np.empty((n.value, getattr(self, "_n_el", 0)))
+        if n.value:
+            _check(lib().cep_tissue_get_ecg(self._h, _dptr(out), ctypes.byref(n)))
+        return out
 
     def set_activation_threshold(self, vm: float) -> "Tissue":
         _check(lib().cep_tissue_set_activation_threshold(self._h, vm))

@@ -684,6 +684,9 @@ struct cep_fem {
   int n_classes = 0;
   int dim = 0, gnx = 0, gny = 0, gnz = 0;
   double *r = nullptr, *q = nullptr, *part = nullptr;
+  double *D = nullptr;  // grid operators: conductivity per element [n_elem][n_d] (pseudo-ECG)
+  int n_d = 0;
+  double h = 0.0;
   double *p0 = nullptr, *p1 = nullptr, *z = nullptr;  // row 0 of [guard | ld | guard] zero-filled buffers
   int64_t guard = 0;  // rows a grid-format gather may reach past either end
   Ctl *ctl = nullptr;
@@ -948,7 +951,129 @@ struct cep_tissue {
   double act_thr = -30.0;
   double dt = 0.01, t = 0.0;
   long steps = 0;
+  // pseudo-ECG: electrodes, per-block partials, records on the device
+  int n_el = 0;
+  double *el = nullptr, *ecg_part = nullptr, *ecg_rec = nullptr;
+  long ecg_every = 1, ecg_max = 0, ecg_n = 0;
 };
+
+namespace {
+
+constexpr int kEcgBlock = 256, kEcgChunk = 16;
+
+// Pseudo-ECG of a grid tissue (Cheart::Radiate, heart.cpp:640-690): for
+// each electrode x, phi = w sum_e sum_g (D_e grad V(g)) . (c_e - x) detJ /
+// |c_e - x|^3, c_e the element centroid, w = 1/6 (the reference's weight),
+// Gauss points +-0.57735 as the assembly. With symmetric Gauss points the
+// element's sum over g of grad V is (2/h) sum_n V_n s_n (s_n = the local
+// node's corner signs), so each element costs one gradient and one dot
+// product per electrode. Electrodes kEcgChunk at a time; each block writes
+// one partial per electrode, summed in a fixed order by ecg_sum_kernel.
+template <int DIM>
+__global__ void __launch_bounds__(kEcgBlock) ecg_kernel(const double *__restrict__ v, const double *__restrict__ D,
+                                                        int n_d, int nx, int ny, int nz, double h,
+                                                        const double *__restrict__ el, int e0, int ne,
+                                                        double *__restrict__ part) {
+  const int64_t n_elem = (int64_t)(nx - 1) * (ny - 1) * (DIM == 3 ? (nz - 1) : 1);
+  const double inv = 2.0 / h, jac = 0.5 * h;
+  const double detJ = DIM == 3 ? jac * jac * jac : jac * jac;
+  constexpr int NN = DIM == 3 ? 8 : 4;
+  double acc[kEcgChunk];
+#pragma unroll
+  for (int k = 0; k < kEcgChunk; ++k) acc[k] = 0.0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_elem; e += (int64_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(e % (nx - 1)), ey = (int)((e / (nx - 1)) % (ny - 1));
+    const int ez = DIM == 3 ? (int)(e / ((int64_t)(nx - 1) * (ny - 1))) : 0;
+    // sum over Gauss points of grad V, times detJ (local node order of the assembly)
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      const int ox = (a == 1 || a == 2 || a == 5 || a == 6) ? 1 : 0;
+      const int oy = (a == 2 || a == 3 || a == 6 || a == 7) ? 1 : 0;
+      const int oz = a >= 4 ? 1 : 0;
+      const double va = v[(int64_t)(ex + ox) + (int64_t)nx * ((ey + oy) + (int64_t)ny * (ez + oz))];
+      gx += ox ? va : -va;
+      gy += oy ? va : -va;
+      if (DIM == 3) gz += oz ? va : -va;
+    }
+    const double sc = inv * detJ;
+    gx *= sc;
+    gy *= sc;
+    gz *= sc;
+    const double *d = D + e * n_d;
+    double qx, qy, qz;
+    if (n_d == 1) {
+      qx = d[0] * gx; qy = d[0] * gy; qz = DIM == 3 ? d[0] * gz : 0.0;
+    } else if (DIM == 2) {
+      qx = d[0] * gx + d[1] * gy; qy = d[1] * gx + d[2] * gy; qz = 0.0;
+    } else {
+      qx = d[0] * gx + d[1] * gy + d[2] * gz; qy = d[1] * gx + d[3] * gy + d[4] * gz;
+      qz = d[2] * gx + d[4] * gy + d[5] * gz;
+    }
+    const double cx = (ex + 0.5) * h, cy = (ey + 0.5) * h, cz = DIM == 3 ? (ez + 0.5) * h : 0.0;
+#pragma unroll
+    for (int k = 0; k < kEcgChunk; ++k) {
+      if (k < ne) {
+        const double rx = cx - el[3 * (e0 + k)], ry = cy - el[3 * (e0 + k) + 1], rz = cz - el[3 * (e0 + k) + 2];
+        const double rr = sqrt(rx * rx + ry * ry + rz * rz);
+        acc[k] += (qx * rx + qy * ry + qz * rz) / (rr * rr * rr);
+      }
+    }
+  }
+  // fixed-order block sums, one partial per electrode and block
+  __shared__ double sm[kEcgBlock / 32];
+  for (int k = 0; k < ne; ++k) {
+    double x = acc[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kEcgBlock / 32; ++w) t += sm[w];
+      part[(int64_t)(e0 + k) * gridDim.x + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void ecg_sum_kernel(const double *part, int blocks, int n_el, double w, double *rec) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_el) return;
+  double t = 0.0;
+  for (int b = 0; b < blocks; ++b) t += part[(int64_t)k * blocks + b];
+  rec[k] = w * t;
+}
+
+int ecg_blocks() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, 2 * sms);
+}
+
+// record the tissue's pseudo-ECG for its current V (asynchronous)
+int ecg_record(cep_tissue *t) {
+  if (t->n_el == 0 || t->ecg_n >= t->ecg_max || t->steps % t->ecg_every != 0) return CEP_OK;
+  const cep_fem *f = t->fem;
+  const int blocks = ecg_blocks();
+  const double *v = cep_internal_batch_v(t->cells);
+  for (int e0 = 0; e0 < t->n_el; e0 += kEcgChunk) {
+    const int ne = std::min(kEcgChunk, t->n_el - e0);
+    if (f->dim == 3)
+      ecg_kernel<3><<<blocks, kEcgBlock, 0, t->stream>>>(v, f->D, f->n_d, f->gnx, f->gny, f->gnz, f->h, t->el, e0, ne,
+                                                         t->ecg_part);
+    else
+      ecg_kernel<2><<<blocks, kEcgBlock, 0, t->stream>>>(v, f->D, f->n_d, f->gnx, f->gny, 1, f->h, t->el, e0, ne,
+                                                         t->ecg_part);
+  }
+  ecg_sum_kernel<<<(t->n_el + 127) / 128, 128, 0, t->stream>>>(t->ecg_part, blocks, t->n_el, 1.0 / 6.0,
+                                                                t->ecg_rec + (int64_t)t->ecg_n * t->n_el);
+  FEM_CUDA(cudaGetLastError());
+  ++t->ecg_n;
+  return CEP_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -996,10 +1121,13 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
     fem_free(f);
     return rc;
   }
-  if (cudaMalloc(&d_D, sizeof(double) * n_elem * n_d) != cudaSuccess) {
+  if ((rc = fem_alloc(f, &d_D, (size_t)n_elem * n_d))) {
     fem_free(f);
-    return fail_msg(CEP_ERR_OOM, "cudaMalloc for the conductivity field failed");
+    return rc;
   }
+  f->D = d_D;
+  f->n_d = n_d;
+  f->h = h;
   cudaError_t e = cudaMemcpyAsync(f->rp, rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, f->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_D, D, sizeof(double) * n_elem * n_d, cudaMemcpyHostToDevice, f->stream);
   if (e == cudaSuccess && cep_internal_fem_assemble_grid(dim, nx, ny, nz, h, dt, d_D, n_d, f->rp, f->col, f->a, f->b,
@@ -1011,7 +1139,6 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
-  cudaFree(d_D);
   if (e != cudaSuccess) {
     fem_free(f);
     return fail_msg(CEP_ERR_CUDA, "grid assembly failed: %s", cudaGetErrorString(e));
@@ -1386,6 +1513,7 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
     for (cep_tissue_t t : g->ts) {
       t->t += t->dt;
       ++t->steps;
+      if ((rc = ecg_record(t))) return rc;
     }
   }
   return CEP_OK;
@@ -1436,6 +1564,9 @@ int cep_tissue_destroy(cep_tissue_t t) {
   cudaStreamSynchronize(t->stream);
   cudaFree(t->mask);
   cudaFree(t->tact);
+  cudaFree(t->el);
+  cudaFree(t->ecg_part);
+  cudaFree(t->ecg_rec);
   delete t;
   return CEP_OK;
 }
@@ -1469,7 +1600,47 @@ int cep_tissue_run(cep_tissue_t t, long n_steps) {
     t->t += t->dt;
     ++t->steps;
     if ((rc = fem_solve_async(t->fem, v, t->tact, t->t, t->act_thr))) return rc;
+    if ((rc = ecg_record(t))) return rc;
   }
+  return CEP_OK;
+}
+
+int cep_tissue_set_electrodes(cep_tissue_t t, int n_el, const double *xyz, long every, long max_records) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (n_el < 0 || (n_el > 0 && !xyz) || every <= 0 || max_records < 0)
+    return fail_msg(CEP_ERR_ARG, "bad electrode set (n_el >= 0, every > 0, max_records >= 0)");
+  if (n_el > 0 && !t->fem->D) return fail_msg(CEP_ERR_UNSUPPORTED, "pseudo-ECG needs a grid operator");
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  cudaFree(t->el);
+  cudaFree(t->ecg_part);
+  cudaFree(t->ecg_rec);
+  t->el = t->ecg_part = t->ecg_rec = nullptr;
+  t->n_el = 0;
+  t->ecg_n = 0;
+  if (n_el == 0) return CEP_OK;
+  const int blocks = ecg_blocks();
+  if (cudaMalloc((void **)&t->el, sizeof(double) * 3 * n_el) != cudaSuccess ||
+      cudaMalloc((void **)&t->ecg_part, sizeof(double) * (size_t)n_el * blocks) != cudaSuccess ||
+      cudaMalloc((void **)&t->ecg_rec, sizeof(double) * (size_t)n_el * std::max(1L, max_records)) != cudaSuccess) {
+    cudaFree(t->el);
+    cudaFree(t->ecg_part);
+    cudaFree(t->ecg_rec);
+    t->el = t->ecg_part = t->ecg_rec = nullptr;
+    return fail_msg(CEP_ERR_OOM, "pseudo-ECG buffers");
+  }
+  FEM_CUDA(cudaMemcpy(t->el, xyz, sizeof(double) * 3 * n_el, cudaMemcpyHostToDevice));
+  t->n_el = n_el;
+  t->ecg_every = every;
+  t->ecg_max = max_records;
+  return CEP_OK;
+}
+
+int cep_tissue_get_ecg(cep_tissue_t t, double *phi, long *n_records) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  if (n_records) *n_records = t->ecg_n;
+  if (phi && t->ecg_n > 0)
+    FEM_CUDA(cudaMemcpy(phi, t->ecg_rec, sizeof(double) * (size_t)t->ecg_n * t->n_el, cudaMemcpyDeviceToHost));
   return CEP_OK;
 }
 

@@ -369,6 +369,18 @@ int cep_tissue_sync(cep_tissue_t t);
 int cep_tissue_get_v(cep_tissue_t t, double *v);
 int cep_tissue_get_activation(cep_tissue_t t, double *t_act);
 int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, int *not_converged);
+/* Pseudo-ECG (Cheart::Radiate, heart.cpp:640-690, and its callers at
+ * heart.cpp:560-576): after every `every`-th step the tissue records, for
+ * each of n_el electrodes at xyz[3*k..] (cm; node (i, j, k) of the grid sits
+ * at (i h, j h, k h)), phi = w sum_elements sum_gauss (D grad V) . (c - x)
+ * detJ / |c - x|^3, c the element centroid, w = 1/6 as the reference; at
+ * most max_records records are kept on the device. The reference's
+ * uninitialised Gauss counter and its accumulator that is never reset
+ * between calls are not reproduced. Grid operators only
+ * (CEP_ERR_UNSUPPORTED otherwise); n_el = 0 turns it off. */
+int cep_tissue_set_electrodes(cep_tissue_t t, int n_el, const double *xyz, long every, long max_records);
+/* Copy the records so far (phi[n_records][n_el]; phi may be NULL). */
+int cep_tissue_get_ecg(cep_tissue_t t, double *phi, long *n_records);
 
 /* A group of tissues stepped together: each keeps its own cells, operator,
  * stimulus and solver state, but their diffusion solves share one

@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
         L.cepo_fem_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, _dp, ctypes.c_int, _ip, _ip, _dp, _dp]
         L.cepo_fem_element.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp, _dp]
+        L.cepo_pseudo_ecg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp,
+                                      ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
         L.cepo_spmv.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
         L.cepo_pcg2.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                 _dp]
@@ -278,6 +280,18 @@ def fem_assemble(dim: int, nx: int, ny: int, nz: int, h: float, dt: float, D):
     bv = np.zeros(nnz)
     lib().cepo_fem_assemble(dim, nx, ny, nz, h, dt, _ptr(d), d.shape[1], _iptr(rp), _iptr(ci), _ptr(av), _ptr(bv))
     return rp, ci, av, bv
+
+
+def pseudo_ecg(dim: int, nx: int, ny: int, nz: int, h: float, D, V, xyz) -> np.ndarray:
+    """Pseudo-ECG of a grid tissue's V at electrodes xyz [n_el, 3] (cm)."""
+    if dim == 2:
+        nz = 1
+    d = element_D(dim, nx, ny, nz, D)
+    e = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    vv = np.ascontiguousarray(V, np.float64)
+    out = np.zeros(e.shape[0])
+    lib().cepo_pseudo_ecg(dim, nx, ny, nz, h, _ptr(d), d.shape[1], _ptr(vv), e.shape[0], _ptr(e), _ptr(out))
+    return out
 
 
 def fem_element(dim: int, h: float, dt: float, D) -> tuple[np.ndarray, np.ndarray]:

@@ -109,6 +109,10 @@ int cepo_pcg2(int n, const int *row_ptr, const int *col_idx, const double *a_val
               double rtol, int max_iter, int precond_norm, double *rel_res);
 /* Element matrices (nn x nn, row-major) of an axis-aligned element of edge h. */
 void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be);
+/* Pseudo-ECG at n_el electrodes xyz[3*k..] of a grid tissue's V
+ * (Cheart::Radiate, heart.cpp:640-690). */
+void cepo_pseudo_ecg(int dim, int nx, int ny, int nz, double h, const double *D, int n_d, const double *V,
+                     int n_el, const double *xyz, double *phi);
 /* Godunov-split tissue run on a structured grid (heart.cpp:127-165). */
 long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,

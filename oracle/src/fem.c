@@ -100,6 +100,85 @@ void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, do
   }
 }
 
+/* Shape-function gradients (reference coordinates) at Gauss point g of the
+ * reference's element (fem.cpp:398-478), as cepo_fem_element uses them. */
+static void gauss_gradients(int dim, int g, double dS[8][3]) {
+  double s, t, z = 0.0;
+  if (dim == 2) {
+    const double g4[4][2] = {{-GA, -GA}, {GA, -GA}, {GA, GA}, {-GA, GA}};
+    s = g4[g][0]; t = g4[g][1];
+    dS[0][0] = -(1. - t) / 4.; dS[0][1] = -(1. - s) / 4.;
+    dS[1][0] = +(1. - t) / 4.; dS[1][1] = -(1. + s) / 4.;
+    dS[2][0] = +(1. + t) / 4.; dS[2][1] = +(1. + s) / 4.;
+    dS[3][0] = -(1. + t) / 4.; dS[3][1] = +(1. - s) / 4.;
+    return;
+  }
+  const double aa[2] = {-GA, GA};
+  s = aa[(g >> 2) & 1]; t = aa[(g >> 1) & 1]; z = aa[g & 1];
+  const double sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  for (int n = 0; n < 8; ++n) {
+    const double fs = 1 + sg[n][0] * s, ft = 1 + sg[n][1] * t, fz = 1 + sg[n][2] * z;
+    dS[n][0] = sg[n][0] * ft * fz / 8.; dS[n][1] = sg[n][1] * fs * fz / 8.; dS[n][2] = sg[n][2] * fs * ft / 8.;
+  }
+}
+
+/* Pseudo-ECG of a structured-grid tissue at n_el electrodes (Cheart::Radiate,
+ * heart.cpp:640-690): for every element, r = centroid - electrode, and for
+ * every Gauss point bsp -= (D grad V) . r detJ w / |r|^3 with w = 1/6; the
+ * electrode's value is -sum over elements of bsp. Node (i, j, k) sits at
+ * (i h, j h, k h). The reference's Gauss counter is uninitialised and its
+ * accumulator is never reset between calls; here the loop starts at 0 and
+ * every call starts from 0. */
+void cepo_pseudo_ecg(int dim, int nx, int ny, int nz, double h, const double *D, int n_d, const double *V,
+                     int n_el, const double *xyz, double *phi) {
+  if (dim == 2) nz = 1;
+  const int nn = dim == 2 ? 4 : 8;
+  int off[8][3];
+  local_offsets(dim, off);
+  const double jac = 0.5 * h, inv = 1.0 / jac;
+  const double detJ = dim == 2 ? jac * jac : jac * jac * jac;
+  const double w = 1.0 / 6.0;
+  for (int k = 0; k < n_el; ++k) phi[k] = 0.0;
+  const long nex = nx - 1, ney = ny - 1, nez = dim == 3 ? nz - 1 : 1;
+  for (long ez = 0; ez < nez; ++ez)
+    for (long ey = 0; ey < ney; ++ey)
+      for (long ex = 0; ex < nex; ++ex) {
+        const long e = ex + nex * (ey + ney * ez);
+        const double *d = D + e * n_d;
+        double Dm[3][3] = {{0}};
+        if (n_d == 1) {
+          for (int a = 0; a < dim; ++a) Dm[a][a] = d[0];
+        } else if (dim == 2) {
+          Dm[0][0] = d[0]; Dm[0][1] = Dm[1][0] = d[1]; Dm[1][1] = d[2];
+        } else {
+          Dm[0][0] = d[0]; Dm[0][1] = Dm[1][0] = d[1]; Dm[0][2] = Dm[2][0] = d[2];
+          Dm[1][1] = d[3]; Dm[1][2] = Dm[2][1] = d[4]; Dm[2][2] = d[5];
+        }
+        double ve[8], c[3] = {0, 0, 0};
+        for (int a = 0; a < nn; ++a) {
+          const long i = ex + off[a][0], j = ey + off[a][1], kk = ez + off[a][2];
+          ve[a] = V[i + (long)nx * (j + (long)ny * kk)];
+          c[0] += (double)i * h / nn; c[1] += (double)j * h / nn; c[2] += dim == 3 ? (double)kk * h / nn : 0.0;
+        }
+        for (int g = 0; g < nn; ++g) {
+          double dS[8][3];
+          gauss_gradients(dim, g, dS);
+          double vd[3] = {0, 0, 0}, vel[3] = {0, 0, 0};
+          for (int a = 0; a < nn; ++a)
+            for (int q = 0; q < dim; ++q) vd[q] += dS[a][q] * inv * ve[a];
+          for (int q = 0; q < dim; ++q)
+            for (int p2 = 0; p2 < dim; ++p2) vel[q] += Dm[q][p2] * vd[p2];
+          for (int k = 0; k < n_el; ++k) {
+            const double r[3] = {c[0] - xyz[3 * k], c[1] - xyz[3 * k + 1], c[2] - xyz[3 * k + 2]};
+            const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            const double bsp = -(vel[0] * r[0] + vel[1] * r[1] + vel[2] * r[2]) * detJ * w / pow(rr, 3);
+            phi[k] -= bsp;
+          }
+        }
+      }
+}
+
 static long node_id(int dim, int nx, int ny, int i, int j, int k) {
   (void)dim;
   return (long)i + (long)nx * ((long)j + (long)ny * (long)k);

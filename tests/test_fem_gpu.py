@@ -359,3 +359,65 @@ def test_ord_slab_3d_anisotropic_matches_oracle(cep, gpu, oracle):
     assert (tacto > 0).all()
     assert np.abs(t.v() - vo).max() <= 1e-6
     assert np.array_equal(t.activation(), tacto)
+
+
+ELECTRODES = [[0.1, 0.2, 1.0], [0.5, -0.3, 0.4], [0.2, 0.1, -0.6], [2.0, 2.0, 0.0]]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim", [2, 3])
+def test_pseudo_ecg_matches_oracle(cep, gpu, oracle, dim):
+    """The pseudo-ECG recorded after each step equals the oracle's
+    restatement of Cheart::Radiate on the same V (relative 1e-10)."""
+    if dim == 2:
+        nx, ny, nz = 21, 17, 1
+        D = _tensor_field(2, (nx - 1) * (ny - 1), 11)
+        n = nx * ny
+        cells = cep.Batch("tt2006", n, "fp64")
+        cells.init()
+        mask = np.zeros((ny, nx), np.uint8)
+        mask[:3, :3] = 1
+        mask = mask.ravel()
+    else:
+        import bench
+        nx, ny, nz = 9, 8, 6
+        ct, D, mask = bench.slab_fields(nx, ny, nz)
+        n = nx * ny * nz
+        cells = cep.Batch("ord2011", n, "fp64")
+        cells.init(celltype=ct, quirks=False)
+    fem = cep.Fem.grid(dim, nx, ny, nz, 0.025, 0.01, D).set_solver(1e-10)
+    t = cep.Tissue(cells, fem, 0.01)
+    t.set_stimulus(mask, 1000.0, 0.0, 1.0, 1)
+    t.set_electrodes(ELECTRODES * 5, every=1, max_records=100)  # 20 electrodes: two chunks
+    t.run(120)
+    rec = t.ecg()
+    assert rec.shape == (100, 20)
+    t.set_electrodes(ELECTRODES * 5, every=1, max_records=5)
+    t.run(1)
+    last = t.ecg()[0]
+    ref = oracle.pseudo_ecg(dim, nx, ny, nz, 0.025, D, t.v(), np.array(ELECTRODES * 5))
+    assert np.abs(ref).max() > 0
+    assert np.all(np.abs(last - ref) <= 1e-10 * np.abs(ref).max()), np.abs(last - ref).max()
+
+
+@pytest.mark.gpu
+def test_pseudo_ecg_cadence_and_limits(cep, gpu, oracle):
+    n = 12 * 10
+    cells = cep.Batch("tt2006", n, "mixed")
+    cells.init()
+    fem = cep.Fem.grid(2, 12, 10, 1, 0.025, 0.01, 0.0013)
+    t = cep.Tissue(cells, fem, 0.01)
+    t.set_electrodes(ELECTRODES[:2], every=3, max_records=2)
+    t.run(10)
+    assert t.ecg().shape == (2, 2)
+    t.set_electrodes([], every=1, max_records=0)
+    t.run(3)
+    assert t.ecg().shape == (0, 0)
+    rp, ci, a, b = oracle.fem_assemble(2, 12, 10, 1, 0.025, 0.01, 0.0013)
+    u = cep.Fem.csr(rp, ci, a, b, 0.01)
+    cells2 = cep.Batch("tt2006", n, "mixed")
+    cells2.init()
+    t2 = cep.Tissue(cells2, u, 0.01)
+    with pytest.raises(cep.CepError) as e:
+        t2.set_electrodes(ELECTRODES[:1])
+    assert e.value.code == cep.ERR_UNSUPPORTED

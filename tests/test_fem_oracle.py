@@ -85,3 +85,27 @@ def test_tissue_wave_propagates(oracle):
     assert T[0, 0] < T[0, -1] < T[-1, -1]
     assert np.abs(T - T.T).max() < 1e-9
     assert (its > 0).all()
+
+
+def test_pseudo_ecg_oracle_properties(oracle):
+    """The pseudo-ECG restatement: zero for a uniform V; for a linear ramp
+    it is the element-centroid quadrature of w * int (D grad V) . r / |r|^3
+    (w = 1/6); linear in V."""
+    nx, ny, h, D = 20, 16, 0.025, 0.0013
+    el = np.array([[0.2, 0.2, 1.0], [5.0, 0.2, 0.0]])
+    assert np.abs(oracle.pseudo_ecg(2, nx, ny, 1, h, D, np.full(nx * ny, -80.0), el)).max() <= 1e-15
+    x = (np.arange(nx * ny) % nx) * h
+    got = oracle.pseudo_ecg(2, nx, ny, 1, h, D, 100.0 * x, el)
+    ref = np.zeros(2)
+    for ey in range(ny - 1):
+        for ex in range(nx - 1):
+            c = np.array([(ex + 0.5) * h, (ey + 0.5) * h, 0.0])
+            for k in range(2):
+                r = c - el[k]
+                ref[k] += D * 100.0 * r[0] / np.linalg.norm(r) ** 3 * h * h / 6.0
+    assert np.allclose(got, ref, rtol=1e-12, atol=0)
+    rng = np.random.default_rng(3)
+    v1, v2 = rng.normal(size=nx * ny), rng.normal(size=nx * ny)
+    lhs = oracle.pseudo_ecg(2, nx, ny, 1, h, D, 2.0 * v1 - v2, el)
+    rhs = 2.0 * oracle.pseudo_ecg(2, nx, ny, 1, h, D, v1, el) - oracle.pseudo_ecg(2, nx, ny, 1, h, D, v2, el)
+    assert np.allclose(lhs, rhs, rtol=1e-12, atol=1e-18)
