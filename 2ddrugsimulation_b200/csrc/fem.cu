@@ -123,6 +123,11 @@ struct CsrView {
   __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
     return apply(val, i, [&](int j) { return d(j); });
   }
+  // a per-row key the product pass may load a trip ahead (none here)
+  __device__ __forceinline__ int row_key(int64_t) const { return 0; }
+  __device__ __forceinline__ double apply_dir_key(const double *val, int64_t i, int, const Dir &d) const {
+    return apply_dir(val, i, d);
+  }
   __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const Dir &) const {}
 };
 
@@ -140,6 +145,10 @@ struct EllView {
   }
   __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
     return apply(val, i, [&](int j) { return d(j); });
+  }
+  __device__ __forceinline__ int row_key(int64_t) const { return 0; }
+  __device__ __forceinline__ double apply_dir_key(const double *val, int64_t i, int, const Dir &d) const {
+    return apply_dir(val, i, d);
   }
   __device__ __forceinline__ void prefetch(int64_t, int64_t, int64_t, const Dir &) const {}
 };
@@ -194,6 +203,10 @@ struct StencilView {
       }
     return s;
   }
+  __device__ __forceinline__ int row_key(int64_t) const { return 0; }
+  __device__ __forceinline__ double apply_dir_key(const double *val, int64_t i, int, const Dir &d) const {
+    return apply_dir(val, i, d);
+  }
   // Rows [b, b + count) come next: fetch into L2 what the sweep has not
   // touched yet, the leading plane (3D) or line (2D) of their
   // neighbourhood (rounded out to 16-byte boundaries).
@@ -245,7 +258,12 @@ struct ClassView {
   }
   // Unchecked gathers as StencilView::apply_dir; coefficients two at a time.
   __device__ __forceinline__ double apply_dir(const double *val, int64_t i, const Dir &d) const {
-    const double2 *c2 = reinterpret_cast<const double2 *>(val + (int64_t)__ldg(cls + i) * kStride);
+    return apply_dir_key(val, i, __ldg(cls + i), d);
+  }
+  // the row's class, loaded a trip ahead by the product pass
+  __device__ __forceinline__ int row_key(int64_t i) const { return __ldg(cls + i); }
+  __device__ __forceinline__ double apply_dir_key(const double *val, int64_t i, int key, const Dir &d) const {
+    const double2 *c2 = reinterpret_cast<const double2 *>(val + (int64_t)key * kStride);
     const int plane = nx * ny;
     double s = 0.0;
     double2 cp = make_double2(0.0, 0.0);
@@ -494,6 +512,11 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
     // A: p_k and q = A p_k (operators still iterating); report completions
     if (!done) {
       double spq = 0.0, unused = 0.0;
+      int key1 = 0, key2 = 0;  // this trip's row keys (the classed format's class index)
+      if (i0 < a.n) {
+        key1 = m.row_key(i0);
+        key2 = m.row_key(i0 + stride < a.n ? i0 + stride : i0);
+      }
       for (int64_t i = i0; i < a.n; i += 2 * stride) {
         // the block's rows two trips ahead, fetched into L2 by one thread
         const Dir d{pc, a.z, beta};
@@ -504,8 +527,13 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
         }
         const bool two = i + stride < a.n;
         const int64_t i2 = two ? i + stride : i;
-        const double q1 = m.apply_dir(m.a, i, d);
-        const double q2 = m.apply_dir(m.a, i2, d);
+        // next trip's keys, in flight while this trip computes
+        const int64_t j1 = i + 2 * stride, j2 = j1 + stride < a.n ? j1 + stride : j1;
+        const int nkey1 = j1 < a.n ? m.row_key(j1) : 0, nkey2 = j1 < a.n ? m.row_key(j2) : 0;
+        const double q1 = m.apply_dir_key(m.a, i, key1, d);
+        const double q2 = m.apply_dir_key(m.a, i2, key2, d);
+        key1 = nkey1;
+        key2 = nkey2;
         const double c1 = pc[i], c2 = pc[i2];
         const double p1 = fma(beta, c1, a.z[i]), p2 = fma(beta, c2, a.z[i2]);
         pn[i] = p1;
