@@ -169,6 +169,8 @@ _SIGS = {
                                                  ctypes.c_long, ctypes.c_long]),
     "cep_tissue_get_ecg": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_long)]),
+    "cep_tissue_set_s2": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.POINTER(ctypes.c_uint8), ctypes.c_double]),
     "cep_tissue_group_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "cep_tissue_group_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long)]),
@@ -352,6 +354,7 @@ def qinward(control: Biomarkers, drug: Biomarkers) -> float:
 
 
 FEM_AUTO, FEM_CSR, FEM_ELL, FEM_STENCIL, FEM_CLASSED = -1, 0, 1, 2, 3
+S2_NONE, S2_RESET, S2_ECTOPIC = 0, 1, 2
 
 
 def _iptr(a: np.ndarray | None):
@@ -492,6 +495,18 @@ class Tissue:
         e = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
         self._n_el = e.shape[0]
         _check(lib().cep_tissue_set_electrodes(self._h, self._n_el, _dptr(e), int(every), int(max_records)))
+        return self
+
+    def set_s2(self, kind: int, target: int, vm_threshold: float, region=None, ectopic_dur: float = 0.0) -> "Tissue":
+        """Arm the S1-S2 reset (S2_RESET) or ectopic (S2_ECTOPIC) protocol on
+        region [n] monitored at node `target`; S2_NONE disarms."""
+        m = None
+        if region is not None:
+            m = np.ascontiguousarray(np.asarray(region, np.uint8).ravel())
+        _check(lib().cep_tissue_set_s2(self._h, int(kind), int(target), float(vm_threshold),
+                                       None if m is None else m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                       float(ectopic_dur)))
+        self._s2_region = m
         return self
 
     def ecg(self) -> np.ndarray:

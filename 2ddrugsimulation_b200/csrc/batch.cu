@@ -480,6 +480,8 @@ struct TissueArgs {
   double t, dt;
   const unsigned char *mask;  // null: stim_on is the mode of every instance
   int stim_on;  // the window test, uniform over the tissue (or -1/0/1 without a mask)
+  const CepProto *proto;       // S1-S2 / ectopic state on the device, or null
+  const unsigned char *mask2;  // ectopic region (with proto)
 };
 
 template <class M, class P>
@@ -492,7 +494,11 @@ __global__ void __launch_bounds__(128) tissue_kernel(TissueArgs a) {
   M::template load<G>(y, a.y, a.ld, i);
   M::template load_par<G>(q, a.par, a.ld, i);
   typename M::template Cur<G> c;
-  const int mode = a.mask ? ((a.stim_on && a.mask[i]) ? 1 : 0) : a.stim_on;
+  int mode = a.mask ? ((a.stim_on && a.mask[i]) ? 1 : 0) : a.stim_on;
+  if (a.proto) {  // S1 stays off once the protocol fired; the ectopic region as S1 (isEctopic)
+    if (a.proto->fired && a.mask) mode = 0;
+    if (a.mask2 && a.proto->ecto_on && a.mask2[i]) mode = 1;
+  }
   M::template step<P>(y, q, a.t, a.dt, mode, true, c);
   M::template store<G>(y, a.y, a.ld, i);
 }
@@ -1130,10 +1136,11 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
 }
 
 int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, double t, double bcl, double t_crt,
-                                   double dur, int n_pace) {
+                                   double dur, int n_pace, const CepProto *proto, const unsigned char *d_mask2) {
   if (!b || !b->initialized) return fail(CEP_ERR_STATE, "tissue batch not initialised");
   TissueArgs a;
   a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = t; a.dt = b->dt; a.mask = d_mask;
+  a.proto = proto; a.mask2 = d_mask2;
   // the "square" mesh S1 window (heart.cpp:309-323)
   const int iia = (int)(t / bcl);
   a.stim_on = (iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt) ? 1 : 0;
@@ -1171,6 +1178,7 @@ int cep_batch_step(cep_batch_t b, double t, double dt, int stim_mode) {
   if (stim_mode < -1 || stim_mode > 1) return fail(CEP_ERR_ARG, "stim_mode must be -1, 0 or 1");
   TissueArgs a;
   a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = t; a.dt = dt; a.mask = nullptr;
+  a.proto = nullptr; a.mask2 = nullptr;
   a.stim_on = stim_mode;
   return model_info(b->model)->tissue(b, a);
 }

@@ -983,6 +983,12 @@ struct cep_tissue {
   int n_el = 0;
   double *el = nullptr, *ecg_part = nullptr, *ecg_rec = nullptr;
   long ecg_every = 1, ecg_max = 0, ecg_n = 0;
+  // S1-S2 / ectopic protocol: device state, region, reset snapshot
+  int proto_kind = CEP_S2_NONE;
+  CepProto *proto = nullptr;
+  unsigned char *mask2 = nullptr;
+  int *s2_nodes = nullptr, s2_count = 0, ns = 0;
+  double *s2_snap = nullptr;  // [ns][s2_count]
 };
 
 namespace {
@@ -1098,6 +1104,50 @@ int ecg_record(cep_tissue *t) {
                                                                 t->ecg_rec + (int64_t)t->ecg_n * t->n_el);
   FEM_CUDA(cudaGetLastError());
   ++t->ecg_n;
+  return CEP_OK;
+}
+
+// The protocol trigger of one tissue before its ionic step at time t
+// (Cheart::apply_s2 / apply_ectopic, heart.cpp:452-501, evaluated only in
+// the last S1 pace, heart.cpp:322-323).
+__global__ void proto_kernel(CepProto *p, const double *v, double t, double bcl, int n_pace) {
+  p->reset_now = 0;
+  if ((int)(t / bcl) != n_pace - 1) return;
+  const double vt = v[p->target];
+  if (vt > p->thr) p->depol = 1;
+  if (p->depol && vt < p->thr) p->repol = 1;
+  if (p->repol && !p->fired) {
+    p->fired = 1;
+    p->t_fire = t;
+    if (p->kind == CEP_S2_RESET) p->reset_now = 1;
+    if (p->kind == CEP_S2_ECTOPIC) p->ecto_on = 1;
+  }
+  if (p->kind == CEP_S2_ECTOPIC && p->fired && t - p->t_fire > p->dur) p->ecto_on = 0;
+}
+
+// S2: the region back to its snapshot, in the step the protocol fired.
+__global__ void s2_reset_kernel(const CepProto *p, double *y, int64_t ld, int ns, const int *nodes, int count,
+                                const double *snap) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count || !p->reset_now) return;
+  const int64_t i = nodes[k];
+  for (int s = 0; s < ns; ++s) y[(int64_t)s * ld + i] = snap[(int64_t)s * count + k];
+}
+
+int tissue_pre_step(cep_tissue *t) {
+  if (t->proto_kind == CEP_S2_NONE) return CEP_OK;
+  proto_kernel<<<1, 1, 0, t->stream>>>(t->proto, cep_internal_batch_v(t->cells), t->t, t->bcl, t->n_pace);
+  if (t->proto_kind == CEP_S2_RESET && t->s2_count > 0) {
+    int n = 0, ns = 0;
+    cep_batch_size(t->cells, &n, &ns);
+    long ld = 0;
+    void *dev = nullptr;
+    int rc = cep_batch_device_states(t->cells, &dev, &ld);
+    if (rc) return rc;
+    s2_reset_kernel<<<(t->s2_count + 255) / 256, 256, 0, t->stream>>>(t->proto, static_cast<double *>(dev), ld,
+                                                                       t->ns, t->s2_nodes, t->s2_count, t->s2_snap);
+  }
+  FEM_CUDA(cudaGetLastError());
   return CEP_OK;
 }
 
@@ -1524,7 +1574,9 @@ int cep_tissue_group_run(cep_tissue_group_t g, long n_steps) {
       if ((rc = group_event(g))) return rc;
     }
     for (cep_tissue_t t : g->ts) {
-      rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
+      if ((rc = tissue_pre_step(t))) return rc;
+      rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace, t->proto,
+                                          t->mask2);
       if (rc) return rc;
     }
     if (g->timing && (rc = group_event(g))) return rc;
@@ -1595,6 +1647,10 @@ int cep_tissue_destroy(cep_tissue_t t) {
   cudaFree(t->el);
   cudaFree(t->ecg_part);
   cudaFree(t->ecg_rec);
+  cudaFree(t->proto);
+  cudaFree(t->mask2);
+  cudaFree(t->s2_nodes);
+  cudaFree(t->s2_snap);
   delete t;
   return CEP_OK;
 }
@@ -1623,7 +1679,10 @@ int cep_tissue_run(cep_tissue_t t, long n_steps) {
   if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");
   double *v = cep_internal_batch_v(t->cells);
   for (long s = 0; s < n_steps; ++s) {
-    int rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace);
+    int rc = tissue_pre_step(t);
+    if (rc) return rc;
+    rc = cep_internal_batch_tissue_step(t->cells, t->mask, t->t, t->bcl, t->t_crt, t->dur, t->n_pace, t->proto,
+                                        t->mask2);
     if (rc) return rc;
     t->t += t->dt;
     ++t->steps;
@@ -1660,6 +1719,71 @@ int cep_tissue_set_electrodes(cep_tissue_t t, int n_el, const double *xyz, long 
   t->n_el = n_el;
   t->ecg_every = every;
   t->ecg_max = max_records;
+  return CEP_OK;
+}
+
+int cep_tissue_set_s2(cep_tissue_t t, int kind, int target_node, double vm_threshold, const unsigned char *region,
+                      double ectopic_dur) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (kind != CEP_S2_NONE && kind != CEP_S2_RESET && kind != CEP_S2_ECTOPIC)
+    return fail_msg(CEP_ERR_ARG, "unknown protocol %d", kind);
+  if (kind != CEP_S2_NONE && (!region || target_node < 0 || target_node >= t->n || !std::isfinite(vm_threshold)))
+    return fail_msg(CEP_ERR_ARG, "protocol needs a region and a target node in 0..%d", t->n - 1);
+  if (kind == CEP_S2_ECTOPIC && !(ectopic_dur >= 0)) return fail_msg(CEP_ERR_ARG, "ectopic_dur must be >= 0");
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  cudaFree(t->proto);
+  cudaFree(t->mask2);
+  cudaFree(t->s2_nodes);
+  cudaFree(t->s2_snap);
+  t->proto = nullptr;
+  t->mask2 = nullptr;
+  t->s2_nodes = nullptr;
+  t->s2_snap = nullptr;
+  t->s2_count = 0;
+  t->proto_kind = CEP_S2_NONE;
+  if (kind == CEP_S2_NONE) return CEP_OK;
+  CepProto p{};
+  p.kind = kind;
+  p.target = target_node;
+  p.thr = vm_threshold;
+  p.dur = ectopic_dur;
+  std::vector<int> nodes;
+  for (int i = 0; i < t->n; ++i)
+    if (region[i]) nodes.push_back(i);
+  int n = 0, ns = 0;
+  int rc;
+  if ((rc = cep_batch_size(t->cells, &n, &ns))) return rc;
+  bool ok = cudaMalloc((void **)&t->proto, sizeof(CepProto)) == cudaSuccess;
+  if (ok && kind == CEP_S2_ECTOPIC) {
+    ok = cudaMalloc((void **)&t->mask2, (size_t)t->n) == cudaSuccess &&
+         cudaMemcpy(t->mask2, region, (size_t)t->n, cudaMemcpyHostToDevice) == cudaSuccess;
+  }
+  if (ok && kind == CEP_S2_RESET && !nodes.empty()) {
+    // snapshot of the region's states now (the batch's SoA rows)
+    std::vector<double> all((size_t)ns * n), snap((size_t)ns * nodes.size());
+    if ((rc = cep_batch_get_states(t->cells, all.data(), CEP_LAYOUT_SOA))) return rc;
+    for (int s = 0; s < ns; ++s)
+      for (size_t k = 0; k < nodes.size(); ++k) snap[(size_t)s * nodes.size() + k] = all[(size_t)s * n + nodes[k]];
+    ok = cudaMalloc((void **)&t->s2_nodes, sizeof(int) * nodes.size()) == cudaSuccess &&
+         cudaMalloc((void **)&t->s2_snap, sizeof(double) * snap.size()) == cudaSuccess &&
+         cudaMemcpy(t->s2_nodes, nodes.data(), sizeof(int) * nodes.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(t->s2_snap, snap.data(), sizeof(double) * snap.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    t->s2_count = (int)nodes.size();
+    t->ns = ns;
+  }
+  if (!ok || cudaMemcpy(t->proto, &p, sizeof(CepProto), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(t->proto);
+    cudaFree(t->mask2);
+    cudaFree(t->s2_nodes);
+    cudaFree(t->s2_snap);
+    t->proto = nullptr;
+    t->mask2 = nullptr;
+    t->s2_nodes = nullptr;
+    t->s2_snap = nullptr;
+    t->s2_count = 0;
+    return fail_msg(CEP_ERR_OOM, "S2 protocol buffers");
+  }
+  t->proto_kind = kind;
   return CEP_OK;
 }
 

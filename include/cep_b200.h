@@ -381,6 +381,22 @@ int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, 
 int cep_tissue_set_electrodes(cep_tissue_t t, int n_el, const double *xyz, long every, long max_records);
 /* Copy the records so far (phi[n_records][n_el]; phi may be NULL). */
 int cep_tissue_get_ecg(cep_tissue_t t, double *phi, long *n_records);
+/* S1-S2 protocols of the reference (Cheart::apply_s2 / apply_ectopic,
+ * heart.cpp:452-501, armed at heart.cpp:322-323), evaluated on the device
+ * before every ionic step of the last S1 pace ((int)(t/bcl) == n_pace - 1 of
+ * cep_tissue_set_stimulus): once the monitored node has risen above
+ * vm_threshold and fallen back below it, the protocol fires once and the S1
+ * stimulus stays off. CEP_S2_RESET (the reference uses -45 mV) sets every
+ * node of region[n] back to the states it had when this call was made (call
+ * it before running: the initial states); CEP_S2_ECTOPIC (-75 mV) drives
+ * the region with the S1 stimulus current for ectopic_dur ms (isEctopic),
+ * switched off, as in the reference, only while still in that pace.
+ * CEP_S2_NONE disarms. */
+#define CEP_S2_NONE 0
+#define CEP_S2_RESET 1
+#define CEP_S2_ECTOPIC 2
+int cep_tissue_set_s2(cep_tissue_t t, int kind, int target_node, double vm_threshold, const unsigned char *region,
+                      double ectopic_dur);
 
 /* A group of tissues stepped together: each keeps its own cells, operator,
  * stimulus and solver state, but their diffusion solves share one

@@ -108,6 +108,9 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_int, _dp, _dp, _ip, ctypes.c_double, _dp]
         L.cepo_tissue_run.restype = ctypes.c_long
+        L.cepo_tissue_run_s2.argtypes = L.cepo_tissue_run.argtypes + [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                                      ctypes.POINTER(ctypes.c_uint8), ctypes.c_double]
+        L.cepo_tissue_run_s2.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -322,8 +325,10 @@ def pcg(rp, ci, a_val, b, rtol: float, max_iter: int = 10000, precond_norm: bool
 
 def tissue_run(model: str, dim: int, nx: int, ny: int, nz: int, h: float, D, dt: float, n_steps: int, s1_mask,
                bcl: float, t_crt: float, dur: float, n_pace: int, conc: float = 0.0, hill=None,
-               rtol: float = 1e-5, precond_norm: bool = True, celltype=None, act_thr: float = -30.0):
-    """Godunov-split tissue run: (final V, CG iterations per step, activation times)."""
+               rtol: float = 1e-5, precond_norm: bool = True, celltype=None, act_thr: float = -30.0,
+               s2_kind: int = 0, s2_target: int = 0, s2_thr: float = -45.0, s2_region=None, ecto_dur: float = 0.0):
+    """Godunov-split tissue run: (final V, CG iterations per step, activation times); s2_kind 1/2 adds the
+    S1-S2 reset / ectopic protocol on s2_region monitored at node s2_target."""
     if dim == 2:
         nz = 1
     d = element_D(dim, nx, ny, nz, D)
@@ -334,9 +339,11 @@ def tissue_run(model: str, dim: int, nx: int, ny: int, nz: int, h: float, D, dt:
     v = np.zeros(n)
     its = np.zeros(n_steps, np.int32)
     tact = np.zeros(n)
-    lib().cepo_tissue_run(MODELS[model], dim, nx, ny, nz, h, _ptr(d), d.shape[1], dt, n_steps,
-                          m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt, dur, n_pace, conc,
-                          _ptr(hh) if hh is not None else None, 0 if hh is None else len(hh), rtol,
-                          int(precond_norm), _ptr(ct) if ct is not None else None, _ptr(v), _iptr(its), act_thr,
-                          _ptr(tact))
+    reg = np.ascontiguousarray(np.zeros(n, np.uint8) if s2_region is None else np.asarray(s2_region, np.uint8).ravel())
+    lib().cepo_tissue_run_s2(MODELS[model], dim, nx, ny, nz, h, _ptr(d), d.shape[1], dt, n_steps,
+                             m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt, dur, n_pace, conc,
+                             _ptr(hh) if hh is not None else None, 0 if hh is None else len(hh), rtol,
+                             int(precond_norm), _ptr(ct) if ct is not None else None, _ptr(v), _iptr(its), act_thr,
+                             _ptr(tact), int(s2_kind), int(s2_target), float(s2_thr),
+                             reg.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), float(ecto_dur))
     return v, its, tact

@@ -118,6 +118,12 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                      double conc, const double *hill, int n_hill, double rtol, int precond_norm,
                      const double *celltype, double *V, int *iters_out, double act_thr, double *t_act);
+/* The same with the S1-S2 reset (s2_kind 1) or ectopic (2) protocol. */
+long cepo_tissue_run_s2(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+                        long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                        double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                        const double *celltype, double *V, int *iters_out, double act_thr, double *t_act,
+                        int s2_kind, int target, double thr, const unsigned char *region, double ecto_dur);
 
 #ifdef __cplusplus
 }

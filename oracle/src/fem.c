@@ -306,6 +306,22 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                      double conc, const double *hill, int n_hill, double rtol, int precond_norm,
                      const double *celltype, double *V, int *iters_out, double act_thr, double *t_act) {
+  return cepo_tissue_run_s2(model, dim, nx, ny, nz, h, D, n_d, dt, n_steps, s1, bcl, t_crt, dur, n_pace, conc, hill,
+                            n_hill, rtol, precond_norm, celltype, V, iters_out, act_thr, t_act, 0, 0, 0.0, NULL, 0.0);
+}
+
+/* The same with an S1-S2 protocol (Cheart::apply_s2 / apply_ectopic,
+ * heart.cpp:452-501, called before the node loop of every step of the last
+ * S1 pace, heart.cpp:322-323): s2_kind 1 resets the region's nodes to their
+ * initial states once node `target` has gone above thr and back below it;
+ * s2_kind 2 instead drives the region with the S1 current (isEctopic) for
+ * ecto_dur ms. After the protocol fires the S1 stimulus stays off (the
+ * "square" mesh branch runs only while idid is false, heart.cpp:300). */
+long cepo_tissue_run_s2(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+                        long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                        double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                        const double *celltype, double *V, int *iters_out, double act_thr, double *t_act,
+                        int s2_kind, int target, double thr, const unsigned char *region, double ecto_dur) {
   if (dim == 2) nz = 1;
   const int n = nx * ny * nz;
   const long nnz = cepo_fem_nnz(dim, nx, ny, nz);
@@ -325,11 +341,32 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
   long total = 0;
   if (t_act)
     for (int i = 0; i < n; ++i) t_act[i] = -1.0;
+  double *y0 = NULL;  /* initial states, for the S2 reset */
+  if (s2_kind == 1) {
+    y0 = malloc(sizeof(double) * (size_t)n * CEPO_MAX_STATES);
+    memcpy(y0, y, sizeof(double) * (size_t)n * CEPO_MAX_STATES);
+  }
+  int depol = 0, repol = 0, fired = 0, ecto = 0;
+  double t_fire = 0.0;
   for (long st = 0; st < n_steps; ++st) {
+    if (s2_kind && (int)(t / bcl) == n_pace - 1) {
+      const double vt = y[(size_t)target * CEPO_MAX_STATES];
+      if (vt > thr) depol = 1;
+      if (depol && vt < thr) repol = 1;
+      if (repol && !fired) {
+        fired = 1;
+        t_fire = t;
+        if (s2_kind == 1)
+          for (int i = 0; i < n; ++i)
+            if (region[i]) memcpy(y + (size_t)i * CEPO_MAX_STATES, y0 + (size_t)i * CEPO_MAX_STATES, sizeof(double) * ns);
+        if (s2_kind == 2) ecto = 1;
+      }
+      if (s2_kind == 2 && fired && t - t_fire > ecto_dur) ecto = 0;
+    }
     const int iia = (int)(t / bcl);
-    const int on = iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt;
+    const int on = !fired && iia < n_pace && t < (double)iia * bcl + dur + t_crt && t > (double)iia * bcl + t_crt;
     for (int i = 0; i < n; ++i) {
-      cells[i].is_s1 = on && s1[i];
+      cells[i].is_s1 = (on && s1[i]) || (ecto && region[i]);
       cepo_step(&cells[i], t, dt, y + (size_t)i * CEPO_MAX_STATES, NULL);
       vs[i] = y[(size_t)i * CEPO_MAX_STATES];
     }
@@ -347,6 +384,6 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
   }
   (void)ns;
   for (int i = 0; i < n; ++i) V[i] = y[(size_t)i * CEPO_MAX_STATES];
-  free(rp); free(ci); free(av); free(bv); free(cells); free(y); free(vs); free(b);
+  free(rp); free(ci); free(av); free(bv); free(cells); free(y); free(vs); free(b); free(y0);
   return total;
 }

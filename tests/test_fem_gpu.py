@@ -421,3 +421,51 @@ def test_pseudo_ecg_cadence_and_limits(cep, gpu, oracle):
     with pytest.raises(cep.CepError) as e:
         t2.set_electrodes(ELECTRODES[:1])
     assert e.value.code == cep.ERR_UNSUPPORTED
+
+
+def _s2_sheet(cep, kind, region, target, thr, ecto_dur):
+    nx = ny = 16
+    n = nx * ny
+    cells = cep.Batch("tt2006", n, "fp64")
+    cells.init()
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(1e-10)
+    t = cep.Tissue(cells, fem, 0.01)
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:, :2] = 1
+    t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 1)
+    if kind:
+        t.set_s2(kind, target, thr, region, ecto_dur)
+    return t, mask
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,thr,steps", [(1, -45.0, 28500), (2, -75.0, 30500)])
+def test_s1s2_protocols_match_oracle(cep, gpu, oracle, kind, thr, steps):
+    """S1-S2 reset (kind 1) and ectopic (kind 2) protocols, triggered on the
+    device by a monitored node's depolarisation and repolarisation in the
+    last S1 pace: FP64 V within 1e-6 mV and activation times equal to the
+    oracle's tissue loop, and the protocol changed the result."""
+    nx = ny = 16
+    region = np.zeros((ny, nx), np.uint8)
+    region[:6, 8:] = 1
+    target = 8 + nx * 8
+    t, mask = _s2_sheet(cep, kind, region.ravel(), target, thr, 2.0)
+    t.run(steps)
+    vo, _, tao = oracle.tissue_run("tt2006", 2, nx, ny, 1, 0.025, 0.0013, 0.01, steps, mask.ravel(), 1000.0, 0.0,
+                                   1.0, 1, rtol=1e-10, s2_kind=kind, s2_target=target, s2_thr=thr,
+                                   s2_region=region.ravel(), ecto_dur=2.0)
+    assert np.abs(t.v() - vo).max() <= 1e-6
+    assert np.array_equal(t.activation(), tao)
+    plain, _ = _s2_sheet(cep, 0, None, 0, 0.0, 0.0)
+    plain.run(steps)
+    assert np.abs(plain.v() - t.v())[region.ravel() == 1].max() > 10.0  # shortly after the protocol fired
+
+
+@pytest.mark.gpu
+def test_s1s2_argument_checks(cep, gpu):
+    t, _ = _s2_sheet(cep, 0, None, 0, 0.0, 0.0)
+    with pytest.raises(cep.CepError):
+        t.set_s2(7, 0, -45.0, np.ones(256, np.uint8))
+    with pytest.raises(cep.CepError):
+        t.set_s2(cep.S2_RESET, 256, -45.0, np.ones(256, np.uint8))
+    t.set_s2(cep.S2_NONE, 0, 0.0)
