@@ -138,6 +138,8 @@ _SIGS = {
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "cep_fem_create_csr": (ctypes.c_int, [ctypes.c_int, _ip, _ip, _dp, _dp, ctypes.c_double, ctypes.c_int,
                                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_fem_create_tet": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "cep_fem_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_fem_info": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.POINTER(ctypes.c_long), _ip, _ip]),
     "cep_fem_set_format": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -401,6 +403,19 @@ class Fem:
         bv = np.ascontiguousarray(b_val, np.float64)
         hnd = ctypes.c_void_p()
         _check(lib().cep_fem_create_csr(len(rp) - 1, _iptr(rp), _iptr(ci), _dptr(av), _dptr(bv), dt, fmt, stream,
+                                        ctypes.byref(hnd)))
+        return cls(hnd)
+
+    @classmethod
+    def tet(cls, xyz, conn, D, dt: float, fmt: int = FEM_ELL, stream: int | None = None) -> "Fem":
+        """Operator of a P1 tetrahedral mesh: xyz [n, 3] cm, conn [e, 4] 0-based,
+        D scalar, [e] or [e, 6] tensors; assembled on the device."""
+        x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+        c = np.ascontiguousarray(np.asarray(conn, np.int32).reshape(-1, 4))
+        d = np.asarray(D, np.float64)
+        d = np.ascontiguousarray(np.full((len(c), 1), float(d)) if d.ndim == 0 else d.reshape(len(c), -1))
+        hnd = ctypes.c_void_p()
+        _check(lib().cep_fem_create_tet(len(x), _dptr(x), len(c), _iptr(c), _dptr(d), d.shape[1], dt, fmt, stream,
                                         ctypes.byref(hnd)))
         return cls(hnd)
 

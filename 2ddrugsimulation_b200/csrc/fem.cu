@@ -53,6 +53,11 @@ extern "C" int cep_internal_fem_assemble_grid(int dim, int nx, int ny, int nz, d
                                               int width, int64_t ld, int *d_ecol, double *d_ea, double *d_eb,
                                               double *d_dinv, void *stream);
 
+extern "C" int cep_internal_fem_assemble_tet(int n_nodes, const double *d_xyz, const int *d_conn, const double *d_D,
+                                             int n_d, double dt, const int *d_inc_ptr, const int *d_inc,
+                                             const int *d_rp, const int *d_col, double *d_a, double *d_b,
+                                             void *stream);
+
 namespace {
 
 #define FEM_CUDA(call)                                                                                   \
@@ -1227,6 +1232,78 @@ int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, co
   }
   *out = f;
   return CEP_OK;
+}
+
+int cep_fem_create_tet(int n_nodes, const double *xyz, int n_elem, const int *conn, const double *D, int n_d,
+                       double dt, int format, void *stream, cep_fem_t *out) {
+  if (!out || !xyz || !conn || !D) return fail_msg(CEP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (n_nodes < 4 || n_elem < 1) return fail_msg(CEP_ERR_ARG, "mesh needs >= 4 nodes and >= 1 element");
+  if (n_d != 1 && n_d != 6) return fail_msg(CEP_ERR_ARG, "n_d must be 1 (scalar) or 6 (tensor)");
+  if (!(dt > 0)) return fail_msg(CEP_ERR_ARG, "dt must be positive");
+  if (format == CEP_FEM_STENCIL || format == CEP_FEM_CLASSED)
+    return fail_msg(CEP_ERR_ARG, "grid formats need a structured grid");
+  for (long k = 0; k < 4L * n_elem; ++k)
+    if (conn[k] < 0 || conn[k] >= n_nodes) return fail_msg(CEP_ERR_ARG, "element node %d out of range", conn[k]);
+  // node -> (element, local node) in ascending element order, and each row's
+  // columns: the nodes sharing an element with it, ascending
+  std::vector<int> inc_ptr(n_nodes + 1, 0), fill(n_nodes, 0);
+  for (long k = 0; k < 4L * n_elem; ++k) inc_ptr[conn[k] + 1]++;
+  for (int i = 0; i < n_nodes; ++i) inc_ptr[i + 1] += inc_ptr[i];
+  std::vector<int> inc(2 * (size_t)inc_ptr[n_nodes]);
+  for (int e = 0; e < n_elem; ++e)
+    for (int k = 0; k < 4; ++k) {
+      const int i = conn[4 * (size_t)e + k], p = inc_ptr[i] + fill[i]++;
+      inc[2 * (size_t)p] = e;
+      inc[2 * (size_t)p + 1] = k;
+    }
+  std::vector<int> rp(n_nodes + 1, 0), col, nb;
+  for (int i = 0; i < n_nodes; ++i) {
+    nb.clear();
+    for (int p = inc_ptr[i]; p < inc_ptr[i + 1]; ++p)
+      for (int k = 0; k < 4; ++k) nb.push_back(conn[4 * (size_t)inc[2 * (size_t)p] + k]);
+    std::sort(nb.begin(), nb.end());
+    nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+    col.insert(col.end(), nb.begin(), nb.end());
+    rp[i + 1] = (int)col.size();
+  }
+  const size_t nnz = col.size();
+  cudaStream_t st = (cudaStream_t)stream;
+  double *d_xyz = nullptr, *d_D = nullptr, *d_a = nullptr, *d_b = nullptr;
+  int *d_conn = nullptr, *d_incp = nullptr, *d_inc = nullptr, *d_rp = nullptr, *d_col = nullptr;
+  auto release = [&] {
+    for (void *q : {(void *)d_xyz, (void *)d_D, (void *)d_a, (void *)d_b, (void *)d_conn, (void *)d_incp,
+                    (void *)d_inc, (void *)d_rp, (void *)d_col})
+      cudaFree(q);
+  };
+  bool ok = cudaMalloc(&d_xyz, sizeof(double) * 3 * (size_t)n_nodes) == cudaSuccess &&
+            cudaMalloc(&d_D, sizeof(double) * (size_t)n_d * n_elem) == cudaSuccess &&
+            cudaMalloc(&d_a, sizeof(double) * nnz) == cudaSuccess && cudaMalloc(&d_b, sizeof(double) * nnz) == cudaSuccess &&
+            cudaMalloc(&d_conn, sizeof(int) * 4 * (size_t)n_elem) == cudaSuccess &&
+            cudaMalloc(&d_incp, sizeof(int) * inc_ptr.size()) == cudaSuccess &&
+            cudaMalloc(&d_inc, sizeof(int) * inc.size()) == cudaSuccess &&
+            cudaMalloc(&d_rp, sizeof(int) * rp.size()) == cudaSuccess && cudaMalloc(&d_col, sizeof(int) * nnz) == cudaSuccess;
+  if (!ok) {
+    release();
+    return fail_msg(CEP_ERR_OOM, "tetrahedral assembly buffers");
+  }
+  cudaError_t e = cudaMemcpyAsync(d_xyz, xyz, sizeof(double) * 3 * (size_t)n_nodes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_D, D, sizeof(double) * (size_t)n_d * n_elem, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_conn, conn, sizeof(int) * 4 * (size_t)n_elem, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_incp, inc_ptr.data(), sizeof(int) * inc_ptr.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_inc, inc.data(), sizeof(int) * inc.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_rp, rp.data(), sizeof(int) * rp.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_col, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && cep_internal_fem_assemble_tet(n_nodes, d_xyz, d_conn, d_D, n_d, dt, d_incp, d_inc, d_rp, d_col,
+                                                        d_a, d_b, st))
+    e = cudaGetLastError();
+  std::vector<double> a(nnz), b(nnz);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(a.data(), d_a, sizeof(double) * nnz, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b.data(), d_b, sizeof(double) * nnz, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return fail_msg(CEP_ERR_CUDA, "tetrahedral assembly failed: %s", cudaGetErrorString(e));
+  return cep_fem_create_csr(n_nodes, rp.data(), col.data(), a.data(), b.data(), dt, format, stream, out);
 }
 
 int cep_fem_create_csr(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b_val,

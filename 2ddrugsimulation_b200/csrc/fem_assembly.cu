@@ -196,3 +196,104 @@ extern "C" int cep_internal_fem_assemble_grid(int dim, int nx, int ny, int nz, d
   cep::fem::assemble_grid_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(g);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+
+// ------------------------------------------------ P1 tetrahedral meshes
+// Unstructured meshes of linear tetrahedra (the reference's "tet" meshes:
+// Gauss points fem.cpp:209-229, shape functions fem.cpp:342-373, element
+// matrices fem.cpp:628-661 with unit Gauss weights). One thread per node
+// (row): its incident elements in ascending order, each adding its row of
+// the element matrices to the row's sorted columns, local nodes in order.
+namespace cep {
+namespace fem {
+
+__device__ void tet_row(const double x[4][3], const double *D, int n_d, double dt, int la, double *arow,
+                        double *brow) {
+  const double aaa = (5. - sqrt(5.)) / 20., bbb = (5. + 3. * sqrt(5.)) / 20.;
+  const double gp[4][3] = {{aaa, aaa, aaa}, {aaa, aaa, bbb}, {aaa, bbb, aaa}, {bbb, aaa, aaa}};
+  const double dS[4][3] = {{-1., -1., -1.}, {1., 0., 0.}, {0., 1., 0.}, {0., 0., 1.}};
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.;
+      for (int a = 0; a < 4; ++a) s += dS[a][r] * x[a][c];
+      J[r][c] = s;
+    }
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double xJ[3][3];
+  xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+  xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
+  xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+  xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
+  xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+  xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
+  xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+  xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
+  xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  double dX[4][3];
+  for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.;
+      for (int j = 0; j < 3; ++j) s += dS[a][j] * xJ[i][j];
+      dX[a][i] = s;
+    }
+  double Dm[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+  if (n_d == 1) {
+    Dm[0][0] = Dm[1][1] = Dm[2][2] = D[0];
+  } else {
+    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
+    Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
+  }
+  for (int k = 0; k < 4; ++k) {
+    double gdg = 0.;
+    for (int p = 0; p < 3; ++p)
+      for (int q = 0; q < 3; ++q) gdg += dX[la][p] * Dm[p][q] * dX[k][q];
+    double av = 0., bv = 0.;
+    for (int g = 0; g < 4; ++g) {
+      const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
+      const double phi[4] = {1. - s - t - z, s, t, z};
+      av += phi[la] * phi[k] * det / dt + gdg * det;
+      bv += phi[la] * phi[k] * det;
+    }
+    arow[k] = av;
+    brow[k] = bv;
+  }
+}
+
+__global__ void assemble_tet_kernel(int n_nodes, const double *xyz, const int *conn, const double *D, int n_d,
+                                    double dt, const int *inc_ptr, const int *inc, const int *rp, const int *col,
+                                    double *a, double *b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  const int r0 = rp[i], r1 = rp[i + 1];
+  for (int q = r0; q < r1; ++q) {
+    a[q] = 0.;
+    b[q] = 0.;
+  }
+  for (int p = inc_ptr[i]; p < inc_ptr[i + 1]; ++p) {
+    const int e = inc[2 * p], la = inc[2 * p + 1];
+    double x[4][3], ar[4], br[4];
+    for (int k = 0; k < 4; ++k)
+      for (int c = 0; c < 3; ++c) x[k][c] = xyz[3 * (int64_t)conn[4 * (int64_t)e + k] + c];
+    tet_row(x, D + (int64_t)e * n_d, n_d, dt, la, ar, br);
+    for (int k = 0; k < 4; ++k) {
+      const int j = conn[4 * (int64_t)e + k];
+      int q = r0;
+      while (q < r1 - 1 && col[q] != j) ++q;
+      a[q] += ar[k];
+      b[q] += br[k];
+    }
+  }
+}
+
+}  // namespace fem
+}  // namespace cep
+
+extern "C" int cep_internal_fem_assemble_tet(int n_nodes, const double *d_xyz, const int *d_conn, const double *d_D,
+                                             int n_d, double dt, const int *d_inc_ptr, const int *d_inc,
+                                             const int *d_rp, const int *d_col, double *d_a, double *d_b,
+                                             void *stream) {
+  cep::fem::assemble_tet_kernel<<<(n_nodes + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+      n_nodes, d_xyz, d_conn, d_D, n_d, dt, d_inc_ptr, d_inc, d_rp, d_col, d_a, d_b);
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -298,6 +298,15 @@ typedef struct cep_fem *cep_fem_t;
  * runs on the device. stream as in cep_batch_create. */
 int cep_fem_create_grid(int dim, int nx, int ny, int nz, double h, double dt, const double *D, int n_d,
                         int format, void *stream, cep_fem_t *out);
+/* An unstructured mesh of linear tetrahedra (the reference's "tet" meshes,
+ * mesh.cpp:59-186; Gauss points fem.cpp:209-229, shape functions
+ * fem.cpp:342-373, element matrices fem.cpp:628-661): xyz[n_nodes*3] (cm),
+ * conn[n_elem*4] (0-based nodes), D[n_elem*n_d] with n_d 1 (scalar, the
+ * reference's DE) or 6 (xx, xy, xz, yy, yz, zz). Assembled on the device,
+ * one thread per row summing its incident elements in ascending order; CSR
+ * or ELL (or CEP_FEM_AUTO between them). No pseudo-ECG on these operators. */
+int cep_fem_create_tet(int n_nodes, const double *xyz, int n_elem, const int *conn, const double *D, int n_d,
+                       double dt, int format, void *stream, cep_fem_t *out);
 /* An operator assembled by the caller (any mesh), CSR with sorted columns. */
 int cep_fem_create_csr(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b_val,
                        double dt, int format, void *stream, cep_fem_t *out);

@@ -111,6 +111,15 @@ def lib() -> ctypes.CDLL:
         L.cepo_tissue_run_s2.argtypes = L.cepo_tissue_run.argtypes + [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                                       ctypes.POINTER(ctypes.c_uint8), ctypes.c_double]
         L.cepo_tissue_run_s2.restype = ctypes.c_long
+        L.cepo_tissue_run_csr.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _dp, ctypes.c_double,
+                                          ctypes.c_long, ctypes.POINTER(ctypes.c_uint8), ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, _dp,
+                                          ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp, _ip,
+                                          ctypes.c_double, _dp]
+        L.cepo_tissue_run_csr.restype = ctypes.c_long
+        L.cepo_fem_assemble_tet.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _dp, ctypes.c_int, ctypes.c_double,
+                                            _ip, _ip, _dp, _dp]
+        L.cepo_fem_assemble_tet.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -283,6 +292,45 @@ def fem_assemble(dim: int, nx: int, ny: int, nz: int, h: float, dt: float, D):
     bv = np.zeros(nnz)
     lib().cepo_fem_assemble(dim, nx, ny, nz, h, dt, _ptr(d), d.shape[1], _iptr(rp), _iptr(ci), _ptr(av), _ptr(bv))
     return rp, ci, av, bv
+
+
+def fem_assemble_tet(xyz, conn, D, dt: float):
+    """CSR (row_ptr, col, A, B) of a P1 tetrahedral mesh (D: scalar, [n_elem] or [n_elem, 6])."""
+    x = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    c = np.ascontiguousarray(np.asarray(conn, np.int32).reshape(-1, 4))
+    d = np.asarray(D, np.float64)
+    d = np.ascontiguousarray(np.full((len(c), 1), float(d)) if d.ndim == 0 else d.reshape(len(c), -1))
+    n = len(x)
+    rp = np.zeros(n + 1, np.int32)
+    nnz = lib().cepo_fem_assemble_tet(n, _ptr(x), len(c), _iptr(c), _ptr(d), d.shape[1], dt, _iptr(rp), None, None,
+                                      None)
+    ci = np.zeros(nnz, np.int32)
+    av = np.zeros(nnz)
+    bv = np.zeros(nnz)
+    lib().cepo_fem_assemble_tet(n, _ptr(x), len(c), _iptr(c), _ptr(d), d.shape[1], dt, _iptr(rp), _iptr(ci), _ptr(av),
+                                _ptr(bv))
+    return rp, ci, av, bv
+
+
+def tissue_run_csr(model: str, rp, ci, a_val, b_val, dt: float, n_steps: int, s1_mask, bcl: float, t_crt: float,
+                   dur: float, n_pace: int, conc: float = 0.0, hill=None, rtol: float = 1e-5,
+                   precond_norm: bool = True, celltype=None, act_thr: float = -30.0):
+    """Godunov tissue run on a CSR operator: (final V, CG iterations per step, activation times)."""
+    n = len(rp) - 1
+    m = np.ascontiguousarray(s1_mask, np.uint8)
+    hh = None if hill is None else np.ascontiguousarray(hill, np.float64)
+    ct = None if celltype is None else np.ascontiguousarray(celltype, np.float64)
+    v = np.zeros(n)
+    its = np.zeros(n_steps, np.int32)
+    tact = np.zeros(n)
+    lib().cepo_tissue_run_csr(MODELS[model], n, _iptr(np.ascontiguousarray(rp, np.int32)),
+                              _iptr(np.ascontiguousarray(ci, np.int32)), _ptr(np.ascontiguousarray(a_val)),
+                              _ptr(np.ascontiguousarray(b_val)), dt, n_steps,
+                              m.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), bcl, t_crt, dur, n_pace, conc,
+                              _ptr(hh) if hh is not None else None, 0 if hh is None else len(hh), rtol,
+                              int(precond_norm), _ptr(ct) if ct is not None else None, _ptr(v), _iptr(its), act_thr,
+                              _ptr(tact))
+    return v, its, tact
 
 
 def pseudo_ecg(dim: int, nx: int, ny: int, nz: int, h: float, D, V, xyz) -> np.ndarray:

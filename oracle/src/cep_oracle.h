@@ -109,6 +109,16 @@ int cepo_pcg2(int n, const int *row_ptr, const int *col_idx, const double *a_val
               double rtol, int max_iter, int precond_norm, double *rel_res);
 /* Element matrices (nn x nn, row-major) of an axis-aligned element of edge h. */
 void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be);
+/* The Godunov tissue loop on a caller's CSR operator (any mesh). */
+long cepo_tissue_run_csr(int model, int n, const int *rp, const int *ci, const double *av, const double *bv, double dt,
+                         long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                         double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                         const double *celltype, double *V, int *iters_out, double act_thr, double *t_act);
+/* P1 tetrahedral mesh: one row of the element matrices and the CSR of the
+ * whole mesh (row_ptr[n_nodes+1]; col == NULL counts nnz only). */
+void cepo_tet_row(const double x[4][3], const double *D, int n_d, double dt, int la, double *arow, double *brow);
+long cepo_fem_assemble_tet(int n_nodes, const double *xyz, int n_elem, const int *conn, const double *D, int n_d,
+                           double dt, int *row_ptr, int *col, double *a, double *b);
 /* Pseudo-ECG at n_el electrodes xyz[3*k..] of a grid tissue's V
  * (Cheart::Radiate, heart.cpp:640-690). */
 void cepo_pseudo_ecg(int dim, int nx, int ny, int nz, double h, const double *D, int n_d, const double *V,

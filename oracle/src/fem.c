@@ -317,17 +317,11 @@ long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const
  * s2_kind 2 instead drives the region with the S1 current (isEctopic) for
  * ecto_dur ms. After the protocol fires the S1 stimulus stays off (the
  * "square" mesh branch runs only while idid is false, heart.cpp:300). */
-long cepo_tissue_run_s2(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+static long tissue_loop(int model, int n, const int *rp, const int *ci, const double *av, const double *bv, double dt,
                         long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                         double conc, const double *hill, int n_hill, double rtol, int precond_norm,
                         const double *celltype, double *V, int *iters_out, double act_thr, double *t_act,
                         int s2_kind, int target, double thr, const unsigned char *region, double ecto_dur) {
-  if (dim == 2) nz = 1;
-  const int n = nx * ny * nz;
-  const long nnz = cepo_fem_nnz(dim, nx, ny, nz);
-  int *rp = malloc(sizeof(int) * (n + 1)), *ci = malloc(sizeof(int) * nnz);
-  double *av = malloc(sizeof(double) * nnz), *bv = malloc(sizeof(double) * nnz);
-  cepo_fem_assemble(dim, nx, ny, nz, h, dt, D, n_d, rp, ci, av, bv);
   const int ns = cepo_n_states(model);
   cepo_cell *cells = malloc(sizeof(cepo_cell) * n);
   double *y = malloc(sizeof(double) * (size_t)n * CEPO_MAX_STATES);
@@ -384,6 +378,154 @@ long cepo_tissue_run_s2(int model, int dim, int nx, int ny, int nz, double h, co
   }
   (void)ns;
   for (int i = 0; i < n; ++i) V[i] = y[(size_t)i * CEPO_MAX_STATES];
-  free(rp); free(ci); free(av); free(bv); free(cells); free(y); free(vs); free(b); free(y0);
+  free(cells); free(y); free(vs); free(b); free(y0);
   return total;
+}
+
+long cepo_tissue_run_s2(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
+                        long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                        double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                        const double *celltype, double *V, int *iters_out, double act_thr, double *t_act,
+                        int s2_kind, int target, double thr, const unsigned char *region, double ecto_dur) {
+  if (dim == 2) nz = 1;
+  const int n = nx * ny * nz;
+  const long nnz = cepo_fem_nnz(dim, nx, ny, nz);
+  int *rp = malloc(sizeof(int) * (n + 1)), *ci = malloc(sizeof(int) * nnz);
+  double *av = malloc(sizeof(double) * nnz), *bv = malloc(sizeof(double) * nnz);
+  cepo_fem_assemble(dim, nx, ny, nz, h, dt, D, n_d, rp, ci, av, bv);
+  const long total = tissue_loop(model, n, rp, ci, av, bv, dt, n_steps, s1, bcl, t_crt, dur, n_pace, conc, hill,
+                                 n_hill, rtol, precond_norm, celltype, V, iters_out, act_thr, t_act, s2_kind, target,
+                                 thr, region, ecto_dur);
+  free(rp); free(ci); free(av); free(bv);
+  return total;
+}
+
+/* The Godunov tissue loop on a caller's CSR operator (any mesh). */
+long cepo_tissue_run_csr(int model, int n, const int *rp, const int *ci, const double *av, const double *bv, double dt,
+                         long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
+                         double conc, const double *hill, int n_hill, double rtol, int precond_norm,
+                         const double *celltype, double *V, int *iters_out, double act_thr, double *t_act) {
+  return tissue_loop(model, n, rp, ci, av, bv, dt, n_steps, s1, bcl, t_crt, dur, n_pace, conc, hill, n_hill, rtol,
+                     precond_norm, celltype, V, iters_out, act_thr, t_act, 0, 0, 0.0, NULL, 0.0);
+}
+
+/* ---- unstructured P1 tetrahedra (fem.cpp:209-229 Gauss points,
+ * 342-373 shape functions, 628-661 element matrices) ---- */
+
+/* Row la of the element matrices of tetrahedron x[4][3] (unit Gauss
+ * weights as the reference; D scalar (n_d 1) or xx,xy,xz,yy,yz,zz (6)).
+ * The expression order is shared with the device assembly. */
+void cepo_tet_row(const double x[4][3], const double *D, int n_d, double dt, int la, double *arow, double *brow) {
+  const double aaa = (5. - sqrt(5.)) / 20., bbb = (5. + 3. * sqrt(5.)) / 20.;
+  const double gp[4][3] = {{aaa, aaa, aaa}, {aaa, aaa, bbb}, {aaa, bbb, aaa}, {bbb, aaa, aaa}};
+  const double dS[4][3] = {{-1., -1., -1.}, {1., 0., 0.}, {0., 1., 0.}, {0., 0., 1.}};
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.;
+      for (int a = 0; a < 4; ++a) s += dS[a][r] * x[a][c];
+      J[r][c] = s;
+    }
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double xJ[3][3];
+  xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+  xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
+  xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+  xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
+  xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+  xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
+  xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+  xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
+  xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  double dX[4][3];
+  for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.;
+      for (int j = 0; j < 3; ++j) s += dS[a][j] * xJ[i][j];
+      dX[a][i] = s;
+    }
+  double Dm[3][3] = {{0}};
+  if (n_d == 1) {
+    Dm[0][0] = Dm[1][1] = Dm[2][2] = D[0];
+  } else {
+    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
+    Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
+  }
+  for (int k = 0; k < 4; ++k) {
+    double gdg = 0.;
+    for (int p = 0; p < 3; ++p)
+      for (int q = 0; q < 3; ++q) gdg += dX[la][p] * Dm[p][q] * dX[k][q];
+    double av = 0., bv = 0.;
+    for (int g = 0; g < 4; ++g) {
+      const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
+      const double phi[4] = {1. - s - t - z, s, t, z};
+      av += phi[la] * phi[k] * det / dt + gdg * det;
+      bv += phi[la] * phi[k] * det;
+    }
+    arow[k] = av;
+    brow[k] = bv;
+  }
+}
+
+/* CSR of a tetrahedral mesh: columns of row i = the nodes sharing an element
+ * with i, ascending; each row sums its incident elements in ascending
+ * element order, local nodes in order. row_ptr must hold n_nodes + 1
+ * entries; col/a/b the returned nnz (call with col == NULL to count). */
+long cepo_fem_assemble_tet(int n_nodes, const double *xyz, int n_elem, const int *conn, const double *D, int n_d,
+                           double dt, int *row_ptr, int *col, double *a, double *b) {
+  /* incidence, node -> (element, local) in ascending element order */
+  int *cnt = calloc((size_t)n_nodes + 1, sizeof(int));
+  for (long e = 0; e < n_elem; ++e)
+    for (int k = 0; k < 4; ++k) cnt[conn[4 * e + k] + 1]++;
+  for (int i = 0; i < n_nodes; ++i) cnt[i + 1] += cnt[i];
+  int *fill = calloc((size_t)n_nodes, sizeof(int));
+  int *inc = malloc(sizeof(int) * 2 * (size_t)cnt[n_nodes]);
+  for (long e = 0; e < n_elem; ++e)
+    for (int k = 0; k < 4; ++k) {
+      const int i = conn[4 * e + k];
+      const int p = cnt[i] + fill[i]++;
+      inc[2 * p] = (int)e;
+      inc[2 * p + 1] = k;
+    }
+  /* sparsity */
+  long nnz = 0;
+  int *nb = malloc(sizeof(int) * 64);
+  for (int i = 0; i < n_nodes; ++i) {
+    int m = 0;
+    for (int p = cnt[i]; p < cnt[i + 1]; ++p)
+      for (int k = 0; k < 4; ++k) {
+        const int j = conn[4 * inc[2 * p] + k];
+        int seen = 0;
+        for (int q = 0; q < m; ++q) seen |= nb[q] == j;
+        if (!seen) {
+          if (m % 64 == 0 && m) nb = realloc(nb, sizeof(int) * (size_t)(m + 64));
+          nb[m++] = j;
+        }
+      }
+    for (int u = 1; u < m; ++u)  /* insertion sort */
+      for (int v = u; v > 0 && nb[v - 1] > nb[v]; --v) { const int tmp = nb[v]; nb[v] = nb[v - 1]; nb[v - 1] = tmp; }
+    if (row_ptr) row_ptr[i] = (int)nnz;
+    if (col) {
+      for (int q = 0; q < m; ++q) { col[nnz + q] = nb[q]; a[nnz + q] = 0.; b[nnz + q] = 0.; }
+      for (int p = cnt[i]; p < cnt[i + 1]; ++p) {
+        const int e = inc[2 * p], la = inc[2 * p + 1];
+        double x[4][3], ar[4], br[4];
+        for (int k = 0; k < 4; ++k)
+          for (int c = 0; c < 3; ++c) x[k][c] = xyz[3 * (long)conn[4 * e + k] + c];
+        cepo_tet_row(x, D + (long)e * n_d, n_d, dt, la, ar, br);
+        for (int k = 0; k < 4; ++k) {
+          const int j = conn[4 * e + k];
+          int q = 0;
+          while (col[nnz + q] != j) ++q;
+          a[nnz + q] += ar[k];
+          b[nnz + q] += br[k];
+        }
+      }
+    }
+    nnz += m;
+  }
+  if (row_ptr) row_ptr[n_nodes] = (int)nnz;
+  free(cnt); free(fill); free(inc); free(nb);
+  return nnz;
 }

@@ -1,0 +1,106 @@
+"""Mesh files and unstructured P1 tetrahedra: the .inp reader/writer of the
+reference's format, the VTK writer, the oracle's tetrahedral element
+matrices against closed forms (CPU), and on the GPU the device assembly
+(bit for bit) and a tissue on a tetrahedral mesh against the oracle."""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+
+mesh = importlib.import_module("2ddrugsimulation_b200.mesh")
+
+
+def _volumes(m):
+    p = m.xyz[m.elements]
+    return np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0]) / 6.0
+
+
+def test_inp_round_trip(tmp_path):
+    m = mesh.box_tets(4, 3, 3, 0.025)
+    m.targets = (0, 5, 35)
+    for ct in (None, np.arange(len(m.xyz)) % 3):
+        m.celltype = ct
+        mesh.write_inp(tmp_path / "m.inp", m)
+        r = mesh.read_inp(tmp_path / "m.inp")
+        assert r.etype == "C3D4" and r.targets == m.targets
+        assert np.array_equal(r.xyz, m.xyz) and np.array_equal(r.elements, m.elements)
+        assert (r.celltype is None) == (ct is None)
+        if ct is not None:
+            assert np.array_equal(r.celltype, ct)
+
+
+def test_box_tets_tile_the_box():
+    m = mesh.box_tets(5, 4, 3, 0.1)
+    v = _volumes(m)
+    assert (v > 0).all() and np.isclose(v.sum(), 0.4 * 0.3 * 0.2)
+
+
+def test_vtk_writer(tmp_path):
+    m = mesh.box_tets(3, 3, 2, 0.1)
+    mesh.write_vtk(tmp_path / "v.vtk", m, {"Voltage": np.linspace(-85, 20, len(m.xyz))})
+    txt = (tmp_path / "v.vtk").read_text().splitlines()
+    assert txt[0].startswith("# vtk DataFile") and f"POINTS {len(m.xyz)} float" in txt
+    assert f"CELLS {len(m.elements)} {5 * len(m.elements)}" in txt and "SCALARS Voltage float" in txt
+
+
+def test_oracle_tet_element_closed_forms(oracle):
+    """Unit Gauss weights as the reference: B_e = 24 V (1 + delta_jk) / 20
+    (the consistent mass times 24), K_e = 24 V grad phi_j . D grad phi_k;
+    A = B/dt + K; symmetric; stiffness rows sum to 0."""
+    rng = np.random.default_rng(2)
+    x = np.array([[0, 0, 0], [0.03, 0.002, 0.001], [0.004, 0.025, 0.003], [0.002, 0.001, 0.028]]) + rng.normal(0, 1e-3, (4, 3))
+    D = np.array([2e-3, 3e-4, -1e-4, 1.2e-3, 2e-4, 8e-4])
+    dt = 0.01
+    rp, ci, a, b = oracle.fem_assemble_tet(x, [[0, 1, 2, 3]], D[None, :], dt)
+    A = np.zeros((4, 4))
+    B = np.zeros((4, 4))
+    for i in range(4):
+        for q in range(rp[i], rp[i + 1]):
+            A[i, ci[q]], B[i, ci[q]] = a[q], b[q]
+    V = np.dot(np.cross(x[1] - x[0], x[2] - x[0]), x[3] - x[0]) / 6.0
+    Bref = 24 * V * (np.ones((4, 4)) + np.eye(4)) / 20
+    T = np.vstack([np.ones(4), x.T])
+    G = np.linalg.inv(T)[:, 1:]  # rows: grad phi_j
+    Dm = np.array([[D[0], D[1], D[2]], [D[1], D[3], D[4]], [D[2], D[4], D[5]]])
+    Kref = 24 * V * G @ Dm @ G.T
+    assert np.allclose(B, Bref, rtol=1e-12, atol=0)
+    assert np.allclose(A - B / dt, Kref, rtol=1e-10, atol=1e-16)
+    assert np.allclose(A, A.T, rtol=1e-12, atol=1e-18)
+
+
+@pytest.mark.gpu
+def test_tet_assembly_bitwise(cep, gpu, oracle):
+    m = mesh.box_tets(6, 5, 4, 0.025)
+    rng = np.random.default_rng(4)
+    m.xyz = m.xyz + rng.uniform(-0.003, 0.003, m.xyz.shape)  # irregular, still positively oriented
+    D = np.zeros((len(m.elements), 6))
+    D[:, 0], D[:, 3], D[:, 5] = rng.uniform(5e-4, 2e-3, (3, len(m.elements)))
+    D[:, 1] = 1e-4 * rng.uniform(-1, 1, len(m.elements))
+    for d in (0.0013, D):
+        f = cep.Fem.tet(m.xyz, m.elements, d, 0.01, fmt=cep.FEM_CSR)
+        rp, ci, a, b = f.get_csr()
+        orp, oci, oa, ob = oracle.fem_assemble_tet(m.xyz, m.elements, d, 0.01)
+        assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+        assert np.array_equal(a, oa) and np.array_equal(b, ob)
+
+
+@pytest.mark.gpu
+def test_tissue_on_tet_mesh_matches_oracle(cep, gpu, oracle):
+    m = mesh.box_tets(10, 8, 4, 0.025)
+    n = len(m.xyz)
+    mask = (m.xyz[:, 0] < 0.03).astype(np.uint8)
+    cells = cep.Batch("tt2006", n, "fp64")
+    cells.init()
+    fem = cep.Fem.tet(m.xyz, m.elements, 0.0013, 0.01, fmt=cep.FEM_AUTO).set_solver(1e-10)
+    t = cep.Tissue(cells, fem, 0.01)
+    t.set_stimulus(mask, 1000.0, 0.0, 1.0, 1)
+    t.run(800)
+    rp, ci, a, b = oracle.fem_assemble_tet(m.xyz, m.elements, 0.0013, 0.01)
+    vo, _, tao = oracle.tissue_run_csr("tt2006", rp, ci, a, b, 0.01, 800, mask, 1000.0, 0.0, 1.0, 1, rtol=1e-10)
+    assert (tao > 0).any()
+    assert np.abs(t.v() - vo).max() <= 1e-6
+    assert np.array_equal(t.activation(), tao)
+    with pytest.raises(cep.CepError):
+        t.set_electrodes([[0.0, 0.0, 1.0]])  # no pseudo-ECG on unstructured operators
