@@ -26,7 +26,9 @@ INST_RUNNING, INST_DONE, INST_NONFINITE, INST_IDLE = 0, 1, 2, 3
 MODELS = {"ord2011": 0, "cipa2017": 1, "tt2006": 2, "tt2004": 3, "tomek2019": 4}
 N_STATES = {"ord2011": 41, "cipa2017": 49, "tt2006": 19, "tt2004": 17, "tomek2019": 43}
 PREC = {"fp64": 0, "mixed": 1}
-FLAG_DUTTA, FLAG_QUIRKS = 1, 2
+FLAG_DUTTA, FLAG_QUIRKS, FLAG_TT04_MCELL = 1, 2, 4
+CURRENTS = ("INa", "INaL", "Ito", "ICaL", "IKr", "IKs", "IK1")
+APDR_FIELDS = ("pace", "recal", "bcl", "apd90", "di", "t")
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
 HILL_WIDTH = 20
 
@@ -52,6 +54,11 @@ class TissueJob(ctypes.Structure):
                 ("dt", ctypes.c_double), ("duration", ctypes.c_double), ("conc", ctypes.c_double),
                 ("hill", ctypes.POINTER(ctypes.c_double)), ("bcl", ctypes.c_double), ("stim_nx", ctypes.c_int),
                 ("stim_ny", ctypes.c_int), ("rtol", ctypes.c_double)]
+
+
+class ApdrRecord(ctypes.Structure):
+    _fields_ = [("pace", ctypes.c_int32), ("recal", ctypes.c_int32), ("bcl", ctypes.c_double),
+                ("apd90", ctypes.c_double), ("di", ctypes.c_double), ("t", ctypes.c_double)]
 
 
 class JobTimes(ctypes.Structure):
@@ -107,6 +114,11 @@ _SIGS = {
                                            _dp]),
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
+    "cep_batch_restitution": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_long, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int)]),
+    "cep_batch_clamp": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, _dp]),
     "cep_batch_reserve_biomarkers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                     ctypes.c_double]),
     "cep_batch_init_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int,
@@ -252,7 +264,8 @@ class Batch:
     def __exit__(self, *exc):
         self.close()
 
-    def init(self, celltype=None, conc=None, hill=None, dutta: bool = False, quirks: bool = True) -> "Batch":
+    def init(self, celltype=None, conc=None, hill=None, dutta: bool = False, quirks: bool = True,
+             mcell: bool = False) -> "Batch":
         ct = None if celltype is None else np.ascontiguousarray(np.broadcast_to(celltype, (self.n,)), np.float64)
         cc = None if conc is None else np.ascontiguousarray(np.broadcast_to(conc, (self.n,)), np.float64)
         hh = None
@@ -263,7 +276,7 @@ class Batch:
                 hh = np.broadcast_to(hh, (self.n, hh.shape[0]))
             hh = np.ascontiguousarray(hh)
             stride = hh.shape[1]
-        flags = (FLAG_DUTTA if dutta else 0) | (FLAG_QUIRKS if quirks else 0)
+        flags = (FLAG_DUTTA if dutta else 0) | (FLAG_QUIRKS if quirks else 0) | (FLAG_TT04_MCELL if mcell else 0)
         _check(lib().cep_batch_init(self._h, _dptr(ct), _dptr(cc), _dptr(hh), stride, flags))
         return self
 
@@ -349,6 +362,51 @@ class Batch:
         cur = np.zeros((7, self.n))
         _check(lib().cep_batch_rates(self._h, t, _dptr(dv), _dptr(cur)))
         return dv, cur
+
+    def restitution(self, bcls, n_pace: int, dt: float, steps_per_launch: int = 20000) -> dict[str, np.ndarray]:
+        """Dynamic restitution (apdr_bench.cpp:103-232) of every instance: the
+        recorded paces as arrays [n, records] keyed by APDR_FIELDS."""
+        b = np.ascontiguousarray(bcls, np.float64)
+        m = restitution_records(b, n_pace, dt)
+        arr = (ApdrRecord * max(1, self.n * m))()
+        cnt = ctypes.c_int()
+        _check(lib().cep_batch_restitution(self._h, _dptr(b), len(b), int(n_pace), float(dt), int(steps_per_launch),
+                                           arr, m, ctypes.byref(cnt)))
+        assert cnt.value == m
+        raw = np.ctypeslib.as_array(arr)[: self.n * m].reshape(self.n, m)
+        return {f: np.array(raw[f]) for f in APDR_FIELDS}
+
+    def clamp(self, v, t0: float, dt: float, current: str | int) -> np.ndarray:
+        """Voltage-clamp replay (CEPPatch/benchpatch.cpp:83-100): V of every
+        instance forced to v[k] before step k; returns the chosen channel
+        current, [len(v), n]."""
+        idx = CURRENTS.index(current) if isinstance(current, str) else int(current)
+        vv = np.ascontiguousarray(v, np.float64)
+        out = np.zeros((len(vv), self.n))
+        _check(lib().cep_batch_clamp(self._h, _dptr(vv), len(vv), float(t0), float(dt), idx, _dptr(out)))
+        return out
+
+
+def restitution_records(bcls, n_pace: int, dt: float) -> int:
+    """Recorded paces per instance of a restitution run: per BCL, the pace
+    boundaries among iout = 1 .. (int)(n_pace*bcl/dt) + 1 minus the first two."""
+    m = 0
+    for bcl in np.asarray(bcls, np.float64):
+        steps, imax = int(float(bcl) / dt), int((n_pace * float(bcl)) / dt)
+        m += max(0, (imax + 1) // max(1, steps) - 2)
+    return m
+
+
+def apdr_bcls(bcl_init: float, bcl_end: float, bcl_decrement: float) -> list[float]:
+    """The BCL list of apdr_bench.cpp:103,229-230: from bcl_init while
+    bcl >= bcl_end, the decrement becoming 10 once bcl <= 300."""
+    out, bcl, dec = [], float(bcl_init), float(bcl_decrement)
+    while bcl >= bcl_end:
+        out.append(bcl)
+        if bcl <= 300.0:
+            dec = 10.0
+        bcl -= dec
+    return out
 
 
 def qinward(control: Biomarkers, drug: Biomarkers) -> float:

@@ -14,6 +14,7 @@
 // for n_steps steps; HBM is touched once per launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -180,7 +181,8 @@ struct Tt04Model {
   __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
                               const double *hill, unsigned flags) {
     (void)ct;
-    tt04::init_instance(par, s, ld, i, conc, hill, (flags & CEP_FLAG_QUIRKS) != 0);
+    tt04::init_instance(par, s, ld, i, conc, hill, (flags & CEP_FLAG_QUIRKS) != 0,
+                        (flags & CEP_FLAG_TT04_MCELL) != 0);
   }
   template <class G>
   __device__ static double cai_of(const Y<G> &y) { return y.Ca_i; }
@@ -503,6 +505,210 @@ __global__ void __launch_bounds__(128) tissue_kernel(TissueArgs a) {
   M::template store<G>(y, a.y, a.ld, i);
 }
 
+// Dynamic restitution (apdr_bench.cpp:103-232): one thread per instance, a
+// launch advances up to n_steps steps of the current BCL segment with the
+// per-pace APD90 tracker in registers. The tracker and the segment clock
+// persist between launches in rf/ri; the pace's Vm samples go to trace
+// ([S][ld], coalesced) for the recalibration search at a boundary whose
+// windowed peak stayed below 10 mV. The products and sums the reference
+// writes as one expression are rounded separately (__dmul_rn/__dadd_rn) so
+// no FMA contraction changes them.
+enum : int { RF_peak = 0, RF_valley, RF_repol, RF_tpeak, RF_tdepol, RF_trepol, RF_apd, RF_t, RF_tp0, kRF };
+enum : int { RI_repl = 0, RI_pace, RI_all, RI_iout, RI_nrec, RI_recal, RI_status, kRI };
+
+struct RestitArgs {
+  double *y;
+  const double *par;
+  int64_t ld;
+  int n;
+  double dt, bcl;
+  int S, imax, n_steps;
+  double *rf;      // [kRF][ld]
+  int *ri;         // [kRI][ld]
+  double *trace;   // [S][ld]
+  cep_apdr_record_t *rec;  // [n][max_rec]
+  int max_rec;
+};
+
+__global__ void restit_init_kernel(RestitArgs a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int64_t ld = a.ld;
+  const double v0 = a.y[i];
+  for (int k = 0; k < kRF; ++k) a.rf[k * ld + i] = 0.0;
+  for (int k = 0; k < kRI; ++k) a.ri[k * ld + i] = 0;
+  a.rf[RF_peak * ld + i] = v0;  // vm_valley = vm_peak = STATES[V] (:97)
+  a.rf[RF_valley * ld + i] = v0;
+}
+
+// Segment start (:111-130): the clock restarts, the tracker carries over.
+__global__ void restit_segment_kernel(RestitArgs a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int64_t ld = a.ld;
+  a.rf[RF_t * ld + i] = 0.0;
+  a.rf[RF_tp0 * ld + i] = 0.0;
+  a.rf[RF_tdepol * ld + i] = 0.0;
+  a.rf[RF_trepol * ld + i] = 0.0;
+  a.ri[RI_iout * ld + i] = 0;
+  a.ri[RI_pace * ld + i] = 0;
+}
+
+template <class M, class P>
+__global__ void __launch_bounds__(128) restit_kernel(RestitArgs a) {
+  using G = typename P::G;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int64_t ld = a.ld;
+  int st = a.ri[RI_status * ld + i];
+  int iout = a.ri[RI_iout * ld + i];
+  if (st != 0 || iout > a.imax) return;
+  typename M::template Y<G> y;
+  typename M::template Par<G> q;
+  M::template load<G>(y, a.y, ld, i);
+  M::template load_par<G>(q, a.par, ld, i);
+  double vm_peak = a.rf[RF_peak * ld + i], vm_valley = a.rf[RF_valley * ld + i];
+  double vm_repol = a.rf[RF_repol * ld + i], t_peak = a.rf[RF_tpeak * ld + i];
+  double t_depol = a.rf[RF_tdepol * ld + i], t_repol = a.rf[RF_trepol * ld + i];
+  double apd90 = a.rf[RF_apd * ld + i], t = a.rf[RF_t * ld + i], tp0 = a.rf[RF_tp0 * ld + i];
+  int repl = a.ri[RI_repl * ld + i], pace = a.ri[RI_pace * ld + i], all_pace = a.ri[RI_all * ld + i];
+  int n_rec = a.ri[RI_nrec * ld + i], recal = a.ri[RI_recal * ld + i];
+  const double stim_start = a.par[M::p_stim_start() * ld + i];
+  const double bcl = a.bcl, dt = a.dt;
+  const int S = a.S;
+  typename M::template Cur<G> c;
+  for (int k = 0; k < a.n_steps && iout <= a.imax; ++k) {
+    M::template step<P>(y, q, t, dt, -1, true, c);
+    ++iout;
+    t += dt;
+    const double V = y.V;
+    if (!isfinite(V)) {
+      st = CEP_INST_NONFINITE;
+      break;
+    }
+    const int j = iout - 1 - S * pace;  // sample index within the pace, in [0, S)
+    a.trace[(int64_t)j * ld + i] = V;
+    const double lo = __dadd_rn(__dmul_rn(bcl, (double)pace), stim_start);
+    if (lo + 4. < t && t < lo + 56.) {  // :149-157
+      if (vm_peak < V) {
+        vm_peak = V;
+        t_peak = t;
+      }
+    } else if (t > lo + 56.) {
+      vm_repol = __dsub_rn(vm_peak, __dmul_rn(0.9, __dsub_rn(vm_peak, vm_valley)));
+    }
+    if (t > lo + 56. && vm_repol >= V && V > vm_repol - 2) {  // :161-166
+      t_depol = lo;
+      t_repol = t;
+      apd90 = t_repol - t_depol;
+      repl = 1;
+    }
+    if (iout % S == 0) {  // pace boundary :169-213
+      if (vm_peak < 0 || (vm_peak >= 0 && vm_peak < 10)) {
+        repl = 0;
+        recal = 1;
+        double tt = tp0;
+        for (int jj = 0; jj < S; ++jj) {
+          tt += dt;
+          const double v = a.trace[(int64_t)jj * ld + i];
+          if (vm_peak < v) {
+            vm_peak = v;
+            vm_repol = __dsub_rn(vm_peak, __dmul_rn(0.9, __dsub_rn(vm_peak, vm_valley)));
+            t_peak = tt;
+          }
+        }
+        tt = tp0;
+        for (int jj = 0; jj < S; ++jj) {
+          tt += dt;
+          const double v = a.trace[(int64_t)jj * ld + i];
+          if (tt > t_peak && vm_repol >= v && v > vm_repol - 1) {
+            t_depol = lo;
+            t_repol = tt;
+            apd90 = t_repol - t_depol;
+            repl = 1;
+          }
+        }
+      }
+      if (!repl) {
+        t_depol = lo;
+        t_repol = t;
+        apd90 = t_repol - t_depol;
+      }
+      vm_valley = V;
+      vm_peak = -999;
+      vm_repol = 0;
+      ++pace;
+      ++all_pace;
+      repl = 0;
+      if (pace > 2) {
+        if (n_rec < a.max_rec) {
+          cep_apdr_record_t r;
+          r.pace = all_pace;
+          r.recal = recal;
+          r.bcl = bcl;
+          r.apd90 = apd90;
+          r.di = (t + stim_start) - t_repol;
+          r.t = t;
+          a.rec[i * a.max_rec + n_rec] = r;
+        }
+        ++n_rec;
+      }
+      recal = 0;
+      tp0 = t;
+    }
+  }
+  M::template store<G>(y, a.y, ld, i);
+  a.rf[RF_peak * ld + i] = vm_peak; a.rf[RF_valley * ld + i] = vm_valley; a.rf[RF_repol * ld + i] = vm_repol;
+  a.rf[RF_tpeak * ld + i] = t_peak; a.rf[RF_tdepol * ld + i] = t_depol; a.rf[RF_trepol * ld + i] = t_repol;
+  a.rf[RF_apd * ld + i] = apd90; a.rf[RF_t * ld + i] = t; a.rf[RF_tp0 * ld + i] = tp0;
+  a.ri[RI_repl * ld + i] = repl; a.ri[RI_pace * ld + i] = pace; a.ri[RI_all * ld + i] = all_pace;
+  a.ri[RI_iout * ld + i] = iout; a.ri[RI_nrec * ld + i] = n_rec; a.ri[RI_recal * ld + i] = recal;
+  a.ri[RI_status * ld + i] = st;
+}
+
+// Voltage-clamp replay (CEPPatch/benchpatch.cpp:83-100): V set to v[k]
+// before step k, the selected channel current of the step to out[k][ld].
+struct ClampArgs {
+  double *y;
+  const double *par;
+  int64_t ld;
+  int n;
+  const double *v;  // [m] clamp potentials of this chunk
+  int m, current;
+  double t0, dt;
+  double *out;      // [m][ld]
+};
+
+template <class M, class P>
+__global__ void __launch_bounds__(128) clamp_kernel(ClampArgs a) {
+  using G = typename P::G;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  typename M::template Y<G> y;
+  typename M::template Par<G> q;
+  M::template load<G>(y, a.y, a.ld, i);
+  M::template load_par<G>(q, a.par, a.ld, i);
+  typename M::template Cur<G> c;
+  double t = a.t0;
+  for (int k = 0; k < a.m; ++k) {
+    y.V = a.v[k];
+    M::template step<P>(y, q, t, a.dt, -1, true, c);
+    double x;
+    switch (a.current) {
+      case 0: x = (double)c.INa; break;
+      case 1: x = (double)c.INaL; break;
+      case 2: x = (double)c.Ito; break;
+      case 3: x = (double)c.ICaL; break;
+      case 4: x = (double)c.IKr; break;
+      case 5: x = (double)c.IKs; break;
+      default: x = (double)c.IK1; break;
+    }
+    a.out[(int64_t)k * a.ld + i] = x;
+    t += a.dt;
+  }
+  M::template store<G>(y, a.y, a.ld, i);
+}
+
 // Rates at the current state (no update).
 template <class M>
 __global__ void rates_kernel(const double *s, const double *par, int64_t ld, int n, double t, int stim_mode,
@@ -616,6 +822,24 @@ struct Ops {
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "tissue launch failed: %s", cudaGetErrorString(e));
   }
+  static int launch_restit(cep_batch *b, const RestitArgs &a) {
+    const int grid = (b->n + 127) / 128;
+    if (b->precision == CEP_PREC_MIXED)
+      restit_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
+    else
+      restit_kernel<M, F64><<<grid, 128, 0, b->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "restitution launch failed: %s", cudaGetErrorString(e));
+  }
+  static int launch_clamp(cep_batch *b, const ClampArgs &a) {
+    const int grid = (b->n + 127) / 128;
+    if (b->precision == CEP_PREC_MIXED)
+      clamp_kernel<M, Mixed><<<grid, 128, 0, b->stream>>>(a);
+    else
+      clamp_kernel<M, F64><<<grid, 128, 0, b->stream>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "clamp launch failed: %s", cudaGetErrorString(e));
+  }
   static int launch_rates(cep_batch *b, double t, double *dvdt, double *cur) {
     const int grid = (b->n + kBlock - 1) / kBlock;
     rates_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->states, b->params, b->ld, b->n, t, -1, dvdt, cur);
@@ -632,29 +856,36 @@ struct ModelInfo {
   int (*rates)(cep_batch *, double, double *, double *);
   int p_bcl;
   int (*tissue)(cep_batch *, const TissueArgs &);
+  int (*restit)(cep_batch *, const RestitArgs &);
+  int (*clamp)(cep_batch *, const ClampArgs &);
 };
 
 const ModelInfo *model_info(int model) {
   static const ModelInfo ord_info{OrdModel::kStates, OrdModel::kParams, OrdModel::kCai,
                                   &Ops<OrdModel>::launch_init, &Ops<OrdModel>::launch_pacing,
                                   &Ops<OrdModel>::launch_reset, &Ops<OrdModel>::launch_run,
-                                  &Ops<OrdModel>::launch_rates, OrdModel::p_bcl(), &Ops<OrdModel>::launch_tissue};
+                                  &Ops<OrdModel>::launch_rates, OrdModel::p_bcl(), &Ops<OrdModel>::launch_tissue,
+                                  &Ops<OrdModel>::launch_restit, &Ops<OrdModel>::launch_clamp};
   static const ModelInfo cipa_info{CipaModel::kStates, CipaModel::kParams, CipaModel::kCai,
                                    &Ops<CipaModel>::launch_init, &Ops<CipaModel>::launch_pacing,
                                    &Ops<CipaModel>::launch_reset, &Ops<CipaModel>::launch_run,
-                                   &Ops<CipaModel>::launch_rates, CipaModel::p_bcl(), &Ops<CipaModel>::launch_tissue};
+                                   &Ops<CipaModel>::launch_rates, CipaModel::p_bcl(), &Ops<CipaModel>::launch_tissue,
+                                  &Ops<CipaModel>::launch_restit, &Ops<CipaModel>::launch_clamp};
   static const ModelInfo tt06_info{Tt06Model::kStates, Tt06Model::kParams, Tt06Model::kCai,
                                    &Ops<Tt06Model>::launch_init, &Ops<Tt06Model>::launch_pacing,
                                    &Ops<Tt06Model>::launch_reset, &Ops<Tt06Model>::launch_run,
-                                   &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl(), &Ops<Tt06Model>::launch_tissue};
+                                   &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl(), &Ops<Tt06Model>::launch_tissue,
+                                  &Ops<Tt06Model>::launch_restit, &Ops<Tt06Model>::launch_clamp};
   static const ModelInfo tomek_info{TomekModel::kStates, TomekModel::kParams, TomekModel::kCai,
                                    &Ops<TomekModel>::launch_init, &Ops<TomekModel>::launch_pacing,
                                    &Ops<TomekModel>::launch_reset, &Ops<TomekModel>::launch_run,
-                                   &Ops<TomekModel>::launch_rates, TomekModel::p_bcl(), &Ops<TomekModel>::launch_tissue};
+                                   &Ops<TomekModel>::launch_rates, TomekModel::p_bcl(), &Ops<TomekModel>::launch_tissue,
+                                  &Ops<TomekModel>::launch_restit, &Ops<TomekModel>::launch_clamp};
   static const ModelInfo tt04_info{Tt04Model::kStates, Tt04Model::kParams, Tt04Model::kCai,
                                    &Ops<Tt04Model>::launch_init, &Ops<Tt04Model>::launch_pacing,
                                    &Ops<Tt04Model>::launch_reset, &Ops<Tt04Model>::launch_run,
-                                   &Ops<Tt04Model>::launch_rates, Tt04Model::p_bcl(), &Ops<Tt04Model>::launch_tissue};
+                                   &Ops<Tt04Model>::launch_rates, Tt04Model::p_bcl(), &Ops<Tt04Model>::launch_tissue,
+                                  &Ops<Tt04Model>::launch_restit, &Ops<Tt04Model>::launch_clamp};
   switch (model) {
     case CEP_MODEL_TT2006: return &tt06_info;
     case CEP_MODEL_TT2004: return &tt04_info;
@@ -1132,6 +1363,123 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
   if (currents) CEP_CUDA(cudaMemcpyAsync(currents, d + b->n, sizeof(double) * 7 * b->n, cudaMemcpyDeviceToHost, b->stream));
   CEP_CUDA(cudaFreeAsync(d, b->stream));
   CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Device scratch of one blocking protocol call, released on every return.
+struct Scratch {
+  std::vector<void *> p;
+  ~Scratch() {
+    for (void *q : p) cudaFree(q);
+  }
+  template <class T>
+  int get(T **out, size_t count) {
+    void *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CEP_ERR_OOM, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    p.push_back(q);
+    *out = static_cast<T *>(q);
+    return CEP_OK;
+  }
+};
+}  // namespace
+
+extern "C" {
+
+int cep_batch_restitution(cep_batch_t b, const double *bcl, int n_bcl, int n_pace, double dt,
+                          long steps_per_launch, cep_apdr_record_t *out, int max_records, int *n_records) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (!bcl || n_bcl <= 0) return fail(CEP_ERR_ARG, "bcl list is empty");
+  if (n_pace <= 0) return fail(CEP_ERR_ARG, "n_pace must be positive (got %d)", n_pace);
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(CEP_ERR_ARG, "dt must be positive");
+  if (max_records < 0 || (max_records > 0 && !out)) return fail(CEP_ERR_ARG, "bad record buffer");
+  if (steps_per_launch <= 0) steps_per_launch = 20000;
+  if (steps_per_launch > (1L << 30)) steps_per_launch = 1L << 30;
+  std::vector<int> S(n_bcl), imax(n_bcl);
+  int s_max = 1;
+  long expected = 0;
+  for (int k = 0; k < n_bcl; ++k) {
+    if (!(bcl[k] > 0) || !std::isfinite(bcl[k])) return fail(CEP_ERR_ARG, "bcl[%d] must be positive", k);
+    const double steps = bcl[k] / dt, total = (n_pace * bcl[k]) / dt;  // apdr_bench.cpp:128,169
+    if (steps < 1 || total > 2.0e9) return fail(CEP_ERR_ARG, "bcl[%d]/dt out of range", k);
+    S[k] = (int)steps;
+    imax[k] = (int)total;
+    if (S[k] > s_max) s_max = S[k];
+    const long boundaries = ((long)imax[k] + 1) / S[k];
+    if (boundaries > 2) expected += boundaries - 2;
+  }
+  if (n_records) *n_records = (int)expected;
+  const ModelInfo *mi = model_info(b->model);
+  Scratch sc;
+  RestitArgs a;
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.dt = dt;
+  a.max_rec = max_records;
+  int rc;
+  if ((rc = sc.get(&a.rf, (size_t)kRF * b->ld))) return rc;
+  if ((rc = sc.get(&a.ri, (size_t)kRI * b->ld))) return rc;
+  if ((rc = sc.get(&a.trace, (size_t)s_max * b->ld))) return rc;
+  a.rec = nullptr;
+  if (max_records > 0 && (rc = sc.get(&a.rec, (size_t)max_records * b->n))) return rc;
+  const int grid = (b->n + 127) / 128;
+  restit_init_kernel<<<grid, 128, 0, b->stream>>>(a);
+  CEP_CUDA(cudaGetLastError());
+  for (int k = 0; k < n_bcl; ++k) {
+    if ((rc = mi->pacing(b, 0, b->n, bcl[k], -1.0, -1.0, 1.0))) return rc;  // CONSTANTS[stim_period] = bcl (:105)
+    a.bcl = bcl[k]; a.S = S[k]; a.imax = imax[k]; a.n_steps = (int)steps_per_launch;
+    restit_segment_kernel<<<grid, 128, 0, b->stream>>>(a);
+    CEP_CUDA(cudaGetLastError());
+    const long total = (long)imax[k] + 1;
+    for (long done = 0; done < total; done += steps_per_launch)
+      if ((rc = mi->restit(b, a))) return rc;
+  }
+  std::vector<int> st(b->n);
+  CEP_CUDA(cudaMemcpyAsync(st.data(), a.ri + (size_t)RI_status * b->ld, sizeof(int) * b->n, cudaMemcpyDeviceToHost,
+                           b->stream));
+  if (max_records > 0)
+    CEP_CUDA(cudaMemcpyAsync(out, a.rec, sizeof(cep_apdr_record_t) * (size_t)max_records * b->n,
+                             cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->n; ++i)
+    if (st[i] != 0) return fail(CEP_ERR_NONFINITE, "instance %d turned non-finite during restitution", i);
+  return CEP_OK;
+}
+
+int cep_batch_clamp(cep_batch_t b, const double *v, long n_samples, double t0, double dt, int current,
+                    double *out) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (!v || !out || n_samples <= 0) return fail(CEP_ERR_ARG, "empty clamp trace");
+  if (current < 0 || current > 6) return fail(CEP_ERR_ARG, "current index %d not in 0..6", current);
+  if (!(dt > 0) || !std::isfinite(dt) || !std::isfinite(t0)) return fail(CEP_ERR_ARG, "bad t0/dt");
+  const int chunk = 2048;
+  Scratch sc;
+  ClampArgs a;
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.current = current; a.dt = dt;
+  double *dv = nullptr, *dout = nullptr;
+  int rc;
+  if ((rc = sc.get(&dv, chunk))) return rc;
+  if ((rc = sc.get(&dout, (size_t)chunk * b->ld))) return rc;
+  a.v = dv; a.out = dout;
+  const ModelInfo *mi = model_info(b->model);
+  double t = t0;
+  for (long k0 = 0; k0 < n_samples; k0 += chunk) {
+    const int m = (int)std::min<long>(chunk, n_samples - k0);
+    CEP_CUDA(cudaMemcpyAsync(dv, v + k0, sizeof(double) * m, cudaMemcpyHostToDevice, b->stream));
+    a.m = m;
+    a.t0 = t;
+    if ((rc = mi->clamp(b, a))) return rc;
+    CEP_CUDA(cudaMemcpy2DAsync(out + (size_t)k0 * b->n, sizeof(double) * b->n, dout, sizeof(double) * b->ld,
+                               sizeof(double) * b->n, m, cudaMemcpyDeviceToHost, b->stream));
+    CEP_CUDA(cudaStreamSynchronize(b->stream));  // dv is reused by the next chunk
+    for (int k = 0; k < m; ++k) t += dt;          // the kernel's clock, same additions
+  }
   return CEP_OK;
 }
 

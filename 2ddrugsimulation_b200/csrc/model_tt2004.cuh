@@ -221,8 +221,10 @@ __device__ __forceinline__ double hill_factor(double conc, double ic50, double h
 // initConsts (:185-359) plus the reference's Hill hook (:361-377).
 __device__ __forceinline__ void init_instance(double *__restrict__ par, double *__restrict__ s_, int64_t ld,
                                               int64_t i, double conc, const double *__restrict__ hill,
-                                              bool quirks) {
-  double gCaL = 0.000175, gK1 = 5.405, gKs = 0.245, gNa = 14.838, gto = 0.294, gKr = 0.096;
+                                              bool quirks, bool mcell) {
+  // mcell: the 2004_a build (tentusscher_noble_noble_panfilov_2004_a.cpp:265),
+  // identical to 2004_b but for g_Ks.
+  double gCaL = 0.000175, gK1 = 5.405, gKs = mcell ? 0.062 : 0.245, gNa = 14.838, gto = 0.294, gKr = 0.096;
   if (hill) {
     gCaL *= hill_factor(conc, hill[0], hill[1]);
     gK1 *= hill_factor(conc, hill[2], hill[3]);

@@ -55,6 +55,9 @@ extern "C" {
 /* init flags */
 #define CEP_FLAG_DUTTA 1u  /* Dutta et al. 2017 conductance scaling (ORd)          */
 #define CEP_FLAG_QUIRKS 2u /* reproduce the reference's documented quirks exactly  */
+#define CEP_FLAG_TT04_MCELL 4u /* TT2004: the 2004_a build (g_Ks 0.062, M cell) instead of
+                                  2004_b (g_Ks 0.245): tentusscher_noble_noble_panfilov_2004_a.cpp:265,
+                                  chosen by celltype 0 in apdr_bench.cpp:77-84 */
 
 /* state array layouts for set/get */
 #define CEP_LAYOUT_SOA 0 /* states[k * n + i] (k = state index, i = instance) */
@@ -163,6 +166,47 @@ int cep_batch_sync(cep_batch_t b);
  * Ohara_Rudy_2011.cpp:742): dVdt[n] and the seven channel currents
  * currents[7*n] (INa, INaL, Ito, ICaL, IKr, IKs, IK1; SoA). */
 int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
+
+/* ------------------------------------------------- protocol variants */
+/* One pace of a dynamic (S1-S1) restitution run, as apdr_bench.cpp:211
+ * writes it ("all_pace bcl apd90 t_di tcurr"); recal = 1 when the pace's
+ * windowed Vm peak was below 10 mV and the APD came from the search over the
+ * pace's whole Vm trace (:172-191). */
+typedef struct {
+  int32_t pace;  /* running pace number over all BCLs (all_pace)        */
+  int32_t recal; /* 1: the recalibration search set the APD              */
+  double bcl;    /* ms                                                   */
+  double apd90;  /* ms                                                   */
+  double di;     /* diastolic interval: next stimulus - repolarisation   */
+  double t;      /* segment clock at the end of the pace (tcurr)         */
+} cep_apdr_record_t;
+
+/* Dynamic restitution of every instance (apdr_bench.cpp:103-232, the CVODE
+ * integration replaced by the fixed-step scheme): for each bcl[s] in order,
+ * CONSTANTS[BCL] = bcl[s], the segment clock restarts at 0 and the cell
+ * state carries over; iout = 1 .. (int)(n_pace*bcl/dt) + 1 steps; at every
+ * pace boundary (iout % (int)(bcl/dt) == 0) the pace's APD90 (90 %
+ * repolarisation from the peak in (start+4, start+56) ms against the
+ * previous boundary's Vm) is closed, and paces after the first two of each
+ * BCL are recorded. out[n * max_records] (instance-major); *n_records
+ * receives the records per instance (the same for every instance; at most
+ * max_records are written). The run keeps each instance's Vm over the
+ * current pace in device memory (max over s of (int)(bcl[s]/dt) doubles
+ * per instance) for the recalibration search. Blocking.
+ * apdr_bcls() in the Python package builds the reference's BCL list
+ * (bcl_init down to bcl_end, decrement 10 once bcl <= 300). */
+int cep_batch_restitution(cep_batch_t b, const double *bcl, int n_bcl, int n_pace, double dt,
+                          long steps_per_launch, cep_apdr_record_t *out, int max_records, int *n_records);
+
+/* Voltage-clamp replay (CEPPatch/benchpatch.cpp:83-100): before step k the
+ * membrane potential of every instance is set to v[k]; the step runs the
+ * model from t0 + k*dt (t += dt) with its periodic stimulus; out[k * n + i]
+ * receives channel current `current` of instance i at that step (0 INa,
+ * 1 INaL, 2 Ito, 3 ICaL, 4 IKr, 5 IKs, 6 IK1: the order of
+ * cep_batch_rates). The instances' states advance; the batch clock is not
+ * touched. Blocking. */
+int cep_batch_clamp(cep_batch_t b, const double *v, long n_samples, double t0, double dt, int current,
+                    double *out);
 
 /* ---------------------------------------------------- instance ranges */
 /* Heterogeneous batches: a batch used as a pool of slots whose ranges hold

@@ -63,6 +63,13 @@ class CepoBiomarkers(ctypes.Structure):
                 ("qnet_last", ctypes.c_double), ("status", ctypes.c_int)]
 
 
+class CepoApdrRecord(ctypes.Structure):
+    _fields_ = [("pace", ctypes.c_int), ("recal", ctypes.c_int), ("bcl", ctypes.c_double),
+                ("apd90", ctypes.c_double), ("di", ctypes.c_double), ("t", ctypes.c_double)]
+
+
+APDR_FIELDS = ("pace", "recal", "bcl", "apd90", "di", "t")
+
 _lib = None
 
 
@@ -90,6 +97,13 @@ def lib() -> ctypes.CDLL:
                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_long, _dp,
                                      ctypes.c_int]
         L.cepo_run_batch.restype = ctypes.c_int
+        L.cepo_restitution.argtypes = [ctypes.POINTER(CepoCell), _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.POINTER(CepoApdrRecord), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int)]
+        L.cepo_restitution.restype = ctypes.c_int
+        L.cepo_clamp.argtypes = [ctypes.POINTER(CepoCell), _dp, _dp, ctypes.c_long, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int, _dp]
+        L.cepo_tt04_mcell.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_double, _dp]
         _ip = ctypes.POINTER(ctypes.c_int)
         L.cepo_fem_nnz.argtypes = [ctypes.c_int] * 4
         L.cepo_fem_nnz.restype = ctypes.c_long
@@ -135,7 +149,7 @@ class Cell:
     """One oracle cell instance."""
 
     def __init__(self, model: str, celltype: float = 0.0, conc: float = 0.0, hill=None,
-                 is_dutta: bool = False, quirks: bool = True, tissue_stim: bool = False):
+                 is_dutta: bool = False, quirks: bool = True, tissue_stim: bool = False, mcell: bool = False):
         self.model = model
         self.c = CepoCell()
         h = None if hill is None else np.ascontiguousarray(hill, dtype=np.float64)
@@ -143,6 +157,10 @@ class Cell:
                              _ptr(h), 0 if h is None else len(h), int(is_dutta), int(quirks))
         if rc != 0:
             raise RuntimeError(f"oracle init failed for {model}: {rc}")
+        if mcell:
+            if model != "tt2004":
+                raise ValueError("mcell is the TT2004 2004_a variant")
+            lib().cepo_tt04_mcell(ctypes.byref(self.c), float(conc), _ptr(h))
         self.c.tissue_stim = int(tissue_stim)
         self.y = np.zeros(64)
         lib().cepo_init_states(ctypes.byref(self.c), _ptr(self.y))
@@ -186,6 +204,39 @@ class Cell:
         out = {f: getattr(bm.result, f) for f in BEAT_FIELDS}
         out.update(steepest_pace=bm.steepest_pace, n_eligible=bm.n_eligible, status=bm.status)
         return out, (vt if v_stride else None)
+
+
+    def restitution(self, bcls, n_pace: int, dt: float, max_records: int = 100000):
+        """apdr_bench.cpp:103-232 on the fixed-step scheme; returns (records as a
+        dict of arrays, status)."""
+        b = np.ascontiguousarray(bcls, dtype=np.float64)
+        recs = (CepoApdrRecord * max_records)()
+        n = ctypes.c_int(0)
+        st = lib().cepo_restitution(ctypes.byref(self.c), _ptr(self.y), _ptr(b), len(b), int(n_pace), float(dt),
+                                    recs, max_records, ctypes.byref(n))
+        k = min(n.value, max_records)
+        out = {f: np.array([getattr(recs[j], f) for j in range(k)]) for f in APDR_FIELDS}
+        return out, st
+
+    def clamp(self, v, t0: float, dt: float, current: int) -> np.ndarray:
+        """CEPPatch/benchpatch.cpp:83-100: V forced to v[k] before step k."""
+        vv = np.ascontiguousarray(v, dtype=np.float64)
+        out = np.zeros(len(vv))
+        lib().cepo_clamp(ctypes.byref(self.c), _ptr(self.y), _ptr(vv), len(vv), float(t0), float(dt), int(current),
+                         _ptr(out))
+        return out
+
+
+def apdr_bcls(bcl_init: float, bcl_end: float, bcl_decrement: float) -> list[float]:
+    """BCL list of apdr_bench.cpp:103,229-230: from bcl_init while bcl >= bcl_end,
+    the decrement becoming 10 once bcl <= 300."""
+    out, bcl, dec = [], float(bcl_init), float(bcl_decrement)
+    while bcl >= bcl_end:
+        out.append(bcl)
+        if bcl <= 300.0:
+            dec = 10.0
+        bcl -= dec
+    return out
 
 
 def run_batch(model: str, celltype, conc, hill, bcl: float, dt: float, n_steps: int,

@@ -90,6 +90,25 @@ int cepo_run_batch(int model, int n, const double *celltype, const double *conc,
                    int n_hill, int is_dutta, int quirks, double bcl, double dt, long n_steps,
                    double *states_out, int n_threads);
 
+/* ------------------------------------------------------------ protocols */
+/* One recorded pace of a restitution run (apdr_bench.cpp:211). */
+typedef struct {
+  int pace, recal;
+  double bcl, apd90, di, t;
+} cepo_apdr_record;
+
+/* Dynamic restitution of CEPCell_NEO/modules/apdr_bench.cpp:103-232 on the
+ * fixed-step scheme; y carries the state in and out. Returns 0, or 1 when
+ * V turned non-finite. *n_records = records produced (at most max_records
+ * written). */
+int cepo_restitution(const cepo_cell *c, double *y, const double *bcls, int n_bcl, int n_pace, double dt,
+                     cepo_apdr_record *out, int max_records, int *n_records);
+/* Voltage-clamp replay (CEPPatch/benchpatch.cpp:83-100). */
+void cepo_clamp(const cepo_cell *c, double *y, const double *v, long n_samples, double t0, double dt,
+                int current, double *out);
+/* TT2004: the 2004_a build (g_Ks 0.062) after cepo_init. */
+void cepo_tt04_mcell(cepo_cell *c, double conc, const double *hill);
+
 /* -------------------------------------------------------------------- FEM */
 /* Structured-grid Q1 (2D) / trilinear hex (3D) assembly of A = M/dt + K_D and
  * B = M into CSR (fem.cpp:628-661,721-752; Gauss points at +-0.57735, unit

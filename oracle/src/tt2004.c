@@ -57,6 +57,15 @@ int cepo_tt04_init(cepo_cell *c, double celltype, double conc, const double *hil
   return 0;
 }
 
+/* The 2004_a build (tentusscher_noble_noble_panfilov_2004_a.cpp:265): the
+ * same model with g_Ks = 0.062 (M cell) instead of 0.245; the Hill factor of
+ * initConsts(type, conc, hill) applies on top, as in init. */
+void cepo_tt04_mcell(cepo_cell *c, double conc, const double *hill) {
+  tt04_p *q = (tt04_p *)c->p;
+  q->g_Ks = 0.062;
+  if (hill) q->g_Ks *= hb(conc, hill[4], hill[5]);
+}
+
 void cepo_tt04_init_states(double *y) {
   y[V] = -86.2; y[K_i] = 138.3; y[Na_i] = 11.6; y[Ca_i] = 0.0002; y[Xr1] = 0; y[Xr2] = 1; y[Xs] = 0;
   y[m] = 0; y[h] = 0.75; y[j] = 0.75; y[d] = 0; y[f] = 1; y[fCa] = 1; y[s] = 1; y[r] = 0; y[Ca_SR] = 0.2;
