@@ -98,6 +98,56 @@ __device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, type
   }
 }
 
+// A gate's time constant in the form each policy integrates with. F64 keeps
+// tau itself, computed as the reference writes it, for exp(-dt/tau). Mixed
+// keeps the rate 1/tau: where tau is a quotient num/sum of the model's rate
+// terms, a = dt*sum/num needs no SFU reciprocal or division (two dependent
+// MUFU ops fewer per gate).
+template <class P>
+struct Tau {
+  typename P::G v;
+};
+// tau = num / sum (num a constant; 1/sum when num == 1)
+template <class P>
+__device__ __forceinline__ Tau<P> tau_quot(double num, typename P::G sum) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) {
+    if (num == 1.0) return {sum};
+    return {sum * (G)(1.0 / num)};
+  } else {
+    return {num == 1.0 ? P::rc(sum) : P::dv((G)num, sum)};
+  }
+}
+// tau * s (s a constant)
+template <class P>
+__device__ __forceinline__ Tau<P> tau_scaled(Tau<P> t, double s) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) return {t.v * (G)(1.0 / s)};
+  else return {(G)s * t.v};
+}
+// a constant tau
+template <class P>
+__device__ __forceinline__ Tau<P> tau_const(double tau) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) return {(G)(1.0 / tau)};
+  else return {(G)tau};
+}
+template <class P, bool slow = false>
+__device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, Tau<P> t, double dt) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) {
+    const G a = (G)dt * t.v;
+    G f;
+    if constexpr (slow)
+      f = a * ((G)1 - a * ((G)0.5 - a * ((G)(1.0 / 6.0) - a * (G)(1.0 / 24.0))));
+    else
+      f = (G)1 - P::ex(-a);
+    return y + (double)((yinf - (G)y) * f);
+  } else {
+    return rush_larsen<P, slow>(y, yinf, t.v, dt);
+  }
+}
+
 // Per-instance biomarker bookkeeping (the CiPA per-beat state machine) kept in
 // global memory between launches; the hot fields live in registers during a
 // launch.

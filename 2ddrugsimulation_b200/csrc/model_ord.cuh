@@ -305,12 +305,12 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   const G mss = P::rc((one + P::ex(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2))));
-  const G tm = P::rc(((G)k::mtD1 * P::ex((v + (G)k::mtV1) * (G)(1.0 / k::mtV2)) +
+  const Tau<P> tm = tau_quot<P>(1.0, ((G)k::mtD1 * P::ex((v + (G)k::mtV1) * (G)(1.0 / k::mtV2)) +
                       (G)k::mtD2 * P::ex(-(v + (G)k::mtV3) * (G)(1.0 / k::mtV4))));
   const G hss = P::rc((one + P::ex((v + (G)k::hssV1) * (G)(1.0 / k::hssV2))));
-  const G thf = P::rc(((G)1.432e-05 * P::ex(-(v + (G)1.196) * (G)(1.0 / 6.285)) +
+  const Tau<P> thf = tau_quot<P>(1.0, ((G)1.432e-05 * P::ex(-(v + (G)1.196) * (G)(1.0 / 6.285)) +
                        (G)6.149 * P::ex((v + (G)0.5096) * (G)(1.0 / 20.27))));
-  const G ths = P::rc(((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
+  const Tau<P> ths = tau_quot<P>(1.0, ((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
                        (G)0.3343 * P::ex((v + (G)5.73) * (G)(1.0 / 56.66))));
   const G tj = (G)2.038 + P::rc(((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
                                  (G)0.3052 * P::ex((v + (G)0.9941) * (G)(1.0 / 38.45))));
@@ -362,11 +362,11 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
   y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
   y.j = rush_larsen<P, true>(y.j, hss, tj, dt);
-  y.hsp = rush_larsen<P, true>(y.hsp, hssp, (G)3.0 * ths, dt);
+  y.hsp = rush_larsen<P, true>(y.hsp, hssp, tau_scaled<P>(ths, 3.0), dt);
   y.jp = rush_larsen<P, true>(y.jp, hss, (G)1.46 * tj, dt);
   y.mL = rush_larsen<P>(y.mL, mLss, tm, dt);
-  y.hL = rush_larsen<P, true>(y.hL, hLss, (G)k::thL, dt);
-  y.hLp = rush_larsen<P, true>(y.hLp, hLssp, (G)k::thLp, dt);
+  y.hL = rush_larsen<P, true>(y.hL, hLss, tau_const<P>(k::thL), dt);
+  y.hLp = rush_larsen<P, true>(y.hLp, hLssp, tau_const<P>(k::thLp), dt);
 }
 
 // role 1: transient outward, slow/rapid (ORd) delayed rectifier, inward
@@ -377,7 +377,7 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   const G ass = P::rc((one + P::ex(-(v - (G)14.34) * (G)(1.0 / 14.82))));
-  const G ta = P::dv((G)1.0515, (P::rc(((G)1.2089 * (one + P::ex(-(v - (G)18.4099) * (G)(1.0 / 29.3814))))) +
+  const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + P::ex(-(v - (G)18.4099) * (G)(1.0 / 29.3814))))) +
                             P::dv((G)3.5, (one + P::ex((v + (G)100.0) * (G)(1.0 / 29.3814))))));
   const G assp = P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
   const G iss = P::rc((one + P::ex((v + (G)43.94) * (G)(1.0 / 5.711))));
@@ -393,9 +393,11 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const G xs1ss = P::rc((one + P::ex(-(v + (G)11.60) * (G)(1.0 / 8.932))));
   const G txs1 = (G)817.3 + P::rc(((G)2.326e-04 * P::ex((v + (G)48.28) * (G)(1.0 / 17.80)) +
                                    (G)0.001292 * P::ex(-(v + (G)210.0) * (G)(1.0 / 230.0))));
-  const G txs2 = P::rc(((G)0.01 * P::ex((v - (G)50.0) * (G)0.05) + (G)0.0193 * P::ex(-(v + (G)66.54) * (G)(1.0 / 31.0))));
+  const Tau<P> txs2 =
+      tau_quot<P>(1.0, ((G)0.01 * P::ex((v - (G)50.0) * (G)0.05) + (G)0.0193 * P::ex(-(v + (G)66.54) * (G)(1.0 / 31.0))));
   const G xk1ss = P::rc((one + P::ex(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den))));
-  const G txk1 = P::dv((G)122.2, (P::ex(-(v + (G)127.2) * (G)(1.0 / 20.36)) + P::ex((v + (G)236.8) * (G)(1.0 / 69.33))));
+  const Tau<P> txk1 =
+      tau_quot<P>(122.2, (P::ex(-(v + (G)127.2) * (G)(1.0 / 20.36)) + P::ex((v + (G)236.8) * (G)(1.0 / 69.33))));
   const G fp_ = c.fCaMKp;
   const G EK = (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
   const G AiF = P::rc((one + P::ex((v - (G)213.6) * (G)(1.0 / 151.2))));
@@ -517,7 +519,7 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   else
     y.fcafp = rush_larsen<P, true>(y.fcafp, fss, (G)2.5 * tfcaf, dt);
   // nca relaxes at rate km2n towards anca*k2n/km2n (Ohara_Rudy_2011.cpp:1065-1066)
-  y.nca = rush_larsen<P, true>(y.nca, anca * P::dv((G)k::k2n, km2n), P::rc(km2n), dt);
+  y.nca = rush_larsen<P, true>(y.nca, anca * P::dv((G)k::k2n, km2n), tau_quot<P>(1.0, km2n), dt);
   y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, dt);
   y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, dt);
 }
