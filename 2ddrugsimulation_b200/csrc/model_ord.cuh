@@ -93,6 +93,14 @@ constexpr double sqrt_ko54 = 1.0;  // pow(ko/5.4, 1/2) with ko = 5.4
 constexpr double sqrt_ko = 2.32379000772445;  // pow(5.4, 1/2)
 constexpr double xk1_off = 2.55380 * ko + 144.590, xk1_den = 1.56920 * ko + 3.81150;
 constexpr double a3c = k3p * (ko / Kko) * (ko / Kko), ko_Kko_sq = (1.0 + ko / Kko) * (1.0 + ko / Kko);
+// Mixed-policy shortcuts (one SFU op each): gates whose steady states share
+// a slope differ by a constant factor of the exponential,
+// e^((V+89.1)/6.086) = e^((V+82.9)/6.086) e^(6.2/6.086) (hssp vs hss),
+// e^((V+93.81)/7.488) = e^((V+87.61)/7.488) e^(6.2/7.488) (hLssp vs hLss),
+// e^(-(V-24.34)/14.82) = e^(-(V-14.34)/14.82) e^(10/14.82) (assp vs ass);
+// and log(c_o/c_i) = log(c_o) - log(c_i) for ENa and EK.
+constexpr double hssp_shift = 2.769679238039406, hLssp_shift = 2.288717124596483, assp_shift = 1.9635691902911017;
+constexpr double log_nao = 4.941642422609304, log_ko = 1.6863989535702288;
 }  // namespace k
 
 template <class G>
@@ -307,20 +315,26 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G mss = P::rc((one + P::ex(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2))));
   const Tau<P> tm = tau_quot<P>(1.0, ((G)k::mtD1 * P::ex((v + (G)k::mtV1) * (G)(1.0 / k::mtV2)) +
                       (G)k::mtD2 * P::ex(-(v + (G)k::mtV3) * (G)(1.0 / k::mtV4))));
-  const G hss = P::rc((one + P::ex((v + (G)k::hssV1) * (G)(1.0 / k::hssV2))));
+  const G e_hss = P::ex((v + (G)k::hssV1) * (G)(1.0 / k::hssV2));
+  const G hss = P::rc((one + e_hss));
   const Tau<P> thf = tau_quot<P>(1.0, ((G)1.432e-05 * P::ex(-(v + (G)1.196) * (G)(1.0 / 6.285)) +
                        (G)6.149 * P::ex((v + (G)0.5096) * (G)(1.0 / 20.27))));
   const Tau<P> ths = tau_quot<P>(1.0, ((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
                        (G)0.3343 * P::ex((v + (G)5.73) * (G)(1.0 / 56.66))));
   const G tj = (G)2.038 + P::rc(((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
                                  (G)0.3052 * P::ex((v + (G)0.9941) * (G)(1.0 / 38.45))));
-  const G hssp = P::rc((one + P::ex((v + (G)89.1) * (G)(1.0 / 6.086))));
+  static_assert(k::hssV1 == 82.9 && k::hssV2 == 6.086, "hssp_shift assumes hss = 1/(1+e^((V+82.9)/6.086))");
+  const G hssp = P::kMixed ? P::rc(one + e_hss * (G)k::hssp_shift)
+                           : P::rc((one + P::ex((v + (G)89.1) * (G)(1.0 / 6.086))));
   const G mLss = P::rc((one + P::ex(-(v + (G)42.85) * (G)(1.0 / 5.264))));
-  const G hLss = P::rc((one + P::ex((v + (G)87.61) * (G)(1.0 / 7.488))));
-  const G hLssp = P::rc((one + P::ex((v + (G)93.81) * (G)(1.0 / 7.488))));
+  const G e_hL = P::ex((v + (G)87.61) * (G)(1.0 / 7.488));
+  const G hLss = P::rc((one + e_hL));
+  const G hLssp = P::kMixed ? P::rc(one + e_hL * (G)k::hLssp_shift)
+                            : P::rc((one + P::ex((v + (G)93.81) * (G)(1.0 / 7.488))));
   const G fp_ = c.fCaMKp;
   // INa, INaL
-  const G ENa = (G)k::RTF * P::lg(P::dv((G)k::nao, (G)y.nai));
+  const G ENa = P::kMixed ? (G)k::RTF * ((G)k::log_nao - P::lg((G)y.nai))
+                          : (G)k::RTF * P::lg(P::dv((G)k::nao, (G)y.nai));
   const G h_ = (G)k::Ahf * (G)y.hf + (G)k::Ahs * (G)y.hs;
   const G hp = (G)k::Ahf * (G)y.hf + (G)k::Ahs * (G)y.hsp;
   const G INa = q.GNa * (v - ENa) * p3((G)y.m) * ((one - fp_) * h_ * (G)y.j + fp_ * hp * (G)y.jp);
@@ -331,18 +345,27 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G INab = (G)k::PNab * fac * ((G)y.nai * e1 - (G)k::nao);
   // INaK
   const G nai_g = (G)y.nai, ki_g = (G)y.ki;
-  const G Knao = (G)k::Knao0 * P::ex(((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
-  const G Knai = (G)k::Knai0 * P::ex(((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
-  const G nak_den_o = (p3(one + P::dv((G)k::nao, Knao)) + (G)k::ko_Kko_sq) - one;
-  const G nak_den_i = (p3(one + P::dv(nai_g, Knai)) + p2(one + ki_g * (G)(1.0 / k::Kki))) - one;
+  // nao/Knao and nai/Knai: in mixed, nao/Knao0 e^(-c v) without a division
+  G nao_Knao, nai_Knai;
+  if constexpr (P::kMixed) {
+    nao_Knao = (G)(k::nao / k::Knao0) * P::ex(-((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+    nai_Knai = nai_g * (G)(1.0 / k::Knai0) * P::ex(-((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+  } else {
+    const G Knao = (G)k::Knao0 * P::ex(((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+    const G Knai = (G)k::Knai0 * P::ex(((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
+    nao_Knao = P::dv((G)k::nao, Knao);
+    nai_Knai = P::dv(nai_g, Knai);
+  }
+  const G nak_den_o = (p3(one + nao_Knao) + (G)k::ko_Kko_sq) - one;
+  const G nak_den_i = (p3(one + nai_Knai) + p2(one + ki_g * (G)(1.0 / k::Kki))) - one;
   const G a3 = P::dv((G)k::a3c, nak_den_o);
   // P = eP / (1 + H/Khp + nai/Knap + ki/Kxkur) with the instance's H folded
   // into b3c = k3m*H/(1+MgATP/Kmgatp)
   const G H_Khp = q.b3c * (G)((1.0 + k::MgATP / k::Kmgatp) / (k::k3m * k::Khp));
   const G PP = P::dv((G)k::eP, (one + H_Khp + nai_g * (G)(1.0 / k::Knap) + ki_g * (G)(1.0 / k::Kxkur)));
   const G b3 = q.b3c * PP;
-  const G a1 = P::dv(((G)k::k1p * p3(P::dv(nai_g, Knai))), nak_den_i);
-  const G b2 = P::dv(((G)k::k2m * p3(P::dv((G)k::nao, Knao))), nak_den_o);
+  const G a1 = P::dv(((G)k::k1p * p3(nai_Knai)), nak_den_i);
+  const G b2 = P::dv(((G)k::k2m * p3(nao_Knao)), nak_den_o);
   const G b4 = P::dv(((G)k::k4m * p2(ki_g * (G)(1.0 / k::Kki))), nak_den_i);
   const G x1 = (G)k::a4 * a1 * (G)k::a2 + b2 * b4 * b3 + (G)k::a2 * b4 * b3 + b3 * a1 * (G)k::a2;
   const G x2 = b2 * (G)k::b1 * b4 + a1 * (G)k::a2 * a3 + a3 * (G)k::b1 * b4 + (G)k::a2 * a3 * b4;
@@ -376,10 +399,12 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
                                        double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
   const G v = c.v, one = (G)1;
-  const G ass = P::rc((one + P::ex(-(v - (G)14.34) * (G)(1.0 / 14.82))));
+  const G e_a = P::ex(-(v - (G)14.34) * (G)(1.0 / 14.82));
+  const G ass = P::rc((one + e_a));
   const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + P::ex(-(v - (G)18.4099) * (G)(1.0 / 29.3814))))) +
                             P::dv((G)3.5, (one + P::ex((v + (G)100.0) * (G)(1.0 / 29.3814))))));
-  const G assp = P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
+  const G assp = P::kMixed ? P::rc(one + e_a * (G)k::assp_shift)
+                           : P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
   const G iss = P::rc((one + P::ex((v + (G)43.94) * (G)(1.0 / 5.711))));
   const G delta_epi = q.celltype == 1 ? one - P::dv((G)0.95, (one + P::ex((v + (G)70.0) * (G)0.2))) : one;
   const G tiF = ((G)4.562 + P::rc(((G)0.3933 * P::ex(-(v + (G)100.0) * (G)0.01) +
@@ -399,7 +424,8 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const Tau<P> txk1 =
       tau_quot<P>(122.2, (P::ex(-(v + (G)127.2) * (G)(1.0 / 20.36)) + P::ex((v + (G)236.8) * (G)(1.0 / 69.33))));
   const G fp_ = c.fCaMKp;
-  const G EK = (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
+  const G EK = P::kMixed ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+                         : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
   const G AiF = P::rc((one + P::ex((v - (G)213.6) * (G)(1.0 / 151.2))));
   const G AiS = one - AiF;
   const G i_ = AiF * (G)y.iF + AiS * (G)y.iS;
@@ -636,7 +662,8 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
   G IKr = (G)0;
   if constexpr (kCipa) {
     // dynamic hERG: IKr = GKr sqrt(ko/5.4) O (V - EK) (ohara_rudy_cipa_v1_2017.cpp:2307)
-    const G EK = (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
+    const G EK = P::kMixed ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+                           : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
     IKr = q.GKr * (G)k::sqrt_ko54 * (G)y.O * (v - EK);
   }
   o.f[S_iV] = INaCa_i + INaCa_ss + IKr;
