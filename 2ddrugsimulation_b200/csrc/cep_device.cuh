@@ -125,6 +125,21 @@ __device__ __forceinline__ Tau<P> tau_scaled(Tau<P> t, double s) {
   if constexpr (P::kMixed) return {t.v * (G)(1.0 / s)};
   else return {(G)s * t.v};
 }
+// tau = (c + 1/sum) * s (c a constant, s = 1 unless given): F64 as written;
+// Mixed 1/tau = sum / ((c sum + 1) s), one SFU division for the two the
+// written form takes
+template <class P>
+__device__ __forceinline__ Tau<P> tau_affine(double c, typename P::G sum, typename P::G s = (typename P::G)1) {
+  using G = typename P::G;
+  if constexpr (P::kMixed) return {P::dv(sum, ((G)c * sum + (G)1) * s)};
+  else return {((G)c + P::rc(sum)) * s};
+}
+// tau * s for a computed s: F64 s * tau; Mixed (1/tau) / s
+template <class P>
+__device__ __forceinline__ Tau<P> tau_times(Tau<P> t, typename P::G s) {
+  if constexpr (P::kMixed) return {P::dv(t.v, s)};
+  else return {s * t.v};
+}
 // a constant tau
 template <class P>
 __device__ __forceinline__ Tau<P> tau_const(double tau) {

@@ -321,7 +321,7 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
                        (G)6.149 * P::ex((v + (G)0.5096) * (G)(1.0 / 20.27))));
   const Tau<P> ths = tau_quot<P>(1.0, ((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
                        (G)0.3343 * P::ex((v + (G)5.73) * (G)(1.0 / 56.66))));
-  const G tj = (G)2.038 + P::rc(((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
+  const Tau<P> tj = tau_affine<P>(2.038, ((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
                                  (G)0.3052 * P::ex((v + (G)0.9941) * (G)(1.0 / 38.45))));
   static_assert(k::hssV1 == 82.9 && k::hssV2 == 6.086, "hssp_shift assumes hss = 1/(1+e^((V+82.9)/6.086))");
   const G hssp = P::kMixed ? P::rc(one + e_hss * (G)k::hssp_shift)
@@ -386,7 +386,7 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
   y.j = rush_larsen<P, true>(y.j, hss, tj, dt);
   y.hsp = rush_larsen<P, true>(y.hsp, hssp, tau_scaled<P>(ths, 3.0), dt);
-  y.jp = rush_larsen<P, true>(y.jp, hss, (G)1.46 * tj, dt);
+  y.jp = rush_larsen<P, true>(y.jp, hss, tau_scaled<P>(tj, 1.46), dt);
   y.mL = rush_larsen<P>(y.mL, mLss, tm, dt);
   y.hL = rush_larsen<P, true>(y.hL, hLss, tau_const<P>(k::thL), dt);
   y.hLp = rush_larsen<P, true>(y.hLp, hLssp, tau_const<P>(k::thLp), dt);
@@ -407,16 +407,16 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
                            : P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
   const G iss = P::rc((one + P::ex((v + (G)43.94) * (G)(1.0 / 5.711))));
   const G delta_epi = q.celltype == 1 ? one - P::dv((G)0.95, (one + P::ex((v + (G)70.0) * (G)0.2))) : one;
-  const G tiF = ((G)4.562 + P::rc(((G)0.3933 * P::ex(-(v + (G)100.0) * (G)0.01) +
-                                   (G)0.08004 * P::ex((v + (G)50.0) * (G)(1.0 / 16.59))))) * delta_epi;
-  const G tiS = ((G)23.62 + P::rc(((G)0.001416 * P::ex(-(v + (G)96.52) * (G)(1.0 / 59.05)) +
-                                   (G)1.78e-08 * P::ex((v + (G)114.1) * (G)(1.0 / 8.079))))) * delta_epi;
+  const Tau<P> tiF = tau_affine<P>(4.562, ((G)0.3933 * P::ex(-(v + (G)100.0) * (G)0.01) +
+                                            (G)0.08004 * P::ex((v + (G)50.0) * (G)(1.0 / 16.59))), delta_epi);
+  const Tau<P> tiS = tau_affine<P>(23.62, ((G)0.001416 * P::ex(-(v + (G)96.52) * (G)(1.0 / 59.05)) +
+                                            (G)1.78e-08 * P::ex((v + (G)114.1) * (G)(1.0 / 8.079))), delta_epi);
   const G dti_develop = (G)1.354 + P::dv((G)1e-4, (P::ex((v - (G)167.4) * (G)(1.0 / 15.89)) +
                                               P::ex(-(v - (G)12.23) * (G)(1.0 / 0.2154))));
   const G dti_recover = one - P::dv((G)0.5, (one + P::ex((v + (G)70.0) * (G)0.05)));
   const G dti = dti_develop * dti_recover;
   const G xs1ss = P::rc((one + P::ex(-(v + (G)11.60) * (G)(1.0 / 8.932))));
-  const G txs1 = (G)817.3 + P::rc(((G)2.326e-04 * P::ex((v + (G)48.28) * (G)(1.0 / 17.80)) +
+  const Tau<P> txs1 = tau_affine<P>(817.3, ((G)2.326e-04 * P::ex((v + (G)48.28) * (G)(1.0 / 17.80)) +
                                    (G)0.001292 * P::ex(-(v + (G)210.0) * (G)(1.0 / 230.0))));
   const Tau<P> txs2 =
       tau_quot<P>(1.0, ((G)0.01 * P::ex((v - (G)50.0) * (G)0.05) + (G)0.0193 * P::ex(-(v + (G)66.54) * (G)(1.0 / 31.0))));
@@ -431,12 +431,13 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const G i_ = AiF * (G)y.iF + AiS * (G)y.iS;
   const G ip = AiF * (G)y.iFp + AiS * (G)y.iSp;
   const G Ito = q.Gto * (v - EK) * ((one - fp_) * (G)y.a * i_ + fp_ * (G)y.ap * ip);
-  G IKr = (G)0, xrss = (G)0, txrf = (G)1, txrs = (G)1;
+  G IKr = (G)0, xrss = (G)0;
+  Tau<P> txrf = tau_const<P>(1.0), txrs = tau_const<P>(1.0);
   if constexpr (!kCipa) {
     xrss = P::rc((one + P::ex(-(v + (G)8.337) * (G)(1.0 / 6.789))));
-    txrf = (G)12.98 + P::rc(((G)0.3652 * P::ex((v - (G)31.66) * (G)(1.0 / 3.869)) +
+    txrf = tau_affine<P>(12.98, ((G)0.3652 * P::ex((v - (G)31.66) * (G)(1.0 / 3.869)) +
                              (G)4.123e-05 * P::ex(-(v - (G)47.78) * (G)(1.0 / 20.38))));
-    txrs = (G)1.865 + P::rc(((G)0.06629 * P::ex((v - (G)34.70) * (G)(1.0 / 7.355)) +
+    txrs = tau_affine<P>(1.865, ((G)0.06629 * P::ex((v - (G)34.70) * (G)(1.0 / 7.355)) +
                              (G)1.128e-05 * P::ex(-(v - (G)29.74) * (G)(1.0 / 25.94))));
     const G Axrf = P::rc((one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21))));
     const G xr = Axrf * (G)y.xrf + (one - Axrf) * (G)y.xrs;
@@ -462,8 +463,8 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
   y.iS = rush_larsen<P, true>(y.iS, iss, tiS, dt);
   y.ap = rush_larsen<P, true>(y.ap, assp, ta, dt);
-  y.iFp = rush_larsen<P, true>(y.iFp, iss, dti * tiF, dt);
-  y.iSp = rush_larsen<P, true>(y.iSp, iss, dti * tiS, dt);
+  y.iFp = rush_larsen<P, true>(y.iFp, iss, tau_times<P>(tiF, dti), dt);
+  y.iSp = rush_larsen<P, true>(y.iSp, iss, tau_times<P>(tiS, dti), dt);
   y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
   y.xs2 = rush_larsen<P, true>(y.xs2, xs1ss, txs2, dt);
   y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
@@ -481,14 +482,14 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   const G dss = P::rc((one + P::ex(-(v + (G)3.94) * (G)(1.0 / 4.23))));
-  const G td = (G)0.6 + P::rc((P::ex((G)-0.05 * (v + (G)6.0)) + P::ex((G)0.09 * (v + (G)14.0))));
+  const Tau<P> td = tau_affine<P>(0.6, (P::ex((G)-0.05 * (v + (G)6.0)) + P::ex((G)0.09 * (v + (G)14.0))));
   const G fss = P::rc((one + P::ex((v + (G)19.58) * (G)(1.0 / 3.696))));
-  const G tff = (G)7.0 + P::rc(((G)0.0045 * P::ex(-(v + (G)20.0) * (G)0.1) + (G)0.0045 * P::ex((v + (G)20.0) * (G)0.1)));
-  const G tfs = (G)1000.0 + P::rc(((G)3.5e-05 * P::ex(-(v + (G)5.0) * (G)0.25) +
+  const Tau<P> tff = tau_affine<P>(7.0, ((G)0.0045 * P::ex(-(v + (G)20.0) * (G)0.1) + (G)0.0045 * P::ex((v + (G)20.0) * (G)0.1)));
+  const Tau<P> tfs = tau_affine<P>(1000.0, ((G)3.5e-05 * P::ex(-(v + (G)5.0) * (G)0.25) +
                                    (G)3.5e-05 * P::ex((v + (G)5.0) * (G)(1.0 / 6.0))));
-  const G tfcaf = (G)7.0 + P::rc(((G)0.04 * P::ex(-(v - (G)4.0) * (G)(1.0 / 7.0)) +
+  const Tau<P> tfcaf = tau_affine<P>(7.0, ((G)0.04 * P::ex(-(v - (G)4.0) * (G)(1.0 / 7.0)) +
                                   (G)0.04 * P::ex((v - (G)4.0) * (G)(1.0 / 7.0))));
-  const G tfcas = (G)100.0 + P::rc(((G)0.00012 * P::ex(-v * (G)(1.0 / 3.0)) + (G)0.00012 * P::ex(v * (G)(1.0 / 7.0))));
+  const Tau<P> tfcas = tau_affine<P>(100.0, ((G)0.00012 * P::ex(-v * (G)(1.0 / 3.0)) + (G)0.00012 * P::ex(v * (G)(1.0 / 7.0))));
   const G km2n = (G)y.jca;
   const G cass_g = (G)y.cass, cai_g = (G)y.cai, cajsr_g = (G)y.cajsr;
   const G anca = P::rc((P::dv((G)k::k2n, km2n) + p4(one + P::dv((G)k::Kmn, cass_g))));
@@ -537,13 +538,13 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   y.fcaf = rush_larsen<P, true>(y.fcaf, fss, tfcaf, dt);
   y.fcas = rush_larsen<P, true>(y.fcas, fss, tfcas, dt);
   y.jca = rush_larsen<P, true>(y.jca, fss, q.tjca, dt);
-  y.ffp = rush_larsen<P, true>(y.ffp, fss, (G)2.5 * tff, dt);
+  y.ffp = rush_larsen<P, true>(y.ffp, fss, tau_scaled<P>(tff, 2.5), dt);
   // quirk (1): the reference steps fcafp by d = 25 (exp(-25/tfcafp)), far
   // outside the Taylor range, so that case takes the exponential form
   if (q.fcafp_dt != (G)0)
-    y.fcafp = rush_larsen<P>(y.fcafp, fss, (G)2.5 * tfcaf, (double)q.fcafp_dt);
+    y.fcafp = rush_larsen<P>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), (double)q.fcafp_dt);
   else
-    y.fcafp = rush_larsen<P, true>(y.fcafp, fss, (G)2.5 * tfcaf, dt);
+    y.fcafp = rush_larsen<P, true>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), dt);
   // nca relaxes at rate km2n towards anca*k2n/km2n (Ohara_Rudy_2011.cpp:1065-1066)
   y.nca = rush_larsen<P, true>(y.nca, anca * P::dv((G)k::k2n, km2n), tau_quot<P>(1.0, km2n), dt);
   y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, dt);
