@@ -67,7 +67,12 @@ template <class T> __device__ __forceinline__ T p4(T x) { T y = x * x; return y 
 template <class T> __device__ __forceinline__ T p8(T x) { T y = x * x; y = y * y; return y * y; }
 
 // x / (e^x - 1), the Goldman-Hodgkin-Katz factor, evaluated without the
-// cancellation the direct form suffers for |x| -> 0 (series below 1e-3).
+// cancellation the direct form suffers for |x| -> 0 (series below 1e-3);
+// ghk_factor_e takes e = e^x already at hand.
+__device__ __forceinline__ float ghk_factor_e(float x, float e) {
+  if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x + x * x * (1.0f / 12.0f);
+  return __fdividef(x, e - 1.0f);
+}
 __device__ __forceinline__ float ghk_factor(float x) {
   if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x + x * x * (1.0f / 12.0f);
   return __fdividef(x, __expf(x) - 1.0f);

@@ -101,6 +101,8 @@ constexpr double a3c = k3p * (ko / Kko) * (ko / Kko), ko_Kko_sq = (1.0 + ko / Kk
 // and log(c_o/c_i) = log(c_o) - log(c_i) for ENa and EK.
 constexpr double hssp_shift = 2.769679238039406, hLssp_shift = 2.288717124596483, assp_shift = 1.9635691902911017;
 constexpr double log_nao = 4.941642422609304, log_ko = 1.6863989535702288;
+// log(ko + PKNa nao) for EKs, log(3.8e-5) for the IKs calcium factor
+constexpr double log_ks_o = 2.0752075911477745, log_ks_ca = -10.177924398237888;
 }  // namespace k
 
 template <class G>
@@ -272,9 +274,12 @@ __device__ __forceinline__ Ctx<typename P::G> context(const Y<typename P::G> &y,
   using G = typename P::G;
   Ctx<G> c;
   c.v = (G)y.V;
-  const G CaMKb = P::dv(((G)k::CaMKo * ((G)1 - (G)y.CaMKt)), ((G)1 + P::dv((G)k::KmCaM, (G)y.cass)));
+  // mixed: a/(1 + K/c) as a c/(c + K), one division for two
+  const G cass = (G)y.cass;
+  const G CaMKb = P::kMixed ? P::dv((G)k::CaMKo * ((G)1 - (G)y.CaMKt) * cass, cass + (G)k::KmCaM)
+                            : P::dv(((G)k::CaMKo * ((G)1 - (G)y.CaMKt)), ((G)1 + P::dv((G)k::KmCaM, cass)));
   const G CaMKa = CaMKb + (G)y.CaMKt;
-  c.fCaMKp = P::rc(((G)1 + P::dv((G)k::KmCaMK, CaMKa)));
+  c.fCaMKp = P::kMixed ? P::dv(CaMKa, CaMKa + (G)k::KmCaMK) : P::rc(((G)1 + P::dv((G)k::KmCaMK, CaMKa)));
   c.stim = stim_mode < 0 ? stim_on(t, q.stim_start, q.BCL, q.duration) : (stim_mode != 0);
   return c;
 }
@@ -290,7 +295,7 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
   if constexpr (P::kMixed) {
     const G x = (G)z * v * (G)k::FRT;
     e = P::ex(x);
-    fac = ghk_factor(x) * (G)k::F / (G)z;  // = vffrt / (e^{z vfrt} - 1)
+    fac = ghk_factor_e(x, e) * (G)k::F / (G)z;  // = vffrt / (e^{z vfrt} - 1)
   } else if constexpr (kCipa) {
     const double ffrt = k::F * k::FRT, B = (double)z * k::FRT;
     const double U = B * V;
@@ -441,11 +446,18 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
                              (G)1.128e-05 * P::ex(-(v - (G)29.74) * (G)(1.0 / 25.94))));
     const G Axrf = P::rc((one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21))));
     const G xr = Axrf * (G)y.xrf + (one - Axrf) * (G)y.xrs;
-    const G rkr = P::dv((P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))))), (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0))));
+    const G rkr = P::kMixed ? P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))) *
+                                    (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0))))
+                            : P::dv((P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))))),
+                                    (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0))));
     IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
   }
-  const G EKs = (G)k::RTF * P::lg(P::dv((G)(k::ko + k::PKNa * k::nao), (G)(y.ki + k::PKNa * y.nai)));
-  const G KsCa = one + P::dv((G)0.6, (one + P::pw(P::dv((G)3.8e-05, (G)y.cai), (G)1.4)));
+  const G EKs = P::kMixed
+                    ? (G)k::RTF * ((G)k::log_ks_o - P::lg((G)(y.ki + k::PKNa * y.nai)))
+                    : (G)k::RTF * P::lg(P::dv((G)(k::ko + k::PKNa * k::nao), (G)(y.ki + k::PKNa * y.nai)));
+  const G KsCa = P::kMixed
+                     ? one + P::dv((G)0.6, (one + P::ex((G)1.4 * ((G)k::log_ks_ca - P::lg((G)y.cai)))))
+                     : one + P::dv((G)0.6, (one + P::pw(P::dv((G)3.8e-05, (G)y.cai), (G)1.4)));
   const G IKs = q.GKs * KsCa * (G)y.xs1 * (G)y.xs2 * (v - EKs);
   const G rk1 = P::rc((one + P::ex(((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493))));
   const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
@@ -505,7 +517,13 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   const G gate_p = d_ * (fp * (one - nca_) + jca_ * fcap * nca_);
   G fac1, e1, fac2, e2;
   ghk<P, kCipa, 1>(y.V, v, fac1, e1);
-  ghk<P, kCipa, 2>(y.V, v, fac2, e2);
+  if constexpr (P::kMixed) {  // e^{2x} = (e^x)^2
+    const G x2 = (G)2 * v * (G)k::FRT;
+    e2 = e1 * e1;
+    fac2 = ghk_factor_e(x2, e2) * (G)k::F / (G)2;
+  } else {
+    ghk<P, kCipa, 2>(y.V, v, fac2, e2);
+  }
   const G PhiCaL = (G)4.0 * fac2 * (cass_g * e2 - (G)(0.341 * k::cao));
   const G PhiCaNa = fac1 * ((G)0.75 * (G)y.nass * e1 - (G)(0.75 * k::nao));
   const G PhiCaK = fac1 * ((G)0.75 * (G)y.kss * e1 - (G)(0.75 * k::ko));
@@ -524,14 +542,25 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   o.f[S_ICaL] = ICaL;
   if (!update) return;
   const G rel_den = one + p8(P::dv((G)1.5, cajsr_g));
-  const G Jrel_inf_t = P::dv(((G)k::a_rel * -ICaL), rel_den);
+  const G den_tau = one + P::dv((G)0.0123, cajsr_g);
+  G Jrel_inf_t, Jrel_t;
+  Tau<P> tau_rel, tau_relp;  // bt / den_tau, floored at 0.001 ms
+  if constexpr (P::kMixed) {  // one reciprocal for both targets; rates capped at 1000 /ms
+    const G r = P::rc(rel_den);
+    Jrel_inf_t = (G)k::a_rel * -ICaL * r;
+    Jrel_t = (G)k::a_relp * -ICaL * r;
+    const G r1 = den_tau * (G)(1.0 / k::bt), r2 = den_tau * (G)(1.0 / k::btp);
+    tau_rel = Tau<P>{r1 > (G)1000 ? (G)1000 : r1};
+    tau_relp = Tau<P>{r2 > (G)1000 ? (G)1000 : r2};
+  } else {
+    Jrel_inf_t = P::dv(((G)k::a_rel * -ICaL), rel_den);
+    Jrel_t = P::dv(((G)k::a_relp * -ICaL), rel_den);
+    const G t1 = P::dv((G)k::bt, den_tau), t2 = P::dv((G)k::btp, den_tau);
+    tau_rel = Tau<P>{t1 < (G)0.001 ? (G)0.001 : t1};
+    tau_relp = Tau<P>{t2 < (G)0.001 ? (G)0.001 : t2};
+  }
   const G Jrel_inf = q.celltype == 2 ? Jrel_inf_t * (G)1.7 : Jrel_inf_t;
-  const G tau_rel_t = P::dv((G)k::bt, (one + P::dv((G)0.0123, cajsr_g)));
-  const G tau_rel = tau_rel_t < (G)0.001 ? (G)0.001 : tau_rel_t;
-  const G Jrel_t = P::dv(((G)k::a_relp * -ICaL), rel_den);
   const G Jrel_infp = q.celltype == 2 ? Jrel_t * (G)1.7 : Jrel_t;
-  const G tau_relp_t = P::dv((G)k::btp, (one + P::dv((G)0.0123, cajsr_g)));
-  const G tau_relp = tau_relp_t < (G)0.001 ? (G)0.001 : tau_relp_t;
   y.d = rush_larsen<P, true>(y.d, dss, td, dt);
   y.ff = rush_larsen<P, true>(y.ff, fss, tff, dt);
   y.fs = rush_larsen<P, true>(y.fs, fss, tfs, dt);
@@ -562,14 +591,23 @@ __device__ __forceinline__ typename P::G naca(typename P::G na, typename P::G ca
   using G = typename P::G;
   const G one = (G)1;
   const G h1 = one + ((na) * (G)(1.0 / k::kna3)) * (one + hna);
-  const G h2 = P::dv((na * hna), ((G)k::kna3 * h1));
-  const G k4pp = h2 * (G)k::wnaca;
   const G h4 = one + ((na) * (G)(1.0 / k::kna1)) * (one + (na) * (G)(1.0 / k::kna2));
-  const G h5 = P::dv((na * na), (h4 * (G)k::kna1 * (G)k::kna2));
+  G h2, h5, k4p, k6;
+  if constexpr (P::kMixed) {  // 1/h1, 1/h4 (and 1/hca, shared by both compartments) each once
+    const G rh1 = P::rc(h1), rh4 = P::rc(h4);
+    h2 = na * hna * (G)(1.0 / k::kna3) * rh1;
+    h5 = na * na * (G)(1.0 / (k::kna1 * k::kna2)) * rh4;
+    k4p = rh1 * (G)k::wca * P::rc(hca);
+    k6 = rh4 * ca * (G)k::kcaon;
+  } else {
+    h2 = P::dv((na * hna), ((G)k::kna3 * h1));
+    h5 = P::dv((na * na), (h4 * (G)k::kna1 * (G)k::kna2));
+    k4p = P::dv(((P::rc(h1)) * (G)k::wca), hca);
+    k6 = (P::rc(h4)) * ca * (G)k::kcaon;
+  }
+  const G k4pp = h2 * (G)k::wnaca;
   const G k7 = h5 * h2 * (G)k::wna;
-  const G k4p = P::dv(((P::rc(h1)) * (G)k::wca), hca);
   const G k4 = k4p + k4pp;
-  const G k6 = (P::rc(h4)) * ca * (G)k::kcaon;
   const G x1 = (G)k::k2x * k4 * (k7 + k6) + (G)k::k5x * k7 * ((G)k::k2x + k3);
   const G x2 = (G)k::k1x * k7 * (k4 + (G)k::k5x) + k4 * k6 * ((G)k::k1x + k8);
   const G x3 = (G)k::k1x * k3 * (k7 + k6) + k8 * k6 * ((G)k::k2x + k3);
