@@ -1,0 +1,65 @@
+"""Size-independent properties at the full sizes of the tissue workloads:
+the 512 x 512 TT2006 sheet with a corner S1 (a mirror-symmetric problem, so
+its solution must be symmetric about the diagonal) and the diffusion
+operators of that sheet and of the 256 x 256 x 48 anisotropic slab (the
+implicit step conserves 1^T M V: K has zero row sums, so
+1^T A V_new = 1^T M V_old / dt up to the solver's residual). The oracle
+checks the same code paths at sizes it finishes in seconds."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+@pytest.mark.gpu
+def test_sheet_512_corner_stimulus_is_mirror_symmetric(cep, gpu):
+    nx = ny = 512
+    n = nx * ny
+    cells = cep.Batch("tt2006", n, "fp64")
+    cells.init()
+    fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(1e-8)
+    t = cep.Tissue(cells, fem, 0.01)
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:8, :8] = 1
+    t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 1)
+    t.run(1500)
+    assert t.stats()["not_converged"] == 0
+    v = t.v().reshape(ny, nx)
+    act = t.activation().reshape(ny, nx)
+    assert np.isfinite(v).all()
+    # the wave has left the stimulus square but not crossed the sheet
+    activated = act > 0
+    assert activated[:8, :8].all() and activated.sum() > 4 * 64 and not activated[-1, -1]
+    assert np.abs(v - v.T).max() <= 1e-6, np.abs(v - v.T).max()
+    assert np.array_equal(act, act.T)
+
+
+def _rotated_tensor(n_elem: int, angle_deg: float, dl: float, dt_: float) -> np.ndarray:
+    a = np.deg2rad(angle_deg)
+    f = np.array([np.cos(a), np.sin(a), 0.0])
+    D = dt_ * np.eye(3) + (dl - dt_) * np.outer(f, f)
+    row = np.array([D[0, 0], D[0, 1], D[0, 2], D[1, 1], D[1, 2], D[2, 2]])
+    return np.ascontiguousarray(np.broadcast_to(row, (n_elem, 6)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,shape", [(2, (512, 512, 1)), (3, (256, 256, 48))], ids=["sheet512", "slab256x256x48"])
+def test_full_size_implicit_step_conserves_charge(cep, gpu, dim, shape):
+    nx, ny, nz = shape
+    dt, rtol = 0.01, 1e-10
+    if dim == 2:
+        D = 0.0013
+    else:
+        D = _rotated_tensor((nx - 1) * (ny - 1) * (nz - 1), 30.0, 0.0013, 0.00045)
+    fem = cep.Fem.grid(dim, nx, ny, nz, 0.025, dt, D).set_solver(rtol, 10000, precond_norm=False)
+    n = nx * ny * nz
+    rng = np.random.default_rng(17)
+    v0 = rng.uniform(-85.0, 20.0, n)
+    b = fem.spmv(v0, "B") / dt
+    v1, iters, res = fem.solve(v0)
+    assert 0 < iters < 10000 and res <= rtol
+    q0, q1 = b.sum() * dt, fem.spmv(v1, "B").sum()
+    # |1^T r| <= sqrt(n) ||r|| <= sqrt(n) rtol ||b||, and q1 - q0 = -dt 1^T r
+    bound = dt * np.sqrt(n) * rtol * np.linalg.norm(b)
+    assert abs(q1 - q0) <= 1.01 * bound + 1e-12 * abs(q0), (q1 - q0, bound)
+    assert np.isfinite(v1).all() and np.abs(v1 - v0).max() > 0
