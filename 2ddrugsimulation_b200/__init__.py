@@ -372,7 +372,8 @@ class Batch:
         cnt = ctypes.c_int()
         _check(lib().cep_batch_restitution(self._h, _dptr(b), len(b), int(n_pace), float(dt), int(steps_per_launch),
                                            arr, m, ctypes.byref(cnt)))
-        assert cnt.value == m
+        if cnt.value != m:
+            raise CepError(ERR_STATE, f"restitution produced {cnt.value} records per instance, expected {m}")
         raw = np.ctypeslib.as_array(arr)[: self.n * m].reshape(self.n, m)
         return {f: np.array(raw[f]) for f in APDR_FIELDS}
 
