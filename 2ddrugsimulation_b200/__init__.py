@@ -410,6 +410,48 @@ def apdr_bcls(bcl_init: float, bcl_end: float, bcl_decrement: float) -> list[flo
     return out
 
 
+def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, first_pace: int,
+                   precision: str = "mixed", celltype=None, dutta: bool = False, quirks: bool = True,
+                   dt_write: float = 1.0, refine_above_vm: float | None = -80.0,
+                   steps_per_launch: int = 50000) -> dict[str, np.ndarray]:
+    """A population run to the end of its protocol (the reference's bench loop
+    for every instance), returning the biomarker records.
+
+    With precision "mixed" and refine_above_vm set, the instances whose mixed
+    diastolic Vm stays above refine_above_vm (drug-depolarised cells that do
+    not repolarise: their 90 % level is crossed at ~0.1 mV/ms, so their APD90
+    moves by tenths of a ms under perturbations of 1e-5 and FP32 gates cannot
+    hold it to 0.1 ms) are run again in FP64 from their initial state and
+    their records replaced; out["refined"] marks them."""
+    conc = np.ascontiguousarray(conc, np.float64)
+    n = len(conc)
+    hill = np.asarray(hill, np.float64)
+    ct = None if celltype is None else np.ascontiguousarray(np.broadcast_to(celltype, (n,)), np.float64)
+
+    def run(prec, idx):
+        b = Batch(model, len(idx), prec)
+        try:
+            b.init(celltype=None if ct is None else ct[idx], conc=conc[idx],
+                   hill=hill[idx] if hill.ndim == 2 else hill, dutta=dutta, quirks=quirks)
+            b.set_pacing(bcl)
+            b.set_protocol(dt, n_pace, first_pace, dt_write=dt_write)
+            b.run_to_end(steps_per_launch)
+            return b.biomarkers()
+        finally:
+            b.close()
+
+    out = run(precision, np.arange(n))
+    out["refined"] = np.zeros(n, bool)
+    if precision == "mixed" and refine_above_vm is not None:
+        idx = np.flatnonzero(~(out["vm_valley"] < refine_above_vm))
+        if len(idx):
+            ref = run("fp64", idx)
+            for k, v in ref.items():
+                out[k][idx] = v
+            out["refined"][idx] = True
+    return out
+
+
 def qinward(control: Biomarkers, drug: Biomarkers) -> float:
     return float(lib().cep_qinward(ctypes.byref(control), ctypes.byref(drug)))
 

@@ -103,3 +103,20 @@ def test_cipa_full_population_mixed_within_bars_of_fp64(cep, gpu):
     assert d_q[rep].max() <= 0.01, d_q[rep].max()
     assert d_apd[~rep].max() <= 1.0 and d_cad[~rep].max() <= 1.0 + 1e-9
     assert d_q.max() <= 0.01
+
+
+@pytest.mark.gpu
+def test_cipa_full_population_refined_mixed_meets_bars(cep, gpu):
+    """run_population in mixed precision with the FP64 re-run of the
+    non-repolarising instances: every one of the 10,000 instances within
+    the bars of the all-FP64 run."""
+    from test_cipa_gpu import cipa_population
+    conc, hill = cipa_population(2000, 5, seed=1234)
+    kw = dict(bcl=2000.0, dt=0.005, n_pace=2, first_pace=1)
+    f = cep.run_population("cipa2017", conc, hill, precision="fp64", **kw)
+    m = cep.run_population("cipa2017", conc, hill, precision="mixed", **kw)
+    assert 0 < m["refined"].sum() < 0.05 * len(conc)
+    assert (m["status"] == cep.INST_DONE).all()
+    assert np.abs(m["apd90"] - f["apd90"]).max() <= 0.1
+    assert np.abs(m["cad90"] - f["cad90"]).max() <= 0.1
+    assert (np.abs(m["qnet"] - f["qnet"]) / np.maximum(np.abs(f["qnet"]), 1e-3)).max() <= 0.01
