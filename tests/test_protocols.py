@@ -60,20 +60,36 @@ def test_oracle_restitution_properties(oracle, cep):
     assert (r["apd90"][:2] > re_["apd90"]).all()
 
 
-def test_oracle_clamp_replays_a_free_run(oracle):
-    """Clamping V to the trace a free run produced reproduces that run."""
-    free = oracle.Cell("ord2011")
-    n, dt = 400, 0.005
-    v, cur = np.zeros(n), np.zeros(n)
+@pytest.mark.parametrize("model", ["ord2011", "cipa2017", "tt2006", "tt2004", "tomek2019"])
+def test_oracle_clamp_replays_a_free_run(oracle, model):
+    """Clamping V to the trace a free run produced reproduces that run
+    (through the stimulus, so the upstroke is included)."""
+    free = oracle.Cell(model)
+    n, dt = 3000, 0.005
+    v, cur = np.zeros(n), np.zeros((n, 2))
     t = 0.0
     for k in range(n):
         v[k] = free.y[0]
-        cur[k] = free.step(t, dt).ICaL
+        c_ = free.step(t, dt)
+        cur[k] = c_.ICaL, c_.IKr
         t += dt
-    c = oracle.Cell("ord2011")
-    out = c.clamp(v, 0.0, dt, 3)
-    assert np.array_equal(out, cur)
-    assert np.array_equal(c.states[1:], free.states[1:])
+    for j, idx in enumerate((3, 4)):
+        c = oracle.Cell(model)
+        out = c.clamp(v, 0.0, dt, idx)
+        assert np.array_equal(out, cur[:, j])
+        assert np.array_equal(c.states[1:], free.states[1:])
+    assert v.max() > 0  # the stimulus fired inside the window
+
+
+@pytest.mark.parametrize("bcls,n_pace,dt", [([500.0], 4, 0.03), ([410.0, 333.0], 3, 0.007), ([400.0], 2, 0.02),
+                                            ([400.0], 1, 0.02)])
+def test_oracle_restitution_record_count(oracle, cep, bcls, n_pace, dt):
+    """The record count of the host formula (pace boundaries among
+    iout = 1 .. (int)(n_pace*bcl/dt) + 1, minus two per BCL) against the
+    oracle's loop, with bcl/dt not an integer and with n_pace <= 2."""
+    r, st = oracle.Cell("tt2004").restitution(bcls, n_pace, dt)
+    assert st == 0
+    assert len(r["pace"]) == cep.restitution_records(bcls, n_pace, dt)
 
 
 # --------------------------------------------------------------------- GPU
