@@ -114,6 +114,8 @@ _SIGS = {
                                            _dp]),
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
+    "cep_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
     "cep_batch_restitution": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_long, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int)]),
@@ -302,6 +304,13 @@ class Batch:
     def run(self, n_steps: int):
         _check(lib().cep_batch_run(self._h, int(n_steps)))
         return self
+
+    def autotune(self, n_steps: int = 400) -> tuple[str, int]:
+        """Time each kernel form and block size on this batch's instances
+        (state restored after every trial) and keep the fastest."""
+        v, blk = ctypes.c_int(), ctypes.c_int()
+        _check(lib().cep_batch_autotune(self._h, int(n_steps), ctypes.byref(v), ctypes.byref(blk)))
+        return {0: "cell", 1: "roles", 2: "pairs"}[v.value], blk.value
 
     def step(self, t: float, dt: float, stim_mode: int = -1):
         """One step of every instance from time t (computeRates + solveAnalytical)."""

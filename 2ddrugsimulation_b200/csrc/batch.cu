@@ -1013,6 +1013,101 @@ int cep_batch_set_kernel(cep_batch_t b, int variant) {
   return CEP_OK;
 }
 
+int cep_batch_autotune(cep_batch_t b, long n_steps, int *variant_out, int *block_out) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (n_steps <= 0) n_steps = 400;
+  if (n_steps > 100000) return fail(CEP_ERR_ARG, "n_steps out of range (1..100000)");
+  // everything a run launch writes, saved once and put back before each
+  // trial and at the end
+  struct Region {
+    void *p;
+    size_t bytes;
+    void *save;
+  };
+  std::vector<Region> regions = {{b->states, sizeof(double) * (size_t)b->ns * b->ld, nullptr},
+                                 {b->t, sizeof(double) * (size_t)b->ld, nullptr},
+                                 {b->iout, sizeof(int) * (size_t)b->ld, nullptr},
+                                 {b->status, sizeof(int) * (size_t)b->ld, nullptr}};
+  if (b->bmf) {
+    regions.push_back({b->bmf, sizeof(double) * (size_t)bm::kNumF * b->ld, nullptr});
+    regions.push_back({b->bmi, sizeof(int) * (size_t)bm::kNumI * b->ld, nullptr});
+  }
+  if (b->ca_t) {
+    regions.push_back({b->ca_t, sizeof(double) * (size_t)b->ca_cap * b->ld, nullptr});
+    regions.push_back({b->ca_v, sizeof(double) * (size_t)b->ca_cap * b->ld, nullptr});
+  }
+  struct Saved {
+    std::vector<Region> *r;
+    ~Saved() {
+      for (Region &g : *r)
+        if (g.save) cudaFree(g.save);
+    }
+  } saved{&regions};
+  for (Region &g : regions) {
+    if (cudaMalloc(&g.save, g.bytes) != cudaSuccess) {
+      cudaGetLastError();
+      g.save = nullptr;
+      return fail(CEP_ERR_OOM, "autotune: no room to save %zu bytes of batch state", g.bytes);
+    }
+    CEP_CUDA(cudaMemcpyAsync(g.save, g.p, g.bytes, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  auto restore = [&]() -> int {
+    for (Region &g : regions) CEP_CUDA(cudaMemcpyAsync(g.p, g.save, g.bytes, cudaMemcpyDeviceToDevice, b->stream));
+    return CEP_OK;
+  };
+  struct Cand {
+    int variant, block;
+  };
+  std::vector<Cand> cands = {{CEP_KERNEL_CELL, 32}, {CEP_KERNEL_CELL, 64}, {CEP_KERNEL_CELL, 128}};
+  if (b->model == CEP_MODEL_ORD2011 || b->model == CEP_MODEL_CIPA2017) {
+    cands.push_back({CEP_KERNEL_PAIRS, b->block});
+    cands.push_back({CEP_KERNEL_ROLES, b->block});
+  }
+  const int keep_variant = b->variant, keep_block = b->block;
+  cudaEvent_t e0, e1;
+  CEP_CUDA(cudaEventCreate(&e0));
+  CEP_CUDA(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  Cand best{keep_variant, keep_block};
+  int rc = CEP_OK;
+  const ModelInfo *mi = model_info(b->model);
+  for (const Cand &c : cands) {
+    b->variant = c.variant;
+    b->block = c.block;
+    RunArgs a = make_args(b, n_steps);
+    if (!b->has_protocol) a.bm_on = 0;
+    // one untimed launch (code and caches warm), then the timed one, both
+    // from the saved state
+    if ((rc = restore()) || (rc = mi->run(b, a)) || (rc = restore())) break;
+    if (cudaEventRecord(e0, b->stream) != cudaSuccess || (rc = mi->run(b, a)) ||
+        cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      if (!rc) rc = fail(CEP_ERR_CUDA, "autotune trial failed");
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int rc2 = restore();
+  const cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (rc || rc2 || e != cudaSuccess) {
+    b->variant = keep_variant;
+    b->block = keep_block;
+    return rc ? rc : rc2 ? rc2 : fail(CEP_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+  }
+  b->variant = best.variant;
+  b->block = best.block;
+  if (variant_out) *variant_out = best.variant;
+  if (block_out) *block_out = best.block;
+  return CEP_OK;
+}
+
 int cep_batch_size(cep_batch_t b, int *n, int *n_states) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (n) *n = b->n;

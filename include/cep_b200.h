@@ -109,6 +109,15 @@ int cep_batch_set_block(cep_batch_t b, int threads_per_block);
 #define CEP_KERNEL_ROLES 1
 #define CEP_KERNEL_PAIRS 2 /* 2 warps per 32 cells, two channel groups each */
 int cep_batch_set_kernel(cep_batch_t b, int variant);
+/* Launch-shape autotuner (no counterpart in the reference, which runs one
+ * cell per object): times one run of n_steps steps (default 400) in each
+ * kernel form and block size on this batch's own instances and keeps the
+ * fastest. Every array a run writes (states, clocks, status, biomarker
+ * records, Ca ring) is saved first and restored after every trial, so the
+ * batch continues exactly where it was. Blocking; needs room for one copy
+ * of those arrays. The chosen form and block are returned if the pointers
+ * are not NULL. */
+int cep_batch_autotune(cep_batch_t b, long n_steps, int *variant, int *block);
 
 /* initConsts for every instance and the model's initial STATES.
  * celltype[n] (NULL = 0, endo), conc[n] (drug concentration, same unit as

@@ -178,3 +178,33 @@ def test_roles_kernel_matches_cell_kernel(cep, gpu, model, precision):
         for key in ("apd90", "apd50", "cad90"):
             assert np.abs(b0[key] - b1[key]).max() <= 0.01, (kern, key)
         assert np.array_equal(b0["status"], b1["status"]), kern
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_the_batch_state(cep, gpu):
+    """cep_batch_autotune part-way through a protocol: the state, clocks and
+    biomarker bookkeeping continue exactly where they were, and the run
+    then ends within the mixed bars of a batch left on the default form."""
+    conc, hill = cipa_population(100, 5, seed=4)
+
+    def make():
+        b = cep.Batch("cipa2017", len(conc), "mixed")
+        b.init(conc=conc, hill=hill, quirks=True)
+        b.set_pacing(1000.0)
+        b.set_protocol(0.005, 2, 1, dt_write=1.0)
+        return b
+
+    a = make()
+    a.run(30000)
+    s0, clk0 = a.get_states(), a.clock(0)
+    form, block = a.autotune(300)
+    assert form in ("cell", "roles", "pairs") and block in (32, 64, 96, 128)
+    assert np.array_equal(a.get_states(), s0) and a.clock(0) == clk0
+    a.run_to_end(50000)
+    ref = make()
+    ref.run(30000)
+    ref.run_to_end(50000)
+    ba, br = a.biomarkers(), ref.biomarkers()
+    assert (ba["status"] == cep.INST_DONE).all()
+    rep = br["vm_valley"] < -80.0
+    assert np.abs(ba["apd90"] - br["apd90"])[rep].max() <= APD_TOL_MIXED
