@@ -114,6 +114,9 @@ _SIGS = {
                                            _dp]),
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
+    "cep_batch_checkpoint_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "cep_batch_checkpoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "cep_batch_restore": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "cep_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int)]),
     "cep_batch_restitution": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -303,6 +306,19 @@ class Batch:
 
     def run(self, n_steps: int):
         _check(lib().cep_batch_run(self._h, int(n_steps)))
+        return self
+
+    def checkpoint(self) -> bytes:
+        """The whole batch mid-protocol as a self-describing blob."""
+        n = ctypes.c_size_t()
+        _check(lib().cep_batch_checkpoint_size(self._h, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(lib().cep_batch_checkpoint(self._h, buf, n.value))
+        return buf.raw
+
+    def restore(self, blob: bytes) -> "Batch":
+        """Resume from a checkpoint() of a batch of the same model, size and precision."""
+        _check(lib().cep_batch_restore(self._h, blob, len(blob)))
         return self
 
     def autotune(self, n_steps: int = 400) -> tuple[str, int]:

@@ -1108,6 +1108,109 @@ int cep_batch_autotune(cep_batch_t b, long n_steps, int *variant_out, int *block
   return CEP_OK;
 }
 
+// ------------------------------------------------------------ checkpoint
+// Blob layout: CkptHeader, then each device array in the order of
+// ckpt_regions(), each the full [rows][ld] block.
+namespace {
+struct CkptHeader {
+  char magic[8];  // "CEPBATC1"
+  int32_t model, n, ns, np, precision, ca_cap, n_pace, first_pace, variant, block;
+  int32_t initialized, has_protocol, has_bm, reserved;
+  int64_t ld;
+  double dt, dt_write, qnet_thr;
+};
+struct CkptRegion {
+  void *p;
+  size_t bytes;
+};
+std::vector<CkptRegion> ckpt_regions(const cep_batch *b, bool has_bm, int ca_cap) {
+  std::vector<CkptRegion> r = {{b->states, sizeof(double) * (size_t)b->ns * b->ld},
+                               {b->params, sizeof(double) * (size_t)b->np * b->ld},
+                               {b->t, sizeof(double) * (size_t)b->ld},
+                               {b->iout, sizeof(int) * (size_t)b->ld},
+                               {b->status, sizeof(int) * (size_t)b->ld},
+                               {b->sched, sizeof(int) * (size_t)4 * b->ld}};
+  if (has_bm) {
+    r.push_back({b->bmf, sizeof(double) * (size_t)bm::kNumF * b->ld});
+    r.push_back({b->bmi, sizeof(int) * (size_t)bm::kNumI * b->ld});
+  }
+  if (ca_cap > 0) {
+    r.push_back({b->ca_t, sizeof(double) * (size_t)ca_cap * b->ld});
+    r.push_back({b->ca_v, sizeof(double) * (size_t)ca_cap * b->ld});
+  }
+  return r;
+}
+}  // namespace
+
+int cep_batch_checkpoint_size(cep_batch_t b, size_t *bytes) {
+  if (!b || !bytes) return fail(CEP_ERR_ARG, "null argument");
+  size_t total = sizeof(CkptHeader);
+  for (const CkptRegion &g : ckpt_regions(b, b->bmf != nullptr, b->ca_t ? b->ca_cap : 0)) total += g.bytes;
+  *bytes = total;
+  return CEP_OK;
+}
+
+int cep_batch_checkpoint(cep_batch_t b, void *buf, size_t bytes) {
+  if (!b || !buf) return fail(CEP_ERR_ARG, "null argument");
+  size_t need = 0;
+  int rc = cep_batch_checkpoint_size(b, &need);
+  if (rc) return rc;
+  if (bytes < need) return fail(CEP_ERR_ARG, "checkpoint buffer has %zu bytes, needs %zu", bytes, need);
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "CEPBATC1", 8);
+  h.model = b->model; h.n = b->n; h.ns = b->ns; h.np = b->np; h.precision = b->precision;
+  h.ca_cap = b->ca_t ? b->ca_cap : 0; h.n_pace = b->n_pace; h.first_pace = b->first_pace;
+  h.variant = b->variant; h.block = b->block; h.initialized = b->initialized; h.has_protocol = b->has_protocol;
+  h.has_bm = b->bmf != nullptr; h.ld = b->ld; h.dt = b->dt; h.dt_write = b->dt_write; h.qnet_thr = b->qnet_thr;
+  char *out = static_cast<char *>(buf);
+  std::memcpy(out, &h, sizeof(h));
+  size_t off = sizeof(h);
+  for (const CkptRegion &g : ckpt_regions(b, h.has_bm, h.ca_cap)) {
+    CEP_CUDA(cudaMemcpyAsync(out + off, g.p, g.bytes, cudaMemcpyDeviceToHost, b->stream));
+    off += g.bytes;
+  }
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_restore(cep_batch_t b, const void *buf, size_t bytes) {
+  if (!b || !buf) return fail(CEP_ERR_ARG, "null argument");
+  if (bytes < sizeof(CkptHeader)) return fail(CEP_ERR_ARG, "checkpoint too short");
+  CkptHeader h;
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, "CEPBATC1", 8) != 0) return fail(CEP_ERR_ARG, "not a batch checkpoint");
+  if (h.model != b->model || h.n != b->n || h.precision != b->precision || h.ld != b->ld || h.ns != b->ns ||
+      h.np != b->np)
+    return fail(CEP_ERR_ARG, "checkpoint of model %d, %d instances, precision %d does not fit this batch", h.model,
+                h.n, h.precision);
+  if (h.ca_cap < 0 || h.ca_cap > (1 << 24)) return fail(CEP_ERR_ARG, "corrupt checkpoint header");
+  int rc;
+  if (h.has_bm && !b->bmf &&
+      ((rc = dev_alloc(b, &b->bmf, (size_t)bm::kNumF * b->ld)) || (rc = dev_alloc(b, &b->bmi, (size_t)bm::kNumI * b->ld))))
+    return rc;
+  if (h.ca_cap > 0 && (!b->ca_t || b->ca_cap != h.ca_cap)) {
+    if ((rc = dev_alloc(b, &b->ca_t, (size_t)h.ca_cap * b->ld)) || (rc = dev_alloc(b, &b->ca_v, (size_t)h.ca_cap * b->ld)))
+      return rc;
+  }
+  b->ca_cap = h.ca_cap > 0 ? h.ca_cap : b->ca_cap;
+  size_t need = sizeof(CkptHeader);
+  const std::vector<CkptRegion> regs = ckpt_regions(b, h.has_bm, h.ca_cap);
+  for (const CkptRegion &g : regs) need += g.bytes;
+  if (bytes < need) return fail(CEP_ERR_ARG, "checkpoint has %zu bytes, needs %zu", bytes, need);
+  const char *in = static_cast<const char *>(buf);
+  size_t off = sizeof(CkptHeader);
+  for (const CkptRegion &g : regs) {
+    CEP_CUDA(cudaMemcpyAsync(g.p, in + off, g.bytes, cudaMemcpyHostToDevice, b->stream));
+    off += g.bytes;
+  }
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  b->n_pace = h.n_pace; b->first_pace = h.first_pace; b->variant = h.variant; b->block = h.block;
+  b->initialized = h.initialized != 0; b->has_protocol = h.has_protocol != 0;
+  b->dt = h.dt; b->dt_write = h.dt_write; b->qnet_thr = h.qnet_thr;
+  return CEP_OK;
+}
+
 int cep_batch_size(cep_batch_t b, int *n, int *n_states) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (n) *n = b->n;

@@ -167,6 +167,16 @@ int cep_batch_device_states(cep_batch_t b, void **dev_ptr, long *ld);
 
 int cep_batch_get_biomarkers(cep_batch_t b, cep_biomarkers_t *out /* [n] */);
 int cep_batch_get_status(cep_batch_t b, int32_t *status /* [n] */);
+/* Checkpoint / resume of a whole batch mid-protocol (the reference writes
+ * node states to output.<rank> and resumes with iopt = 1, heart.cpp:141,
+ * 595-616, 943-963; this also keeps the clocks, schedules, parameters and
+ * the biomarker state machine with its Ca ring, so a resumed run ends
+ * bit-identical to an uninterrupted one). The blob is self-describing and
+ * restores into a batch created with the same model, size and precision.
+ * Both calls are blocking. */
+int cep_batch_checkpoint_size(cep_batch_t b, size_t *bytes);
+int cep_batch_checkpoint(cep_batch_t b, void *buf, size_t bytes);
+int cep_batch_restore(cep_batch_t b, const void *buf, size_t bytes);
 /* Current step count and time of instance i. */
 int cep_batch_get_clock(cep_batch_t b, int i, long *step, double *t);
 int cep_batch_sync(cep_batch_t b);

@@ -208,3 +208,34 @@ def test_autotune_keeps_the_batch_state(cep, gpu):
     assert (ba["status"] == cep.INST_DONE).all()
     rep = br["vm_valley"] < -80.0
     assert np.abs(ba["apd90"] - br["apd90"])[rep].max() <= APD_TOL_MIXED
+
+
+@pytest.mark.gpu
+def test_checkpoint_resume_is_bit_identical(cep, gpu):
+    """A batch checkpointed mid-protocol (inside the evaluated beats, with
+    the Ca ring part-filled) and restored into a fresh batch ends with the
+    same states and biomarker records, bit for bit, as the run that was
+    never interrupted."""
+    conc, hill = cipa_population(50, 4, seed=6)
+    n = len(conc)
+    a = cep.Batch("cipa2017", n, "mixed")
+    a.init(conc=conc, hill=hill, quirks=True)
+    a.set_pacing(1000.0)
+    a.set_protocol(0.005, 3, 1, dt_write=1.0)
+    a.run(250000)
+    blob = a.checkpoint()
+    clk = a.clock(7)
+    a.run_to_end(50000)
+    ra, sa = a.biomarkers(), a.get_states()
+    b = cep.Batch("cipa2017", n, "mixed")
+    b.restore(blob)
+    assert b.clock(7) == clk
+    b.run_to_end(50000)
+    rb, sb = b.biomarkers(), b.get_states()
+    assert np.array_equal(sa, sb)
+    for k in ra:
+        assert np.array_equal(ra[k], rb[k], equal_nan=True), k
+    with pytest.raises(cep.CepError):
+        cep.Batch("cipa2017", n + 32, "mixed").restore(blob)
+    with pytest.raises(cep.CepError):
+        cep.Batch("cipa2017", n, "fp64").restore(blob)
