@@ -72,7 +72,7 @@ class ServeStats(ctypes.Structure):
                 ("cell_steps", ctypes.c_double), ("busy_ms", ctypes.c_double), ("wall_ms", ctypes.c_double)]
 
 
-JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 
 
 class CepError(RuntimeError):
@@ -147,6 +147,7 @@ _SIGS = {
     "cep_serve_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Biomarkers),
                                         ctypes.POINTER(JobTimes)]),
     "cep_serve_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "cep_serve_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "cep_serve_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServeStats)]),
     "cep_serve_stop": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_qinward": (ctypes.c_double, [ctypes.POINTER(Biomarkers), ctypes.POINTER(Biomarkers)]),
@@ -771,6 +772,10 @@ class Server:
     def release(self, jid: int) -> None:
         _check(lib().cep_serve_release(self._h, jid))
         self._n.pop(jid, None)
+
+    def cancel(self, jid: int) -> None:
+        """Queued: leaves at once; running: leaves between two launches."""
+        _check(lib().cep_serve_cancel(self._h, jid))
 
     def stats(self) -> dict:
         st = ServeStats()

@@ -57,6 +57,7 @@ struct Job {
   unsigned flags = 0;
   int first = -1;  // slot range while admitted
   int state = CEP_JOB_QUEUED;
+  bool cancel = false;  // set by cep_serve_cancel; a running job leaves at the next round boundary
   int error = CEP_OK;
   std::string msg;  // the scheduler thread's error message when failed
   std::vector<cep_biomarkers_t> result;
@@ -309,6 +310,35 @@ void worker_loop(cep_server *s) {
       fail_all(s, rc);
       return;
     }
+    // cancelled jobs leave between launches: their slots return to the pool,
+    // a patch's cells and operator are freed and the tissue group is rebuilt
+    for (auto it = s->running.begin(); it != s->running.end();) {
+      Job &j = **it;
+      if (!j.cancel) {
+        ++it;
+        continue;
+      }
+      cep_batch_release_range(s->pool, j.first, j.n);
+      for (int k = 0; k < j.n; ++k) s->owner[j.first + k] = -1;
+      j.t_done = Clock::now();
+      j.state = CEP_JOB_CANCELLED;
+      it = s->running.erase(it);
+      s->cv_done.notify_all();
+    }
+    for (auto it = s->trunning.begin(); it != s->trunning.end();) {
+      Job &j = **it;
+      if (!j.cancel) {
+        ++it;
+        continue;
+      }
+      tissue_free(j);
+      s->tissue_used -= j.bytes;
+      j.t_done = Clock::now();
+      j.state = CEP_JOB_CANCELLED;
+      s->group_dirty = true;
+      it = s->trunning.erase(it);
+      s->cv_done.notify_all();
+    }
     for (auto it = s->running.begin(); it != s->running.end() && have_pop;) {
       Job &j = **it;
       bool done = true;
@@ -519,7 +549,9 @@ int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s) {
   auto it = s->jobs.find(id);
   if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
   auto j = it->second;
-  auto finished = [&] { return j->state == CEP_JOB_DONE || j->state == CEP_JOB_FAILED; };
+  auto finished = [&] {
+    return j->state == CEP_JOB_DONE || j->state == CEP_JOB_FAILED || j->state == CEP_JOB_CANCELLED;
+  };
   if (timeout_s > 0) {
     if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), finished))
       return cep_internal_set_fail(CEP_ERR_TIMEOUT, "job not finished within the timeout");
@@ -528,6 +560,30 @@ int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s) {
   }
   if (j->state == CEP_JOB_FAILED)
     return fail_fmt(j->error ? j->error : CEP_ERR_STATE, "job failed: %s", j->msg.empty() ? "stopped" : j->msg.c_str());
+  if (j->state == CEP_JOB_CANCELLED) return cep_internal_set_fail(CEP_ERR_STATE, "job cancelled");
+  return CEP_OK;
+}
+
+int cep_serve_cancel(cep_server_t s, uint64_t id) {
+  if (!s) return cep_internal_set_fail(CEP_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->jobs.find(id);
+  if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
+  auto j = it->second;
+  if (j->state != CEP_JOB_QUEUED && j->state != CEP_JOB_RUNNING)
+    return cep_internal_set_fail(CEP_ERR_STATE, "job already finished");
+  for (auto *q : {&s->queue, &s->tqueue}) {
+    auto pos = std::find(q->begin(), q->end(), j);
+    if (pos != q->end()) {  // not admitted yet: it leaves at once
+      q->erase(pos);
+      j->t_admit = j->t_done = Clock::now();
+      j->state = CEP_JOB_CANCELLED;
+      s->cv_done.notify_all();
+      return CEP_OK;
+    }
+  }
+  j->cancel = true;  // admitted (or being admitted): the scheduler releases it between launches
+  s->cv_work.notify_all();
   return CEP_OK;
 }
 
@@ -554,7 +610,8 @@ int cep_serve_release(cep_server_t s, uint64_t id) {
   std::lock_guard<std::mutex> lock(s->mu);
   auto it = s->jobs.find(id);
   if (it == s->jobs.end()) return cep_internal_set_fail(CEP_ERR_ARG, "unknown job id");
-  if (it->second->state != CEP_JOB_DONE && it->second->state != CEP_JOB_FAILED)
+  if (it->second->state != CEP_JOB_DONE && it->second->state != CEP_JOB_FAILED &&
+      it->second->state != CEP_JOB_CANCELLED)
     return cep_internal_set_fail(CEP_ERR_STATE, "job still queued or running");
   s->jobs.erase(it);
   return CEP_OK;

@@ -268,6 +268,7 @@ typedef struct cep_server *cep_server_t;
 #define CEP_JOB_RUNNING 1
 #define CEP_JOB_DONE 2
 #define CEP_JOB_FAILED 3
+#define CEP_JOB_CANCELLED 4
 
 typedef struct {
   int n;                  /* instances                                    */
@@ -305,6 +306,11 @@ int cep_serve_wait(cep_server_t s, uint64_t id, double timeout_s);
 int cep_serve_result(cep_server_t s, uint64_t id, cep_biomarkers_t *out, cep_job_times_t *times);
 /* Forget a finished job (frees its host-side record). */
 int cep_serve_release(cep_server_t s, uint64_t id);
+/* Cancel a job: a queued one leaves at once; a running one leaves between
+ * two launches (its slots return to the pool, a patch's device memory is
+ * freed) and never blocks the others. Its state becomes CEP_JOB_CANCELLED
+ * and cep_serve_wait returns CEP_ERR_STATE for it. */
+int cep_serve_cancel(cep_server_t s, uint64_t id);
 int cep_serve_stats(cep_server_t s, cep_serve_stats_t *st);
 
 /* A 2D TT2006 tissue patch as a screening job (an nx x ny sheet of Q1 nodes

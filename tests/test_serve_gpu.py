@@ -165,3 +165,43 @@ def test_tissue_job_rejections(cep, gpu):
         assert e.value.code in (cep.ERR_OOM, cep.ERR_ARG)
     finally:
         srv.close()
+
+
+@pytest.mark.gpu
+def test_cancel_queued_and_running_jobs(cep, gpu):
+    """A queued job cancelled leaves at once; a running population job and
+    a running patch job leave between launches, their slots and memory
+    return, and the server goes on serving."""
+    import time
+    srv = cep.Server("ord2011", "mixed", capacity=64, dt=0.005, max_bcl=1000.0, steps_per_launch=2000)
+    try:
+        conc, hill = _job(5, 16, 3)  # 48 instances
+        long_job = srv.submit(conc, hill, bcl=1000.0, n_pace=500, first_pace=499)
+        queued = srv.submit(conc, hill, bcl=1000.0, n_pace=1, first_pace=0)  # cannot fit beside it
+        assert srv.poll(queued) == cep.JOB_QUEUED
+        srv.cancel(queued)
+        assert srv.poll(queued) == cep.JOB_CANCELLED
+        with pytest.raises(cep.CepError):
+            srv.wait(queued, 5)
+        patch = srv.submit_tissue(64, 64, 2000.0)
+        t0 = time.time()
+        while (srv.poll(long_job) != cep.JOB_RUNNING or srv.poll(patch) != cep.JOB_RUNNING) and time.time() - t0 < 60:
+            time.sleep(0.01)
+        srv.cancel(long_job)
+        srv.cancel(patch)
+        for j in (long_job, patch):
+            with pytest.raises(cep.CepError):
+                srv.wait(j, 120)
+            assert srv.poll(j) == cep.JOB_CANCELLED
+        c2, h2 = _job(6, 16, 4)  # the whole pool
+        j = srv.submit(c2, h2, bcl=1000.0, n_pace=1, first_pace=0)
+        srv.wait(j, 300)
+        res, _ = srv.result(j)
+        assert (res["status"] == cep.INST_DONE).all()
+        assert srv.stats()["slots_used"] == 0
+        with pytest.raises(cep.CepError):
+            srv.cancel(j)
+        for k in (long_job, queued, patch, j):
+            srv.release(k)
+    finally:
+        srv.close()
