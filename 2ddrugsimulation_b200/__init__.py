@@ -439,7 +439,8 @@ def apdr_bcls(bcl_init: float, bcl_end: float, bcl_decrement: float) -> list[flo
 def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, first_pace: int,
                    precision: str = "mixed", celltype=None, dutta: bool = False, quirks: bool = True,
                    dt_write: float = 1.0, refine_above_vm: float | None = -80.0,
-                   steps_per_launch: int = 50000) -> dict[str, np.ndarray]:
+                   steps_per_launch: int = 50000, amp_scale: float = 1.0,
+                   states_init=None) -> dict[str, np.ndarray]:
     """A population run to the end of its protocol (the reference's bench loop
     for every instance), returning the biomarker records.
 
@@ -448,7 +449,10 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
     not repolarise: their 90 % level is crossed at ~0.1 mV/ms, so their APD90
     moves by tenths of a ms under perturbations of 1e-5 and FP32 gates cannot
     hold it to 0.1 ms) are run again in FP64 from their initial state and
-    their records replaced; out["refined"] marks them."""
+    their records replaced; out["refined"] marks them. amp_scale multiplies
+    the stimulus amplitude (CONSTANTS[amp] *= Stim_Amplitude,
+    cipa_drug_bench.cpp:147); states_init, one state vector, replaces every
+    instance's initial states after initConsts (Is_Using_Output, :149)."""
     conc = np.ascontiguousarray(conc, np.float64)
     n = len(conc)
     hill = np.asarray(hill, np.float64)
@@ -459,7 +463,10 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
         try:
             b.init(celltype=None if ct is None else ct[idx], conc=conc[idx],
                    hill=hill[idx] if hill.ndim == 2 else hill, dutta=dutta, quirks=quirks)
-            b.set_pacing(bcl)
+            b.set_pacing(bcl, amp_scale=amp_scale)
+            if states_init is not None:
+                y0 = np.asarray(states_init, np.float64).reshape(-1)
+                b.set_states(np.ascontiguousarray(np.broadcast_to(y0, (len(idx), len(y0)))))
             b.set_protocol(dt, n_pace, first_pace, dt_write=dt_write)
             b.run_to_end(steps_per_launch)
             return b.biomarkers()
