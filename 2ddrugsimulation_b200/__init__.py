@@ -177,6 +177,7 @@ _SIGS = {
     "cep_tissue_set_stimulus": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_double,
                                                ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "cep_tissue_set_activation_threshold": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "cep_tissue_set_clock": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "cep_tissue_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_tissue_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_tissue_get_v": (ctypes.c_int, [ctypes.c_void_p, _dp]),
@@ -669,6 +670,11 @@ class Tissue:
 
     def set_activation_threshold(self, vm: float) -> "Tissue":
         _check(lib().cep_tissue_set_activation_threshold(self._h, vm))
+        return self
+
+    def set_clock(self, time: float) -> "Tissue":
+        """Resume at `time` ms (node states loaded through the cells' batch)."""
+        _check(lib().cep_tissue_set_clock(self._h, float(time)))
         return self
 
     def run(self, n_steps: int) -> "Tissue":

@@ -1751,6 +1751,14 @@ int cep_tissue_set_activation_threshold(cep_tissue_t t, double vm_threshold) {
   return CEP_OK;
 }
 
+int cep_tissue_set_clock(cep_tissue_t t, double time) {
+  if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
+  if (!std::isfinite(time) || time < 0) return fail_msg(CEP_ERR_ARG, "time must be finite and >= 0");
+  FEM_CUDA(cudaStreamSynchronize(t->stream));
+  t->t = time;
+  return CEP_OK;
+}
+
 int cep_tissue_run(cep_tissue_t t, long n_steps) {
   if (!t) return fail_msg(CEP_ERR_ARG, "null argument");
   if (n_steps < 0) return fail_msg(CEP_ERR_ARG, "n_steps must be >= 0");

@@ -19,6 +19,7 @@ examples.
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 
@@ -121,3 +122,37 @@ def box_tets(nx: int, ny: int, nz: int, h: float) -> Mesh:
                         ids[1], ids[2] = ids[2], ids[1]
                     els.append(ids)
     return Mesh(xyz.astype(np.float64), np.array(els, np.int32), "C3D4")
+
+
+def write_output(path, time: float, states: np.ndarray) -> None:
+    """A tissue snapshot in the reference's output.<rank> format
+    (heart.cpp:943-963): the time ("%f \\n"), then one line per node with
+    its states ("%f " each). Six decimals, as the reference writes them."""
+    st = np.asarray(states, np.float64)
+    with open(path, "w") as f:
+        f.write("%f \n" % time)
+        for row in st:
+            f.write("".join("%f " % x for x in row) + "\n")
+
+
+def read_output(path, n_states: int) -> tuple[float, np.ndarray]:
+    """An output.<rank> snapshot as heart.cpp:595-616 reads it (fscanf
+    "%lf " throughout): the time, then n_states values per node."""
+    vals = np.array(Path(path).read_text().split(), dtype=np.float64)
+    if len(vals) < 1 or (len(vals) - 1) % n_states:
+        raise ValueError(f"{path}: {len(vals) - 1} state values is not a multiple of {n_states}")
+    return float(vals[0]), vals[1:].reshape(-1, n_states)
+
+
+def write_states(path, y) -> None:
+    """One cell's states, one "%lf" per line (drug_sim_full.cpp:318), the
+    file the single-cell benches read back as output_orudy.dat."""
+    with open(path, "w") as f:
+        for x in np.asarray(y, np.float64).reshape(-1):
+            f.write("%f\n" % x)
+
+
+def read_states(path) -> np.ndarray:
+    """A single-cell states file as cipa_drug_bench.cpp:104-111 reads it
+    (strtod per line)."""
+    return np.array([float(ln.split()[0]) for ln in Path(path).read_text().splitlines() if ln.split()])

@@ -441,6 +441,10 @@ int cep_tissue_set_stimulus(cep_tissue_t t, const unsigned char *s1_mask, double
 /* Activation time of a node = the first step end at which V >= threshold
  * (default -30 mV); -1 until then. No counterpart in the reference. */
 int cep_tissue_set_activation_threshold(cep_tissue_t t, double vm_threshold);
+/* Set the tissue clock (ms), e.g. to the time of an output.<rank> snapshot
+ * whose node states were loaded with cep_batch_set_states: the resume of
+ * heart.cpp:595-616 (iopt = 1). Blocking. */
+int cep_tissue_set_clock(cep_tissue_t t, double time);
 /* Advance n_steps Godunov steps (asynchronous). */
 int cep_tissue_run(cep_tissue_t t, long n_steps);
 int cep_tissue_sync(cep_tissue_t t);

@@ -104,3 +104,57 @@ def test_tissue_on_tet_mesh_matches_oracle(cep, gpu, oracle):
     assert np.array_equal(t.activation(), tao)
     with pytest.raises(cep.CepError):
         t.set_electrodes([[0.0, 0.0, 1.0]])  # no pseudo-ECG on unstructured operators
+
+
+def test_output_and_states_files_round_trip(tmp_path):
+    rng = np.random.default_rng(3)
+    st = rng.uniform(-90, 40, (7, 19))
+    mesh.write_output(tmp_path / "output.0", 1234.5, st)
+    first = (tmp_path / "output.0").read_text().splitlines()[0]
+    assert first == "1234.500000 "
+    t, back = mesh.read_output(tmp_path / "output.0", 19)
+    assert t == 1234.5 and back.shape == (7, 19)
+    assert np.abs(back - st).max() <= 5e-7  # six decimals, as the reference writes
+    with pytest.raises(ValueError):
+        mesh.read_output(tmp_path / "output.0", 18)
+    y = rng.uniform(-1, 1, 41)
+    mesh.write_states(tmp_path / "output_orudy.dat", y)
+    assert np.abs(mesh.read_states(tmp_path / "output_orudy.dat") - y).max() <= 5e-7
+
+
+@pytest.mark.gpu
+def test_tissue_resumes_from_an_output_snapshot(cep, gpu, tmp_path):
+    """iopt = 1: a TT2006 sheet resumed at 6 ms in a new tissue. From the
+    exact states and clock the run continues bit for bit; from the
+    output.<rank> file (six decimals) it stays close."""
+    nx = ny = 24
+    n = nx * ny
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[:3, :3] = 1
+
+    def make():
+        cells = cep.Batch("tt2006", n, "fp64")
+        cells.init()
+        fem = cep.Fem.grid(2, nx, ny, 1, 0.025, 0.01, 0.0013).set_solver(1e-10)
+        t = cep.Tissue(cells, fem, 0.01)
+        t.set_stimulus(mask.ravel(), 1000.0, 0.0, 1.0, 1)
+        return cells, fem, t
+
+    c1, f1, t1 = make()
+    t1.run(600)
+    clock, states = t1.stats()["time"], c1.get_states()
+    mesh.write_output(tmp_path / "output.0", clock, states)
+    t1.run(600)
+    v_ref = t1.v()
+    c2, f2, t2 = make()
+    c2.set_states(states)
+    t2.set_clock(clock)
+    t2.run(600)
+    assert np.array_equal(t2.v(), v_ref)
+    c3, f3, t3 = make()
+    time, st = mesh.read_output(tmp_path / "output.0", 19)
+    c3.set_states(st)
+    t3.set_clock(time)
+    t3.run(600)
+    d = np.abs(t3.v() - v_ref)
+    assert np.median(d) <= 0.1, (np.median(d), d.max())
