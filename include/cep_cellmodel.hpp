@@ -74,6 +74,32 @@ class Population {
     check(cep_batch_get_biomarkers(h_, b.data()));
     return b;
   }
+  /* Fastest kernel form and block size for this population (state kept). */
+  void autotune(long n_steps = 400) { check(cep_batch_autotune(h_, n_steps, nullptr, nullptr)); }
+  /* The whole population mid-protocol, and its resume (heart.cpp iopt = 1
+   * style, but exact). */
+  std::vector<unsigned char> checkpoint() const {
+    size_t bytes = 0;
+    check(cep_batch_checkpoint_size(h_, &bytes));
+    std::vector<unsigned char> buf(bytes);
+    check(cep_batch_checkpoint(h_, buf.data(), buf.size()));
+    return buf;
+  }
+  void restore(const std::vector<unsigned char> &buf) { check(cep_batch_restore(h_, buf.data(), buf.size())); }
+  /* apdr_bench.cpp's dynamic restitution: records [n][max_records]. */
+  std::vector<cep_apdr_record_t> restitution(const std::vector<double> &bcl, int n_pace, double dt, int max_records,
+                                             int *n_records = nullptr, long steps_per_launch = 20000) {
+    std::vector<cep_apdr_record_t> out((size_t)n_ * (size_t)max_records);
+    check(cep_batch_restitution(h_, bcl.data(), (int)bcl.size(), n_pace, dt, steps_per_launch, out.data(),
+                                max_records, n_records));
+    return out;
+  }
+  /* CEPPatch/benchpatch.cpp's voltage-clamp replay: out [v.size()][n]. */
+  std::vector<double> clamp(const std::vector<double> &v, double t0, double dt, int current) {
+    std::vector<double> out(v.size() * (size_t)n_);
+    check(cep_batch_clamp(h_, v.data(), (long)v.size(), t0, dt, current, out.data()));
+    return out;
+  }
 
  private:
   cep_batch_t h_ = nullptr;
