@@ -142,7 +142,10 @@ long cepo_fem_assemble_tet(int n_nodes, const double *xyz, int n_elem, const int
  * (Cheart::Radiate, heart.cpp:640-690). */
 void cepo_pseudo_ecg(int dim, int nx, int ny, int nz, double h, const double *D, int n_d, const double *V,
                      int n_el, const double *xyz, double *phi);
-/* Godunov-split tissue run on a structured grid (heart.cpp:127-165). */
+/* Godunov-split tissue run on a structured grid (heart.cpp:127-165).
+ * V[n] receives the final potentials, iters_out[n_steps] (or NULL) the CG
+ * iterations of every step, t_act[n] (or NULL) the activation times;
+ * returns the total CG iterations. */
 long cepo_tissue_run(int model, int dim, int nx, int ny, int nz, double h, const double *D, int n_d, double dt,
                      long n_steps, const unsigned char *s1, double bcl, double t_crt, double dur, int n_pace,
                      double conc, const double *hill, int n_hill, double rtol, int precond_norm,
