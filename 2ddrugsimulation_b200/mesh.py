@@ -100,6 +100,30 @@ def write_vtk(path, mesh: Mesh, point_data: dict) -> None:
             fh.write("".join(f"{float(v):.9g}\n" for v in np.asarray(vals).ravel()))
 
 
+def grid_mesh(dim: int, nx: int, ny: int, nz: int, h: float) -> Mesh:
+    """The structured grid of cep_fem_create_grid as a Mesh (node
+    i + nx*(j + ny*k) at (i h, j h, k h); S4 quads in 2D, C3D8I hexahedra in
+    3D, corners in VTK order), so a grid tissue's V can go to write_vtk."""
+    if dim == 2:
+        nz = 1
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    xyz = np.stack([ii.transpose(2, 1, 0).ravel(), jj.transpose(2, 1, 0).ravel(), kk.transpose(2, 1, 0).ravel()],
+                   1).astype(np.float64) * h
+    i, j = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1), indexing="xy")
+    i, j = i.ravel(), j.ravel()
+    if dim == 2:
+        n0 = i + nx * j
+        els = np.stack([n0, n0 + 1, n0 + 1 + nx, n0 + nx], 1)
+        return Mesh(xyz, els.astype(np.int32), "S4")
+    els = []
+    plane = nx * ny
+    for k in range(nz - 1):
+        n0 = i + nx * j + plane * k
+        quad = np.stack([n0, n0 + 1, n0 + 1 + nx, n0 + nx], 1)
+        els.append(np.concatenate([quad, quad + plane], 1))
+    return Mesh(xyz, np.concatenate(els).astype(np.int32), "C3D8I")
+
+
 def box_tets(nx: int, ny: int, nz: int, h: float) -> Mesh:
     """Tetrahedral mesh of an (nx-1) x (ny-1) x (nz-1) box of cubes of edge h,
     node (i, j, k) = i + nx*(j + ny*k) at (i h, j h, k h)."""

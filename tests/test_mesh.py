@@ -158,3 +158,19 @@ def test_tissue_resumes_from_an_output_snapshot(cep, gpu, tmp_path):
     t3.run(600)
     d = np.abs(t3.v() - v_ref)
     assert np.median(d) <= 0.1, (np.median(d), d.max())
+
+
+def test_grid_mesh_matches_the_grid_operator_numbering(tmp_path):
+    m2 = mesh.grid_mesh(2, 5, 4, 1, 0.1)
+    assert m2.etype == "S4" and m2.elements.shape == (12, 4) and len(m2.xyz) == 20
+    p = m2.xyz[m2.elements]
+    area = 0.5 * np.cross(p[:, 2] - p[:, 0], p[:, 1] - p[:, 3])[:, 2]  # quad diagonals
+    assert np.allclose(np.abs(area), 0.01)
+    assert np.array_equal(m2.xyz[7], [0.2, 0.1, 0.0])  # node i + nx*j
+    m3 = mesh.grid_mesh(3, 4, 3, 3, 0.1)
+    assert m3.etype == "C3D8I" and m3.elements.shape == (12, 8) and len(m3.xyz) == 36
+    e = m3.xyz[m3.elements[0]]
+    assert np.allclose(e[6] - e[0], [0.1, 0.1, 0.1]) and np.allclose(e[4] - e[0], [0, 0, 0.1])
+    mesh.write_vtk(tmp_path / "g.vtk", m3, {"Voltage": np.arange(36.0)})
+    text = (tmp_path / "g.vtk").read_text()
+    assert "CELL_TYPES 12\n12\n" in text and "POINT_DATA 36" in text
