@@ -104,9 +104,15 @@ _KEYS = {
 
 
 def _text(src) -> str:
-    if isinstance(src, Path) or (isinstance(src, str) and src and "\n" not in src and Path(src).is_file()):
-        return Path(src).read_text()
-    return str(src)
+    """The text of a deck or Hill file given as a path or as its text. A
+    single line without "=" or "," is a path, and a missing file raises (the
+    reference stops with "Cannot open file", commons.cpp:110-113)."""
+    if isinstance(src, Path):
+        return src.read_text()
+    s = str(src)
+    if s and "\n" not in s and "=" not in s and "," not in s:
+        return Path(s).read_text()
+    return s
 
 
 def _fgets_chunks(text: str, size: int):

@@ -47,6 +47,14 @@ def test_deck_parsing_rules():
     assert np.array_equal(deck.split_values("0,1,"), [0.0, 1.0, 0.0])  # trailing comma adds a 0
 
 
+def test_deck_from_a_path_and_a_missing_path(tmp_path):
+    f = tmp_path / "deck.txt"
+    f.write_text(DECK)
+    assert deck.read_deck(f) == deck.read_deck(str(f)) == deck.read_deck(DECK)
+    with pytest.raises(FileNotFoundError):
+        deck.read_deck(str(tmp_path / "missing_deck.txt"))
+
+
 def test_long_deck_line_is_read_in_fgets_pieces():
     # 99 characters per fgets piece: the value of an over-long line is cut
     d = deck.read_deck("Drug_Name = " + "x" * 120 + "\n")
