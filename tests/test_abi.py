@@ -45,3 +45,21 @@ def test_server_without_device_fails_loudly(cep):
     with pytest.raises(cep.CepError) as e:
         cep.Server("ord2011")
     assert e.value.code == cep.ERR_NO_DEVICE
+
+
+def test_host_helpers_without_device_fail_loudly(cep):
+    """run_population and the deck runner go through the device library only:
+    without a GPU they raise, they never fall back to the CPU oracle."""
+    if cep.device_count() > 0:
+        return
+    import importlib
+
+    import numpy as np
+    import pytest
+    with pytest.raises(cep.CepError) as e:
+        cep.run_population("cipa2017", np.zeros(2), np.zeros((2, 20)), bcl=2000.0, dt=0.005, n_pace=1, first_pace=0)
+    assert e.value.code == cep.ERR_NO_DEVICE
+    deck = importlib.import_module("2ddrugsimulation_b200.deck")
+    with pytest.raises(cep.CepError) as e:
+        deck.run(deck.read_deck("Simulation_Mode = 1\nBasic_Cycle_Length = 400\nBCL_End = 400\n"))
+    assert e.value.code == cep.ERR_NO_DEVICE
