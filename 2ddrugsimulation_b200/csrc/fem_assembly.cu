@@ -65,31 +65,100 @@ __device__ __forceinline__ void shape(int dim, int a, double s, double t, double
   ds[2] = sz * gs * gt / 8.;
 }
 
-// Entry (a, b) of the element matrices of an axis-aligned element of edge h.
-__device__ void element_entry(int dim, double h, double dt, const double (&Dm)[3][3], int a, int b, double &ae,
-                              double &be) {
-  const double jac = 0.5 * h;
-  const double detJ = dim == 2 ? jac * jac : jac * jac * jac;
-  const double inv = 1.0 / jac;
+// Per-Gauss-point geometry of an element with node coordinates x[nn][dim],
+// in the reference's sequence of operations (Cfem::set_amat_bmat,
+// fem.cpp:628-661 with inverseMat, fem.cpp:557-589): the Jacobian
+// J[r][c] = sum_a dS[a][r] x[a][c] over the nodes in order, its determinant
+// and cofactor inverse xJ, and the physical gradient of node a,
+// dX[i] = sum_j dS[a][j] xJ[i][j].
+struct ElemGeom {
+  double det, xJ[3][3];
+};
+
+__device__ void elem_geom(int dim, int nn, const double (*dS)[3], const double *x, ElemGeom &eg) {
+  double J[3][3];
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) {
+      double acc = 0.0;
+      for (int a = 0; a < nn; ++a) acc += dS[a][r] * x[a * dim + c];
+      J[r][c] = acc;
+    }
+  if (dim == 3) {
+    const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                       J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                       J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    eg.det = det;
+    eg.xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+    eg.xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
+    eg.xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+    eg.xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
+    eg.xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+    eg.xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
+    eg.xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+    eg.xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
+    eg.xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  } else {
+    const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    eg.det = det;
+    eg.xJ[0][0] = J[1][1] / det;
+    eg.xJ[0][1] = -J[0][1] / det;
+    eg.xJ[1][0] = -J[1][0] / det;
+    eg.xJ[1][1] = J[0][0] / det;
+  }
+}
+
+__device__ __forceinline__ void phys_grad(int dim, const double ds[3], const ElemGeom &eg, double dx[3]) {
+  for (int i = 0; i < dim; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < dim; ++j) acc += ds[j] * eg.xJ[i][j];
+    dx[i] = acc;
+  }
+}
+
+// The stiffness contribution of one Gauss point: with a scalar D the
+// reference's (sum_i dX_a[i] dX_b[i]) detJ D; with a tensor (the
+// anisotropic extension) grad Phi_a . D grad Phi_b detJ.
+__device__ __forceinline__ double stiffness(int dim, const double dxa[3], const double dxb[3], const double *D,
+                                            int n_d, const double (&Dm)[3][3], double det) {
+  if (n_d == 1) {
+    double acc = 0.0;
+    for (int i = 0; i < dim; ++i) acc += dxa[i] * dxb[i];
+    return acc * det * D[0];
+  }
+  double gdg = 0.0;
+  for (int u = 0; u < dim; ++u)
+    for (int v = 0; v < dim; ++v) gdg += dxa[u] * Dm[u][v] * dxb[v];
+  return gdg * det;
+}
+
+// Entry (a, b) of the element matrices of the axis-aligned grid element of
+// edge h with its first node at the origin (every element of the grid uses
+// these), Gauss point by Gauss point with unit weights:
+//   A_e[a][b] += Phi_a Phi_b detJ / dt + stiffness,  B_e[a][b] += Phi_a Phi_b detJ.
+__device__ void element_entry(int dim, double h, double dt, const double *D, int n_d, const double (&Dm)[3][3],
+                              int a, int b, double &ae, double &be) {
   const int ng = dim == 2 ? 4 : 8;
+  double x[24];
+  for (int n = 0; n < ng; ++n) {
+    const int q = n & 3;
+    x[n * dim + 0] = (q == 1 || q == 2) ? 1.0 * h : 0.0 * h;
+    x[n * dim + 1] = (q >= 2) ? 1.0 * h : 0.0 * h;
+    if (dim == 3) x[n * dim + 2] = (n >= 4) ? 1.0 * h : 0.0 * h;
+  }
   ae = 0.0;
   be = 0.0;
   for (int g = 0; g < ng; ++g) {
     double s, t, z;
     gauss_point(dim, g, s, t, z);
-    double pa, pb, dsa[3], dsb[3];
-    shape(dim, a, s, t, z, pa, dsa);
-    shape(dim, b, s, t, z, pb, dsb);
+    double dS[8][3], phi[8];
+    for (int n = 0; n < ng; ++n) shape(dim, n, s, t, z, phi[n], dS[n]);
+    ElemGeom eg;
+    elem_geom(dim, ng, dS, x, eg);
     double dxa[3], dxb[3];
-    for (int d = 0; d < dim; ++d) {
-      dxa[d] = dsa[d] * inv;
-      dxb[d] = dsb[d] * inv;
-    }
-    double gdg = 0.0;
-    for (int u = 0; u < dim; ++u)
-      for (int v = 0; v < dim; ++v) gdg += dxa[u] * Dm[u][v] * dxb[v];
-    ae += pa * pb * detJ / dt + gdg * detJ;
-    be += pa * pb * detJ;
+    phys_grad(dim, dS[a], eg, dxa);
+    phys_grad(dim, dS[b], eg, dxb);
+    ae += phi[a] * phi[b] * eg.det / dt + stiffness(dim, dxa, dxb, D, n_d, Dm, eg.det);
+    be += phi[a] * phi[b] * eg.det;
   }
 }
 
@@ -159,7 +228,7 @@ __global__ void assemble_grid_kernel(GridArgs g) {
               const int la = local_index(ix - ex, iy - ey, g.dim == 3 ? iz - ez : 0);
               const int lb = local_index(jx - ex, jy - ey, g.dim == 3 ? jz - ez : 0);
               double ae, be;
-              element_entry(g.dim, g.h, g.dt, Dm, la, lb, ae, be);
+              element_entry(g.dim, g.h, g.dt, g.D + e * g.n_d, g.n_d, Dm, la, lb, ae, be);
               av += ae;
               bv += be;
             }
@@ -206,57 +275,33 @@ extern "C" int cep_internal_fem_assemble_grid(int dim, int nx, int ny, int nz, d
 namespace cep {
 namespace fem {
 
+// Row la of the element matrices of tetrahedron x[4][3] in the reference's
+// sequence of operations (the constant Jacobian is recomputed at each of
+// the four Gauss points, as fem.cpp:640-651 does).
 __device__ void tet_row(const double x[4][3], const double *D, int n_d, double dt, int la, double *arow,
                         double *brow) {
   const double aaa = (5. - sqrt(5.)) / 20., bbb = (5. + 3. * sqrt(5.)) / 20.;
   const double gp[4][3] = {{aaa, aaa, aaa}, {aaa, aaa, bbb}, {aaa, bbb, aaa}, {bbb, aaa, aaa}};
   const double dS[4][3] = {{-1., -1., -1.}, {1., 0., 0.}, {0., 1., 0.}, {0., 0., 1.}};
-  double J[3][3];
-  for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 3; ++c) {
-      double s = 0.;
-      for (int a = 0; a < 4; ++a) s += dS[a][r] * x[a][c];
-      J[r][c] = s;
-    }
-  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-  double xJ[3][3];
-  xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
-  xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
-  xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
-  xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
-  xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
-  xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
-  xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
-  xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
-  xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
-  double dX[4][3];
-  for (int a = 0; a < 4; ++a)
-    for (int i = 0; i < 3; ++i) {
-      double s = 0.;
-      for (int j = 0; j < 3; ++j) s += dS[a][j] * xJ[i][j];
-      dX[a][i] = s;
-    }
-  double Dm[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
-  if (n_d == 1) {
-    Dm[0][0] = Dm[1][1] = Dm[2][2] = D[0];
-  } else {
-    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
-    Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
-  }
+  double Dm[3][3];
+  tensor_of(3, D, n_d, Dm);
   for (int k = 0; k < 4; ++k) {
-    double gdg = 0.;
-    for (int p = 0; p < 3; ++p)
-      for (int q = 0; q < 3; ++q) gdg += dX[la][p] * Dm[p][q] * dX[k][q];
-    double av = 0., bv = 0.;
-    for (int g = 0; g < 4; ++g) {
-      const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
-      const double phi[4] = {1. - s - t - z, s, t, z};
-      av += phi[la] * phi[k] * det / dt + gdg * det;
-      bv += phi[la] * phi[k] * det;
+    arow[k] = 0.;
+    brow[k] = 0.;
+  }
+  for (int g = 0; g < 4; ++g) {
+    ElemGeom eg;
+    elem_geom(3, 4, dS, &x[0][0], eg);
+    const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
+    const double phi[4] = {1. - s - t - z, s, t, z};
+    double dxa[3];
+    phys_grad(3, dS[la], eg, dxa);
+    for (int k = 0; k < 4; ++k) {
+      double dxb[3];
+      phys_grad(3, dS[k], eg, dxb);
+      arow[k] += phi[la] * phi[k] * eg.det / dt + stiffness(3, dxa, dxb, D, n_d, Dm, eg.det);
+      brow[k] += phi[la] * phi[k] * eg.det;
     }
-    arow[k] = av;
-    brow[k] = bv;
   }
 }
 

@@ -27,6 +27,7 @@ REF_LIBS = {
     "tt2006_tissue": "libref_tt2006_epi_tissue.so",
     "tt2004": "libref_tt2004b.so",
     "tomek2019": "libref_tomek2019.so",
+    "fem": "libref_fem.so",
 }
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -110,6 +111,7 @@ def lib() -> ctypes.CDLL:
         L.cepo_fem_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, _dp, ctypes.c_int, _ip, _ip, _dp, _dp]
         L.cepo_fem_element.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp, _dp]
+        L.cepo_element.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.cepo_pseudo_ecg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp,
                                       ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
         L.cepo_spmv.argtypes = [ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
@@ -311,6 +313,21 @@ def ref_available(key: str) -> bool:
     return (REF_DIR / REF_LIBS[key]).exists()
 
 
+def ref_fem_element(kind: str, xy, de: float, dt: float) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's own element matrices (Cfem::set_amat_bmat, fem.cpp:
+    628-661, compiled from fem.cpp) of one square, hex or tet element with
+    node coordinates xy[nn][dim] and scalar conductivity de."""
+    L = ctypes.CDLL(str(REF_DIR / REF_LIBS["fem"]))
+    L.ref_fem_element.argtypes = [ctypes.c_char_p, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp]
+    x = np.ascontiguousarray(xy, np.float64)
+    nn = len(x)
+    ae = np.zeros(nn * nn)
+    be = np.zeros(nn * nn)
+    if L.ref_fem_element(kind.encode(), _ptr(x), de, dt, _ptr(ae), _ptr(be)) != 0:
+        raise ValueError(kind)
+    return ae.reshape(nn, nn), be.reshape(nn, nn)
+
+
 # ------------------------------------------------------------------ FEM
 _ip = ctypes.POINTER(ctypes.c_int)
 
@@ -402,6 +419,18 @@ def fem_element(dim: int, h: float, dt: float, D) -> tuple[np.ndarray, np.ndarra
     ae = np.zeros(nn * nn)
     be = np.zeros(nn * nn)
     lib().cepo_fem_element(dim, h, dt, _ptr(d), len(d), _ptr(ae), _ptr(be))
+    return ae.reshape(nn, nn), be.reshape(nn, nn)
+
+
+def element(kind: str, xy, D, dt: float) -> tuple[np.ndarray, np.ndarray]:
+    """Element matrices (A = M/dt + D K, B = M) of one square, hex or tet
+    element with node coordinates xy[nn][dim]."""
+    x = np.ascontiguousarray(xy, np.float64)
+    d = np.ascontiguousarray(np.atleast_1d(np.asarray(D, np.float64)))
+    nn = len(x)
+    ae = np.zeros(nn * nn)
+    be = np.zeros(nn * nn)
+    lib().cepo_element({"square": 0, "hex": 1, "tet": 2}[kind], _ptr(x), _ptr(d), len(d), dt, _ptr(ae), _ptr(be))
     return ae.reshape(nn, nn), be.reshape(nn, nn)
 
 

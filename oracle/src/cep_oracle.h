@@ -126,6 +126,9 @@ void cepo_spmv(int n, const int *row_ptr, const int *col_idx, const double *val,
  * default for CG), 0 = ||r||/||b||. */
 int cepo_pcg2(int n, const int *row_ptr, const int *col_idx, const double *a_val, const double *b, double *x,
               double rtol, int max_iter, int precond_norm, double *rel_res);
+/* Element matrices (nn x nn, row-major) of one element of the reference's
+ * kinds (0 square, 1 hex, 2 tet) with node coordinates x[nn][dim]. */
+void cepo_element(int kind, const double *x, const double *D, int n_d, double dt, double *Ae, double *Be);
 /* Element matrices (nn x nn, row-major) of an axis-aligned element of edge h. */
 void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be);
 /* The Godunov tissue loop on a caller's CSR operator (any mesh). */

@@ -2,11 +2,12 @@
  * TEST INFRASTRUCTURE ONLY. CPU restatement of the reference's monodomain
  * FEM diffusion solve (fem.cpp / heart.cpp) on structured grids.
  *
- * Elements: Q1 quadrilaterals (2D) and trilinear hexahedra (3D) with the
- * reference's local node order and shape functions (fem.cpp:398-478), its
- * Gauss points at +-0.57735 with unit weights (fem.cpp:231-271), and its
- * element matrices (fem.cpp:628-661):
- *   A_e[j][k] = sum_g Phi_j Phi_k detJ/dt + grad Phi_j . D grad Phi_k detJ
+ * Elements: Q1 quadrilaterals (2D), trilinear hexahedra (3D) and P1
+ * tetrahedra with the reference's local node order and shape functions
+ * (fem.cpp:342-478), its Gauss points (+-0.57735 with unit weights,
+ * fem.cpp:209-271), and its element matrices (fem.cpp:628-661) in its own
+ * sequence of floating-point operations (cepo_element):
+ *   A_e[j][k] = sum_g Phi_j Phi_k detJ/dt + grad Phi_j . grad Phi_k detJ D
  *   B_e[j][k] = sum_g Phi_j Phi_k detJ
  * D per element is the reference's scalar DE (n_d == 1) or, as an
  * extension for anisotropic tissue, a symmetric tensor. The global solve
@@ -37,67 +38,126 @@ static void local_offsets(int dim, int off[8][3]) {
   memcpy(off, dim == 2 ? (const void *)q4 : (const void *)h8, sizeof(int) * 3 * (dim == 2 ? 4 : 8));
 }
 
-/* Element matrices of an axis-aligned element of edge h (fem.cpp:628-661).
- * D: 1 value (scalar) or 3 (2D: xx,xy,yy) / 6 (3D: xx,xy,xz,yy,yz,zz). */
-void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be) {
-  const int nn = dim == 2 ? 4 : 8;
-  double gp[8][3];
-  if (dim == 2) {
+/* Gauss points, shape functions and their reference-space gradients of the
+ * reference's element types: kind 0 Q1 square (fem.cpp:256-271,398-425),
+ * kind 1 trilinear hex (fem.cpp:231-248,427-478), kind 2 P1 tetrahedron
+ * (fem.cpp:209-229,342-373); nodes in the reference's local order. */
+static void element_basis(int kind, int g, double Phi[8], double dS[8][3]) {
+  if (kind == 0) {
     const double g4[4][2] = {{-GA, -GA}, {GA, -GA}, {GA, GA}, {-GA, GA}};
-    for (int g = 0; g < 4; ++g) { gp[g][0] = g4[g][0]; gp[g][1] = g4[g][1]; gp[g][2] = 0; }
-  } else {
+    const double s = g4[g][0], t = g4[g][1];
+    Phi[0] = (1. - s) * (1. - t) / 4.; Phi[1] = (1. + s) * (1. - t) / 4.;
+    Phi[2] = (1. + s) * (1. + t) / 4.; Phi[3] = (1. - s) * (1. + t) / 4.;
+    dS[0][0] = -(1. - t) / 4.; dS[0][1] = -(1. - s) / 4.;
+    dS[1][0] = +(1. - t) / 4.; dS[1][1] = -(1. + s) / 4.;
+    dS[2][0] = +(1. + t) / 4.; dS[2][1] = +(1. + s) / 4.;
+    dS[3][0] = -(1. + t) / 4.; dS[3][1] = +(1. - s) / 4.;
+  } else if (kind == 1) {
     const double aa[2] = {-GA, GA};
-    int n = 0;
-    for (int ix = 0; ix < 2; ++ix)
-      for (int iy = 0; iy < 2; ++iy)
-        for (int iz = 0; iz < 2; ++iz) { gp[n][0] = aa[ix]; gp[n][1] = aa[iy]; gp[n][2] = aa[iz]; ++n; }
-  }
-  double Dm[3][3] = {{0}};
-  if (n_d == 1) {
-    for (int a = 0; a < dim; ++a) Dm[a][a] = D[0];
-  } else if (dim == 2) {
-    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[1][1] = D[2];
+    const double s = aa[(g >> 2) & 1], t = aa[(g >> 1) & 1], z = aa[g & 1];
+    const double sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    for (int n = 0; n < 8; ++n) {
+      const double fs = 1 + sg[n][0] * s, ft = 1 + sg[n][1] * t, fz = 1 + sg[n][2] * z;
+      Phi[n] = fs * ft * fz / 8.;
+      dS[n][0] = sg[n][0] * ft * fz / 8.; dS[n][1] = sg[n][1] * fs * fz / 8.; dS[n][2] = sg[n][2] * fs * ft / 8.;
+    }
   } else {
+    const double aaa = (5. - sqrt(5.)) / 20., bbb = (5. + 3. * sqrt(5.)) / 20.;
+    const double gp[4][3] = {{aaa, aaa, aaa}, {aaa, aaa, bbb}, {aaa, bbb, aaa}, {bbb, aaa, aaa}};
+    const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
+    Phi[0] = 1. - s - t - z; Phi[1] = s; Phi[2] = t; Phi[3] = z;
+    const double d4[4][3] = {{-1., -1., -1.}, {1., 0., 0.}, {0., 1., 0.}, {0., 0., 1.}};
+    memcpy(dS, d4, sizeof(d4));
+  }
+}
+
+/* Element matrices of one element with node coordinates x[nn][dim]
+ * (fem.cpp:628-661), in the reference's sequence of operations: per Gauss
+ * point the Jacobian J[r][c] = sum_a dS[a][r] x[a][c] summed over the nodes
+ * in order, its determinant and cofactor inverse (fem.cpp:544-589), the
+ * physical gradients dX[a][i] = sum_j dS[a][j] xJ[i][j] and
+ * K[j][k] = sum_i dX[j][i] dX[k][i]; then, Gauss point by Gauss point,
+ *   A_e[j][k] += Phi_j Phi_k detJ / dt + K[j][k] detJ D
+ *   B_e[j][k] += Phi_j Phi_k detJ
+ * with unit weights. D: the reference's scalar DE (n_d == 1); a symmetric
+ * tensor (2D: xx,xy,yy; 3D: xx,xy,xz,yy,yz,zz) is an extension for
+ * anisotropic tissue, whose stiffness term is grad Phi_j . D grad Phi_k
+ * detJ. */
+void cepo_element(int kind, const double *x, const double *D, int n_d, double dt, double *Ae, double *Be) {
+  const int dim = kind == 0 ? 2 : 3, nn = kind == 1 ? 8 : 4;
+  double Dm[3][3] = {{0}};
+  if (n_d > 1 && dim == 2) {
+    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[1][1] = D[2];
+  } else if (n_d > 1) {
     Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
     Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
   }
-  const double jac = 0.5 * h;                      /* dx/dxi on each axis */
-  const double detJ = dim == 2 ? jac * jac : jac * jac * jac;
-  const double inv = 1.0 / jac;
   for (int j = 0; j < nn * nn; ++j) { Ae[j] = 0; Be[j] = 0; }
   for (int g = 0; g < nn; ++g) {
-    const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
-    double Phi[8], dS[8][3];
-    if (dim == 2) {
-      Phi[0] = (1. - s) * (1. - t) / 4.; Phi[1] = (1. + s) * (1. - t) / 4.;
-      Phi[2] = (1. + s) * (1. + t) / 4.; Phi[3] = (1. - s) * (1. + t) / 4.;
-      dS[0][0] = -(1. - t) / 4.; dS[0][1] = -(1. - s) / 4.;
-      dS[1][0] = +(1. - t) / 4.; dS[1][1] = -(1. + s) / 4.;
-      dS[2][0] = +(1. + t) / 4.; dS[2][1] = +(1. + s) / 4.;
-      dS[3][0] = -(1. + t) / 4.; dS[3][1] = +(1. - s) / 4.;
-    } else {
-      const double sp = 1 + s, sm = 1 - s, tp = 1 + t, tm = 1 - t, zp = 1 + z, zm = 1 - z;
-      Phi[0] = sm * tm * zm / 8.; Phi[1] = sp * tm * zm / 8.; Phi[2] = sp * tp * zm / 8.; Phi[3] = sm * tp * zm / 8.;
-      Phi[4] = sm * tm * zp / 8.; Phi[5] = sp * tm * zp / 8.; Phi[6] = sp * tp * zp / 8.; Phi[7] = sm * tp * zp / 8.;
-      const double sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
-                               {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
-      for (int n = 0; n < 8; ++n) {
-        const double fs = 1 + sg[n][0] * s, ft = 1 + sg[n][1] * t, fz = 1 + sg[n][2] * z;
-        dS[n][0] = sg[n][0] * ft * fz / 8.; dS[n][1] = sg[n][1] * fs * fz / 8.; dS[n][2] = sg[n][2] * fs * ft / 8.;
+    double Phi[8], dS[8][3], J[3][3], xJ[3][3], det;
+    element_basis(kind, g, Phi, dS);
+    for (int r = 0; r < dim; ++r)
+      for (int c = 0; c < dim; ++c) {
+        double acc = 0.;
+        for (int a = 0; a < nn; ++a) acc += dS[a][r] * x[a * dim + c];
+        J[r][c] = acc;
       }
+    if (dim == 3) {
+      det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+            J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+      xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+      xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
+      xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+      xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
+      xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+      xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
+      xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+      xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
+      xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    } else {
+      det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      xJ[0][0] = J[1][1] / det; xJ[0][1] = -J[0][1] / det;
+      xJ[1][0] = -J[1][0] / det; xJ[1][1] = J[0][0] / det;
     }
     double dX[8][3];
-    for (int n = 0; n < nn; ++n)
-      for (int a = 0; a < dim; ++a) dX[n][a] = dS[n][a] * inv;
+    for (int a = 0; a < nn; ++a)
+      for (int i = 0; i < dim; ++i) {
+        double acc = 0.;
+        for (int j = 0; j < dim; ++j) acc += dS[a][j] * xJ[i][j];
+        dX[a][i] = acc;
+      }
     for (int j = 0; j < nn; ++j)
       for (int k = 0; k < nn; ++k) {
-        double gdg = 0;
-        for (int a = 0; a < dim; ++a)
-          for (int b = 0; b < dim; ++b) gdg += dX[j][a] * Dm[a][b] * dX[k][b];
-        Ae[j * nn + k] += Phi[j] * Phi[k] * detJ / dt + gdg * detJ;
-        Be[j * nn + k] += Phi[j] * Phi[k] * detJ;
+        double stiff;
+        if (n_d == 1) {
+          double acc = 0.;
+          for (int i = 0; i < dim; ++i) acc += dX[j][i] * dX[k][i];
+          stiff = acc * det * D[0];
+        } else {
+          double gdg = 0.;
+          for (int u = 0; u < dim; ++u)
+            for (int v = 0; v < dim; ++v) gdg += dX[j][u] * Dm[u][v] * dX[k][v];
+          stiff = gdg * det;
+        }
+        Ae[j * nn + k] += Phi[j] * Phi[k] * det / dt + stiff;
+        Be[j * nn + k] += Phi[j] * Phi[k] * det;
       }
   }
+}
+
+/* Element matrices of the axis-aligned grid element of edge h with its
+ * first node at the origin; every element of a structured grid uses these
+ * (the reference's own matrices of translated elements differ from them
+ * only by the rounding of its node coordinates). */
+void cepo_fem_element(int dim, double h, double dt, const double *D, int n_d, double *Ae, double *Be) {
+  int off[8][3];
+  local_offsets(dim, off);
+  const int nn = dim == 2 ? 4 : 8;
+  double x[24];
+  for (int a = 0; a < nn; ++a)
+    for (int c = 0; c < dim; ++c) x[a * dim + c] = off[a][c] * h;
+  cepo_element(dim == 2 ? 0 : 1, x, D, n_d, dt, Ae, Be);
 }
 
 /* Shape-function gradients (reference coordinates) at Gauss point g of the
@@ -412,59 +472,14 @@ long cepo_tissue_run_csr(int model, int n, const int *rp, const int *ci, const d
 /* ---- unstructured P1 tetrahedra (fem.cpp:209-229 Gauss points,
  * 342-373 shape functions, 628-661 element matrices) ---- */
 
-/* Row la of the element matrices of tetrahedron x[4][3] (unit Gauss
- * weights as the reference; D scalar (n_d 1) or xx,xy,xz,yy,yz,zz (6)).
- * The expression order is shared with the device assembly. */
+/* Row la of the element matrices of tetrahedron x[4][3] (cepo_element,
+ * kind 2; D scalar (n_d 1) or xx,xy,xz,yy,yz,zz (6)). */
 void cepo_tet_row(const double x[4][3], const double *D, int n_d, double dt, int la, double *arow, double *brow) {
-  const double aaa = (5. - sqrt(5.)) / 20., bbb = (5. + 3. * sqrt(5.)) / 20.;
-  const double gp[4][3] = {{aaa, aaa, aaa}, {aaa, aaa, bbb}, {aaa, bbb, aaa}, {bbb, aaa, aaa}};
-  const double dS[4][3] = {{-1., -1., -1.}, {1., 0., 0.}, {0., 1., 0.}, {0., 0., 1.}};
-  double J[3][3];
-  for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 3; ++c) {
-      double s = 0.;
-      for (int a = 0; a < 4; ++a) s += dS[a][r] * x[a][c];
-      J[r][c] = s;
-    }
-  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-  double xJ[3][3];
-  xJ[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
-  xJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) / det;
-  xJ[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
-  xJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) / det;
-  xJ[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
-  xJ[2][1] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]) / det;
-  xJ[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
-  xJ[1][2] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]) / det;
-  xJ[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
-  double dX[4][3];
-  for (int a = 0; a < 4; ++a)
-    for (int i = 0; i < 3; ++i) {
-      double s = 0.;
-      for (int j = 0; j < 3; ++j) s += dS[a][j] * xJ[i][j];
-      dX[a][i] = s;
-    }
-  double Dm[3][3] = {{0}};
-  if (n_d == 1) {
-    Dm[0][0] = Dm[1][1] = Dm[2][2] = D[0];
-  } else {
-    Dm[0][0] = D[0]; Dm[0][1] = Dm[1][0] = D[1]; Dm[0][2] = Dm[2][0] = D[2];
-    Dm[1][1] = D[3]; Dm[1][2] = Dm[2][1] = D[4]; Dm[2][2] = D[5];
-  }
+  double Ae[16], Be[16];
+  cepo_element(2, &x[0][0], D, n_d, dt, Ae, Be);
   for (int k = 0; k < 4; ++k) {
-    double gdg = 0.;
-    for (int p = 0; p < 3; ++p)
-      for (int q = 0; q < 3; ++q) gdg += dX[la][p] * Dm[p][q] * dX[k][q];
-    double av = 0., bv = 0.;
-    for (int g = 0; g < 4; ++g) {
-      const double s = gp[g][0], t = gp[g][1], z = gp[g][2];
-      const double phi[4] = {1. - s - t - z, s, t, z};
-      av += phi[la] * phi[k] * det / dt + gdg * det;
-      bv += phi[la] * phi[k] * det;
-    }
-    arow[k] = av;
-    brow[k] = bv;
+    arow[k] = Ae[la * 4 + k];
+    brow[k] = Be[la * 4 + k];
   }
 }
 

@@ -2,13 +2,15 @@
 models compiled from their own sources (oracle/_ref, built by
 `make -C oracle ref` where the reference tree is present).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [ord cipa tt2006 tt2004 tomek fem]
 
 Each fixture holds the inputs (celltype, concentration, Hill row, flags),
 the reference's V trace sampled every `stride` steps of its explicit loop
 (computeRates(t); solveAnalytical(dt); t += dt), its final STATES, and its
-RATES at t = 0. The oracle and the GPU path are checked against these files
-on machines where the reference itself is not available.
+RATES at t = 0. fem_elements.npz holds the reference's FEM element
+matrices (fem.cpp set_amat_bmat) of square, hex and tet elements. The
+oracle and the GPU path are checked against these files on machines where
+the reference itself is not available.
 """
 from __future__ import annotations
 
@@ -177,11 +179,52 @@ def make_tomek(dt: float = 0.005, n_steps: int = 200000, every: int = 10000):
         print("wrote", c["name"])
 
 
+def fem_element_cases(seed: int = 20):
+    """Element node coordinates of each kind: the grid element at the
+    origin (edge 0.025 cm), one translated far from it, and distorted ones."""
+    rng = np.random.default_rng(seed)
+    h = 0.025
+    base = {"square": np.array([[0, 0], [h, 0], [h, h], [0, h]], float),
+            "hex": np.array([[0, 0, 0], [h, 0, 0], [h, h, 0], [0, h, 0], [0, 0, h], [h, 0, h], [h, h, h], [0, h, h]],
+                            float),
+            "tet": np.array([[0, 0, 0], [h, 0, 0], [0, h, 0], [0, 0, h]], float)}
+    cases = []
+    for kind, x in base.items():
+        cases.append((kind, x.copy()))
+        cases.append((kind, x + 7.3))
+        for _ in range(3):
+            cases.append((kind, x + rng.uniform(-0.25, 0.25, x.shape) * h + rng.uniform(-3, 3)))
+    return cases
+
+
+def make_fem(dt: float = 0.01, de: float = 0.0013):
+    """The reference's element matrices (fem.cpp set_amat_bmat, compiled from
+    fem.cpp) for every case of fem_element_cases()."""
+    kinds, xs, As, Bs = [], [], [], []
+    for kind, x in fem_element_cases():
+        a, b = O.ref_fem_element(kind, x, de, dt)
+        kinds.append(kind)
+        xs.append(np.pad(x, ((0, 8 - len(x)), (0, 3 - x.shape[1]))))
+        As.append(np.pad(a, ((0, 8 - len(a)), (0, 8 - len(a)))))
+        Bs.append(np.pad(b, ((0, 8 - len(b)), (0, 8 - len(b)))))
+    np.savez_compressed(OUT / "fem_elements.npz", kind=np.array(kinds), x=np.array(xs), A=np.array(As),
+                        B=np.array(Bs), dt=dt, de=de)
+    print("wrote fem_elements")
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
-    make_ord()
-    make_cipa()
-    make_tt2006()
-    make_tt2004()
-    make_tomek()
+    which = set(sys.argv[1:]) or {"ord", "cipa", "tt2006", "tt2004", "tomek", "fem"}
+    if "ord" in which:
+        make_ord()
+    if "cipa" in which:
+        make_cipa()
+    if "tt2006" in which:
+        make_tt2006()
+    if "tt2004" in which:
+        make_tt2004()
+    if "tomek" in which:
+        make_tomek()
+    if "fem" in which:
+        make_fem()

@@ -244,3 +244,63 @@ def test_tomek_oracle_rates_bitwise_vs_compiled_reference(oracle, celltype):
             assert np.array_equal(r.arr("rates", r.n), c.rates(t)[0])
         c.step(t, 0.005)
         t += 0.005
+
+
+# ---------------------------------------------------------------- FEM
+def _fem_cases():
+    g = np.load(GOLD / "fem_elements.npz")
+    dims = {"square": (4, 2), "hex": (8, 3), "tet": (4, 3)}
+    out = []
+    for k, kind in enumerate(g["kind"]):
+        nn, dim = dims[str(kind)]
+        out.append((str(kind), g["x"][k][:nn, :dim], g["A"][k][:nn, :nn], g["B"][k][:nn, :nn]))
+    return out, float(g["dt"]), float(g["de"])
+
+
+def test_fem_element_oracle_matches_reference_golden(oracle):
+    """The oracle's element matrices (cepo_element) equal, bit for bit, the
+    reference's Cfem::set_amat_bmat (fem.cpp:628-661) compiled from its own
+    sources, for square, hex and tet elements at the origin, translated far
+    from it, and distorted."""
+    cases, dt, de = _fem_cases()
+    assert len(cases) == 15
+    for kind, x, A, B in cases:
+        a, b = oracle.element(kind, x, de, dt)
+        assert np.array_equal(a, A), kind
+        assert np.array_equal(b, B), kind
+
+
+def test_fem_grid_element_is_the_reference_origin_element(oracle):
+    """The structured-grid assembly uses the reference's matrices of the
+    element at the origin for every element; the reference's own matrices
+    of a translated element differ from them only by the rounding of its
+    node coordinates (eps |x| / h relative: the reference's operator is not
+    translation invariant in the last bits)."""
+    cases, dt, de = _fem_cases()
+    for dim, kind in ((2, "square"), (3, "hex")):
+        a, b = oracle.fem_element(dim, 0.025, dt, de)
+        (x0, A0, B0), (xt, At, Bt) = [(x, A, B) for k, x, A, B in cases if k == kind][:2]
+        assert np.array_equal(a, A0) and np.array_equal(b, B0)
+        # the Jacobian sums coordinates of size |x| to get differences of
+        # size h: its rounding is ~eps |x| / h relative
+        scale = 4 * np.finfo(float).eps * np.abs(xt).max() / 0.025
+        assert 0 < np.abs(At - A0).max() <= scale * np.abs(A0).max()
+        assert np.abs(Bt - B0).max() <= scale * np.abs(B0).max()
+
+
+@pytest.mark.parametrize("kind", ["square", "hex", "tet"])
+def test_fem_element_bitwise_vs_compiled_reference(oracle, kind):
+    if not oracle.ref_available("fem"):
+        pytest.skip("reference not compiled here (oracle/_ref); golden fixtures cover this")
+    rng = np.random.default_rng({"square": 1, "hex": 2, "tet": 3}[kind])
+    h = 0.02
+    base = {"square": [[0, 0], [h, 0], [h, h], [0, h]],
+            "hex": [[0, 0, 0], [h, 0, 0], [h, h, 0], [0, h, 0], [0, 0, h], [h, 0, h], [h, h, h], [0, h, h]],
+            "tet": [[0, 0, 0], [h, 0, 0], [0, h, 0], [0, 0, h]]}[kind]
+    x0 = np.array(base, float)
+    for trial in range(20):
+        x = x0 + rng.uniform(-0.3, 0.3, x0.shape) * h + rng.uniform(-5, 5)
+        de, dt = rng.uniform(5e-4, 3e-3), rng.choice([0.005, 0.01, 0.02])
+        A, B = oracle.ref_fem_element(kind, x, de, dt)
+        a, b = oracle.element(kind, x, de, dt)
+        assert np.array_equal(a, A) and np.array_equal(b, B), (kind, trial)
