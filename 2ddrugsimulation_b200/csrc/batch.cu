@@ -1185,6 +1185,13 @@ int cep_batch_restore(cep_batch_t b, const void *buf, size_t bytes) {
     return fail(CEP_ERR_ARG, "checkpoint of model %d, %d instances, precision %d does not fit this batch", h.model,
                 h.n, h.precision);
   if (h.ca_cap < 0 || h.ca_cap > (1 << 24)) return fail(CEP_ERR_ARG, "corrupt checkpoint header");
+  {  // the blob must hold every region its header announces before anything of the batch changes
+    const size_t ld = (size_t)b->ld;
+    size_t need = sizeof(CkptHeader) + ld * (sizeof(double) * ((size_t)b->ns + b->np + 1) + sizeof(int) * 6);
+    if (h.has_bm) need += ld * (sizeof(double) * bm::kNumF + sizeof(int) * bm::kNumI);
+    need += ld * sizeof(double) * 2 * (size_t)h.ca_cap;
+    if (bytes < need) return fail(CEP_ERR_ARG, "checkpoint has %zu bytes, needs %zu", bytes, need);
+  }
   int rc;
   if (h.has_bm && !b->bmf &&
       ((rc = dev_alloc(b, &b->bmf, (size_t)bm::kNumF * b->ld)) || (rc = dev_alloc(b, &b->bmi, (size_t)bm::kNumI * b->ld))))

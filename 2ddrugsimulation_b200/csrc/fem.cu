@@ -1922,15 +1922,18 @@ int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, 
 // vectors in a fixed scratch area of this library (no counterpart in the
 // reference). The scratch is one file-scope device array; its address is
 // resolved once per device (the first call, which must precede any stream
-// capture) and every later call only launches work. Calls that overlap in
-// time on one device share the scratch and race: the caller serialises them.
+// capture) and every later call only launches work. The cached address
+// assumes the device's primary context lives as long as the process: after
+// cudaDeviceReset the module is loaded again and the cache is stale. Calls
+// that overlap in time on one device share the scratch and race: the caller
+// serialises them.
 namespace {
 
 constexpr int64_t kNaRows = CEP_NOALLOC_MAX_ROWS;
 constexpr int kNaMaxGrid = 1024;
-// dinv, r, q, p0, p1, z | partials [3][kNaMaxGrid] | Ctl | Status
+// dinv, r, q, p0, p1, z | partials [3][kNaMaxGrid] | Ctl | Status | first bad row
 constexpr int64_t kNaVecWords = 6 * kNaRows;
-constexpr int64_t kNaWords = kNaVecWords + 3 * kNaMaxGrid + 8 + 8;
+constexpr int64_t kNaWords = kNaVecWords + 3 * kNaMaxGrid + 8 + 8 + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNaWords];
 
@@ -1941,12 +1944,21 @@ struct NaDevice {
 NaDevice g_na_dev[64];
 std::mutex g_na_mu;
 
-__global__ void noalloc_dinv_kernel(int64_t n, const int *rp, const int *col, const double *a, double *dinv) {
+// Jacobi inverse of the caller's operator. A row without a diagonal entry,
+// or with a zero or non-finite one, keeps dinv = 1 so the solve stays finite,
+// and its index goes to *bad (smallest such row) for the blocking form to
+// report.
+__global__ void noalloc_dinv_kernel(int64_t n, const int *rp, const int *col, const double *a, double *dinv,
+                                    int *bad) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double diag = 1.0;
+  double diag = 0.0;
   for (int k = rp[i]; k < rp[i + 1]; ++k)
     if (col[k] == i) diag = a[k];
+  if (diag == 0.0 || !isfinite(diag)) {
+    atomicMin(bad, (int)i);
+    diag = 1.0;
+  }
   dinv[i] = 1.0 / diag;
 }
 
@@ -1984,15 +1996,17 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   double *p0 = base + 3 * kNaRows, *p1 = base + 4 * kNaRows, *z = base + 5 * kNaRows;
   Ctl *ctl = reinterpret_cast<Ctl *>(part + 3 * kNaMaxGrid);
   Status *stat = reinterpret_cast<Status *>(part + 3 * kNaMaxGrid + 8);
+  int *bad = reinterpret_cast<int *>(part + 3 * kNaMaxGrid + 16);
   // the same grid rule as an operator handle: one block per SM, no more
   // blocks than rows need
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nd.grid, (n + kPcgBlock - 1) / kPcgBlock));
   // what must start at zero: the barrier words and the counters
   FEM_CUDA(cudaMemsetAsync(ctl, 0, sizeof(Ctl), st));
   FEM_CUDA(cudaMemsetAsync(stat, 0, sizeof(Status), st));
+  FEM_CUDA(cudaMemsetAsync(bad, 0x7f, sizeof(int), st));  // 0x7f7f7f7f: no bad row
   const CsrView m{static_cast<const int *>(d_row_ptr), static_cast<const int *>(d_col_idx),
                   static_cast<const double *>(d_a_val), static_cast<const double *>(d_b_val)};
-  noalloc_dinv_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, m.rp, m.col, m.a, dinv);
+  noalloc_dinv_kernel<<<(n + 127) / 128, 128, 0, st>>>(n, m.rp, m.col, m.a, dinv, bad);
   FEM_CUDA(cudaGetLastError());
   PcgArgs a;
   a.n = n;
@@ -2016,9 +2030,13 @@ extern "C" int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const voi
   if (iters_out) {  // blocking status read
     Ctl c;
     Status s;
+    int first_bad = 0;
     FEM_CUDA(cudaMemcpyAsync(&c, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     FEM_CUDA(cudaMemcpyAsync(&s, stat, sizeof(Status), cudaMemcpyDeviceToHost, st));
+    FEM_CUDA(cudaMemcpyAsync(&first_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     FEM_CUDA(cudaStreamSynchronize(st));
+    if (first_bad != 0x7f7f7f7f)
+      return fail_msg(CEP_ERR_ARG, "row %d has no usable diagonal entry (missing, zero or not finite)", first_bad);
     if (c.err) return fail_msg(CEP_ERR_TIMEOUT, "PCG grid barrier ran out of its spin limit");
     *iters_out = s.last_iters;
     if (s.last_iters < 0) return fail_msg(CEP_ERR_NOT_CONVERGED, "PCG hit max_iter (%d)", max_iter);

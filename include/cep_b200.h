@@ -414,9 +414,16 @@ int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves,
  * (larger n is rejected with CEP_ERR_ARG). The first call on a device
  * resolves that area and must come before any stream capture. Calls that
  * overlap in time on one device (two streams or two host threads) share
- * the scratch and race: serialise them. Asynchronous on `stream` unless
- * iters_out is non-null, in which case the call waits and stores the
- * iteration count (CEP_ERR_NOT_CONVERGED past max_iter). */
+ * the scratch and race: serialise them. The scratch address is resolved
+ * once per device and assumes the device is never reset (cudaDeviceReset)
+ * while the library is loaded. Asynchronous on `stream` unless iters_out is
+ * non-null, in which case the call waits and stores the iteration count and
+ * reports CEP_ERR_NOT_CONVERGED past max_iter, CEP_ERR_TIMEOUT when a device
+ * barrier ran out of its spin limit, and CEP_ERR_ARG for a row without a
+ * usable (present, nonzero, finite) diagonal entry. The asynchronous form
+ * reports none of these: the next call clears the status words, and d_v may
+ * hold a partial solve. A row without a usable diagonal is preconditioned
+ * with 1 in both forms. */
 #define CEP_NOALLOC_MAX_ROWS 262144
 int cep_fem_solve_csr_noalloc(int n, const void *d_row_ptr, const void *d_col_idx, const void *d_a_val,
                               const void *d_b_val, double dt, double rtol, int max_iter, void *d_v, void *stream,

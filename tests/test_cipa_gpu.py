@@ -239,3 +239,13 @@ def test_checkpoint_resume_is_bit_identical(cep, gpu):
         cep.Batch("cipa2017", n + 32, "mixed").restore(blob)
     with pytest.raises(cep.CepError):
         cep.Batch("cipa2017", n, "fp64").restore(blob)
+    # a truncated blob is rejected before the batch changes: a restore of
+    # the whole blob afterwards still resumes bit for bit
+    c = cep.Batch("cipa2017", n, "mixed")
+    with pytest.raises(cep.CepError):
+        c.restore(blob[: len(blob) - 8])
+    c.restore(blob)
+    c.run_to_end(50000)
+    rc = c.biomarkers()
+    for k in ra:
+        assert np.array_equal(ra[k], rc[k], equal_nan=True), k

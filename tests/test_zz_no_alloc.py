@@ -65,3 +65,44 @@ def test_noalloc_rejects_oversized_and_reports_not_converged(cep, gpu, oracle):
     it = ctypes.c_int()
     rc = lib.cep_fem_solve_csr_noalloc(n, *ptrs, 0.01, 1e-15, 2, v.data_ptr(), None, ctypes.byref(it))
     assert rc == cep.ERR_NOT_CONVERGED and it.value == -2
+
+
+@pytest.mark.gpu
+def test_noalloc_on_a_second_stream_and_missing_diagonal(cep, gpu, oracle):
+    """After a call on the default stream, a call on another stream gets the
+    handle solve's result bit for bit (the per-device set-up is shared by
+    every stream); a row without a diagonal entry is reported by the
+    blocking form as an argument error."""
+    import torch
+    lib = cep.lib()
+    dt, rtol, max_iter = 0.01, 1e-9, 500
+    rp, ci, a, b = oracle.fem_assemble(2, 64, 48, 1, 0.025, dt, 0.0013)
+    n = len(rp) - 1
+    ref = cep.Fem.csr(rp, ci, a, b, dt, fmt=cep.FEM_CSR).set_solver(rtol, max_iter)
+    d = [torch.from_numpy(x).cuda() for x in (rp, ci, a, b)]
+    ptrs = [x.data_ptr() for x in d]
+    rng = np.random.default_rng(3)
+    it = ctypes.c_int()
+    v0 = torch.from_numpy(rng.uniform(-90, 30, n)).cuda()
+    assert lib.cep_fem_solve_csr_noalloc(n, *ptrs, dt, rtol, max_iter, v0.data_ptr(), None, ctypes.byref(it)) == 0
+    side = torch.cuda.Stream()
+    v = rng.uniform(-90, 30, n)
+    xr, itr, _ = ref.solve(v)
+    with torch.cuda.stream(side):
+        dv = torch.from_numpy(v.copy()).to("cuda", non_blocking=False)
+        side.synchronize()
+        rc = lib.cep_fem_solve_csr_noalloc(n, *ptrs, dt, rtol, max_iter, dv.data_ptr(), side.cuda_stream,
+                                           ctypes.byref(it))
+        assert rc == cep.OK, lib.cep_last_error().decode()
+    assert it.value == itr
+    assert np.array_equal(dv.cpu().numpy(), xr)
+    # drop the diagonal of row 5: its entry takes the left neighbour's column
+    ci2 = ci.copy()
+    k = rp[5] + int(np.flatnonzero(ci[rp[5]:rp[6]] == 5)[0])
+    ci2[k] = ci[k - 1]
+    d_ci2 = torch.from_numpy(ci2).cuda()
+    dv = torch.from_numpy(v.copy()).cuda()
+    rc = lib.cep_fem_solve_csr_noalloc(n, ptrs[0], d_ci2.data_ptr(), ptrs[2], ptrs[3], dt, rtol, max_iter,
+                                       dv.data_ptr(), None, ctypes.byref(it))
+    assert rc == cep.ERR_ARG
+    assert "row 5" in lib.cep_last_error().decode()
