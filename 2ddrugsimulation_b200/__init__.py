@@ -30,6 +30,10 @@ FLAG_DUTTA, FLAG_QUIRKS, FLAG_TT04_MCELL = 1, 2, 4
 CURRENTS = ("INa", "INaL", "Ito", "ICaL", "IKr", "IKs", "IK1")
 APDR_FIELDS = ("pace", "recal", "bcl", "apd90", "di", "t")
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+# conductances cep_batch_scale multiplies (CEP_SCALE_*), by the reference
+# deck's key stem (gna_scale -> "gna")
+SCALE = {"gna": 0, "gnal": 1, "gto": 2, "gcal": 3, "gkr": 4, "gks": 5, "gk1": 6, "gbna": 7, "gbca": 8, "gpca": 9,
+         "gpk": 10, "gkb": 11, "gncx": 12, "pnak": 13}
 HILL_WIDTH = 20
 
 BM_FIELDS = ("qnet", "inal_auc", "ical_auc", "dvmdt_repol", "dvmdt_max", "vm_peak", "vm_valley", "vm_dia",
@@ -101,6 +105,7 @@ _SIGS = {
                                             ctypes.c_double]),
     "cep_batch_set_protocol": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_double]),
+    "cep_batch_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
@@ -291,6 +296,15 @@ class Batch:
         _check(lib().cep_batch_set_pacing(self._h, bcl, stim_start, stim_dur, amp_scale))
         return self
 
+    def scale(self, conductance: str, factor):
+        """CONSTANTS[g] *= factor[i] for every instance i after init (the
+        reference's G*_Scale keys and population-of-models sweeps);
+        conductance is a SCALE key, factor a scalar or one value per
+        instance."""
+        f = np.ascontiguousarray(np.broadcast_to(np.asarray(factor, np.float64), (self.n,)))
+        _check(lib().cep_batch_scale(self._h, SCALE[conductance], _dptr(f)))
+        return self
+
     def set_protocol(self, dt: float, n_pace: int, first_pace: int = -1, dt_write: float = 1.0,
                      qnet_vm_threshold: float = -1e300):
         _check(lib().cep_batch_set_protocol(self._h, dt, n_pace, first_pace, dt_write, qnet_vm_threshold))
@@ -441,7 +455,7 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
                    precision: str = "mixed", celltype=None, dutta: bool = False, quirks: bool = True,
                    dt_write: float = 1.0, refine_above_vm: float | None = -80.0,
                    steps_per_launch: int = 50000, amp_scale: float = 1.0,
-                   states_init=None) -> dict[str, np.ndarray]:
+                   states_init=None, scales=None) -> dict[str, np.ndarray]:
     """A population run to the end of its protocol (the reference's bench loop
     for every instance), returning the biomarker records.
 
@@ -453,7 +467,9 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
     their records replaced; out["refined"] marks them. amp_scale multiplies
     the stimulus amplitude (CONSTANTS[amp] *= Stim_Amplitude,
     cipa_drug_bench.cpp:147); states_init, one state vector, replaces every
-    instance's initial states after initConsts (Is_Using_Output, :149)."""
+    instance's initial states after initConsts (Is_Using_Output, :149);
+    scales maps SCALE keys to a factor (scalar or one per instance) applied
+    after initConsts (CONSTANTS[GNa] *= gna_scale, :148)."""
     conc = np.ascontiguousarray(conc, np.float64)
     n = len(conc)
     hill = np.asarray(hill, np.float64)
@@ -465,6 +481,9 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
             b.init(celltype=None if ct is None else ct[idx], conc=conc[idx],
                    hill=hill[idx] if hill.ndim == 2 else hill, dutta=dutta, quirks=quirks)
             b.set_pacing(bcl, amp_scale=amp_scale)
+            for g, f in (scales or {}).items():
+                f = np.asarray(f, np.float64)
+                b.scale(g, f[idx] if f.ndim else f)
             if states_init is not None:
                 y0 = np.asarray(states_init, np.float64).reshape(-1)
                 b.set_states(np.ascontiguousarray(np.broadcast_to(y0, (len(idx), len(y0)))))

@@ -247,6 +247,14 @@ __global__ void pacing_kernel(double *par, int64_t ld, int64_t first, int count,
   par[p_amp * ld + i] *= amp_scale;
 }
 
+// par[pidx][i] *= factor[i] for every instance (a caller's conductance
+// scale, applied after init)
+__global__ void scale_kernel(double *par, int64_t ld, int n, int pidx, const double *factor) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  par[pidx * ld + i] *= factor[i];
+}
+
 struct RunArgs {
   double *y;
   const double *par;
@@ -1263,6 +1271,72 @@ int cep_batch_set_pacing(cep_batch_t b, double bcl, double stim_start, double st
   if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
   if (!(bcl > 0) || !std::isfinite(bcl)) return fail(CEP_ERR_ARG, "bcl must be positive");
   return model_info(b->model)->pacing(b, 0, b->n, bcl, stim_start, stim_dur, amp_scale);
+}
+
+// Parameter row of a scalable conductance for a model, or -1.
+static int scale_param_index(int model, int g) {
+  using namespace cep;
+  switch (model) {
+    case CEP_MODEL_ORD2011:
+    case CEP_MODEL_CIPA2017:
+      switch (g) {
+        case CEP_SCALE_GNA: return ord::P_GNa; case CEP_SCALE_GNAL: return ord::P_GNaL;
+        case CEP_SCALE_GTO: return ord::P_Gto; case CEP_SCALE_GCAL: return ord::P_PCa;
+        case CEP_SCALE_GKR: return ord::P_GKr; case CEP_SCALE_GKS: return ord::P_GKs;
+        case CEP_SCALE_GK1: return ord::P_GK1; case CEP_SCALE_GKB: return ord::P_GKb;
+        case CEP_SCALE_GNCX: return ord::P_Gncx; case CEP_SCALE_PNAK: return ord::P_Pnak;
+        default: return -1;
+      }
+    case CEP_MODEL_TOMEK2019:
+      switch (g) {
+        case CEP_SCALE_GNA: return tomek::P_GNa; case CEP_SCALE_GNAL: return tomek::P_GNaL;
+        case CEP_SCALE_GTO: return tomek::P_Gto; case CEP_SCALE_GCAL: return tomek::P_PCa;
+        case CEP_SCALE_GKR: return tomek::P_GKr; case CEP_SCALE_GKS: return tomek::P_GKs;
+        case CEP_SCALE_GK1: return tomek::P_GK1; case CEP_SCALE_GKB: return tomek::P_GKb;
+        case CEP_SCALE_GNCX: return tomek::P_Gncx; case CEP_SCALE_PNAK: return tomek::P_Pnak;
+        default: return -1;
+      }
+    case CEP_MODEL_TT2006:
+      switch (g) {
+        case CEP_SCALE_GNA: return tt06::P_gNa; case CEP_SCALE_GTO: return tt06::P_gto;
+        case CEP_SCALE_GCAL: return tt06::P_gCaL; case CEP_SCALE_GKR: return tt06::P_gKr;
+        case CEP_SCALE_GKS: return tt06::P_gKs; case CEP_SCALE_GK1: return tt06::P_gK1;
+        case CEP_SCALE_GBNA: return tt06::P_gbna; case CEP_SCALE_GBCA: return tt06::P_gbca;
+        case CEP_SCALE_GPCA: return tt06::P_gpCa; case CEP_SCALE_GPK: return tt06::P_gpK;
+        default: return -1;
+      }
+    case CEP_MODEL_TT2004:
+      switch (g) {
+        case CEP_SCALE_GNA: return tt04::P_gNa; case CEP_SCALE_GTO: return tt04::P_gto;
+        case CEP_SCALE_GCAL: return tt04::P_gCaL; case CEP_SCALE_GKR: return tt04::P_gKr;
+        case CEP_SCALE_GKS: return tt04::P_gKs; case CEP_SCALE_GK1: return tt04::P_gK1;
+        case CEP_SCALE_GBNA: return tt04::P_gbna; case CEP_SCALE_GBCA: return tt04::P_gbca;
+        case CEP_SCALE_GPCA: return tt04::P_gpCa; case CEP_SCALE_GPK: return tt04::P_gpK;
+        default: return -1;
+      }
+    default: return -1;
+  }
+}
+
+int cep_batch_scale(cep_batch_t b, int conductance, const double *factor) {
+  if (!b || !factor) return fail(CEP_ERR_ARG, "null argument");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (conductance < 0 || conductance >= CEP_SCALE_COUNT)
+    return fail(CEP_ERR_ARG, "conductance %d is not a CEP_SCALE_* value", conductance);
+  const int pidx = scale_param_index(b->model, conductance);
+  if (pidx < 0) return fail(CEP_ERR_UNSUPPORTED, "model %d has no scalable parameter for conductance %d", b->model,
+                            conductance);
+  for (int i = 0; i < b->n; ++i)
+    if (!std::isfinite(factor[i]) || factor[i] < 0.0)
+      return fail(CEP_ERR_ARG, "factor[%d] = %g is not a finite non-negative value", i, factor[i]);
+  double *d_f = nullptr;
+  CEP_CUDA(cudaMallocAsync((void **)&d_f, sizeof(double) * b->n, b->stream));
+  CEP_CUDA(cudaMemcpyAsync(d_f, factor, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
+  cep::scale_kernel<<<(b->n + kBlock - 1) / kBlock, kBlock, 0, b->stream>>>(b->params, b->ld, b->n, pidx, d_f);
+  CEP_CUDA(cudaGetLastError());
+  CEP_CUDA(cudaFreeAsync(d_f, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
 }
 
 int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,

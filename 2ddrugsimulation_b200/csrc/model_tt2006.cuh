@@ -16,7 +16,11 @@ namespace tt06 {
 
 constexpr int kNumStates = 19;
 enum : int { V = 0, K_i, Na_i, Ca_i, Xr1, Xr2, Xs, m, h, j, Ca_ss, d, f, f2, fCass, s, r, Ca_SR, R_prime };
-enum : int { P_gCaL = 0, P_gK1, P_gKs, P_gNa, P_gto, P_gKr, P_amp, P_BCL, P_stim_start, P_duration, kNumParams };
+enum : int {
+  P_gCaL = 0, P_gK1, P_gKs, P_gNa, P_gto, P_gKr, P_amp, P_BCL, P_stim_start, P_duration,
+  P_gbna, P_gbca, P_gpCa, P_gpK,  // background and pump conductances (scalable per instance)
+  kNumParams
+};
 
 namespace k {
 constexpr double R = 8314.472, T = 310, F = 96485.3415, Cm = 0.185, V_c = 0.016404, P_kna = 0.03, K_o = 5.4;
@@ -41,6 +45,7 @@ template <class G>
 struct Par {
   G gCaL, gK1, gKs, gNa, gto, gKr;
   double amp, BCL, stim_start, duration;
+  G gbna, gbca, gpCa, gpK;
 };
 template <class G>
 struct Cur {
@@ -68,6 +73,8 @@ __device__ __forceinline__ void load_par(Par<G> &q, const double *__restrict__ p
   q.gNa = (G)p[P_gNa * ld + i]; q.gto = (G)p[P_gto * ld + i]; q.gKr = (G)p[P_gKr * ld + i];
   q.amp = p[P_amp * ld + i]; q.BCL = p[P_BCL * ld + i]; q.stim_start = p[P_stim_start * ld + i];
   q.duration = p[P_duration * ld + i];
+  q.gbna = (G)p[P_gbna * ld + i]; q.gbca = (G)p[P_gbca * ld + i]; q.gpCa = (G)p[P_gpCa * ld + i];
+  q.gpK = (G)p[P_gpK * ld + i];
 }
 
 // One cell step: rates at (t, y); if `update`, the reference's Rush-Larsen /
@@ -131,7 +138,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
                   P::rc(one + (G)0.1245 * P::ex((G)-0.1 * v * (G)k::FRT) + (G)0.0353 * P::ex(-v * (G)k::FRT));
   const G E_Na = (G)k::RTF * P::lg(P::dv((G)k::Na_o, nai_g));
   const G i_Na = q.gNa * p3((G)y.m) * (G)y.h * (G)y.j * (v - E_Na);
-  const G i_b_Na = (G)k::g_bna * (v - E_Na);
+  const G i_b_Na = q.gbna * (v - E_Na);
   const G eg = P::ex((G)k::gmma * v * (G)k::FRT), eg1 = P::ex(((G)k::gmma - one) * v * (G)k::FRT);
   const G i_NaCa = P::dv((G)k::K_NaCa * (eg * p3(nai_g) * (G)k::Ca_o - eg1 * (G)k::Na_o3 * cai_g * (G)k::alpha),
                          (G)k::naca_den * (one + (G)k::K_sat * eg1));
@@ -161,9 +168,9 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
                   e - 1.0);
   }
   const G E_Ca = (G)(0.5 * k::RTF) * P::lg(P::dv((G)k::Ca_o, cai_g));
-  const G i_b_Ca = (G)k::g_bca * (v - E_Ca);
-  const G i_p_K = P::dv((G)k::g_pK * vek, one + P::ex(((G)25.0 - v) * (G)(1.0 / 5.98)));
-  const G i_p_Ca = P::dv((G)k::g_pCa * cai_g, cai_g + (G)k::K_pCa);
+  const G i_b_Ca = q.gbca * (v - E_Ca);
+  const G i_p_K = P::dv(q.gpK * vek, one + P::ex(((G)25.0 - v) * (G)(1.0 / 5.98)));
+  const G i_p_Ca = P::dv(q.gpCa * cai_g, cai_g + (G)k::K_pCa);
   const G dV = -(i_K1 + i_to + i_Kr + i_Ks + i_CaL + i_NaK + i_Na + i_b_Na + i_NaCa + i_b_Ca + i_p_K + i_p_Ca + i_Stim);
   cur.INa = i_Na; cur.INaL = (G)0; cur.Ito = i_to; cur.ICaL = i_CaL; cur.IKr = i_Kr; cur.IKs = i_Ks;
   cur.IK1 = i_K1; cur.dVdt = dV;
@@ -237,6 +244,7 @@ __device__ __forceinline__ void init_instance(double *__restrict__ par, double *
   double *p = par + i;
   p[P_gCaL * ld] = gCaL; p[P_gK1 * ld] = gK1; p[P_gKs * ld] = gKs; p[P_gNa * ld] = gNa; p[P_gto * ld] = gto;
   p[P_gKr * ld] = gKr; p[P_amp * ld] = 52; p[P_BCL * ld] = 1000; p[P_stim_start * ld] = 10; p[P_duration * ld] = 1;
+  p[P_gbna * ld] = k::g_bna; p[P_gbca * ld] = k::g_bca; p[P_gpCa * ld] = k::g_pCa; p[P_gpK * ld] = k::g_pK;
   const double y0[kNumStates] = {-85.23, 136.89, 8.604, 0.000126, 0.00621, 0.4712, 0.0095, 0.00172, 0.7444, 0.7045,
                                  0.00036, 3.373e-5, 0.7888, 0.9755, 0.9953, 0.999998, 2.42e-8, 3.64, 0.9073};
 #pragma unroll

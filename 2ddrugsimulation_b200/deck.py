@@ -21,6 +21,11 @@ therefore uses this library's ORd with Dutta on and without the
 DrugSimulation build's quirks by default. One difference remains: that
 build, like DrugSimulation's, leaves PCap, PCaNa and PCaK unblocked when
 the Hill row blocks PCa, while the quirk-free form here blocks them too.
+Of the deck's conductance scales, these benches apply only Gna_Scale
+(CONSTANTS[GNa] *= gna_scale after initConsts, cipa_drug_bench.cpp:148);
+`run` does the same. The other G*_Scale keys are read (the ANM benches of
+the ten Tusscher models use them) and, as in the reference's drug benches,
+have no effect here; Batch.scale applies any of them to a population.
 """
 from __future__ import annotations
 
@@ -191,11 +196,6 @@ def run(d: Deck, hill=None, precision: str = "mixed", states_init=None, quirks: 
     (conc, hill) rows (modes 2, 3, 33333)."""
     import importlib
     cep = importlib.import_module("2ddrugsimulation_b200")
-    unsupported = [f for f in ("gks_scale", "gkr_scale", "gcal_scale", "gna_scale", "gk1_scale", "gbna_scale",
-                               "gbca_scale", "gto_scale", "gpca_scale", "gpk_scale", "gnal_scale")
-                   if getattr(d, f) != 1.0]
-    if unsupported:
-        raise cep.CepError(cep.ERR_UNSUPPORTED, f"conductance scales {unsupported} are not supported")
     mode = d.simulation_mode
     if mode == 1:  # apdr_bench: 2004_a (M cell) for celltype 0, 2004_b otherwise (apdr_bench.cpp:77-84)
         bcls = cep.apdr_bcls(d.bcl_init, d.bcl_end, d.bcl_decrement)
@@ -220,6 +220,7 @@ def run(d: Deck, hill=None, precision: str = "mixed", states_init=None, quirks: 
     out = cep.run_population(models[mode], conc, rows, bcl=d.bcl_init, dt=d.dt, n_pace=n_pace,
                              first_pace=first_pace, precision=precision,
                              celltype=d.celltype, dutta=models[mode] == "ord2011", quirks=quirks,
-                             dt_write=d.dt_write, amp_scale=d.stim_amp, states_init=states_init)
+                             dt_write=d.dt_write, amp_scale=d.stim_amp, states_init=states_init,
+                             scales={"gna": d.gna_scale})
     out["conc"], out["hill"] = conc, rows
     return out

@@ -135,6 +135,23 @@ int cep_batch_init(cep_batch_t b, const double *celltype, const double *conc, co
  * model defaults. */
 int cep_batch_set_pacing(cep_batch_t b, double bcl, double stim_start, double stim_dur, double amp_scale);
 
+/* Per-instance conductance scaling applied after init, the reference's
+ * CONSTANTS[x] *= scale at its call sites: the deck's G*_Scale keys
+ * (CONSTANTS[GNa] *= gna_scale, cipa_drug_bench.cpp:148, heart.cpp:222;
+ * the TT benches' g_Ks .. g_pK, anm_bench_custom.cpp:62-71) and the
+ * population-of-models sweeps (population_tn2006.cpp:72-101: ten scale
+ * factors per instance). factor[n] multiplies the named conductance of
+ * every instance; like the reference, a derived constant computed inside
+ * initConsts from it (ORd's PCap from PCa) is left as it is.
+ * CEP_ERR_UNSUPPORTED for a conductance the model does not have as a
+ * parameter (ORd's background currents are fixed constants). */
+enum {
+  CEP_SCALE_GNA = 0, CEP_SCALE_GNAL, CEP_SCALE_GTO, CEP_SCALE_GCAL, CEP_SCALE_GKR, CEP_SCALE_GKS,
+  CEP_SCALE_GK1, CEP_SCALE_GBNA, CEP_SCALE_GBCA, CEP_SCALE_GPCA, CEP_SCALE_GPK, CEP_SCALE_GKB,
+  CEP_SCALE_GNCX, CEP_SCALE_PNAK, CEP_SCALE_COUNT
+};
+int cep_batch_scale(cep_batch_t b, int conductance, const double *factor);
+
 /* Protocol of the run: fixed step dt (ms), n_pace paces at the instance's
  * BCL, biomarkers evaluated on paces >= first_pace (first_pace = n_pace-250
  * reproduces cipa_drug_bench.cpp:296; n_pace-1 is last-beat mode; -1 turns

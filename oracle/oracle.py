@@ -110,6 +110,7 @@ def lib() -> ctypes.CDLL:
         L.cepo_fem_nnz.restype = ctypes.c_long
         L.cepo_fem_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, _dp, ctypes.c_int, _ip, _ip, _dp, _dp]
+        L.cepo_scale.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_int, ctypes.c_double]
         L.cepo_fem_element.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp, _dp]
         L.cepo_element.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.cepo_pseudo_ecg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp,
@@ -177,6 +178,11 @@ class Cell:
 
     def set_pacing(self, bcl: float, stim_start: float = -1.0, stim_dur: float = -1.0, amp_scale: float = 1.0):
         lib().cepo_set_pacing(ctypes.byref(self.c), bcl, stim_start, stim_dur, amp_scale)
+
+    def scale(self, conductance: int, factor: float):
+        """CONSTANTS[x] *= factor (conductance numbered as CEP_SCALE_*)."""
+        if lib().cepo_scale(ctypes.byref(self.c), int(conductance), float(factor)) != 0:
+            raise ValueError(f"{self.model} has no scalable conductance {conductance}")
 
     def step(self, t: float, dt: float) -> CepoCurrents:
         cur = CepoCurrents()

@@ -117,6 +117,17 @@ void cepo_set_pacing(cepo_cell *c, double bcl, double stim_start, double stim_du
   }
 }
 
+int cepo_scale(cepo_cell *c, int g, double f) {
+  switch (c->model) {
+    case CEPO_ORD2011: return cepo_ord_scale(c, g, f);
+    case CEPO_CIPA2017: return cepo_cipa_scale(c, g, f);
+    case CEPO_TT2006: return cepo_tt06_scale(c, g, f);
+    case CEPO_TT2004: return cepo_tt04_scale(c, g, f);
+    case CEPO_TOMEK2019: return cepo_tomek_scale(c, g, f);
+  }
+  return -1;
+}
+
 void cepo_step(const cepo_cell *c, double t, double dt, double *y, cepo_currents *cur) {
   switch (c->model) {
     case CEPO_ORD2011: cepo_ord_step(c, t, dt, y, cur); break;

@@ -48,6 +48,15 @@ void cepo_init_states(const cepo_cell *c, double *y);
 /* Overrides used by the drivers (CONSTANTS[BCL], CONSTANTS[amp] *= scale). */
 void cepo_set_pacing(cepo_cell *c, double bcl, double stim_start, double stim_dur, double stim_amp_scale);
 
+/* CONSTANTS[x] *= f after init for conductance x (numbered as the
+ * library's CEP_SCALE_*); -1 if the model has no such constant. */
+int cepo_scale(cepo_cell *c, int g, double f);
+int cepo_ord_scale(cepo_cell *c, int g, double f);
+int cepo_cipa_scale(cepo_cell *c, int g, double f);
+int cepo_tt06_scale(cepo_cell *c, int g, double f);
+int cepo_tt04_scale(cepo_cell *c, int g, double f);
+int cepo_tomek_scale(cepo_cell *c, int g, double f);
+
 /* One fixed-step update of the reference scheme: rates at (t, y), then the
  * model's Rush-Larsen / forward-Euler update into y. `cur` (may be NULL)
  * receives the currents at (t, y). */

@@ -525,3 +525,16 @@ void cepo_tomek_step(const cepo_cell *c, double t, double dt, double *S, cepo_cu
   static const int fe[] = {V, CaMKt, cass, nai, nass, ki, kss, cansr, cajsr, cai, C1, C2, C3, I, O};
   for (unsigned k = 0; k < sizeof(fe) / sizeof(fe[0]); ++k) S[fe[k]] += R_[fe[k]] * dt;
 }
+
+/* CONSTANTS[x] *= f after initConsts, x one of the CEP scale conductances
+ * (0 GNa, 1 GNaL, 2 Gto, 3 PCa, 4 GKr, 5 GKs, 6 GK1, 11 GKb, 12 Gncx,
+ * 13 Pnak), as the reference's call sites do (cipa_drug_bench.cpp:148).
+ * Returns -1 for a conductance the model has no constant for here. */
+int cepo_tomek_scale(cepo_cell *c, int g, double f) {
+  tomek_p *q = (tomek_p *)c->p;
+  double *x = g == 0 ? &q->GNa : g == 1 ? &q->GNaL : g == 2 ? &q->Gto : g == 3 ? &q->PCa : g == 4 ? &q->GKr
+            : g == 5 ? &q->GKs : g == 6 ? &q->GK1 : g == 11 ? &q->GKb : g == 12 ? &q->Gncx : g == 13 ? &q->Pnak : 0;
+  if (!x) return -1;
+  *x *= f;
+  return 0;
+}

@@ -237,3 +237,15 @@ void cepo_tt04_step(const cepo_cell *c, double t, double dt, double *S, cepo_cur
   S[Ca_i] += R_[Ca_i] * dt;
   S[Ca_SR] += R_[Ca_SR] * dt;
 }
+
+/* CONSTANTS[x] *= f after initConsts (population_tn2006.cpp:92-101,
+ * anm_bench_custom.cpp:62-71): 0 g_Na, 2 g_to, 3 g_CaL, 4 g_Kr, 5 g_Ks,
+ * 6 g_K1, 7 g_bna, 8 g_bca, 9 g_pCa, 10 g_pK. Returns -1 otherwise. */
+int cepo_tt04_scale(cepo_cell *c, int g, double f) {
+  tt04_p *q = (tt04_p *)c->p;
+  double *x = g == 0 ? &q->g_Na : g == 2 ? &q->g_to : g == 3 ? &q->g_CaL : g == 4 ? &q->g_Kr : g == 5 ? &q->g_Ks
+            : g == 6 ? &q->g_K1 : g == 7 ? &q->g_bna : g == 8 ? &q->g_bca : g == 9 ? &q->g_pCa : g == 10 ? &q->g_pK : 0;
+  if (!x) return -1;
+  *x *= f;
+  return 0;
+}

@@ -74,11 +74,11 @@ def test_hill_csv_and_population_order(tmp_path):
         deck.read_hill_csv("header only\n")
 
 
-def test_unsupported_modes_and_scales_are_refused(cep):
+def test_unsupported_modes_are_refused(cep):
     with pytest.raises(cep.CepError):
         deck.run(deck.read_deck("Simulation_Mode = 5\n"))
-    with pytest.raises(cep.CepError):
-        deck.run(deck.read_deck("Simulation_Mode = 3\nGNa_Scale = 0.5\n"), hill=np.zeros((1, 14)))
+    d = deck.read_deck("Simulation_Mode = 3\nGNa_Scale = 0.5\nGKs_Scale = 2\n")
+    assert d.gna_scale == 0.5 and d.gks_scale == 2.0
 
 
 @pytest.mark.gpu
@@ -94,6 +94,13 @@ def test_deck_runs_match_the_direct_calls(cep, gpu):
     for k in ("apd90", "apd50", "cad90", "qnet", "vm_peak"):
         assert np.array_equal(out[k], ref[k]), k
     assert (out["status"] == cep.INST_DONE).all() and out["apd90"].shape == (6,)
+    # Gna_Scale multiplies GNa after initConsts (cipa_drug_bench.cpp:148)
+    d2 = deck.read_deck(DECK + "Gna_Scale = 0.5\n")
+    out2 = deck.run(d2, hill, precision="fp64")
+    ref2 = cep.run_population("ord2011", conc, rows, bcl=1000.0, dt=0.005, n_pace=2, first_pace=1, precision="fp64",
+                              celltype=1.0, dutta=True, quirks=False, amp_scale=1.5, scales={"gna": 0.5})
+    assert np.array_equal(out2["dvmdt_max"], ref2["dvmdt_max"])
+    assert (out2["dvmdt_max"] < out["dvmdt_max"]).all()
     # Simulation_Mode 1: dynamic restitution of the M cell (celltype 0)
     a = deck.read_deck("Simulation_Mode = 1\nBasic_Cycle_Length = 500\nBCL_End = 300\nBCL_Step = 100\n"
                        "Number_of_Pacing = 4\nTime_Step = 0.02\n")
