@@ -106,6 +106,8 @@ _SIGS = {
     "cep_batch_set_protocol": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_double]),
     "cep_batch_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "cep_batch_get_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "cep_batch_set_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
@@ -119,6 +121,7 @@ _SIGS = {
                                            _dp]),
     "cep_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "cep_batch_rates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp, _dp]),
+    "cep_batch_rates_all": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, _dp]),
     "cep_batch_checkpoint_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
     "cep_batch_checkpoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "cep_batch_restore": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
@@ -305,6 +308,17 @@ class Batch:
         _check(lib().cep_batch_scale(self._h, SCALE[conductance], _dptr(f)))
         return self
 
+    def conductance(self, conductance: str) -> np.ndarray:
+        """The named conductance of every instance (its CONSTANTS value)."""
+        v = np.zeros(self.n)
+        _check(lib().cep_batch_get_conductance(self._h, SCALE[conductance], _dptr(v)))
+        return v
+
+    def set_conductance(self, conductance: str, values):
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), (self.n,)))
+        _check(lib().cep_batch_set_conductance(self._h, SCALE[conductance], _dptr(v)))
+        return self
+
     def set_protocol(self, dt: float, n_pace: int, first_pace: int = -1, dt_write: float = 1.0,
                      qnet_vm_threshold: float = -1e300):
         _check(lib().cep_batch_set_protocol(self._h, dt, n_pace, first_pace, dt_write, qnet_vm_threshold))
@@ -403,6 +417,13 @@ class Batch:
         cur = np.zeros((7, self.n))
         _check(lib().cep_batch_rates(self._h, t, _dptr(dv), _dptr(cur)))
         return dv, cur
+
+    def rates_all(self, t: float) -> np.ndarray:
+        """The model's full RATES vector of every instance at its current
+        state, [n, n_states]."""
+        r = np.zeros((self.n, self.ns))
+        _check(lib().cep_batch_rates_all(self._h, t, _dptr(r)))
+        return r
 
     def restitution(self, bcls, n_pace: int, dt: float, steps_per_launch: int = 20000) -> dict[str, np.ndarray]:
         """Dynamic restitution (apdr_bench.cpp:103-232) of every instance: the

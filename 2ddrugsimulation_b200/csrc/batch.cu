@@ -79,6 +79,7 @@ namespace cep {
 // ------------------------------------------------------------------ traits
 struct OrdModel {
   static constexpr bool kCipa = false;
+  static constexpr bool kHasRates = true;  // the step runs under F64Rates
   static constexpr int kStates = ord::kNumStates;
   static constexpr int kParams = ord::kNumParams;
   static constexpr int kCai = ord::cai;
@@ -129,6 +130,7 @@ struct CipaModel : OrdModel {
 
 struct Tt06Model {
   static constexpr bool kCipa = false;
+  static constexpr bool kHasRates = false;
   static constexpr int kStates = tt06::kNumStates;
   static constexpr int kParams = tt06::kNumParams;
   static constexpr int kCai = tt06::Ca_i;
@@ -161,6 +163,7 @@ struct Tt06Model {
 
 struct Tt04Model {
   static constexpr bool kCipa = false;
+  static constexpr bool kHasRates = false;
   static constexpr int kStates = tt04::kNumStates;
   static constexpr int kParams = tt04::kNumParams;
   static constexpr int kCai = tt04::Ca_i;
@@ -194,6 +197,7 @@ struct Tt04Model {
 
 struct TomekModel {
   static constexpr bool kCipa = false;
+  static constexpr bool kHasRates = true;
   static constexpr int kStates = tomek::kNumStates;
   static constexpr int kParams = tomek::kNumParams;
   static constexpr int kCai = tomek::cai;
@@ -737,6 +741,23 @@ __global__ void rates_kernel(const double *s, const double *par, int64_t ld, int
   }
 }
 
+// The full RATES vector at the current state: one step under F64Rates
+// leaves every state's right-hand side in its place; out[i][ns] (AoS).
+template <class M>
+__global__ void rates_all_kernel(const double *s, const double *par, int64_t ld, int n, double t, double *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  typename M::template Y<double> y;
+  typename M::template Par<double> q;
+  M::template load<double>(y, s, ld, i);
+  M::template load_par<double>(q, par, ld, i);
+  typename M::template Cur<double> c;
+  M::template step<F64Rates>(y, q, t, 0.0, -1, true, c);
+  double tmp[64];
+  M::template store<double>(y, tmp, 1, 0);  // state order, stride 1
+  for (int k = 0; k < M::kStates; ++k) out[i * M::kStates + k] = tmp[k];
+}
+
 __global__ void collect_bm_kernel(bm::View v, const int *status, int64_t first, int count, cep_biomarkers_t *out) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
@@ -848,6 +869,17 @@ struct Ops {
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "clamp launch failed: %s", cudaGetErrorString(e));
   }
+  static int launch_rates_all(cep_batch *b, double t, double *out) {
+    if constexpr (M::kHasRates) {
+      const int grid = (b->n + kBlock - 1) / kBlock;
+      rates_all_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->states, b->params, b->ld, b->n, t, out);
+      return cudaGetLastError() == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "rates launch failed");
+    } else {
+      (void)t; (void)out;
+      return fail(CEP_ERR_UNSUPPORTED, "model %d integrates with its own fixed-step scheme only (no RATES vector)",
+                  b->model);
+    }
+  }
   static int launch_rates(cep_batch *b, double t, double *dvdt, double *cur) {
     const int grid = (b->n + kBlock - 1) / kBlock;
     rates_kernel<M><<<grid, kBlock, 0, b->stream>>>(b->states, b->params, b->ld, b->n, t, -1, dvdt, cur);
@@ -866,6 +898,7 @@ struct ModelInfo {
   int (*tissue)(cep_batch *, const TissueArgs &);
   int (*restit)(cep_batch *, const RestitArgs &);
   int (*clamp)(cep_batch *, const ClampArgs &);
+  int (*rates_all)(cep_batch *, double, double *);
 };
 
 const ModelInfo *model_info(int model) {
@@ -873,27 +906,32 @@ const ModelInfo *model_info(int model) {
                                   &Ops<OrdModel>::launch_init, &Ops<OrdModel>::launch_pacing,
                                   &Ops<OrdModel>::launch_reset, &Ops<OrdModel>::launch_run,
                                   &Ops<OrdModel>::launch_rates, OrdModel::p_bcl(), &Ops<OrdModel>::launch_tissue,
-                                  &Ops<OrdModel>::launch_restit, &Ops<OrdModel>::launch_clamp};
+                                  &Ops<OrdModel>::launch_restit, &Ops<OrdModel>::launch_clamp,
+                                  &Ops<OrdModel>::launch_rates_all};
   static const ModelInfo cipa_info{CipaModel::kStates, CipaModel::kParams, CipaModel::kCai,
                                    &Ops<CipaModel>::launch_init, &Ops<CipaModel>::launch_pacing,
                                    &Ops<CipaModel>::launch_reset, &Ops<CipaModel>::launch_run,
                                    &Ops<CipaModel>::launch_rates, CipaModel::p_bcl(), &Ops<CipaModel>::launch_tissue,
-                                  &Ops<CipaModel>::launch_restit, &Ops<CipaModel>::launch_clamp};
+                                  &Ops<CipaModel>::launch_restit, &Ops<CipaModel>::launch_clamp,
+                                  &Ops<CipaModel>::launch_rates_all};
   static const ModelInfo tt06_info{Tt06Model::kStates, Tt06Model::kParams, Tt06Model::kCai,
                                    &Ops<Tt06Model>::launch_init, &Ops<Tt06Model>::launch_pacing,
                                    &Ops<Tt06Model>::launch_reset, &Ops<Tt06Model>::launch_run,
                                    &Ops<Tt06Model>::launch_rates, Tt06Model::p_bcl(), &Ops<Tt06Model>::launch_tissue,
-                                  &Ops<Tt06Model>::launch_restit, &Ops<Tt06Model>::launch_clamp};
+                                  &Ops<Tt06Model>::launch_restit, &Ops<Tt06Model>::launch_clamp,
+                                  &Ops<Tt06Model>::launch_rates_all};
   static const ModelInfo tomek_info{TomekModel::kStates, TomekModel::kParams, TomekModel::kCai,
                                    &Ops<TomekModel>::launch_init, &Ops<TomekModel>::launch_pacing,
                                    &Ops<TomekModel>::launch_reset, &Ops<TomekModel>::launch_run,
                                    &Ops<TomekModel>::launch_rates, TomekModel::p_bcl(), &Ops<TomekModel>::launch_tissue,
-                                  &Ops<TomekModel>::launch_restit, &Ops<TomekModel>::launch_clamp};
+                                  &Ops<TomekModel>::launch_restit, &Ops<TomekModel>::launch_clamp,
+                                  &Ops<TomekModel>::launch_rates_all};
   static const ModelInfo tt04_info{Tt04Model::kStates, Tt04Model::kParams, Tt04Model::kCai,
                                    &Ops<Tt04Model>::launch_init, &Ops<Tt04Model>::launch_pacing,
                                    &Ops<Tt04Model>::launch_reset, &Ops<Tt04Model>::launch_run,
                                    &Ops<Tt04Model>::launch_rates, Tt04Model::p_bcl(), &Ops<Tt04Model>::launch_tissue,
-                                  &Ops<Tt04Model>::launch_restit, &Ops<Tt04Model>::launch_clamp};
+                                  &Ops<Tt04Model>::launch_restit, &Ops<Tt04Model>::launch_clamp,
+                                  &Ops<Tt04Model>::launch_rates_all};
   switch (model) {
     case CEP_MODEL_TT2006: return &tt06_info;
     case CEP_MODEL_TT2004: return &tt04_info;
@@ -1339,6 +1377,40 @@ int cep_batch_scale(cep_batch_t b, int conductance, const double *factor) {
   return CEP_OK;
 }
 
+static int conductance_row(cep_batch_t b, int conductance, int *pidx) {
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (conductance < 0 || conductance >= CEP_SCALE_COUNT)
+    return fail(CEP_ERR_ARG, "conductance %d is not a CEP_SCALE_* value", conductance);
+  *pidx = scale_param_index(b->model, conductance);
+  if (*pidx < 0) return fail(CEP_ERR_UNSUPPORTED, "model %d has no parameter for conductance %d", b->model, conductance);
+  return CEP_OK;
+}
+
+int cep_batch_get_conductance(cep_batch_t b, int conductance, double *values) {
+  if (!b || !values) return fail(CEP_ERR_ARG, "null argument");
+  int pidx = 0;
+  const int rc = conductance_row(b, conductance, &pidx);
+  if (rc) return rc;
+  CEP_CUDA(cudaMemcpyAsync(values, b->params + (size_t)pidx * b->ld, sizeof(double) * b->n, cudaMemcpyDeviceToHost,
+                           b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
+int cep_batch_set_conductance(cep_batch_t b, int conductance, const double *values) {
+  if (!b || !values) return fail(CEP_ERR_ARG, "null argument");
+  int pidx = 0;
+  const int rc = conductance_row(b, conductance, &pidx);
+  if (rc) return rc;
+  for (int i = 0; i < b->n; ++i)
+    if (!std::isfinite(values[i]) || values[i] < 0.0)
+      return fail(CEP_ERR_ARG, "values[%d] = %g is not a finite non-negative value", i, values[i]);
+  CEP_CUDA(cudaMemcpyAsync(b->params + (size_t)pidx * b->ld, values, sizeof(double) * b->n, cudaMemcpyHostToDevice,
+                           b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return CEP_OK;
+}
+
 int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,
                            double qnet_vm_threshold) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
@@ -1643,6 +1715,19 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents) {
   CEP_CUDA(cudaFreeAsync(d, b->stream));
   CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;
+}
+
+int cep_batch_rates_all(cep_batch_t b, double t, double *rates) {
+  if (!b || !rates) return fail(CEP_ERR_ARG, "null argument");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  double *d = nullptr;
+  const size_t bytes = sizeof(double) * (size_t)b->ns * b->n;
+  CEP_CUDA(cudaMallocAsync((void **)&d, bytes, b->stream));
+  int rc = model_info(b->model)->rates_all(b, t, d);
+  if (!rc) CEP_CUDA(cudaMemcpyAsync(rates, d, bytes, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaFreeAsync(d, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
+  return rc;
 }
 
 }  // extern "C"

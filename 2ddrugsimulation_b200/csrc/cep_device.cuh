@@ -37,6 +37,7 @@ __device__ __forceinline__ double div64(double a, double b) {
 struct F64 {
   using G = double;
   static constexpr bool kMixed = false;
+  static constexpr bool kRates = false;
   __device__ __forceinline__ static double ex(double x) { return ::exp(x); }
   __device__ __forceinline__ static double lg(double x) { return ::log(x); }
   __device__ __forceinline__ static double dv(double a, double b) { return div64(a, b); }
@@ -50,6 +51,7 @@ struct F64 {
 struct Mixed {
   using G = float;
   static constexpr bool kMixed = true;
+  static constexpr bool kRates = false;
   __device__ __forceinline__ static float ex(float x) { return __expf(x); }
   __device__ __forceinline__ static float lg(float x) { return __logf(x); }
   __device__ __forceinline__ static float dv(float a, float b) { return __fdividef(a, b); }
@@ -57,6 +59,23 @@ struct Mixed {
   __device__ __forceinline__ static float pw(float x, float y) { return __powf(x, y); }
   __device__ __forceinline__ static float sq(float x) { return sqrtf(x); }
 };
+
+// FP64 with every update of a step replaced by the state's right-hand side:
+// after one step in this policy the state array holds the model's RATES
+// (a gate's (y_inf - y)/tau, the forward-Euler derivative of every other
+// state), as computeRates fills them for an ODE solver (the reference
+// integrates CiPA-ORd and ToR-ORd with CVODE through computeRates,
+// CEPCell_NEO/modules/commons.cpp:26-35).
+struct F64Rates : F64 {
+  static constexpr bool kRates = true;
+};
+
+// Forward-Euler update y += d dt, or y = d (the rate) under F64Rates.
+template <class P>
+__device__ __forceinline__ void fe(double &y, double d, double dt) {
+  if constexpr (P::kRates) y = d;
+  else y = y + d * dt;
+}
 
 // x^2, x^3, x^4, x^8 by repeated products (the reference calls pow() with
 // integral exponents; products differ from a correctly rounded pow by at
@@ -98,6 +117,8 @@ __device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, type
     else
       f = (G)1 - P::ex(-a);
     return y + (double)((yinf - (G)y) * f);
+  } else if constexpr (P::kRates) {
+    return div64(yinf - y, tau);
   } else {
     return yinf - (yinf - y) * ::exp(div64(-dt, tau));
   }

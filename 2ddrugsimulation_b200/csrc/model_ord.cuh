@@ -757,7 +757,10 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
     const G ftc = trap * Cb;
     G d[9] = {-f11 + f51, (f11 - f3) + f52, -f1 - f51, (f1 - f31) - f52, (f31 - f53) - fbo, (f3 + f53) - fbi,
               (fbi + ftc) - q.Kt * IOb, (fbo + ftc) - q.Kt * Ob, -(ftc - q.Kt * Ob) - (ftc - q.Kt * IOb)};
-    if ((G)dt * lam > (G)1.8) {
+    if constexpr (P::kRates) {  // the chain's right-hand side
+      y.IC1 = (double)d[0]; y.IC2 = (double)d[1]; y.C1 = (double)d[2]; y.C2 = (double)d[3]; y.O = (double)d[4];
+      y.IO = (double)d[5]; y.IObound = (double)d[6]; y.Obound = (double)d[7]; y.Cbound = (double)d[8];
+    } else if ((G)dt * lam > (G)1.8) {
       const G hh = (G)dt;
 #pragma unroll
       for (int s = 0; s < 9; ++s) d[s] *= hh;
@@ -826,16 +829,16 @@ __device__ __forceinline__ void combine(Y<typename P::G> &y, const Par<typename 
                          Jdiff * (G)(k::vss / k::vmyo));
   const G dcansr = s.f[S_Jup] - Jtr * (G)(k::vjsr / k::vnsr);
   const G dcajsr = Bcajsr * (Jtr - s.f[S_Jrel]);
-  y.CaMKt = y.CaMKt + dCaMKt * dt;
-  y.V = y.V + (double)dV * dt;
-  y.nai = y.nai + (double)dnai * dt;
-  y.nass = y.nass + (double)dnass * dt;
-  y.ki = y.ki + (double)dki * dt;
-  y.kss = y.kss + (double)dkss * dt;
-  y.cai = y.cai + (double)dcai * dt;
-  y.cass = y.cass + (double)dcass * dt;
-  y.cansr = y.cansr + (double)dcansr * dt;
-  y.cajsr = y.cajsr + (double)dcajsr * dt;
+  fe<P>(y.CaMKt, dCaMKt, dt);
+  fe<P>(y.V, (double)dV, dt);
+  fe<P>(y.nai, (double)dnai, dt);
+  fe<P>(y.nass, (double)dnass, dt);
+  fe<P>(y.ki, (double)dki, dt);
+  fe<P>(y.kss, (double)dkss, dt);
+  fe<P>(y.cai, (double)dcai, dt);
+  fe<P>(y.cass, (double)dcass, dt);
+  fe<P>(y.cansr, (double)dcansr, dt);
+  fe<P>(y.cajsr, (double)dcajsr, dt);
 }
 
 // One cell step on one thread: rates at (t, y); if `update`, the

@@ -397,21 +397,21 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   y.nca_ss = rush_larsen<P, true>(y.nca_ss, P::dv(anca_ss * (G)k::k2n, km2n), P::rc(km2n), dt);
   y.nca_i = rush_larsen<P, true>(y.nca_i, P::dv(anca_i * (G)k::k2n, km2n), P::rc(km2n), dt);
   // forward Euler
-  y.V += (double)dV * dt;
-  y.CaMKt += (double)dCaMKt * dt;
-  y.cass += (double)dcass * dt;
-  y.nai += (double)dnai * dt;
-  y.nass += (double)dnass * dt;
-  y.ki += (double)dki * dt;
-  y.kss += (double)dkss * dt;
-  y.cansr += (double)dcansr * dt;
-  y.cajsr += (double)dcajsr * dt;
-  y.cai += (double)dcai * dt;
-  y.C1 += (double)dC1 * dt;
-  y.C2 += (double)dC2 * dt;
-  y.C3 += (double)dC3 * dt;
-  y.I += (double)dI * dt;
-  y.O += (double)dO * dt;
+  fe<P>(y.V, (double)dV, dt);
+  fe<P>(y.CaMKt, (double)dCaMKt, dt);
+  fe<P>(y.cass, (double)dcass, dt);
+  fe<P>(y.nai, (double)dnai, dt);
+  fe<P>(y.nass, (double)dnass, dt);
+  fe<P>(y.ki, (double)dki, dt);
+  fe<P>(y.kss, (double)dkss, dt);
+  fe<P>(y.cansr, (double)dcansr, dt);
+  fe<P>(y.cajsr, (double)dcajsr, dt);
+  fe<P>(y.cai, (double)dcai, dt);
+  fe<P>(y.C1, (double)dC1, dt);
+  fe<P>(y.C2, (double)dC2, dt);
+  fe<P>(y.C3, (double)dC3, dt);
+  fe<P>(y.I, (double)dI, dt);
+  fe<P>(y.O, (double)dO, dt);
 }
 
 __device__ __forceinline__ double hill_factor(double conc, double ic50, double h) {

@@ -151,6 +151,13 @@ enum {
   CEP_SCALE_GNCX, CEP_SCALE_PNAK, CEP_SCALE_COUNT
 };
 int cep_batch_scale(cep_batch_t b, int conductance, const double *factor);
+/* The same conductance of every instance read or written as values[n]
+ * (the instance's CONSTANTS entry after init, scaling and Hill block).
+ * cep::Cellmodel mirrors these at the reference's CONSTANTS indices, so a
+ * caller's CONSTANTS[GNa] *= gna_scale (heart.cpp:222) reaches the device
+ * unchanged. Blocking. */
+int cep_batch_get_conductance(cep_batch_t b, int conductance, double *values);
+int cep_batch_set_conductance(cep_batch_t b, int conductance, const double *values);
 
 /* Protocol of the run: fixed step dt (ms), n_pace paces at the instance's
  * BCL, biomarkers evaluated on paces >= first_pace (first_pace = n_pace-250
@@ -202,6 +209,15 @@ int cep_batch_sync(cep_batch_t b);
  * Ohara_Rudy_2011.cpp:742): dVdt[n] and the seven channel currents
  * currents[7*n] (INa, INaL, Ito, ICaL, IKr, IKs, IK1; SoA). */
 int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
+/* The whole RATES vector at the current state, as computeRates fills it for
+ * an ODE solver (the reference's CVODE right-hand side rhs_fn,
+ * CEPCell_NEO/modules/commons.cpp:26-35; ORd computeRates
+ * Ohara_Rudy_2011.cpp:742-989): rates[n * n_states] (AoS, the STATES order),
+ * a gate's (y_inf - y)/tau and every other state's forward-Euler
+ * derivative, in FP64. ORd 2011, CiPA-ORd and ToR-ORd; the ten Tusscher
+ * models (stepped with their own solveAnalytical) return
+ * CEP_ERR_UNSUPPORTED. Blocking. */
+int cep_batch_rates_all(cep_batch_t b, double t, double *rates);
 
 /* ------------------------------------------------- protocol variants */
 /* One pace of a dynamic (S1-S1) restitution run, as apdr_bench.cpp:211

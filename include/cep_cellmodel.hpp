@@ -60,6 +60,8 @@ class Population {
   void setProtocol(double dt, int n_pace, int first_pace, double dt_write = 1.0, double qnet_thr = -1e300) {
     check(cep_batch_set_protocol(h_, dt, n_pace, first_pace, dt_write, qnet_thr));
   }
+  /* CONSTANTS[g] *= factor[i] for every instance (CEP_SCALE_*). */
+  void scale(int conductance, const double *factor) { check(cep_batch_scale(h_, conductance, factor)); }
   void run(long n_steps) { check(cep_batch_run(h_, n_steps)); }
   void runToEnd(long steps_per_launch = 20000) { check(cep_batch_run_to_end(h_, steps_per_launch)); }
   void step(double t, double dt, int stim_mode = -1) { check(cep_batch_step(h_, t, dt, stim_mode)); }
@@ -106,32 +108,51 @@ class Population {
   int n_ = 0, ns_ = 0;
 };
 
-/* One cell with the reference's member layout, stepped on the device.
+/* One cell with the reference's member layout (cellmodel.hpp:4-36: the
+ * unsigned short sizes, inline 255-entry arrays and the gate / current /
+ * concentration index tables), stepped on the device.
  *
  *  - STATES mirrors the device state after every solveAnalytical; edits a
  *    caller makes to STATES (e.g. V from the diffusion solve) are uploaded
  *    before the next computeRates.
- *  - computeRates fills RATES[0] (dV/dt) and, for ORd 2011, the seven
- *    channel currents at the reference's ALGEBRAIC indices (INa 62, INaL 64,
- *    Ito 70, ICaL 81, IKr 96, IKs 98, IK1 100: enum_Ohara_Rudy_2011.hpp), so
- *    qNet code reading ALGEBRAIC[INaL] etc. keeps working; the other RATES
- *    and ALGEBRAIC entries are not produced.
- *  - For ORd 2011, CONSTANTS[BCL] (140), [stim_start] (139), [duration] (13)
- *    and [amp] (12) hold the pacing and a caller's writes to them reach the
- *    device before the next step (cipa_drug_bench.cpp:146-147 style); other
- *    models take setPacing().
+ *  - computeRates fills the whole RATES vector (dy/dt of every state, as the
+ *    reference's CVODE right-hand side uses it: CEPCell_NEO/modules/
+ *    commons.cpp:26-35) for ORd 2011, CiPA-ORd and ToR-ORd, and RATES[0]
+ *    for the ten Tusscher models. For ORd 2011 and CiPA-ORd the seven
+ *    channel currents are written at the reference's ALGEBRAIC indices
+ *    (ORd: INa 62, INaL 64, Ito 70, ICaL 81, IKr 96, IKs 98, IK1 100,
+ *    enum_Ohara_Rudy_2011.hpp; CiPA: 58, 60, 66, 83, 90, 96, 98,
+ *    enum_ohara_rudy_cipa_v1_2017.hpp), so qNet code reading
+ *    ALGEBRAIC[INaL] etc. keeps working; other ALGEBRAIC entries are not
+ *    produced.
+ *  - For ORd 2011 and CiPA-ORd, CONSTANTS holds the pacing (ORd: BCL 140,
+ *    stim_start 139, duration 13, amp 12; CiPA: 15, 12, 16, 14) and the
+ *    per-instance conductances (ORd: GNa 42, GNaL 96, Gto 97, PCa 99, GKr
+ *    101, GKs 102, GK1 103, GKb 105, Gncx 128, Pnak 138; CiPA: 45, 153,
+ *    154, 156, 159, 160, 161, 163, 194, 204) after initConsts. A caller's
+ *    write to any of them (cipa_drug_bench.cpp:146-148, heart.cpp:219-222:
+ *    CONSTANTS[BCL] = ..., CONSTANTS[amp] *= ..., CONSTANTS[GNa] *= ...)
+ *    reaches the device before the next step. Other CONSTANTS entries are
+ *    not read. Other models take setPacing() and Population::scale.
  *  - tissue = true reproduces the reference's TISSUE builds: the stimulus is
  *    isS1 (-DTISSUE), else the model's periodic single-cell stimulus. */
 class Cellmodel {
  public:
   static constexpr int kArr = 255;
+  bool isEctopic = false;
+  bool isS1 = false;
+  unsigned short algebraic_size = 0, constants_size = 0, states_size = 0;
+  unsigned short gates_size = 0, current_size = 0, concs_size = 0;
   double ALGEBRAIC[kArr];
   double CONSTANTS[kArr];
   double RATES[kArr];
   double STATES[kArr];
-  bool isS1 = false;
-  bool isEctopic = false;
-  unsigned int algebraic_size = 0, constants_size = 0, states_size = 0;
+  char gates_header[kArr];
+  unsigned short gates_indices[kArr];
+  char current_header[kArr];
+  unsigned short current_indices[kArr];
+  char concs_header[kArr];
+  unsigned short concs_indices[kArr];
 
   explicit Cellmodel(int model, int precision = CEP_PREC_FP64, bool tissue = false)
       : pop_(model, 1, precision), model_(model), tissue_(tissue) {
@@ -139,7 +160,37 @@ class Cellmodel {
     std::memset(CONSTANTS, 0, sizeof(CONSTANTS));
     std::memset(RATES, 0, sizeof(RATES));
     std::memset(STATES, 0, sizeof(STATES));
-    states_size = (unsigned)pop_.states_size();
+    std::memset(gates_header, 0, sizeof(gates_header));
+    std::memset(current_header, 0, sizeof(current_header));
+    std::memset(concs_header, 0, sizeof(concs_header));
+    std::memset(gates_indices, 0, sizeof(gates_indices));
+    std::memset(current_indices, 0, sizeof(current_indices));
+    std::memset(concs_indices, 0, sizeof(concs_indices));
+    states_size = (unsigned short)pop_.states_size();
+    if (model == CEP_MODEL_ORD2011) {  // the DrugSimulation ORd's tables (Ohara_Rudy_2011.cpp:438-453)
+      algebraic_size = 198;
+      constants_size = 144;
+      static const unsigned short g[] = {14, 13, 40, 17, 37, 6,  3,  36, 34, 30, 16, 5,  32, 4,  21,
+                                         38, 1,  35, 7,  23, 19, 10, 28, 27, 24, 11, 31, 20, 8,  22};
+      static const unsigned short c[] = {16, 67, 30, 187, 157, 168, 169, 73, 178, 150, 135,
+                                         42, 1,  9,  26,  49,  147, 143, 17, 184, 36};
+      static const unsigned short k[] = {18, 5, 2, 0, 25, 26, 29, 9};
+      gates_size = 30;
+      current_size = 21;
+      concs_size = 8;
+      std::memcpy(gates_indices, g, sizeof(g));
+      std::memcpy(current_indices, c, sizeof(c));
+      std::memcpy(concs_indices, k, sizeof(k));
+      std::strncpy(gates_header,
+                   "m,j,jp,hf,hs,hsp,mL,hL,hLp,a,ap,ki,iF,iS,iFp,iSp,xrf,xrs,xs1,xs2,xk1,d,ff,fs,fcaf,nca,jca,fca"
+                   "     s,ffp,fcafp,",
+                   kArr - 1);
+      std::strncpy(current_header,
+                   "INa,INaL,Ito,IKr,IKs,IK1,ICaL,ICaNa,ICaK,INaCa_ss,INaK,Jdiff,JdiffK,JdiffNa,Jup,Jrel,Jtr,"
+                   "     ,IpCa,ICab,INab,IKb",
+                   kArr - 1);
+      std::strncpy(concs_header, "nai,ki,cass,nass,cai,kss,CaMKT,cansr,cajsr", kArr - 1);
+    }
   }
   virtual ~Cellmodel() {}
 
@@ -148,71 +199,105 @@ class Cellmodel {
   virtual void initConsts(double type, bool is_dutta) { init(type, 0.0, nullptr, is_dutta); }
   virtual void initConsts(double type, double conc, double *hill) { init(type, conc, hill, false); }
   virtual void initConsts(double type, double conc, double *hill, bool is_dutta) { init(type, conc, hill, is_dutta); }
+  /* The bootstrap overload of the reference's base class, which no model
+   * of the reference overrides: it does nothing there and here. */
+  virtual void initConsts(double type, double conc, double *hill, double *boot) {
+    (void)type; (void)conc; (void)hill; (void)boot;
+  }
 
   virtual void computeRates(double TIME, double *C, double *R, double *S, double *A) {
-    (void)C;
+    if (C != CONSTANTS) std::memcpy(CONSTANTS, C, sizeof(CONSTANTS));
     sync_in(S);
-    sync_pacing();
+    sync_consts();
     double dvdt = 0, cur[7] = {0};
     check(cep_batch_rates(pop_.handle(), TIME, &dvdt, cur));
-    R[0] = dvdt;
-    if (model_ == CEP_MODEL_ORD2011) {
-      static const int idx[7] = {62, 64, 70, 81, 96, 98, 100};  // INa INaL Ito ICaL IKr IKs IK1
-      for (int k = 0; k < 7; ++k) A[idx[k]] = cur[k];
+    if (model_ == CEP_MODEL_ORD2011 || model_ == CEP_MODEL_CIPA2017 || model_ == CEP_MODEL_TOMEK2019) {
+      check(cep_batch_rates_all(pop_.handle(), TIME, R));
+    } else {
+      R[0] = dvdt;
     }
+    const int *idx = alg_index();
+    if (idx)
+      for (int k = 0; k < 7; ++k) A[idx[k]] = cur[k];
     t_ = TIME;
   }
 
   virtual void solveAnalytical(double dt) {
     sync_in(STATES);
-    sync_pacing();
+    sync_consts();
     pop_.step(t_, dt, tissue_ ? (isS1 ? 1 : 0) : -1);
     sync_out();
   }
+  /* The reference's base class declares an RK4 step that no model
+   * implements (DrugSimulation/modules/drug_sim.cpp:227 calls it); like
+   * there, it does nothing. */
+  virtual void solveRK4(double TIME, double dt) { (void)TIME; (void)dt; }
 
   /* Pacing for every model (BCL, stimulus start and duration in ms; the
    * amplitude as a factor on the model default). */
   void setPacing(double bcl, double stim_start = -1, double stim_dur = -1, double amp_scale = 1) {
     pop_.setPacing(bcl, stim_start, stim_dur, amp_scale);
-    if (model_ == CEP_MODEL_ORD2011) {
-      CONSTANTS[140] = bcl;
-      if (stim_start >= 0) CONSTANTS[139] = stim_start;
-      if (stim_dur >= 0) CONSTANTS[13] = stim_dur;
-      CONSTANTS[12] *= amp_scale;
-      remember_pacing();
+    const int *p = pacing_index();
+    if (p) {
+      CONSTANTS[p[0]] = bcl;
+      if (stim_start >= 0) CONSTANTS[p[1]] = stim_start;
+      if (stim_dur >= 0) CONSTANTS[p[2]] = stim_dur;
+      CONSTANTS[p[3]] *= amp_scale;
+      remember();
     }
   }
 
   Population &population() { return pop_; }
 
  private:
+  // CONSTANTS indices of BCL, stim_start, duration, amp
+  const int *pacing_index() const {
+    static const int ord[4] = {140, 139, 13, 12}, cipa[4] = {15, 12, 16, 14};
+    return model_ == CEP_MODEL_ORD2011 ? ord : model_ == CEP_MODEL_CIPA2017 ? cipa : nullptr;
+  }
+  // ALGEBRAIC indices of INa, INaL, Ito, ICaL, IKr, IKs, IK1
+  const int *alg_index() const {
+    static const int ord[7] = {62, 64, 70, 81, 96, 98, 100}, cipa[7] = {58, 60, 66, 83, 90, 96, 98};
+    return model_ == CEP_MODEL_ORD2011 ? ord : model_ == CEP_MODEL_CIPA2017 ? cipa : nullptr;
+  }
+  // CONSTANTS indices of the CEP_SCALE_* conductances (-1: not mirrored)
+  const int *conductance_index() const {
+    static const int ord[CEP_SCALE_COUNT] = {42, 96, 97, 99, 101, 102, 103, -1, -1, -1, -1, 105, 128, 138};
+    static const int cipa[CEP_SCALE_COUNT] = {45, 153, 154, 156, 159, 160, 161, -1, -1, -1, -1, 163, 194, 204};
+    return model_ == CEP_MODEL_ORD2011 ? ord : model_ == CEP_MODEL_CIPA2017 ? cipa : nullptr;
+  }
   void init(double type, double conc, double *hill, bool is_dutta) {
     double ct = type, cc = conc;
     pop_.initConsts(&ct, &cc, hill, hill ? (model_ == CEP_MODEL_CIPA2017 ? CEP_HILL_WIDTH : 14) : 0,
                     CEP_FLAG_QUIRKS | (is_dutta ? CEP_FLAG_DUTTA : 0u));
-    if (model_ == CEP_MODEL_ORD2011) {  // Ohara_Rudy_2011.cpp initConsts defaults
-      CONSTANTS[140] = 1000.0;
-      CONSTANTS[139] = 10.0;
-      CONSTANTS[13] = 0.5;
-      CONSTANTS[12] = -80.0;
-      remember_pacing();
+    if (const int *p = pacing_index()) {  // initConsts defaults (Ohara_Rudy_2011.cpp:494-678)
+      CONSTANTS[p[0]] = 1000.0;
+      CONSTANTS[p[1]] = 10.0;
+      CONSTANTS[p[2]] = 0.5;
+      CONSTANTS[p[3]] = -80.0;
     }
+    if (const int *g = conductance_index())
+      for (int k = 0; k < CEP_SCALE_COUNT; ++k)
+        if (g[k] >= 0) check(cep_batch_get_conductance(pop_.handle(), k, &CONSTANTS[g[k]]));
+    remember();
     sync_out();
   }
-  void remember_pacing() {
-    pacing_[0] = CONSTANTS[140];
-    pacing_[1] = CONSTANTS[139];
-    pacing_[2] = CONSTANTS[13];
-    pacing_[3] = CONSTANTS[12];
-  }
-  void sync_pacing() {
-    if (model_ != CEP_MODEL_ORD2011) return;
-    if (CONSTANTS[140] == pacing_[0] && CONSTANTS[139] == pacing_[1] && CONSTANTS[13] == pacing_[2] &&
-        CONSTANTS[12] == pacing_[3])
-      return;
-    const double scale = pacing_[3] != 0.0 ? CONSTANTS[12] / pacing_[3] : 1.0;
-    check(cep_batch_set_pacing(pop_.handle(), CONSTANTS[140], CONSTANTS[139], CONSTANTS[13], scale));
-    remember_pacing();
+  void remember() { std::memcpy(consts_seen_, CONSTANTS, sizeof(CONSTANTS)); }
+  // uploads what a caller changed in the mirrored CONSTANTS entries
+  void sync_consts() {
+    const int *p = pacing_index();
+    if (!p) return;
+    bool pacing = false;
+    for (int k = 0; k < 4; ++k) pacing |= CONSTANTS[p[k]] != consts_seen_[p[k]];
+    if (pacing) {
+      const double scale = consts_seen_[p[3]] != 0.0 ? CONSTANTS[p[3]] / consts_seen_[p[3]] : 1.0;
+      check(cep_batch_set_pacing(pop_.handle(), CONSTANTS[p[0]], CONSTANTS[p[1]], CONSTANTS[p[2]], scale));
+    }
+    const int *g = conductance_index();
+    for (int k = 0; k < CEP_SCALE_COUNT; ++k)
+      if (g[k] >= 0 && CONSTANTS[g[k]] != consts_seen_[g[k]])
+        check(cep_batch_set_conductance(pop_.handle(), k, &CONSTANTS[g[k]]));
+    remember();
   }
   void sync_in(const double *S) {
     if (S != STATES) std::memcpy(STATES, S, sizeof(double) * states_size);
@@ -230,7 +315,7 @@ class Cellmodel {
   int model_;
   bool tissue_;
   double t_ = 0.0;
-  double pacing_[4] = {0, 0, 0, 0};
+  double consts_seen_[kArr] = {0};
   double shadow_[kArr] = {0};
 };
 

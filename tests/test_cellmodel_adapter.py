@@ -55,3 +55,35 @@ def test_adapter_tt2006_tissue_flag_matches_reference_golden(cep, gpu, tmp_path)
     assert out.returncode == 0, out.stderr
     v = np.array([float(x) for x in out.stdout.split()])
     assert np.abs(v - g["v_trace"]).max() <= 1e-6
+
+
+@pytest.mark.gpu
+def test_adapter_full_rates_and_constants_writes(cep, gpu, oracle, tmp_path):
+    """computeRates fills every RATES entry of CiPA-ORd (the CVODE
+    right-hand side of the reference), and the bench's CONSTANTS writes
+    (BCL, GNa *= gna_scale) reach the device: the trace follows an oracle
+    cell with the same constants within 1e-6 mV, and the RATES at every
+    printed state equal the oracle's rates at that state (1e-9 relative to
+    the largest rate of the state, FP64 with a different division)."""
+    exe = _build(tmp_path)
+    n, stride = 60000, 3000
+    out = subprocess.run([str(exe), "cipa_rates", str(n), str(stride), "1000"], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr
+    rows = np.array([[float(x) for x in ln.split()] for ln in out.stdout.strip().splitlines()])
+    ns = 49
+    hill = np.array([1.5, 0.9, 20.0, 1.1, 0, 0, 3.0, 1.3, 5.0, 0.8, 12.0, 1.0, 0, 0, 5e3, 2e-3, 0.9, 1e4, -40.0,
+                     3.5e-5])
+    c = oracle.Cell("cipa2017", 0.0, 0.4, hill, quirks=True)
+    c.set_pacing(1000.0)
+    c.scale(cep.SCALE["gna"], 0.7)
+    t = 0.0
+    for r in rows:
+        steps = int(round((r[-1] - t) / 0.005))
+        c.run(t, 0.005, steps)
+        t = r[-1]
+        assert abs(r[0] - c.states[0]) <= 1e-6, (t, r[0], c.states[0])
+        c.y[:ns] = r[:ns]  # the oracle's rates at the adapter's own state
+        ro, _ = c.rates(t)
+        scale = np.abs(ro).max()
+        assert np.abs(r[ns:2 * ns] - ro).max() <= 1e-9 * scale, (t, np.abs(r[ns:2 * ns] - ro).max(), scale)
