@@ -53,6 +53,17 @@ class CepJob(ctypes.Structure):
                 ("first_pace", ctypes.c_int), ("flags", ctypes.c_uint)]
 
 
+class PopulationJob(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int), ("n", ctypes.c_int), ("celltype", ctypes.POINTER(ctypes.c_double)),
+                ("conc", ctypes.POINTER(ctypes.c_double)), ("hill", ctypes.POINTER(ctypes.c_double)),
+                ("hill_stride", ctypes.c_int), ("flags", ctypes.c_uint), ("bcl", ctypes.c_double),
+                ("amp_scale", ctypes.c_double), ("scale", ctypes.POINTER(ctypes.c_double)),
+                ("states_init", ctypes.POINTER(ctypes.c_double)), ("dt", ctypes.c_double),
+                ("dt_write", ctypes.c_double), ("n_pace", ctypes.c_int), ("first_pace", ctypes.c_int),
+                ("precision", ctypes.c_int), ("refine_above_vm", ctypes.c_double), ("screen_paces", ctypes.c_int),
+                ("steps_per_launch", ctypes.c_long)]
+
+
 class TissueJob(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("h", ctypes.c_double), ("D", ctypes.c_double),
                 ("dt", ctypes.c_double), ("duration", ctypes.c_double), ("conc", ctypes.c_double),
@@ -109,6 +120,7 @@ _SIGS = {
     "cep_batch_get_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_set_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    "cep_population_run": (ctypes.c_int, [ctypes.POINTER(PopulationJob), ctypes.c_void_p, _ip]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "cep_batch_set_states": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int]),
@@ -476,53 +488,49 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
                    precision: str = "mixed", celltype=None, dutta: bool = False, quirks: bool = True,
                    dt_write: float = 1.0, refine_above_vm: float | None = -80.0,
                    steps_per_launch: int = 50000, amp_scale: float = 1.0,
-                   states_init=None, scales=None) -> dict[str, np.ndarray]:
+                   states_init=None, scales=None, screen_paces: int = 1) -> dict[str, np.ndarray]:
     """A population run to the end of its protocol (the reference's bench loop
-    for every instance), returning the biomarker records.
+    for every instance, cep_population_run), returning the biomarker records.
 
-    With precision "mixed" and refine_above_vm set, the instances whose mixed
-    diastolic Vm stays above refine_above_vm (drug-depolarised cells that do
-    not repolarise: their 90 % level is crossed at ~0.1 mV/ms, so their APD90
-    moves by tenths of a ms under perturbations of 1e-5 and FP32 gates cannot
-    hold it to 0.1 ms) are run again in FP64 from their initial state and
-    their records replaced; out["refined"] marks them. amp_scale multiplies
-    the stimulus amplitude (CONSTANTS[amp] *= Stim_Amplitude,
-    cipa_drug_bench.cpp:147); states_init, one state vector, replaces every
-    instance's initial states after initConsts (Is_Using_Output, :149);
-    scales maps SCALE keys to a factor (scalar or one per instance) applied
-    after initConsts (CONSTANTS[GNa] *= gna_scale, :148)."""
+    With precision "mixed" and refine_above_vm set, the instances whose
+    diastolic Vm after screen_paces mixed paces is above refine_above_vm
+    (drug-depolarised cells that do not repolarise: their 90 % level is
+    crossed at ~0.1 mV/ms, so their APD90 moves by tenths of a ms under
+    perturbations of 1e-5 and FP32 gates cannot hold it to 0.1 ms) run in
+    FP64 from their initial state concurrently with the mixed population,
+    and any instance whose record still shows such a diastolic Vm runs again
+    in FP64 afterwards; out["refined"] marks both (out["refined_how"]: 1
+    concurrent, 2 afterwards). amp_scale multiplies the stimulus amplitude
+    (CONSTANTS[amp] *= Stim_Amplitude, cipa_drug_bench.cpp:147);
+    states_init, one state vector, replaces every instance's initial states
+    after initConsts (Is_Using_Output, :149); scales maps SCALE keys to a
+    factor (scalar or one per instance) applied after initConsts
+    (CONSTANTS[GNa] *= gna_scale, :148)."""
     conc = np.ascontiguousarray(conc, np.float64)
     n = len(conc)
     hill = np.asarray(hill, np.float64)
+    h = np.ascontiguousarray(np.broadcast_to(hill, (n, hill.shape[-1])) if hill.ndim == 1 else hill)
     ct = None if celltype is None else np.ascontiguousarray(np.broadcast_to(celltype, (n,)), np.float64)
-
-    def run(prec, idx):
-        b = Batch(model, len(idx), prec)
-        try:
-            b.init(celltype=None if ct is None else ct[idx], conc=conc[idx],
-                   hill=hill[idx] if hill.ndim == 2 else hill, dutta=dutta, quirks=quirks)
-            b.set_pacing(bcl, amp_scale=amp_scale)
-            for g, f in (scales or {}).items():
-                f = np.asarray(f, np.float64)
-                b.scale(g, f[idx] if f.ndim else f)
-            if states_init is not None:
-                y0 = np.asarray(states_init, np.float64).reshape(-1)
-                b.set_states(np.ascontiguousarray(np.broadcast_to(y0, (len(idx), len(y0)))))
-            b.set_protocol(dt, n_pace, first_pace, dt_write=dt_write)
-            b.run_to_end(steps_per_launch)
-            return b.biomarkers()
-        finally:
-            b.close()
-
-    out = run(precision, np.arange(n))
-    out["refined"] = np.zeros(n, bool)
-    if precision == "mixed" and refine_above_vm is not None:
-        idx = np.flatnonzero(~(out["vm_valley"] < refine_above_vm))
-        if len(idx):
-            ref = run("fp64", idx)
-            for k, v in ref.items():
-                out[k][idx] = v
-            out["refined"][idx] = True
+    sc = None
+    if scales:
+        sc = np.ones((n, len(SCALE)))
+        for g, f in scales.items():
+            sc[:, SCALE[g]] = np.broadcast_to(np.asarray(f, np.float64), (n,))
+    y0 = None if states_init is None else np.ascontiguousarray(np.asarray(states_init, np.float64).reshape(-1))
+    flags = (FLAG_DUTTA if dutta else 0) | (FLAG_QUIRKS if quirks else 0)
+    job = PopulationJob(MODELS[model], n, _dptr(ct), _dptr(conc), _dptr(h), h.shape[1], flags, bcl, amp_scale,
+                        _dptr(sc), _dptr(y0), dt, dt_write, n_pace, first_pace, PREC[precision],
+                        float("nan") if refine_above_vm is None else refine_above_vm, max(1, screen_paces),
+                        steps_per_launch)
+    arr = (Biomarkers * n)()
+    how = np.zeros(n, np.int32)
+    _check(lib().cep_population_run(ctypes.byref(job), arr, how.ctypes.data_as(_ip)))
+    raw = np.ctypeslib.as_array(arr)
+    out = {f: np.array(raw[f]) for f in BM_FIELDS}
+    for f in ("steepest_pace", "n_eligible", "status"):
+        out[f] = np.array(raw[f])
+    out["refined"] = how > 0
+    out["refined_how"] = how
     return out
 
 

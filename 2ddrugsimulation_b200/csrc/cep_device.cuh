@@ -15,23 +15,57 @@ namespace cep {
 
 // Reciprocal in FP64 by Newton-Raphson refinement of the hardware's 20-bit
 // reciprocal seed (rcp.approx.ftz.f64): two steps r <- r + r(1 - x r) give
-// a result within about an ulp. +-inf maps to +-0 as IEEE division would.
-__device__ __forceinline__ double rcp64(double x) {
+// a result within about an ulp for 2^-1021 <= |x| <= 2^1021. Outside that
+// range the seed is flushed or infinite and the steps end in NaN (zero,
+// subnormal, infinite or NaN x), which the callers below send to an exact
+// special-case path.
+__device__ __forceinline__ double rcp64_nr(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
   double e = fma(-x, r, 1.0);
   r = fma(r, e, r);
   e = fma(-x, r, 1.0);
-  r = fma(r, e, r);
-  return isinf(x) ? copysign(0.0, x) : r;
+  return fma(r, e, r);
 }
-// a / b as a * (1/b) with one residual correction (q + r (a - b q)).
+// 1/x for x = +-0 (+-inf), +-inf (+-0), NaN, and subnormal x, scaled by
+// 2^64 into the normal range (the result overflows to inf as IEEE's does
+// when |x| < 2^-1024).
+__device__ __noinline__ double rcp64_special(double x) {
+  if (isnan(x)) return x;
+  if (x == 0.0) return copysign(INFINITY, x);
+  if (isinf(x)) return copysign(0.0, x);
+  return rcp64_nr(x * 0x1p64) * 0x1p64;
+}
+__device__ __forceinline__ double rcp64(double x) {
+  const double r = rcp64_nr(x);
+  return isnan(r) ? rcp64_special(x) : r;
+}
+// a / b for the operands the fast path turns into NaN: NaN operands, zero,
+// subnormal or infinite divisors, infinite dividends and quotients that
+// overflow. Finite cases divide the frexp mantissas and scale the result
+// back with ldexp (one extra rounding for subnormal quotients).
+__device__ __noinline__ double div64_special(double a, double b) {
+  if (isnan(a) || isnan(b)) return a + b;
+  const bool neg = signbit(a) != signbit(b);
+  if (isinf(b)) return isinf(a) ? NAN : (neg ? -0.0 : 0.0);
+  if (b == 0.0) return a == 0.0 ? NAN : (neg ? -INFINITY : INFINITY);
+  if (isinf(a)) return neg ? -INFINITY : INFINITY;
+  if (a == 0.0) return neg ? -0.0 : 0.0;
+  int ea, eb;
+  const double ma = frexp(a, &ea), mb = frexp(b, &eb);
+  const double r = rcp64_nr(mb);
+  const double q = ma * r;
+  return ldexp(fma(r, fma(-mb, q, ma), q), ea - eb);
+}
+// a / b as a * (1/b) with one residual correction (q + r (a - b q)), within
+// an ulp of the correctly rounded quotient for divisors of magnitude up to
+// 2^1021 (every division of the models here); IEEE results for zero,
+// subnormal, infinite and NaN operands.
 __device__ __forceinline__ double div64(double a, double b) {
-  const double r = rcp64(b);
+  const double r = rcp64_nr(b);
   const double q = a * r;
-  const double res = fma(-b, q, a);
-  const double out = fma(r, res, q);
-  return isinf(b) ? a * r : out;
+  const double out = fma(r, fma(-b, q, a), q);
+  return isnan(out) ? div64_special(a, b) : out;
 }
 
 struct F64 {

@@ -221,6 +221,6 @@ def run(d: Deck, hill=None, precision: str = "mixed", states_init=None, quirks: 
                              first_pace=first_pace, precision=precision,
                              celltype=d.celltype, dutta=models[mode] == "ord2011", quirks=quirks,
                              dt_write=d.dt_write, amp_scale=d.stim_amp, states_init=states_init,
-                             scales={"gna": d.gna_scale})
+                             scales={"gna": d.gna_scale} if d.gna_scale != 1.0 else None)
     out["conc"], out["hill"] = conc, rows
     return out

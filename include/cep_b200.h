@@ -219,6 +219,45 @@ int cep_batch_rates(cep_batch_t b, double t, double *dvdt, double *currents);
  * CEP_ERR_UNSUPPORTED. Blocking. */
 int cep_batch_rates_all(cep_batch_t b, double t, double *rates);
 
+/* ------------------------------------------------------- whole jobs */
+/* One screening job: the CiPA bench loop over every sample and
+ * concentration (CEPCell_NEO/modules/cipa_drug_bench.cpp:128-380:
+ * initConsts(celltype, conc, hill, is_dutta), CONSTANTS[BCL] = bcl,
+ * CONSTANTS[amp] *= stim_amp, CONSTANTS[GNa] *= gna_scale (here any of the
+ * CEP_SCALE_* conductances per instance), optional initial states, n_pace
+ * paces, biomarkers from the steepest evaluated beat) as
+ * one population on the device. precision CEP_PREC_MIXED with a finite
+ * refine_above_vm keeps the mixed path's accuracy bar for every instance:
+ * after screen_paces mixed paces, the instances whose membrane potential
+ * at the pace boundary is above refine_above_vm (drug-depolarised cells
+ * that do not repolarise, whose APD90 FP32 gates cannot hold) run from
+ * their initial state in FP64 on a second stream concurrently with the
+ * mixed population, and any instance whose evaluated record still shows a
+ * diastolic Vm above it runs again in FP64 afterwards. refine_above_vm =
+ * NaN (or CEP_PREC_FP64) runs the single precision alone. No counterpart
+ * in the reference beyond the loop it replaces. Blocking. */
+typedef struct {
+  int model, n;
+  const double *celltype; /* [n] or NULL (endo) */
+  const double *conc;     /* [n] or NULL */
+  const double *hill;     /* [n * hill_stride] or NULL */
+  int hill_stride;
+  unsigned flags;         /* CEP_FLAG_* */
+  double bcl, amp_scale;
+  const double *scale;       /* [n * CEP_SCALE_COUNT] factors (cep_batch_scale) or NULL */
+  const double *states_init; /* one state vector for every instance, or NULL */
+  double dt, dt_write;
+  int n_pace, first_pace;
+  int precision;
+  double refine_above_vm; /* mV; NaN: no refinement */
+  int screen_paces;       /* >= 1 */
+  long steps_per_launch;  /* <= 0: 20000 */
+} cep_population_job_t;
+/* out[n] receives the records; refined[n] (may be NULL) 0 for a mixed
+ * record, 1 for an FP64 record of a screened instance, 2 for one re-run
+ * after the mixed run. */
+int cep_population_run(const cep_population_job_t *job, cep_biomarkers_t *out, int *refined);
+
 /* ------------------------------------------------- protocol variants */
 /* One pace of a dynamic (S1-S1) restitution run, as apdr_bench.cpp:211
  * writes it ("all_pace bcl apd90 t_di tcurr"); recal = 1 when the pace's
