@@ -120,6 +120,7 @@ _SIGS = {
     "cep_batch_get_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_set_conductance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    "cep_fem_set_wait_test": (ctypes.c_int, [ctypes.c_long, ctypes.c_uint]),
     "cep_population_run": (ctypes.c_int, [ctypes.POINTER(PopulationJob), ctypes.c_void_p, _ip]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),

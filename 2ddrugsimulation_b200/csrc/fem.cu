@@ -331,6 +331,20 @@ __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volati
 // at its next arrival or poll and leaves.
 constexpr unsigned kPoison = 0x80000000u;
 
+// Test hooks of the bounded waits (cep_fem_set_wait_test): a smaller spin
+// limit for every grid barrier on this device (0 = kSpinLimit) and a
+// bounded sleep of block 0 before its first barrier, so that a test can make
+// the other blocks' waits run out without any fault.
+__device__ long long g_spin_limit_test = 0;
+__device__ unsigned g_block0_delay_ns = 0;
+
+__device__ __forceinline__ void test_delay_block0() {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned d = g_block0_delay_ns;
+    for (unsigned t = 0; t < d; t += 1024u) __nanosleep(1024u);
+  }
+}
+
 __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
   unsigned old;
   asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
@@ -348,7 +362,8 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned &epoch) {
     if (old & kPoison) {
       ok = 0;
     } else if (old + 1u < target) {
-      long spins = 0;
+      const long long lim = g_spin_limit_test > 0 ? g_spin_limit_test : (long long)kSpinLimit;
+      long long spins = 0;
       for (;;) {
         const unsigned c = ld_acquire(&ctl->count);
         if (c & kPoison) {
@@ -356,7 +371,7 @@ __device__ __forceinline__ bool grid_sync(Ctl *ctl, unsigned &epoch) {
           break;
         }
         if (c >= target) break;
-        if (++spins > kSpinLimit) {
+        if (++spins > lim) {
           atomicOr(&ctl->count, kPoison);
           atomicExch(&ctl->err, 1);
           ok = 0;
@@ -631,6 +646,7 @@ __device__ __forceinline__ void pcg_body(const M &m, const PcgArgs &a, int NB, i
 template <class M>
 __global__ void __launch_bounds__(kPcgBlock) pcg_kernel(const __grid_constant__ M m,
                                                         const __grid_constant__ PcgArgs a) {
+  test_delay_block0();
   pcg_body(m, a, (int)gridDim.x, (int)blockIdx.x, a.ctl, nullptr, 1, a.t_new);
 }
 
@@ -638,6 +654,7 @@ __global__ void __launch_bounds__(kPcgBlock) pcg_kernel(const __grid_constant__ 
 template <class M>
 __global__ void __launch_bounds__(kPcgBlock) pcg_many_kernel(const __grid_constant__ PcgOps<M> ops, int n_ops,
                                                              Ctl *ctl, int *ops_done) {
+  test_delay_block0();
   int o = 0;
   while (o + 1 < n_ops && (int)blockIdx.x >= ops.op[o + 1].block0) ++o;
   const PcgOp<M> &op = ops.op[o];
@@ -1916,6 +1933,16 @@ int cep_tissue_stats(cep_tissue_t t, double *time, long *steps, long *cg_iters, 
 }
 
 }  // extern "C"
+
+// Test hook of the bounded barrier waits (no counterpart in the reference).
+extern "C" int cep_fem_set_wait_test(long spin_limit, unsigned block0_delay_ns) {
+  if (spin_limit < 0) return fail_msg(CEP_ERR_ARG, "spin_limit must be >= 0");
+  if (block0_delay_ns > 100000000u) return fail_msg(CEP_ERR_ARG, "block0_delay_ns above 0.1 s");
+  const long long lim = spin_limit;
+  FEM_CUDA(cudaMemcpyToSymbol(cep::fem::g_spin_limit_test, &lim, sizeof(lim)));
+  FEM_CUDA(cudaMemcpyToSymbol(cep::fem::g_block0_delay_ns, &block0_delay_ns, sizeof(block0_delay_ns)));
+  return CEP_OK;
+}
 
 // ------------------------------------------------------ allocation-free solve
 // Jacobi-PCG on a caller-owned device CSR operator with the solver's work

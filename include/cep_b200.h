@@ -476,6 +476,15 @@ int cep_fem_solve_device(cep_fem_t f, void *d_v);
 int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves, int *not_converged,
                   double *last_res);
 
+/* Test hook of the bounded device waits (no counterpart in the reference):
+ * every grid barrier of the PCG kernels on the current device gives up
+ * after spin_limit polls (0 restores the default of ~1-2 s) and block 0
+ * sleeps block0_delay_ns (at most 0.1 s) before its first barrier. With a
+ * short limit and a delay, the other blocks' waits run out: the solve ends
+ * early, every block leaves, and the blocking calls report CEP_ERR_TIMEOUT;
+ * the context stays usable. Reset with (0, 0). */
+int cep_fem_set_wait_test(long spin_limit, unsigned block0_delay_ns);
+
 /* Allocation-free solve. No counterpart in the reference. One implicit
  * diffusion step A V = B V / dt, Jacobi-PCG from a zero guess with the
  * default stopping rule (preconditioned norm), for a CSR operator the

@@ -469,3 +469,30 @@ def test_s1s2_argument_checks(cep, gpu):
     with pytest.raises(cep.CepError):
         t.set_s2(cep.S2_RESET, 256, -45.0, np.ones(256, np.uint8))
     t.set_s2(cep.S2_NONE, 0, 0.0)
+
+
+@pytest.mark.gpu
+def test_pcg_barrier_wait_runs_out_and_recovers(cep, gpu):
+    """The one device-side failure form that is safe to provoke: with the
+    grid barrier's spin limit cut to 64 polls and block 0 held back for
+    5 ms before its first barrier, the other blocks' waits run out; every
+    block leaves, the solve reports CEP_ERR_TIMEOUT, and once the hook is
+    reset the next solve of the same operator is bit-identical to one that
+    never timed out (the context stays usable)."""
+    nx = 400  # 160,000 rows: every SM holds a block of the cooperative grid
+    rng = np.random.default_rng(12)
+    v = rng.uniform(-90, 30, nx * nx)
+    ref = cep.Fem.grid(2, nx, nx, 1, 0.025, 0.01, 0.0013).set_solver(1e-9)
+    xr, itr, _ = ref.solve(v)
+    f = cep.Fem.grid(2, nx, nx, 1, 0.025, 0.01, 0.0013).set_solver(1e-9)
+    lib = cep.lib()
+    try:
+        assert lib.cep_fem_set_wait_test(64, 5_000_000) == cep.OK
+        with pytest.raises(cep.CepError) as e:
+            f.solve(v)
+        assert e.value.code == cep.ERR_TIMEOUT
+    finally:
+        assert lib.cep_fem_set_wait_test(0, 0) == cep.OK
+    x, it, _ = f.solve(v)
+    assert it == itr and np.array_equal(x, xr)
+    assert lib.cep_fem_set_wait_test(-1, 0) == cep.ERR_ARG

@@ -106,3 +106,32 @@ def test_noalloc_on_a_second_stream_and_missing_diagonal(cep, gpu, oracle):
                                        dv.data_ptr(), None, ctypes.byref(it))
     assert rc == cep.ERR_ARG
     assert "row 5" in lib.cep_last_error().decode()
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_a_barrier_timeout(cep, gpu, oracle):
+    """The blocking form reports a grid-barrier wait that ran out (forced by
+    the wait test hook) as CEP_ERR_TIMEOUT, and the next call, with the hook
+    reset, solves normally."""
+    import torch
+    lib = cep.lib()
+    dt, rtol, max_iter = 0.01, 1e-9, 500
+    rp, ci, a, b = oracle.fem_assemble(2, 400, 400, 1, 0.025, dt, 0.0013)
+    n = len(rp) - 1
+    ref = cep.Fem.csr(rp, ci, a, b, dt, fmt=cep.FEM_CSR).set_solver(rtol, max_iter)
+    d = [torch.from_numpy(x).cuda() for x in (rp, ci, a, b)]
+    ptrs = [x.data_ptr() for x in d]
+    v = np.random.default_rng(9).uniform(-90, 30, n)
+    it = ctypes.c_int()
+    try:
+        assert lib.cep_fem_set_wait_test(64, 5_000_000) == cep.OK
+        dv = torch.from_numpy(v.copy()).cuda()
+        rc = lib.cep_fem_solve_csr_noalloc(n, *ptrs, dt, rtol, max_iter, dv.data_ptr(), None, ctypes.byref(it))
+        assert rc == cep.ERR_TIMEOUT
+    finally:
+        assert lib.cep_fem_set_wait_test(0, 0) == cep.OK
+    xr, itr, _ = ref.solve(v)
+    dv = torch.from_numpy(v.copy()).cuda()
+    rc = lib.cep_fem_solve_csr_noalloc(n, *ptrs, dt, rtol, max_iter, dv.data_ptr(), None, ctypes.byref(it))
+    assert rc == cep.OK and it.value == itr
+    assert np.array_equal(dv.cpu().numpy(), xr)
