@@ -1411,12 +1411,34 @@ int cep_batch_set_conductance(cep_batch_t b, int conductance, const double *valu
   return CEP_OK;
 }
 
+// Largest dt (ms) at which the mixed path's slow gates may take the 4-term
+// series of 1 - e^{-a}, a = dt/tau (cep_device.cuh rush_larsen): the series
+// error a^5/120 stays below FP32 rounding while a <= 0.1. The slow gates'
+// smallest time constants: ORd / CiPA-ORd 0.5 ms, ToR-ORd about 0.1 ms (j
+// and jp near +50 mV), ten Tusscher 2 ms (fCass, fCa).
+static double mixed_dt_max(int model) {
+  switch (model) {
+    case CEP_MODEL_ORD2011:
+    case CEP_MODEL_CIPA2017: return 0.05;
+    case CEP_MODEL_TOMEK2019: return 0.01;
+    default: return 0.2;
+  }
+}
+static int check_mixed_dt(cep_batch_t b, double dt) {
+  if (b->precision == CEP_PREC_MIXED && dt > mixed_dt_max(b->model))
+    return fail(CEP_ERR_UNSUPPORTED,
+                "mixed precision of model %d is validated for dt <= %g ms (dt = %g): use FP64 or a smaller dt",
+                b->model, mixed_dt_max(b->model), dt);
+  return CEP_OK;
+}
+
 int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace, double dt_write,
                            double qnet_vm_threshold) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
   if (!(dt > 0) || !(dt_write > 0) || n_pace <= 0 || first_pace >= n_pace)
     return fail(CEP_ERR_ARG, "bad protocol (dt=%g n_pace=%d first_pace=%d dt_write=%g)", dt, n_pace, first_pace, dt_write);
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   const ModelInfo *mi = model_info(b->model);
   b->dt = dt; b->n_pace = n_pace; b->first_pace = first_pace; b->dt_write = dt_write;
   b->qnet_thr = qnet_vm_threshold;
@@ -1569,6 +1591,7 @@ int cep_batch_reserve_biomarkers(cep_batch_t b, int max_samples_per_beat, double
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
   if (max_samples_per_beat < 1 || !(dt > 0) || !(dt_write > 0)) return fail(CEP_ERR_ARG, "bad reservation");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   int rc;
   if (!b->bmf && ((rc = dev_alloc(b, &b->bmf, (size_t)bm::kNumF * b->ld)) ||
                   (rc = dev_alloc(b, &b->bmi, (size_t)bm::kNumI * b->ld))))
@@ -1763,6 +1786,7 @@ int cep_batch_restitution(cep_batch_t b, const double *bcl, int n_bcl, int n_pac
   if (!bcl || n_bcl <= 0) return fail(CEP_ERR_ARG, "bcl list is empty");
   if (n_pace <= 0) return fail(CEP_ERR_ARG, "n_pace must be positive (got %d)", n_pace);
   if (!(dt > 0) || !std::isfinite(dt)) return fail(CEP_ERR_ARG, "dt must be positive");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   if (max_records < 0 || (max_records > 0 && !out)) return fail(CEP_ERR_ARG, "bad record buffer");
   if (steps_per_launch <= 0) steps_per_launch = 20000;
   if (steps_per_launch > (1L << 30)) steps_per_launch = 1L << 30;
@@ -1822,6 +1846,7 @@ int cep_batch_clamp(cep_batch_t b, const double *v, long n_samples, double t0, d
   if (!v || !out || n_samples <= 0) return fail(CEP_ERR_ARG, "empty clamp trace");
   if (current < 0 || current > 6) return fail(CEP_ERR_ARG, "current index %d not in 0..6", current);
   if (!(dt > 0) || !std::isfinite(dt) || !std::isfinite(t0)) return fail(CEP_ERR_ARG, "bad t0/dt");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   const int chunk = 2048;
   Scratch sc;
   ClampArgs a;
@@ -1862,6 +1887,7 @@ int cep_internal_batch_tissue_step(cep_batch_t b, const unsigned char *d_mask, d
 int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {
   if (!b || !b->initialized) return fail(CEP_ERR_STATE, "tissue batch not initialised");
   if (!(dt > 0)) return fail(CEP_ERR_ARG, "dt must be positive");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   b->dt = dt; b->n_pace = 1; b->first_pace = -1; b->dt_write = 1.0; b->qnet_thr = -1e300;
   std::vector<int> sc((size_t)4 * b->ld, 0);
   for (int i = 0; i < b->n; ++i) {
@@ -1887,6 +1913,7 @@ int cep_batch_step(cep_batch_t b, double t, double dt, int stim_mode) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
   if (!(dt > 0) || !std::isfinite(t)) return fail(CEP_ERR_ARG, "bad t or dt");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
   if (stim_mode < -1 || stim_mode > 1) return fail(CEP_ERR_ARG, "stim_mode must be -1, 0 or 1");
   TissueArgs a;
   a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.t = t; a.dt = dt; a.mask = nullptr;

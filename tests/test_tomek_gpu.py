@@ -90,3 +90,42 @@ def test_tomek_biomarkers_fp64_and_mixed(cep, gpu, oracle):
         assert abs(bmx["cad90"][k] - r["cad90"]) <= CAD_TOL_MIXED, (k, bmx["cad90"][k], r["cad90"])
         q = r["qnet"] / 1000
         assert abs(bmx["qnet"][k] - q) <= QNET_RTOL_MIXED * abs(q) + 1e-6, (k, bmx["qnet"][k], q)
+
+
+@pytest.mark.gpu
+def test_tomek_mixed_at_its_largest_dt(cep, gpu, oracle):
+    """The mixed path at dt = 0.01 ms, the largest its slow-gate series form
+    accepts (j and jp reach tau ~0.1 ms near +50 mV), against the FP64
+    oracle at the same dt; a larger dt is refused in mixed precision and
+    accepted in FP64."""
+    ct, conc, hill = _cases(23, 4)
+    n = len(conc)
+    n_pace, first, dt, bcl = 3, 1, 0.01, 1000.0
+    ref = [None] * n
+
+    def work(k):
+        c = oracle.Cell("tomek2019", ct[k], conc[k], hill[k], quirks=True)
+        c.set_pacing(bcl)
+        ref[k], _ = c.run_biomarkers(dt, n_pace, first, dt_write=1.0)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(n)]
+    [x.start() for x in th]
+    [x.join() for x in th]
+    b = cep.Batch("tomek2019", n, "mixed")
+    b.init(celltype=ct, conc=conc, hill=hill)
+    b.set_pacing(bcl)
+    with pytest.raises(cep.CepError) as e:
+        b.set_protocol(0.02, n_pace, first, dt_write=1.0)
+    assert e.value.code == cep.ERR_UNSUPPORTED
+    b.set_protocol(dt, n_pace, first, dt_write=1.0)
+    b.run_to_end(30000)
+    bmx = b.biomarkers()
+    for k, r in enumerate(ref):
+        assert bmx["status"][k] == cep.INST_DONE
+        assert abs(bmx["apd90"][k] - r["apd90"]) <= APD_TOL_MIXED, (k, bmx["apd90"][k], r["apd90"])
+        assert abs(bmx["cad90"][k] - r["cad90"]) <= CAD_TOL_MIXED, (k, bmx["cad90"][k], r["cad90"])
+        q = r["qnet"] / 1000
+        assert abs(bmx["qnet"][k] - q) <= QNET_RTOL_MIXED * abs(q) + 1e-6, (k, bmx["qnet"][k], q)
+    f = cep.Batch("tomek2019", n, "fp64")
+    f.init(celltype=ct, conc=conc, hill=hill)
+    f.set_protocol(0.02, n_pace, first, dt_write=1.0)
