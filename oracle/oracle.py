@@ -28,6 +28,7 @@ REF_LIBS = {
     "tt2004": "libref_tt2004b.so",
     "tomek2019": "libref_tomek2019.so",
     "fem": "libref_fem.so",
+    "bench": "libref_bench.so",
 }
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -317,6 +318,37 @@ class RefCell:
 
 def ref_available(key: str) -> bool:
     return (REF_DIR / REF_LIBS[key]).exists()
+
+
+def ref_cipa_bench(workdir: str, hill_rows, concs, celltype: float, bcl: float, dt: float, dt_write: float,
+                   num_pace: int, drug: str = "pin") -> dict:
+    """The reference's CiPA drug bench (cipa_drug_bench.cpp, compiled from
+    its sources over the oracle's ORd; ref_shim/bench_shim.cpp) for every
+    Hill row and concentration. Returns {conc_text: {"ap": [...], "ca":
+    [...], "qni": [...]}}, each a list of rows of the printed text fields."""
+    import tempfile
+    import zipfile
+    L = ctypes.CDLL(str(REF_DIR / REF_LIBS["bench"]))
+    L.ref_cipa_bench.argtypes = [ctypes.c_char_p] * 4 + [ctypes.c_double] * 4 + [ctypes.c_int]
+    wd = Path(workdir)
+    (wd / "result").mkdir(parents=True, exist_ok=True)
+    hill_path = wd / "hill.csv"
+    rows = np.atleast_2d(np.asarray(hill_rows, np.float64))
+    hill_path.write_text("header\n" + "".join(",".join(repr(float(x)) for x in r) + "\n" for r in rows))
+    conc_text = "0," + ",".join(repr(float(c)) for c in concs)
+    if L.ref_cipa_bench(str(wd).encode(), str(hill_path).encode(), conc_text.encode(), drug.encode(), celltype, bcl,
+                        dt, dt_write, num_pace) != 0:
+        raise RuntimeError("reference bench failed")
+    z = zipfile.ZipFile(sorted((wd / "result").glob("*.zip"))[-1])
+    out: dict = {}
+    for name in z.namelist():
+        parts = name.split("/")
+        kind = "ap" if "ap_profile" in name else "ca" if "ca_profile" in name else "qni" if "qni" in name else None
+        if kind is None:
+            continue
+        lines = z.read(name).decode().strip().splitlines()[1:]
+        out.setdefault(parts[1], {})[kind] = [ln.split() for ln in lines]
+    return out
 
 
 def ref_fem_element(kind: str, xy, de: float, dt: float) -> tuple[np.ndarray, np.ndarray]:

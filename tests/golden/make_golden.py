@@ -2,13 +2,15 @@
 models compiled from their own sources (oracle/_ref, built by
 `make -C oracle ref` where the reference tree is present).
 
-    python tests/golden/make_golden.py [ord cipa tt2006 tt2004 tomek fem]
+    python tests/golden/make_golden.py [ord cipa tt2006 tt2004 tomek fem bench]
 
 Each fixture holds the inputs (celltype, concentration, Hill row, flags),
 the reference's V trace sampled every `stride` steps of its explicit loop
 (computeRates(t); solveAnalytical(dt); t += dt), its final STATES, and its
 RATES at t = 0. fem_elements.npz holds the reference's FEM element
-matrices (fem.cpp set_amat_bmat) of square, hex and tet elements. The
+matrices (fem.cpp set_amat_bmat) of square, hex and tet elements;
+cipa_bench_records.json the records the reference's CiPA drug bench prints
+(cipa_drug_bench.cpp) for the oracle's ORd trajectory. The
 oracle and the GPU path are checked against these files on machines where
 the reference itself is not available.
 """
@@ -212,10 +214,29 @@ def make_fem(dt: float = 0.01, de: float = 0.0013):
     print("wrote fem_elements")
 
 
+BENCH_CASE = dict(celltype=0.0, bcl=500.0, dt=0.02, dt_write=1.0, num_pace=251, concs=[1.5, 0.3],
+                  hill=[[5.0, 1.0, 20.0, 1.1, 30.0, 0.9, 8.0, 1.2, 4.0, 0.8, 15.0, 1.0, 0.6, 1.1],
+                        [2.5, 0.9, 60.0, 1.0, 10.0, 1.3, 40.0, 0.7, 1.2, 1.1, 80.0, 0.6, 3.0, 0.8]])
+
+
+def make_bench():
+    """The reference's CiPA drug bench (cipa_drug_bench.cpp compiled from its
+    sources, run over the oracle's ORd with a fixed-step CVode stand-in) on
+    BENCH_CASE: its printed records (ap_profile, ca_profile, qni) as text."""
+    import json
+    import tempfile
+    c = BENCH_CASE
+    with tempfile.TemporaryDirectory() as wd:
+        rec = O.ref_cipa_bench(wd, c["hill"], c["concs"], c["celltype"], c["bcl"], c["dt"], c["dt_write"],
+                               c["num_pace"])
+    (OUT / "cipa_bench_records.json").write_text(json.dumps(dict(case=c, records=rec), indent=1))
+    print("wrote cipa_bench_records")
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
-    which = set(sys.argv[1:]) or {"ord", "cipa", "tt2006", "tt2004", "tomek", "fem"}
+    which = set(sys.argv[1:]) or {"ord", "cipa", "tt2006", "tt2004", "tomek", "fem", "bench"}
     if "ord" in which:
         make_ord()
     if "cipa" in which:
@@ -228,3 +249,5 @@ if __name__ == "__main__":
         make_tomek()
     if "fem" in which:
         make_fem()
+    if "bench" in which:
+        make_bench()

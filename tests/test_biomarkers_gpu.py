@@ -123,3 +123,40 @@ def test_qinward_of_control_drug_pairs(cep, gpu, oracle, prec):
             qo = 0.5 * (ref[d]["inal_auc"] / ref[c]["inal_auc"] + ref[d]["ical_auc"] / ref[c]["ical_auc"])
             assert abs(qi - qo) <= (1e-9 if prec == "fp64" else 0.01) * abs(qo), (s, d, qi, qo)
             assert qi < 1.0  # the drug blocks INaL and ICaL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_device_records_match_the_reference_bench(cep, gpu, prec):
+    """The device's records against what the reference's own CiPA bench
+    prints (tests/golden/cipa_bench_records.json: cipa_drug_bench.cpp over
+    the oracle's ORd, 251 paces at BCL 500 ms, dt 0.02 ms, Dutta scaling,
+    two Hill rows at a control and two drug concentrations), within this
+    file's tolerances plus the printed rounding (5e-7)."""
+    import json
+    from pathlib import Path
+    g = json.loads((Path(__file__).resolve().parent / "golden" / "cipa_bench_records.json").read_text())
+    c, rec = g["case"], g["records"]
+    concs = [0.0] + list(c["concs"])
+    hill = np.repeat(np.array(c["hill"]), len(concs), axis=0)
+    conc = np.tile(concs, len(c["hill"]))
+    out = cep.run_population("ord2011", conc, hill, bcl=c["bcl"], dt=c["dt"], n_pace=c["num_pace"],
+                             first_pace=c["num_pace"] - 250, precision=prec, celltype=c["celltype"], dutta=True,
+                             quirks=False, dt_write=c["dt_write"], refine_above_vm=None)
+    fp = prec == "fp64"
+    t_tol, rel = (0.01, 1e-6) if fp else (0.1, 0.02)
+    for k in range(len(conc)):
+        i, key = k // len(concs), f"{conc[k]:.2f}"
+        ap = [float(x) for x in rec[key]["ap"][i]]
+        ca = [float(x) for x in rec[key]["ca"][i]]
+        qn = [float(x) for x in rec[key]["qni"][i]]
+        for got, want in ((out["apd90"][k], ap[5]), (out["apd50"][k], ap[6]), (out["cad90"][k], ca[3]),
+                          (out["cad50"][k], ca[4])):
+            assert abs(got - want) <= t_tol + 5e-7, (key, i, got, want)
+        for got, want in ((out["dvmdt_max"][k], ap[2]), (out["dvmdt_repol"][k], ap[1])):
+            assert abs(got - want) <= rel * abs(want) + 5e-7, (key, i, got, want)
+        for got, want in ((out["vm_peak"][k], ap[3]), (out["vm_dia"][k], ap[4])):
+            assert abs(got - want) <= (1e-6 if fp else 0.5) + 5e-7, (key, i, got, want)
+        assert abs(out["qnet"][k] - qn[1]) <= (1e-9 if fp else 0.01) * abs(qn[1]) + 5e-7, (key, i)
+        if fp:
+            assert out["steepest_pace"][k] == int(ap[8])

@@ -304,3 +304,52 @@ def test_fem_element_bitwise_vs_compiled_reference(oracle, kind):
         A, B = oracle.ref_fem_element(kind, x, de, dt)
         a, b = oracle.element(kind, x, de, dt)
         assert np.array_equal(a, A) and np.array_equal(b, B), (kind, trial)
+
+
+# ------------------------------------------------------- biomarker machine
+def _c_float(x: float) -> str:
+    """A double as C's printf("%lf") writes it."""
+    if x != x:
+        return "-nan" if np.signbit(x) else "nan"
+    return f"{x:.6f}"
+
+
+def test_biomarker_machine_matches_reference_bench(oracle):
+    """The oracle's restatement of the CiPA bench's biomarker state machine
+    prints exactly what the reference's own bench prints. The goldens come
+    from cipa_drug_bench.cpp compiled from its sources and run over the
+    oracle's ORd 2011 (oracle/ref_shim/bench_shim.cpp: the CVODE call
+    replaced by one fixed step of the oracle's scheme), 251 paces so that
+    its last-250-paces evaluation runs: every field of ap_profile,
+    ca_profile and qni (APD90/50/triangulation, dVm/dt max and repolarising,
+    Vm peak and diastolic, Ca peak / diastolic, CaD90/50/triangulation,
+    qNet, qInward) and the steepest pace, for two Hill rows at a control and
+    two drug concentrations."""
+    import json
+    import threading
+    g = json.loads((GOLD / "cipa_bench_records.json").read_text())
+    c, rec = g["case"], g["records"]
+    concs = [0.0] + list(c["concs"])
+    res = {}
+
+    def work(i, conc):
+        cell = oracle.Cell("ord2011", c["celltype"], conc, np.array(c["hill"][i]), is_dutta=True, quirks=False)
+        cell.set_pacing(c["bcl"])
+        res[(i, conc)], _ = cell.run_biomarkers(c["dt"], c["num_pace"], c["num_pace"] - 250, dt_write=c["dt_write"])
+
+    th = [threading.Thread(target=work, args=(i, conc)) for i in range(len(c["hill"])) for conc in concs]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    for i in range(len(c["hill"])):
+        ctrl = res[(i, 0.0)]
+        for conc in concs:
+            r = res[(i, conc)]
+            key = f"{conc:.2f}"
+            ap, ca, qni = rec[key]["ap"][i], rec[key]["ca"][i], rec[key]["qni"][i]
+            assert ap == [str(i), _c_float(r["dvmdt_repol"]), _c_float(r["dvmdt_max"]), _c_float(r["vm_peak"]),
+                          _c_float(r["vm_dia"]), _c_float(r["apd90"]), _c_float(r["apd50"]),
+                          _c_float(r["apd90"] - r["apd50"]), str(r["steepest_pace"])], (key, i, ap)
+            assert ca == [str(i), _c_float(r["ca_peak"]), _c_float(r["ca_dia"]), _c_float(r["cad90"]),
+                          _c_float(r["cad50"]), _c_float(r["cad90"] - r["cad50"]), str(r["steepest_pace"])], (key, i)
+            qin = 0.0 if conc == 0.0 else 0.5 * (r["inal_auc"] / ctrl["inal_auc"] + r["ical_auc"] / ctrl["ical_auc"])
+            assert qni == [str(i), _c_float(r["qnet"] / 1000.0), _c_float(qin)], (key, i, qni)
