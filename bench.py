@@ -94,6 +94,7 @@ def parse():
     ap.add_argument("--concs", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sub", action="store_true", help="skip the other configurations' sub-results")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     ap.add_argument("--kernel", default="auto", choices=["auto", "cell", "roles", "pairs"],
                     help="one thread per cell, 4 warps per 32 cells, or the library's default for the size")
@@ -547,6 +548,80 @@ def config_of(args, model, n, world):
             "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instance sharding x{world}"}
 
 
+# ------------------------------------------------------------ single-cell configuration
+def config1_run(args):
+    """ORd 2011 single cells as the single-cell configuration runs them: one
+    seeded drug (IC50 log-U[0.1,100] uM, h U[0.6,1.8], Cmax log-U[0.01,10]
+    uM) at 0..4 x Cmax, BCL 1000 ms, dt 0.005 ms, 100 paces, last-beat
+    biomarkers. Five instances are latency-bound: each precision is timed
+    over 2 paces after a warm-up pace (CUDA events) and the 100-pace time is
+    projected from it; the compiled reference on 5 host threads beside it."""
+    import torch
+    cep = importlib.import_module("2ddrugsimulation_b200")
+    rng = np.random.default_rng(7)
+    h = np.zeros(14)
+    h[0::2] = 10 ** rng.uniform(-1, 2, 7)
+    h[1::2] = rng.uniform(0.6, 1.8, 7)
+    cmax = 10 ** rng.uniform(-2, 1)
+    conc = np.arange(5) * cmax
+    hill = np.repeat(h[None, :], 5, axis=0)
+    spp = int(round(1000.0 / DT))
+    out = {"workload": "ORd 2011, 5 concentrations of one drug, BCL 1000 ms, dt 0.005 ms, 100 paces; timed over "
+                       "2 paces after 1 warm-up pace, 100-pace time projected"}
+    for prec in ("fp64", "mixed"):
+        b = cep.Batch("ord2011", 5, prec)
+        b.init(conc=conc, hill=hill, quirks=True)
+        b.set_pacing(1000.0)
+        b.set_protocol(DT, 100, 99, dt_write=1.0)
+        for _ in range(spp // 50000):
+            b.run(50000)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(2 * spp // 50000):
+            b.run(50000)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 2
+        out[prec] = {"ms_per_pace": ms, "s_per_100_paces": ms * 100 / 1e3, "us_per_step": ms * 1e3 / spp,
+                     "cell_steps_per_s": 5 * spp / (ms / 1e3)}
+        b.close()
+    if not args.no_cpu:
+        r, kind, secs = cpu_rate("ord2011", conc, hill, 5, spp // 2)
+        out["cpu_baseline"] = {"cell_steps_per_s": r, "kind": kind, "cores": 5,
+                               "s_per_100_paces": 5 * 100 * spp / r / 5,
+                               "sample": f"5 instances x {spp // 2} steps, one per thread ({secs:.1f} s)"}
+    return out
+
+
+def sub_results(args):
+    """The other configurations, each bounded to seconds of GPU time, as
+    extra keys of the default line: the single-cell configuration, the
+    TT2006 sheets, the ORd slab and the serving trace."""
+    import copy
+    subs = {}
+    jobs = [("config1", lambda a: config1_run(a), {}),
+            ("tt06_sheet_512x512x3", lambda a: tissue_main(a, 1, 0, 0, None),
+             dict(workload="tt06_sheet", nx=512, seg=200, steps=2, warmup=1)),
+            ("ord_slab_256x256x48x2", lambda a: slab_main(a, 1, 0, 0, None),
+             dict(workload="ord_slab", nx=512, seg=20, steps=2, warmup=1)),
+            ("serve", lambda a: serve_main(a), dict(workload="serve", jobs=20))]
+    for name, fn, over in jobs:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        try:
+            r = fn(a)
+        except Exception as e:  # a failing sub-configuration must not hide the headline
+            r = {"error": f"{type(e).__name__}: {e}"}
+        if isinstance(r, dict):
+            r.pop("peaks", None)
+            r["wall_s"] = time.perf_counter() - t0
+        subs[name] = r
+    return subs
+
+
 # ------------------------------------------------------------ tissue workload
 TISSUE_DT, TISSUE_H, TISSUE_D, TISSUE_RTOL = 0.01, 0.025, 0.0013, 1e-8
 def pcg_bytes_per_row(fmt: int, slots: int, iters: float) -> float:
@@ -782,7 +857,7 @@ def tissue_main(args, world, rank, local, pg):
         "cpu_baseline": None if args.no_cpu else tissue_cpu(args),
         "e2e": res.get("e2e"),
     }
-    print(json.dumps(line))
+    return line
 
 
 # ------------------------------------------------------------ serving workload
@@ -901,7 +976,7 @@ def serve_main(args):
         "throughput_speedup_vs_serial": b["cell_steps_per_s"] / s_["cell_steps_per_s"],
         "gpu_launches": b["launches"], "cpu_baseline": None, "e2e": None,
     }
-    print(json.dumps(line))
+    return line
 
 
 # ------------------------------------------------------------ 3D ORd slab workload
@@ -1030,7 +1105,7 @@ def slab_main(args, world, rank, local, pg):
         "gpu_launches": args.steps * args.seg * 3, "clocks": mixed["clocks"],
         "cpu_baseline": cpu, "e2e": None,
     }
-    print(json.dumps(line))
+    return line
 
 
 def main():
@@ -1038,12 +1113,14 @@ def main():
     model = model_of(args.workload)
     if args.workload == "ord_slab":
         world, rank, local, pg = dist_setup()
-        slab_main(args, world, rank, local, pg)
+        line = slab_main(args, world, rank, local, pg)
+        if line is not None:
+            print(json.dumps(line))
         if pg is not None:
             pg.destroy_process_group()
         return
     if args.workload == "serve":
-        serve_main(args)
+        print(json.dumps(serve_main(args)))
         return
     if args.workload == "tt06_sheet":
         world, rank, local, pg = dist_setup()
@@ -1059,7 +1136,9 @@ def main():
                                   "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "node-steps/s",
                                                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
             return
-        tissue_main(args, world, rank, local, pg)
+        line = tissue_main(args, world, rank, local, pg)
+        if line is not None:
+            print(json.dumps(line))
         if pg is not None:
             pg.destroy_process_group()
         return
@@ -1148,6 +1227,8 @@ def main():
         "instances_nonfinite": mixed["n_nonfinite"] + fp64["n_nonfinite"] + comp["n_nonfinite"],
         "peaks": {k: v for k, v in peaks.items() if k != "measured_peaks_json"},
     }
+    if world == 1 and not args.no_sub and args.workload == "cipa_pop":
+        line["sub_results"] = sub_results(args)
     print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
