@@ -114,12 +114,13 @@ def test_ord_fp64_biomarkers_match_oracle_short(cep, gpu, oracle):
 
 
 @pytest.mark.gpu
-def test_ord_config1_fp64_20_paces(cep, gpu, oracle):
-    """The single-cell configuration's inputs (5 concentrations, BCL 1000 ms,
-    dt 0.005 ms, last-beat biomarkers) on the FP64 path over 20 paces."""
+def test_ord_config1_fp64_100_paces(cep, gpu, oracle):
+    """The single-cell configuration end to end on the FP64 path: 5
+    concentrations, 100 paces at BCL 1000 ms, dt 0.005 ms, last-beat
+    biomarkers, against the oracle."""
     cases = _config1_cases(seed=7)
-    ref = _oracle_biomarkers(oracle, cases, 20, 19, 0.005, 1000.0)
-    b64, s64 = _gpu_biomarkers(cep, cases, "fp64", 20, 19, 0.005, 1000.0)
+    ref = _oracle_biomarkers(oracle, cases, 100, 99, 0.005, 1000.0)
+    b64, s64 = _gpu_biomarkers(cep, cases, "fp64", 100, 99, 0.005, 1000.0)
     for k, r in enumerate(ref):
         assert abs(s64[k, 0] - r["final"][0]) <= VM_TOL_FP64
         for key in ("apd90", "apd50", "cad90", "cad50"):
