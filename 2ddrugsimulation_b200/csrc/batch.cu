@@ -310,6 +310,8 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
   const double bcl = a.par[M::p_bcl() * a.ld + i];
   const double stim_start = a.par[M::p_stim_start() * a.ld + i];
   typename M::template Cur<G> c;
+  bm::Hot hot;
+  if (bm_on) bm::hot_load(a.bv, i, hot);
   for (int k = 0; k <= a.n_steps; ++k) {
     const bool can_update = iout < sc.imax;
     if (can_update && k == a.n_steps) break;  // budget spent; sample iout is taken next launch
@@ -319,7 +321,7 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
     if (bm_on && iout >= 1)
       bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
                  (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
-                 cnt_print, cnt_bcl);
+                 cnt_print, cnt_bcl, hot);
     if (!can_update) {
       st = CEP_INST_DONE;
       break;
@@ -332,6 +334,7 @@ __global__ void __launch_bounds__(kBlock) run_kernel(RunArgs a) {
     }
   }
   M::template store<G>(y, a.y, a.ld, i);
+  if (bm_on) bm::hot_store(a.bv, i, hot);
   a.t[i] = t;
   a.iout[i] = iout;
   a.status[i] = st;
@@ -369,6 +372,8 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   const double bcl = a.par[M::p_bcl() * a.ld + il];
   const double stim_start = a.par[M::p_stim_start() * a.ld + il];
   typename M::template Cur<G> c;
+  bm::Hot hot;
+  if (bm_on) bm::hot_load(a.bv, il, hot);
   int buf = 0;
   for (int k = 0; k <= a.n_steps; ++k) {
     const bool can_update = iout < sc.imax;
@@ -411,7 +416,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     if (bm_on && active && iout >= 1)
       bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
                  (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
-                 cnt_print, cnt_bcl);
+                 cnt_print, cnt_bcl, hot);
     if (active) {
       if (!can_update) {
         st = CEP_INST_DONE;
@@ -428,6 +433,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     buf ^= 1;
   }
   if (valid) {
+    if (bm_on) bm::hot_store(a.bv, i, hot);
     ord::store_role<M::kCipa>(R, y, a.y, a.ld, i);
     if constexpr (R2 >= 0) ord::store_role<M::kCipa>(R2, y, a.y, a.ld, i);
     if (R == 0) {
@@ -1006,11 +1012,20 @@ int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     b->block = (n <= sms * 8 * 32) ? 32 : 128;
-    // Below ~1.5 waves of one-thread-per-cell occupancy the 2-warps-per-32-
-    // cells kernel keeps twice the warps in flight (10,000 CiPA instances:
-    // 4.8e9 cell-steps/s against 3.6e9 for either other form).
-    b->variant = (model == CEP_MODEL_ORD2011 || model == CEP_MODEL_CIPA2017) && n <= sms * 12 * 32 ? CEP_KERNEL_PAIRS
-                                                                                               : CEP_KERNEL_CELL;
+    // Below ~1.5 waves of one-thread-per-cell occupancy the warp-specialised
+    // kernels keep more warps in flight. Measured on the CiPA population
+    // (us per step; cell / 4 roles / 2 pairs): mixed, 10,000 instances
+    // 2.90 / 2.47 / 2.16, 320 instances 2.69 / 1.38 / 1.71; FP64 (exp and
+    // log out of line), 10,000 instances 22.2 / 9.5 / 11.7, 320 instances
+    // 21.5 / 7.2 / 11.1. So FP64 takes the four roles, mixed the four roles
+    // up to one 32-cell group per SM and the pairs above.
+    const bool ord_family = model == CEP_MODEL_ORD2011 || model == CEP_MODEL_CIPA2017;
+    if (!ord_family || n > sms * 12 * 32)
+      b->variant = CEP_KERNEL_CELL;
+    else if (precision == CEP_PREC_FP64 || n <= sms * 32)
+      b->variant = CEP_KERNEL_ROLES;
+    else
+      b->variant = CEP_KERNEL_PAIRS;
   }
   int rc = CEP_OK;
   if ((rc = dev_alloc(b, &b->states, (size_t)b->ns * b->ld)) || (rc = dev_alloc(b, &b->params, (size_t)b->np * b->ld)) ||

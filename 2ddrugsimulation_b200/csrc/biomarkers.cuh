@@ -106,25 +106,54 @@ __device__ __forceinline__ void reset(const View &v, int64_t i, double vm0, doub
   v.I(I_next_peak, i) = next_multiple(1, ps);
 }
 
+// The fields the state machine touches on every step, held in registers for
+// the length of a launch: loaded before the step loop (hot_load), written
+// back after it (hot_store) and around the once-per-beat pace boundary,
+// which works on the global record. Everything else stays in global memory.
+struct Hot {
+  double qnet, inal, ical;                    // running integrals of the beat
+  double dvmdt_max, dvmdt_repol, ca_peak;     // of the temp beat record
+  double peak_time, r30, r50, r90;            // Vm-peak time, repolarisation levels
+  int pace, next_peak, eligible;
+};
+
+__device__ __forceinline__ void hot_load(const View &v, int64_t i, Hot &h) {
+  h.qnet = v.F(F_qnet, i); h.inal = v.F(F_inal, i); h.ical = v.F(F_ical, i);
+  h.dvmdt_max = v.F(F_T0 + B_dvmdt_max, i); h.dvmdt_repol = v.F(F_T0 + B_dvmdt_repol, i);
+  h.ca_peak = v.F(F_T0 + B_ca_peak, i);
+  h.peak_time = v.F(F_peak_time, i);
+  h.r30 = v.F(F_repol30, i); h.r50 = v.F(F_repol50, i); h.r90 = v.F(F_repol90, i);
+  h.pace = v.I(I_pace, i); h.next_peak = v.I(I_next_peak, i); h.eligible = v.I(I_eligible, i);
+}
+
+__device__ __forceinline__ void hot_store(const View &v, int64_t i, const Hot &h) {
+  v.F(F_qnet, i) = h.qnet; v.F(F_inal, i) = h.inal; v.F(F_ical, i) = h.ical;
+  v.F(F_T0 + B_dvmdt_max, i) = h.dvmdt_max; v.F(F_T0 + B_dvmdt_repol, i) = h.dvmdt_repol;
+  v.F(F_T0 + B_ca_peak, i) = h.ca_peak;
+  v.F(F_peak_time, i) = h.peak_time;
+  v.F(F_repol30, i) = h.r30; v.F(F_repol50, i) = h.r50; v.F(F_repol90, i) = h.r90;
+  v.I(I_pace, i) = h.pace; v.I(I_next_peak, i) = h.next_peak; v.I(I_eligible, i) = h.eligible;
+}
+
 // One sample (iout >= 1) of the state machine. V, CAI, dVdt and the six
-// qNet currents are the values at sample iout; tcurr its time.
+// qNet currents are the values at sample iout; tcurr its time. h holds the
+// hot fields (hot_load before the first sample of a launch).
 __device__ __forceinline__ void sample(const View &v, int64_t i, const Sched &s, int iout, double tcurr,
                                        double dt, double bcl, double stim_start, double V, double CAI,
                                        double dVdt, double INaL, double ICaL, double Ito, double IKr,
                                        double IKs, double IK1, double qnet_thr, int &cnt_print,
-                                       int &cnt_bcl) {
+                                       int &cnt_bcl, Hot &h) {
   // qnet and AUCs (:225-227)
   if (V > qnet_thr) {
-    v.F(F_qnet, i) += (INaL + ICaL + Ito + IKr + IKs + IK1) * dt;
-    v.F(F_inal, i) += INaL * dt;
-    v.F(F_ical, i) += ICaL * dt;
+    h.qnet += (INaL + ICaL + Ito + IKr + IKs + IK1) * dt;
+    h.inal += INaL * dt;
+    h.ical += ICaL * dt;
   }
-  int pace = v.I(I_pace, i);
   // cai samples of the evaluated beats (:230-235); cnt_print counts down to
   // the next multiple of print_freq
   if (--cnt_print == 0) {
     cnt_print = s.print_freq;
-    if (pace >= s.first_pace) {
+    if (h.pace >= s.first_pace) {
       const int n = v.I(I_n_ca, i);
       if (n < v.ca_cap) {
         v.ca_t[(int64_t)n * v.ld + i] = tcurr;
@@ -133,9 +162,11 @@ __device__ __forceinline__ void sample(const View &v, int64_t i, const Sched &s,
       }
     }
   }
-  // pace boundary (:238-293)
+  // pace boundary (:238-293), once per beat, on the global record
   if (--cnt_bcl == 0) {
     cnt_bcl = s.steps_per_bcl;
+    hot_store(v, i, h);
+    int pace = h.pace;
     if (v.I(I_eligible, i) && pace >= s.first_pace) {
       const double t_ca_peak = v.F(F_t_ca_peak, i), amp50 = v.F(F_ca_amp50, i), amp90 = v.F(F_ca_amp90, i);
       double c50c = v.F(F_cad50_curr, i), c50p = v.F(F_cad50_prev, i);
@@ -184,35 +215,35 @@ __device__ __forceinline__ void sample(const View &v, int64_t i, const Sched &s,
     v.I(I_peak_step, i) = ps;
     v.I(I_next_peak, i) = next_multiple(iout, ps);
     v.F(F_peak_time, i) = (bcl * pace) + (stim_start + 6.);
+    hot_load(v, i, h);
   }
   // last evaluated paces (:296-330)
-  if (s.first_pace >= 0 && pace >= s.first_pace) {
-    if (v.F(F_T0 + B_dvmdt_max, i) < dVdt) v.F(F_T0 + B_dvmdt_max, i) = dVdt;
-    if (iout == v.I(I_next_peak, i)) {
-      v.I(I_next_peak, i) = iout + v.I(I_peak_step, i);
+  if (s.first_pace >= 0 && h.pace >= s.first_pace) {
+    if (h.dvmdt_max < dVdt) h.dvmdt_max = dVdt;
+    if (iout == h.next_peak) {
+      h.next_peak = iout + v.I(I_peak_step, i);
       v.F(F_T0 + B_vm_peak, i) = V;
       if (V > 0.) {
         const double valley = v.F(F_T0 + B_vm_valley, i);
-        v.F(F_repol30, i) = V - (0.3 * (V - valley));
-        v.F(F_repol50, i) = V - (0.5 * (V - valley));
-        v.F(F_repol90, i) = V - (0.9 * (V - valley));
-        v.I(I_eligible, i) = 1;
+        h.r30 = V - (0.3 * (V - valley));
+        h.r50 = V - (0.5 * (V - valley));
+        h.r90 = V - (0.9 * (V - valley));
+        h.eligible = 1;
       }
-    } else if (v.I(I_eligible, i) && tcurr > v.F(F_peak_time, i)) {
-      const double r30 = v.F(F_repol30, i), r50 = v.F(F_repol50, i), r90 = v.F(F_repol90, i);
-      if (r30 >= V && V >= r90 && v.F(F_T0 + B_dvmdt_repol, i) < dVdt) v.F(F_T0 + B_dvmdt_repol, i) = dVdt;
-      if (r50 > V && V > r50 - 2) v.F(F_T0 + B_apd50, i) = tcurr - v.F(F_t_depol, i);
-      if (r90 > V && V > r90 - 2) v.F(F_T0 + B_apd90, i) = tcurr - v.F(F_t_depol, i);
-      if (v.F(F_T0 + B_ca_peak, i) < CAI) {
-        v.F(F_T0 + B_ca_peak, i) = CAI;
+    } else if (h.eligible && tcurr > h.peak_time) {
+      if (h.r30 >= V && V >= h.r90 && h.dvmdt_repol < dVdt) h.dvmdt_repol = dVdt;
+      if (h.r50 > V && V > h.r50 - 2) v.F(F_T0 + B_apd50, i) = tcurr - v.F(F_t_depol, i);
+      if (h.r90 > V && V > h.r90 - 2) v.F(F_T0 + B_apd90, i) = tcurr - v.F(F_t_depol, i);
+      if (h.ca_peak < CAI) {
+        h.ca_peak = CAI;
         const double valley = v.F(F_T0 + B_ca_valley, i);
         v.F(F_ca_amp50, i) = CAI - (0.5 * (CAI - valley));
         v.F(F_ca_amp90, i) = CAI - (0.9 * (CAI - valley));
         v.F(F_t_ca_peak, i) = tcurr;
       }
     }
-  } else if (iout == v.I(I_next_peak, i)) {
-    v.I(I_next_peak, i) = iout + v.I(I_peak_step, i);
+  } else if (iout == h.next_peak) {
+    h.next_peak = iout + v.I(I_peak_step, i);
   }
 }
 

@@ -1,8 +1,9 @@
 // Shared device-side definitions for the ionic-model kernels.
 //
 // Two precision policies drive every model template:
-//   F64   - plain FP64 path: every quantity in double, libm-equivalent exp/log
-//           (CUDA's double exp/log, <= 1 ulp), reference expression order.
+//   F64   - plain FP64 path: every quantity in double, CUDA's double exp/log
+//           (<= 1 ulp); the ORd family takes the algebraic rewrites below
+//           (CEP_F64_REWRITES), the other models the reference's forms.
 //   Mixed - gates, rate constants and channel currents in FP32 with SFU
 //           exp/log (ex2.approx / lg2.approx) and approximate division; the
 //           membrane voltage, the ionic concentrations, CaMKII and every
@@ -68,26 +69,61 @@ __device__ __forceinline__ double div64(double a, double b) {
   return isnan(out) ? div64_special(a, b) : out;
 }
 
+// FP64 takes the same algebraic rewrites as the mixed policy (rate-form
+// time constants, shared exponentials, log differences, shared reciprocals:
+// model_ord.cuh) and the series of e^{-a} for slow gates with a < 0.1; each
+// changes a result by a few ulp, far inside the FP64 path's bound against
+// the reference (1e-6 mV). Building with -DCEP_F64_REWRITES=0 restores the
+// reference's written forms.
+#ifndef CEP_F64_REWRITES
+#define CEP_F64_REWRITES 1
+#endif
+
+// CUDA's double exp and log called out of line: each inlined copy is a few
+// dozen instructions, and the ORd family's FP64 step calls them ~130 times,
+// which made the step's code too large for the instruction caches
+// (no_instruction stalls 6 cycles per issued instruction in the 2-warp form);
+// one shared copy of each keeps it resident (about 2x the FP64 throughput).
+__device__ __noinline__ double exp_f64(double x) { return ::exp(x); }
+__device__ __noinline__ double log_f64(double x) { return ::log(x); }
+
+// Two exponentials of independent arguments in one out-of-line body, where
+// the two instruction streams interleave: one call's latency for two
+// results (the ORd family's time constants are sums of two exponentials).
+__device__ __noinline__ double2 exp2_f64(double a, double b) { return make_double2(::exp(a), ::exp(b)); }
+
+template <class G>
+struct Exp2 {
+  G a, b;
+};
+
 struct F64 {
   using G = double;
   static constexpr bool kMixed = false;
+  static constexpr bool kFast = CEP_F64_REWRITES != 0;
   static constexpr bool kRates = false;
-  __device__ __forceinline__ static double ex(double x) { return ::exp(x); }
-  __device__ __forceinline__ static double lg(double x) { return ::log(x); }
+  __device__ __forceinline__ static double ex(double x) { return exp_f64(x); }
+  __device__ __forceinline__ static double lg(double x) { return log_f64(x); }
+  __device__ __forceinline__ static Exp2<double> ex2(double a, double b) {
+    const double2 r = exp2_f64(a, b);
+    return {r.x, r.y};
+  }
   __device__ __forceinline__ static double dv(double a, double b) { return div64(a, b); }
   __device__ __forceinline__ static double rc(double x) { return rcp64(x); }
   // x^y for x > 0 as exp(y log x) (the exponents here are constants of
   // order 1, so the error stays at a few ulp)
-  __device__ __forceinline__ static double pw(double x, double y) { return ::exp(y * ::log(x)); }
+  __device__ __forceinline__ static double pw(double x, double y) { return exp_f64(y * log_f64(x)); }
   __device__ __forceinline__ static double sq(double x) { return ::sqrt(x); }
 };
 
 struct Mixed {
   using G = float;
   static constexpr bool kMixed = true;
+  static constexpr bool kFast = true;
   static constexpr bool kRates = false;
   __device__ __forceinline__ static float ex(float x) { return __expf(x); }
   __device__ __forceinline__ static float lg(float x) { return __logf(x); }
+  __device__ __forceinline__ static Exp2<float> ex2(float a, float b) { return {__expf(a), __expf(b)}; }
   __device__ __forceinline__ static float dv(float a, float b) { return __fdividef(a, b); }
   __device__ __forceinline__ static float rc(float x) { return __fdividef(1.0f, x); }
   __device__ __forceinline__ static float pw(float x, float y) { return __powf(x, y); }
@@ -111,6 +147,13 @@ __device__ __forceinline__ void fe(double &y, double d, double dt) {
   else y = y + d * dt;
 }
 
+// c1 e^{x1} + c2 e^{x2} with both exponentials from one paired evaluation
+template <class P>
+__device__ __forceinline__ typename P::G esum(typename P::G c1, typename P::G x1, typename P::G c2, typename P::G x2) {
+  const auto e = P::ex2(x1, x2);
+  return c1 * e.a + c2 * e.b;
+}
+
 // x^2, x^3, x^4, x^8 by repeated products (the reference calls pow() with
 // integral exponents; products differ from a correctly rounded pow by at
 // most an ulp).
@@ -129,6 +172,22 @@ __device__ __forceinline__ float ghk_factor_e(float x, float e) {
 __device__ __forceinline__ float ghk_factor(float x) {
   if (fabsf(x) < 1e-3f) return 1.0f - 0.5f * x + x * x * (1.0f / 12.0f);
   return __fdividef(x, __expf(x) - 1.0f);
+}
+
+// e^{-a} for 0 <= a < 0.1 from its Taylor series to degree 10 (Horner):
+// the remainder a^11/11! is below 2.6e-19, under FP64 rounding.
+__device__ __forceinline__ double exp_neg_series(double a) {
+  double s = 1.0 / 3628800.0;
+  s = fma(s, -a, 1.0 / 362880.0);
+  s = fma(s, -a, 1.0 / 40320.0);
+  s = fma(s, -a, 1.0 / 5040.0);
+  s = fma(s, -a, 1.0 / 720.0);
+  s = fma(s, -a, 1.0 / 120.0);
+  s = fma(s, -a, 1.0 / 24.0);
+  s = fma(s, -a, 1.0 / 6.0);
+  s = fma(s, -a, 0.5);
+  s = fma(s, -a, 1.0);
+  return fma(s, -a, 1.0);
 }
 
 // Rush-Larsen update of a gate whose state is kept in FP64.
@@ -153,14 +212,18 @@ __device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, type
     return y + (double)((yinf - (G)y) * f);
   } else if constexpr (P::kRates) {
     return div64(yinf - y, tau);
+  } else if constexpr (P::kFast && slow) {
+    const double a = div64(dt, tau);
+    return yinf - (yinf - y) * (a < 0.1 ? exp_neg_series(a) : exp_f64(-a));
   } else {
-    return yinf - (yinf - y) * ::exp(div64(-dt, tau));
+    return yinf - (yinf - y) * exp_f64(div64(-dt, tau));
   }
 }
 
-// A gate's time constant in the form each policy integrates with. F64 keeps
-// tau itself, computed as the reference writes it, for exp(-dt/tau). Mixed
-// keeps the rate 1/tau: where tau is a quotient num/sum of the model's rate
+// A gate's time constant in the form each policy integrates with. With the
+// written forms (CEP_F64_REWRITES=0) F64 keeps tau itself, computed as the
+// reference writes it, for exp(-dt/tau). Otherwise both policies keep the
+// rate 1/tau: where tau is a quotient num/sum of the model's rate
 // terms, a = dt*sum/num needs no SFU reciprocal or division (two dependent
 // MUFU ops fewer per gate).
 template <class P>
@@ -171,7 +234,7 @@ struct Tau {
 template <class P>
 __device__ __forceinline__ Tau<P> tau_quot(double num, typename P::G sum) {
   using G = typename P::G;
-  if constexpr (P::kMixed) {
+  if constexpr (P::kFast) {
     if (num == 1.0) return {sum};
     return {sum * (G)(1.0 / num)};
   } else {
@@ -182,7 +245,7 @@ __device__ __forceinline__ Tau<P> tau_quot(double num, typename P::G sum) {
 template <class P>
 __device__ __forceinline__ Tau<P> tau_scaled(Tau<P> t, double s) {
   using G = typename P::G;
-  if constexpr (P::kMixed) return {t.v * (G)(1.0 / s)};
+  if constexpr (P::kFast) return {t.v * (G)(1.0 / s)};
   else return {(G)s * t.v};
 }
 // tau = (c + 1/sum) * s (c a constant, s = 1 unless given): F64 as written;
@@ -191,20 +254,20 @@ __device__ __forceinline__ Tau<P> tau_scaled(Tau<P> t, double s) {
 template <class P>
 __device__ __forceinline__ Tau<P> tau_affine(double c, typename P::G sum, typename P::G s = (typename P::G)1) {
   using G = typename P::G;
-  if constexpr (P::kMixed) return {P::dv(sum, ((G)c * sum + (G)1) * s)};
+  if constexpr (P::kFast) return {P::dv(sum, ((G)c * sum + (G)1) * s)};
   else return {((G)c + P::rc(sum)) * s};
 }
 // tau * s for a computed s: F64 s * tau; Mixed (1/tau) / s
 template <class P>
 __device__ __forceinline__ Tau<P> tau_times(Tau<P> t, typename P::G s) {
-  if constexpr (P::kMixed) return {P::dv(t.v, s)};
+  if constexpr (P::kFast) return {P::dv(t.v, s)};
   else return {s * t.v};
 }
 // a constant tau
 template <class P>
 __device__ __forceinline__ Tau<P> tau_const(double tau) {
   using G = typename P::G;
-  if constexpr (P::kMixed) return {(G)(1.0 / tau)};
+  if constexpr (P::kFast) return {(G)(1.0 / tau)};
   else return {(G)tau};
 }
 template <class P, bool slow = false>
@@ -218,6 +281,10 @@ __device__ __forceinline__ double rush_larsen(double y, typename P::G yinf, Tau<
     else
       f = (G)1 - P::ex(-a);
     return y + (double)((yinf - (G)y) * f);
+  } else if constexpr (P::kFast) {  // t.v is the rate 1/tau
+    if constexpr (P::kRates) return (yinf - y) * t.v;
+    const double a = dt * t.v;
+    return yinf - (yinf - y) * ((slow && a < 0.1) ? exp_neg_series(a) : exp_f64(-a));
   } else {
     return rush_larsen<P, slow>(y, yinf, t.v, dt);
   }

@@ -276,10 +276,10 @@ __device__ __forceinline__ Ctx<typename P::G> context(const Y<typename P::G> &y,
   c.v = (G)y.V;
   // mixed: a/(1 + K/c) as a c/(c + K), one division for two
   const G cass = (G)y.cass;
-  const G CaMKb = P::kMixed ? P::dv((G)k::CaMKo * ((G)1 - (G)y.CaMKt) * cass, cass + (G)k::KmCaM)
+  const G CaMKb = P::kFast ? P::dv((G)k::CaMKo * ((G)1 - (G)y.CaMKt) * cass, cass + (G)k::KmCaM)
                             : P::dv(((G)k::CaMKo * ((G)1 - (G)y.CaMKt)), ((G)1 + P::dv((G)k::KmCaM, cass)));
   const G CaMKa = CaMKb + (G)y.CaMKt;
-  c.fCaMKp = P::kMixed ? P::dv(CaMKa, CaMKa + (G)k::KmCaMK) : P::rc(((G)1 + P::dv((G)k::KmCaMK, CaMKa)));
+  c.fCaMKp = P::kFast ? P::dv(CaMKa, CaMKa + (G)k::KmCaMK) : P::rc(((G)1 + P::dv((G)k::KmCaMK, CaMKa)));
   c.stim = stim_mode < 0 ? stim_on(t, q.stim_start, q.BCL, q.duration) : (stim_mode != 0);
   return c;
 }
@@ -299,13 +299,13 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
   } else if constexpr (kCipa) {
     const double ffrt = k::F * k::FRT, B = (double)z * k::FRT;
     const double U = B * V;
-    const double ee = ::exp((double)z * (V * k::FRT));
+    const double ee = exp_f64((double)z * (V * k::FRT));
     e = ee;
     // A*U/(e^U - 1) with A = ffrt*(...)/B  ->  factor = ffrt/B * U/(e^U - 1)
     fac = (-1.0e-07 <= U && U <= 1.0e-07) ? (ffrt / B) * (1.0 - 0.5 * U) : (ffrt / B) * div64(U, ee - 1.0);
   } else {
     const double vffrt = (V * k::F * k::F) / (k::R * k::T);
-    const double ee = ::exp((double)z * ((V * k::F) / (k::R * k::T)));
+    const double ee = exp_f64((double)z * ((V * k::F) / (k::R * k::T)));
     e = ee;
     fac = div64(vffrt, ee - 1.0);
   }
@@ -318,27 +318,23 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   const G mss = P::rc((one + P::ex(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2))));
-  const Tau<P> tm = tau_quot<P>(1.0, ((G)k::mtD1 * P::ex((v + (G)k::mtV1) * (G)(1.0 / k::mtV2)) +
-                      (G)k::mtD2 * P::ex(-(v + (G)k::mtV3) * (G)(1.0 / k::mtV4))));
+  const Tau<P> tm = tau_quot<P>(1.0, (esum<P>((G)k::mtD1, (v + (G)k::mtV1) * (G)(1.0 / k::mtV2), (G)k::mtD2, -(v + (G)k::mtV3) * (G)(1.0 / k::mtV4))));
   const G e_hss = P::ex((v + (G)k::hssV1) * (G)(1.0 / k::hssV2));
   const G hss = P::rc((one + e_hss));
-  const Tau<P> thf = tau_quot<P>(1.0, ((G)1.432e-05 * P::ex(-(v + (G)1.196) * (G)(1.0 / 6.285)) +
-                       (G)6.149 * P::ex((v + (G)0.5096) * (G)(1.0 / 20.27))));
-  const Tau<P> ths = tau_quot<P>(1.0, ((G)0.009794 * P::ex(-(v + (G)17.95) * (G)(1.0 / 28.05)) +
-                       (G)0.3343 * P::ex((v + (G)5.73) * (G)(1.0 / 56.66))));
-  const Tau<P> tj = tau_affine<P>(2.038, ((G)0.02136 * P::ex(-(v + (G)100.6) * (G)(1.0 / 8.281)) +
-                                 (G)0.3052 * P::ex((v + (G)0.9941) * (G)(1.0 / 38.45))));
+  const Tau<P> thf = tau_quot<P>(1.0, (esum<P>((G)1.432e-05, -(v + (G)1.196) * (G)(1.0 / 6.285), (G)6.149, (v + (G)0.5096) * (G)(1.0 / 20.27))));
+  const Tau<P> ths = tau_quot<P>(1.0, (esum<P>((G)0.009794, -(v + (G)17.95) * (G)(1.0 / 28.05), (G)0.3343, (v + (G)5.73) * (G)(1.0 / 56.66))));
+  const Tau<P> tj = tau_affine<P>(2.038, (esum<P>((G)0.02136, -(v + (G)100.6) * (G)(1.0 / 8.281), (G)0.3052, (v + (G)0.9941) * (G)(1.0 / 38.45))));
   static_assert(k::hssV1 == 82.9 && k::hssV2 == 6.086, "hssp_shift assumes hss = 1/(1+e^((V+82.9)/6.086))");
-  const G hssp = P::kMixed ? P::rc(one + e_hss * (G)k::hssp_shift)
+  const G hssp = P::kFast ? P::rc(one + e_hss * (G)k::hssp_shift)
                            : P::rc((one + P::ex((v + (G)89.1) * (G)(1.0 / 6.086))));
   const G mLss = P::rc((one + P::ex(-(v + (G)42.85) * (G)(1.0 / 5.264))));
   const G e_hL = P::ex((v + (G)87.61) * (G)(1.0 / 7.488));
   const G hLss = P::rc((one + e_hL));
-  const G hLssp = P::kMixed ? P::rc(one + e_hL * (G)k::hLssp_shift)
+  const G hLssp = P::kFast ? P::rc(one + e_hL * (G)k::hLssp_shift)
                             : P::rc((one + P::ex((v + (G)93.81) * (G)(1.0 / 7.488))));
   const G fp_ = c.fCaMKp;
   // INa, INaL
-  const G ENa = P::kMixed ? (G)k::RTF * ((G)k::log_nao - P::lg((G)y.nai))
+  const G ENa = P::kFast ? (G)k::RTF * ((G)k::log_nao - P::lg((G)y.nai))
                           : (G)k::RTF * P::lg(P::dv((G)k::nao, (G)y.nai));
   const G h_ = (G)k::Ahf * (G)y.hf + (G)k::Ahs * (G)y.hs;
   const G hp = (G)k::Ahf * (G)y.hf + (G)k::Ahs * (G)y.hsp;
@@ -352,7 +348,7 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G nai_g = (G)y.nai, ki_g = (G)y.ki;
   // nao/Knao and nai/Knai: in mixed, nao/Knao0 e^(-c v) without a division
   G nao_Knao, nai_Knai;
-  if constexpr (P::kMixed) {
+  if constexpr (P::kFast) {
     nao_Knao = (G)(k::nao / k::Knao0) * P::ex(-((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
     nai_Knai = nai_g * (G)(1.0 / k::Knai0) * P::ex(-((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
   } else {
@@ -408,28 +404,24 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const G ass = P::rc((one + e_a));
   const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + P::ex(-(v - (G)18.4099) * (G)(1.0 / 29.3814))))) +
                             P::dv((G)3.5, (one + P::ex((v + (G)100.0) * (G)(1.0 / 29.3814))))));
-  const G assp = P::kMixed ? P::rc(one + e_a * (G)k::assp_shift)
+  const G assp = P::kFast ? P::rc(one + e_a * (G)k::assp_shift)
                            : P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
   const G iss = P::rc((one + P::ex((v + (G)43.94) * (G)(1.0 / 5.711))));
   const G delta_epi = q.celltype == 1 ? one - P::dv((G)0.95, (one + P::ex((v + (G)70.0) * (G)0.2))) : one;
-  const Tau<P> tiF = tau_affine<P>(4.562, ((G)0.3933 * P::ex(-(v + (G)100.0) * (G)0.01) +
-                                            (G)0.08004 * P::ex((v + (G)50.0) * (G)(1.0 / 16.59))), delta_epi);
-  const Tau<P> tiS = tau_affine<P>(23.62, ((G)0.001416 * P::ex(-(v + (G)96.52) * (G)(1.0 / 59.05)) +
-                                            (G)1.78e-08 * P::ex((v + (G)114.1) * (G)(1.0 / 8.079))), delta_epi);
-  const G dti_develop = (G)1.354 + P::dv((G)1e-4, (P::ex((v - (G)167.4) * (G)(1.0 / 15.89)) +
-                                              P::ex(-(v - (G)12.23) * (G)(1.0 / 0.2154))));
+  const Tau<P> tiF = tau_affine<P>(4.562, (esum<P>((G)0.3933, -(v + (G)100.0) * (G)0.01, (G)0.08004, (v + (G)50.0) * (G)(1.0 / 16.59))), delta_epi);
+  const Tau<P> tiS = tau_affine<P>(23.62, (esum<P>((G)0.001416, -(v + (G)96.52) * (G)(1.0 / 59.05), (G)1.78e-08, (v + (G)114.1) * (G)(1.0 / 8.079))), delta_epi);
+  const G dti_develop = (G)1.354 + P::dv((G)1e-4, (esum<P>((G)1, (v - (G)167.4) * (G)(1.0 / 15.89), (G)1, -(v - (G)12.23) * (G)(1.0 / 0.2154))));
   const G dti_recover = one - P::dv((G)0.5, (one + P::ex((v + (G)70.0) * (G)0.05)));
   const G dti = dti_develop * dti_recover;
   const G xs1ss = P::rc((one + P::ex(-(v + (G)11.60) * (G)(1.0 / 8.932))));
-  const Tau<P> txs1 = tau_affine<P>(817.3, ((G)2.326e-04 * P::ex((v + (G)48.28) * (G)(1.0 / 17.80)) +
-                                   (G)0.001292 * P::ex(-(v + (G)210.0) * (G)(1.0 / 230.0))));
+  const Tau<P> txs1 = tau_affine<P>(817.3, (esum<P>((G)2.326e-04, (v + (G)48.28) * (G)(1.0 / 17.80), (G)0.001292, -(v + (G)210.0) * (G)(1.0 / 230.0))));
   const Tau<P> txs2 =
-      tau_quot<P>(1.0, ((G)0.01 * P::ex((v - (G)50.0) * (G)0.05) + (G)0.0193 * P::ex(-(v + (G)66.54) * (G)(1.0 / 31.0))));
+      tau_quot<P>(1.0, (esum<P>((G)0.01, (v - (G)50.0) * (G)0.05, (G)0.0193, -(v + (G)66.54) * (G)(1.0 / 31.0))));
   const G xk1ss = P::rc((one + P::ex(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den))));
   const Tau<P> txk1 =
-      tau_quot<P>(122.2, (P::ex(-(v + (G)127.2) * (G)(1.0 / 20.36)) + P::ex((v + (G)236.8) * (G)(1.0 / 69.33))));
+      tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
   const G fp_ = c.fCaMKp;
-  const G EK = P::kMixed ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+  const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
                          : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
   const G AiF = P::rc((one + P::ex((v - (G)213.6) * (G)(1.0 / 151.2))));
   const G AiS = one - AiF;
@@ -440,22 +432,20 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   Tau<P> txrf = tau_const<P>(1.0), txrs = tau_const<P>(1.0);
   if constexpr (!kCipa) {
     xrss = P::rc((one + P::ex(-(v + (G)8.337) * (G)(1.0 / 6.789))));
-    txrf = tau_affine<P>(12.98, ((G)0.3652 * P::ex((v - (G)31.66) * (G)(1.0 / 3.869)) +
-                             (G)4.123e-05 * P::ex(-(v - (G)47.78) * (G)(1.0 / 20.38))));
-    txrs = tau_affine<P>(1.865, ((G)0.06629 * P::ex((v - (G)34.70) * (G)(1.0 / 7.355)) +
-                             (G)1.128e-05 * P::ex(-(v - (G)29.74) * (G)(1.0 / 25.94))));
+    txrf = tau_affine<P>(12.98, (esum<P>((G)0.3652, (v - (G)31.66) * (G)(1.0 / 3.869), (G)4.123e-05, -(v - (G)47.78) * (G)(1.0 / 20.38))));
+    txrs = tau_affine<P>(1.865, (esum<P>((G)0.06629, (v - (G)34.70) * (G)(1.0 / 7.355), (G)1.128e-05, -(v - (G)29.74) * (G)(1.0 / 25.94))));
     const G Axrf = P::rc((one + P::ex((v + (G)54.81) * (G)(1.0 / 38.21))));
     const G xr = Axrf * (G)y.xrf + (one - Axrf) * (G)y.xrs;
-    const G rkr = P::kMixed ? P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))) *
+    const G rkr = P::kFast ? P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))) *
                                     (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0))))
                             : P::dv((P::rc((one + P::ex((v + (G)55.0) * (G)(1.0 / 75.0))))),
                                     (one + P::ex((v - (G)10.0) * (G)(1.0 / 30.0))));
     IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
   }
-  const G EKs = P::kMixed
+  const G EKs = P::kFast
                     ? (G)k::RTF * ((G)k::log_ks_o - P::lg((G)(y.ki + k::PKNa * y.nai)))
                     : (G)k::RTF * P::lg(P::dv((G)(k::ko + k::PKNa * k::nao), (G)(y.ki + k::PKNa * y.nai)));
-  const G KsCa = P::kMixed
+  const G KsCa = P::kFast
                      ? one + P::dv((G)0.6, (one + P::ex((G)1.4 * ((G)k::log_ks_ca - P::lg((G)y.cai)))))
                      : one + P::dv((G)0.6, (one + P::pw(P::dv((G)3.8e-05, (G)y.cai), (G)1.4)));
   const G IKs = q.GKs * KsCa * (G)y.xs1 * (G)y.xs2 * (v - EKs);
@@ -494,14 +484,12 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   const G dss = P::rc((one + P::ex(-(v + (G)3.94) * (G)(1.0 / 4.23))));
-  const Tau<P> td = tau_affine<P>(0.6, (P::ex((G)-0.05 * (v + (G)6.0)) + P::ex((G)0.09 * (v + (G)14.0))));
+  const Tau<P> td = tau_affine<P>(0.6, (esum<P>((G)1, (G)-0.05 * (v + (G)6.0), (G)1, (G)0.09 * (v + (G)14.0))));
   const G fss = P::rc((one + P::ex((v + (G)19.58) * (G)(1.0 / 3.696))));
-  const Tau<P> tff = tau_affine<P>(7.0, ((G)0.0045 * P::ex(-(v + (G)20.0) * (G)0.1) + (G)0.0045 * P::ex((v + (G)20.0) * (G)0.1)));
-  const Tau<P> tfs = tau_affine<P>(1000.0, ((G)3.5e-05 * P::ex(-(v + (G)5.0) * (G)0.25) +
-                                   (G)3.5e-05 * P::ex((v + (G)5.0) * (G)(1.0 / 6.0))));
-  const Tau<P> tfcaf = tau_affine<P>(7.0, ((G)0.04 * P::ex(-(v - (G)4.0) * (G)(1.0 / 7.0)) +
-                                  (G)0.04 * P::ex((v - (G)4.0) * (G)(1.0 / 7.0))));
-  const Tau<P> tfcas = tau_affine<P>(100.0, ((G)0.00012 * P::ex(-v * (G)(1.0 / 3.0)) + (G)0.00012 * P::ex(v * (G)(1.0 / 7.0))));
+  const Tau<P> tff = tau_affine<P>(7.0, (esum<P>((G)0.0045, -(v + (G)20.0) * (G)0.1, (G)0.0045, (v + (G)20.0) * (G)0.1)));
+  const Tau<P> tfs = tau_affine<P>(1000.0, (esum<P>((G)3.5e-05, -(v + (G)5.0) * (G)0.25, (G)3.5e-05, (v + (G)5.0) * (G)(1.0 / 6.0))));
+  const Tau<P> tfcaf = tau_affine<P>(7.0, (esum<P>((G)0.04, -(v - (G)4.0) * (G)(1.0 / 7.0), (G)0.04, (v - (G)4.0) * (G)(1.0 / 7.0))));
+  const Tau<P> tfcas = tau_affine<P>(100.0, (esum<P>((G)0.00012, -v * (G)(1.0 / 3.0), (G)0.00012, v * (G)(1.0 / 7.0))));
   const G km2n = (G)y.jca;
   const G cass_g = (G)y.cass, cai_g = (G)y.cai, cajsr_g = (G)y.cajsr;
   const G anca = P::rc((P::dv((G)k::k2n, km2n) + p4(one + P::dv((G)k::Kmn, cass_g))));
@@ -545,7 +533,7 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   const G den_tau = one + P::dv((G)0.0123, cajsr_g);
   G Jrel_inf_t, Jrel_t;
   Tau<P> tau_rel, tau_relp;  // bt / den_tau, floored at 0.001 ms
-  if constexpr (P::kMixed) {  // one reciprocal for both targets; rates capped at 1000 /ms
+  if constexpr (P::kFast) {  // one reciprocal for both targets; rates capped at 1000 /ms
     const G r = P::rc(rel_den);
     Jrel_inf_t = (G)k::a_rel * -ICaL * r;
     Jrel_t = (G)k::a_relp * -ICaL * r;
@@ -593,7 +581,7 @@ __device__ __forceinline__ typename P::G naca(typename P::G na, typename P::G ca
   const G h1 = one + ((na) * (G)(1.0 / k::kna3)) * (one + hna);
   const G h4 = one + ((na) * (G)(1.0 / k::kna1)) * (one + (na) * (G)(1.0 / k::kna2));
   G h2, h5, k4p, k6;
-  if constexpr (P::kMixed) {  // 1/h1, 1/h4 (and 1/hca, shared by both compartments) each once
+  if constexpr (P::kFast) {  // 1/h1, 1/h4 (and 1/hca, shared by both compartments) each once
     const G rh1 = P::rc(h1), rh4 = P::rc(h4);
     h2 = na * hna * (G)(1.0 / k::kna3) * rh1;
     h5 = na * na * (G)(1.0 / (k::kna1 * k::kna2)) * rh4;
@@ -701,7 +689,7 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
   G IKr = (G)0;
   if constexpr (kCipa) {
     // dynamic hERG: IKr = GKr sqrt(ko/5.4) O (V - EK) (ohara_rudy_cipa_v1_2017.cpp:2307)
-    const G EK = P::kMixed ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+    const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
                            : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
     IKr = q.GKr * (G)k::sqrt_ko54 * (G)y.O * (v - EK);
   }
@@ -719,20 +707,27 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
     // 2157-2165), forward Euler like every other non-gate state. Rates
     // k = A exp(B V) Q10; bound-drug states use the instance's bind = Kmax Ku
     // D^n/(D^n + halfmax), Ku, and Kt / (1 + exp(-(V - Vhalf)/6.789)).
-    const G k1 = (G)cipa::A1 * P::ex((G)cipa::B1 * v) * (G)cipa::Q1;
-    const G k2 = (G)cipa::A2 * P::ex((G)cipa::B2 * v) * (G)cipa::Q2;
-    const G k3m = (G)cipa::A3 * P::ex((G)cipa::B3 * v) * (G)cipa::Q3;
-    const G k4m = (G)cipa::A4 * P::ex((G)cipa::B4 * v) * (G)cipa::Q4;
-    const G k11 = (G)cipa::A11 * P::ex((G)cipa::B11 * v) * (G)cipa::Q11;
-    const G k21 = (G)cipa::A21 * P::ex((G)cipa::B21 * v) * (G)cipa::Q21;
-    const G k31 = (G)cipa::A31 * P::ex((G)cipa::B31 * v) * (G)cipa::Q31;
-    const G k41 = (G)cipa::A41 * P::ex((G)cipa::B41 * v) * (G)cipa::Q41;
-    const G k51 = (G)cipa::A51 * P::ex((G)cipa::B51 * v) * (G)cipa::Q51;
-    const G k52 = (G)cipa::A52 * P::ex((G)cipa::B52 * v) * (G)cipa::Q52;
-    const G k53 = (G)cipa::A53 * P::ex((G)cipa::B53 * v) * (G)cipa::Q53;
-    const G k61 = (G)cipa::A61 * P::ex((G)cipa::B61 * v) * (G)cipa::Q61;
-    const G k62 = (G)cipa::A62 * P::ex((G)cipa::B62 * v) * (G)cipa::Q62;
-    const G k63 = (G)cipa::A63 * P::ex((G)cipa::B63 * v) * (G)cipa::Q63;
+    const auto e1_2 = P::ex2((G)cipa::B1 * v, (G)cipa::B2 * v);
+    const G k1 = (G)cipa::A1 * e1_2.a * (G)cipa::Q1;
+    const G k2 = (G)cipa::A2 * e1_2.b * (G)cipa::Q2;
+    const auto e3_4 = P::ex2((G)cipa::B3 * v, (G)cipa::B4 * v);
+    const G k3m = (G)cipa::A3 * e3_4.a * (G)cipa::Q3;
+    const G k4m = (G)cipa::A4 * e3_4.b * (G)cipa::Q4;
+    const auto e11_21 = P::ex2((G)cipa::B11 * v, (G)cipa::B21 * v);
+    const G k11 = (G)cipa::A11 * e11_21.a * (G)cipa::Q11;
+    const G k21 = (G)cipa::A21 * e11_21.b * (G)cipa::Q21;
+    const auto e31_41 = P::ex2((G)cipa::B31 * v, (G)cipa::B41 * v);
+    const G k31 = (G)cipa::A31 * e31_41.a * (G)cipa::Q31;
+    const G k41 = (G)cipa::A41 * e31_41.b * (G)cipa::Q41;
+    const auto e51_52 = P::ex2((G)cipa::B51 * v, (G)cipa::B52 * v);
+    const G k51 = (G)cipa::A51 * e51_52.a * (G)cipa::Q51;
+    const G k52 = (G)cipa::A52 * e51_52.b * (G)cipa::Q52;
+    const auto e53_61 = P::ex2((G)cipa::B53 * v, (G)cipa::B61 * v);
+    const G k53 = (G)cipa::A53 * e53_61.a * (G)cipa::Q53;
+    const G k61 = (G)cipa::A61 * e53_61.b * (G)cipa::Q61;
+    const auto e62_63 = P::ex2((G)cipa::B62 * v, (G)cipa::B63 * v);
+    const G k62 = (G)cipa::A62 * e62_63.a * (G)cipa::Q62;
+    const G k63 = (G)cipa::A63 * e62_63.b * (G)cipa::Q63;
     const G unb = P::dv(q.Ku * k53, k63);
     const G trap = P::dv(q.Kt, one + P::ex(-(v - q.Vhalf) * (G)(1.0 / 6.789)));
     // The chain is linear in its states for this step's V: forward Euler

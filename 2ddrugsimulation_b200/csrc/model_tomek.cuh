@@ -109,7 +109,7 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
     fac = ghk_factor(x) * (G)(k::F / z);
   } else {
     const double vffrt = (V * k::F * k::F) / (k::R * k::T);
-    const double ee = ::exp((double)z * ((V * k::F) / (k::R * k::T)));
+    const double ee = exp_f64((double)z * ((V * k::F) / (k::R * k::T)));
     e = ee;
     fac = div64(vffrt, ee - 1.0);
   }

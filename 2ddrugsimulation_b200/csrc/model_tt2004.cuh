@@ -166,7 +166,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
     i_CaL = q.gCaL * (G)y.d * (G)y.f * (G)y.fCa * (G)(2.0 * k::F) * ghk_factor(x) * (cai * e - (G)(0.341 * k::Ca_o));
   } else {
     const double vv = y.V;
-    const double e = ::exp((2.0 * vv * k::F) / k::RT);
+    const double e = exp_f64((2.0 * vv * k::F) / k::RT);
     i_CaL = div64(((q.gCaL * y.d * y.f * y.fCa * 4.0 * vv * (k::F * k::F)) / k::RT) * (y.Ca_i * e - 0.341 * k::Ca_o),
                   e - 1.0);
   }
@@ -204,7 +204,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
     y.j = rush_larsen<P>(y.j, j_inf, tau_j, dt);
     y.d = rush_larsen<P>(y.d, d_inf, tau_d, dt);
   } else {
-#define CEP_RL(n, inf, tau) y.n = ((y.n - (inf)) * ::exp(div64(-dt, (tau)))) + (inf);
+#define CEP_RL(n, inf, tau) y.n = ((y.n - (inf)) * exp_f64(div64(-dt, (tau)))) + (inf);
     CEP_RL(f, f_inf, tau_f) CEP_RL(s, s_inf, tau_s) CEP_RL(r, r_inf, tau_r) CEP_RL(Xr1, xr1_inf, tau_xr1)
     CEP_RL(Xr2, xr2_inf, tau_xr2) CEP_RL(Xs, xs_inf, tau_xs) CEP_RL(m, m_inf, tau_m) CEP_RL(h, h_inf, tau_h)
     CEP_RL(j, j_inf, tau_j) CEP_RL(d, d_inf, tau_d)

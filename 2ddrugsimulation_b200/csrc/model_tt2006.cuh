@@ -162,7 +162,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
             ((G)0.25 * cass_g * e - (G)k::Ca_o);
   } else {
     const double vv = y.V;
-    const double e = ::exp((2.0 * (vv - 15.0) * k::F) / (k::R * k::T));
+    const double e = exp_f64((2.0 * (vv - 15.0) * k::F) / (k::R * k::T));
     i_CaL = div64(((q.gCaL * y.d * y.f * y.f2 * y.fCass * 4.0 * (vv - 15.0) * (k::F * k::F)) / (k::R * k::T)) *
                       (0.25 * y.Ca_ss * e - k::Ca_o),
                   e - 1.0);
@@ -209,7 +209,7 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
     y.j = rush_larsen<P>(y.j, j_inf, tau_j, dt);
     y.d = rush_larsen<P>(y.d, d_inf, tau_d, dt);
   } else {
-#define CEP_RL(n, inf, tau) y.n = ((y.n - (inf)) * ::exp(div64(-dt, (tau)))) + (inf);
+#define CEP_RL(n, inf, tau) y.n = ((y.n - (inf)) * exp_f64(div64(-dt, (tau)))) + (inf);
     CEP_RL(f, f_inf, tau_f) CEP_RL(f2, f2_inf, tau_f2) CEP_RL(fCass, fCass_inf, tau_fCass) CEP_RL(s, s_inf, tau_s)
     CEP_RL(r, r_inf, tau_r) CEP_RL(Xr1, xr1_inf, tau_xr1) CEP_RL(Xr2, xr2_inf, tau_xr2) CEP_RL(Xs, xs_inf, tau_xs)
     CEP_RL(m, m_inf, tau_m) CEP_RL(h, h_inf, tau_h) CEP_RL(j, j_inf, tau_j) CEP_RL(d, d_inf, tau_d)
