@@ -28,6 +28,7 @@ REF_LIBS = {
     "tt2004": "libref_tt2004b.so",
     "tomek2019": "libref_tomek2019.so",
     "fem": "libref_fem.so",
+    "ord2011_neo": "libref_ord2011_neo.so",
     "bench": "libref_bench.so",
 }
 
@@ -58,6 +59,10 @@ BEAT_FIELDS = ("qnet", "inal_auc", "ical_auc", "dvmdt_repol", "dvmdt_max", "vm_p
 
 class CepoBeat(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in BEAT_FIELDS]
+
+
+class CepoHrvRecord(ctypes.Structure):
+    _fields_ = [("beat", CepoBeat), ("bcl", ctypes.c_int), ("steepest_pace", ctypes.c_int)]
 
 
 class CepoBiomarkers(ctypes.Structure):
@@ -112,6 +117,9 @@ def lib() -> ctypes.CDLL:
         L.cepo_fem_assemble.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, _dp, ctypes.c_int, _ip, _ip, _dp, _dp]
         L.cepo_scale.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_int, ctypes.c_double]
+        L.cepo_ord_set_cumm.argtypes = [ctypes.POINTER(CepoCell), ctypes.c_double]
+        L.cepo_hrv_run.argtypes = [ctypes.POINTER(CepoCell), _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int, ctypes.POINTER(CepoHrvRecord)]
         L.cepo_fem_element.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_int, _dp, _dp]
         L.cepo_element.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.cepo_pseudo_ecg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp,
@@ -214,6 +222,18 @@ class Cell:
         out.update(steepest_pace=bm.steepest_pace, n_eligible=bm.n_eligible, status=bm.status)
         return out, (vt if v_stride else None)
 
+
+    def hrv(self, bcls, dt: float, dt_write: float = 1.0, num_pace1: int | None = None) -> dict:
+        """hrv_bench.cpp:146-343 on the fixed-step scheme (ORd 2011, the
+        CEPCell_NEO build: quirks=2): one pace per BCL. Returns the printed
+        record's fields (the chosen beat, its BCL and pace)."""
+        b = np.ascontiguousarray(bcls, dtype=np.float64)
+        rec = CepoHrvRecord()
+        st = lib().cepo_hrv_run(ctypes.byref(self.c), _ptr(self.y), _ptr(b), len(b), float(dt), float(dt_write),
+                                int(len(b) if num_pace1 is None else num_pace1), ctypes.byref(rec))
+        out = {f: getattr(rec.beat, f) for f in BEAT_FIELDS}
+        out.update(bcl=rec.bcl, steepest_pace=rec.steepest_pace, status=st)
+        return out
 
     def restitution(self, bcls, n_pace: int, dt: float, max_records: int = 100000):
         """apdr_bench.cpp:103-232 on the fixed-step scheme; returns (records as a

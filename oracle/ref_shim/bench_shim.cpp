@@ -31,6 +31,7 @@
 
 #include "../modules/cipa_drug_bench.hpp"
 #include "../modules/commons.hpp"
+#include "../modules/hrv_bench.hpp"
 #include "../modules/globals.hpp"
 #include "Ohara_Rudy_2011.hpp"
 #include "cep_oracle.h"
@@ -44,6 +45,9 @@ struct OracleCell {
   double bcl = 1000.0, amp = -80.0, gna = 75.0;
 };
 std::map<const patch_clamp *, OracleCell> g_cells;
+// hrv_bench runs the CEPCell_NEO build (oracle quirk mode 2) with its
+// cumulative stimulus (the oracle's tissue_stim 2)
+bool g_hrv = false;
 
 // a caller's CONSTANTS writes (cipa_drug_bench.cpp:146-148) into the oracle cell
 void sync_consts(const patch_clamp *p, const double *C) {
@@ -57,6 +61,7 @@ void sync_consts(const patch_clamp *p, const double *C) {
     cepo_scale(&o.c, 0, C[GNa] / o.gna);
     o.gna = C[GNa];
   }
+  if (g_hrv) cepo_ord_set_cumm(&o.c, C[cumm_BCL]);
 }
 
 struct CvMem {
@@ -91,7 +96,8 @@ void Ohara_Rudy_2011::initConsts(double type) { initConsts(type, 0.0, nullptr, f
 void Ohara_Rudy_2011::initConsts(double type, bool is_dutta) { initConsts(type, 0.0, nullptr, is_dutta); }
 void Ohara_Rudy_2011::initConsts(double type, double D, double *hill, bool is_dutta) {
   OracleCell o;
-  cepo_init(&o.c, CEPO_ORD2011, type, D, hill, hill ? 14 : 0, is_dutta ? 1 : 0, 0);
+  cepo_init(&o.c, CEPO_ORD2011, type, D, hill, hill ? 14 : 0, is_dutta ? 1 : 0, g_hrv ? 2 : 0);
+  if (g_hrv) o.c.tissue_stim = 2;
   cepo_init_states(&o.c, STATES);
   g_cells[this] = o;
   // the pacing the bench reads back (stimulus at 10 ms for 0.5 ms: the
@@ -101,6 +107,7 @@ void Ohara_Rudy_2011::initConsts(double type, double D, double *hill, bool is_du
   CONSTANTS[GNa] = o.gna;
   CONSTANTS[stim_start] = 10.0;
   CONSTANTS[duration] = 0.5;
+  CONSTANTS[cumm_BCL] = 0.0;
 }
 void Ohara_Rudy_2011::computeRates(double TIME, double *C, double *R, double *S, double *A) {
   sync_consts(this, C);
@@ -114,6 +121,7 @@ void Ohara_Rudy_2011::computeRates(double TIME, double *C, double *R, double *S,
 N_Vector N_VMake_Serial(long length, realtype *data) { return new cep_nvector{length, data}; }
 realtype *N_VGetArrayPointer_Serial(N_Vector v) { return v->data; }
 void N_VDestroy(N_Vector v) { delete v; }
+void N_VDestroy_Serial(N_Vector v) { delete v; }
 void *CVodeCreate(int, int) { return new CvMem(); }
 int CVodeInit(void *mem, CVRhsFn, realtype t0, N_Vector) {
   static_cast<CvMem *>(mem)->t = t0;
@@ -134,8 +142,12 @@ int CVode(void *mem, realtype tout, N_Vector y, realtype *tret, int) {
   CvMem *m = static_cast<CvMem *>(mem);
   const patch_clamp *p = static_cast<const patch_clamp *>(m->user);
   sync_consts(p, p->CONSTANTS);
-  cepo_step(&g_cells[p].c, m->t, tout - m->t, y->data, nullptr);
-  m->t = tout;
+  // a time already reached (hrv_bench.cpp:185-192 rewinds tnext by dt) is no
+  // step: the state stays as it is
+  if (tout > m->t) {
+    cepo_step(&g_cells[p].c, m->t, tout - m->t, y->data, nullptr);
+    m->t = tout;
+  }
   *tret = tout;
   return CV_SUCCESS;
 }
@@ -173,5 +185,33 @@ extern "C" int ref_cipa_bench(const char *workdir, const char *hill_file, const 
   char cwd[4096];
   if (!getcwd(cwd, sizeof(cwd)) || chdir(workdir) != 0) return 1;
   cipa_drug_bench(0, nullptr, &p, true);  // writes result/result_<drug>_<time>.zip
+  return chdir(cwd) == 0 ? 0 : 2;
+}
+
+// The reference's HRV bench (hrv_bench.cpp) over the same cell: one pace per
+// line of the HRV file, results in result/<conc>/ (not zipped).
+extern "C" int ref_hrv_bench(const char *workdir, const char *hill_file, const char *hrv_file, const char *concs,
+                             const char *drug, double celltype, double dt, double dt_write, int num_pace) {
+  param_t &p = *static_cast<param_t *>(std::calloc(1, sizeof(param_t)));
+  set_default_values(&p);
+  p.celltype = celltype;
+  p.dt = dt;
+  p.dt_write = dt_write;
+  p.num_pace1 = num_pace;
+  p.is_print_graph = 0;
+  p.stim_amp = 1.0;
+  std::snprintf(p.hill_file, sizeof(p.hill_file), "%s", hill_file);
+  std::snprintf(p.hrv_files, sizeof(p.hrv_files), "%s", hrv_file);
+  std::snprintf(p.concs, sizeof(p.concs), "%s", concs);
+  std::snprintf(p.drug_name, sizeof(p.drug_name), "%s", drug);
+  mympi::rank = 0;
+  mympi::size = 1;
+  glob_var::is_hrv = true;
+  g_hrv = true;
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof(cwd)) || chdir(workdir) != 0) return 1;
+  hrv_bench(0, nullptr, &p);
+  g_hrv = false;
+  glob_var::is_hrv = false;
   return chdir(cwd) == 0 ? 0 : 2;
 }

@@ -21,11 +21,15 @@
  *           CEPCell_NEO/cellmodels/ten_tusscher_model_2006_IK1Ko_epi_units.cpp:196)
  *        4: like 2 but the class stores arrays inline (Cellmodel base)
  *   -DREF_INLINE_ARRAYS  the class derives from Cellmodel (arrays inline)
+ *   -DREF_NEO_HRV        adds ref_set_hrv (the CEPCell_NEO ORd's HRV stimulus)
  */
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include REF_HEADER
+#ifdef REF_NEO_HRV
+#include "globals.hpp"
+#endif
 
 /* The reference's cell models print through mpi_printf
  * (DrugSimulation/modules/glob_funct.hpp:16); the oracle silences it. */
@@ -88,5 +92,12 @@ void ref_run(void *h, double *t, double dt, long n_steps, double *v_out, long st
   }
   *t = tc;
 }
+
+#ifdef REF_NEO_HRV
+/* The CEPCell_NEO ORd switches its stimulus to the cumulative-BCL window
+ * when glob_var::is_hrv is set (CEPCell_NEO/cellmodels/Ohara_Rudy_2011.cpp:
+ * 694-695); CONSTANTS[cumm_BCL] (141) is set through ref_consts. */
+void ref_set_hrv(int on) { glob_var::is_hrv = (on != 0); }
+#endif
 
 }  // extern "C"

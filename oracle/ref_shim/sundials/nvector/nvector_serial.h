@@ -14,4 +14,5 @@ typedef struct cep_nvector *N_Vector;
 N_Vector N_VMake_Serial(long length, realtype *data);
 realtype *N_VGetArrayPointer_Serial(N_Vector v);
 void N_VDestroy(N_Vector v);
+void N_VDestroy_Serial(N_Vector v);
 #endif

@@ -100,6 +100,25 @@ int cepo_run_batch(int model, int n, const double *celltype, const double *conc,
                    double *states_out, int n_threads);
 
 /* ------------------------------------------------------------ protocols */
+/* ORd 2011: start of the current pace of the cumulative stimulus
+ * (tissue_stim == 2, the CEPCell_NEO build under hrv_bench). */
+void cepo_ord_set_cumm(cepo_cell *c, double cumm_bcl);
+
+/* HRV pacing, CEPCell_NEO/modules/hrv_bench.cpp:146-343, for one cell (ORd
+ * 2011, the CEPCell_NEO build: quirks 2): one pace per entry of bcls (the
+ * HRV file's values and the trailing 1000 ms the bench appends), the
+ * cumulative stimulus, biomarkers of the steepest of the last 250 paces.
+ * Fixed steps stand for the bench's CVODE calls; every pace after the first
+ * begins with the bench's zero-length call (it rewinds tcurr and tnext by dt
+ * and asks for a time already reached). rec receives the printed record:
+ * rec->bcl the chosen beat's BCL, *steepest its pace. */
+typedef struct {
+  cepo_beat beat;
+  int bcl, steepest_pace;
+} cepo_hrv_record;
+int cepo_hrv_run(const cepo_cell *c, double *y, const double *bcls, int n_bcl, double dt, double dt_write,
+                 int num_pace1, cepo_hrv_record *rec);
+
 /* One recorded pace of a restitution run (apdr_bench.cpp:211). */
 typedef struct {
   int pace, recal;

@@ -38,6 +38,7 @@ typedef struct {
   double h10_i, h11_i, h12_i, k1_i, k2_i, k5_i, Gncx, h10_ss, h11_ss, h12_ss, k1_ss, k2_ss, k5_ss;
   double b1, a2, a4, Pnak;
   double fcafp_dt; /* step used in the fcafp gate: 25 under quirk (1), else dt (0 = use dt) */
+  double cumm_BCL; /* start of the current pace under the cumulative stimulus (hrv_bench) */
 } ord_p;
 
 _Static_assert(sizeof(ord_p) <= CEPO_MAX_PARAMS * sizeof(double), "ord_p too large");
@@ -130,10 +131,18 @@ static double hill_factor(double conc, double ic50, double h) {
   return (ic50 > 10E-14 && h > 10E-14) ? 1. / (1. + pow(conc / ic50, h)) : 1.;
 }
 
+/* quirks: 0 the intended forms; 1 the DrugSimulation build's quirks
+ * (documented in cep_oracle.h); 2 the CEPCell_NEO build
+ * (CEPCell_NEO/cellmodels/Ohara_Rudy_2011.cpp:456-520): celltype kept,
+ * ___applyDutta on the intended constants (GKs, GKr, GK1, PCa, GNaL,
+ * :456-463) but, like the Hill block (:505-520), after ___initConsts has
+ * derived PCap, PCaNa and PCaK from PCa, which therefore stay unscaled. */
 int cepo_ord_init(cepo_cell *c, double celltype, double conc, const double *ic50, int is_dutta,
                   int quirks) {
   ord_p *q = (ord_p *)c->p;
   memset(c->p, 0, sizeof(c->p));
+  const int neo = quirks == 2;
+  if (neo) quirks = 0;
   ord_base_consts(q, quirks ? 0.0 : celltype);
   if (is_dutta) {
     if (quirks) { /* ___applyDutta as written, Ohara_Rudy_2011.cpp:460-467 */
@@ -147,7 +156,7 @@ int cepo_ord_init(cepo_cell *c, double celltype, double conc, const double *ic50
       q->GKr *= 1.013;
       q->GK1 *= 1.698;
       q->PCa *= 1.007;
-      derive_pca(q);
+      if (!neo) derive_pca(q);
       q->GNaL *= 2.661;
     }
   }
@@ -159,7 +168,7 @@ int cepo_ord_init(cepo_cell *c, double celltype, double conc, const double *ic50
     q->GNaL *= hill_factor(conc, ic50[8], ic50[9]);
     q->Gto *= hill_factor(conc, ic50[10], ic50[11]);
     q->GKr *= hill_factor(conc, ic50[12], ic50[13]);
-    if (!quirks) derive_pca(q);
+    if (!quirks && !neo) derive_pca(q);
   }
   q->fcafp_dt = quirks ? 25.0 : 0.0;
   return 0;
@@ -176,6 +185,10 @@ void cepo_ord_set_pacing(cepo_cell *c, double bcl, double stim_start, double sti
   if (stim_dur >= 0) q->duration = stim_dur;
   q->amp *= amp_scale;
 }
+
+/* CONSTANTS[cumm_BCL], the start of the current pace of the cumulative
+ * stimulus (tissue_stim == 2; CEPCell_NEO/cellmodels/Ohara_Rudy_2011.cpp:694-695). */
+void cepo_ord_set_cumm(cepo_cell *c, double cumm_bcl) { ((ord_p *)c->p)->cumm_BCL = cumm_bcl; }
 
 void cepo_ord_pacing(const cepo_cell *c, double *bcl, double *stim_start) {
   const ord_p *q = (const ord_p *)c->p;
@@ -208,7 +221,9 @@ static void ord_compute(const cepo_cell *c, double TIME, const double *S, double
   const ord_p *q = (const ord_p *)c->p;
   const double v = S[V];
   double Istim;
-  if (c->tissue_stim)
+  if (c->tissue_stim == 2)  /* hrv: the pace starts at cumm_BCL (:694-695) */
+    Istim = (q->stim_start + q->cumm_BCL <= TIME && TIME < q->stim_start + q->cumm_BCL + q->duration ? q->amp : 0.0);
+  else if (c->tissue_stim)
     Istim = c->is_s1 ? q->amp : 0.0;
   else
     Istim = (TIME >= q->stim_start && (TIME - q->stim_start) -

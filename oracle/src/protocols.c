@@ -167,3 +167,163 @@ void cepo_clamp(const cepo_cell *c, double *y, const double *v, long n_samples, 
     t += dt;
   }
 }
+
+/* ------------------------------------------------------------- HRV pacing
+ * CEPCell_NEO/modules/hrv_bench.cpp:146-343 for one cell of ORd 2011 (the
+ * CEPCell_NEO build, quirks 2) at one concentration:
+ *  - one pace per entry of bcls: CONSTANTS[BCL] = bcls[k] (:176), the
+ *    integrals reset (:180), iout = 0 .. imax = (int)(BCL / dt) inclusive
+ *    (:181, :191), the stimulus window at cumm_BCL + stim_start
+ *    (Ohara_Rudy_2011.cpp:695), cumm_BCL += BCL after the pace (:331);
+ *  - every pace after the first rewinds tcurr and tnext by dt (:185-188):
+ *    its first call asks CVODE for the time it has already reached, which
+ *    returns the state unchanged; here that call is no step at all, and,
+ *    like every call, it still adds the currents times dt to the integrals;
+ *  - computeRates(tnext) after each call (:196) gives the currents and
+ *    RATES[V] of the sample; the last 250 entries are evaluated (:216-265,
+ *    with the bench's unsigned arithmetic: fewer than 250 entries evaluate
+ *    none), the steepest repolarisation kept (:268-299); the record of pace
+ *    num_pace1 - 249 replaces the selection once (:334-336, the bench
+ *    tests p_param->num_pace1, not the number of entries);
+ *  - afterwards an APD90 below the APD50 becomes the beat's BCL (:352).
+ * The bench leaves t_depol, the repolarisation levels, the Ca amplitudes,
+ * the CaD crossing times and the steepest pace uninitialised until first
+ * set; here they start at 0. The Ca samples of a pace are sorted by time
+ * (a std::multimap in the bench, :209). */
+typedef struct {
+  double t, c;
+  long seq;
+} ca_entry;
+
+static int cmp_ca(const void *a, const void *b) {
+  const ca_entry *x = (const ca_entry *)a, *y = (const ca_entry *)b;
+  if (x->t < y->t) return -1;
+  if (x->t > y->t) return 1;
+  return (x->seq < y->seq) ? -1 : (x->seq > y->seq);
+}
+
+static void beat_reset(cepo_beat *b, double vm, double ca) {  /* cipa_t::init, commons.hpp:88-108 */
+  memset(b, 0, sizeof(*b));
+  b->dvmdt_repol = -999; b->dvmdt_max = -999; b->vm_peak = -999; b->vm_valley = vm; b->vm_dia = -999;
+  b->ca_peak = -999; b->ca_valley = ca; b->ca_dia = -999;
+}
+
+int cepo_hrv_run(const cepo_cell *c0, double *y, const double *bcls, int n_bcl, double dt, double dt_write,
+                 int num_pace1, cepo_hrv_record *rec) {
+  cepo_cell c = *c0;
+  c.tissue_stim = 2;
+  double bcl0, stim_start;
+  cepo_pacing_of(&c, &bcl0, &stim_start);
+  const int print_freq = (int)((1. / dt) * dt_write);
+  const int peak_every = (int)((stim_start + 6.) / dt);
+  const long first_eval = n_bcl >= 250 ? n_bcl - 250 : (long)n_bcl + 1;  /* size_t wrap: none evaluated */
+  double tcurr = 0.0, tnext = dt, t_solver = 0.0, cumm = 0.0;
+  cepo_beat best, temp;
+  beat_reset(&best, y[0], y[9]);
+  beat_reset(&temp, y[0], y[9]);
+  int best_bcl = 0, temp_bcl = 0, steepest = 0;
+  double t_depol = 0, r30 = 0, r50 = 0, r90 = 0, amp50 = 0, amp90 = 0;
+  double c50p = 0, c90p = 0, c50c = 0, c90c = 0;
+  long cap = 4096, n_ca = 0;
+  ca_entry *ca = malloc(sizeof(ca_entry) * cap);
+  int status = 0;
+  for (int pace = 0; pace < n_bcl; ++pace) {
+    const double bcl = bcls[pace];
+    cepo_set_pacing(&c, bcl, -1.0, -1.0, 1.0);
+    cepo_ord_set_cumm(&c, cumm);
+    double qnet = 0, inal = 0, ical = 0;
+    const int imax = (int)(bcl / dt);
+    int peak_found = 0, eligible = 0;
+    double t_ca_peak = tcurr;
+    if (pace > 0) {
+      tcurr -= dt;
+      tnext -= dt;
+    }
+    const int last = pace >= first_eval;
+    if (last) {
+      beat_reset(&temp, y[0], y[9]);
+      n_ca = 0;
+    }
+    for (int iout = 0; iout <= imax;) {
+      const double h = tnext - t_solver;
+      if (h > 0) {
+        cepo_step(&c, t_solver, h, y, NULL);
+        t_solver = tnext;
+      }
+      tcurr = tnext;
+      double dydt[CEPO_MAX_STATES];
+      cepo_currents cur;
+      cepo_rates(&c, tnext, y, dydt, &cur);
+      ++iout;
+      tnext += dt;
+      if (!isfinite(y[0])) status = 1;
+      qnet += (cur.INaL + cur.ICaL + cur.Ito + cur.IKr + cur.IKs + cur.IK1) * dt;
+      inal += cur.INaL * dt;
+      ical += cur.ICaL * dt;
+      if (!last) continue;
+      if (iout % print_freq == 0) {
+        if (n_ca == cap) ca = realloc(ca, sizeof(ca_entry) * (cap *= 2));
+        ca[n_ca].t = tcurr; ca[n_ca].c = y[9]; ca[n_ca].seq = n_ca; ++n_ca;
+      }
+      const double V = y[0], dV = dydt[0];
+      if (temp.dvmdt_max < dV) temp.dvmdt_max = dV;
+      if (iout % peak_every == 0 && !peak_found) {
+        temp.vm_peak = V;
+        t_depol = tcurr;
+        if (temp.vm_peak > 0.) {
+          r30 = temp.vm_peak - (0.3 * (temp.vm_peak - temp.vm_valley));
+          r50 = temp.vm_peak - (0.5 * (temp.vm_peak - temp.vm_valley));
+          r90 = temp.vm_peak - (0.9 * (temp.vm_peak - temp.vm_valley));
+          eligible = 1;
+        }
+        peak_found = 1;
+      } else if (eligible && tcurr > cumm + (stim_start + 6.)) {
+        if (r30 >= V && V >= r90 && temp.dvmdt_repol < dV) temp.dvmdt_repol = dV;
+        if (r50 > V && V > r50 - 2) temp.apd50 = tcurr - t_depol;
+        if (r90 > V && V > r90 - 2) temp.apd90 = tcurr - t_depol;
+        if (temp.ca_peak < y[9]) {
+          temp.ca_peak = y[9];
+          amp50 = temp.ca_peak - (0.5 * (temp.ca_peak - temp.ca_valley));
+          amp90 = temp.ca_peak - (0.9 * (temp.ca_peak - temp.ca_valley));
+          t_ca_peak = tcurr;
+        }
+      }
+    }
+    if (last) {
+      qsort(ca, (size_t)n_ca, sizeof(ca_entry), cmp_ca);
+      for (long k = 0; k < n_ca; ++k) {
+        if (ca[k].t < t_ca_peak) {
+          if (ca[k].c < amp50) c50p = ca[k].t;
+          if (ca[k].c < amp90) c90p = ca[k].t;
+        } else {
+          if (ca[k].c > amp50) c50c = ca[k].t;
+          if (ca[k].c > amp90) c90c = ca[k].t;
+        }
+      }
+      temp.cad50 = c50c - c50p;
+      temp.cad90 = c90c - c90p;
+      temp.qnet = qnet;
+      temp.inal_auc = inal;
+      temp.ical_auc = ical;
+      temp.vm_dia = y[0];
+      temp.ca_dia = y[9];
+      temp_bcl = (int)bcl;
+      if (temp.dvmdt_repol > best.dvmdt_repol) {
+        steepest = pace;
+        best = temp;
+        best_bcl = temp_bcl;
+      }
+    }
+    cumm += bcl;
+    if (pace + 1 == num_pace1 - 249) {
+      best = temp;
+      best_bcl = temp_bcl;
+    }
+  }
+  free(ca);
+  if (best.apd90 < best.apd50) best.apd90 = best_bcl;
+  rec->beat = best;
+  rec->bcl = best_bcl;
+  rec->steepest_pace = steepest;
+  return status;
+}

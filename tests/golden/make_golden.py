@@ -2,7 +2,7 @@
 models compiled from their own sources (oracle/_ref, built by
 `make -C oracle ref` where the reference tree is present).
 
-    python tests/golden/make_golden.py [ord cipa tt2006 tt2004 tomek fem bench]
+    python tests/golden/make_golden.py [ord cipa tt2006 tt2004 tomek fem bench neo hrv]
 
 Each fixture holds the inputs (celltype, concentration, Hill row, flags),
 the reference's V trace sampled every `stride` steps of its explicit loop
@@ -10,7 +10,9 @@ the reference's V trace sampled every `stride` steps of its explicit loop
 RATES at t = 0. fem_elements.npz holds the reference's FEM element
 matrices (fem.cpp set_amat_bmat) of square, hex and tet elements;
 cipa_bench_records.json the records the reference's CiPA drug bench prints
-(cipa_drug_bench.cpp) for the oracle's ORd trajectory. The
+(cipa_drug_bench.cpp) for the oracle's ORd trajectory; neo_ord_*.npz the
+RATES of the CEPCell_NEO ORd build; hrv_bench_records.json the records of
+the reference's HRV bench (hrv_bench.cpp). The
 oracle and the GPU path are checked against these files on machines where
 the reference itself is not available.
 """
@@ -233,10 +235,84 @@ def make_bench():
     print("wrote cipa_bench_records")
 
 
+NEO_CASES = [dict(celltype=0.0, dutta=True, conc=1.5), dict(celltype=1.0, dutta=True, conc=0.7),
+             dict(celltype=2.0, dutta=False, conc=3.0)]
+NEO_HILL = [5.0, 1.0, 20.0, 1.1, 30.0, 0.9, 8.0, 1.2, 4.0, 0.8, 15.0, 1.0, 0.6, 1.1]
+
+
+def make_ord_neo(dt: float = 0.005, n_steps: int = 60000, every: int = 1000):
+    """RATES of the CEPCell_NEO build of ORd 2011 (compiled from its own
+    sources, HRV stimulus on) at states along the oracle's trajectory, the
+    stimulus window moved to cumm_BCL = 150 ms halfway."""
+    import ctypes
+    for k, c in enumerate(NEO_CASES):
+        r = O.RefCell("ord2011_neo", c["celltype"], c["conc"], np.array(NEO_HILL), is_dutta=c["dutta"])
+        r.L.ref_set_hrv.argtypes = [ctypes.c_int]
+        r.L.ref_set_hrv(1)
+        cell = O.Cell("ord2011", c["celltype"], c["conc"], np.array(NEO_HILL), is_dutta=c["dutta"], quirks=2)
+        cell.c.tissue_stim = 2
+        t, cumm = 0.0, 0.0
+        times, cumms, states, rates = [], [], [], []
+        for i in range(n_steps):
+            if i == n_steps // 2:
+                cumm = 150.0
+            if i % every == 0:
+                r.states[:] = cell.states
+                r.consts[141] = cumm
+                r.L.ref_compute_rates(r.h, t)
+                times.append(t); cumms.append(cumm); states.append(cell.states.copy())
+                rates.append(r.arr("rates", r.n).copy())
+            O.lib().cepo_ord_set_cumm(ctypes.byref(cell.c), cumm)
+            cell.step(t, dt)
+            t += dt
+        np.savez_compressed(OUT / f"neo_ord_{k}.npz", hill=np.array(NEO_HILL), dt=dt, times=np.array(times),
+                            cumm=np.array(cumms), states=np.array(states), ref_rates=np.array(rates), **c)
+        print("wrote", f"neo_ord_{k}")
+
+
+HRV_CASE = dict(celltype=0.0, dt=0.02, dt_write=1.0, concs=[1.5], hill=NEO_HILL, n_bcl=259, seed=3)
+
+
+def hrv_bcls(case=HRV_CASE) -> list[float]:
+    """The HRV file's intervals: a seeded slow oscillation with noise (ms,
+    one decimal), n_bcl of them."""
+    rng = np.random.default_rng(case["seed"])
+    n = case["n_bcl"]
+    return [float(x) for x in np.round(600 + 80 * np.sin(np.arange(n) / 7.0) + rng.normal(0, 20, n), 1)]
+
+
+def make_hrv():
+    """The reference's HRV bench (hrv_bench.cpp compiled from its sources
+    over the oracle's ORd, CEPCell_NEO build) on HRV_CASE: its printed
+    records as text."""
+    import ctypes
+    import json
+    import tempfile
+    c = HRV_CASE
+    L = ctypes.CDLL(str(O.REF_DIR / O.REF_LIBS["bench"]))
+    L.ref_hrv_bench.argtypes = [ctypes.c_char_p] * 5 + [ctypes.c_double] * 3 + [ctypes.c_int]
+    bcls = hrv_bcls()
+    with tempfile.TemporaryDirectory() as wd:
+        w = Path(wd)
+        (w / "result").mkdir()
+        (w / "hrv.txt").write_text("".join(f"{b}\n" for b in bcls))
+        (w / "hill.csv").write_text("header\n" + ",".join(repr(x) for x in c["hill"]) + "\n")
+        concs = "0," + ",".join(repr(x) for x in c["concs"])
+        rc = L.ref_hrv_bench(str(w).encode(), str(w / "hill.csv").encode(), str(w / "hrv.txt").encode(),
+                             concs.encode(), b"hrv", c["celltype"], c["dt"], c["dt_write"], len(bcls) + 1)
+        assert rc == 0
+        rec = {}
+        for f in sorted((w / "result").glob("*/*.plt")):
+            kind = "ap" if "ap_profile" in f.name else "ca" if "ca_profile" in f.name else "qni"
+            rec.setdefault(f.parent.name, {})[kind] = [ln.split() for ln in f.read_text().strip().splitlines()[1:]]
+    (OUT / "hrv_bench_records.json").write_text(json.dumps(dict(case=c, bcls=bcls, records=rec), indent=1))
+    print("wrote hrv_bench_records")
+
+
 if __name__ == "__main__":
     if not O.ref_available("ord2011"):
         sys.exit("reference models not built: run `make -C oracle ref` where the reference tree exists")
-    which = set(sys.argv[1:]) or {"ord", "cipa", "tt2006", "tt2004", "tomek", "fem", "bench"}
+    which = set(sys.argv[1:]) or {"ord", "cipa", "tt2006", "tt2004", "tomek", "fem", "bench", "neo", "hrv"}
     if "ord" in which:
         make_ord()
     if "cipa" in which:
@@ -251,3 +327,7 @@ if __name__ == "__main__":
         make_fem()
     if "bench" in which:
         make_bench()
+    if "neo" in which:
+        make_ord_neo()
+    if "hrv" in which:
+        make_hrv()

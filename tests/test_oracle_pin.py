@@ -353,3 +353,60 @@ def test_biomarker_machine_matches_reference_bench(oracle):
                           _c_float(r["cad50"]), _c_float(r["cad90"] - r["cad50"]), str(r["steepest_pace"])], (key, i)
             qin = 0.0 if conc == 0.0 else 0.5 * (r["inal_auc"] / ctrl["inal_auc"] + r["ical_auc"] / ctrl["ical_auc"])
             assert qni == [str(i), _c_float(r["qnet"] / 1000.0), _c_float(qin)], (key, i, qni)
+
+
+# ------------------------------------------------ CEPCell_NEO ORd, HRV bench
+NEO_CASES = sorted(GOLD.glob("neo_ord_*.npz"))
+
+
+@pytest.mark.parametrize("path", NEO_CASES, ids=lambda p: p.stem)
+def test_ord_neo_rates_match_reference_golden(oracle, path):
+    """The oracle's CEPCell_NEO ORd 2011 variant (quirks 2: celltype kept,
+    Dutta on the intended constants, PCa-derived permeabilities not rescaled,
+    the HRV stimulus window at cumm_BCL) gives, bit for bit, the RATES of the
+    reference's CEPCell_NEO build compiled from its sources."""
+    import ctypes
+    g = np.load(path)
+    c = oracle.Cell("ord2011", float(g["celltype"]), float(g["conc"]), g["hill"], is_dutta=bool(g["dutta"]),
+                    quirks=2)
+    c.c.tissue_stim = 2
+    for t, cumm, y, r in zip(g["times"], g["cumm"], g["states"], g["ref_rates"]):
+        c.y[:41] = y
+        oracle.lib().cepo_ord_set_cumm(ctypes.byref(c.c), float(cumm))
+        ro, _ = c.rates(float(t))
+        assert np.array_equal(ro, r), (float(t), np.flatnonzero(ro != r))
+
+
+def test_hrv_bench_matches_reference(oracle):
+    """The oracle's restatement of the HRV bench prints exactly what the
+    reference's hrv_bench.cpp (compiled from its sources over the oracle's
+    CEPCell_NEO ORd) prints: every field of ap_profile (BCL of the chosen
+    beat included), ca_profile and qni, for a control and a drug, over 259
+    intervals plus the appended 1000 ms, with the zero-length first call of
+    every pace."""
+    import json
+    import threading
+    g = json.loads((GOLD / "hrv_bench_records.json").read_text())
+    c, bcls, rec = g["case"], g["bcls"] + [1000.0], g["records"]
+    concs = [0.0] + list(c["concs"])
+    res = {}
+
+    def work(conc):
+        cell = oracle.Cell("ord2011", c["celltype"], conc, np.array(c["hill"]), is_dutta=True, quirks=2)
+        res[conc] = cell.hrv(bcls, c["dt"], c["dt_write"])
+
+    th = [threading.Thread(target=work, args=(x,)) for x in concs]
+    [t.start() for t in th]
+    [t.join() for t in th]
+    ctrl = res[0.0]
+    for conc in concs:
+        r = res[conc]
+        key = f"{conc:.2f}"
+        assert rec[key]["ap"][0] == ["0", _c_float(r["dvmdt_repol"]), _c_float(r["dvmdt_max"]), _c_float(r["vm_peak"]),
+                                     _c_float(r["vm_dia"]), _c_float(r["apd90"]), _c_float(r["apd50"]),
+                                     _c_float(r["apd90"] - r["apd50"]), str(r["steepest_pace"]), str(r["bcl"])], key
+        assert rec[key]["ca"][0] == ["0", _c_float(r["ca_peak"]), _c_float(r["ca_dia"]), _c_float(r["cad90"]),
+                                     _c_float(r["cad50"]), _c_float(r["cad90"] - r["cad50"]),
+                                     str(r["steepest_pace"])], key
+        qin = 0.0 if conc == 0.0 else 0.5 * (r["inal_auc"] / ctrl["inal_auc"] + r["ical_auc"] / ctrl["ical_auc"])
+        assert rec[key]["qni"][0] == ["0", _c_float(r["qnet"] / 1000.0), _c_float(qin)], key
