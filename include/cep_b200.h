@@ -102,9 +102,10 @@ int cep_batch_size(cep_batch_t b, int *n, int *n_states);
  * spreads small populations over every SM. Used by the autotuner. */
 int cep_batch_set_block(cep_batch_t b, int threads_per_block);
 /* Kernel form: one thread per cell; 4 warps per 32 cells each evaluating
- * one group of channels; or 2 warps per 32 cells with two groups each (the
- * default for populations smaller than ~1.5 waves of the GPU; ORd family
- * only). */
+ * one group of channels; or 2 warps per 32 cells with two groups each (ORd
+ * family only). Defaults for populations below ~1.5 waves of the GPU: FP64
+ * the 4 roles; mixed the 4 roles up to one 32-cell group per SM and the
+ * pairs above; larger populations one thread per cell. */
 #define CEP_KERNEL_CELL 0
 #define CEP_KERNEL_ROLES 1
 #define CEP_KERNEL_PAIRS 2 /* 2 warps per 32 cells, two channel groups each */
