@@ -26,7 +26,7 @@ INST_RUNNING, INST_DONE, INST_NONFINITE, INST_IDLE = 0, 1, 2, 3
 MODELS = {"ord2011": 0, "cipa2017": 1, "tt2006": 2, "tt2004": 3, "tomek2019": 4}
 N_STATES = {"ord2011": 41, "cipa2017": 49, "tt2006": 19, "tt2004": 17, "tomek2019": 43}
 PREC = {"fp64": 0, "mixed": 1}
-FLAG_DUTTA, FLAG_QUIRKS, FLAG_TT04_MCELL = 1, 2, 4
+FLAG_DUTTA, FLAG_QUIRKS, FLAG_TT04_MCELL, FLAG_NEO_ORD = 1, 2, 4, 8
 CURRENTS = ("INa", "INaL", "Ito", "ICaL", "IKr", "IKs", "IK1")
 APDR_FIELDS = ("pace", "recal", "bcl", "apd90", "di", "t")
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
@@ -44,6 +44,10 @@ class Biomarkers(ctypes.Structure):
     _fields_ = [(f, ctypes.c_double) for f in BM_FIELDS] + [
         ("steepest_pace", ctypes.c_int32), ("n_eligible", ctypes.c_int32), ("status", ctypes.c_int32),
         ("reserved", ctypes.c_int32)]
+
+
+class HrvRecord(ctypes.Structure):
+    _fields_ = [("beat", Biomarkers), ("bcl", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class CepJob(ctypes.Structure):
@@ -145,6 +149,8 @@ _SIGS = {
                                              ctypes.POINTER(ctypes.c_int)]),
     "cep_batch_clamp": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int, _dp]),
+    "cep_batch_hrv": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                     ctypes.c_long, ctypes.c_void_p]),
     "cep_batch_reserve_biomarkers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                     ctypes.c_double]),
     "cep_batch_init_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int,
@@ -293,7 +299,9 @@ class Batch:
         self.close()
 
     def init(self, celltype=None, conc=None, hill=None, dutta: bool = False, quirks: bool = True,
-             mcell: bool = False) -> "Batch":
+             mcell: bool = False, neo: bool = False) -> "Batch":
+        """neo (ORd 2011) selects the CEPCell_NEO build the HRV bench drives,
+        in place of the quirks / intended choice."""
         ct = None if celltype is None else np.ascontiguousarray(np.broadcast_to(celltype, (self.n,)), np.float64)
         cc = None if conc is None else np.ascontiguousarray(np.broadcast_to(conc, (self.n,)), np.float64)
         hh = None
@@ -304,7 +312,8 @@ class Batch:
                 hh = np.broadcast_to(hh, (self.n, hh.shape[0]))
             hh = np.ascontiguousarray(hh)
             stride = hh.shape[1]
-        flags = (FLAG_DUTTA if dutta else 0) | (FLAG_QUIRKS if quirks else 0) | (FLAG_TT04_MCELL if mcell else 0)
+        flags = (FLAG_DUTTA if dutta else 0) | (FLAG_QUIRKS if quirks and not neo else 0) | \
+            (FLAG_TT04_MCELL if mcell else 0) | (FLAG_NEO_ORD if neo else 0)
         _check(lib().cep_batch_init(self._h, _dptr(ct), _dptr(cc), _dptr(hh), stride, flags))
         return self
 
@@ -451,6 +460,26 @@ class Batch:
             raise CepError(ERR_STATE, f"restitution produced {cnt.value} records per instance, expected {m}")
         raw = np.ctypeslib.as_array(arr)[: self.n * m].reshape(self.n, m)
         return {f: np.array(raw[f]) for f in APDR_FIELDS}
+
+    def hrv(self, bcls, dt: float, dt_write: float = 1.0, num_pace1: int | None = None,
+            steps_per_launch: int = 0) -> dict[str, np.ndarray]:
+        """Heart-rate-variability pacing (CEPCell_NEO/modules/hrv_bench.cpp:
+        146-343): one pace per entry of bcls (the bench appends 1000 ms to its
+        interval file), the last 250 paces evaluated. Returns the printed
+        beat of every instance keyed like biomarkers(), plus "bcl", the BCL
+        printed with it. num_pace1 defaults to len(bcls)."""
+        b = np.ascontiguousarray(bcls, np.float64)
+        arr = (HrvRecord * self.n)()
+        np1 = len(b) if num_pace1 is None else int(num_pace1)
+        _check(lib().cep_batch_hrv(self._h, _dptr(b), len(b), float(dt), float(dt_write), np1,
+                                   int(steps_per_launch), arr))
+        raw = np.ctypeslib.as_array(arr)
+        beat = raw["beat"]
+        out = {f: np.array(beat[f]) for f in BM_FIELDS}
+        for f in ("steepest_pace", "n_eligible", "status"):
+            out[f] = np.array(beat[f])
+        out["bcl"] = np.array(raw["bcl"])
+        return out
 
     def clamp(self, v, t0: float, dt: float, current: str | int) -> np.ndarray:
         """Voltage-clamp replay (CEPPatch/benchpatch.cpp:83-100): V of every

@@ -31,6 +31,7 @@
 #include "model_tt2006.cuh"
 #include "model_tt2004.cuh"
 #include "model_tomek.cuh"
+#include "hrv.cuh"
 #include "internal.h"
 
 namespace {
@@ -99,7 +100,8 @@ struct OrdModel {
   }
   __device__ static void init(double *par, double *s, int64_t ld, int64_t i, double ct, double conc,
                               const double *hill, unsigned flags) {
-    ord::init_instance(par, s, ld, i, ct, conc, hill, flags & CEP_FLAG_DUTTA, flags & CEP_FLAG_QUIRKS);
+    ord::init_instance(par, s, ld, i, ct, conc, hill, flags & CEP_FLAG_DUTTA, flags & CEP_FLAG_QUIRKS,
+                       flags & CEP_FLAG_NEO_ORD);
   }
   template <class G>
   __device__ static double cai_of(const Y<G> &y) { return y.cai; }
@@ -442,22 +444,6 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
       a.status[i] = st;
     }
   }
-}
-
-// The role of a warp follows the SM sub-partition (SMSP) it was placed on
-// (the warp slot modulo 4) whenever the block's four warps sit on four
-// different SMSPs, so every SMSP streams one role's instructions and its
-// instruction cache holds a quarter of the step's code; otherwise the warp
-// index decides.
-__device__ __forceinline__ int pick_role() {
-  __shared__ int slot[4];
-  const int w = threadIdx.x >> 5;
-  unsigned wid;
-  asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
-  if ((threadIdx.x & 31) == 0) slot[w] = (int)(wid & 3u);
-  __syncthreads();
-  const int m = (1 << slot[0]) | (1 << slot[1]) | (1 << slot[2]) | (1 << slot[3]);
-  return m == 0xF ? slot[w] : w;
 }
 
 template <class M, class P>
@@ -1633,6 +1619,10 @@ int cep_batch_init_range(cep_batch_t b, int first, int count, const double *cell
   int rc = check_range(b, first, count);
   if (rc) return rc;
   if (hill && hill_stride < 14) return fail(CEP_ERR_ARG, "hill_stride must be >= 14 (got %d)", hill_stride);
+  if ((flags & CEP_FLAG_NEO_ORD) && b->model != CEP_MODEL_ORD2011)
+    return fail(CEP_ERR_UNSUPPORTED, "CEP_FLAG_NEO_ORD selects a build of ORd 2011 only");
+  if ((flags & CEP_FLAG_NEO_ORD) && (flags & CEP_FLAG_QUIRKS))
+    return fail(CEP_ERR_ARG, "CEP_FLAG_NEO_ORD and CEP_FLAG_QUIRKS name two different builds");
   if (conc)
     for (int k = 0; k < count; ++k)
       if (!(conc[k] >= 0.0) || !std::isfinite(conc[k]))
@@ -1884,6 +1874,83 @@ int cep_batch_clamp(cep_batch_t b, const double *v, long n_samples, double t0, d
     CEP_CUDA(cudaStreamSynchronize(b->stream));  // dv is reused by the next chunk
     for (int k = 0; k < m; ++k) t += dt;          // the kernel's clock, same additions
   }
+  return CEP_OK;
+}
+
+int cep_batch_hrv(cep_batch_t b, const double *bcls, int n_bcl, double dt, double dt_write, int num_pace1,
+                  long steps_per_launch, cep_hrv_record_t *out) {
+  if (!b) return fail(CEP_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(CEP_ERR_STATE, "cep_batch_init must come first");
+  if (b->model != CEP_MODEL_ORD2011) return fail(CEP_ERR_UNSUPPORTED, "the HRV bench drives ORd 2011 only");
+  if (!bcls || n_bcl <= 0) return fail(CEP_ERR_ARG, "bcl list is empty");
+  if (!out) return fail(CEP_ERR_ARG, "null record buffer");
+  if (!(dt > 0) || !std::isfinite(dt) || !(dt_write > 0) || !std::isfinite(dt_write))
+    return fail(CEP_ERR_ARG, "dt and dt_write must be positive");
+  if (int rc_dt = check_mixed_dt(b, dt)) return rc_dt;
+  const double pf = (1. / dt) * dt_write;  // hrv_bench.cpp:140
+  if (!(pf >= 1.0) || pf > 2.0e9) return fail(CEP_ERR_ARG, "dt_write must be at least dt");
+  const int print_freq = (int)pf;
+  if (steps_per_launch <= 0) steps_per_launch = 20000;
+  if (steps_per_launch > (1L << 30)) steps_per_launch = 1L << 30;
+  // the last 250 paces are evaluated; fewer than 250 paces evaluate none
+  // (the bench's size_t subtraction wraps, :244)
+  const long first_eval = n_bcl >= 250 ? (long)n_bcl - 250 : (long)n_bcl + 1;
+  std::vector<int> imax(n_bcl);
+  long cap = 1;
+  for (int k = 0; k < n_bcl; ++k) {
+    if (!(bcls[k] > 0) || !std::isfinite(bcls[k])) return fail(CEP_ERR_ARG, "bcls[%d] must be positive", k);
+    const double steps = bcls[k] / dt;
+    if (steps > 2.0e9) return fail(CEP_ERR_ARG, "bcls[%d]/dt out of range", k);
+    imax[k] = (int)steps;  // :223
+    if (k >= first_eval) cap = std::max(cap, ((long)imax[k] + 1) / print_freq + 1);
+  }
+  Scratch sc;
+  hrv::Args a{};
+  a.y = b->states; a.par = b->params; a.ld = b->ld; a.n = b->n; a.dt = dt; a.print_freq = print_freq;
+  a.max_evals = (int)steps_per_launch;
+  a.n_eligible = n_bcl >= 250 ? 250 : 0;
+  int rc;
+  if ((rc = sc.get(&a.v.f, (size_t)hrv::kNumF * b->ld))) return rc;
+  if ((rc = sc.get(&a.v.fi, (size_t)hrv::kNumI * b->ld))) return rc;
+  if ((rc = sc.get(&a.v.ca_t, (size_t)cap * b->ld))) return rc;
+  if ((rc = sc.get(&a.v.ca_v, (size_t)cap * b->ld))) return rc;
+  a.v.ca_cap = (int)cap;
+  a.v.ld = b->ld;
+  cep_hrv_record_t *d_out = nullptr;
+  if ((rc = sc.get(&d_out, (size_t)b->n))) return rc;
+  const int grid = (b->n + 127) / 128, grid32 = (b->n + 31) / 32;
+  const bool mixed = b->precision == CEP_PREC_MIXED;
+  hrv::init_kernel<<<grid, 128, 0, b->stream>>>(a);
+  CEP_CUDA(cudaGetLastError());
+  double cumm = 0.0;  // CONSTANTS[cumm_BCL] (:330)
+  for (int p = 0; p < n_bcl; ++p) {
+    a.bcl = bcls[p]; a.cumm = cumm; a.imax = imax[p]; a.pace = p;
+    a.last = p >= first_eval ? 1 : 0;
+    a.replace = (p + 1 == num_pace1 - 249) ? 1 : 0;
+    hrv::pace_begin_kernel<<<grid, 128, 0, b->stream>>>(a);
+    // evaluations of a pace: one per call (imax + 1) plus at most two of a
+    // sample alone (the rewound first call, the last call)
+    const long evals = (long)imax[p] + 3;
+    for (long done = 0; done < evals; done += steps_per_launch) {
+      if (b->variant == CEP_KERNEL_ROLES) {
+        if (mixed) hrv::calls_roles_kernel<Mixed><<<grid32, 128, 0, b->stream>>>(a);
+        else hrv::calls_roles_kernel<F64><<<grid32, 128, 0, b->stream>>>(a);
+      } else if (b->variant == CEP_KERNEL_PAIRS) {
+        if (mixed) hrv::calls_pairs_kernel<Mixed><<<grid32, 64, 0, b->stream>>>(a);
+        else hrv::calls_pairs_kernel<F64><<<grid32, 64, 0, b->stream>>>(a);
+      } else {
+        if (mixed) hrv::calls_kernel<Mixed><<<grid, 128, 0, b->stream>>>(a);
+        else hrv::calls_kernel<F64><<<grid, 128, 0, b->stream>>>(a);
+      }
+    }
+    hrv::pace_end_kernel<<<grid, 128, 0, b->stream>>>(a);
+    CEP_CUDA(cudaGetLastError());
+    cumm += bcls[p];
+  }
+  hrv::collect_kernel<<<grid, 128, 0, b->stream>>>(a, d_out);
+  CEP_CUDA(cudaGetLastError());
+  CEP_CUDA(cudaMemcpyAsync(out, d_out, sizeof(cep_hrv_record_t) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  CEP_CUDA(cudaStreamSynchronize(b->stream));
   return CEP_OK;
 }
 

@@ -298,4 +298,20 @@ struct BeatRec {
       apd50, ca_peak, ca_valley, ca_dia, cad90, cad50;
 };
 
+// The role of a warp follows the SM sub-partition (SMSP) it was placed on
+// (the warp slot modulo 4) whenever the block's four warps sit on four
+// different SMSPs, so every SMSP streams one role's instructions and its
+// instruction cache holds a quarter of the step's code; otherwise the warp
+// index decides.
+__device__ __forceinline__ int pick_role() {
+  __shared__ int slot[4];
+  const int w = threadIdx.x >> 5;
+  unsigned wid;
+  asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
+  if ((threadIdx.x & 31) == 0) slot[w] = (int)(wid & 3u);
+  __syncthreads();
+  const int m = (1 << slot[0]) | (1 << slot[1]) | (1 << slot[2]) | (1 << slot[3]);
+  return m == 0xF ? slot[w] : w;
+}
+
 }  // namespace cep

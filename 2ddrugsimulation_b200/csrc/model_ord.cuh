@@ -909,10 +909,16 @@ __device__ __forceinline__ double hill_factor(double conc, double ic50, double h
 // block, and the model's initial STATES. `quirks` reproduces the reference's
 // documented quirks (celltype forced to endo, the mis-indexed Dutta scaling,
 // the drug block of PCa not reaching the derived permeabilities, and the
-// STATES enum value d = 25 used as the fcafp step).
+// STATES enum value d = 25 used as the fcafp step). `neo` is the
+// CEPCell_NEO build of the model (CEPCell_NEO/cellmodels/Ohara_Rudy_2011.cpp:
+// 456-520): celltype honoured, ___applyDutta on the intended constants and
+// the Hill block both applied after ___initConsts has derived PCap, PCaNa
+// and PCaK from PCa, which therefore stay unscaled; fcafp steps normally.
 __device__ __forceinline__ void init_instance(double *__restrict__ par, double *__restrict__ s, int64_t ld,
                                               int64_t i, double celltype_in, double conc,
-                                              const double *__restrict__ hill, bool dutta, bool quirks) {
+                                              const double *__restrict__ hill, bool dutta, bool quirks,
+                                              bool neo = false) {
+  if (neo) quirks = false;
   const double ct = quirks ? 0.0 : celltype_in;
   double GNaL = ct == 1.0 ? 0.0075 * 0.6 : 0.0075;
   double Gto = ct == 1.0 ? 0.02 * 4.0 : ct == 2.0 ? 0.02 * 4.0 : 0.02;
@@ -934,8 +940,10 @@ __device__ __forceinline__ void init_instance(double *__restrict__ par, double *
       Aff *= 1.870; GNaL *= 1.013; tjca *= 1.698; H *= 1.007;
     } else {
       GKs *= 1.870; GKr *= 1.013; GK1 *= 1.698; PCa *= 1.007; GNaL *= 2.661;
-      PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
-      PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
+      if (!neo) {
+        PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
+        PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
+      }
     }
   }
   if (hill) {
@@ -946,7 +954,7 @@ __device__ __forceinline__ void init_instance(double *__restrict__ par, double *
     GNaL *= hill_factor(conc, hill[8], hill[9]);
     Gto *= hill_factor(conc, hill[10], hill[11]);
     GKr *= hill_factor(conc, hill[12], hill[13]);
-    if (!quirks) {
+    if (!quirks && !neo) {
       PCap = 1.1 * PCa; PCaNa = 0.00125 * PCa; PCaK = 0.0003574 * PCa;
       PCaNap = 0.00125 * PCap; PCaKp = 0.0003574 * PCap;
     }

@@ -1180,7 +1180,8 @@ def main():
                          f"thread ({secs:.1f} s)"}
     mixed, fp64 = res["mixed"], res["fp64"]
     fl = flops_per_step(model)
-    cell_steps_launch = n * args.seg * beat_launches(args)  # per bench step (kernel_ms is per bench step)
+    steps_per_bench_step = args.seg * beat_launches(args)  # time steps every instance takes per bench step
+    cell_steps_launch = n * steps_per_bench_step  # per bench step (kernel_ms is per bench step)
 
     def roof(kernel_ms, peak_key, label, per_step=fl, source="bench.py FMA probe on this GPU (2 flop/FMA)"):
         ach = per_step * cell_steps_launch / (kernel_ms * 1e-3) / 1e12
@@ -1201,6 +1202,8 @@ def main():
         "config": config_of(args, model, n, world),
         "compliant": {k: comp[k] for k in ("n_candidates", "candidate_fraction", "refine_above_vm",
                                            "kernel_ms_mixed", "kernel_ms_fp64_candidates", "clocks")} | {
+            "us_per_step_fp64_candidates": comp["kernel_ms_fp64_candidates"] * 1e3 / steps_per_bench_step,
+            "us_per_step_mixed": comp["kernel_ms_mixed"] * 1e3 / steps_per_bench_step,
             "what": "value = the mixed population (stream 1) with the instances whose diastolic Vm after the "
                     "screening beat stays above refine_above_vm in FP64 (stream 2), one beat of both per step: "
                     "the path whose records meet APD90 <= 0.1 ms against FP64 for every instance"},
@@ -1208,6 +1211,7 @@ def main():
                         "note": "mixed precision for every instance, no FP64 refinement (misses the APD90 bar "
                                 "for non-repolarising instances)"},
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"], "kernel_ms": fp64["kernel_ms"],
+                 "us_per_step": fp64["kernel_ms"] * 1e3 / steps_per_bench_step,
                  "roofline": roof(fp64["kernel_ms"], "fp64_tflops", "fp64"), "clocks": fp64["clocks"]},
         "mixed_over_fp64": comp["value"] / fp64["value"],
         "mixed_plain_over_fp64": mixed["value"] / fp64["value"],

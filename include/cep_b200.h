@@ -58,6 +58,11 @@ extern "C" {
 #define CEP_FLAG_TT04_MCELL 4u /* TT2004: the 2004_a build (g_Ks 0.062, M cell) instead of
                                   2004_b (g_Ks 0.245): tentusscher_noble_noble_panfilov_2004_a.cpp:265,
                                   chosen by celltype 0 in apdr_bench.cpp:77-84 */
+#define CEP_FLAG_NEO_ORD 8u /* ORd 2011: the CEPCell_NEO build driven by the HRV bench
+                               (CEPCell_NEO/cellmodels/Ohara_Rudy_2011.cpp:456-520):
+                               celltype honoured, Dutta on the intended constants and
+                               the Hill block after PCap/PCaNa/PCaK were derived, so
+                               those stay unscaled. Not with CEP_FLAG_QUIRKS. */
 
 /* state array layouts for set/get */
 #define CEP_LAYOUT_SOA 0 /* states[k * n + i] (k = state index, i = instance) */
@@ -299,6 +304,32 @@ int cep_batch_restitution(cep_batch_t b, const double *bcl, int n_bcl, int n_pac
  * touched. Blocking. */
 int cep_batch_clamp(cep_batch_t b, const double *v, long n_samples, double t0, double dt, int current,
                     double *out);
+
+/* The HRV bench's result for one instance: the beat it prints (qnet in the
+ * printed unit, integral / 1000; steepest_pace = the pace it came from;
+ * status CEP_INST_DONE or CEP_INST_NONFINITE) and that beat's BCL as the
+ * bench prints it, (int)BCL. */
+typedef struct {
+  cep_biomarkers_t beat;
+  int32_t bcl;
+  int32_t reserved;
+} cep_hrv_record_t;
+
+/* Heart-rate-variability pacing (CEPCell_NEO/modules/hrv_bench.cpp:
+ * 146-343, the CVODE integration replaced by the fixed-step scheme):
+ * pace p lasts bcls[p] ms (the bench's interval file with 1000 ms
+ * appended), the stimulus starts stim_start after the cumulative start of
+ * the pace (CONSTANTS[cumm_BCL], Ohara_Rudy_2011.cpp:694-695), the clock
+ * carries over between paces with the bench's one-step rewind at each
+ * pace start (a zero-length first call), and the CiPA biomarkers of the
+ * last 250 paces are evaluated (none when n_bcl < 250, as the bench's
+ * size_t arithmetic gives); the beat with the steepest repolarisation is
+ * kept, the beat of pace num_pace1 - 250 replaces it once, and APD90 <
+ * APD50 reports APD90 = BCL. ORd 2011 batches only (the model the bench
+ * drives; CEP_FLAG_NEO_ORD at init gives its build). The instances' states
+ * advance. out[n]. steps_per_launch <= 0 picks 20,000. Blocking. */
+int cep_batch_hrv(cep_batch_t b, const double *bcls, int n_bcl, double dt, double dt_write, int num_pace1,
+                  long steps_per_launch, cep_hrv_record_t *out);
 
 /* ---------------------------------------------------- instance ranges */
 /* Heterogeneous batches: a batch used as a pool of slots whose ranges hold
