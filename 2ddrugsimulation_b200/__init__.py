@@ -224,6 +224,36 @@ _SIGS = {
                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long)]),
     "cep_tissue_stats": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_long), _ip]),
+    # slab parts (slab.py)
+    "cep_part_split": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int)]),
+    "cep_part_create_grid": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "cep_part_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "cep_part_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long),
+                                     ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]),
+    "cep_part_get_csr": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "cep_part_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "cep_part_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cep_part_cg_begin": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    "cep_part_cg_direction": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_void_p]),
+    "cep_part_cg_product": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
+    "cep_part_cg_update": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p]),
+    "cep_part_cg_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "cep_part_cg_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]),
+    "cep_part_bind_cells": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]),
+    "cep_part_ionic_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "cep_part_get_activation": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
 }
 
 

@@ -194,17 +194,22 @@ struct GridArgs {
   int *ecol;        // ELL [width][ld]
   double *ea, *eb;
   double *dinv;
+  // A row range of the grid (a slab part): rows row0 .. row0 + n_rows - 1
+  // (n_rows 0: every row), stored at local index row - row0 with columns
+  // shifted by -col_off; D holds elements e_off onwards.
+  int64_t row0, n_rows, col_off, e_off;
 };
 
 __global__ void assemble_grid_kernel(GridArgs g) {
-  const int64_t n = (int64_t)g.nx * g.ny * g.nz;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int64_t n = g.n_rows > 0 ? g.n_rows : (int64_t)g.nx * g.ny * g.nz;
+  const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= n) return;
+  const int64_t i = g.row0 + li;  // global row
   const int ix = (int)(i % g.nx);
   const int iy = (int)((i / g.nx) % g.ny);
   const int iz = (int)(i / ((int64_t)g.nx * g.ny));
   const int ex_n = g.nx - 1, ey_n = g.ny - 1, ez_n = g.dim == 3 ? g.nz - 1 : 1;
-  int64_t q = g.rp[i];
+  int64_t q = g.rp[li];
   int slot = 0;
   double diag = 1.0;
   const int dk0 = g.dim == 3 ? -1 : 0, dk1 = g.dim == 3 ? 1 : 0;
@@ -223,31 +228,32 @@ __global__ void assemble_grid_kernel(GridArgs g) {
           for (int ey = y_lo; ey <= y_hi; ++ey)
             for (int ex = x_lo; ex <= x_hi; ++ex) {
               const int64_t e = (int64_t)ex + (int64_t)ex_n * ((int64_t)ey + (int64_t)ey_n * ez);
+              const double *De = g.D + (e - g.e_off) * g.n_d;
               double Dm[3][3];
-              tensor_of(g.dim, g.D + e * g.n_d, g.n_d, Dm);
+              tensor_of(g.dim, De, g.n_d, Dm);
               const int la = local_index(ix - ex, iy - ey, g.dim == 3 ? iz - ez : 0);
               const int lb = local_index(jx - ex, jy - ey, g.dim == 3 ? jz - ez : 0);
               double ae, be;
-              element_entry(g.dim, g.h, g.dt, g.D + e * g.n_d, g.n_d, Dm, la, lb, ae, be);
+              element_entry(g.dim, g.h, g.dt, De, g.n_d, Dm, la, lb, ae, be);
               av += ae;
               bv += be;
             }
-        g.col[q] = (int)j;
+        g.col[q] = (int)(j - g.col_off);
         g.a[q] = av;
         g.b[q] = bv;
         ++q;
-        g.ecol[(int64_t)slot * g.ld + i] = (int)j;
-        g.ea[(int64_t)slot * g.ld + i] = av;
-        g.eb[(int64_t)slot * g.ld + i] = bv;
+        g.ecol[(int64_t)slot * g.ld + li] = (int)(j - g.col_off);
+        g.ea[(int64_t)slot * g.ld + li] = av;
+        g.eb[(int64_t)slot * g.ld + li] = bv;
         ++slot;
         if (j == i) diag = av;
       }
   for (; slot < g.width; ++slot) {  // padding: the row's own column with zero weight
-    g.ecol[(int64_t)slot * g.ld + i] = (int)i;
-    g.ea[(int64_t)slot * g.ld + i] = 0.0;
-    g.eb[(int64_t)slot * g.ld + i] = 0.0;
+    g.ecol[(int64_t)slot * g.ld + li] = (int)(i - g.col_off);
+    g.ea[(int64_t)slot * g.ld + li] = 0.0;
+    g.eb[(int64_t)slot * g.ld + li] = 0.0;
   }
-  g.dinv[i] = 1.0 / diag;
+  g.dinv[li] = 1.0 / diag;
 }
 
 }  // namespace fem
@@ -258,10 +264,26 @@ extern "C" int cep_internal_fem_assemble_grid(int dim, int nx, int ny, int nz, d
                                               int width, int64_t ld, int *d_ecol, double *d_ea, double *d_eb,
                                               double *d_dinv, void *stream) {
   cep::fem::GridArgs g{dim, nx, ny, dim == 3 ? nz : 1, h, dt, d_D, n_d, d_rp, d_col, d_a, d_b,
-                       width, ld, d_ecol, d_ea, d_eb, d_dinv};
+                       width, ld, d_ecol, d_ea, d_eb, d_dinv, 0, 0, 0, 0};
   const int64_t n = (int64_t)g.nx * g.ny * g.nz;
   const int block = 128;
   const unsigned grid = (unsigned)((n + block - 1) / block);
+  cep::fem::assemble_grid_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Rows row0 .. row0 + n_rows - 1 of the same operator (a slab part), with
+// the same kernel and so the same bits; columns shifted by -col_off, D
+// starting at element e_off.
+extern "C" int cep_internal_fem_assemble_grid_rows(int dim, int nx, int ny, int nz, double h, double dt,
+                                                   const double *d_D, int n_d, int64_t e_off, int64_t row0,
+                                                   int64_t n_rows, int64_t col_off, const int *d_rp, int *d_col,
+                                                   double *d_a, double *d_b, int width, int64_t ld, int *d_ecol,
+                                                   double *d_ea, double *d_eb, double *d_dinv, void *stream) {
+  cep::fem::GridArgs g{dim, nx, ny, dim == 3 ? nz : 1, h, dt, d_D, n_d, d_rp, d_col, d_a, d_b,
+                       width, ld, d_ecol, d_ea, d_eb, d_dinv, row0, n_rows, col_off, e_off};
+  const int block = 128;
+  const unsigned grid = (unsigned)((n_rows + block - 1) / block);
   cep::fem::assemble_grid_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(g);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }

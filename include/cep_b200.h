@@ -622,6 +622,75 @@ int cep_tissue_group_destroy(cep_tissue_group_t g);
 int cep_tissue_group_set_timing(cep_tissue_group_t g, int on);
 int cep_tissue_group_timing(cep_tissue_group_t g, double *ionic_ms, double *diffusion_ms, long *steps);
 
+/* ---------------------------------------------------------- slab parts */
+/* A structured-grid tissue split into parts that each own a contiguous
+ * range of planes (the last axis: y in 2D, z in 3D), one part per GPU: the
+ * reference's row distribution of A, B and V (MatCreateMPIAIJ with
+ * PETSC_DECIDE, fem.cpp:667-670; the ghost exchange and dot-product
+ * reductions inside MatMult / KSPSolve, fem.cpp:705-718). The part holds its
+ * rows of A and B (bit-identical to the same rows of cep_fem_create_grid's
+ * operator) and the split Jacobi-PCG; moving the boundary planes between
+ * neighbouring parts and gathering the parts' partial sums is the
+ * caller's (NCCL or peer copies across GPUs; plain device buffers for
+ * several parts on one GPU). No V is gathered: each part's cells need only
+ * their own rows.
+ *
+ * split: planes [first, first + planes) of part `part`, the first
+ * n_planes % n_parts parts one plane longer (PETSc's PETSC_DECIDE rule).
+ * create_grid: arguments as cep_fem_create_grid with the whole grid's D
+ * (host); the part keeps the elements its rows touch. info: global index
+ * of the first owned row, owned rows (whole planes), rows per plane, and
+ * whether a lower / upper neighbour exists. get_csr: the owned rows with
+ * global column indices. */
+typedef struct cep_part *cep_part_t;
+int cep_part_split(int n_planes, int n_parts, int part, int *first_plane, int *planes);
+int cep_part_create_grid(int dim, int nx, int ny, int nz, double h, double dt, const double *D, int n_d, int part,
+                         int n_parts, void *stream, cep_part_t *out);
+int cep_part_destroy(cep_part_t p);
+int cep_part_info(cep_part_t p, long *row0, long *n_own, long *plane, int *has_lo, int *has_hi);
+int cep_part_get_csr(cep_part_t p, int *row_ptr, int *col_idx, double *a_val, double *b_val);
+/* rtol, max_iter and the norm as cep_fem_set_solver (same defaults). */
+int cep_part_set_solver(cep_part_t p, double rtol, int max_iter, int precond_norm);
+/* One implicit diffusion step A V = B V / dt split across the parts (all
+ * asynchronous on the part's stream; device pointers; a plane is `plane`
+ * doubles; partial buffers are 2 doubles per part, `all` the n_parts
+ * parts' partials in part order):
+ *   pack(d_v, lo, hi)          the first / last owned plane of V into lo / hi
+ *                              (to the lower / upper neighbour)
+ *   cg_begin(d_v, v_lo, v_hi, partial)      b = B V / dt with the
+ *                              neighbours' planes of V; r = b, z = D^-1 b
+ *   for iter = 0, 1, ... while not done:
+ *     cg_direction(iter, all, n_parts, send_lo, send_hi)   convergence test
+ *                              on the gathered partials, p = z + beta p, its
+ *                              boundary planes into send_lo / send_hi
+ *     cg_product(iter, p_lo, p_hi, partial)  q = A p with the neighbours'
+ *                              planes of p
+ *     cg_update(iter, all, n_parts, partial)  x += alpha p, r -= alpha q,
+ *                              z = D^-1 r
+ *   cg_end(d_v, t_new)         V = x (activation times at t_new when cells
+ *                              are bound)
+ * Every part sums the gathered partials in part order, so all parts stop
+ * together and the result does not depend on which rank holds which part.
+ * Once done, the remaining launches of a chunk return at once: the caller
+ * may run several iterations between cg_status calls (blocking; iters is
+ * negative when max_iter was reached). */
+int cep_part_pack(cep_part_t p, const void *d_v, void *d_lo, void *d_hi);
+int cep_part_cg_begin(cep_part_t p, const void *d_v, const void *d_v_lo, const void *d_v_hi, void *d_partial);
+int cep_part_cg_direction(cep_part_t p, int iter, const void *d_all, int n_parts, void *d_send_lo, void *d_send_hi);
+int cep_part_cg_product(cep_part_t p, int iter, const void *d_p_lo, const void *d_p_hi, void *d_partial);
+int cep_part_cg_update(cep_part_t p, int iter, const void *d_all, int n_parts, void *d_partial);
+int cep_part_cg_status(cep_part_t p, int iter, int *done, int *iters, double *res);
+int cep_part_cg_end(cep_part_t p, void *d_v, double t_new);
+/* The part's cells (one instance per owned row, on the part's stream): the
+ * tissue's S1 stimulus over the owned rows (mask of n_own bytes, NULL = none)
+ * as cep_tissue_set_stimulus, and activation times (first step with
+ * V >= act_thr). ionic_step: every owned node's ionic update at tissue time
+ * t (Cheart::cellular_reaction, heart.cpp:274-430). */
+int cep_part_bind_cells(cep_part_t p, cep_batch_t cells, const unsigned char *s1_mask, double bcl, double t_crt,
+                        double dur, int n_pace, double act_thr);
+int cep_part_ionic_step(cep_part_t p, double t);
+int cep_part_get_activation(cep_part_t p, double *t_act);
+
 #ifdef __cplusplus
 }
 #endif

@@ -533,3 +533,146 @@ def tissue_run(model: str, dim: int, nx: int, ny: int, nz: int, h: float, D, dt:
                              _ptr(tact), int(s2_kind), int(s2_target), float(s2_thr),
                              reg.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), float(ecto_dur))
     return v, its, tact
+
+
+class SlabPart:
+    """CPU restatement of one slab part (the cep_part_* operations of the
+    product: csrc/slab.cu) over the oracle's grid operator: the rows of part
+    `part` of n_parts (contiguous planes of the last axis, PETSC_DECIDE's
+    split, fem.cpp:667-670), columns in the part's extended numbering
+    [lower halo plane | owned rows | upper halo plane], and the split
+    Jacobi-PCG whose dot products are per-part partials added in part
+    order. Vectors are numpy arrays or CPU torch tensors (so that gloo can
+    carry the exchange)."""
+
+    def __init__(self, dim: int, nx: int, ny: int, nz: int, h: float, dt: float, D, part: int, n_parts: int):
+        if dim == 2:
+            nz = 1
+        rp, ci, av, bv = fem_assemble(dim, nx, ny, nz, h, dt, D)
+        n_planes = ny if dim == 2 else nz
+        self.plane = nx if dim == 2 else nx * ny
+        if not (1 <= n_parts <= n_planes and 0 <= part < n_parts):
+            raise ValueError("bad split")
+        base, rem = divmod(n_planes, n_parts)
+        first, planes = part * base + min(part, rem), base + (1 if part < rem else 0)
+        self.index, self.n_parts, self.dim, self.dt = part, n_parts, dim, dt
+        self.row0, self.n_own = first * self.plane, planes * self.plane
+        self.has_lo, self.has_hi = part > 0, part < n_parts - 1
+        lo = self.plane if self.has_lo else 0
+        r0, r1 = rp[self.row0], rp[self.row0 + self.n_own]
+        self.rp = (rp[self.row0: self.row0 + self.n_own + 1] - r0).astype(np.int64)
+        self.ci = (ci[r0:r1] - (self.row0 - lo)).astype(np.int64)
+        self.av, self.bv = av[r0:r1].copy(), bv[r0:r1].copy()
+        rows = np.repeat(np.arange(self.n_own), np.diff(self.rp))
+        diag = self.av[self.ci == rows + lo]
+        self.dinv = 1.0 / diag
+        self._rows = rows
+        self.rtol, self.max_iter, self.precond_norm = 1e-5, 10000, True
+        n = self.n_own
+        self.x, self.r, self.z, self.q, self.p = (np.zeros(n) for _ in range(5))
+        self.st = [dict(rz=0.0, n0=0.0, res=0.0, used=0, done=0, conv=0) for _ in range(2)]
+
+    @staticmethod
+    def _np(x):
+        return None if x is None else (x.numpy() if hasattr(x, "numpy") else x)
+
+    def buffer(self, n: int):
+        import torch
+        return torch.zeros(n, dtype=torch.float64)
+
+    def set_solver(self, rtol: float, max_iter: int = 10000, precond_norm: bool = True):
+        self.rtol, self.max_iter, self.precond_norm = float(rtol), int(max_iter), bool(precond_norm)
+
+    def _apply(self, val, lo, own, hi):
+        parts = ([self._np(lo)] if self.has_lo else []) + [self._np(own)[: self.n_own]] + \
+            ([self._np(hi)] if self.has_hi else [])
+        ext = np.concatenate(parts)
+        return np.bincount(self._rows, weights=val * ext[self.ci], minlength=self.n_own)
+
+    @staticmethod
+    def _dot(a, b) -> float:
+        return float(np.sum(a * b))
+
+    @staticmethod
+    def _total(all_partials, n_parts):
+        a = SlabPart._np(all_partials)
+        s0 = s1 = 0.0
+        for k in range(n_parts):
+            s0 += float(a[2 * k])
+            s1 += float(a[2 * k + 1])
+        return s0, s1
+
+    def pack(self, v, lo, hi):
+        vv = self._np(v)
+        if lo is not None:
+            self._np(lo)[:] = vv[: self.plane]
+        if hi is not None:
+            self._np(hi)[:] = vv[self.n_own - self.plane: self.n_own]
+
+    def cg_begin(self, v, v_lo, v_hi, partial):
+        b = self._apply(self.bv, v_lo, v, v_hi) / self.dt
+        self.r[:] = b
+        self.z[:] = self.dinv * b
+        self.x[:] = 0.0
+        self.p[:] = 0.0
+        self.st[0] = dict(rz=0.0, n0=0.0, res=0.0, used=0, done=0, conv=0)
+        out = self._np(partial)
+        out[0] = self._dot(b, self.z)
+        out[1] = self._dot(self.z, self.z) if self.precond_norm else self._dot(b, b)
+
+    def cg_direction(self, it: int, all_partials, send_lo, send_hi):
+        s = self.st[it & 1]
+        t = dict(s)
+        beta = 0.0
+        if not s["done"]:
+            a0, a1 = self._total(all_partials, self.n_parts)
+            if it == 0:
+                t["rz"], t["n0"] = a0, float(np.sqrt(a1))
+                t["res"] = 1.0 if t["n0"] > 0.0 else 0.0
+                if t["n0"] == 0.0:
+                    t["done"] = t["conv"] = 1
+            else:
+                nr = float(np.sqrt(a1))
+                t["res"], t["used"] = nr / s["n0"], it
+                if nr <= self.rtol * s["n0"]:
+                    t["done"] = t["conv"] = 1
+                elif it >= self.max_iter:
+                    t["done"] = 1
+                beta = a0 / s["rz"]
+                t["rz"] = a0
+        self.st[(it + 1) & 1] = t
+        if t["done"]:
+            return
+        self.p[:] = beta * self.p + self.z
+        if self.has_lo and send_lo is not None:
+            self._np(send_lo)[:] = self.p[: self.plane]
+        if self.has_hi and send_hi is not None:
+            self._np(send_hi)[:] = self.p[self.n_own - self.plane:]
+
+    def cg_product(self, it: int, p_lo, p_hi, partial):
+        if self.st[(it + 1) & 1]["done"]:
+            return
+        self.q[:] = self._apply(self.av, p_lo, self.p, p_hi)
+        out = self._np(partial)
+        out[0] = self._dot(self.p, self.q)
+        out[1] = 0.0
+
+    def cg_update(self, it: int, all_partials, partial):
+        s = self.st[(it + 1) & 1]
+        if s["done"]:
+            return
+        pq, _ = self._total(all_partials, self.n_parts)
+        alpha = s["rz"] / pq
+        self.x += alpha * self.p
+        self.r -= alpha * self.q
+        self.z[:] = self.dinv * self.r
+        out = self._np(partial)
+        out[0] = self._dot(self.r, self.z)
+        out[1] = self._dot(self.z, self.z) if self.precond_norm else self._dot(self.r, self.r)
+
+    def cg_status(self, it: int):
+        s = self.st[(it + 1) & 1]
+        return bool(s["done"]), (s["used"] if s["conv"] else -self.max_iter), s["res"]
+
+    def cg_end(self, v, t_new: float = 0.0):
+        self._np(v)[: self.n_own] = self.x
