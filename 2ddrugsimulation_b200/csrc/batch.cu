@@ -56,6 +56,16 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr int kBlock = 128;
 
+// A copy on the batch's own stream, finished before returning. A plain
+// cudaMemcpy runs on the legacy stream, which a non-blocking stream does
+// not wait for (a read-back can see a kernel's output half written), and
+// returns before a pageable upload has landed.
+int copy_sync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? CEP_OK : fail(CEP_ERR_CUDA, "copy of %zu bytes: %s", bytes, cudaGetErrorString(e));
+}
+
 }  // namespace
 
 struct cep_batch {
@@ -1153,7 +1163,7 @@ int cep_batch_create(int model, int n, int precision, void *stream, cep_batch_t 
   // default schedule: unbounded run, biomarkers off
   std::vector<int> sc((size_t)4 * b->ld, 0);
   for (int64_t i = 0; i < b->ld; ++i) { sc[i] = 0x7fffffff; sc[3 * b->ld + i] = -1; }
-  if (cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (copy_sync(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream) != CEP_OK) {
     cep_batch_destroy(b);
     return fail(CEP_ERR_CUDA, "schedule upload failed");
   }
@@ -1405,6 +1415,10 @@ int cep_batch_init(cep_batch_t b, const double *celltype, const double *conc, co
                    unsigned flags) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
   if (hill && hill_stride < 14) return fail(CEP_ERR_ARG, "hill_stride must be >= 14 (got %d)", hill_stride);
+  if ((flags & CEP_FLAG_NEO_ORD) && b->model != CEP_MODEL_ORD2011)
+    return fail(CEP_ERR_UNSUPPORTED, "CEP_FLAG_NEO_ORD selects a build of ORd 2011 only");
+  if ((flags & CEP_FLAG_NEO_ORD) && (flags & CEP_FLAG_QUIRKS))
+    return fail(CEP_ERR_ARG, "CEP_FLAG_NEO_ORD and CEP_FLAG_QUIRKS name two different builds");
   const ModelInfo *mi = model_info(b->model);
   const int n = b->n;
   // validate the drug inputs on the host: NaN/negative IC50 rows are rejected
@@ -1575,7 +1589,9 @@ int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace,
   // per-instance loop bounds from each instance's BCL, computed as the
   // reference computes them (cipa_drug_bench.cpp:136,188,240)
   std::vector<double> bcl(b->n);
-  CEP_CUDA(cudaMemcpy(bcl.data(), b->params + (size_t)mi->p_bcl * b->ld, sizeof(double) * b->n, cudaMemcpyDeviceToHost));
+  if (int rc_c = copy_sync(bcl.data(), b->params + (size_t)mi->p_bcl * b->ld, sizeof(double) * b->n,
+                          cudaMemcpyDeviceToHost, b->stream))
+    return rc_c;
   std::vector<int> sc((size_t)4 * b->ld, 0);
   const int print_freq = (int)((1. / dt) * dt_write);
   int max_per_beat = 1;
@@ -1587,7 +1603,8 @@ int cep_batch_set_protocol(cep_batch_t b, double dt, int n_pace, int first_pace,
     const int per_beat = print_freq > 0 ? sc[b->ld + i] / print_freq + 2 : 2;
     if (per_beat > max_per_beat) max_per_beat = per_beat;
   }
-  CEP_CUDA(cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (int rc_c = copy_sync(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream))
+    return rc_c;
   if (first_pace >= 0) {
     if (!b->bmf) {
       int rc;
@@ -2106,7 +2123,8 @@ int cep_internal_batch_tissue_begin(cep_batch_t b, double dt) {
     sc[b->ld + i] = 0x7fffffff;     // no beat boundary
     sc[3 * b->ld + i] = -1;         // biomarkers off
   }
-  CEP_CUDA(cudaMemcpy(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (int rc_c = copy_sync(b->sched, sc.data(), sc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream))
+    return rc_c;
   b->has_protocol = true;
   RunArgs a = make_args(b, 0);
   a.bm_on = 0;

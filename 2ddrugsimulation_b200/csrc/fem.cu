@@ -60,6 +60,14 @@ extern "C" int cep_internal_fem_assemble_tet(int n_nodes, const double *d_xyz, c
 
 namespace {
 
+// A copy on the object's own stream, finished before returning. A plain
+// cudaMemcpy runs on the legacy stream, which a non-blocking stream does
+// not wait for, and returns before a pageable upload has landed.
+inline cudaError_t copy_sync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
 #define FEM_CUDA(call)                                                                                   \
   do {                                                                                                   \
     cudaError_t e_ = (call);                                                                             \
@@ -793,8 +801,8 @@ int fem_build_classes(cep_fem *f) {
   const int slots = f->dim == 3 ? 27 : 9;
   const int64_t n = f->n, ld = f->ld;
   std::vector<double> sa((size_t)slots * ld), sb((size_t)slots * ld);
-  FEM_CUDA(cudaMemcpy(sa.data(), f->sa, sizeof(double) * sa.size(), cudaMemcpyDeviceToHost));
-  FEM_CUDA(cudaMemcpy(sb.data(), f->sb, sizeof(double) * sb.size(), cudaMemcpyDeviceToHost));
+  FEM_CUDA(copy_sync(sa.data(), f->sa, sizeof(double) * sa.size(), cudaMemcpyDeviceToHost, f->stream));
+  FEM_CUDA(copy_sync(sb.data(), f->sb, sizeof(double) * sb.size(), cudaMemcpyDeviceToHost, f->stream));
   std::unordered_map<uint64_t, std::vector<int>> buckets;
   std::vector<int> cls(ld, 0);
   std::vector<double> ta, tb;
@@ -838,9 +846,9 @@ int fem_build_classes(cep_fem *f) {
   if ((rc = fem_alloc(f, &f->cls, (size_t)ld)) || (rc = fem_alloc(f, &f->ca, ta.size())) ||
       (rc = fem_alloc(f, &f->cb, tb.size())))
     return rc;
-  FEM_CUDA(cudaMemcpy(f->cls, cls.data(), sizeof(int) * ld, cudaMemcpyHostToDevice));
-  FEM_CUDA(cudaMemcpy(f->ca, ta.data(), sizeof(double) * ta.size(), cudaMemcpyHostToDevice));
-  FEM_CUDA(cudaMemcpy(f->cb, tb.data(), sizeof(double) * tb.size(), cudaMemcpyHostToDevice));
+  FEM_CUDA(copy_sync(f->cls, cls.data(), sizeof(int) * ld, cudaMemcpyHostToDevice, f->stream));
+  FEM_CUDA(copy_sync(f->ca, ta.data(), sizeof(double) * ta.size(), cudaMemcpyHostToDevice, f->stream));
+  FEM_CUDA(copy_sync(f->cb, tb.data(), sizeof(double) * tb.size(), cudaMemcpyHostToDevice, f->stream));
   f->n_classes = (int)(ta.size() / stride);
   return CEP_OK;
 }
@@ -933,7 +941,7 @@ int fem_autotune(cep_fem *f) {
   double *tv = nullptr;
   FEM_CUDA(cudaMalloc(&tv, sizeof(double) * f->ld));
   Status saved;
-  FEM_CUDA(cudaMemcpy(&saved, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  FEM_CUDA(copy_sync(&saved, f->st, sizeof(Status), cudaMemcpyDeviceToHost, f->stream));
   const double rtol = f->rtol;
   const int max_iter = f->max_iter;
   f->rtol = 1e-300;
@@ -968,7 +976,7 @@ int fem_autotune(cep_fem *f) {
   cudaFree(tv);
   if (rc) return rc;
   if ((rc = fem_check_ctl(f))) return rc;
-  FEM_CUDA(cudaMemcpy(f->st, &saved, sizeof(Status), cudaMemcpyHostToDevice));
+  FEM_CUDA(copy_sync(f->st, &saved, sizeof(Status), cudaMemcpyHostToDevice, f->stream));
   FEM_CUDA(cudaGetLastError());
   f->format = best_fmt;
   return CEP_OK;
@@ -1450,7 +1458,7 @@ int cep_fem_solve(cep_fem_t f, double *v, int *iters, double *rel_res) {
   if (rc) return rc;
   if ((rc = fem_check_ctl(f))) return rc;
   Status s;
-  FEM_CUDA(cudaMemcpy(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  FEM_CUDA(copy_sync(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost, f->stream));
   if (iters) *iters = s.last_iters;
   if (rel_res) *rel_res = s.last_res;
   if (s.last_iters < 0) return fail_msg(CEP_ERR_NOT_CONVERGED, "PCG hit max_iter (%d), relative residual %g", f->max_iter, s.last_res);
@@ -1462,7 +1470,7 @@ int cep_fem_stats(cep_fem_t f, int *last_iters, long *total_iters, long *solves,
   int rc;
   if ((rc = fem_check_ctl(f))) return rc;
   Status s;
-  FEM_CUDA(cudaMemcpy(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost));
+  FEM_CUDA(copy_sync(&s, f->st, sizeof(Status), cudaMemcpyDeviceToHost, f->stream));
   if (last_iters) *last_iters = s.last_iters;
   if (total_iters) *total_iters = (long)s.total_iters;
   if (solves) *solves = (long)s.solves;
@@ -1817,7 +1825,7 @@ int cep_tissue_set_electrodes(cep_tissue_t t, int n_el, const double *xyz, long 
     t->el = t->ecg_part = t->ecg_rec = nullptr;
     return fail_msg(CEP_ERR_OOM, "pseudo-ECG buffers");
   }
-  FEM_CUDA(cudaMemcpy(t->el, xyz, sizeof(double) * 3 * n_el, cudaMemcpyHostToDevice));
+  FEM_CUDA(copy_sync(t->el, xyz, sizeof(double) * 3 * n_el, cudaMemcpyHostToDevice, t->stream));
   t->n_el = n_el;
   t->ecg_every = every;
   t->ecg_max = max_records;
@@ -1858,7 +1866,7 @@ int cep_tissue_set_s2(cep_tissue_t t, int kind, int target_node, double vm_thres
   bool ok = cudaMalloc((void **)&t->proto, sizeof(CepProto)) == cudaSuccess;
   if (ok && kind == CEP_S2_ECTOPIC) {
     ok = cudaMalloc((void **)&t->mask2, (size_t)t->n) == cudaSuccess &&
-         cudaMemcpy(t->mask2, region, (size_t)t->n, cudaMemcpyHostToDevice) == cudaSuccess;
+         copy_sync(t->mask2, region, (size_t)t->n, cudaMemcpyHostToDevice, t->stream) == cudaSuccess;
   }
   if (ok && kind == CEP_S2_RESET && !nodes.empty()) {
     // snapshot of the region's states now (the batch's SoA rows)
@@ -1868,12 +1876,12 @@ int cep_tissue_set_s2(cep_tissue_t t, int kind, int target_node, double vm_thres
       for (size_t k = 0; k < nodes.size(); ++k) snap[(size_t)s * nodes.size() + k] = all[(size_t)s * n + nodes[k]];
     ok = cudaMalloc((void **)&t->s2_nodes, sizeof(int) * nodes.size()) == cudaSuccess &&
          cudaMalloc((void **)&t->s2_snap, sizeof(double) * snap.size()) == cudaSuccess &&
-         cudaMemcpy(t->s2_nodes, nodes.data(), sizeof(int) * nodes.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMemcpy(t->s2_snap, snap.data(), sizeof(double) * snap.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+         copy_sync(t->s2_nodes, nodes.data(), sizeof(int) * nodes.size(), cudaMemcpyHostToDevice, t->stream) == cudaSuccess &&
+         copy_sync(t->s2_snap, snap.data(), sizeof(double) * snap.size(), cudaMemcpyHostToDevice, t->stream) == cudaSuccess;
     t->s2_count = (int)nodes.size();
     t->ns = ns;
   }
-  if (!ok || cudaMemcpy(t->proto, &p, sizeof(CepProto), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (!ok || copy_sync(t->proto, &p, sizeof(CepProto), cudaMemcpyHostToDevice, t->stream) != cudaSuccess) {
     cudaFree(t->proto);
     cudaFree(t->mask2);
     cudaFree(t->s2_nodes);
@@ -1894,7 +1902,7 @@ int cep_tissue_get_ecg(cep_tissue_t t, double *phi, long *n_records) {
   FEM_CUDA(cudaStreamSynchronize(t->stream));
   if (n_records) *n_records = t->ecg_n;
   if (phi && t->ecg_n > 0)
-    FEM_CUDA(cudaMemcpy(phi, t->ecg_rec, sizeof(double) * (size_t)t->ecg_n * t->n_el, cudaMemcpyDeviceToHost));
+    FEM_CUDA(copy_sync(phi, t->ecg_rec, sizeof(double) * (size_t)t->ecg_n * t->n_el, cudaMemcpyDeviceToHost, t->stream));
   return CEP_OK;
 }
 
@@ -1941,6 +1949,7 @@ extern "C" int cep_fem_set_wait_test(long spin_limit, unsigned block0_delay_ns) 
   const long long lim = spin_limit;
   FEM_CUDA(cudaMemcpyToSymbol(cep::fem::g_spin_limit_test, &lim, sizeof(lim)));
   FEM_CUDA(cudaMemcpyToSymbol(cep::fem::g_block0_delay_ns, &block0_delay_ns, sizeof(block0_delay_ns)));
+  FEM_CUDA(cudaDeviceSynchronize());  // landed before any stream's next launch reads them
   return CEP_OK;
 }
 
