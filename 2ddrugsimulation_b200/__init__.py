@@ -381,9 +381,9 @@ class Batch:
         return self
 
     def set_kernel(self, variant: str):
-        """'cell' (one thread per cell), 'roles' (4 warps per 32 cells),
-        'pairs' (2 warps per 32 cells) or 'split' (8 warps per 32 cells)."""
-        _check(lib().cep_batch_set_kernel(self._h, {"cell": 0, "roles": 1, "pairs": 2, "split": 3}[variant]))
+        """'cell' (one thread per cell), 'roles' (4 warps per 32 cells) or
+        'pairs' (2 warps per 32 cells)."""
+        _check(lib().cep_batch_set_kernel(self._h, {"cell": 0, "roles": 1, "pairs": 2}[variant]))
         return self
 
     def run(self, n_steps: int):
@@ -408,7 +408,7 @@ class Batch:
         (state restored after every trial) and keep the fastest."""
         v, blk = ctypes.c_int(), ctypes.c_int()
         _check(lib().cep_batch_autotune(self._h, int(n_steps), ctypes.byref(v), ctypes.byref(blk)))
-        return {0: "cell", 1: "roles", 2: "pairs", 3: "split"}[v.value], blk.value
+        return {0: "cell", 1: "roles", 2: "pairs"}[v.value], blk.value
 
     def step(self, t: float, dt: float, stim_mode: int = -1):
         """One step of every instance from time t (computeRates + solveAnalytical)."""

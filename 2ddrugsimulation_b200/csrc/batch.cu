@@ -456,127 +456,6 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   }
 }
 
-// Split form of role_loop: 8 warps per 32 cells. Warp r (r < 4) runs the
-// currents and A gates of role r, warp r + 4 its B gates (ord::role's half
-// H = 1 / 2), so each warp's dependent chain per step is about half a
-// role's. After the step's barrier every warp applies the forward-Euler
-// update of V and the ions (as in role_loop), and the A warps take the B
-// gates just written by their partner from shared memory ([2][4][8][32]
-// doubles, double-buffered by step parity like the Parts), so both halves
-// start the next step from the same states the whole role would hold. The
-// states stored at the end are the A warps' (every state of their role),
-// except the CiPA Markov chain, which its B warp owns. Bit-identical to
-// role_loop: the same operations on the same values.
-template <class M, class P, int R, int H>
-__device__ __forceinline__ void split_loop(const RunArgs &a, typename P::G (*part)[4][8][32], double (*gx)[4][8][32],
-                                           int lane) {
-  using G = typename P::G;
-  const int64_t i = (int64_t)blockIdx.x * 32 + lane;
-  const bool valid = i < a.n;
-  const int64_t il = valid ? i : (int64_t)a.n - 1;
-  int st = a.status[il];
-  bool alive = valid && st == CEP_INST_RUNNING;
-  if (!__syncthreads_or(alive)) return;  // uniform: every warp sees the same 32 cells
-  typename M::template Y<G> y;
-  typename M::template Par<G> q;
-  M::template load<G>(y, a.y, a.ld, il);
-  M::template load_par<G>(q, a.par, a.ld, il);
-  double t = a.t[il];
-  int iout = a.iout[il];
-  const bm::Sched sc{a.sched[il], a.sched[a.ld + il], a.sched[2 * a.ld + il], a.sched[3 * a.ld + il]};
-  const bool bm_on = R == 0 && H == 1 && a.bm_on && sc.first_pace >= 0;
-  int cnt_print = bm::countdown(iout, sc.print_freq);
-  int cnt_bcl = bm::countdown(iout, sc.steps_per_bcl);
-  const double bcl = a.par[M::p_bcl() * a.ld + il];
-  const double stim_start = a.par[M::p_stim_start() * a.ld + il];
-  typename M::template Cur<G> c;
-  bm::Hot hot;
-  if (bm_on) bm::hot_load(a.bv, il, hot);
-  int buf = 0;
-  for (int k = 0; k <= a.n_steps; ++k) {
-    const bool can_update = iout < sc.imax;
-    const bool active = alive && !(can_update && k == a.n_steps);
-    const bool upd = active && can_update;
-    const double V0 = y.V;
-    const double cai0 = M::cai_of(y);
-    const auto ctx = ord::context<P>(y, q, t, a.stim_mode);
-    {
-      ord::Part<G> p;
-      ord::role<P, M::kCipa, R, H>(y, q, ctx, a.dt, upd, p);
-      if constexpr (H == 1) {
-#pragma unroll
-        for (int f = 0; f < 8; ++f) {
-          const int fld = ord::role_field(R, f);
-          if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
-        }
-      } else {
-        ord::split_put<M::kCipa, R>(y, gx[buf][R], lane);
-      }
-    }
-    __syncthreads();
-    ord::Part<G> s;
-#pragma unroll
-    for (int f = 0; f < ord::kNumSums; ++f) s.f[f] = (G)0;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-#pragma unroll
-      for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(r, f);
-        if (fld >= 0) s.f[fld] += part[buf][r][f][lane];
-      }
-    }
-    ord::combine<P>(y, q, s, a.dt, upd, c);
-    if constexpr (H == 1) {
-      if (upd) ord::split_get<M::kCipa, R>(y, gx[buf][R], lane);
-    }
-    if (bm_on && active && iout >= 1)
-      bm::sample(a.bv, i, sc, iout, t, a.dt, bcl, stim_start, V0, cai0, (double)c.dVdt, (double)c.INaL,
-                 (double)c.ICaL, (double)c.Ito, (double)c.IKr, (double)c.IKs, (double)c.IK1, a.qnet_thr,
-                 cnt_print, cnt_bcl, hot);
-    if (active) {
-      if (!can_update) {
-        st = CEP_INST_DONE;
-        alive = false;
-      } else {
-        t += a.dt;
-        ++iout;
-        if (!isfinite(y.V)) {
-          st = CEP_INST_NONFINITE;
-          alive = false;
-        }
-      }
-    }
-    buf ^= 1;
-  }
-  if (valid) {
-    if (bm_on) bm::hot_store(a.bv, i, hot);
-    if constexpr (R < 3 ? H == 1 : H == 2) ord::store_role<M::kCipa>(R, y, a.y, a.ld, i);
-    if (R == 0 && H == 1) {
-      a.t[i] = t;
-      a.iout[i] = iout;
-      a.status[i] = st;
-    }
-  }
-}
-
-template <class M, class P>
-__global__ void __launch_bounds__(256) run_split_kernel(RunArgs a) {
-  using G = typename P::G;
-  __shared__ G part[2][4][8][32];
-  __shared__ double gx[2][4][8][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  switch (w) {
-    case 0: split_loop<M, P, 0, 1>(a, part, gx, lane); break;
-    case 1: split_loop<M, P, 1, 1>(a, part, gx, lane); break;
-    case 2: split_loop<M, P, 2, 1>(a, part, gx, lane); break;
-    case 3: split_loop<M, P, 3, 1>(a, part, gx, lane); break;
-    case 4: split_loop<M, P, 0, 2>(a, part, gx, lane); break;
-    case 5: split_loop<M, P, 1, 2>(a, part, gx, lane); break;
-    case 6: split_loop<M, P, 2, 2>(a, part, gx, lane); break;
-    default: split_loop<M, P, 3, 2>(a, part, gx, lane); break;
-  }
-}
-
 template <class M, class P>
 __global__ void __launch_bounds__(128) run_roles_kernel(RunArgs a) {
   using G = typename P::G;
@@ -954,12 +833,6 @@ struct Ops {
         run_pairs_kernel<M, Mixed><<<grid, 64, 0, b->stream>>>(a);
       else
         run_pairs_kernel<M, F64><<<grid, 64, 0, b->stream>>>(a);
-    } else if (b->variant == CEP_KERNEL_SPLIT) {
-      const int grid = (b->n + 31) / 32;
-      if (b->precision == CEP_PREC_MIXED)
-        run_split_kernel<M, Mixed><<<grid, 256, 0, b->stream>>>(a);
-      else
-        run_split_kernel<M, F64><<<grid, 256, 0, b->stream>>>(a);
     } else {
       const int block = b->block;
       const int grid = (b->n + block - 1) / block;
@@ -1189,8 +1062,7 @@ int cep_batch_set_block(cep_batch_t b, int threads_per_block) {
 
 int cep_batch_set_kernel(cep_batch_t b, int variant) {
   if (!b) return fail(CEP_ERR_ARG, "null batch");
-  if (variant != CEP_KERNEL_CELL && variant != CEP_KERNEL_ROLES && variant != CEP_KERNEL_PAIRS &&
-      variant != CEP_KERNEL_SPLIT)
+  if (variant != CEP_KERNEL_CELL && variant != CEP_KERNEL_ROLES && variant != CEP_KERNEL_PAIRS)
     return fail(CEP_ERR_ARG, "bad kernel variant %d", variant);
   if (variant != CEP_KERNEL_CELL && b->model != CEP_MODEL_ORD2011 && b->model != CEP_MODEL_CIPA2017)
     return fail(CEP_ERR_UNSUPPORTED, "warp-specialised kernel exists for the ORd family only");
@@ -1248,7 +1120,6 @@ int cep_batch_autotune(cep_batch_t b, long n_steps, int *variant_out, int *block
   if (b->model == CEP_MODEL_ORD2011 || b->model == CEP_MODEL_CIPA2017) {
     cands.push_back({CEP_KERNEL_PAIRS, b->block});
     cands.push_back({CEP_KERNEL_ROLES, b->block});
-    cands.push_back({CEP_KERNEL_SPLIT, b->block});
   }
   const int keep_variant = b->variant, keep_block = b->block;
   cudaEvent_t e0, e1;
@@ -2078,7 +1949,7 @@ int cep_batch_hrv(cep_batch_t b, const double *bcls, int n_bcl, double dt, doubl
     // sample alone (the rewound first call, the last call)
     const long evals = (long)imax[p] + 3;
     for (long done = 0; done < evals; done += steps_per_launch) {
-      if (b->variant == CEP_KERNEL_ROLES || b->variant == CEP_KERNEL_SPLIT) {
+      if (b->variant == CEP_KERNEL_ROLES) {
         if (mixed) hrv::calls_roles_kernel<Mixed><<<grid32, 128, 0, b->stream>>>(a);
         else hrv::calls_roles_kernel<F64><<<grid32, 128, 0, b->stream>>>(a);
       } else if (b->variant == CEP_KERNEL_PAIRS) {

@@ -31,7 +31,7 @@ __device__ __forceinline__ double rcp64_nr(double x) {
 // 1/x for x = +-0 (+-inf), +-inf (+-0), NaN, and subnormal x, scaled by
 // 2^64 into the normal range (the result overflows to inf as IEEE's does
 // when |x| < 2^-1024).
-__device__ __noinline__ __attribute__((const)) double rcp64_special(double x) {
+__device__ __noinline__ double rcp64_special(double x) {
   if (isnan(x)) return x;
   if (x == 0.0) return copysign(INFINITY, x);
   if (isinf(x)) return copysign(0.0, x);
@@ -45,7 +45,7 @@ __device__ __forceinline__ double rcp64(double x) {
 // subnormal or infinite divisors, infinite dividends and quotients that
 // overflow. Finite cases divide the frexp mantissas and scale the result
 // back with ldexp (one extra rounding for subnormal quotients).
-__device__ __noinline__ __attribute__((const)) double div64_special(double a, double b) {
+__device__ __noinline__ double div64_special(double a, double b) {
   if (isnan(a) || isnan(b)) return a + b;
   const bool neg = signbit(a) != signbit(b);
   if (isinf(b)) return isinf(a) ? NAN : (neg ? -0.0 : 0.0);
@@ -84,13 +84,13 @@ __device__ __forceinline__ double div64(double a, double b) {
 // which made the step's code too large for the instruction caches
 // (no_instruction stalls 6 cycles per issued instruction in the 2-warp form);
 // one shared copy of each keeps it resident (about 2x the FP64 throughput).
-__device__ __noinline__ __attribute__((const)) double exp_f64(double x) { return ::exp(x); }
-__device__ __noinline__ __attribute__((const)) double log_f64(double x) { return ::log(x); }
+__device__ __noinline__ double exp_f64(double x) { return ::exp(x); }
+__device__ __noinline__ double log_f64(double x) { return ::log(x); }
 
 // Two exponentials of independent arguments in one out-of-line body, where
 // the two instruction streams interleave: one call's latency for two
 // results (the ORd family's time constants are sums of two exponentials).
-__device__ __noinline__ __attribute__((const)) double2 exp2_f64(double a, double b) { return make_double2(::exp(a), ::exp(b)); }
+__device__ __noinline__ double2 exp2_f64(double a, double b) { return make_double2(::exp(a), ::exp(b)); }
 
 template <class G>
 struct Exp2 {

@@ -311,19 +311,8 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
   }
 }
 
-// Halves of a role in the split form (8 warps per 32 cells): H = 0 the
-// whole role; H = 1 its currents and A gates; H = 2 its B gates (in role 3
-// the CiPA Markov chain). A half computes only what its outputs need (the
-// rest is dead code: the out-of-line FP64 functions are pure). The B gates
-// reach the A half through shared memory after every step (split_put /
-// split_get), so both halves advance exactly the states the whole role does.
-template <int H>
-inline constexpr bool kGateA = H != 2;
-template <int H>
-inline constexpr bool kGateB = H != 1;
-
 // role 0: fast and late sodium, background sodium, Na/K pump
-template <class P, bool kCipa, int H = 0>
+template <class P, bool kCipa>
 __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                         double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
@@ -387,28 +376,26 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G JnakNa = (G)3.0 * (x1 * xs_inv * a3 - x2 * xs_inv * b3);
   const G JnakK = (G)2.0 * (x4 * xs_inv * (G)k::b1 - x3 * xs_inv * a1);
   const G INaK = q.Pnak * ((G)k::zna * JnakNa + (G)k::zk * JnakK);
-  if constexpr (H != 2) {
-    o.f[S_iV] = INa + INaL + INaK + INab;
-    o.f[S_iNa] = INa + INaL + (G)3.0 * INaK + INab;
-    o.f[S_iK] = -(G)2.0 * INaK;
-    o.f[S_INa] = INa;
-    o.f[S_INaL] = INaL;
-  }
+  o.f[S_iV] = INa + INaL + INaK + INab;
+  o.f[S_iNa] = INa + INaL + (G)3.0 * INaK + INab;
+  o.f[S_iK] = -(G)2.0 * INaK;
+  o.f[S_INa] = INa;
+  o.f[S_INaL] = INaL;
   if (!update) return;
-  if constexpr (kGateA<H>) y.m = rush_larsen<P>(y.m, mss, tm, dt);
-  if constexpr (kGateB<H>) y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
-  if constexpr (kGateB<H>) y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
-  if constexpr (kGateB<H>) y.j = rush_larsen<P, true>(y.j, hss, tj, dt);
-  if constexpr (kGateB<H>) y.hsp = rush_larsen<P, true>(y.hsp, hssp, tau_scaled<P>(ths, 3.0), dt);
-  if constexpr (kGateB<H>) y.jp = rush_larsen<P, true>(y.jp, hss, tau_scaled<P>(tj, 1.46), dt);
-  if constexpr (kGateA<H>) y.mL = rush_larsen<P>(y.mL, mLss, tm, dt);
-  if constexpr (kGateA<H>) y.hL = rush_larsen<P, true>(y.hL, hLss, tau_const<P>(k::thL), dt);
-  if constexpr (kGateA<H>) y.hLp = rush_larsen<P, true>(y.hLp, hLssp, tau_const<P>(k::thLp), dt);
+  y.m = rush_larsen<P>(y.m, mss, tm, dt);
+  y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
+  y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
+  y.j = rush_larsen<P, true>(y.j, hss, tj, dt);
+  y.hsp = rush_larsen<P, true>(y.hsp, hssp, tau_scaled<P>(ths, 3.0), dt);
+  y.jp = rush_larsen<P, true>(y.jp, hss, tau_scaled<P>(tj, 1.46), dt);
+  y.mL = rush_larsen<P>(y.mL, mLss, tm, dt);
+  y.hL = rush_larsen<P, true>(y.hL, hLss, tau_const<P>(k::thL), dt);
+  y.hLp = rush_larsen<P, true>(y.hLp, hLssp, tau_const<P>(k::thLp), dt);
 }
 
 // role 1: transient outward, slow/rapid (ORd) delayed rectifier, inward
 // rectifier and background potassium currents; the stimulus
-template <class P, bool kCipa, int H = 0>
+template <class P, bool kCipa>
 __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                        double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
@@ -467,33 +454,31 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const G xkb = P::rc((one + P::ex(-(v - (G)14.48) * (G)(1.0 / 18.34))));
   const G IKb = q.GKb * xkb * (v - EK);
   const G Istim = c.stim ? (G)q.amp : (G)0;
-  if constexpr (H != 2) {
-    o.f[S_iV] = Ito + IKr + IKs + IK1 + IKb + Istim;
-    o.f[S_iK] = Ito + IKr + IKs + IK1 + IKb + Istim;
-    o.f[S_Ito] = Ito;
-    o.f[S_IKr] = IKr;
-    o.f[S_IKs] = IKs;
-    o.f[S_IK1] = IK1;
-  }
+  o.f[S_iV] = Ito + IKr + IKs + IK1 + IKb + Istim;
+  o.f[S_iK] = Ito + IKr + IKs + IK1 + IKb + Istim;
+  o.f[S_Ito] = Ito;
+  o.f[S_IKr] = IKr;
+  o.f[S_IKs] = IKs;
+  o.f[S_IK1] = IK1;
   if (!update) return;
-  if constexpr (kGateA<H>) y.a = rush_larsen<P, true>(y.a, ass, ta, dt);
-  if constexpr (kGateB<H>) y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
-  if constexpr (kGateB<H>) y.iS = rush_larsen<P, true>(y.iS, iss, tiS, dt);
-  if constexpr (kGateA<H>) y.ap = rush_larsen<P, true>(y.ap, assp, ta, dt);
-  if constexpr (kGateB<H>) y.iFp = rush_larsen<P, true>(y.iFp, iss, tau_times<P>(tiF, dti), dt);
-  if constexpr (kGateB<H>) y.iSp = rush_larsen<P, true>(y.iSp, iss, tau_times<P>(tiS, dti), dt);
-  if constexpr (kGateA<H>) y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
-  if constexpr (kGateA<H>) y.xs2 = rush_larsen<P, true>(y.xs2, xs1ss, txs2, dt);
-  if constexpr (kGateA<H>) y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
+  y.a = rush_larsen<P, true>(y.a, ass, ta, dt);
+  y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
+  y.iS = rush_larsen<P, true>(y.iS, iss, tiS, dt);
+  y.ap = rush_larsen<P, true>(y.ap, assp, ta, dt);
+  y.iFp = rush_larsen<P, true>(y.iFp, iss, tau_times<P>(tiF, dti), dt);
+  y.iSp = rush_larsen<P, true>(y.iSp, iss, tau_times<P>(tiS, dti), dt);
+  y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
+  y.xs2 = rush_larsen<P, true>(y.xs2, xs1ss, txs2, dt);
+  y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
   if constexpr (!kCipa) {
-    if constexpr (kGateB<H>) y.xrf = rush_larsen<P, true>(y.xrf, xrss, txrf, dt);
-    if constexpr (kGateB<H>) y.xrs = rush_larsen<P, true>(y.xrs, xrss, txrs, dt);
+    y.xrf = rush_larsen<P, true>(y.xrf, xrss, txrf, dt);
+    y.xrs = rush_larsen<P, true>(y.xrs, xrss, txrs, dt);
   }
 }
 
 // role 2: L-type calcium channel (Ca, Na, K components), background and
 // pump calcium currents, ryanodine-receptor release
-template <class P, bool kCipa, int H = 0>
+template <class P, bool kCipa>
 __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                         double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
@@ -536,15 +521,13 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   const G ICaK = (one - fICaLp) * q.PCaK * PhiCaK * gate_np + fICaLp * q.PCaKp * PhiCaK * gate_p;
   const G IpCa = P::dv(((G)k::GpCa * cai_g), ((G)k::KmCap + cai_g));
   const G Jrel = (one - fICaLp) * (G)y.Jrelnp + fICaLp * (G)y.Jrelp;
-  if constexpr (H != 2) {
-    o.f[S_iV] = ICaL + ICaNa + ICaK + IpCa + ICab;
-    o.f[S_iNass] = ICaNa;
-    o.f[S_iKss] = ICaK;
-    o.f[S_iCass] = ICaL;
-    o.f[S_iCai] = IpCa + ICab;
-    o.f[S_Jrel] = Jrel;
-    o.f[S_ICaL] = ICaL;
-  }
+  o.f[S_iV] = ICaL + ICaNa + ICaK + IpCa + ICab;
+  o.f[S_iNass] = ICaNa;
+  o.f[S_iKss] = ICaK;
+  o.f[S_iCass] = ICaL;
+  o.f[S_iCai] = IpCa + ICab;
+  o.f[S_Jrel] = Jrel;
+  o.f[S_ICaL] = ICaL;
   if (!update) return;
   const G rel_den = one + p8(P::dv((G)1.5, cajsr_g));
   const G den_tau = one + P::dv((G)0.0123, cajsr_g);
@@ -566,25 +549,23 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
   }
   const G Jrel_inf = q.celltype == 2 ? Jrel_inf_t * (G)1.7 : Jrel_inf_t;
   const G Jrel_infp = q.celltype == 2 ? Jrel_t * (G)1.7 : Jrel_t;
-  if constexpr (kGateA<H>) y.d = rush_larsen<P, true>(y.d, dss, td, dt);
-  if constexpr (kGateB<H>) y.ff = rush_larsen<P, true>(y.ff, fss, tff, dt);
-  if constexpr (kGateB<H>) y.fs = rush_larsen<P, true>(y.fs, fss, tfs, dt);
-  if constexpr (kGateB<H>) y.fcaf = rush_larsen<P, true>(y.fcaf, fss, tfcaf, dt);
-  if constexpr (kGateB<H>) y.fcas = rush_larsen<P, true>(y.fcas, fss, tfcas, dt);
-  if constexpr (kGateB<H>) y.jca = rush_larsen<P, true>(y.jca, fss, q.tjca, dt);
-  if constexpr (kGateB<H>) y.ffp = rush_larsen<P, true>(y.ffp, fss, tau_scaled<P>(tff, 2.5), dt);
+  y.d = rush_larsen<P, true>(y.d, dss, td, dt);
+  y.ff = rush_larsen<P, true>(y.ff, fss, tff, dt);
+  y.fs = rush_larsen<P, true>(y.fs, fss, tfs, dt);
+  y.fcaf = rush_larsen<P, true>(y.fcaf, fss, tfcaf, dt);
+  y.fcas = rush_larsen<P, true>(y.fcas, fss, tfcas, dt);
+  y.jca = rush_larsen<P, true>(y.jca, fss, q.tjca, dt);
+  y.ffp = rush_larsen<P, true>(y.ffp, fss, tau_scaled<P>(tff, 2.5), dt);
   // quirk (1): the reference steps fcafp by d = 25 (exp(-25/tfcafp)), far
   // outside the Taylor range, so that case takes the exponential form
-  if constexpr (kGateB<H>) {
-    if (q.fcafp_dt != (G)0)
-      y.fcafp = rush_larsen<P>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), (double)q.fcafp_dt);
-    else
-      y.fcafp = rush_larsen<P, true>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), dt);
-  }
+  if (q.fcafp_dt != (G)0)
+    y.fcafp = rush_larsen<P>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), (double)q.fcafp_dt);
+  else
+    y.fcafp = rush_larsen<P, true>(y.fcafp, fss, tau_scaled<P>(tfcaf, 2.5), dt);
   // nca relaxes at rate km2n towards anca*k2n/km2n (Ohara_Rudy_2011.cpp:1065-1066)
-  if constexpr (kGateA<H>) y.nca = rush_larsen<P, true>(y.nca, anca * P::dv((G)k::k2n, km2n), tau_quot<P>(1.0, km2n), dt);
-  if constexpr (kGateA<H>) y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, dt);
-  if constexpr (kGateA<H>) y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, dt);
+  y.nca = rush_larsen<P, true>(y.nca, anca * P::dv((G)k::k2n, km2n), tau_quot<P>(1.0, km2n), dt);
+  y.Jrelnp = rush_larsen<P>(y.Jrelnp, Jrel_inf, tau_rel, dt);
+  y.Jrelp = rush_larsen<P>(y.Jrelp, Jrel_infp, tau_relp, dt);
 }
 
 // Na/Ca exchanger current of one compartment (INaCa_i or INaCa_ss, the
@@ -685,7 +666,7 @@ __device__ __forceinline__ void markov_be(typename P::G h, const typename P::G *
   g[1] = xIC2; g[2] = xC1; g[3] = xC2; g[4] = xO; g[5] = xIO; g[6] = xIOb; g[7] = xOb;
 }
 
-template <class P, bool kCipa, int H = 0>
+template <class P, bool kCipa>
 __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                        double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
@@ -712,17 +693,15 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
                            : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
     IKr = q.GKr * (G)k::sqrt_ko54 * (G)y.O * (v - EK);
   }
-  if constexpr (H != 2) {
-    o.f[S_iV] = INaCa_i + INaCa_ss + IKr;
-    o.f[S_iNa] = (G)3.0 * INaCa_i;
-    o.f[S_iNass] = (G)3.0 * INaCa_ss;
-    o.f[S_iCass] = -(G)2.0 * INaCa_ss;
-    o.f[S_iCai] = -(G)2.0 * INaCa_i;
-    o.f[S_Jup] = Jup;
-    o.f[S_IKr] = IKr;
-    o.f[S_iK] = IKr;  // CiPA's IKr is a potassium flux too (zero for ORd: role 1 carries it)
-  }
-  if constexpr (kCipa && kGateB<H>) {
+  o.f[S_iV] = INaCa_i + INaCa_ss + IKr;
+  o.f[S_iNa] = (G)3.0 * INaCa_i;
+  o.f[S_iNass] = (G)3.0 * INaCa_ss;
+  o.f[S_iCass] = -(G)2.0 * INaCa_ss;
+  o.f[S_iCai] = -(G)2.0 * INaCa_i;
+  o.f[S_Jup] = Jup;
+  o.f[S_IKr] = IKr;
+  o.f[S_iK] = IKr;  // CiPA's IKr is a potassium flux too (zero for ORd: role 1 carries it)
+  if constexpr (kCipa) {
     if (!update) return;
     // Markov IKr with drug binding and trapping (ohara_rudy_cipa_v1_2017.cpp:
     // 2157-2165), forward Euler like every other non-gate state. Rates
@@ -793,45 +772,13 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
   }
 }
 
-template <class P, bool kCipa, int R, int H = 0>
+template <class P, bool kCipa, int R>
 __device__ __forceinline__ void role(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                      double dt, bool update, Part<typename P::G> &o) {
-  if constexpr (R == 0) role_na<P, kCipa, H>(y, q, c, dt, update, o);
-  if constexpr (R == 1) role_k<P, kCipa, H>(y, q, c, dt, update, o);
-  if constexpr (R == 2) role_ca<P, kCipa, H>(y, q, c, dt, update, o);
-  if constexpr (R == 3) role_x<P, kCipa, H>(y, q, c, dt, update, o);
-}
-
-// The states the B half of role r advances, in its shared-memory slots
-// (at most 8); CiPA role 3 passes only O, the one Markov state the A half's
-// IKr reads.
-template <bool kCipa, int R, class G>
-__device__ __forceinline__ void split_put(const Y<G> &y, double (*gx)[32], int lane) {
-  if constexpr (R == 0) {
-    gx[0][lane] = y.hf; gx[1][lane] = y.hs; gx[2][lane] = y.j; gx[3][lane] = y.hsp; gx[4][lane] = y.jp;
-  } else if constexpr (R == 1) {
-    gx[0][lane] = y.iF; gx[1][lane] = y.iS; gx[2][lane] = y.iFp; gx[3][lane] = y.iSp;
-    if constexpr (!kCipa) { gx[4][lane] = y.xrf; gx[5][lane] = y.xrs; }
-  } else if constexpr (R == 2) {
-    gx[0][lane] = y.ff; gx[1][lane] = y.fs; gx[2][lane] = y.fcaf; gx[3][lane] = y.fcas; gx[4][lane] = y.jca;
-    gx[5][lane] = y.ffp; gx[6][lane] = y.fcafp;
-  } else {
-    if constexpr (kCipa) gx[0][lane] = y.O;
-  }
-}
-template <bool kCipa, int R, class G>
-__device__ __forceinline__ void split_get(Y<G> &y, const double (*gx)[32], int lane) {
-  if constexpr (R == 0) {
-    y.hf = gx[0][lane]; y.hs = gx[1][lane]; y.j = gx[2][lane]; y.hsp = gx[3][lane]; y.jp = gx[4][lane];
-  } else if constexpr (R == 1) {
-    y.iF = gx[0][lane]; y.iS = gx[1][lane]; y.iFp = gx[2][lane]; y.iSp = gx[3][lane];
-    if constexpr (!kCipa) { y.xrf = gx[4][lane]; y.xrs = gx[5][lane]; }
-  } else if constexpr (R == 2) {
-    y.ff = gx[0][lane]; y.fs = gx[1][lane]; y.fcaf = gx[2][lane]; y.fcas = gx[3][lane]; y.jca = gx[4][lane];
-    y.ffp = gx[5][lane]; y.fcafp = gx[6][lane];
-  } else {
-    if constexpr (kCipa) y.O = gx[0][lane];
-  }
+  if constexpr (R == 0) role_na<P, kCipa>(y, q, c, dt, update, o);
+  if constexpr (R == 1) role_k<P, kCipa>(y, q, c, dt, update, o);
+  if constexpr (R == 2) role_ca<P, kCipa>(y, q, c, dt, update, o);
+  if constexpr (R == 3) role_x<P, kCipa>(y, q, c, dt, update, o);
 }
 
 // Sum of the four roles' contributions, in role order (both kernels).

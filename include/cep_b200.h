@@ -114,7 +114,6 @@ int cep_batch_set_block(cep_batch_t b, int threads_per_block);
 #define CEP_KERNEL_CELL 0
 #define CEP_KERNEL_ROLES 1
 #define CEP_KERNEL_PAIRS 2 /* 2 warps per 32 cells, two channel groups each */
-#define CEP_KERNEL_SPLIT 3 /* 8 warps per 32 cells, each channel group split in two (ORd family) */
 int cep_batch_set_kernel(cep_batch_t b, int variant);
 /* Launch-shape autotuner (no counterpart in the reference, which runs one
  * cell per object): times one run of n_steps steps (default 400) in each

@@ -155,16 +155,14 @@ def test_cipa_stiff_drug_binding_stays_finite(cep, gpu, oracle, precision):
 @pytest.mark.parametrize("model", ["cipa2017", "ord2011"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_roles_kernel_matches_cell_kernel(cep, gpu, model, precision):
-    """The warp-specialised kernels (4, 2 or 8 warps per 32 cells) and the
+    """The warp-specialised kernels (4 or 2 warps per 32 cells) and the
     one-thread-per-cell kernel compute the same trajectory and biomarkers
-    (the roles' contributions are added in the same order in both); the
-    8-warp split form does exactly the 4-role form's operations, so its
-    states and records are bit-identical to it."""
+    (the roles' contributions are added in the same order in both)."""
     conc, hill = cipa_population(20, 3, seed=21)  # 60 instances: two blocks, one partial
     if model == "ord2011":
         hill = hill[:, :14].copy()
     out = {}
-    for kern in ("cell", "roles", "pairs", "split"):
+    for kern in ("cell", "roles", "pairs"):
         b = cep.Batch(model, len(conc), precision)
         b.set_kernel(kern)
         b.init(conc=conc, hill=hill, quirks=True)
@@ -174,17 +172,12 @@ def test_roles_kernel_matches_cell_kernel(cep, gpu, model, precision):
         out[kern] = (b.get_states(), b.biomarkers())
     s0, b0 = out["cell"]
     tol = 1e-9 if precision == "fp64" else 1e-4
-    for kern in ("roles", "pairs", "split"):
+    for kern in ("roles", "pairs"):
         s1, b1 = out[kern]
         assert np.abs(s0[:, 0] - s1[:, 0]).max() <= tol, kern
         for key in ("apd90", "apd50", "cad90"):
             assert np.abs(b0[key] - b1[key]).max() <= 0.01, (kern, key)
         assert np.array_equal(b0["status"], b1["status"]), kern
-    sr, br = out["roles"]
-    ss, bs = out["split"]
-    assert np.array_equal(sr, ss)
-    for key in br:
-        assert np.array_equal(br[key], bs[key]), key
 
 
 @pytest.mark.gpu
@@ -205,7 +198,7 @@ def test_autotune_keeps_the_batch_state(cep, gpu):
     a.run(30000)
     s0, clk0 = a.get_states(), a.clock(0)
     form, block = a.autotune(300)
-    assert form in ("cell", "roles", "pairs", "split") and block in (32, 64, 96, 128)
+    assert form in ("cell", "roles", "pairs") and block in (32, 64, 96, 128)
     assert np.array_equal(a.get_states(), s0) and a.clock(0) == clk0
     a.run_to_end(50000)
     ref = make()

@@ -134,8 +134,8 @@ def test_hrv_short_protocols_and_the_one_off_replacement(cep, gpu, oracle, kerne
     oracle's bit for bit, and the final states follow the oracle's
     trajectory through every rewound pace start. With num_pace1 = 250 the
     one-off replacement (:336-338) fires at the end of pace 0 and copies the
-    unevaluated beat, as the bench does. The three kernel forms give the
-    same states bit for bit."""
+    unevaluated beat, as the bench does. The three kernel forms agree to
+    1e-9 (relative to max(1, |state|))."""
     bcls = [812.5, 640.0, 700.3, 1000.0]
     ct = np.array([0.0, 1.0])
     conc = np.array([0.0, 1.0])
@@ -153,9 +153,9 @@ def test_hrv_short_protocols_and_the_one_off_replacement(cep, gpu, oracle, kerne
             assert got["n_eligible"][k] == 0 and got["status"][k] == 1
             assert abs(y[k, 0] - r["y"][0]) <= 1e-6, (k, y[k, 0], r["y"][0])
             assert np.all(np.abs(y[k] - r["y"]) <= 1e-6 * np.maximum(1.0, np.abs(r["y"]))), k
-        if kernel != "cell":
+        if kernel != "cell":  # the forms add the same terms, the FMA contractions differ (as in the run kernels)
             yc = _gpu_hrv(cep, ct, conc, hill, bcls, 0.02, "fp64", kernel="cell", num_pace1=np1)[1]
-            assert np.array_equal(y, yc), kernel
+            assert np.all(np.abs(y - yc) <= 1e-9 * np.maximum(1.0, np.abs(yc))), kernel
 
 
 @pytest.mark.gpu
