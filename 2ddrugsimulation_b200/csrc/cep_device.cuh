@@ -96,6 +96,19 @@ template <class G>
 struct Exp2 {
   G a, b;
 };
+template <class G>
+struct Exp4 {
+  G a, b, c, d;
+};
+// Four exponentials of independent arguments in one out-of-line body: the
+// steady states of a channel group are each a logistic of V, and one call
+// overlaps their four dependency chains.
+struct Dbl4 {
+  double a, b, c, d;
+};
+__device__ __noinline__ __attribute__((const)) Dbl4 exp4_f64(double a, double b, double c, double d) {
+  return Dbl4{::exp(a), ::exp(b), ::exp(c), ::exp(d)};
+}
 
 struct F64 {
   using G = double;
@@ -107,6 +120,10 @@ struct F64 {
   __device__ __forceinline__ static Exp2<double> ex2(double a, double b) {
     const double2 r = exp2_f64(a, b);
     return {r.x, r.y};
+  }
+  __device__ __forceinline__ static Exp4<double> ex4(double a, double b, double c, double d) {
+    const Dbl4 r = exp4_f64(a, b, c, d);
+    return {r.a, r.b, r.c, r.d};
   }
   __device__ __forceinline__ static double dv(double a, double b) { return div64(a, b); }
   __device__ __forceinline__ static double rc(double x) { return rcp64(x); }
@@ -124,6 +141,9 @@ struct Mixed {
   __device__ __forceinline__ static float ex(float x) { return __expf(x); }
   __device__ __forceinline__ static float lg(float x) { return __logf(x); }
   __device__ __forceinline__ static Exp2<float> ex2(float a, float b) { return {__expf(a), __expf(b)}; }
+  __device__ __forceinline__ static Exp4<float> ex4(float a, float b, float c, float d) {
+    return {__expf(a), __expf(b), __expf(c), __expf(d)};
+  }
   __device__ __forceinline__ static float dv(float a, float b) { return __fdividef(a, b); }
   __device__ __forceinline__ static float rc(float x) { return __fdividef(1.0f, x); }
   __device__ __forceinline__ static float pw(float x, float y) { return __powf(x, y); }

@@ -200,3 +200,34 @@ def test_ord_bad_inputs_rejected(cep, gpu):
     b.init()
     with pytest.raises(cep.CepError):
         b.set_protocol(0.005, 10, 10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cajsr", [0.5, 1e-4, -0.005, -0.05])
+def test_ord_rates_hold_the_jrel_floor_at_any_cajsr(cep, gpu, oracle, cajsr):
+    """Forward Euler lets cajsr dip below zero in long protocols (the
+    oracle's own trajectory of the HRV epicardial case does from pace 139
+    on). For -0.0123 < cajsr < 0 the written time constant bt / (1 +
+    0.0123 / cajsr) is negative and the reference floors it at 0.001 ms
+    (Ohara_Rudy_2011.cpp:1063-1066); the device's rate form must take the
+    same floor there, or the release gates grow without bound. Every RATES
+    entry at such states against the oracle's computeRates, within 1e-9 of
+    the largest rate."""
+    ct, conc = np.array([0.0, 1.0]), np.array([0.0, 0.5])
+    hill = np.tile(np.array([5.0, 1.0, 20.0, 1.1, 30.0, 0.9, 8.0, 1.2, 4.0, 0.8, 15.0, 1.0, 0.6, 1.1]), (2, 1))
+    b = cep.Batch("ord2011", 2, "fp64")
+    b.init(celltype=ct, conc=conc, hill=hill, dutta=True, quirks=False)
+    y = b.get_states()
+    y[:, 0] = -10.0  # an open L-type channel: a nonzero release target
+    y[:, 8] = cajsr
+    y[:, 39:41] = [0.02, 0.03]  # Jrelnp, Jrelp away from their targets
+    b.set_states(y)
+    r = b.rates_all(0.0)
+    b.close()
+    for k in range(2):
+        c = oracle.Cell("ord2011", ct[k], conc[k], hill[k], is_dutta=True, quirks=False)
+        c.y[:41] = y[k]
+        ro, _ = c.rates(0.0)
+        scale = np.abs(ro[:41]).max()
+        assert np.isfinite(r[k]).all()
+        assert np.abs(r[k] - ro[:41]).max() <= 1e-9 * scale, (k, np.abs(r[k] - ro[:41]).argmax())
