@@ -67,7 +67,47 @@ __global__ void warp_slot_probe(int *out) {
   if ((threadIdx.x & 31) == 0) out[blockIdx.x * 4 + (threadIdx.x >> 5)] = (int)(wid & 3u);
 }
 
+// b = a over n 16-byte elements, `passes` times: with both arrays inside
+// the L2 after the first pass, the copy streams at L2 bandwidth.
+__global__ void l2_copy(const double2 *__restrict__ a, double2 *__restrict__ b, long n, int passes) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (int p = 0; p < passes; ++p)
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) b[i] = a[i];
+}
+
 extern "C" {
+// L2 copy bandwidth in bytes/s (read + write) over a 2 x 24 MiB working set.
+double cep_probe_l2_copy_bytes(void) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long n = (24L << 20) / (long)sizeof(double2);
+  double2 *a = nullptr, *b = nullptr;
+  if (cudaMalloc(&a, n * sizeof(double2)) != cudaSuccess) return -1.0;
+  if (cudaMalloc(&b, n * sizeof(double2)) != cudaSuccess) {
+    cudaFree(a);
+    return -1.0;
+  }
+  cudaMemset(a, 0, n * sizeof(double2));
+  const int block = 256, grid = sms * 8, passes = 64;
+  l2_copy<<<grid, block>>>(a, b, n, 2);  // warm: both arrays into the L2
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  l2_copy<<<grid, block>>>(a, b, n, passes);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(a);
+  cudaFree(b);
+  const double bytes = 2.0 * (double)n * sizeof(double2) * passes;
+  return cudaGetLastError() == cudaSuccess && ms > 0 ? bytes / (ms * 1e-3) : -1.0;
+}
+
 // SFU operations/s (ex2.approx) on the current device.
 double cep_probe_sfu_ops(void) {
   int dev = 0, sms = 0;

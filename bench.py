@@ -238,6 +238,8 @@ def measured_peaks():
         L.cep_probe_warp_slots.restype = ctypes.c_double
         L.cep_probe_warp_slots.argtypes = [ctypes.c_int]
         out["sfu_tops"] = max(L.cep_probe_sfu_ops() for _ in range(3)) / 1e12
+        L.cep_probe_l2_copy_bytes.restype = ctypes.c_double
+        out["l2_gbs"] = max(L.cep_probe_l2_copy_bytes() for _ in range(3)) / 1e9
         out["role_blocks_on_distinct_smsp"] = L.cep_probe_warp_slots(313)
     except OSError:
         pass
@@ -684,13 +686,22 @@ def phase_rooflines(model: str, prec: str, cells: int, steps: int, timing: dict,
                frac=ion["achieved"] / ion["peak"], traffic=tr * cells if tr else None,
                other_bound_ms={"hbm": ion_hbm_ms, "sfu": ion_sfu_ms or None})
     dif_bytes = cells * pcg_bytes_per_row(fmt, slots, iters)
-    dif = {"bound": "hbm", "kernel": "pcg_many_kernel (one cooperative launch per step for the group)",
-           "achieved": dif_bytes / (dif_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s", "peak_source": hbm_src,
+    # An operator whose ncu DRAM traffic is far below its algorithmic bytes
+    # runs out of the L2 (the 512^2 sheets): its bound is the L2 bandwidth
+    # (the bench's L2 copy probe), not HBM.
+    meas = PCG_TRAFFIC_PER_ROW_SOLVE.get(model) if fmt == 3 else None
+    l2 = peaks.get("l2_gbs")
+    if meas is not None and l2 and meas < 0.25 * pcg_bytes_per_row(fmt, slots, iters):
+        dif_bound, dif_peak, dif_src = "l2", l2, "bench.py L2 copy probe on this GPU (2 x 24 MiB working set)"
+    else:
+        dif_bound, dif_peak, dif_src = "hbm", hbm, hbm_src
+    dif = {"bound": dif_bound, "kernel": "pcg_many_kernel (one cooperative launch per step for the group)",
+           "achieved": dif_bytes / (dif_ms * 1e-3) / 1e9, "peak": dif_peak, "unit": "GB/s", "peak_source": dif_src,
            "ms_per_step": dif_ms,
            "traffic": PCG_TRAFFIC_PER_ROW_SOLVE[model] * cells if (fmt == 3 and model in PCG_TRAFFIC_PER_ROW_SOLVE) else None,
            "bytes_per_row_per_solve": pcg_bytes_per_row(fmt, slots, iters),
            "cg_iters_per_solve": iters}
-    dif["frac"] = dif["achieved"] / hbm
+    dif["frac"] = dif["achieved"] / dif_peak
     return {"ionic": ion, "diffusion": dif, "ionic_share": ion_ms / (ion_ms + dif_ms)}
 
 
