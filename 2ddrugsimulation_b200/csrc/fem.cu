@@ -945,7 +945,7 @@ int fem_autotune(cep_fem *f) {
   const double rtol = f->rtol;
   const int max_iter = f->max_iter;
   f->rtol = 1e-300;
-  f->max_iter = 8;
+  f->max_iter = 40;  // long enough that launch and barrier jitter do not decide
   cudaEvent_t e0, e1;
   FEM_CUDA(cudaEventCreate(&e0));
   FEM_CUDA(cudaEventCreate(&e1));
@@ -955,7 +955,7 @@ int fem_autotune(cep_fem *f) {
     if (fmt == CEP_FEM_STENCIL && !f->sa) continue;
     if (fmt == CEP_FEM_CLASSED && !f->cls) continue;
     f->format = fmt;
-    for (int rep = 0; rep < 3 && rc == CEP_OK; ++rep) {
+    for (int rep = 0; rep < 5 && rc == CEP_OK; ++rep) {
       smooth_field_kernel<<<(unsigned)((f->n + 255) / 256), 256, 0, f->stream>>>((int64_t)f->n, tv);
       cudaEventRecord(e0, f->stream);
       rc = fem_solve_async(f, tv, nullptr, 0.0, 0.0);

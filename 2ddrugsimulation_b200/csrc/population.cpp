@@ -14,8 +14,10 @@
 //      start again from their initial state in an FP64 batch on a second
 //      stream, concurrently with the mixed batch's remaining paces;
 //   3. an instance whose evaluated record still shows a diastolic Vm above
-//      the threshold although the screening passed it runs again in FP64
-//      after both batches finish.
+//      the threshold, or an APD90 above 0.9 BCL (a cell at the edge of
+//      2:1 block, whose beat-to-beat dynamics can settle into different
+//      regimes under FP32 and FP64 rounding), runs again in FP64 after both
+//      batches finish.
 // The FP64 records replace the mixed ones; refined[i] says which path
 // produced instance i's record.
 #include <cuda_runtime.h>
@@ -153,8 +155,10 @@ extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_
   }
   if (refine) {  // 3. whatever the screening missed
     std::vector<int> late;
+    constexpr double kNearBlock = 0.9;  // APD90 / BCL above which a beat is at the edge of block
     for (int i = 0; i < j->n; ++i)
-      if (how[i] == 0 && !(out[i].vm_valley < j->refine_above_vm)) late.push_back(i);
+      if (how[i] == 0 && (!(out[i].vm_valley < j->refine_above_vm) || out[i].apd90 > kNearBlock * j->bcl))
+        late.push_back(i);
     if (!late.empty()) {
       Batch c;
       if ((rc = make_batch(j, CEP_PREC_FP64, late, sb.s, c))) return rc;

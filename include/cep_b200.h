@@ -239,7 +239,9 @@ int cep_batch_rates_all(cep_batch_t b, double t, double *rates);
  * that do not repolarise, whose APD90 FP32 gates cannot hold) run from
  * their initial state in FP64 on a second stream concurrently with the
  * mixed population, and any instance whose evaluated record still shows a
- * diastolic Vm above it runs again in FP64 afterwards. refine_above_vm =
+ * diastolic Vm above it, or an APD90 above 0.9 BCL (a beat at the edge of
+ * 2:1 block, whose regime FP32 rounding can change), runs again in FP64
+ * afterwards (refined[i] = 1 concurrent, 2 afterwards). refine_above_vm =
  * NaN (or CEP_PREC_FP64) runs the single precision alone. No counterpart
  * in the reference beyond the loop it replaces. Blocking. */
 typedef struct {
@@ -456,7 +458,7 @@ double cep_qinward(const cep_biomarkers_t *control, const cep_biomarkers_t *drug
  * (fem.cpp:705-718) with PETSc KSPCG + PCJACOBI (fem.cpp:753-760). */
 typedef struct cep_fem *cep_fem_t;
 
-#define CEP_FEM_AUTO (-1) /* time both formats on this operator, keep the faster */
+#define CEP_FEM_AUTO (-1) /* time every format this operator has (40-iteration solves), keep the fastest */
 #define CEP_FEM_CSR 0
 #define CEP_FEM_ELL 1     /* column-major ELL, padded to the widest row */
 #define CEP_FEM_STENCIL 2 /* grid operators: 9/27 fixed slots, implicit columns */
