@@ -137,7 +137,10 @@ def test_cipa_long_protocol_refined_mixed_meets_bars(cep, gpu):
     500 ms: the FP64 reference run is latency-bound (~7 us per step for any
     population below ~10,000), so 260 paces at the headline's 2000 ms would
     take the GPU ~15 minutes. Both runs go through cep_population_run, at
-    the same time on their own streams."""
+    the same time on their own streams. At BCL 500 ms some drugged cells sit
+    at the edge of 2:1 block (APD90 near the BCL), where FP32 and FP64
+    rounding can settle the beat sequence into different regimes; the
+    compliant path re-runs every record with APD90 above 0.9 BCL in FP64."""
     import threading
     from test_cipa_gpu import cipa_population
     conc, hill = cipa_population(500, 5, seed=1234)
