@@ -558,8 +558,9 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
     crossed at ~0.1 mV/ms, so their APD90 moves by tenths of a ms under
     perturbations of 1e-5 and FP32 gates cannot hold it to 0.1 ms) run in
     FP64 from their initial state concurrently with the mixed population,
-    and any instance whose record still shows such a diastolic Vm, or an
-    APD90 above 0.9 BCL (the edge of 2:1 block), runs again in FP64
+    and any instance whose record still shows such a diastolic Vm, an
+    APD90 above 0.9 BCL or an evaluated beat without an action potential
+    (the edge of 2:1 block) runs again in FP64
     afterwards; out["refined"] marks both (out["refined_how"]: 1
     concurrent, 2 afterwards). amp_scale multiplies the stimulus amplitude
     (CONSTANTS[amp] *= Stim_Amplitude, cipa_drug_bench.cpp:147);

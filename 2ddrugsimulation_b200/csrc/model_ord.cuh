@@ -222,9 +222,9 @@ __device__ __forceinline__ bool stim_on(double t, double start, double bcl, doub
 // back to back) and the warp-specialised kernel (one warp per role for 32
 // cells, Parts exchanged through shared memory); both add the Parts in the
 // same order.
-//   role 0 (Na): m hf hs j hsp jp mL hL hLp; INa, INaL, INab, INaK
-//   role 1 (K) : a iF iS ap iFp iSp xs1 xs2 xk1 (ORd: xrf xrs); Ito, IKs, IK1,
-//                IKb, IKr (ORd), Istim
+//   role 0 (Na): m hf hs j hsp jp mL hL hLp xk1; INa, INaL, INab, INaK, IK1
+//   role 1 (K) : a iF iS ap iFp iSp xs1 xs2 (ORd: xrf xrs); Ito, IKs, IKb,
+//                IKr (ORd), Istim
 //   role 2 (Ca): d ff fs fcaf fcas jca ffp fcafp nca Jrelnp Jrelp; ICaL, ICaNa,
 //                ICaK, ICab, IpCa, Jrel
 //   role 3 (X) : INaCa_i, INaCa_ss, Jup; CiPA: the Markov IKr chain and IKr
@@ -253,8 +253,8 @@ struct Part {
 // Fields each role writes, in the order of its packed shared-memory slot
 // (at most 8; -1 = unused).
 __host__ __device__ constexpr int role_field(int role, int k) {
-  constexpr int t[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, -1, -1, -1},
-                           {S_iV, S_iK, S_Ito, S_IKr, S_IKs, S_IK1, -1, -1},
+  constexpr int t[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, S_IK1, -1, -1},
+                           {S_iV, S_iK, S_Ito, S_IKr, S_IKs, -1, -1, -1},
                            {S_iV, S_iNass, S_iKss, S_iCass, S_iCai, S_Jrel, S_ICaL, -1},
                            {S_iV, S_iNa, S_iNass, S_iCass, S_iCai, S_Jup, S_IKr, S_iK}};
   return t[role][k];
@@ -311,7 +311,8 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
   }
 }
 
-// role 0: fast and late sodium, background sodium, Na/K pump
+// role 0: fast and late sodium, background sodium, Na/K pump; the inward
+// rectifier (which balances the groups' dependency chains)
 template <class P, bool kCipa>
 __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                         double dt, bool update, Part<typename P::G> &o) {
@@ -381,12 +382,26 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G JnakNa = (G)3.0 * (x1 * xs_inv * a3 - x2 * xs_inv * b3);
   const G JnakK = (G)2.0 * (x4 * xs_inv * (G)k::b1 - x3 * xs_inv * a1);
   const G INaK = q.Pnak * ((G)k::zna * JnakNa + (G)k::zk * JnakK);
-  o.f[S_iV] = INa + INaL + INaK + INab;
+  // IK1 with its gate xk1: carried by this group, which is the lighter of
+  // the two in the pairs form and in the four-role form (the K group has
+  // the longest dependency chain)
+  const auto e_k1 = P::ex2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
+                           ((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493));
+  const G xk1ss = P::rc((one + e_k1.a));
+  const Tau<P> txk1 =
+      tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
+  const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+                         : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
+  const G rk1 = P::rc((one + e_k1.b));
+  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
+  o.f[S_iV] = INa + INaL + INaK + INab + IK1;
   o.f[S_iNa] = INa + INaL + (G)3.0 * INaK + INab;
-  o.f[S_iK] = -(G)2.0 * INaK;
+  o.f[S_iK] = IK1 - (G)2.0 * INaK;
   o.f[S_INa] = INa;
   o.f[S_INaL] = INaL;
+  o.f[S_IK1] = IK1;
   if (!update) return;
+  y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
   y.m = rush_larsen<P>(y.m, mss, tm, dt);
   y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
   y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
@@ -398,8 +413,8 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   y.hLp = rush_larsen<P, true>(y.hLp, hLssp, tau_const<P>(k::thLp), dt);
 }
 
-// role 1: transient outward, slow/rapid (ORd) delayed rectifier, inward
-// rectifier and background potassium currents; the stimulus
+// role 1: transient outward, slow/rapid (ORd) delayed rectifier and
+// background potassium currents; the stimulus
 template <class P, bool kCipa>
 __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                        double dt, bool update, Part<typename P::G> &o) {
@@ -408,9 +423,8 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   // the group's single exponentials, four per call
   const auto e_k1 = P::ex4(-(v - (G)14.34) * (G)(1.0 / 14.82), -(v - (G)18.4099) * (G)(1.0 / 29.3814),
                            (v + (G)100.0) * (G)(1.0 / 29.3814), (v + (G)43.94) * (G)(1.0 / 5.711));
-  const auto e_k2 = P::ex4(-(v + (G)11.60) * (G)(1.0 / 8.932), -(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
+  const auto e_k2 = P::ex4(-(v + (G)11.60) * (G)(1.0 / 8.932), -(v - (G)14.48) * (G)(1.0 / 18.34),
                            (v - (G)213.6) * (G)(1.0 / 151.2), (v + (G)70.0) * (G)0.05);
-  const auto e_k3 = P::ex2(((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493), -(v - (G)14.48) * (G)(1.0 / 18.34));
   const G e_a = e_k1.a;
   const G ass = P::rc((one + e_a));
   const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + e_k1.b))) + P::dv((G)3.5, (one + e_k1.c))));
@@ -427,9 +441,6 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const Tau<P> txs1 = tau_affine<P>(817.3, (esum<P>((G)2.326e-04, (v + (G)48.28) * (G)(1.0 / 17.80), (G)0.001292, -(v + (G)210.0) * (G)(1.0 / 230.0))));
   const Tau<P> txs2 =
       tau_quot<P>(1.0, (esum<P>((G)0.01, (v - (G)50.0) * (G)0.05, (G)0.0193, -(v + (G)66.54) * (G)(1.0 / 31.0))));
-  const G xk1ss = P::rc((one + e_k2.b));
-  const Tau<P> txk1 =
-      tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
   const G fp_ = c.fCaMKp;
   const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
                          : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
@@ -459,17 +470,14 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
                      ? one + P::dv((G)0.6, (one + P::ex((G)1.4 * ((G)k::log_ks_ca - P::lg((G)y.cai)))))
                      : one + P::dv((G)0.6, (one + P::pw(P::dv((G)3.8e-05, (G)y.cai), (G)1.4)));
   const G IKs = q.GKs * KsCa * (G)y.xs1 * (G)y.xs2 * (v - EKs);
-  const G rk1 = P::rc((one + e_k3.a));
-  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
-  const G xkb = P::rc((one + e_k3.b));
+  const G xkb = P::rc((one + e_k2.b));
   const G IKb = q.GKb * xkb * (v - EK);
   const G Istim = c.stim ? (G)q.amp : (G)0;
-  o.f[S_iV] = Ito + IKr + IKs + IK1 + IKb + Istim;
-  o.f[S_iK] = Ito + IKr + IKs + IK1 + IKb + Istim;
+  o.f[S_iV] = Ito + IKr + IKs + IKb + Istim;
+  o.f[S_iK] = Ito + IKr + IKs + IKb + Istim;
   o.f[S_Ito] = Ito;
   o.f[S_IKr] = IKr;
   o.f[S_IKs] = IKs;
-  o.f[S_IK1] = IK1;
   if (!update) return;
   y.a = rush_larsen<P, true>(y.a, ass, ta, dt);
   y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
@@ -479,7 +487,6 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   y.iSp = rush_larsen<P, true>(y.iSp, iss, tau_times<P>(tiS, dti), dt);
   y.xs1 = rush_larsen<P, true>(y.xs1, xs1ss, txs1, dt);
   y.xs2 = rush_larsen<P, true>(y.xs2, xs1ss, txs2, dt);
-  y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
   if constexpr (!kCipa) {
     y.xrf = rush_larsen<P, true>(y.xrf, xrss, txrf, dt);
     y.xrs = rush_larsen<P, true>(y.xrs, xrss, txrs, dt);
@@ -884,10 +891,10 @@ __device__ __forceinline__ void store_role(int role, const Y<G> &y, double *__re
       CEP_ST_ORD(V) CEP_ST_ORD(CaMKt) CEP_ST_ORD(cass) CEP_ST_ORD(nai) CEP_ST_ORD(nass) CEP_ST_ORD(ki)
       CEP_ST_ORD(kss) CEP_ST_ORD(cansr) CEP_ST_ORD(cajsr) CEP_ST_ORD(cai)
       CEP_ST_ORD(m) CEP_ST_ORD(hf) CEP_ST_ORD(hs) CEP_ST_ORD(j) CEP_ST_ORD(hsp) CEP_ST_ORD(jp) CEP_ST_ORD(mL)
-      CEP_ST_ORD(hL) CEP_ST_ORD(hLp)
+      CEP_ST_ORD(hL) CEP_ST_ORD(hLp) CEP_ST_ORD(xk1)
     } else if (role == 1) {
       CEP_ST_ORD(a) CEP_ST_ORD(iF) CEP_ST_ORD(iS) CEP_ST_ORD(ap) CEP_ST_ORD(iFp) CEP_ST_ORD(iSp)
-      CEP_ST_ORD(xs1) CEP_ST_ORD(xs2) CEP_ST_ORD(xk1) CEP_ST_ORD(xrf) CEP_ST_ORD(xrs)
+      CEP_ST_ORD(xs1) CEP_ST_ORD(xs2) CEP_ST_ORD(xrf) CEP_ST_ORD(xrs)
     } else if (role == 2) {
       CEP_ST_ORD(d) CEP_ST_ORD(ff) CEP_ST_ORD(fs) CEP_ST_ORD(fcaf) CEP_ST_ORD(fcas) CEP_ST_ORD(jca)
       CEP_ST_ORD(ffp) CEP_ST_ORD(fcafp) CEP_ST_ORD(nca) CEP_ST_ORD(Jrelnp) CEP_ST_ORD(Jrelp)
@@ -897,10 +904,10 @@ __device__ __forceinline__ void store_role(int role, const Y<G> &y, double *__re
       CEP_ST_CIPA(V) CEP_ST_CIPA(CaMKt) CEP_ST_CIPA(cass) CEP_ST_CIPA(nai) CEP_ST_CIPA(nass) CEP_ST_CIPA(ki)
       CEP_ST_CIPA(kss) CEP_ST_CIPA(cansr) CEP_ST_CIPA(cajsr) CEP_ST_CIPA(cai)
       CEP_ST_CIPA(m) CEP_ST_CIPA(hf) CEP_ST_CIPA(hs) CEP_ST_CIPA(j) CEP_ST_CIPA(hsp) CEP_ST_CIPA(jp)
-      CEP_ST_CIPA(mL) CEP_ST_CIPA(hL) CEP_ST_CIPA(hLp)
+      CEP_ST_CIPA(mL) CEP_ST_CIPA(hL) CEP_ST_CIPA(hLp) CEP_ST_CIPA(xk1)
     } else if (role == 1) {
       CEP_ST_CIPA(a) CEP_ST_CIPA(iF) CEP_ST_CIPA(iS) CEP_ST_CIPA(ap) CEP_ST_CIPA(iFp) CEP_ST_CIPA(iSp)
-      CEP_ST_CIPA(xs1) CEP_ST_CIPA(xs2) CEP_ST_CIPA(xk1)
+      CEP_ST_CIPA(xs1) CEP_ST_CIPA(xs2)
     } else if (role == 2) {
       CEP_ST_CIPA(d) CEP_ST_CIPA(ff) CEP_ST_CIPA(fs) CEP_ST_CIPA(fcaf) CEP_ST_CIPA(fcas) CEP_ST_CIPA(jca)
       CEP_ST_CIPA(ffp) CEP_ST_CIPA(fcafp) CEP_ST_CIPA(nca) CEP_ST_CIPA(Jrelnp) CEP_ST_CIPA(Jrelp)

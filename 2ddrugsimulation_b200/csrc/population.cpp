@@ -14,10 +14,11 @@
 //      start again from their initial state in an FP64 batch on a second
 //      stream, concurrently with the mixed batch's remaining paces;
 //   3. an instance whose evaluated record still shows a diastolic Vm above
-//      the threshold, or an APD90 above 0.9 BCL (a cell at the edge of
-//      2:1 block, whose beat-to-beat dynamics can settle into different
-//      regimes under FP32 and FP64 rounding), runs again in FP64 after both
-//      batches finish.
+//      the threshold, an APD90 above 0.9 BCL or an evaluated beat without
+//      an action potential (n_eligible below the evaluated paces: a cell at
+//      the edge of 2:1 block, whose beat-to-beat dynamics can settle into
+//      different regimes under FP32 and FP64 rounding) runs again in FP64
+//      after both batches finish.
 // The FP64 records replace the mixed ones; refined[i] says which path
 // produced instance i's record.
 #include <cuda_runtime.h>
@@ -156,8 +157,10 @@ extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_
   if (refine) {  // 3. whatever the screening missed
     std::vector<int> late;
     constexpr double kNearBlock = 0.9;  // APD90 / BCL above which a beat is at the edge of block
+    const int evaluated = j->first_pace >= 0 ? j->n_pace - j->first_pace : 0;
     for (int i = 0; i < j->n; ++i)
-      if (how[i] == 0 && (!(out[i].vm_valley < j->refine_above_vm) || out[i].apd90 > kNearBlock * j->bcl))
+      if (how[i] == 0 && (!(out[i].vm_valley < j->refine_above_vm) || out[i].apd90 > kNearBlock * j->bcl ||
+                          out[i].n_eligible < evaluated))
         late.push_back(i);
     if (!late.empty()) {
       Batch c;
