@@ -559,8 +559,9 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
     perturbations of 1e-5 and FP32 gates cannot hold it to 0.1 ms) run in
     FP64 from their initial state concurrently with the mixed population,
     and any instance whose record still shows such a diastolic Vm, an
-    APD90 above 0.9 BCL or an evaluated beat without an action potential
-    (the edge of 2:1 block) runs again in FP64
+    APD90 above 0.9 BCL or an intermittent rhythm (some evaluated beats
+    without an action potential at the peak sample: the edge of 2:1 block)
+    runs again in FP64
     afterwards; out["refined"] marks both (out["refined_how"]: 1
     concurrent, 2 afterwards). amp_scale multiplies the stimulus amplitude
     (CONSTANTS[amp] *= Stim_Amplitude, cipa_drug_bench.cpp:147);

@@ -96,10 +96,6 @@ template <class G>
 struct Exp2 {
   G a, b;
 };
-template <class G>
-struct Exp4 {
-  G a, b, c, d;
-};
 // Four exponentials of independent arguments in one out-of-line body: the
 // steady states of a channel group are each a logistic of V, and one call
 // overlaps their four dependency chains.
@@ -109,6 +105,24 @@ struct Dbl4 {
 __device__ __noinline__ __attribute__((const)) Dbl4 exp4_f64(double a, double b, double c, double d) {
   return Dbl4{::exp(a), ::exp(b), ::exp(c), ::exp(d)};
 }
+// A group of independent exponentials read through a(), b(), ...: FP64
+// evaluates them together in one out-of-line call (their chains overlap);
+// the mixed path evaluates each SFU exponential where it is read, so the
+// grouping does not hold FP32 results in registers across the code.
+struct GrpD {
+  double v[4];
+  __device__ __forceinline__ double a() const { return v[0]; }
+  __device__ __forceinline__ double b() const { return v[1]; }
+  __device__ __forceinline__ double c() const { return v[2]; }
+  __device__ __forceinline__ double d() const { return v[3]; }
+};
+struct GrpF {
+  float x[4];
+  __device__ __forceinline__ float a() const { return __expf(x[0]); }
+  __device__ __forceinline__ float b() const { return __expf(x[1]); }
+  __device__ __forceinline__ float c() const { return __expf(x[2]); }
+  __device__ __forceinline__ float d() const { return __expf(x[3]); }
+};
 
 struct F64 {
   using G = double;
@@ -121,9 +135,13 @@ struct F64 {
     const double2 r = exp2_f64(a, b);
     return {r.x, r.y};
   }
-  __device__ __forceinline__ static Exp4<double> ex4(double a, double b, double c, double d) {
+  __device__ __forceinline__ static GrpD grp4(double a, double b, double c, double d) {
     const Dbl4 r = exp4_f64(a, b, c, d);
-    return {r.a, r.b, r.c, r.d};
+    return GrpD{{r.a, r.b, r.c, r.d}};
+  }
+  __device__ __forceinline__ static GrpD grp2(double a, double b) {
+    const double2 r = exp2_f64(a, b);
+    return GrpD{{r.x, r.y, 0.0, 0.0}};
   }
   __device__ __forceinline__ static double dv(double a, double b) { return div64(a, b); }
   __device__ __forceinline__ static double rc(double x) { return rcp64(x); }
@@ -141,9 +159,8 @@ struct Mixed {
   __device__ __forceinline__ static float ex(float x) { return __expf(x); }
   __device__ __forceinline__ static float lg(float x) { return __logf(x); }
   __device__ __forceinline__ static Exp2<float> ex2(float a, float b) { return {__expf(a), __expf(b)}; }
-  __device__ __forceinline__ static Exp4<float> ex4(float a, float b, float c, float d) {
-    return {__expf(a), __expf(b), __expf(c), __expf(d)};
-  }
+  __device__ __forceinline__ static GrpF grp4(float a, float b, float c, float d) { return GrpF{{a, b, c, d}}; }
+  __device__ __forceinline__ static GrpF grp2(float a, float b) { return GrpF{{a, b, 0.f, 0.f}}; }
   __device__ __forceinline__ static float dv(float a, float b) { return __fdividef(a, b); }
   __device__ __forceinline__ static float rc(float x) { return __fdividef(1.0f, x); }
   __device__ __forceinline__ static float pw(float x, float y) { return __powf(x, y); }

@@ -319,11 +319,11 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   // the four logistic steady states of the group in one call
-  const auto e_ss = P::ex4(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2), (v + (G)k::hssV1) * (G)(1.0 / k::hssV2),
+  const auto e_ss = P::grp4(-(v + (G)k::mssV1) * (G)(1.0 / k::mssV2), (v + (G)k::hssV1) * (G)(1.0 / k::hssV2),
                            -(v + (G)42.85) * (G)(1.0 / 5.264), (v + (G)87.61) * (G)(1.0 / 7.488));
-  const G mss = P::rc((one + e_ss.a));
+  const G mss = P::rc((one + e_ss.a()));
   const Tau<P> tm = tau_quot<P>(1.0, (esum<P>((G)k::mtD1, (v + (G)k::mtV1) * (G)(1.0 / k::mtV2), (G)k::mtD2, -(v + (G)k::mtV3) * (G)(1.0 / k::mtV4))));
-  const G e_hss = e_ss.b;
+  const G e_hss = e_ss.b();
   const G hss = P::rc((one + e_hss));
   const Tau<P> thf = tau_quot<P>(1.0, (esum<P>((G)1.432e-05, -(v + (G)1.196) * (G)(1.0 / 6.285), (G)6.149, (v + (G)0.5096) * (G)(1.0 / 20.27))));
   const Tau<P> ths = tau_quot<P>(1.0, (esum<P>((G)0.009794, -(v + (G)17.95) * (G)(1.0 / 28.05), (G)0.3343, (v + (G)5.73) * (G)(1.0 / 56.66))));
@@ -331,8 +331,8 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   static_assert(k::hssV1 == 82.9 && k::hssV2 == 6.086, "hssp_shift assumes hss = 1/(1+e^((V+82.9)/6.086))");
   const G hssp = P::kFast ? P::rc(one + e_hss * (G)k::hssp_shift)
                            : P::rc((one + P::ex((v + (G)89.1) * (G)(1.0 / 6.086))));
-  const G mLss = P::rc((one + e_ss.c));
-  const G e_hL = e_ss.d;
+  const G mLss = P::rc((one + e_ss.c()));
+  const G e_hL = e_ss.d();
   const G hLss = P::rc((one + e_hL));
   const G hLssp = P::kFast ? P::rc(one + e_hL * (G)k::hLssp_shift)
                             : P::rc((one + P::ex((v + (G)93.81) * (G)(1.0 / 7.488))));
@@ -353,10 +353,10 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   // nao/Knao and nai/Knai: in mixed, nao/Knao0 e^(-c v) without a division
   G nao_Knao, nai_Knai;
   if constexpr (P::kFast) {
-    const auto e_nak = P::ex2(-((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)),
+    const auto e_nak = P::grp2(-((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)),
                               -((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
-    nao_Knao = (G)(k::nao / k::Knao0) * e_nak.a;
-    nai_Knai = nai_g * (G)(1.0 / k::Knai0) * e_nak.b;
+    nao_Knao = (G)(k::nao / k::Knao0) * e_nak.a();
+    nai_Knai = nai_g * (G)(1.0 / k::Knai0) * e_nak.b();
   } else {
     const G Knao = (G)k::Knao0 * P::ex(((one - (G)k::delta) * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
     const G Knai = (G)k::Knai0 * P::ex(((G)k::delta * v * (G)k::F) * (G)(1.0 / (3.0 * k::R * k::T)));
@@ -385,14 +385,14 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   // IK1 with its gate xk1: carried by this group, which is the lighter of
   // the two in the pairs form and in the four-role form (the K group has
   // the longest dependency chain)
-  const auto e_k1 = P::ex2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
+  const auto e_k1 = P::grp2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
                            ((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493));
-  const G xk1ss = P::rc((one + e_k1.a));
+  const G xk1ss = P::rc((one + e_k1.a()));
   const Tau<P> txk1 =
       tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
   const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
                          : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
-  const G rk1 = P::rc((one + e_k1.b));
+  const G rk1 = P::rc((one + e_k1.b()));
   const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
   o.f[S_iV] = INa + INaL + INaK + INab + IK1;
   o.f[S_iNa] = INa + INaL + (G)3.0 * INaK + INab;
@@ -421,30 +421,30 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   using G = typename P::G;
   const G v = c.v, one = (G)1;
   // the group's single exponentials, four per call
-  const auto e_k1 = P::ex4(-(v - (G)14.34) * (G)(1.0 / 14.82), -(v - (G)18.4099) * (G)(1.0 / 29.3814),
+  const auto e_k1 = P::grp4(-(v - (G)14.34) * (G)(1.0 / 14.82), -(v - (G)18.4099) * (G)(1.0 / 29.3814),
                            (v + (G)100.0) * (G)(1.0 / 29.3814), (v + (G)43.94) * (G)(1.0 / 5.711));
-  const auto e_k2 = P::ex4(-(v + (G)11.60) * (G)(1.0 / 8.932), -(v - (G)14.48) * (G)(1.0 / 18.34),
+  const auto e_k2 = P::grp4(-(v + (G)11.60) * (G)(1.0 / 8.932), -(v - (G)14.48) * (G)(1.0 / 18.34),
                            (v - (G)213.6) * (G)(1.0 / 151.2), (v + (G)70.0) * (G)0.05);
-  const G e_a = e_k1.a;
+  const G e_a = e_k1.a();
   const G ass = P::rc((one + e_a));
-  const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + e_k1.b))) + P::dv((G)3.5, (one + e_k1.c))));
+  const Tau<P> ta = tau_quot<P>(1.0515, (P::rc(((G)1.2089 * (one + e_k1.b()))) + P::dv((G)3.5, (one + e_k1.c()))));
   const G assp = P::kFast ? P::rc(one + e_a * (G)k::assp_shift)
                            : P::rc((one + P::ex(-(v - (G)24.34) * (G)(1.0 / 14.82))));
-  const G iss = P::rc((one + e_k1.d));
+  const G iss = P::rc((one + e_k1.d()));
   const G delta_epi = q.celltype == 1 ? one - P::dv((G)0.95, (one + P::ex((v + (G)70.0) * (G)0.2))) : one;
   const Tau<P> tiF = tau_affine<P>(4.562, (esum<P>((G)0.3933, -(v + (G)100.0) * (G)0.01, (G)0.08004, (v + (G)50.0) * (G)(1.0 / 16.59))), delta_epi);
   const Tau<P> tiS = tau_affine<P>(23.62, (esum<P>((G)0.001416, -(v + (G)96.52) * (G)(1.0 / 59.05), (G)1.78e-08, (v + (G)114.1) * (G)(1.0 / 8.079))), delta_epi);
   const G dti_develop = (G)1.354 + P::dv((G)1e-4, (esum<P>((G)1, (v - (G)167.4) * (G)(1.0 / 15.89), (G)1, -(v - (G)12.23) * (G)(1.0 / 0.2154))));
-  const G dti_recover = one - P::dv((G)0.5, (one + e_k2.d));
+  const G dti_recover = one - P::dv((G)0.5, (one + e_k2.d()));
   const G dti = dti_develop * dti_recover;
-  const G xs1ss = P::rc((one + e_k2.a));
+  const G xs1ss = P::rc((one + e_k2.a()));
   const Tau<P> txs1 = tau_affine<P>(817.3, (esum<P>((G)2.326e-04, (v + (G)48.28) * (G)(1.0 / 17.80), (G)0.001292, -(v + (G)210.0) * (G)(1.0 / 230.0))));
   const Tau<P> txs2 =
       tau_quot<P>(1.0, (esum<P>((G)0.01, (v - (G)50.0) * (G)0.05, (G)0.0193, -(v + (G)66.54) * (G)(1.0 / 31.0))));
   const G fp_ = c.fCaMKp;
   const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
                          : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
-  const G AiF = P::rc((one + e_k2.c));
+  const G AiF = P::rc((one + e_k2.c()));
   const G AiS = one - AiF;
   const G i_ = AiF * (G)y.iF + AiS * (G)y.iS;
   const G ip = AiF * (G)y.iFp + AiS * (G)y.iSp;
@@ -452,15 +452,15 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   G IKr = (G)0, xrss = (G)0;
   Tau<P> txrf = tau_const<P>(1.0), txrs = tau_const<P>(1.0);
   if constexpr (!kCipa) {
-    const auto e_kr = P::ex4(-(v + (G)8.337) * (G)(1.0 / 6.789), (v + (G)54.81) * (G)(1.0 / 38.21),
+    const auto e_kr = P::grp4(-(v + (G)8.337) * (G)(1.0 / 6.789), (v + (G)54.81) * (G)(1.0 / 38.21),
                              (v + (G)55.0) * (G)(1.0 / 75.0), (v - (G)10.0) * (G)(1.0 / 30.0));
-    xrss = P::rc((one + e_kr.a));
+    xrss = P::rc((one + e_kr.a()));
     txrf = tau_affine<P>(12.98, (esum<P>((G)0.3652, (v - (G)31.66) * (G)(1.0 / 3.869), (G)4.123e-05, -(v - (G)47.78) * (G)(1.0 / 20.38))));
     txrs = tau_affine<P>(1.865, (esum<P>((G)0.06629, (v - (G)34.70) * (G)(1.0 / 7.355), (G)1.128e-05, -(v - (G)29.74) * (G)(1.0 / 25.94))));
-    const G Axrf = P::rc((one + e_kr.b));
+    const G Axrf = P::rc((one + e_kr.b()));
     const G xr = Axrf * (G)y.xrf + (one - Axrf) * (G)y.xrs;
-    const G rkr = P::kFast ? P::rc((one + e_kr.c) * (one + e_kr.d))
-                            : P::dv((P::rc((one + e_kr.c))), (one + e_kr.d));
+    const G rkr = P::kFast ? P::rc((one + e_kr.c()) * (one + e_kr.d()))
+                            : P::dv((P::rc((one + e_kr.c()))), (one + e_kr.d()));
     IKr = q.GKr * (G)k::sqrt_ko54 * xr * rkr * (v - EK);
   }
   const G EKs = P::kFast
@@ -470,7 +470,7 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
                      ? one + P::dv((G)0.6, (one + P::ex((G)1.4 * ((G)k::log_ks_ca - P::lg((G)y.cai)))))
                      : one + P::dv((G)0.6, (one + P::pw(P::dv((G)3.8e-05, (G)y.cai), (G)1.4)));
   const G IKs = q.GKs * KsCa * (G)y.xs1 * (G)y.xs2 * (v - EKs);
-  const G xkb = P::rc((one + e_k2.b));
+  const G xkb = P::rc((one + e_k2.b()));
   const G IKb = q.GKb * xkb * (v - EK);
   const G Istim = c.stim ? (G)q.amp : (G)0;
   o.f[S_iV] = Ito + IKr + IKs + IKb + Istim;
@@ -500,10 +500,10 @@ __device__ __forceinline__ void role_ca(Y<typename P::G> &y, const Par<typename 
                                         double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
   const G v = c.v, one = (G)1;
-  const auto e_ca = P::ex2(-(v + (G)3.94) * (G)(1.0 / 4.23), (v + (G)19.58) * (G)(1.0 / 3.696));
-  const G dss = P::rc((one + e_ca.a));
+  const auto e_ca = P::grp2(-(v + (G)3.94) * (G)(1.0 / 4.23), (v + (G)19.58) * (G)(1.0 / 3.696));
+  const G dss = P::rc((one + e_ca.a()));
   const Tau<P> td = tau_affine<P>(0.6, (esum<P>((G)1, (G)-0.05 * (v + (G)6.0), (G)1, (G)0.09 * (v + (G)14.0))));
-  const G fss = P::rc((one + e_ca.b));
+  const G fss = P::rc((one + e_ca.b()));
   const Tau<P> tff = tau_affine<P>(7.0, (esum<P>((G)0.0045, -(v + (G)20.0) * (G)0.1, (G)0.0045, (v + (G)20.0) * (G)0.1)));
   const Tau<P> tfs = tau_affine<P>(1000.0, (esum<P>((G)3.5e-05, -(v + (G)5.0) * (G)0.25, (G)3.5e-05, (v + (G)5.0) * (G)(1.0 / 6.0))));
   const Tau<P> tfcaf = tau_affine<P>(7.0, (esum<P>((G)0.04, -(v - (G)4.0) * (G)(1.0 / 7.0), (G)0.04, (v - (G)4.0) * (G)(1.0 / 7.0))));
@@ -692,9 +692,9 @@ __device__ __forceinline__ void role_x(Y<typename P::G> &y, const Par<typename P
                                        double dt, bool update, Part<typename P::G> &o) {
   using G = typename P::G;
   const G v = c.v, one = (G)1;
-  const auto e_x = P::ex2(((G)k::qna * v) * (G)k::FRT, ((G)k::qca * v) * (G)k::FRT);
-  const G hna = e_x.a;
-  const G hca = e_x.b;
+  const auto e_x = P::grp2(((G)k::qna * v) * (G)k::FRT, ((G)k::qca * v) * (G)k::FRT);
+  const G hna = e_x.a();
+  const G hca = e_x.b();
   const G h7 = one + ((G)k::nao / (G)k::kna3) * (one + P::rc(hna));
   const G h8 = P::dv((G)k::nao, ((G)k::kna3 * hna * h7));
   const G k3pp = h8 * (G)k::wnaca;

@@ -14,11 +14,13 @@
 //      start again from their initial state in an FP64 batch on a second
 //      stream, concurrently with the mixed batch's remaining paces;
 //   3. an instance whose evaluated record still shows a diastolic Vm above
-//      the threshold, an APD90 above 0.9 BCL or an evaluated beat without
-//      an action potential (n_eligible below the evaluated paces: a cell at
-//      the edge of 2:1 block, whose beat-to-beat dynamics can settle into
-//      different regimes under FP32 and FP64 rounding) runs again in FP64
-//      after both batches finish.
+//      the threshold, an APD90 above 0.9 BCL or an intermittent rhythm
+//      (some evaluated beats with an action potential at the peak sample
+//      and some without: a cell at the edge of 2:1 block, whose
+//      beat-to-beat dynamics can settle into different regimes under FP32
+//      and FP64 rounding) runs again in FP64 after both batches finish. A
+//      cell whose upstroke misses the peak sample in every beat (a strong
+//      sodium block) has no APD in either precision and is not re-run.
 // The FP64 records replace the mixed ones; refined[i] says which path
 // produced instance i's record.
 #include <cuda_runtime.h>
@@ -160,7 +162,7 @@ extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_
     const int evaluated = j->first_pace >= 0 ? j->n_pace - j->first_pace : 0;
     for (int i = 0; i < j->n; ++i)
       if (how[i] == 0 && (!(out[i].vm_valley < j->refine_above_vm) || out[i].apd90 > kNearBlock * j->bcl ||
-                          out[i].n_eligible < evaluated))
+                          (out[i].n_eligible > 0 && out[i].n_eligible < evaluated)))
         late.push_back(i);
     if (!late.empty()) {
       Batch c;

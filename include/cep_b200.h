@@ -239,9 +239,9 @@ int cep_batch_rates_all(cep_batch_t b, double t, double *rates);
  * that do not repolarise, whose APD90 FP32 gates cannot hold) run from
  * their initial state in FP64 on a second stream concurrently with the
  * mixed population, and any instance whose evaluated record still shows a
- * diastolic Vm above it, an APD90 above 0.9 BCL or an evaluated beat
- * without an action potential (n_eligible below the evaluated paces: the
- * edge of 2:1 block, whose regime FP32 rounding can change) runs again in FP64
+ * diastolic Vm above it, an APD90 above 0.9 BCL or an intermittent rhythm
+ * (0 < n_eligible < the evaluated paces: the edge of 2:1 block, whose
+ * regime FP32 rounding can change) runs again in FP64
  * afterwards (refined[i] = 1 concurrent, 2 afterwards). refine_above_vm =
  * NaN (or CEP_PREC_FP64) runs the single precision alone. No counterpart
  * in the reference beyond the loop it replaces. Blocking. */

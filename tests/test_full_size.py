@@ -141,7 +141,8 @@ def test_cipa_long_protocol_refined_mixed_meets_bars(cep, gpu):
     at the edge of 2:1 block (APD90 near the BCL), where FP32 and FP64
     rounding can settle the beat sequence into different regimes; the
     compliant path re-runs in FP64 every record with APD90 above 0.9 BCL or
-    an evaluated beat without an action potential."""
+    an intermittent rhythm (some evaluated beats without an action
+    potential at the peak sample)."""
     import threading
     from test_cipa_gpu import cipa_population
     conc, hill = cipa_population(500, 5, seed=1234)
