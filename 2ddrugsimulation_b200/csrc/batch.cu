@@ -399,7 +399,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
       ord::role<P, M::kCipa, R>(y, q, ctx, a.dt, upd, p);
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(R, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(R, f);
         if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
       }
     }
@@ -408,7 +408,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
       ord::role<P, M::kCipa, R2>(y, q, ctx, a.dt, upd, p);
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(R2, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(R2, f);
         if (fld >= 0) part[buf][R2][f][lane] = p.f[fld];
       }
     }
@@ -420,7 +420,7 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
     for (int r = 0; r < 4; ++r) {
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(r, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(r, f);
         if (fld >= 0) s.f[fld] += part[buf][r][f][lane];
       }
     }
@@ -446,8 +446,8 @@ __device__ __forceinline__ void role_loop(const RunArgs &a, typename P::G (*part
   }
   if (valid) {
     if (bm_on) bm::hot_store(a.bv, i, hot);
-    ord::store_role<M::kCipa>(R, y, a.y, a.ld, i);
-    if constexpr (R2 >= 0) ord::store_role<M::kCipa>(R2, y, a.y, a.ld, i);
+    ord::store_role<M::kCipa, ord::kIK1InNa<P>>(R, y, a.y, a.ld, i);
+    if constexpr (R2 >= 0) ord::store_role<M::kCipa, ord::kIK1InNa<P>>(R2, y, a.y, a.ld, i);
     if (R == 0) {
       a.t[i] = t;
       a.iout[i] = iout;

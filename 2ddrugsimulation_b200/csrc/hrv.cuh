@@ -356,7 +356,7 @@ __device__ __forceinline__ void role_calls(const Args &a, typename P::G (*part)[
       ord::role<P, false, R>(y, q, ctx, e.h, active && e.upd, p);
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(R, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(R, f);
         if (fld >= 0) part[buf][R][f][lane] = p.f[fld];
       }
     }
@@ -365,7 +365,7 @@ __device__ __forceinline__ void role_calls(const Args &a, typename P::G (*part)[
       ord::role<P, false, R2>(y, q, ctx, e.h, active && e.upd, p);
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(R2, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(R2, f);
         if (fld >= 0) part[buf][R2][f][lane] = p.f[fld];
       }
     }
@@ -377,7 +377,7 @@ __device__ __forceinline__ void role_calls(const Args &a, typename P::G (*part)[
     for (int r = 0; r < 4; ++r) {
 #pragma unroll
       for (int f = 0; f < 8; ++f) {
-        const int fld = ord::role_field(r, f);
+        const int fld = ord::role_field<ord::kIK1InNa<P>>(r, f);
         if (fld >= 0) s.f[fld] += part[buf][r][f][lane];
       }
     }
@@ -393,8 +393,8 @@ __device__ __forceinline__ void role_calls(const Args &a, typename P::G (*part)[
   }
   if (valid && (alive || st != CEP_INST_RUNNING)) {
     if (bm_on) hot_store(v, i, h);
-    ord::store_role<false>(R, y, a.y, a.ld, i);
-    if constexpr (R2 >= 0) ord::store_role<false>(R2, y, a.y, a.ld, i);
+    ord::store_role<false, ord::kIK1InNa<P>>(R, y, a.y, a.ld, i);
+    if constexpr (R2 >= 0) ord::store_role<false, ord::kIK1InNa<P>>(R2, y, a.y, a.ld, i);
     if (R == 0) {
       clock_store(v, i, k);
       if (st != CEP_INST_RUNNING) v.I(I_status, i) = st;

@@ -222,9 +222,11 @@ __device__ __forceinline__ bool stim_on(double t, double start, double bcl, doub
 // back to back) and the warp-specialised kernel (one warp per role for 32
 // cells, Parts exchanged through shared memory); both add the Parts in the
 // same order.
-//   role 0 (Na): m hf hs j hsp jp mL hL hLp xk1; INa, INaL, INab, INaK, IK1
+//   role 0 (Na): m hf hs j hsp jp mL hL hLp; INa, INaL, INab, INaK
 //   role 1 (K) : a iF iS ap iFp iSp xs1 xs2 (ORd: xrf xrs); Ito, IKs, IKb,
 //                IKr (ORd), Istim
+//   xk1 and IK1 go to role 0 in FP64 and to role 1 in the mixed path
+//   (kIK1InNa)
 //   role 2 (Ca): d ff fs fcaf fcas jca ffp fcafp nca Jrelnp Jrelp; ICaL, ICaNa,
 //                ICaK, ICab, IpCa, Jrel
 //   role 3 (X) : INaCa_i, INaCa_ss, Jup; CiPA: the Markov IKr chain and IKr
@@ -250,14 +252,27 @@ struct Part {
   G f[kNumSums];
 };
 
+// Where IK1 and its gate xk1 are evaluated: the Na group in FP64, where the
+// K group has the longest dependency chain of the four (measured with clock
+// stamps per group: 8,400 cycles per step against 6,000-7,000); the K group
+// in the mixed path, whose pairs form carries Na + Ca in one warp and K + the
+// rest in the other and is balanced that way.
+template <class P>
+inline constexpr bool kIK1InNa = !P::kMixed;
+
 // Fields each role writes, in the order of its packed shared-memory slot
 // (at most 8; -1 = unused).
+template <bool kIK1Na>
 __host__ __device__ constexpr int role_field(int role, int k) {
-  constexpr int t[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, S_IK1, -1, -1},
+  constexpr int a[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, S_IK1, -1, -1},
                            {S_iV, S_iK, S_Ito, S_IKr, S_IKs, -1, -1, -1},
                            {S_iV, S_iNass, S_iKss, S_iCass, S_iCai, S_Jrel, S_ICaL, -1},
                            {S_iV, S_iNa, S_iNass, S_iCass, S_iCai, S_Jup, S_IKr, S_iK}};
-  return t[role][k];
+  constexpr int b[4][8] = {{S_iV, S_iNa, S_iK, S_INa, S_INaL, -1, -1, -1},
+                           {S_iV, S_iK, S_Ito, S_IKr, S_IKs, S_IK1, -1, -1},
+                           {S_iV, S_iNass, S_iKss, S_iCass, S_iCai, S_Jrel, S_ICaL, -1},
+                           {S_iV, S_iNa, S_iNass, S_iCass, S_iCai, S_Jup, S_IKr, S_iK}};
+  return kIK1Na ? a[role][k] : b[role][k];
 }
 
 // Values every role needs at the start of a step.
@@ -311,8 +326,8 @@ __device__ __forceinline__ void ghk(double V, typename P::G v, typename P::G &fa
   }
 }
 
-// role 0: fast and late sodium, background sodium, Na/K pump; the inward
-// rectifier (which balances the groups' dependency chains)
+// role 0: fast and late sodium, background sodium, Na/K pump; in FP64 the
+// inward rectifier (kIK1InNa)
 template <class P, bool kCipa>
 __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                         double dt, bool update, Part<typename P::G> &o) {
@@ -382,26 +397,28 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
   const G JnakNa = (G)3.0 * (x1 * xs_inv * a3 - x2 * xs_inv * b3);
   const G JnakK = (G)2.0 * (x4 * xs_inv * (G)k::b1 - x3 * xs_inv * a1);
   const G INaK = q.Pnak * ((G)k::zna * JnakNa + (G)k::zk * JnakK);
-  // IK1 with its gate xk1: carried by this group, which is the lighter of
-  // the two in the pairs form and in the four-role form (the K group has
-  // the longest dependency chain)
-  const auto e_k1 = P::grp2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
-                           ((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493));
-  const G xk1ss = P::rc((one + e_k1.a()));
-  const Tau<P> txk1 =
-      tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
-  const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
-                         : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
-  const G rk1 = P::rc((one + e_k1.b()));
-  const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
-  o.f[S_iV] = INa + INaL + INaK + INab + IK1;
+  if constexpr (kIK1InNa<P>) {  // IK1 with its gate xk1 (see kIK1InNa)
+    const auto e_k1 = P::grp2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
+                              ((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493));
+    const G xk1ss = P::rc((one + e_k1.a()));
+    const Tau<P> txk1 =
+        tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
+    const G EK = P::kFast ? (G)k::RTF * ((G)k::log_ko - P::lg((G)y.ki))
+                           : (G)k::RTF * P::lg(P::dv((G)k::ko, (G)y.ki));
+    const G rk1 = P::rc((one + e_k1.b()));
+    const G IK1 = q.GK1 * (G)k::sqrt_ko * rk1 * (G)y.xk1 * (v - EK);
+    o.f[S_iV] = INa + INaL + INaK + INab + IK1;
+    o.f[S_iK] = IK1 - (G)2.0 * INaK;
+    o.f[S_IK1] = IK1;
+    if (update) y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
+  } else {
+    o.f[S_iV] = INa + INaL + INaK + INab;
+    o.f[S_iK] = -(G)2.0 * INaK;
+  }
   o.f[S_iNa] = INa + INaL + (G)3.0 * INaK + INab;
-  o.f[S_iK] = IK1 - (G)2.0 * INaK;
   o.f[S_INa] = INa;
   o.f[S_INaL] = INaL;
-  o.f[S_IK1] = IK1;
   if (!update) return;
-  y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
   y.m = rush_larsen<P>(y.m, mss, tm, dt);
   y.hf = rush_larsen<P>(y.hf, hss, thf, dt);
   y.hs = rush_larsen<P, true>(y.hs, hss, ths, dt);
@@ -414,7 +431,8 @@ __device__ __forceinline__ void role_na(Y<typename P::G> &y, const Par<typename 
 }
 
 // role 1: transient outward, slow/rapid (ORd) delayed rectifier and
-// background potassium currents; the stimulus
+// background potassium currents, in the mixed path the inward rectifier
+// (kIK1InNa); the stimulus
 template <class P, bool kCipa>
 __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P::G> &q, const Ctx<typename P::G> &c,
                                        double dt, bool update, Part<typename P::G> &o) {
@@ -473,12 +491,23 @@ __device__ __forceinline__ void role_k(Y<typename P::G> &y, const Par<typename P
   const G xkb = P::rc((one + e_k2.b()));
   const G IKb = q.GKb * xkb * (v - EK);
   const G Istim = c.stim ? (G)q.amp : (G)0;
-  o.f[S_iV] = Ito + IKr + IKs + IKb + Istim;
-  o.f[S_iK] = Ito + IKr + IKs + IKb + Istim;
+  G IK1 = (G)0, xk1ss = (G)0;
+  Tau<P> txk1 = tau_const<P>(1.0);
+  if constexpr (!kIK1InNa<P>) {  // IK1 with its gate xk1 (see kIK1InNa)
+    const auto e_ik1 = P::grp2(-(v + (G)k::xk1_off) * (G)(1.0 / k::xk1_den),
+                               ((v + (G)105.8) - (G)(2.6 * k::ko)) * (G)(1.0 / 9.493));
+    xk1ss = P::rc((one + e_ik1.a()));
+    txk1 = tau_quot<P>(122.2, (esum<P>((G)1, -(v + (G)127.2) * (G)(1.0 / 20.36), (G)1, (v + (G)236.8) * (G)(1.0 / 69.33))));
+    IK1 = q.GK1 * (G)k::sqrt_ko * P::rc((one + e_ik1.b())) * (G)y.xk1 * (v - EK);
+    o.f[S_IK1] = IK1;
+  }
+  o.f[S_iV] = Ito + IKr + IKs + IK1 + IKb + Istim;
+  o.f[S_iK] = Ito + IKr + IKs + IK1 + IKb + Istim;
   o.f[S_Ito] = Ito;
   o.f[S_IKr] = IKr;
   o.f[S_IKs] = IKs;
   if (!update) return;
+  if constexpr (!kIK1InNa<P>) y.xk1 = rush_larsen<P, true>(y.xk1, xk1ss, txk1, dt);
   y.a = rush_larsen<P, true>(y.a, ass, ta, dt);
   y.iF = rush_larsen<P, true>(y.iF, iss, tiF, dt);
   y.iS = rush_larsen<P, true>(y.iS, iss, tiS, dt);
@@ -804,11 +833,11 @@ __device__ __forceinline__ void role(Y<typename P::G> &y, const Par<typename P::
 }
 
 // Sum of the four roles' contributions, in role order (both kernels).
-template <class G>
+template <bool kIK1Na, class G>
 __device__ __forceinline__ void add_part(Part<G> &s, const Part<G> &p, int role) {
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    const int f = role_field(role, k);
+    const int f = role_field<kIK1Na>(role, k);
     if (f >= 0) s.f[f] += p.f[f];
   }
 }
@@ -873,25 +902,32 @@ __device__ __forceinline__ void step(Y<typename P::G> &y, const Par<typename P::
   role<P, kCipa, 1>(y, q, c, dt, update, p[1]);
   role<P, kCipa, 2>(y, q, c, dt, update, p[2]);
   role<P, kCipa, 3>(y, q, c, dt, update, p[3]);
-  add_part(s, p[0], 0);
-  add_part(s, p[1], 1);
-  add_part(s, p[2], 2);
-  add_part(s, p[3], 3);
+  add_part<kIK1InNa<P>>(s, p[0], 0);
+  add_part<kIK1InNa<P>>(s, p[1], 1);
+  add_part<kIK1InNa<P>>(s, p[2], 2);
+  add_part<kIK1InNa<P>>(s, p[3], 3);
   combine<P>(y, q, s, dt, update, cur);
 }
 // Store only the states a role owns (the warp-specialised kernel: each warp
 // holds stale copies of the other roles' gates). Role 0 also owns the FP64
-// states every role carries (V, CaMKt, ions).
-template <bool kCipa, class G>
+// states every role carries (V, CaMKt, ions); xk1 belongs to the group that
+// evaluates IK1 (kIK1Na: the Na group).
+template <bool kCipa, bool kIK1Na, class G>
 __device__ __forceinline__ void store_role(int role, const Y<G> &y, double *__restrict__ s, int64_t ld, int64_t i) {
 #define CEP_ST_ORD(n) s[n * ld + i] = y.n;
 #define CEP_ST_CIPA(n) s[cipa::n * ld + i] = y.n;
+  if (role == (kIK1Na ? 0 : 1)) {
+    if constexpr (kCipa)
+      CEP_ST_CIPA(xk1)
+    else
+      CEP_ST_ORD(xk1)
+  }
   if constexpr (!kCipa) {
     if (role == 0) {
       CEP_ST_ORD(V) CEP_ST_ORD(CaMKt) CEP_ST_ORD(cass) CEP_ST_ORD(nai) CEP_ST_ORD(nass) CEP_ST_ORD(ki)
       CEP_ST_ORD(kss) CEP_ST_ORD(cansr) CEP_ST_ORD(cajsr) CEP_ST_ORD(cai)
       CEP_ST_ORD(m) CEP_ST_ORD(hf) CEP_ST_ORD(hs) CEP_ST_ORD(j) CEP_ST_ORD(hsp) CEP_ST_ORD(jp) CEP_ST_ORD(mL)
-      CEP_ST_ORD(hL) CEP_ST_ORD(hLp) CEP_ST_ORD(xk1)
+      CEP_ST_ORD(hL) CEP_ST_ORD(hLp)
     } else if (role == 1) {
       CEP_ST_ORD(a) CEP_ST_ORD(iF) CEP_ST_ORD(iS) CEP_ST_ORD(ap) CEP_ST_ORD(iFp) CEP_ST_ORD(iSp)
       CEP_ST_ORD(xs1) CEP_ST_ORD(xs2) CEP_ST_ORD(xrf) CEP_ST_ORD(xrs)
@@ -904,7 +940,7 @@ __device__ __forceinline__ void store_role(int role, const Y<G> &y, double *__re
       CEP_ST_CIPA(V) CEP_ST_CIPA(CaMKt) CEP_ST_CIPA(cass) CEP_ST_CIPA(nai) CEP_ST_CIPA(nass) CEP_ST_CIPA(ki)
       CEP_ST_CIPA(kss) CEP_ST_CIPA(cansr) CEP_ST_CIPA(cajsr) CEP_ST_CIPA(cai)
       CEP_ST_CIPA(m) CEP_ST_CIPA(hf) CEP_ST_CIPA(hs) CEP_ST_CIPA(j) CEP_ST_CIPA(hsp) CEP_ST_CIPA(jp)
-      CEP_ST_CIPA(mL) CEP_ST_CIPA(hL) CEP_ST_CIPA(hLp) CEP_ST_CIPA(xk1)
+      CEP_ST_CIPA(mL) CEP_ST_CIPA(hL) CEP_ST_CIPA(hLp)
     } else if (role == 1) {
       CEP_ST_CIPA(a) CEP_ST_CIPA(iF) CEP_ST_CIPA(iS) CEP_ST_CIPA(ap) CEP_ST_CIPA(iFp) CEP_ST_CIPA(iSp)
       CEP_ST_CIPA(xs1) CEP_ST_CIPA(xs2)
