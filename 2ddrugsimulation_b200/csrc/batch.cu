@@ -972,40 +972,9 @@ RunArgs make_args(cep_batch *b, long n_steps) {
   return a;
 }
 
-// out[i] = the FP64 policy's exponential of x[i], ref[i] = CUDA's exp
-__global__ void exp_check_kernel(const double *__restrict__ x, double *__restrict__ out, double *__restrict__ ref,
-                                 int64_t n) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  out[i] = F64::ex(x[i]);
-  ref[i] = ::exp(x[i]);
-}
-
 }  // namespace
 
 extern "C" {
-
-// Test hook: the FP64 exponential the models use (out) and CUDA's exp
-// (ref) of n host values, on a private stream.
-int cep_internal_exp_f64(const double *x, int64_t n, double *out, double *ref) {
-  if (!x || !out || !ref || n <= 0 || n > (int64_t(1) << 28)) return fail(CEP_ERR_ARG, "bad exp check arguments");
-  cudaStream_t s = nullptr;
-  double *d = nullptr;
-  CEP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  cudaError_t e = cudaMalloc(&d, sizeof(double) * 3 * n);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d, x, sizeof(double) * n, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) {
-    exp_check_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d, d + n, d + 2 * n, n);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ref, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (d) cudaFree(d);
-  cudaStreamDestroy(s);
-  if (e != cudaSuccess) return fail(CEP_ERR_CUDA, "exp check: %s", cudaGetErrorString(e));
-  return CEP_OK;
-}
 
 const char *cep_version(void) { return "cep_b200 0.1 (sm_100a)"; }
 const char *cep_last_error(void) { return g_last_error.c_str(); }

@@ -1,10 +1,9 @@
 // Shared device-side definitions for the ionic-model kernels.
 //
 // Two precision policies drive every model template:
-//   F64   - plain FP64 path: every quantity in double, exp within 0.51 ulp
-//           (exp_tab), CUDA's log (<= 1 ulp); the ORd family takes the
-//           algebraic rewrites below (CEP_F64_REWRITES), the other models
-//           the reference's forms.
+//   F64   - plain FP64 path: every quantity in double, CUDA's double exp/log
+//           (<= 1 ulp); the ORd family takes the algebraic rewrites below
+//           (CEP_F64_REWRITES), the other models the reference's forms.
 //   Mixed - gates, rate constants and channel currents in FP32 with SFU
 //           exp/log (ex2.approx / lg2.approx) and approximate division; the
 //           membrane voltage, the ionic concentrations, CaMKII and every
@@ -12,8 +11,6 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
-
-#include "exp2_table.cuh"
 
 namespace cep {
 
@@ -64,9 +61,15 @@ __device__ __noinline__ double div64_special(double a, double b) {
 // a / b as a * (1/b) with one residual correction (q + r (a - b q)), within
 // an ulp of the correctly rounded quotient for divisors of magnitude up to
 // 2^1021 (every division of the models here); IEEE results for zero,
-// subnormal, infinite and NaN operands.
+// subnormal, infinite and NaN operands. 1/b takes one Newton-Raphson step
+// from the seed (relative error e^2 for a seed error e <= 2^-20), which the
+// correction squares again: q + r (a - b q) = (a/b)(1 - e^4) up to the
+// roundings of q and of the result. Zero, subnormal and infinite divisors
+// end in NaN as in rcp64_nr.
 __device__ __forceinline__ double div64(double a, double b) {
-  const double r = rcp64_nr(b);
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+  r = fma(r, fma(-b, r, 1.0), r);
   const double q = a * r;
   const double out = fma(r, fma(-b, q, a), q);
   return isnan(out) ? div64_special(a, b) : out;
@@ -82,63 +85,18 @@ __device__ __forceinline__ double div64(double a, double b) {
 #define CEP_F64_REWRITES 1
 #endif
 
-// The FP64 exponential. CEP_F64_EXP_TABLE=1 (the default) evaluates it by
-// the table-driven method of P. T. P. Tang ("Table-driven implementation of
-// the exponential function in IEEE floating-point arithmetic", ACM TOMS
-// 15(2), 1989), with N = 64 and a Taylor polynomial: eleven dependent FP64
-// operations. CEP_F64_EXP_TABLE=0 calls CUDA's exp.
-#ifndef CEP_F64_EXP_TABLE
-#define CEP_F64_EXP_TABLE 1
-#endif
-
-// e^x for the arguments the table path does not take (|x| >= 707, NaN).
-__device__ __noinline__ double exp_wide(double x) { return ::exp(x); }
-
-// e^x = 2^m 2^(j/64) e^r with x = (64 m + j) ln2/64 + r, |r| <= ln2/128:
-// k = 64 m + j is x 64/ln2 rounded to the nearest integer (the 1.5 2^52
-// shift), r = x - k ln2/64 with ln2/64 split in two parts (each product by
-// an FMA, so r carries no cancellation error), 2^(j/64) = hi + lo from
-// exp2_table.cuh, e^r - 1 = r + r^2 (1/2 + r/6 + ... + r^4/720) (the
-// omitted terms are below r^7/5040 < 3e-20), and 2^m added to the exponent
-// field (the result stays normal for |x| < 707). The result is
-// hi + (lo + hi (e^r - 1)) rounded once: 0.51 ulp from e^x at worst over
-// 52,000 arguments checked against 50-digit values, correctly rounded for
-// 99.85 % of them.
-__device__ __forceinline__ double exp_tab(double x) {
-  // |x| < 707 on the high word (707 = 0x40861800'00000000); NaN fails too
-  if ((__double2hiint(x) & 0x7fffffff) >= 0x40861800) return exp_wide(x);
-  const double shift = 0x1.8p52;
-  const double t = fma(x, exp2tab::kInvStep, shift);
-  const int k = __double2loint(t);
-  const double kd = t - shift;
-  const double r = fma(-kd, exp2tab::kStepLo, fma(-kd, exp2tab::kStepHi, x));
-  const double2 tb = __ldg(&exp2tab::kTab[k & 63]);
-  const double r2 = r * r;
-  const double c = fma(fma(fma(fma(r, 1.0 / 720.0, 1.0 / 120.0), r, 1.0 / 24.0), r, 1.0 / 6.0), r, 0.5);
-  const double em1 = fma(r2, c, r);
-  const double s = tb.x + fma(tb.x, em1, tb.y);
-  return __hiloint2double(__double2hiint(s) + ((k >> 6) << 20), __double2loint(s));
-}
-__device__ __forceinline__ double exp_inl(double x) {
-#if CEP_F64_EXP_TABLE
-  return exp_tab(x);
-#else
-  return ::exp(x);
-#endif
-}
-
-// exp and log called out of line: each inlined copy of CUDA's is a few
+// CUDA's double exp and log called out of line: each inlined copy is a few
 // dozen instructions, and the ORd family's FP64 step calls them ~130 times,
 // which made the step's code too large for the instruction caches
 // (no_instruction stalls 6 cycles per issued instruction in the 2-warp form);
 // one shared copy of each keeps it resident (about 2x the FP64 throughput).
-__device__ __noinline__ double exp_f64(double x) { return exp_inl(x); }
+__device__ __noinline__ double exp_f64(double x) { return ::exp(x); }
 __device__ __noinline__ double log_f64(double x) { return ::log(x); }
 
 // Two exponentials of independent arguments in one out-of-line body, where
 // the two instruction streams interleave: one call's latency for two
 // results (the ORd family's time constants are sums of two exponentials).
-__device__ __noinline__ double2 exp2_f64(double a, double b) { return make_double2(exp_inl(a), exp_inl(b)); }
+__device__ __noinline__ double2 exp2_f64(double a, double b) { return make_double2(::exp(a), ::exp(b)); }
 
 template <class G>
 struct Exp2 {
@@ -151,7 +109,7 @@ struct Dbl4 {
   double a, b, c, d;
 };
 __device__ __noinline__ __attribute__((const)) Dbl4 exp4_f64(double a, double b, double c, double d) {
-  return Dbl4{exp_inl(a), exp_inl(b), exp_inl(c), exp_inl(d)};
+  return Dbl4{::exp(a), ::exp(b), ::exp(c), ::exp(d)};
 }
 // A group of independent exponentials read through a(), b(), ...: FP64
 // evaluates them together in one out-of-line call (their chains overlap);
