@@ -126,6 +126,8 @@ _SIGS = {
     "cep_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_fem_set_wait_test": (ctypes.c_int, [ctypes.c_long, ctypes.c_uint]),
     "cep_population_run": (ctypes.c_int, [ctypes.POINTER(PopulationJob), ctypes.c_void_p, _ip]),
+    "cep_population_late_mask": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_int, _ip]),
     "cep_batch_run_to_end": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     "cep_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "cep_batch_set_states": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int]),
@@ -595,6 +597,26 @@ def run_population(model: str, conc, hill, bcl: float, dt: float, n_pace: int, f
     out["refined"] = how > 0
     out["refined_how"] = how
     return out
+
+
+def population_late_mask(records: dict, refine_above_vm: float, bcl: float, evaluated: int) -> np.ndarray:
+    """Which mixed records run_population re-runs in FP64 after the run
+    (cep_population_late_mask): a diastolic Vm not below refine_above_vm, an
+    APD90 above 0.9 bcl, or an intermittent rhythm (0 < n_eligible <
+    evaluated). records: a dict of arrays keyed like run_population's result
+    (the fields a missing key stands for are 0)."""
+    n = len(records["vm_valley"])
+    if n == 0:
+        return np.zeros(0, bool)
+    arr = (Biomarkers * n)()
+    raw = np.ctypeslib.as_array(arr)
+    for f in BM_FIELDS + ("steepest_pace", "n_eligible", "status"):
+        if f in records:
+            raw[f] = np.asarray(records[f])
+    mask = np.zeros(n, np.int32)
+    _check(lib().cep_population_late_mask(ctypes.cast(arr, ctypes.c_void_p), n, refine_above_vm, bcl, evaluated,
+                                          mask.ctypes.data_as(_ip)))
+    return mask.astype(bool)
 
 
 def qinward(control: Biomarkers, drug: Biomarkers) -> float:

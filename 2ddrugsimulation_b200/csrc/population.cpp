@@ -105,6 +105,21 @@ long launches_left(const cep_population_job_t *j, long done, long spl) {
 
 }  // namespace
 
+extern "C" int cep_population_late_mask(const cep_biomarkers_t *recs, int n, double refine_above_vm, double bcl,
+                                        int evaluated, int *mask) {
+  if (n < 0 || (n > 0 && (!recs || !mask))) return fail(CEP_ERR_ARG, "null records or mask");
+  if (!(bcl > 0) || evaluated < 0) return fail(CEP_ERR_ARG, "bcl must be positive and evaluated >= 0");
+  constexpr double kNearBlock = 0.9;  // APD90 / BCL above which a beat is at the edge of block
+  for (int i = 0; i < n; ++i) {
+    const cep_biomarkers_t &r = recs[i];
+    mask[i] = (!(r.vm_valley < refine_above_vm) || r.apd90 > kNearBlock * bcl ||
+               (r.n_eligible > 0 && r.n_eligible < evaluated))
+                  ? 1
+                  : 0;
+  }
+  return CEP_OK;
+}
+
 extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_t *out, int *refined) {
   if (!j || !out) return fail(CEP_ERR_ARG, "null argument");
   if (j->n <= 0 || !(j->bcl > 0) || !(j->dt > 0) || j->n_pace <= 0)
@@ -157,13 +172,11 @@ extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_
     }
   }
   if (refine) {  // 3. whatever the screening missed
-    std::vector<int> late;
-    constexpr double kNearBlock = 0.9;  // APD90 / BCL above which a beat is at the edge of block
+    std::vector<int> late, mask(j->n);
     const int evaluated = j->first_pace >= 0 ? j->n_pace - j->first_pace : 0;
+    if ((rc = cep_population_late_mask(out, j->n, j->refine_above_vm, j->bcl, evaluated, mask.data()))) return rc;
     for (int i = 0; i < j->n; ++i)
-      if (how[i] == 0 && (!(out[i].vm_valley < j->refine_above_vm) || out[i].apd90 > kNearBlock * j->bcl ||
-                          (out[i].n_eligible > 0 && out[i].n_eligible < evaluated)))
-        late.push_back(i);
+      if (how[i] == 0 && mask[i]) late.push_back(i);
     if (!late.empty()) {
       Batch c;
       if ((rc = make_batch(j, CEP_PREC_FP64, late, sb.s, c))) return rc;

@@ -266,6 +266,13 @@ typedef struct {
  * record, 1 for an FP64 record of a screened instance, 2 for one re-run
  * after the mixed run. */
 int cep_population_run(const cep_population_job_t *job, cep_biomarkers_t *out, int *refined);
+/* The rule of step 3 above on n mixed records, for callers that run their
+ * own batches: mask[i] = 1 when record i shows a diastolic Vm not below
+ * refine_above_vm (a NaN Vm included), an APD90 above 0.9 bcl, or an
+ * intermittent rhythm (0 < n_eligible < evaluated, evaluated = the paces
+ * from first_pace on); else 0. Host only, no device work. */
+int cep_population_late_mask(const cep_biomarkers_t *recs, int n, double refine_above_vm, double bcl, int evaluated,
+                             int *mask);
 
 /* ------------------------------------------------- protocol variants */
 /* One pace of a dynamic (S1-S1) restitution run, as apdr_bench.cpp:211
