@@ -25,6 +25,7 @@
 // produced instance i's record.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -173,7 +174,7 @@ extern "C" int cep_population_run(const cep_population_job_t *j, cep_biomarkers_
   }
   if (refine) {  // 3. whatever the screening missed
     std::vector<int> late, mask(j->n);
-    const int evaluated = j->first_pace >= 0 ? j->n_pace - j->first_pace : 0;
+    const int evaluated = j->first_pace >= 0 ? std::max(0, j->n_pace - j->first_pace) : 0;
     if ((rc = cep_population_late_mask(out, j->n, j->refine_above_vm, j->bcl, evaluated, mask.data()))) return rc;
     for (int i = 0; i < j->n; ++i)
       if (how[i] == 0 && mask[i]) late.push_back(i);
